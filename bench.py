@@ -1,0 +1,394 @@
+#!/usr/bin/env python
+"""Throughput of the fused D3Q19 TRT stream-collide step on B200.
+
+Workload (one "step" = one fused pull-stream + TRT collide pass over the
+grid): periodic D3Q19 Taylor-Green vortex, 256^3 nodes, TRT magic parameter
+1/4, nu = 0.01, u0 = 0.05, rho0 = 1, populations in HBM (default storage:
+FP32 deviations f - w_q; --storage picks f64 | f32 | f32dev | f16dev |
+bf16dev).  Moments are written at the check cadence (every 100 steps), not
+every step.  Each population buffer (1.27 GB in FP32) is larger than the
+126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N --steps K --warmup W --storage S]
+  python bench.py --impl reference ...   # the reference's CPU path (oracle port)
+
+Prints one JSON line (rank 0).  `value` is whole-job MLUPS with populations
+resident in HBM; `e2e` is the same metric through the public API with the
+initial populations copied from pinned host memory and the final moments
+read back inside the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "MLUPS & % HBM roofline per lattice/precision; time-to-steady vs plain"
+N_GRID = 256
+NU, LAMBDA, U0 = 0.01, 0.25, 0.05
+CHECK_EVERY = 100
+FALLBACK_HBM_GBS = 6650.0
+
+STORAGES = {
+    # name: (torch dtype name, deviation, bytes per population, kb dtype label)
+    "f64": ("float64", False, 8, "f64"),
+    "f32": ("float32", False, 4, "f32"),
+    "f32dev": ("float32", True, 4, "f32 (f-w)"),
+    "f16dev": ("float16", True, 2, "f16 (f-w)"),
+    "bf16dev": ("bfloat16", True, 2, "bf16 (f-w)"),
+}
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_launch(storage):
+    """DRAM bytes per launch of the fused TRT kernel from the committed ncu
+    summary (profiles/d3q19_trt_tgv_traffic.txt: lines `storage bytes`)."""
+    p = ROOT / "profiles" / "d3q19_trt_tgv_traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == storage and not line.startswith("#"):
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(gpus):
+    import torch
+    import torch.distributed as dist
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local = _env_int("LOCAL_RANK", 0)
+    if world > 1:
+        from datetime import timedelta
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- CPU arm --
+
+def cpu_reference_mlups(n, steps_cap, budget_s, threads):
+    """The oracle port (C restatement of the reference's CPU path, OpenMP)
+    on a periodic n^3 D3Q19 TRT Taylor-Green vortex.  Returns (MLUPS,
+    steps, seconds, nz) timed after one warm-up step; the z extent is cut to
+    keep one step near budget_s/steps_cap seconds on slow hosts."""
+    import numpy as np
+    import __graft_entry__ as graft
+    orc = graft.load_oracle()
+    pkg = graft.load_package()
+    orc.set_threads(threads)
+    nz = n
+    plane = pkg.drivers.taylor_green_3d_populations(n, U0, Nz=1)
+    f = np.ascontiguousarray(np.broadcast_to(plane, (19, nz, n, n)))
+    g = np.empty_like(f)
+    sp, sm = orc.trt_rates(NU, LAMBDA)
+    t0 = time.perf_counter()
+    orc.fused_trt_3d(g, f, None, None, sp, sm, (1, 1, 1))
+    t1 = time.perf_counter() - t0
+    per_step_budget = budget_s / max(1, steps_cap)
+    if t1 > per_step_budget and nz > 8:
+        nz = max(8, int(nz * per_step_budget / t1))
+        f = np.ascontiguousarray(np.broadcast_to(plane, (19, nz, n, n)))
+        g = np.empty_like(f)
+        orc.fused_trt_3d(g, f, None, None, sp, sm, (1, 1, 1))
+    steps = 0
+    t0 = time.perf_counter()
+    while steps < steps_cap:
+        orc.fused_trt_3d(g, f, None, None, sp, sm, (1, 1, 1))
+        f, g = g, f
+        steps += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return steps * n * n * nz / dt / 1e6, steps, dt, nz
+
+
+def run_reference(args):
+    rank, world, _ = dist_setup(args.gpus)
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    mlups, steps, dt, nz = cpu_reference_mlups(N_GRID, max(1, args.steps), 150.0, threads)
+    sample = (f"periodic D3Q19 TRT Taylor-Green {N_GRID}x{N_GRID}x{nz} (z cut to bound the run), "
+              f"{steps} steps after 1 warm-up, FP64, C restatement of the reference CPU path "
+              f"(Julia reference not runnable here), OpenMP {threads} threads")
+    line = {"impl": "reference", "metric": METRIC, "value": round(mlups, 3), "unit": "MLUPS",
+            "n_gpus": args.gpus, "steps": steps, "warmup": 1, "ms_per_step": round(1e3 * dt / steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"D3Q19 TRT periodic Taylor-Green {N_GRID}^3, Lambda=1/4, "
+                                   f"nu={NU}, u0={U0}", "grid": [N_GRID, N_GRID, N_GRID],
+                       "storage": "f64", "parallelism": "host OpenMP"},
+            "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": threads,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm --
+
+def run_gpu(args):
+    import torch
+    import __graft_entry__ as graft
+
+    rank, world, local = dist_setup(args.gpus)
+    pkg = graft.load_package()
+    pkg._lib.load()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    tname, deviation, bpp, dlabel = STORAGES[args.storage]
+    dtype = getattr(torch, tname)
+    n = args.grid
+    nodes = n ** 3
+    fd = torch.float64 if dtype == torch.float64 else torch.float32
+
+    # initial populations: one z-plane on the host, extruded on the device
+    plane = torch.from_numpy(pkg.drivers.taylor_green_3d_populations(n, U0, Nz=1)).to(dev)
+    f64 = plane.expand(19, n, n, n)
+    f_in = torch.empty((19, n, n, n), dtype=dtype, device=dev)
+    if dtype == torch.float64 and not deviation:
+        f_in.copy_(f64)
+    else:
+        pkg.convert_populations(f_in, _extrude(plane, n), dst_deviation=deviation)
+    del f64
+    f_out = torch.empty_like(f_in)
+    mom = [torch.empty((n, n, n), dtype=fd, device=dev) for _ in range(4)]
+    none4 = (None, None, None, None)
+    stream = torch.cuda.current_stream()
+
+    def step(s, fi, fo):
+        m = mom if (s + 1) % CHECK_EVERY == 0 else none4
+        pkg.fused_trt_step_3d_(fo, fi, *m, None, n, n, n, NU, LAMBDA, periodic=(1, 1, 1),
+                               deviation=deviation)
+
+    a, b = f_in, f_out
+    for s in range(args.warmup):
+        step(s, a, b)
+        a, b = b, a
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for s in range(args.steps):
+        step(s, a, b)
+        a, b = b, a
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms, world)
+    value = world * nodes * args.steps / (ms_max * 1e-3) / 1e6
+    kernel_ms = ms / args.steps
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty((19, n, n, n), dtype=dtype, pin_memory=True)
+        host.copy_(a)
+        out_host = [torch.empty((n, n, n), dtype=fd, pin_memory=True) for _ in range(4)]
+        torch.cuda.synchronize()
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        a.copy_(host, non_blocking=True)
+        for s in range(args.steps):
+            last = s == args.steps - 1
+            m = mom if last else none4
+            pkg.fused_trt_step_3d_(b, a, *m, None, n, n, n, NU, LAMBDA, periodic=(1, 1, 1),
+                                   deviation=deviation)
+            a, b = b, a
+        for h, d in zip(out_host, mom):
+            h.copy_(d, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        ems = max_over_ranks(e0.elapsed_time(e1), world)
+        h2d = host.numel() * host.element_size()
+        d2h = sum(t.numel() * t.element_size() for t in out_host)
+        e2e = {"value": round(world * nodes * args.steps / (ems * 1e-3) / 1e6, 1), "unit": "MLUPS",
+               "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
+               "note": (f"timed: pinned host->device copy of the initial populations, {args.steps} "
+                        "fused steps through the public API, device->host copy of rho,u; bytes "
+                        "per step = total / steps")}
+        del host, out_host
+
+    peak, peak_kind = hbm_peak()
+    alg_bytes = 2 * 19 * bpp * nodes
+    achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
+    traffic = traffic_per_launch(args.storage)
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            threads = os.cpu_count() or 1
+            mlups, steps, dt, nz = cpu_reference_mlups(n, 20, 20.0, threads)
+            cpu = {"value": round(mlups, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
+                   "sample": (f"{steps} steps of the periodic D3Q19 TRT Taylor-Green on "
+                              f"{n}x{n}x{nz} nodes, FP64, C restatement of the reference CPU path, "
+                              f"{dt:.1f} s")}
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dlabel,
+            "data": "synthetic",
+            "config": {"workload": f"D3Q19 TRT periodic Taylor-Green {n}^3, Lambda=1/4, nu={NU}, "
+                                   f"u0={U0}, rho0=1", "grid": [n, n, n], "storage": args.storage,
+                       "moments": f"written every {CHECK_EVERY} steps",
+                       "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                         if peak_kind == "measured" else "fallback 6.65 TB/s",
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def _extrude(plane, n):
+    import torch
+    out = torch.empty((19, n, n, n), dtype=plane.dtype, device=plane.device)
+    out.copy_(plane.expand(19, n, n, n))
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--storage", default="f32dev", choices=sorted(STORAGES))
+    ap.add_argument("--grid", type=int, default=N_GRID)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,245 @@
+/*
+ * krakenb200.h -- C ABI of the B200 stream-collide library (libkrakenb200.so).
+ *
+ * Each entry point replaces one Kraken.jl kernel wrapper on its
+ * stream-collide path; the comment above it cites the reference function
+ * (file:line, paths inside the Kraken.jl repository) whose argument meaning
+ * and error behaviour it keeps.  A Julia backend binds these with `ccall`
+ * (see INTEGRATION.md); the Python host layer in krakenn.jl_b200/ binds them
+ * with ctypes.
+ *
+ * Conventions shared by every entry point
+ *   - Arrays are raw DEVICE pointers owned by the caller, in Julia
+ *     column-major order with 0-based indices:
+ *        D2Q9   f[i + Nx*(j + Ny*q)],         fields  a[i + Nx*j]
+ *        D3Q19  f[i + Nx*(j + Ny*(k + Nz*q))], fields  a[i + Nx*(j + Ny*k)]
+ *     (q is the reference's population index minus one).  A CuArray of
+ *     size (Nx, Ny, 9) passes its pointer unchanged.
+ *   - Masks (`is_solid`) are one byte per node (Julia Bool); NULL means "no
+ *     solid node", which skips the mask read.
+ *   - `dtype` selects the population storage (kb_dtype).  Macroscopic
+ *     fields (rho, ux, ...) are double for KB_F64 and float otherwise.
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).  Calls are
+ *     stream-ordered and asynchronous; nothing synchronises unless the entry
+ *     point says so.  There are no internal host threads.
+ *   - Return value: KB_OK (0) or a negative kb_status.  The message of the
+ *     last failure on the calling thread is kb_last_error().  There is no
+ *     fallback: an unsupported combination is an error, never a CPU path.
+ *   - Operations are in place (the reference's `!` functions); the caller
+ *     swaps f_in/f_out between steps, as the reference drivers do.
+ */
+#ifndef KRAKENB200_H
+#define KRAKENB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    KB_OK = 0,
+    KB_ERR_ARG = -1,         /* bad pointer, size or parameter              */
+    KB_ERR_UNSUPPORTED = -2, /* dtype / option not available for this op    */
+    KB_ERR_CUDA = -3,        /* a CUDA call failed (message says which)     */
+    KB_ERR_TIMEOUT = -4,     /* a bounded device wait ran out               */
+    KB_ERR_NONFINITE = -5,   /* a reduction met NaN or Inf                  */
+    KB_ERR_NOMEM = -6        /* device allocation of a handle failed        */
+} kb_status;
+
+typedef enum {
+    KB_F64 = 0,      /* double populations (reference Float64 semantics)   */
+    KB_F32 = 1,      /* float populations (reference Float32 semantics)    */
+    KB_F32_DEV = 2,  /* float deviations f - w_q, FP32 collision           */
+    KB_F16_DEV = 3,  /* IEEE half deviations f - w_q, FP32 collision       */
+    KB_BF16_DEV = 4  /* bfloat16 deviations f - w_q, FP32 collision        */
+} kb_dtype;
+
+/* Library version string ("krakenb200 <semver> sm_100a"). */
+const char *kb_version(void);
+/* Message of the last error on the calling thread ("" if none). */
+const char *kb_last_error(void);
+/* Block until all work queued on `stream` is done; reports any pending
+ * asynchronous CUDA error.  KernelAbstractions.synchronize(backend). */
+int kb_sync(void *stream);
+
+/* ---------------------------------------------------------------- D2Q9 -- */
+
+/* stream_2d!(f_out, f_in, Nx, Ny)  -- src/kernels/collide_stream_2d.jl:77 */
+int kb_stream_2d(void *f_out, const void *f_in, int Nx, int Ny, int dtype, void *stream);
+
+/* collide_2d!(f, is_solid, omega)  -- src/kernels/collide_stream_2d.jl:96 */
+int kb_collide_2d(void *f, const uint8_t *is_solid, int Nx, int Ny, double omega, int dtype,
+                  void *stream);
+
+/* apply_zou_he_north_2d!(f, u_wall_x, Nx, Ny) -- src/kernels/boundary_2d.jl:56 */
+int kb_apply_zou_he_north_2d(void *f, double u_wall_x, int Nx, int Ny, int dtype, void *stream);
+
+/* apply_zou_he_south_2d!(f, u_wall_x, Nx) -- src/kernels/boundary_2d.jl:163 */
+int kb_apply_zou_he_south_2d(void *f, double u_wall_x, int Nx, int Ny, int dtype, void *stream);
+
+/* apply_zou_he_west_2d!(f, u_in, Nx, Ny) -- src/kernels/boundary_2d.jl:198 */
+int kb_apply_zou_he_west_2d(void *f, double u_in, int Nx, int Ny, int dtype, void *stream);
+
+/* apply_zou_he_pressure_east_2d!(f, Nx, Ny; rho_out) -- src/kernels/boundary_2d.jl:237 */
+int kb_apply_zou_he_pressure_east_2d(void *f, int Nx, int Ny, double rho_out, int dtype,
+                                     void *stream);
+
+/* apply_zou_he_pressure_west_2d!(f, Nx, Ny; rho_in) -- src/kernels/boundary_2d.jl:295 */
+int kb_apply_zou_he_pressure_west_2d(void *f, int Nx, int Ny, double rho_in, int dtype,
+                                     void *stream);
+
+/* apply_extrapolate_east_2d!(f, Nx, Ny) -- src/kernels/boundary_2d.jl:319 */
+int kb_apply_extrapolate_east_2d(void *f, int Nx, int Ny, int dtype, void *stream);
+
+/* apply_bounce_back_wall_2d!(f, Nx, Ny, side) -- src/kernels/boundary_2d.jl:117.
+ * wall_id: 1 south, 2 west, 3 east, 4 north (the reference's Int32 codes). */
+int kb_apply_bounce_back_wall_2d(void *f, int Nx, int Ny, int wall_id, int dtype, void *stream);
+
+/* compute_macroscopic_2d!(rho, ux, uy, f) -- src/kernels/macroscopic.jl:32 */
+int kb_compute_macroscopic_2d(void *rho, void *ux, void *uy, const void *f, int Nx, int Ny,
+                              int dtype, void *stream);
+
+/* fused_bgk_step!(f_out, f_in, rho, ux, uy, is_solid, Nx, Ny, omega)
+ *   -- src/kernels/fused_bgk_2d.jl:67 */
+int kb_fused_bgk_step(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                      const uint8_t *is_solid, int Nx, int Ny, double omega, int dtype,
+                      void *stream);
+
+/* trt_rates(nu; Lambda) -> (s_plus, s_minus) -- src/kernels/fused_trt_2d.jl:129 */
+int kb_trt_rates(double nu, double Lambda, double *s_plus, double *s_minus);
+
+/* fused_trt_step!(f_out, f_in, rho, ux, uy, is_solid, Nx, Ny, nu; Lambda)
+ *   -- src/kernels/fused_trt_2d.jl:145 */
+int kb_fused_trt_step(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                      const uint8_t *is_solid, int Nx, int Ny, double nu, double Lambda, int dtype,
+                      void *stream);
+
+/* aa_even_step!(f, is_solid, Nx, Ny, omega) -- src/kernels/aa_bgk_2d.jl:125 */
+int kb_aa_even_step(void *f, const uint8_t *is_solid, int Nx, int Ny, double omega, int dtype,
+                    void *stream);
+
+/* aa_odd_step!(f, is_solid, Nx, Ny, omega) -- src/kernels/aa_bgk_2d.jl:138 */
+int kb_aa_odd_step(void *f, const uint8_t *is_solid, int Nx, int Ny, double omega, int dtype,
+                   void *stream);
+
+/* collide_mrt_2d!(f, is_solid, nu; s_e, s_eps, s_q) -- src/kernels/collide_mrt_2d.jl:118 */
+int kb_collide_mrt_2d(void *f, const uint8_t *is_solid, int Nx, int Ny, double nu, double s_e,
+                      double s_eps, double s_q, int dtype, void *stream);
+
+/* stream_fully_periodic_2d!(f_out, f_in, Nx, Ny) -- src/kernels/stream_periodic_2d.jl:112 */
+int kb_stream_fully_periodic_2d(void *f_out, const void *f_in, int Nx, int Ny, int dtype,
+                                void *stream);
+
+/* stream_periodic_x_wall_y_2d!(f_out, f_in, Nx, Ny) -- src/kernels/stream_periodic_2d.jl:71 */
+int kb_stream_periodic_x_wall_y_2d(void *f_out, const void *f_in, int Nx, int Ny, int dtype,
+                                   void *stream);
+
+/* One cavity step of run_cavity_2d (src/drivers/basic.jl:121-136) in ONE
+ * launch: stream_2d! -> apply_zou_he_north_2d! -> collide_2d! ->
+ * compute_macroscopic_2d!.  Every stage is node-local after the pull, so the
+ * fused step gives the same bits as the four reference launches. */
+int kb_cavity_step_2d(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                      const uint8_t *is_solid, int Nx, int Ny, double omega, double u_lid,
+                      int dtype, void *stream);
+
+/* fused_natconv_step!(f_out, f_in, g_out, g_in, Temp, Nx, Ny, omega_f,
+ *   omega_T, beta_g, T_ref_buoy, T_hot, T_cold) -- src/kernels/fused_thermal_2d.jl:251 */
+int kb_fused_natconv_step(void *f_out, const void *f_in, void *g_out, const void *g_in,
+                          void *Temp, int Nx, int Ny, double omega_f, double omega_T,
+                          double beta_g, double T_ref_buoy, double T_hot, double T_cold,
+                          int dtype, void *stream);
+
+/* fused_natconv_vt_step!(..., nu_ref, T0_visc, alpha_visc, omega_T, beta_g,
+ *   T_ref_buoy, T_hot, T_cold) -- src/kernels/fused_thermal_2d.jl:268 */
+int kb_fused_natconv_vt_step(void *f_out, const void *f_in, void *g_out, const void *g_in,
+                             void *Temp, int Nx, int Ny, double nu_ref, double T0_visc,
+                             double alpha_visc, double omega_T, double beta_g, double T_ref_buoy,
+                             double T_hot, double T_cold, int dtype, void *stream);
+
+/* compute_temperature_2d!(Temp, g) -- src/kernels/thermal_2d.jl:113 */
+int kb_compute_temperature_2d(void *Temp, const void *g, int Nx, int Ny, int dtype, void *stream);
+
+/* --------------------------------------------------------------- D3Q19 -- */
+
+/* stream_3d!(f_out, f_in, Nx, Ny, Nz) -- src/kernels/collide_stream_3d.jl:119 */
+int kb_stream_3d(void *f_out, const void *f_in, int Nx, int Ny, int Nz, int dtype, void *stream);
+
+/* collide_3d!(f, is_solid, omega) -- src/kernels/collide_stream_3d.jl:137 */
+int kb_collide_3d(void *f, const uint8_t *is_solid, int Nx, int Ny, int Nz, double omega,
+                  int dtype, void *stream);
+
+/* _apply_zou_he_velocity_3d!(f, face, idx_fixed, u_n, u_t1, u_t2)
+ *   -- src/kernels/boundary_3d.jl:154-223, 300-305.
+ * face: 0 west, 1 east, 2 south, 3 north, 4 bottom, 5 top; the fixed index
+ * is the face's own (0 or N-1). */
+int kb_apply_zou_he_velocity_3d(void *f, int Nx, int Ny, int Nz, int face, double u_normal,
+                                double u_tang1, double u_tang2, int dtype, void *stream);
+
+/* apply_zou_he_top_3d!(f, u_wall_x, Nx, Ny, Nz) -- src/kernels/boundary_3d.jl:326 */
+int kb_apply_zou_he_top_3d(void *f, double u_wall_x, int Nx, int Ny, int Nz, int dtype,
+                           void *stream);
+
+/* _apply_zou_he_pressure_3d!(f, face, idx_fixed, rho_out)
+ *   -- src/kernels/boundary_3d.jl:232-288, 307-312 */
+int kb_apply_zou_he_pressure_3d(void *f, int Nx, int Ny, int Nz, int face, double rho_out,
+                                int dtype, void *stream);
+
+/* compute_macroscopic_3d!(rho, ux, uy, uz, f) -- src/kernels/macroscopic.jl:75 */
+int kb_compute_macroscopic_3d(void *rho, void *ux, void *uy, void *uz, const void *f, int Nx,
+                              int Ny, int Nz, int dtype, void *stream);
+
+/* Fused D3Q19 TRT step: the reference's 3D TRT kernel
+ * fused_trt_libb_v2_step_3d!(f_out, f_in, rho, ux, uy, uz, is_solid, ...,
+ * Nx, Ny, Nz, nu; Lambda) (src/kernels/li_bb_3d_v2.jl:31-42; bricks
+ * PullHalfwayBB_3D, SolidInert_3D, Moments_3D, CollideTRTDirect_3D,
+ * WriteMoments_3D in src/kernels/dsl/bricks_3d.jl:64-230, 476-483) with no
+ * interpolated-wall link flagged.
+ *   periodic: bit 0 = x, bit 1 = y, bit 2 = z wrap instead of half-way
+ *             bounce-back (bit 2 alone = PullHalfwayBB_3D{true}).
+ *   rho/ux/uy/uz: NULL skips the moment write (all four NULL or none).
+ *   dtype: any kb_dtype.  KB_F64/KB_F32 follow the reference arithmetic;
+ *   the *_DEV storages hold f - w_q and collide in FP32. */
+int kb_fused_trt_step_3d(void *f_out, const void *f_in, void *rho, void *ux, void *uy, void *uz,
+                         const uint8_t *is_solid, int Nx, int Ny, int Nz, double nu,
+                         double Lambda, int periodic, int dtype, void *stream);
+
+/* stream_periodic_xz_movingwall_y_3d!(f_out, f_in, Ub, Ut, Nx, Ny, Nz; rho_w)
+ *   -- src/kernels/stream_periodic_3d.jl:178 */
+int kb_stream_periodic_xz_movingwall_y_3d(void *f_out, const void *f_in, double Ub, double Ut,
+                                          double rho_w, int Nx, int Ny, int Nz, int dtype,
+                                          void *stream);
+
+/* ------------------------------------------------- precision utilities -- */
+
+/* Convert populations between storages.  KB_*_DEV storages hold f - w_q; the
+ * others hold f.  lattice_q is 9 (D2Q9) or 19 (D3Q19); n_nodes is the node
+ * count of one population plane.  src and dst must not overlap.  No
+ * reference counterpart (the reference stores plain f). */
+int kb_convert_populations(void *dst, int dst_dtype, const void *src, int src_dtype,
+                           int lattice_q, size_t n_nodes, void *stream);
+
+/* ---------------------------------------------------- FP64 reductions -- */
+
+/* Total mass sum_q sum_nodes f (FP64, compensated), written to *out_host.
+ * Synchronises `stream`.  Deviation storages add back w_q.  Returns
+ * KB_ERR_NONFINITE (and still writes the sum) if any population is not
+ * finite.  Replaces the host `sum(Array(rho))` of the reference drivers
+ * (e.g. test/test_lbm_basic.jl:85-96). */
+int kb_mass(const void *f, int lattice_q, size_t n_nodes, int dtype, double *out_host,
+            void *stream);
+
+/* Steady residual r_u = ||u - u_prev||_2 / ||u||_2 over fluid nodes (FP64
+ * accumulation), written to *out_host; synchronises `stream`.  uz/uz_prev
+ * are NULL in 2D.  Fields are double for KB_F64, float otherwise.  The
+ * definition is src/drivers/gnf_periodic_steady.jl:186-194. */
+int kb_residual(const void *ux, const void *uy, const void *uz, const void *ux_prev,
+                const void *uy_prev, const void *uz_prev, const uint8_t *is_solid,
+                size_t n_nodes, int dtype, double *out_host, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KRAKENB200_H */

@@ -1,0 +1,121 @@
+"""ctypes binding of libkrakenb200.so (the C ABI in include/krakenb200.h).
+
+The library is loaded from this directory only.  If it is missing or cannot
+be loaded, every entry point raises: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libkrakenb200.so"
+
+KB_OK = 0
+KB_ERR_ARG = -1
+KB_ERR_UNSUPPORTED = -2
+KB_ERR_CUDA = -3
+KB_ERR_TIMEOUT = -4
+KB_ERR_NONFINITE = -5
+KB_ERR_NOMEM = -6
+
+KB_F64, KB_F32, KB_F32_DEV, KB_F16_DEV, KB_BF16_DEV = 0, 1, 2, 3, 4
+
+_vp, _cvp, _u8p = C.c_void_p, C.c_void_p, C.c_void_p
+_i, _d, _sz = C.c_int, C.c_double, C.c_size_t
+_dp = C.POINTER(C.c_double)
+
+# name -> argtypes (restype is int unless listed in _RESTYPES)
+SIGNATURES: dict[str, list] = {
+    "kb_version": [],
+    "kb_last_error": [],
+    "kb_sync": [_vp],
+    "kb_stream_2d": [_vp, _cvp, _i, _i, _i, _vp],
+    "kb_collide_2d": [_vp, _u8p, _i, _i, _d, _i, _vp],
+    "kb_apply_zou_he_north_2d": [_vp, _d, _i, _i, _i, _vp],
+    "kb_apply_zou_he_south_2d": [_vp, _d, _i, _i, _i, _vp],
+    "kb_apply_zou_he_west_2d": [_vp, _d, _i, _i, _i, _vp],
+    "kb_apply_zou_he_pressure_east_2d": [_vp, _i, _i, _d, _i, _vp],
+    "kb_apply_zou_he_pressure_west_2d": [_vp, _i, _i, _d, _i, _vp],
+    "kb_apply_extrapolate_east_2d": [_vp, _i, _i, _i, _vp],
+    "kb_apply_bounce_back_wall_2d": [_vp, _i, _i, _i, _i, _vp],
+    "kb_compute_macroscopic_2d": [_vp, _vp, _vp, _cvp, _i, _i, _i, _vp],
+    "kb_fused_bgk_step": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _i, _vp],
+    "kb_trt_rates": [_d, _d, _dp, _dp],
+    "kb_fused_trt_step": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _d, _i, _vp],
+    "kb_aa_even_step": [_vp, _u8p, _i, _i, _d, _i, _vp],
+    "kb_aa_odd_step": [_vp, _u8p, _i, _i, _d, _i, _vp],
+    "kb_collide_mrt_2d": [_vp, _u8p, _i, _i, _d, _d, _d, _d, _i, _vp],
+    "kb_stream_fully_periodic_2d": [_vp, _cvp, _i, _i, _i, _vp],
+    "kb_stream_periodic_x_wall_y_2d": [_vp, _cvp, _i, _i, _i, _vp],
+    "kb_cavity_step_2d": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _d, _i, _vp],
+    "kb_fused_natconv_step": [_vp, _cvp, _vp, _cvp, _vp, _i, _i, _d, _d, _d, _d, _d, _d, _i, _vp],
+    "kb_fused_natconv_vt_step": [_vp, _cvp, _vp, _cvp, _vp, _i, _i, _d, _d, _d, _d, _d, _d, _d,
+                                 _d, _i, _vp],
+    "kb_compute_temperature_2d": [_vp, _cvp, _i, _i, _i, _vp],
+    "kb_stream_3d": [_vp, _cvp, _i, _i, _i, _i, _vp],
+    "kb_collide_3d": [_vp, _u8p, _i, _i, _i, _d, _i, _vp],
+    "kb_apply_zou_he_velocity_3d": [_vp, _i, _i, _i, _i, _d, _d, _d, _i, _vp],
+    "kb_apply_zou_he_top_3d": [_vp, _d, _i, _i, _i, _i, _vp],
+    "kb_apply_zou_he_pressure_3d": [_vp, _i, _i, _i, _i, _d, _i, _vp],
+    "kb_compute_macroscopic_3d": [_vp, _vp, _vp, _vp, _cvp, _i, _i, _i, _i, _vp],
+    "kb_fused_trt_step_3d": [_vp, _cvp, _vp, _vp, _vp, _vp, _u8p, _i, _i, _i, _d, _d, _i, _i,
+                             _vp],
+    "kb_stream_periodic_xz_movingwall_y_3d": [_vp, _cvp, _d, _d, _d, _i, _i, _i, _i, _vp],
+    "kb_convert_populations": [_vp, _i, _cvp, _i, _i, _sz, _vp],
+    "kb_mass": [_cvp, _i, _sz, _i, _dp, _vp],
+    "kb_residual": [_cvp, _cvp, _cvp, _cvp, _cvp, _cvp, _u8p, _sz, _i, _dp, _vp],
+}
+_RESTYPES = {"kb_version": C.c_char_p, "kb_last_error": C.c_char_p}
+
+
+class KrakenError(RuntimeError):
+    """A library call failed (CUDA error, timeout, non-finite reduction...)."""
+
+    def __init__(self, name: str, code: int, msg: str):
+        super().__init__(f"{name} failed ({code}): {msg}")
+        self.code = code
+
+
+class KrakenArgumentError(KrakenError, ValueError):
+    """Bad argument or unsupported combination (the reference's ArgumentError)."""
+
+
+_LIB = None
+_LOAD_ERROR: str | None = None
+
+
+def load() -> C.CDLL:
+    """Load the shared library once; raise if it is not there."""
+    global _LIB, _LOAD_ERROR
+    if _LIB is not None:
+        return _LIB
+    if not LIB_PATH.exists():
+        _LOAD_ERROR = (f"{LIB_PATH} is missing: build it with `python krakenn.jl_b200/build.py` "
+                       "(the B200 path has no CPU fallback)")
+        raise RuntimeError(_LOAD_ERROR)
+    lib = C.CDLL(str(LIB_PATH))
+    for name, argt in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argt
+        fn.restype = _RESTYPES.get(name, C.c_int)
+    _LIB = lib
+    return lib
+
+
+def exported_symbols() -> list[str]:
+    return list(SIGNATURES)
+
+
+def call(name: str, *args) -> int:
+    lib = load()
+    rc = getattr(lib, name)(*args)
+    if rc != KB_OK:
+        msg = lib.kb_last_error().decode(errors="replace")
+        if rc in (KB_ERR_ARG, KB_ERR_UNSUPPORTED):
+            raise KrakenArgumentError(name, rc, msg)
+        raise KrakenError(name, rc, msg)
+    return rc
+
+
+def version() -> str:
+    return load().kb_version().decode()

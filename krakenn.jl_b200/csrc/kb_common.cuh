@@ -1,0 +1,87 @@
+// kb_common.cuh -- shared definitions of the B200 stream-collide library.
+//
+// Layout (Julia column-major, 0-based):
+//   D2Q9   f[i + Nx*(j + Ny*q)]
+//   D3Q19  f[i + Nx*(j + Ny*(k + Nz*q))]
+// Populations q are 0-based (Kraken.jl's q minus one).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "../../include/krakenb200.h"
+
+namespace kb {
+
+// Error reporting (kb_error.cu).
+int set_error(int code, const char *fmt, ...);
+int check_launch(const char *what);
+void clear_error();
+
+// ---------------------------------------------------------------- lattice --
+// D2Q9 (src/lattice/d2q9.jl:19-29) and D3Q19 (src/lattice/d3q19.jl:13-47).
+__host__ __device__ constexpr double w9(int q) {
+    return q == 0 ? 4.0 / 9.0 : (q < 5 ? 1.0 / 9.0 : 1.0 / 36.0);
+}
+__host__ __device__ constexpr double w19(int q) {
+    return q == 0 ? 1.0 / 3.0 : (q < 7 ? 1.0 / 18.0 : 1.0 / 36.0);
+}
+__host__ __device__ constexpr int cx19(int q) {
+    constexpr int c[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+    return c[q];
+}
+__host__ __device__ constexpr int cy19(int q) {
+    constexpr int c[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
+    return c[q];
+}
+__host__ __device__ constexpr int cz19(int q) {
+    constexpr int c[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
+    return c[q];
+}
+__host__ __device__ constexpr int opp19(int q) {
+    constexpr int o[19] = {0, 2, 1, 4, 3, 6, 5, 10, 9, 8, 7, 14, 13, 12, 11, 18, 17, 16, 15};
+    return o[q];
+}
+
+// ---------------------------------------------------------------- storage --
+// Storage codecs.  Plain storages (double, float) hold f.  Deviation
+// storages hold d = f - w_q and are decoded to float.
+template <typename R> struct Dev;
+template <> struct Dev<float> {
+    static __device__ __forceinline__ float ld(float r) { return r; }
+    static __device__ __forceinline__ float st(float d) { return d; }
+};
+template <> struct Dev<__half> {
+    static __device__ __forceinline__ float ld(__half r) { return __half2float(r); }
+    static __device__ __forceinline__ __half st(float d) { return __float2half_rn(d); }
+};
+template <> struct Dev<__nv_bfloat16> {
+    static __device__ __forceinline__ float ld(__nv_bfloat16 r) { return __bfloat162float(r); }
+    static __device__ __forceinline__ __nv_bfloat16 st(float d) { return __float2bfloat16_rn(d); }
+};
+
+inline size_t dtype_bytes(int dtype) {
+    switch (dtype) {
+        case KB_F64: return 8;
+        case KB_F32: return 4;
+        case KB_F32_DEV: return 4;
+        case KB_F16_DEV: return 2;
+        case KB_BF16_DEV: return 2;
+        default: return 0;
+    }
+}
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+
+}  // namespace kb
+
+#define KB_REQUIRE(cond, ...)                                        \
+    do {                                                             \
+        if (!(cond)) return ::kb::set_error(KB_ERR_ARG, __VA_ARGS__); \
+    } while (0)

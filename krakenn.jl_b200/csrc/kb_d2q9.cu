@@ -1,0 +1,915 @@
+// kb_d2q9.cu -- D2Q9 kernels with the reference's arithmetic.
+//
+// Compiled with --fmad=false: every multiply and add rounds separately, in
+// the order Kraken.jl writes them, so a double run reproduces the
+// reference's CPU Float64 path bit for bit (and a float run its Float32
+// path).  Each kernel names the reference kernel it restates.
+//
+// Thread mapping: one thread per node, blockDim.x along x (the unit-stride
+// axis of every population plane), so each population load/store of a warp
+// is one contiguous run of 32 elements (shifted by one for the x-pulls).
+#include "kb_common.cuh"
+
+namespace kb {
+namespace d2 {
+
+constexpr int BX = 128;
+
+template <typename T>
+struct Grid2 {
+    int Nx, Ny;
+    size_t plane;  // Nx*Ny
+    __device__ __forceinline__ size_t at(int i, int j) const { return (size_t)i + (size_t)Nx * j; }
+};
+
+// feq_2d(Val(q), rho, ux, uy, usq): src/kernels/equilibrium_helpers.jl:8-50
+template <typename T>
+__device__ __forceinline__ T feq_poly(T w, T rho, T cu, T usq) {
+    return w * rho * (T(1) + T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq);
+}
+
+template <typename T>
+__device__ __forceinline__ void feq_all(T rho, T ux, T uy, T usq, T *feq) {
+    const T w0 = T(4.0 / 9.0), w1 = T(1.0 / 9.0), w5 = T(1.0 / 36.0);
+    feq[0] = w0 * rho * (T(1) - T(1.5) * usq);
+    feq[1] = feq_poly(w1, rho, ux, usq);
+    feq[2] = feq_poly(w1, rho, uy, usq);
+    feq[3] = feq_poly(w1, rho, -ux, usq);
+    feq[4] = feq_poly(w1, rho, -uy, usq);
+    feq[5] = feq_poly(w5, rho, ux + uy, usq);
+    feq[6] = feq_poly(w5, rho, -ux + uy, usq);
+    feq[7] = feq_poly(w5, rho, -ux - uy, usq);
+    feq[8] = feq_poly(w5, rho, ux - uy, usq);
+}
+
+// moments_2d: src/kernels/equilibrium_helpers.jl:54-61
+template <typename T>
+__device__ __forceinline__ void moments(const T *p, T &rho, T &ux, T &uy) {
+    rho = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8];
+    T inv = T(1) / rho;
+    ux = (p[1] - p[3] + p[5] - p[6] - p[7] + p[8]) * inv;
+    uy = (p[2] - p[4] + p[5] + p[6] - p[7] - p[8]) * inv;
+}
+
+// Pull with half-way bounce-back on the four edges:
+// src/kernels/collide_stream_2d.jl:12-23 (same in fused_bgk_2d.jl:13-24).
+template <typename T>
+__device__ __forceinline__ void pull_bb(const T *__restrict__ f, const Grid2<T> &g, int i, int j,
+                                        T *fp) {
+    const int Nx = g.Nx, Ny = g.Ny;
+    const size_t P = g.plane;
+    const bool w = i > 0, e = i < Nx - 1, s = j > 0, n = j < Ny - 1;
+    const size_t c = g.at(i, j);
+    fp[0] = f[c];
+    fp[1] = w ? f[c - 1 + 1 * P] : f[c + 3 * P];
+    fp[2] = s ? f[c - Nx + 2 * P] : f[c + 4 * P];
+    fp[3] = e ? f[c + 1 + 3 * P] : f[c + 1 * P];
+    fp[4] = n ? f[c + Nx + 4 * P] : f[c + 2 * P];
+    fp[5] = (w && s) ? f[c - 1 - Nx + 5 * P] : f[c + 7 * P];
+    fp[6] = (e && s) ? f[c + 1 - Nx + 6 * P] : f[c + 8 * P];
+    fp[7] = (e && n) ? f[c + 1 + Nx + 7 * P] : f[c + 5 * P];
+    fp[8] = (w && n) ? f[c - 1 + Nx + 8 * P] : f[c + 6 * P];
+}
+
+template <typename T>
+__device__ __forceinline__ void swap_pairs(T *p) {
+    T t;
+    t = p[1]; p[1] = p[3]; p[3] = t;
+    t = p[2]; p[2] = p[4]; p[4] = t;
+    t = p[5]; p[5] = p[7]; p[7] = t;
+    t = p[6]; p[6] = p[8]; p[8] = t;
+}
+
+template <typename T>
+__device__ __forceinline__ void bgk(T *p, T omega, T &rho, T &ux, T &uy) {
+    T feq[9];
+    moments(p, rho, ux, uy);
+    T usq = ux * ux + uy * uy;
+    feq_all(rho, ux, uy, usq, feq);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p[q] = p[q] - omega * (p[q] - feq[q]);
+}
+
+#define NODE2                                              \
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;   \
+    const int j = blockIdx.y;                              \
+    if (i >= g.Nx) return;                                 \
+    const size_t c = g.at(i, j);                           \
+    const size_t P = g.plane;
+
+// stream_2d_kernel!: src/kernels/collide_stream_2d.jl:5-31
+template <typename T>
+__global__ void __launch_bounds__(BX) stream_k(T *__restrict__ fo, const T *__restrict__ fi, Grid2<T> g) {
+    NODE2
+    T p[9];
+    pull_bb(fi, g, i, j, p);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) fo[c + q * P] = p[q];
+}
+
+// collide_2d_kernel!: src/kernels/collide_stream_2d.jl:35-61
+template <typename T>
+__global__ void __launch_bounds__(BX) collide_k(T *__restrict__ f, const uint8_t *__restrict__ solid,
+                                                 Grid2<T> g, T omega) {
+    NODE2
+    T p[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p[q] = f[c + q * P];
+    if (solid && solid[c]) {
+        swap_pairs(p);
+    } else {
+        T rho, ux, uy;
+        bgk(p, omega, rho, ux, uy);
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[c + q * P] = p[q];
+}
+
+// zou_he_velocity_north_2d_kernel!: src/kernels/boundary_2d.jl:13-42
+template <typename T>
+__device__ __forceinline__ void zou_he_north_node(T *p, T u) {
+    T rw = (p[0] + p[1] + p[3] + T(2) * (p[2] + p[5] + p[6])) / (T(1) + u * T(0));
+    T f2 = p[1], f4 = p[3], f6 = p[5], f7 = p[6];
+    p[4] = p[2];
+    p[8] = f7 - T(0.5) * (f2 - f4) + T(0.5) * rw * u;
+    p[7] = f6 + T(0.5) * (f2 - f4) - T(0.5) * rw * u;
+}
+
+template <typename T>
+__global__ void zou_he_north_k(T *__restrict__ f, Grid2<T> g, T u) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.Nx) return;
+    const size_t c = g.at(i, g.Ny - 1), P = g.plane;
+    T p[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p[q] = f[c + q * P];
+    zou_he_north_node(p, u);
+    f[c + 4 * P] = p[4];
+    f[c + 8 * P] = p[8];
+    f[c + 7 * P] = p[7];
+}
+
+// zou_he_velocity_south_2d_kernel!: src/kernels/boundary_2d.jl:135-149
+template <typename T>
+__global__ void zou_he_south_k(T *__restrict__ f, Grid2<T> g, T u) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.Nx) return;
+    const size_t c = g.at(i, 0), P = g.plane;
+    T f1 = f[c], f2 = f[c + P], f4 = f[c + 3 * P], f5 = f[c + 4 * P], f8 = f[c + 7 * P],
+      f9 = f[c + 8 * P];
+    T rw = f1 + f2 + f4 + T(2) * (f5 + f8 + f9);
+    f[c + 2 * P] = f5;
+    f[c + 5 * P] = f8 - T(0.5) * (f2 - f4) + T(0.5) * rw * u;
+    f[c + 6 * P] = f9 + T(0.5) * (f2 - f4) - T(0.5) * rw * u;
+}
+
+// zou_he_velocity_west_2d_kernel!: src/kernels/boundary_2d.jl:171-184
+template <typename T>
+__global__ void zou_he_west_k(T *__restrict__ f, Grid2<T> g, T u) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= g.Ny) return;
+    const size_t c = g.at(0, j), P = g.plane;
+    T f1 = f[c], f3 = f[c + 2 * P], f4 = f[c + 3 * P], f5 = f[c + 4 * P], f7 = f[c + 6 * P],
+      f8 = f[c + 7 * P];
+    T rw = (f1 + f3 + f5 + T(2) * (f4 + f7 + f8)) / (T(1) - u);
+    f[c + 1 * P] = f4 + T(2.0 / 3.0) * rw * u;
+    f[c + 5 * P] = f8 - T(0.5) * (f3 - f5) + T(1.0 / 6.0) * rw * u;
+    f[c + 8 * P] = f7 + T(0.5) * (f3 - f5) + T(1.0 / 6.0) * rw * u;
+}
+
+// zou_he_pressure_east_2d_kernel!: src/kernels/boundary_2d.jl:206-223
+template <typename T>
+__global__ void zou_he_pressure_east_k(T *__restrict__ f, Grid2<T> g, T rho_out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= g.Ny) return;
+    const size_t c = g.at(g.Nx - 1, j), P = g.plane;
+    T f1 = f[c], f2 = f[c + P], f3 = f[c + 2 * P], f5 = f[c + 4 * P], f6 = f[c + 5 * P],
+      f9 = f[c + 8 * P];
+    T ux = -T(1) + (f1 + f3 + f5 + T(2) * (f2 + f6 + f9)) / rho_out;
+    f[c + 3 * P] = f2 - T(2.0 / 3.0) * rho_out * ux;
+    f[c + 6 * P] = f9 - T(0.5) * (f3 - f5) - T(1.0 / 6.0) * rho_out * ux;
+    f[c + 7 * P] = f6 + T(0.5) * (f3 - f5) - T(1.0 / 6.0) * rho_out * ux;
+}
+
+// zou_he_pressure_west_2d_kernel!: src/kernels/boundary_2d.jl:264-281
+template <typename T>
+__global__ void zou_he_pressure_west_k(T *__restrict__ f, Grid2<T> g, T rho_in) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= g.Ny) return;
+    const size_t c = g.at(0, j), P = g.plane;
+    T f1 = f[c], f3 = f[c + 2 * P], f4 = f[c + 3 * P], f5 = f[c + 4 * P], f7 = f[c + 6 * P],
+      f8 = f[c + 7 * P];
+    T ux = T(1) - (f1 + f3 + f5 + T(2) * (f4 + f7 + f8)) / rho_in;
+    f[c + 1 * P] = f4 + T(2.0 / 3.0) * rho_in * ux;
+    f[c + 5 * P] = f8 - T(0.5) * (f3 - f5) + T(1.0 / 6.0) * rho_in * ux;
+    f[c + 8 * P] = f7 + T(0.5) * (f3 - f5) + T(1.0 / 6.0) * rho_in * ux;
+}
+
+// extrapolate_east_2d_kernel!: src/kernels/boundary_2d.jl:303-311
+template <typename T>
+__global__ void extrapolate_east_k(T *__restrict__ f, Grid2<T> g) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= g.Ny) return;
+    const size_t c = g.at(g.Nx - 1, j), P = g.plane;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[c + q * P] = f[c - 1 + q * P];
+}
+
+// bounce_back_walls_2d_kernel!: src/kernels/boundary_2d.jl:64-90
+template <typename T>
+__global__ void bounce_back_wall_k(T *__restrict__ f, Grid2<T> g, int wall_id) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t P = g.plane;
+    if (wall_id == 1 || wall_id == 4) {
+        if (idx >= g.Nx) return;
+    } else {
+        if (idx >= g.Ny) return;
+    }
+    if (wall_id == 1) {
+        const size_t c = g.at(idx, 0);
+        f[c + 2 * P] = f[c + 4 * P];
+        f[c + 5 * P] = f[c + 7 * P];
+        f[c + 6 * P] = f[c + 8 * P];
+    } else if (wall_id == 2) {
+        const size_t c = g.at(0, idx);
+        f[c + 1 * P] = f[c + 3 * P];
+        f[c + 5 * P] = f[c + 7 * P];
+        f[c + 8 * P] = f[c + 6 * P];
+    } else if (wall_id == 3) {
+        const size_t c = g.at(g.Nx - 1, idx);
+        f[c + 3 * P] = f[c + 1 * P];
+        f[c + 6 * P] = f[c + 8 * P];
+        f[c + 7 * P] = f[c + 5 * P];
+    } else {
+        const size_t c = g.at(idx, g.Ny - 1);
+        f[c + 4 * P] = f[c + 2 * P];
+        f[c + 7 * P] = f[c + 5 * P];
+        f[c + 8 * P] = f[c + 6 * P];
+    }
+}
+
+// compute_macroscopic_2d_kernel!: src/kernels/macroscopic.jl:5-18
+template <typename T>
+__device__ __forceinline__ void macro_node(const T *p, T &r, T &ux, T &uy) {
+    r = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8];
+    T inv = T(1) / r;
+    ux = (p[1] - p[3] + p[5] - p[6] - p[7] + p[8]) * inv;
+    uy = (p[2] - p[4] + p[5] + p[6] - p[7] - p[8]) * inv;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BX) macroscopic_k(T *__restrict__ rho, T *__restrict__ ux,
+                                                     T *__restrict__ uy, const T *__restrict__ f,
+                                                     Grid2<T> g) {
+    NODE2
+    T p[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p[q] = f[c + q * P];
+    T r, a, b;
+    macro_node(p, r, a, b);
+    rho[c] = r; ux[c] = a; uy[c] = b;
+}
+
+// fused_bgk_step_kernel!: src/kernels/fused_bgk_2d.jl:8-59
+template <typename T>
+__global__ void __launch_bounds__(BX) fused_bgk_k(T *__restrict__ fo, const T *__restrict__ fi,
+                                                   T *__restrict__ rho, T *__restrict__ ux,
+                                                   T *__restrict__ uy,
+                                                   const uint8_t *__restrict__ solid, Grid2<T> g,
+                                                   T omega) {
+    NODE2
+    T p[9];
+    pull_bb(fi, g, i, j, p);
+    T r, a, b;
+    if (solid && solid[c]) {
+        swap_pairs(p);
+        r = T(1); a = T(0); b = T(0);
+    } else {
+        bgk(p, omega, r, a, b);
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) fo[c + q * P] = p[q];
+    rho[c] = r; ux[c] = a; uy[c] = b;
+}
+
+// fused_trt_step_kernel!: src/kernels/fused_trt_2d.jl:29-101
+template <typename T>
+__global__ void __launch_bounds__(BX) fused_trt_k(T *__restrict__ fo, const T *__restrict__ fi,
+                                                   T *__restrict__ rho, T *__restrict__ ux,
+                                                   T *__restrict__ uy,
+                                                   const uint8_t *__restrict__ solid, Grid2<T> g,
+                                                   T sp, T sm) {
+    NODE2
+    T p[9];
+    pull_bb(fi, g, i, j, p);
+    T r, a_, b_;
+    if (solid && solid[c]) {
+        swap_pairs(p);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) fo[c + q * P] = p[q];
+        rho[c] = T(1); ux[c] = T(0); uy[c] = T(0);
+        return;
+    }
+    T feq[9];
+    moments(p, r, a_, b_);
+    T usq = a_ * a_ + b_ * b_;
+    feq_all(r, a_, b_, usq, feq);
+    const T a = (sp + sm) * T(0.5), b = (sp - sm) * T(0.5);
+    fo[c + 0 * P] = p[0] - sp * (p[0] - feq[0]);
+    fo[c + 1 * P] = p[1] - a * (p[1] - feq[1]) - b * (p[3] - feq[3]);
+    fo[c + 3 * P] = p[3] - a * (p[3] - feq[3]) - b * (p[1] - feq[1]);
+    fo[c + 2 * P] = p[2] - a * (p[2] - feq[2]) - b * (p[4] - feq[4]);
+    fo[c + 4 * P] = p[4] - a * (p[4] - feq[4]) - b * (p[2] - feq[2]);
+    fo[c + 5 * P] = p[5] - a * (p[5] - feq[5]) - b * (p[7] - feq[7]);
+    fo[c + 7 * P] = p[7] - a * (p[7] - feq[7]) - b * (p[5] - feq[5]);
+    fo[c + 6 * P] = p[6] - a * (p[6] - feq[6]) - b * (p[8] - feq[8]);
+    fo[c + 8 * P] = p[8] - a * (p[8] - feq[8]) - b * (p[6] - feq[6]);
+    rho[c] = r; ux[c] = a_; uy[c] = b_;
+}
+
+// aa_even_kernel!: src/kernels/aa_bgk_2d.jl:14-53.  `src` is a snapshot of
+// the buffer taken before the launch (see kb_aa_even_step).
+template <typename T>
+__global__ void __launch_bounds__(BX) aa_even_k(T *__restrict__ f, const T *__restrict__ src,
+                                                 const uint8_t *__restrict__ solid, Grid2<T> g,
+                                                 T omega) {
+    NODE2
+    T p[9];
+    pull_bb(src, g, i, j, p);
+    if (solid && solid[c]) {
+        f[c + 1 * P] = p[3]; f[c + 3 * P] = p[1];
+        f[c + 2 * P] = p[4]; f[c + 4 * P] = p[2];
+        f[c + 5 * P] = p[7]; f[c + 7 * P] = p[5];
+        f[c + 6 * P] = p[8]; f[c + 8 * P] = p[6];
+        return;
+    }
+    T r, a, b;
+    bgk(p, omega, r, a, b);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[c + q * P] = p[q];
+}
+
+// aa_odd_kernel!: src/kernels/aa_bgk_2d.jl:57-115 (read local, collide, push).
+template <typename T>
+__global__ void __launch_bounds__(BX) aa_odd_k(T *__restrict__ f, const T *__restrict__ src,
+                                                const uint8_t *__restrict__ solid, Grid2<T> g,
+                                                T omega) {
+    NODE2
+    const int Nx = g.Nx, Ny = g.Ny;
+    T p[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p[q] = src[c + q * P];
+    if (solid && solid[c]) {
+        f[c + 1 * P] = p[3]; f[c + 3 * P] = p[1];
+        f[c + 2 * P] = p[4]; f[c + 4 * P] = p[2];
+        f[c + 5 * P] = p[7]; f[c + 7 * P] = p[5];
+        f[c + 6 * P] = p[8]; f[c + 8 * P] = p[6];
+        return;
+    }
+    T r, a, b;
+    T cc[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) cc[q] = p[q];
+    bgk(cc, omega, r, a, b);
+    const bool w = i > 0, e = i < Nx - 1, s = j > 0, n = j < Ny - 1;
+    f[c] = cc[0];
+    f[(e ? c + 1 : c) + 1 * P] = e ? cc[1] : cc[3];
+    f[(n ? c + Nx : c) + 2 * P] = n ? cc[2] : cc[4];
+    f[(w ? c - 1 : c) + 3 * P] = w ? cc[3] : cc[1];
+    f[(s ? c - Nx : c) + 4 * P] = s ? cc[4] : cc[2];
+    const bool c6 = e && n, c7 = w && n, c8 = w && s, c9 = e && s;
+    f[(c6 ? c + 1 + Nx : c) + 5 * P] = c6 ? cc[5] : cc[7];
+    f[(c7 ? c - 1 + Nx : c) + 6 * P] = c7 ? cc[6] : cc[8];
+    f[(c8 ? c - 1 - Nx : c) + 7 * P] = c8 ? cc[7] : cc[5];
+    f[(c9 ? c + 1 - Nx : c) + 8 * P] = c9 ? cc[8] : cc[6];
+}
+
+// collide_mrt_2d_kernel!: src/kernels/collide_mrt_2d.jl:43-109
+template <typename T>
+__global__ void __launch_bounds__(BX) mrt_k(T *__restrict__ f, const uint8_t *__restrict__ solid,
+                                             Grid2<T> g, T s_e, T s_eps, T s_q, T s_nu) {
+    NODE2
+    T p[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p[q] = f[c + q * P];
+    if (solid && solid[c]) {
+        swap_pairs(p);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) f[c + q * P] = p[q];
+        return;
+    }
+    const T f1 = p[0], f2 = p[1], f3 = p[2], f4 = p[3], f5 = p[4], f6 = p[5], f7 = p[6],
+            f8 = p[7], f9 = p[8];
+    T rho = f1 + f2 + f3 + f4 + f5 + f6 + f7 + f8 + f9;
+    T e = -T(4) * f1 - f2 - f3 - f4 - f5 + T(2) * (f6 + f7 + f8 + f9);
+    T eps = T(4) * f1 - T(2) * (f2 + f3 + f4 + f5) + f6 + f7 + f8 + f9;
+    T jx = f2 - f4 + f6 - f7 - f8 + f9;
+    T qx = -T(2) * f2 + T(2) * f4 + f6 - f7 - f8 + f9;
+    T jy = f3 - f5 + f6 + f7 - f8 - f9;
+    T qy = -T(2) * f3 + T(2) * f5 + f6 + f7 - f8 - f9;
+    T pxx = f2 - f3 + f4 - f5;
+    T pxy = f6 - f7 + f8 - f9;
+    T inv = T(1) / rho;
+    T ux = jx * inv, uy = jy * inv;
+    T usq = ux * ux + uy * uy;
+    T e_eq = -T(2) * rho + T(3) * rho * usq;
+    T eps_eq = rho - T(3) * rho * usq;
+    T qx_eq = -rho * ux;
+    T qy_eq = -rho * uy;
+    T pxx_eq = rho * (ux * ux - uy * uy);
+    T pxy_eq = rho * ux * uy;
+    T es = e - s_e * (e - e_eq);
+    T ep = eps - s_eps * (eps - eps_eq);
+    T qxs = qx - s_q * (qx - qx_eq);
+    T qys = qy - s_q * (qy - qy_eq);
+    T ps = pxx - s_nu * (pxx - pxx_eq);
+    T pxys = pxy - s_nu * (pxy - pxy_eq);
+    const T r = rho, jxs = jx, jys = jy;
+    const T c9 = T(1.0 / 9.0), c36 = T(1.0 / 36.0), c18 = T(1.0 / 18.0), c6 = T(1.0 / 6.0),
+            c4 = T(1.0 / 4.0), c12 = T(1.0 / 12.0);
+    f[c + 0 * P] = c9 * r - c9 * es + c9 * ep;
+    f[c + 1 * P] = c9 * r - c36 * es - c18 * ep + c6 * jxs - c6 * qxs + c4 * ps;
+    f[c + 2 * P] = c9 * r - c36 * es - c18 * ep + c6 * jys - c6 * qys - c4 * ps;
+    f[c + 3 * P] = c9 * r - c36 * es - c18 * ep - c6 * jxs + c6 * qxs + c4 * ps;
+    f[c + 4 * P] = c9 * r - c36 * es - c18 * ep - c6 * jys + c6 * qys - c4 * ps;
+    f[c + 5 * P] = c9 * r + c18 * es + c36 * ep + c6 * jxs + c12 * qxs + c6 * jys + c12 * qys + c4 * pxys;
+    f[c + 6 * P] = c9 * r + c18 * es + c36 * ep - c6 * jxs - c12 * qxs + c6 * jys + c12 * qys - c4 * pxys;
+    f[c + 7 * P] = c9 * r + c18 * es + c36 * ep - c6 * jxs - c12 * qxs - c6 * jys - c12 * qys + c4 * pxys;
+    f[c + 8 * P] = c9 * r + c18 * es + c36 * ep + c6 * jxs + c12 * qxs - c6 * jys - c12 * qys - c4 * pxys;
+}
+
+// stream_fully_periodic_2d_kernel!: src/kernels/stream_periodic_2d.jl:79-98
+template <typename T>
+__global__ void __launch_bounds__(BX) stream_periodic_k(T *__restrict__ fo, const T *__restrict__ fi,
+                                                         Grid2<T> g) {
+    NODE2
+    const int Nx = g.Nx, Ny = g.Ny;
+    const int ip = i > 0 ? i - 1 : Nx - 1, im = i < Nx - 1 ? i + 1 : 0;
+    const int jp = j > 0 ? j - 1 : Ny - 1, jm = j < Ny - 1 ? j + 1 : 0;
+    fo[c + 0 * P] = fi[g.at(i, j) + 0 * P];
+    fo[c + 1 * P] = fi[g.at(ip, j) + 1 * P];
+    fo[c + 2 * P] = fi[g.at(i, jp) + 2 * P];
+    fo[c + 3 * P] = fi[g.at(im, j) + 3 * P];
+    fo[c + 4 * P] = fi[g.at(i, jm) + 4 * P];
+    fo[c + 5 * P] = fi[g.at(ip, jp) + 5 * P];
+    fo[c + 6 * P] = fi[g.at(im, jp) + 6 * P];
+    fo[c + 7 * P] = fi[g.at(im, jm) + 7 * P];
+    fo[c + 8 * P] = fi[g.at(ip, jm) + 8 * P];
+}
+
+// stream_periodic_x_wall_y_2d_kernel!: src/kernels/stream_periodic_2d.jl:5-55
+template <typename T>
+__global__ void __launch_bounds__(BX) stream_px_wy_k(T *__restrict__ fo, const T *__restrict__ fi,
+                                                      Grid2<T> g) {
+    NODE2
+    const int Nx = g.Nx, Ny = g.Ny;
+    const int jm1 = j > 0 ? j - 1 : j, jp1 = j < Ny - 1 ? j + 1 : j;
+    const int iw = i > 0 ? i - 1 : Nx - 1, ie = i < Nx - 1 ? i + 1 : 0;
+    fo[c + 0 * P] = fi[c];
+    fo[c + 1 * P] = fi[g.at(iw, j) + 1 * P];
+    fo[c + 2 * P] = j > 0 ? fi[g.at(i, jm1) + 2 * P] : fi[c + 4 * P];
+    fo[c + 3 * P] = fi[g.at(ie, j) + 3 * P];
+    fo[c + 4 * P] = j < Ny - 1 ? fi[g.at(i, jp1) + 4 * P] : fi[c + 2 * P];
+    fo[c + 5 * P] = j > 0 ? fi[g.at(iw, jm1) + 5 * P] : fi[c + 7 * P];
+    fo[c + 6 * P] = j > 0 ? fi[g.at(ie, jm1) + 6 * P] : fi[c + 8 * P];
+    fo[c + 7 * P] = j < Ny - 1 ? fi[g.at(ie, jp1) + 7 * P] : fi[c + 5 * P];
+    fo[c + 8 * P] = j < Ny - 1 ? fi[g.at(iw, jp1) + 8 * P] : fi[c + 6 * P];
+}
+
+// One step of run_cavity_2d (src/drivers/basic.jl:121-136) in one launch.
+// stream_2d -> zou_he_north (row Ny only) -> collide_2d -> macroscopic on the
+// post-collision populations.  All stages after the pull touch only this node.
+template <typename T>
+__global__ void __launch_bounds__(BX) cavity_step_k(T *__restrict__ fo, const T *__restrict__ fi,
+                                                     T *__restrict__ rho, T *__restrict__ ux,
+                                                     T *__restrict__ uy,
+                                                     const uint8_t *__restrict__ solid, Grid2<T> g,
+                                                     T omega, T u_lid) {
+    NODE2
+    T p[9];
+    pull_bb(fi, g, i, j, p);
+    if (j == g.Ny - 1) zou_he_north_node(p, u_lid);
+    if (solid && solid[c]) {
+        swap_pairs(p);
+    } else {
+        T r, a, b;
+        bgk(p, omega, r, a, b);
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) fo[c + q * P] = p[q];
+    T r, a, b;
+    macro_node(p, r, a, b);
+    rho[c] = r; ux[c] = a; uy[c] = b;
+}
+
+// ------------------------------------------------------------ thermal DDF --
+// src/kernels/fused_thermal_2d.jl:37-151, 178-238.
+template <typename T>
+__device__ __forceinline__ void thermal_bc(T *gp, int i, int Nx, T T_hot, T T_cold) {
+    if (i == 0) {
+        gp[1] = -gp[1] + T(2) * T(1.0 / 9.0) * T_hot;
+        gp[5] = -gp[5] + T(2) * T(1.0 / 36.0) * T_hot;
+        gp[8] = -gp[8] + T(2) * T(1.0 / 36.0) * T_hot;
+    }
+    if (i == Nx - 1) {
+        gp[3] = -gp[3] + T(2) * T(1.0 / 9.0) * T_cold;
+        gp[6] = -gp[6] + T(2) * T(1.0 / 36.0) * T_cold;
+        gp[7] = -gp[7] + T(2) * T(1.0 / 36.0) * T_cold;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void collide_thermal(T *g, T ux, T uy, T wT) {
+    const T Tm = g[0] + g[1] + g[2] + g[3] + g[4] + g[5] + g[6] + g[7] + g[8];
+    const T t3 = T(3), c0 = T(4.0 / 9.0), c1 = T(1.0 / 9.0), c5 = T(1.0 / 36.0);
+    T geq;
+    geq = c0 * Tm;                         g[0] = g[0] - wT * (g[0] - geq);
+    geq = c1 * Tm * (T(1) + t3 * ux);      g[1] = g[1] - wT * (g[1] - geq);
+    geq = c1 * Tm * (T(1) + t3 * uy);      g[2] = g[2] - wT * (g[2] - geq);
+    geq = c1 * Tm * (T(1) - t3 * ux);      g[3] = g[3] - wT * (g[3] - geq);
+    geq = c1 * Tm * (T(1) - t3 * uy);      g[4] = g[4] - wT * (g[4] - geq);
+    geq = c5 * Tm * (T(1) + t3 * (ux + uy));   g[5] = g[5] - wT * (g[5] - geq);
+    geq = c5 * Tm * (T(1) + t3 * (-ux + uy));  g[6] = g[6] - wT * (g[6] - geq);
+    geq = c5 * Tm * (T(1) + t3 * (-ux - uy));  g[7] = g[7] - wT * (g[7] - geq);
+    geq = c5 * Tm * (T(1) + t3 * (ux - uy));   g[8] = g[8] - wT * (g[8] - geq);
+}
+
+template <typename T>
+__device__ __forceinline__ void collide_boussinesq(T *f, T rho, T ux, T uy, T fy, T w) {
+    const T fx = T(0);
+    const T usq = ux * ux + uy * uy;
+    const T gp = T(1) - w / T(2);
+    const T t3 = T(3), c0 = T(4.0 / 9.0), c1 = T(1.0 / 9.0), c5 = T(1.0 / 36.0), n9 = T(9);
+    T feq[9], S[9];
+    feq_all(rho, ux, uy, usq, feq);
+    S[0] = c0 * ((-ux) * fx + (-uy) * fy) * t3;
+    S[1] = c1 * ((T(1) - ux) * fx + (-uy) * fy) * t3 + c1 * ux * fx * n9;
+    S[2] = c1 * ((-ux) * fx + (T(1) - uy) * fy) * t3 + c1 * uy * fy * n9;
+    S[3] = c1 * ((-T(1) - ux) * fx + (-uy) * fy) * t3 + c1 * ux * fx * n9;
+    S[4] = c1 * ((-ux) * fx + (-T(1) - uy) * fy) * t3 + c1 * uy * fy * n9;
+    S[5] = c5 * ((T(1) - ux) * fx + (T(1) - uy) * fy) * t3 + c5 * (ux + uy) * (fx + fy) * n9;
+    S[6] = c5 * ((-T(1) - ux) * fx + (T(1) - uy) * fy) * t3 + c5 * (-ux + uy) * (-fx + fy) * n9;
+    S[7] = c5 * ((-T(1) - ux) * fx + (-T(1) - uy) * fy) * t3 + c5 * (-ux - uy) * (-fx - fy) * n9;
+    S[8] = c5 * ((T(1) - ux) * fx + (-T(1) - uy) * fy) * t3 + c5 * (ux - uy) * (fx - fy) * n9;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[q] = f[q] - w * (f[q] - feq[q]) + gp * S[q];
+}
+
+__device__ __forceinline__ double kb_exp(double x) { return exp(x); }
+__device__ __forceinline__ float kb_exp(float x) { return expf(x); }
+
+template <typename T, bool VT>
+__global__ void __launch_bounds__(BX) natconv_k(T *__restrict__ fo, const T *__restrict__ fi,
+                                                 T *__restrict__ go, const T *__restrict__ gi,
+                                                 T *__restrict__ Temp, Grid2<T> g, T w_f, T w_T,
+                                                 T beta_g, T T_ref, T T_hot, T T_cold, T nu_ref,
+                                                 T T0_visc, T a_visc) {
+    NODE2
+    T fp[9], gp[9];
+    pull_bb(fi, g, i, j, fp);
+    pull_bb(gi, g, i, j, gp);
+    thermal_bc(gp, i, g.Nx, T_hot, T_cold);
+    const T Tl = gp[0] + gp[1] + gp[2] + gp[3] + gp[4] + gp[5] + gp[6] + gp[7] + gp[8];
+    Temp[c] = Tl;
+    // macroscopic_boussinesq: fused_thermal_2d.jl:61-72
+    const T fy = beta_g * (Tl - T_ref);
+    const T rho = fp[0] + fp[1] + fp[2] + fp[3] + fp[4] + fp[5] + fp[6] + fp[7] + fp[8];
+    const T inv = T(1) / rho;
+    const T ux = (fp[1] - fp[3] + fp[5] - fp[6] - fp[7] + fp[8]) * inv;
+    const T uy = ((fp[2] - fp[4] + fp[5] + fp[6] - fp[7] - fp[8]) + fy / T(2)) * inv;
+    collide_thermal(gp, ux, uy, w_T);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) go[c + q * P] = gp[q];
+    T w = w_f;
+    if (VT) {
+        // collide_boussinesq_vt_node: fused_thermal_2d.jl:155-161
+        const T nul = nu_ref * kb_exp(a_visc * (Tl - T0_visc));
+        w = T(1) / (T(3) * nul + T(0.5));
+    }
+    collide_boussinesq(fp, rho, ux, uy, fy, w);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) fo[c + q * P] = fp[q];
+}
+
+// compute_temperature_2d!: src/kernels/thermal_2d.jl:113-138
+template <typename T>
+__global__ void __launch_bounds__(BX) temperature_k(T *__restrict__ Temp, const T *__restrict__ gg,
+                                                     Grid2<T> g) {
+    NODE2
+    Temp[c] = gg[c] + gg[c + P] + gg[c + 2 * P] + gg[c + 3 * P] + gg[c + 4 * P] + gg[c + 5 * P] +
+              gg[c + 6 * P] + gg[c + 7 * P] + gg[c + 8 * P];
+}
+
+}  // namespace d2
+}  // namespace kb
+
+// ----------------------------------------------------------- host wrappers --
+namespace {
+
+using namespace kb::d2;
+
+template <typename T>
+Grid2<T> grid2(int Nx, int Ny) {
+    Grid2<T> g;
+    g.Nx = Nx; g.Ny = Ny; g.plane = (size_t)Nx * (size_t)Ny;
+    return g;
+}
+
+inline dim3 nodes_grid(int Nx, int Ny) { return dim3((Nx + BX - 1) / BX, Ny); }
+inline unsigned line_grid(int n) { return (unsigned)((n + BX - 1) / BX); }
+
+int check_dims(const char *what, int Nx, int Ny) {
+    if (Nx < 1 || Ny < 1 || Ny > 65535)
+        return kb::set_error(KB_ERR_ARG, "%s: bad grid %d x %d (need Nx >= 1, 1 <= Ny <= 65535)",
+                             what, Nx, Ny);
+    return KB_OK;
+}
+
+int plain_dtype(const char *what, int dtype) {
+    if (dtype != KB_F64 && dtype != KB_F32)
+        return kb::set_error(KB_ERR_UNSUPPORTED,
+                             "%s: dtype %d not supported (reference-arithmetic kernels take "
+                             "KB_F64 or KB_F32)", what, dtype);
+    return KB_OK;
+}
+
+#define KB_DISPATCH_PLAIN(what, dtype, BODY)              \
+    do {                                                  \
+        int _e = plain_dtype(what, dtype);                \
+        if (_e) return _e;                                \
+        if (dtype == KB_F64) {                            \
+            using T = double;                             \
+            BODY;                                         \
+        } else {                                          \
+            using T = float;                              \
+            BODY;                                         \
+        }                                                 \
+        return kb::check_launch(what);                    \
+    } while (0)
+
+// Library-owned scratch for the A-A snapshot, one per device, grow-only.
+void *aa_scratch(size_t bytes, int *err) {
+    static void *ptr[64] = {nullptr};
+    static size_t cap[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) { *err = KB_ERR_ARG; return nullptr; }
+    if (cap[dev] < bytes) {
+        if (ptr[dev]) cudaFree(ptr[dev]);
+        ptr[dev] = nullptr; cap[dev] = 0;
+        if (cudaMalloc(&ptr[dev], bytes) != cudaSuccess) {
+            cudaGetLastError();
+            *err = KB_ERR_NOMEM;
+            return nullptr;
+        }
+        cap[dev] = bytes;
+    }
+    *err = KB_OK;
+    return ptr[dev];
+}
+
+}  // namespace
+
+extern "C" {
+
+int kb_stream_2d(void *f_out, const void *f_in, int Nx, int Ny, int dtype, void *stream) {
+    KB_REQUIRE(f_out && f_in, "kb_stream_2d: null population pointer");
+    KB_REQUIRE(f_out != f_in, "kb_stream_2d: f_out and f_in must differ");
+    if (int e = check_dims("kb_stream_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_stream_2d", dtype,
+        (stream_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f_out, (const T *)f_in, grid2<T>(Nx, Ny))));
+}
+
+int kb_collide_2d(void *f, const uint8_t *is_solid, int Nx, int Ny, double omega, int dtype,
+                  void *stream) {
+    KB_REQUIRE(f, "kb_collide_2d: null population pointer");
+    if (int e = check_dims("kb_collide_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_collide_2d", dtype,
+        (collide_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, is_solid, grid2<T>(Nx, Ny), (T)omega)));
+}
+
+int kb_apply_zou_he_north_2d(void *f, double u_wall_x, int Nx, int Ny, int dtype, void *stream) {
+    KB_REQUIRE(f, "kb_apply_zou_he_north_2d: null population pointer");
+    if (int e = check_dims("kb_apply_zou_he_north_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_apply_zou_he_north_2d", dtype,
+        (zou_he_north_k<T><<<line_grid(Nx), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, grid2<T>(Nx, Ny), (T)u_wall_x)));
+}
+
+int kb_apply_zou_he_south_2d(void *f, double u_wall_x, int Nx, int Ny, int dtype, void *stream) {
+    KB_REQUIRE(f, "kb_apply_zou_he_south_2d: null population pointer");
+    if (int e = check_dims("kb_apply_zou_he_south_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_apply_zou_he_south_2d", dtype,
+        (zou_he_south_k<T><<<line_grid(Nx), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, grid2<T>(Nx, Ny), (T)u_wall_x)));
+}
+
+int kb_apply_zou_he_west_2d(void *f, double u_in, int Nx, int Ny, int dtype, void *stream) {
+    KB_REQUIRE(f, "kb_apply_zou_he_west_2d: null population pointer");
+    if (int e = check_dims("kb_apply_zou_he_west_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_apply_zou_he_west_2d", dtype,
+        (zou_he_west_k<T><<<line_grid(Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, grid2<T>(Nx, Ny), (T)u_in)));
+}
+
+int kb_apply_zou_he_pressure_east_2d(void *f, int Nx, int Ny, double rho_out, int dtype,
+                                     void *stream) {
+    KB_REQUIRE(f, "kb_apply_zou_he_pressure_east_2d: null population pointer");
+    if (int e = check_dims("kb_apply_zou_he_pressure_east_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_apply_zou_he_pressure_east_2d", dtype,
+        (zou_he_pressure_east_k<T><<<line_grid(Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, grid2<T>(Nx, Ny), (T)rho_out)));
+}
+
+int kb_apply_zou_he_pressure_west_2d(void *f, int Nx, int Ny, double rho_in, int dtype,
+                                     void *stream) {
+    KB_REQUIRE(f, "kb_apply_zou_he_pressure_west_2d: null population pointer");
+    if (int e = check_dims("kb_apply_zou_he_pressure_west_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_apply_zou_he_pressure_west_2d", dtype,
+        (zou_he_pressure_west_k<T><<<line_grid(Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, grid2<T>(Nx, Ny), (T)rho_in)));
+}
+
+int kb_apply_extrapolate_east_2d(void *f, int Nx, int Ny, int dtype, void *stream) {
+    KB_REQUIRE(f, "kb_apply_extrapolate_east_2d: null population pointer");
+    if (int e = check_dims("kb_apply_extrapolate_east_2d", Nx, Ny)) return e;
+    KB_REQUIRE(Nx >= 2, "kb_apply_extrapolate_east_2d: needs Nx >= 2");
+    KB_DISPATCH_PLAIN("kb_apply_extrapolate_east_2d", dtype,
+        (extrapolate_east_k<T><<<line_grid(Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, grid2<T>(Nx, Ny))));
+}
+
+int kb_apply_bounce_back_wall_2d(void *f, int Nx, int Ny, int wall_id, int dtype, void *stream) {
+    KB_REQUIRE(f, "kb_apply_bounce_back_wall_2d: null population pointer");
+    if (int e = check_dims("kb_apply_bounce_back_wall_2d", Nx, Ny)) return e;
+    KB_REQUIRE(wall_id >= 1 && wall_id <= 4,
+               "kb_apply_bounce_back_wall_2d: unknown side %d (1 south, 2 west, 3 east, 4 north)",
+               wall_id);
+    const int n = (wall_id == 1 || wall_id == 4) ? Nx : Ny;
+    KB_DISPATCH_PLAIN("kb_apply_bounce_back_wall_2d", dtype,
+        (bounce_back_wall_k<T><<<line_grid(n), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, grid2<T>(Nx, Ny), wall_id)));
+}
+
+int kb_compute_macroscopic_2d(void *rho, void *ux, void *uy, const void *f, int Nx, int Ny,
+                              int dtype, void *stream) {
+    KB_REQUIRE(rho && ux && uy && f, "kb_compute_macroscopic_2d: null pointer");
+    if (int e = check_dims("kb_compute_macroscopic_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_compute_macroscopic_2d", dtype,
+        (macroscopic_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)rho, (T *)ux, (T *)uy, (const T *)f, grid2<T>(Nx, Ny))));
+}
+
+int kb_fused_bgk_step(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                      const uint8_t *is_solid, int Nx, int Ny, double omega, int dtype,
+                      void *stream) {
+    KB_REQUIRE(f_out && f_in && rho && ux && uy, "kb_fused_bgk_step: null pointer");
+    KB_REQUIRE(f_out != f_in, "kb_fused_bgk_step: f_out and f_in must differ");
+    if (int e = check_dims("kb_fused_bgk_step", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_fused_bgk_step", dtype,
+        (fused_bgk_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, is_solid, grid2<T>(Nx, Ny),
+            (T)omega)));
+}
+
+int kb_trt_rates(double nu, double Lambda, double *s_plus, double *s_minus) {
+    KB_REQUIRE(s_plus && s_minus, "kb_trt_rates: null output pointer");
+    KB_REQUIRE(nu > 0.0, "kb_trt_rates: nu must be positive (got %g)", nu);
+    KB_REQUIRE(Lambda > 0.0, "kb_trt_rates: Lambda must be positive (got %g)", Lambda);
+    // trt_rates: src/kernels/fused_trt_2d.jl:129-133
+    *s_plus = 1.0 / (3.0 * nu + 0.5);
+    *s_minus = 1.0 / (Lambda / (3.0 * nu) + 0.5);
+    return KB_OK;
+}
+
+int kb_fused_trt_step(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                      const uint8_t *is_solid, int Nx, int Ny, double nu, double Lambda, int dtype,
+                      void *stream) {
+    KB_REQUIRE(f_out && f_in && rho && ux && uy, "kb_fused_trt_step: null pointer");
+    KB_REQUIRE(f_out != f_in, "kb_fused_trt_step: f_out and f_in must differ");
+    if (int e = check_dims("kb_fused_trt_step", Nx, Ny)) return e;
+    double sp, sm;
+    if (int e = kb_trt_rates(nu, Lambda, &sp, &sm)) return e;
+    KB_DISPATCH_PLAIN("kb_fused_trt_step", dtype,
+        (fused_trt_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, is_solid, grid2<T>(Nx, Ny),
+            (T)sp, (T)sm)));
+}
+
+static int aa_step(bool even, void *f, const uint8_t *is_solid, int Nx, int Ny, double omega,
+                   int dtype, void *stream) {
+    const char *what = even ? "kb_aa_even_step" : "kb_aa_odd_step";
+    KB_REQUIRE(f, "%s: null population pointer", what);
+    if (int e = check_dims(what, Nx, Ny)) return e;
+    if (int e = plain_dtype(what, dtype)) return e;
+    const size_t bytes = (size_t)Nx * Ny * 9 * kb::dtype_bytes(dtype);
+    int err = KB_OK;
+    void *snap = aa_scratch(bytes, &err);
+    if (!snap) return kb::set_error(err, "%s: cannot allocate %zu-byte snapshot", what, bytes);
+    cudaStream_t s = kb::as_stream(stream);
+    if (cudaMemcpyAsync(snap, f, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        return kb::set_error(KB_ERR_CUDA, "%s: snapshot copy failed: %s", what,
+                             cudaGetErrorString(cudaGetLastError()));
+    if (dtype == KB_F64) {
+        if (even) aa_even_k<double><<<nodes_grid(Nx, Ny), BX, 0, s>>>((double *)f, (const double *)snap, is_solid, grid2<double>(Nx, Ny), omega);
+        else aa_odd_k<double><<<nodes_grid(Nx, Ny), BX, 0, s>>>((double *)f, (const double *)snap, is_solid, grid2<double>(Nx, Ny), omega);
+    } else {
+        if (even) aa_even_k<float><<<nodes_grid(Nx, Ny), BX, 0, s>>>((float *)f, (const float *)snap, is_solid, grid2<float>(Nx, Ny), (float)omega);
+        else aa_odd_k<float><<<nodes_grid(Nx, Ny), BX, 0, s>>>((float *)f, (const float *)snap, is_solid, grid2<float>(Nx, Ny), (float)omega);
+    }
+    return kb::check_launch(what);
+}
+
+int kb_aa_even_step(void *f, const uint8_t *is_solid, int Nx, int Ny, double omega, int dtype,
+                    void *stream) {
+    return aa_step(true, f, is_solid, Nx, Ny, omega, dtype, stream);
+}
+
+int kb_aa_odd_step(void *f, const uint8_t *is_solid, int Nx, int Ny, double omega, int dtype,
+                   void *stream) {
+    return aa_step(false, f, is_solid, Nx, Ny, omega, dtype, stream);
+}
+
+int kb_collide_mrt_2d(void *f, const uint8_t *is_solid, int Nx, int Ny, double nu, double s_e,
+                      double s_eps, double s_q, int dtype, void *stream) {
+    KB_REQUIRE(f, "kb_collide_mrt_2d: null population pointer");
+    KB_REQUIRE(nu > 0.0, "kb_collide_mrt_2d: nu must be positive (got %g)", nu);
+    if (int e = check_dims("kb_collide_mrt_2d", Nx, Ny)) return e;
+    // s_nu = T(1.0 / (3.0 * nu + 0.5)): src/kernels/collide_mrt_2d.jl:122
+    const double s_nu = 1.0 / (3.0 * nu + 0.5);
+    KB_DISPATCH_PLAIN("kb_collide_mrt_2d", dtype,
+        (mrt_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, is_solid, grid2<T>(Nx, Ny), (T)s_e, (T)s_eps, (T)s_q, (T)s_nu)));
+}
+
+int kb_stream_fully_periodic_2d(void *f_out, const void *f_in, int Nx, int Ny, int dtype,
+                                void *stream) {
+    KB_REQUIRE(f_out && f_in, "kb_stream_fully_periodic_2d: null population pointer");
+    KB_REQUIRE(f_out != f_in, "kb_stream_fully_periodic_2d: f_out and f_in must differ");
+    if (int e = check_dims("kb_stream_fully_periodic_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_stream_fully_periodic_2d", dtype,
+        (stream_periodic_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f_out, (const T *)f_in, grid2<T>(Nx, Ny))));
+}
+
+int kb_stream_periodic_x_wall_y_2d(void *f_out, const void *f_in, int Nx, int Ny, int dtype,
+                                   void *stream) {
+    KB_REQUIRE(f_out && f_in, "kb_stream_periodic_x_wall_y_2d: null population pointer");
+    KB_REQUIRE(f_out != f_in, "kb_stream_periodic_x_wall_y_2d: f_out and f_in must differ");
+    if (int e = check_dims("kb_stream_periodic_x_wall_y_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_stream_periodic_x_wall_y_2d", dtype,
+        (stream_px_wy_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f_out, (const T *)f_in, grid2<T>(Nx, Ny))));
+}
+
+int kb_cavity_step_2d(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                      const uint8_t *is_solid, int Nx, int Ny, double omega, double u_lid,
+                      int dtype, void *stream) {
+    KB_REQUIRE(f_out && f_in && rho && ux && uy, "kb_cavity_step_2d: null pointer");
+    KB_REQUIRE(f_out != f_in, "kb_cavity_step_2d: f_out and f_in must differ");
+    if (int e = check_dims("kb_cavity_step_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_cavity_step_2d", dtype,
+        (cavity_step_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, is_solid, grid2<T>(Nx, Ny),
+            (T)omega, (T)u_lid)));
+}
+
+int kb_fused_natconv_step(void *f_out, const void *f_in, void *g_out, const void *g_in,
+                          void *Temp, int Nx, int Ny, double omega_f, double omega_T,
+                          double beta_g, double T_ref_buoy, double T_hot, double T_cold,
+                          int dtype, void *stream) {
+    KB_REQUIRE(f_out && f_in && g_out && g_in && Temp, "kb_fused_natconv_step: null pointer");
+    KB_REQUIRE(f_out != f_in && g_out != g_in, "kb_fused_natconv_step: in and out must differ");
+    if (int e = check_dims("kb_fused_natconv_step", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_fused_natconv_step", dtype,
+        (natconv_k<T, false><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f_out, (const T *)f_in, (T *)g_out, (const T *)g_in, (T *)Temp, grid2<T>(Nx, Ny),
+            (T)omega_f, (T)omega_T, (T)beta_g, (T)T_ref_buoy, (T)T_hot, (T)T_cold, T(0), T(0),
+            T(0))));
+}
+
+int kb_fused_natconv_vt_step(void *f_out, const void *f_in, void *g_out, const void *g_in,
+                             void *Temp, int Nx, int Ny, double nu_ref, double T0_visc,
+                             double alpha_visc, double omega_T, double beta_g, double T_ref_buoy,
+                             double T_hot, double T_cold, int dtype, void *stream) {
+    KB_REQUIRE(f_out && f_in && g_out && g_in && Temp, "kb_fused_natconv_vt_step: null pointer");
+    KB_REQUIRE(f_out != f_in && g_out != g_in, "kb_fused_natconv_vt_step: in and out must differ");
+    if (int e = check_dims("kb_fused_natconv_vt_step", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_fused_natconv_vt_step", dtype,
+        (natconv_k<T, true><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f_out, (const T *)f_in, (T *)g_out, (const T *)g_in, (T *)Temp, grid2<T>(Nx, Ny),
+            T(0), (T)omega_T, (T)beta_g, (T)T_ref_buoy, (T)T_hot, (T)T_cold, (T)nu_ref,
+            (T)T0_visc, (T)alpha_visc)));
+}
+
+int kb_compute_temperature_2d(void *Temp, const void *g, int Nx, int Ny, int dtype, void *stream) {
+    KB_REQUIRE(Temp && g, "kb_compute_temperature_2d: null pointer");
+    if (int e = check_dims("kb_compute_temperature_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_compute_temperature_2d", dtype,
+        (temperature_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)Temp, (const T *)g, grid2<T>(Nx, Ny))));
+}
+
+}  // extern "C"

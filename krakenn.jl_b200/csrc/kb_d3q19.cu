@@ -1,0 +1,420 @@
+// kb_d3q19.cu -- D3Q19 kernels with the reference's arithmetic.
+//
+// Compiled with --fmad=false so double (float) runs round exactly as the
+// reference's CPU Float64 (Float32) path.  The deviation-storage variants of
+// the fused TRT step live in kb_d3q19_dev.cu.
+#include "kb_d3q19.cuh"
+
+namespace kb {
+namespace d3 {
+
+template <typename T>
+__device__ __forceinline__ T feq_poly(T w, T rho, T cu, T usq) {
+    return w * rho * (T(1) + T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq);
+}
+
+// feq_3d: src/kernels/equilibrium_helpers_3d.jl:26-100 (the same expressions
+// as collide_3d_kernel!, collide_stream_3d.jl:76-100).
+template <typename T>
+__device__ __forceinline__ void feq_all(T rho, T ux, T uy, T uz, T usq, T *feq) {
+    const T wr = T(1.0 / 3.0), wa = T(1.0 / 18.0), we = T(1.0 / 36.0);
+    feq[0] = wr * rho * (T(1) - T(1.5) * usq);
+    feq[1] = feq_poly(wa, rho, ux, usq);
+    feq[2] = feq_poly(wa, rho, -ux, usq);
+    feq[3] = feq_poly(wa, rho, uy, usq);
+    feq[4] = feq_poly(wa, rho, -uy, usq);
+    feq[5] = feq_poly(wa, rho, uz, usq);
+    feq[6] = feq_poly(wa, rho, -uz, usq);
+    feq[7] = feq_poly(we, rho, ux + uy, usq);
+    feq[8] = feq_poly(we, rho, -ux + uy, usq);
+    feq[9] = feq_poly(we, rho, ux - uy, usq);
+    feq[10] = feq_poly(we, rho, -ux - uy, usq);
+    feq[11] = feq_poly(we, rho, ux + uz, usq);
+    feq[12] = feq_poly(we, rho, -ux + uz, usq);
+    feq[13] = feq_poly(we, rho, ux - uz, usq);
+    feq[14] = feq_poly(we, rho, -ux - uz, usq);
+    feq[15] = feq_poly(we, rho, uy + uz, usq);
+    feq[16] = feq_poly(we, rho, -uy + uz, usq);
+    feq[17] = feq_poly(we, rho, uy - uz, usq);
+    feq[18] = feq_poly(we, rho, -uy - uz, usq);
+}
+
+// moments_3d: src/kernels/equilibrium_helpers_3d.jl:102-112
+template <typename T>
+__device__ __forceinline__ void moments(const T *p, T &rho, T &ux, T &uy, T &uz) {
+    rho = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8] + p[9] + p[10] + p[11] +
+          p[12] + p[13] + p[14] + p[15] + p[16] + p[17] + p[18];
+    const T inv = T(1) / rho;
+    ux = (p[1] - p[2] + p[7] - p[8] + p[9] - p[10] + p[11] - p[12] + p[13] - p[14]) * inv;
+    uy = (p[3] - p[4] + p[7] + p[8] - p[9] - p[10] + p[15] - p[16] + p[17] - p[18]) * inv;
+    uz = (p[5] - p[6] + p[11] + p[12] - p[13] - p[14] + p[15] + p[16] - p[17] - p[18]) * inv;
+}
+
+template <typename T>
+__device__ __forceinline__ void swap_pairs(T *p) {
+    const int a[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16};
+    const int b[9] = {2, 4, 6, 10, 9, 14, 13, 18, 17};
+#pragma unroll
+    for (int n = 0; n < 9; ++n) { T t = p[a[n]]; p[a[n]] = p[b[n]]; p[b[n]] = t; }
+}
+
+struct Ident {
+    template <typename V> __device__ __forceinline__ V operator()(V v) const { return v; }
+};
+
+#define NODE3                                                     \
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;          \
+    const int j = blockIdx.y, k = blockIdx.z;                     \
+    if (i >= g.Nx) return;                                        \
+    const size_t c = (size_t)i + (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k); \
+    const size_t P = g.plane;
+
+// stream_3d_kernel!: src/kernels/collide_stream_3d.jl:5-42
+template <typename T>
+__global__ void __launch_bounds__(BX) stream_k(T *__restrict__ fo, const T *__restrict__ fi, Grid3 g) {
+    NODE3
+    T p[19];
+    pull19(fi, P, c, pull_geometry(g, i, j, k), p, Ident());
+#pragma unroll
+    for (int q = 0; q < 19; ++q) fo[c + q * P] = p[q];
+}
+
+// collide_3d_kernel!: src/kernels/collide_stream_3d.jl:46-103
+template <typename T>
+__global__ void __launch_bounds__(BX) collide_k(T *__restrict__ f, const uint8_t *__restrict__ solid,
+                                                 Grid3 g, T omega) {
+    NODE3
+    T p[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) p[q] = f[c + q * P];
+    if (solid && solid[c]) {
+        swap_pairs(p);
+    } else {
+        T rho, ux, uy, uz, feq[19];
+        moments(p, rho, ux, uy, uz);
+        const T usq = ux * ux + uy * uy + uz * uz;
+        feq_all(rho, ux, uy, uz, usq, feq);
+#pragma unroll
+        for (int q = 0; q < 19; ++q) p[q] = p[q] - omega * (p[q] - feq[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 19; ++q) f[c + q * P] = p[q];
+}
+
+// compute_macroscopic_3d_kernel!: src/kernels/macroscopic.jl:42-61
+template <typename T>
+__global__ void __launch_bounds__(BX) macroscopic_k(T *__restrict__ rho, T *__restrict__ ux,
+                                                     T *__restrict__ uy, T *__restrict__ uz,
+                                                     const T *__restrict__ f, Grid3 g) {
+    NODE3
+    T p[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) p[q] = f[c + q * P];
+    T r, a, b, d;
+    moments(p, r, a, b, d);
+    rho[c] = r; ux[c] = a; uy[c] = b; uz[c] = d;
+}
+
+// Fused TRT step with the reference arithmetic (PullHalfwayBB_3D +
+// SolidInert_3D + Moments_3D + CollideTRTDirect_3D + WriteMoments_3D,
+// src/kernels/dsl/bricks_3d.jl:64-230, 476-483).
+template <typename T>
+__global__ void __launch_bounds__(BX) fused_trt_k(T *__restrict__ fo, const T *__restrict__ fi,
+                                                   T *__restrict__ rho, T *__restrict__ ux,
+                                                   T *__restrict__ uy, T *__restrict__ uz,
+                                                   const uint8_t *__restrict__ solid, Grid3 g, T sp,
+                                                   T sm) {
+    NODE3
+    T p[19];
+    pull19(fi, P, c, pull_geometry(g, i, j, k), p, Ident());
+    if (solid && solid[c]) {
+        T feq[19];
+        feq_all(T(1), T(0), T(0), T(0), T(0), feq);
+#pragma unroll
+        for (int q = 0; q < 19; ++q) fo[c + q * P] = feq[q];
+        if (rho) { rho[c] = T(1); ux[c] = T(0); uy[c] = T(0); uz[c] = T(0); }
+        return;
+    }
+    T r, a_, b_, d_, feq[19];
+    moments(p, r, a_, b_, d_);
+    const T usq = a_ * a_ + b_ * b_ + d_ * d_;
+    feq_all(r, a_, b_, d_, usq, feq);
+    const T a = (sp + sm) * T(0.5), b = (sp - sm) * T(0.5);
+    const int pa[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16};
+    const int pb[9] = {2, 4, 6, 10, 9, 14, 13, 18, 17};
+    fo[c] = p[0] - sp * (p[0] - feq[0]);
+#pragma unroll
+    for (int m = 0; m < 9; ++m) {
+        const int x = pa[m], y = pb[m];
+        fo[c + x * P] = p[x] - a * (p[x] - feq[x]) - b * (p[y] - feq[y]);
+        fo[c + y * P] = p[y] - a * (p[y] - feq[y]) - b * (p[x] - feq[x]);
+    }
+    if (rho) { rho[c] = r; ux[c] = a_; uy[c] = b_; uz[c] = d_; }
+}
+
+// Zou-He face descriptors: src/kernels/boundary_3d.jl:39-137 (0-based).
+struct Face {
+    int normal_axis, sign, q_axis, q_axis_opp, q_diag[4], q_diag_opp[4];
+    int t1p, t1m, t2p, t2m, parallel[9], outgoing[5];
+};
+
+static const Face kFaces[6] = {
+    {1, -1, 1, 2, {7, 9, 11, 13}, {10, 8, 14, 12}, 3, 4, 5, 6, {0, 3, 4, 5, 6, 15, 16, 17, 18}, {2, 8, 10, 12, 14}},
+    {1, 1, 2, 1, {8, 10, 12, 14}, {9, 7, 13, 11}, 3, 4, 5, 6, {0, 3, 4, 5, 6, 15, 16, 17, 18}, {1, 7, 9, 11, 13}},
+    {2, -1, 3, 4, {7, 8, 15, 17}, {10, 9, 18, 16}, 1, 2, 5, 6, {0, 1, 2, 5, 6, 11, 12, 13, 14}, {4, 9, 10, 16, 18}},
+    {2, 1, 4, 3, {9, 10, 16, 18}, {8, 7, 17, 15}, 1, 2, 5, 6, {0, 1, 2, 5, 6, 11, 12, 13, 14}, {3, 7, 8, 15, 17}},
+    {3, -1, 5, 6, {11, 12, 15, 16}, {14, 13, 18, 17}, 1, 2, 3, 4, {0, 1, 2, 3, 4, 7, 8, 9, 10}, {6, 13, 14, 17, 18}},
+    {3, 1, 6, 5, {13, 14, 17, 18}, {12, 11, 16, 15}, 1, 2, 3, 4, {0, 1, 2, 3, 4, 7, 8, 9, 10}, {5, 11, 12, 15, 16}},
+};
+
+__device__ __forceinline__ size_t face_node(const Face &F, const Grid3 &g, int a, int b, int fixed) {
+    int i, j, k;
+    if (F.normal_axis == 1) { i = fixed; j = a; k = b; }
+    else if (F.normal_axis == 2) { i = a; j = fixed; k = b; }
+    else { i = a; j = b; k = fixed; }
+    return (size_t)i + (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k);
+}
+
+// zou_he_velocity_3d_kernel!: src/kernels/boundary_3d.jl:154-223
+template <typename T>
+__global__ void zou_he_velocity_k(T *__restrict__ f, Grid3 g, Face F, int fixed, int N1, int N2,
+                                  T u_n, T u_t1, T u_t2) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y;
+    if (a >= N1 || b >= N2) return;
+    const size_t c = face_node(F, g, a, b, fixed), P = g.plane;
+    T sum_par = T(0), sum_out = T(0);
+#pragma unroll
+    for (int n = 0; n < 9; ++n) sum_par += f[c + F.parallel[n] * P];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) sum_out += f[c + F.outgoing[n] * P];
+    const T sg = T(F.sign);
+    const T denom = T(1) + sg * u_n;
+    const T rw = (sum_par + T(2) * sum_out) / denom;
+    f[c + F.q_axis * P] = f[c + F.q_axis_opp * P] - sg * T(1.0 / 3.0) * rw * u_n;
+    const T d1 = f[c + F.parallel[5] * P], d2 = f[c + F.parallel[6] * P];
+    const T d3 = f[c + F.parallel[7] * P], d4 = f[c + F.parallel[8] * P];
+    const T t1 = (f[c + F.t1p * P] - f[c + F.t1m * P]) + (d1 - d2 + d3 - d4);
+    const T t2 = (f[c + F.t2p * P] - f[c + F.t2m * P]) + (d1 + d2 - d3 - d4);
+    const T s6 = sg * T(1.0 / 6.0);
+    f[c + F.q_diag[0] * P] = f[c + F.q_diag_opp[0] * P] - T(0.5) * t1 + T(0.5) * rw * u_t1 - s6 * rw * u_n;
+    f[c + F.q_diag[1] * P] = f[c + F.q_diag_opp[1] * P] + T(0.5) * t1 - T(0.5) * rw * u_t1 - s6 * rw * u_n;
+    f[c + F.q_diag[2] * P] = f[c + F.q_diag_opp[2] * P] - T(0.5) * t2 + T(0.5) * rw * u_t2 - s6 * rw * u_n;
+    f[c + F.q_diag[3] * P] = f[c + F.q_diag_opp[3] * P] + T(0.5) * t2 - T(0.5) * rw * u_t2 - s6 * rw * u_n;
+}
+
+// zou_he_pressure_3d_kernel!: src/kernels/boundary_3d.jl:232-288
+template <typename T>
+__global__ void zou_he_pressure_k(T *__restrict__ f, Grid3 g, Face F, int fixed, int N1, int N2,
+                                  T rho_out) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y;
+    if (a >= N1 || b >= N2) return;
+    const size_t c = face_node(F, g, a, b, fixed), P = g.plane;
+    T sum_par = T(0), sum_out = T(0);
+#pragma unroll
+    for (int n = 0; n < 9; ++n) sum_par += f[c + F.parallel[n] * P];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) sum_out += f[c + F.outgoing[n] * P];
+    const T sg = T(F.sign);
+    const T u_n = -sg * (T(1) - (sum_par + T(2) * sum_out) / rho_out);
+    f[c + F.q_axis * P] = f[c + F.q_axis_opp * P] - sg * T(1.0 / 3.0) * rho_out * u_n;
+    const T t1 = f[c + F.t1p * P] - f[c + F.t1m * P];
+    const T t2 = f[c + F.t2p * P] - f[c + F.t2m * P];
+    const T s6 = sg * T(1.0 / 6.0);
+    f[c + F.q_diag[0] * P] = f[c + F.q_diag_opp[0] * P] - T(0.5) * t1 - s6 * rho_out * u_n;
+    f[c + F.q_diag[1] * P] = f[c + F.q_diag_opp[1] * P] + T(0.5) * t1 - s6 * rho_out * u_n;
+    f[c + F.q_diag[2] * P] = f[c + F.q_diag_opp[2] * P] - T(0.5) * t2 - s6 * rho_out * u_n;
+    f[c + F.q_diag[3] * P] = f[c + F.q_diag_opp[3] * P] + T(0.5) * t2 - s6 * rho_out * u_n;
+}
+
+// stream_periodic_xz_movingwall_y_3d_kernel!: src/kernels/stream_periodic_3d.jl:106-166
+template <typename T>
+__global__ void __launch_bounds__(BX) movingwall_k(T *__restrict__ fo, const T *__restrict__ fi, Grid3 g,
+                                                    T Ub, T Ut, T rho_w) {
+    NODE3
+    const int Nx = g.Nx, Ny = g.Ny, Nz = g.Nz;
+    const long long sy = Nx, sz = (long long)Nx * Ny;
+    const long long im = (i > 0 ? -1 : Nx - 1), ip = (i < Nx - 1 ? 1 : -(Nx - 1));
+    const long long km = (k > 0 ? -1 : Nz - 1) * sz, kp = (k < Nz - 1 ? 1 : -(Nz - 1)) * sz;
+    const bool lo = j == 0, hi = j == Ny - 1;
+    const long long jm = (j > 0 ? -1 : 0) * sy, jp = (j < Ny - 1 ? 1 : 0) * sy;
+    const T cbot = T(1.0 / 6.0) * rho_w * Ub, ctop = T(1.0 / 6.0) * rho_w * Ut;
+    const T *f0 = fi + c;
+    fo[c] = f0[0];
+    fo[c + 1 * P] = f0[im + 1 * P];
+    fo[c + 2 * P] = f0[ip + 2 * P];
+    fo[c + 3 * P] = lo ? f0[4 * P] : f0[jm + 3 * P];
+    fo[c + 4 * P] = hi ? f0[3 * P] : f0[jp + 4 * P];
+    fo[c + 5 * P] = f0[km + 5 * P];
+    fo[c + 6 * P] = f0[kp + 6 * P];
+    fo[c + 7 * P] = lo ? f0[10 * P] + cbot : f0[im + jm + 7 * P];
+    fo[c + 8 * P] = lo ? f0[9 * P] - cbot : f0[ip + jm + 8 * P];
+    fo[c + 9 * P] = hi ? f0[8 * P] + ctop : f0[im + jp + 9 * P];
+    fo[c + 10 * P] = hi ? f0[7 * P] - ctop : f0[ip + jp + 10 * P];
+    fo[c + 11 * P] = f0[im + km + 11 * P];
+    fo[c + 12 * P] = f0[ip + km + 12 * P];
+    fo[c + 13 * P] = f0[im + kp + 13 * P];
+    fo[c + 14 * P] = f0[ip + kp + 14 * P];
+    fo[c + 15 * P] = lo ? f0[18 * P] : f0[jm + km + 15 * P];
+    fo[c + 16 * P] = hi ? f0[17 * P] : f0[jp + km + 16 * P];
+    fo[c + 17 * P] = lo ? f0[16 * P] : f0[jm + kp + 17 * P];
+    fo[c + 18 * P] = hi ? f0[15 * P] : f0[jp + kp + 18 * P];
+}
+
+}  // namespace d3
+}  // namespace kb
+
+// ----------------------------------------------------------- host wrappers --
+namespace {
+
+using namespace kb::d3;
+
+Grid3 grid3(int Nx, int Ny, int Nz, int per = 0) {
+    Grid3 g;
+    g.Nx = Nx; g.Ny = Ny; g.Nz = Nz; g.per = per;
+    g.plane = (size_t)Nx * (size_t)Ny * (size_t)Nz;
+    return g;
+}
+
+int plain_dtype(const char *what, int dtype) {
+    if (dtype != KB_F64 && dtype != KB_F32)
+        return kb::set_error(KB_ERR_UNSUPPORTED,
+                             "%s: dtype %d not supported (reference-arithmetic kernels take "
+                             "KB_F64 or KB_F32)", what, dtype);
+    return KB_OK;
+}
+
+#define KB3_DISPATCH_PLAIN(what, dtype, BODY)             \
+    do {                                                  \
+        int _e = plain_dtype(what, dtype);                \
+        if (_e) return _e;                                \
+        if (dtype == KB_F64) {                            \
+            using T = double;                             \
+            BODY;                                         \
+        } else {                                          \
+            using T = float;                              \
+            BODY;                                         \
+        }                                                 \
+        return kb::check_launch(what);                    \
+    } while (0)
+
+void face_extent(const Face &F, int Nx, int Ny, int Nz, int *N1, int *N2) {
+    if (F.normal_axis == 1) { *N1 = Ny; *N2 = Nz; }
+    else if (F.normal_axis == 2) { *N1 = Nx; *N2 = Nz; }
+    else { *N1 = Nx; *N2 = Ny; }
+}
+
+int face_fixed(const Face &F, int Nx, int Ny, int Nz) {
+    const int n = F.normal_axis == 1 ? Nx : (F.normal_axis == 2 ? Ny : Nz);
+    return F.sign > 0 ? n - 1 : 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kb_stream_3d(void *f_out, const void *f_in, int Nx, int Ny, int Nz, int dtype, void *stream) {
+    KB_REQUIRE(f_out && f_in, "kb_stream_3d: null population pointer");
+    KB_REQUIRE(f_out != f_in, "kb_stream_3d: f_out and f_in must differ");
+    if (int e = check_dims("kb_stream_3d", Nx, Ny, Nz)) return e;
+    KB3_DISPATCH_PLAIN("kb_stream_3d", dtype,
+        (stream_k<T><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f_out, (const T *)f_in, grid3(Nx, Ny, Nz))));
+}
+
+int kb_collide_3d(void *f, const uint8_t *is_solid, int Nx, int Ny, int Nz, double omega,
+                  int dtype, void *stream) {
+    KB_REQUIRE(f, "kb_collide_3d: null population pointer");
+    if (int e = check_dims("kb_collide_3d", Nx, Ny, Nz)) return e;
+    KB3_DISPATCH_PLAIN("kb_collide_3d", dtype,
+        (collide_k<T><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, is_solid, grid3(Nx, Ny, Nz), (T)omega)));
+}
+
+int kb_apply_zou_he_velocity_3d(void *f, int Nx, int Ny, int Nz, int face, double u_normal,
+                                double u_tang1, double u_tang2, int dtype, void *stream) {
+    KB_REQUIRE(f, "kb_apply_zou_he_velocity_3d: null population pointer");
+    KB_REQUIRE(face >= 0 && face < 6, "kb_apply_zou_he_velocity_3d: face %d not in 0..5", face);
+    if (int e = check_dims("kb_apply_zou_he_velocity_3d", Nx, Ny, Nz)) return e;
+    const Face &F = kFaces[face];
+    int N1, N2;
+    face_extent(F, Nx, Ny, Nz, &N1, &N2);
+    const int fixed = face_fixed(F, Nx, Ny, Nz);
+    dim3 grid((N1 + BX - 1) / BX, N2);
+    KB3_DISPATCH_PLAIN("kb_apply_zou_he_velocity_3d", dtype,
+        (zou_he_velocity_k<T><<<grid, BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, grid3(Nx, Ny, Nz), F, fixed, N1, N2, (T)u_normal, (T)u_tang1, (T)u_tang2)));
+}
+
+int kb_apply_zou_he_top_3d(void *f, double u_wall_x, int Nx, int Ny, int Nz, int dtype,
+                           void *stream) {
+    // apply_zou_he_top_3d!: normal z, sign +1, u_n = 0, tangent x = u_wall_x
+    return kb_apply_zou_he_velocity_3d(f, Nx, Ny, Nz, 5, 0.0, u_wall_x, 0.0, dtype, stream);
+}
+
+int kb_apply_zou_he_pressure_3d(void *f, int Nx, int Ny, int Nz, int face, double rho_out,
+                                int dtype, void *stream) {
+    KB_REQUIRE(f, "kb_apply_zou_he_pressure_3d: null population pointer");
+    KB_REQUIRE(face >= 0 && face < 6, "kb_apply_zou_he_pressure_3d: face %d not in 0..5", face);
+    if (int e = check_dims("kb_apply_zou_he_pressure_3d", Nx, Ny, Nz)) return e;
+    const Face &F = kFaces[face];
+    int N1, N2;
+    face_extent(F, Nx, Ny, Nz, &N1, &N2);
+    const int fixed = face_fixed(F, Nx, Ny, Nz);
+    dim3 grid((N1 + BX - 1) / BX, N2);
+    KB3_DISPATCH_PLAIN("kb_apply_zou_he_pressure_3d", dtype,
+        (zou_he_pressure_k<T><<<grid, BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, grid3(Nx, Ny, Nz), F, fixed, N1, N2, (T)rho_out)));
+}
+
+int kb_compute_macroscopic_3d(void *rho, void *ux, void *uy, void *uz, const void *f, int Nx,
+                              int Ny, int Nz, int dtype, void *stream) {
+    KB_REQUIRE(rho && ux && uy && uz && f, "kb_compute_macroscopic_3d: null pointer");
+    if (int e = check_dims("kb_compute_macroscopic_3d", Nx, Ny, Nz)) return e;
+    KB3_DISPATCH_PLAIN("kb_compute_macroscopic_3d", dtype,
+        (macroscopic_k<T><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
+            (T *)rho, (T *)ux, (T *)uy, (T *)uz, (const T *)f, grid3(Nx, Ny, Nz))));
+}
+
+int kb_fused_trt_step_3d(void *f_out, const void *f_in, void *rho, void *ux, void *uy, void *uz,
+                         const uint8_t *is_solid, int Nx, int Ny, int Nz, double nu,
+                         double Lambda, int periodic, int dtype, void *stream) {
+    const char *what = "kb_fused_trt_step_3d";
+    KB_REQUIRE(f_out && f_in, "%s: null population pointer", what);
+    KB_REQUIRE(f_out != f_in, "%s: f_out and f_in must differ", what);
+    const int nm = (rho != nullptr) + (ux != nullptr) + (uy != nullptr) + (uz != nullptr);
+    KB_REQUIRE(nm == 0 || nm == 4, "%s: pass all four moment arrays or none", what);
+    KB_REQUIRE(periodic >= 0 && periodic < 8, "%s: periodic mask %d not in 0..7", what, periodic);
+    if (int e = check_dims(what, Nx, Ny, Nz)) return e;
+    double sp, sm;
+    if (int e = kb_trt_rates(nu, Lambda, &sp, &sm)) return e;
+    const Grid3 g = grid3(Nx, Ny, Nz, periodic);
+    cudaStream_t s = kb::as_stream(stream);
+    if (dtype == KB_F64) {
+        fused_trt_k<double><<<nodes_grid(Nx, Ny, Nz), BX, 0, s>>>(
+            (double *)f_out, (const double *)f_in, (double *)rho, (double *)ux, (double *)uy,
+            (double *)uz, is_solid, g, sp, sm);
+    } else if (dtype == KB_F32) {
+        fused_trt_k<float><<<nodes_grid(Nx, Ny, Nz), BX, 0, s>>>(
+            (float *)f_out, (const float *)f_in, (float *)rho, (float *)ux, (float *)uy,
+            (float *)uz, is_solid, g, (float)sp, (float)sm);
+    } else if (dtype == KB_F32_DEV || dtype == KB_F16_DEV || dtype == KB_BF16_DEV) {
+        return launch_trt3d_dev(dtype, f_out, f_in, (float *)rho, (float *)ux, (float *)uy,
+                                (float *)uz, is_solid, g, (float)sp, (float)sm, s);
+    } else {
+        return kb::set_error(KB_ERR_UNSUPPORTED, "%s: unknown dtype %d", what, dtype);
+    }
+    return kb::check_launch(what);
+}
+
+int kb_stream_periodic_xz_movingwall_y_3d(void *f_out, const void *f_in, double Ub, double Ut,
+                                          double rho_w, int Nx, int Ny, int Nz, int dtype,
+                                          void *stream) {
+    KB_REQUIRE(f_out && f_in, "kb_stream_periodic_xz_movingwall_y_3d: null population pointer");
+    KB_REQUIRE(f_out != f_in, "kb_stream_periodic_xz_movingwall_y_3d: f_out and f_in must differ");
+    if (int e = check_dims("kb_stream_periodic_xz_movingwall_y_3d", Nx, Ny, Nz)) return e;
+    KB3_DISPATCH_PLAIN("kb_stream_periodic_xz_movingwall_y_3d", dtype,
+        (movingwall_k<T><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f_out, (const T *)f_in, grid3(Nx, Ny, Nz), (T)Ub, (T)Ut, (T)rho_w)));
+}
+
+}  // extern "C"

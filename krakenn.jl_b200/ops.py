@@ -1,0 +1,429 @@
+"""Kernel-level API: the reference's stream-collide functions on B200 tensors.
+
+Every function here calls one C-ABI entry point of libkrakenb200.so on the
+current torch CUDA stream.  Names follow Kraken.jl with the trailing `!`
+written as `_` (in-place), and the positional arguments keep the reference's
+order and meaning.  Arrays are torch CUDA tensors laid out like the
+reference's column-major arrays: a Julia `f[i, j, q]` of size (Nx, Ny, 9) is
+a contiguous torch tensor of shape (9, Ny, Nx); D3Q19 `f[i, j, k, q]` is
+(19, Nz, Ny, Nx); fields `rho[i, j]` are (Ny, Nx).
+
+Storage: float64 and float32 tensors hold f with the reference arithmetic.
+float16 / bfloat16 tensors hold the deviation f - w_q (FP32 collision); a
+float32 deviation buffer is selected with `deviation=True`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import _lib
+from ._lib import (KB_BF16_DEV, KB_F16_DEV, KB_F32, KB_F32_DEV, KB_F64, call)
+
+_TORCH_DTYPE = {KB_F64: torch.float64, KB_F32: torch.float32, KB_F32_DEV: torch.float32,
+                KB_F16_DEV: torch.float16, KB_BF16_DEV: torch.bfloat16}
+
+
+def storage_dtype(t: torch.Tensor, deviation: bool = False) -> int:
+    """kb_dtype code of a population tensor."""
+    if t.dtype == torch.float64:
+        if deviation:
+            raise ValueError("float64 storage holds f, not a deviation")
+        return KB_F64
+    if t.dtype == torch.float32:
+        return KB_F32_DEV if deviation else KB_F32
+    if t.dtype == torch.float16:
+        return KB_F16_DEV
+    if t.dtype == torch.bfloat16:
+        return KB_BF16_DEV
+    raise ValueError(f"unsupported population dtype {t.dtype}")
+
+
+def torch_dtype(code: int) -> torch.dtype:
+    return _TORCH_DTYPE[code]
+
+
+def field_dtype(code: int) -> torch.dtype:
+    """dtype of the macroscopic fields that go with a population storage."""
+    return torch.float64 if code == KB_F64 else torch.float32
+
+
+def _t(t: torch.Tensor | None, name: str):
+    if t is None:
+        return None
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"{name} must be a torch tensor")
+    if not t.is_cuda:
+        raise ValueError(f"{name} must live on a CUDA device (the B200 path has no CPU fallback)")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    return C.c_void_p(t.data_ptr())
+
+
+def _mask(m: torch.Tensor | None):
+    if m is None:
+        return None
+    if m.dtype not in (torch.bool, torch.uint8):
+        raise ValueError("is_solid must be a bool or uint8 tensor")
+    return _t(m, "is_solid")
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _plain(f: torch.Tensor) -> int:
+    code = storage_dtype(f)
+    if code not in (KB_F64, KB_F32):
+        raise ValueError("this reference kernel takes float64 or float32 populations")
+    return code
+
+
+def _same(code: int, *fields):
+    want = field_dtype(code)
+    for name, t in fields:
+        if t is not None and t.dtype != want:
+            raise ValueError(f"{name} must be {want} for this population storage")
+
+
+def _dims2(f: torch.Tensor):
+    if f.dim() != 3 or f.shape[0] != 9:
+        raise ValueError("D2Q9 populations must have shape (9, Ny, Nx)")
+    return int(f.shape[2]), int(f.shape[1])
+
+
+def _dims3(f: torch.Tensor):
+    if f.dim() != 4 or f.shape[0] != 19:
+        raise ValueError("D3Q19 populations must have shape (19, Nz, Ny, Nx)")
+    return int(f.shape[3]), int(f.shape[2]), int(f.shape[1])
+
+
+def _match2(f, Nx, Ny):
+    if _dims2(f) != (Nx, Ny):
+        raise ValueError(f"population shape {tuple(f.shape)} does not match Nx={Nx}, Ny={Ny}")
+
+
+def _match3(f, Nx, Ny, Nz):
+    if _dims3(f) != (Nx, Ny, Nz):
+        raise ValueError(f"population shape {tuple(f.shape)} does not match "
+                         f"Nx={Nx}, Ny={Ny}, Nz={Nz}")
+
+
+def _ptrs_2d_fields(code, Nx, Ny, **fields):
+    for name, t in fields.items():
+        if t is not None and tuple(t.shape) != (Ny, Nx):
+            raise ValueError(f"{name} must have shape (Ny, Nx) = ({Ny}, {Nx})")
+    _same(code, *fields.items())
+
+
+def _ptrs_3d_fields(code, Nx, Ny, Nz, **fields):
+    for name, t in fields.items():
+        if t is not None and tuple(t.shape) != (Nz, Ny, Nx):
+            raise ValueError(f"{name} must have shape (Nz, Ny, Nx) = ({Nz}, {Ny}, {Nx})")
+    _same(code, *fields.items())
+
+
+# --------------------------------------------------------------------- D2Q9
+
+def stream_2d_(f_out, f_in, Nx, Ny):
+    """stream_2d! -- src/kernels/collide_stream_2d.jl:77"""
+    code = _plain(f_in)
+    _match2(f_in, Nx, Ny); _match2(f_out, Nx, Ny)
+    call("kb_stream_2d", _t(f_out, "f_out"), _t(f_in, "f_in"), Nx, Ny, code, _stream())
+
+
+def collide_2d_(f, is_solid, omega):
+    """collide_2d! -- src/kernels/collide_stream_2d.jl:96"""
+    code = _plain(f)
+    Nx, Ny = _dims2(f)
+    call("kb_collide_2d", _t(f, "f"), _mask(is_solid), Nx, Ny, float(omega), code, _stream())
+
+
+def apply_zou_he_north_2d_(f, u_wall_x, Nx, Ny):
+    """apply_zou_he_north_2d! -- src/kernels/boundary_2d.jl:56"""
+    code = _plain(f); _match2(f, Nx, Ny)
+    call("kb_apply_zou_he_north_2d", _t(f, "f"), float(u_wall_x), Nx, Ny, code, _stream())
+
+
+def apply_zou_he_south_2d_(f, u_wall_x, Nx):
+    """apply_zou_he_south_2d! -- src/kernels/boundary_2d.jl:163"""
+    code = _plain(f)
+    nx, ny = _dims2(f)
+    if nx != Nx:
+        raise ValueError("Nx does not match the population shape")
+    call("kb_apply_zou_he_south_2d", _t(f, "f"), float(u_wall_x), Nx, ny, code, _stream())
+
+
+def apply_zou_he_west_2d_(f, u_in, Nx, Ny):
+    """apply_zou_he_west_2d! -- src/kernels/boundary_2d.jl:198"""
+    code = _plain(f); _match2(f, Nx, Ny)
+    call("kb_apply_zou_he_west_2d", _t(f, "f"), float(u_in), Nx, Ny, code, _stream())
+
+
+def apply_zou_he_pressure_east_2d_(f, Nx, Ny, rho_out=1.0):
+    """apply_zou_he_pressure_east_2d! -- src/kernels/boundary_2d.jl:237"""
+    code = _plain(f); _match2(f, Nx, Ny)
+    call("kb_apply_zou_he_pressure_east_2d", _t(f, "f"), Nx, Ny, float(rho_out), code, _stream())
+
+
+def apply_zou_he_pressure_west_2d_(f, Nx, Ny, rho_in=1.0):
+    """apply_zou_he_pressure_west_2d! -- src/kernels/boundary_2d.jl:295"""
+    code = _plain(f); _match2(f, Nx, Ny)
+    call("kb_apply_zou_he_pressure_west_2d", _t(f, "f"), Nx, Ny, float(rho_in), code, _stream())
+
+
+def apply_extrapolate_east_2d_(f, Nx, Ny):
+    """apply_extrapolate_east_2d! -- src/kernels/boundary_2d.jl:319"""
+    code = _plain(f); _match2(f, Nx, Ny)
+    call("kb_apply_extrapolate_east_2d", _t(f, "f"), Nx, Ny, code, _stream())
+
+
+_SIDES = {"south": 1, "west": 2, "east": 3, "north": 4}
+
+
+def apply_bounce_back_wall_2d_(f, Nx, Ny, side):
+    """apply_bounce_back_wall_2d! -- src/kernels/boundary_2d.jl:117"""
+    code = _plain(f); _match2(f, Nx, Ny)
+    if side not in _SIDES:
+        raise ValueError(f"apply_bounce_back_wall_2d!: unknown side {side}")
+    call("kb_apply_bounce_back_wall_2d", _t(f, "f"), Nx, Ny, _SIDES[side], code, _stream())
+
+
+def apply_bounce_back_walls_2d_(f, Nx, Ny):
+    """apply_bounce_back_walls_2d! (south, west, east) -- src/kernels/boundary_2d.jl:98"""
+    for side in ("south", "west", "east"):
+        apply_bounce_back_wall_2d_(f, Nx, Ny, side)
+
+
+def compute_macroscopic_2d_(rho, ux, uy, f):
+    """compute_macroscopic_2d! -- src/kernels/macroscopic.jl:32"""
+    code = _plain(f)
+    Nx, Ny = _dims2(f)
+    _ptrs_2d_fields(code, Nx, Ny, rho=rho, ux=ux, uy=uy)
+    call("kb_compute_macroscopic_2d", _t(rho, "rho"), _t(ux, "ux"), _t(uy, "uy"), _t(f, "f"),
+         Nx, Ny, code, _stream())
+
+
+def fused_bgk_step_(f_out, f_in, rho, ux, uy, is_solid, Nx, Ny, omega):
+    """fused_bgk_step! -- src/kernels/fused_bgk_2d.jl:67"""
+    code = _plain(f_in)
+    _match2(f_in, Nx, Ny); _match2(f_out, Nx, Ny)
+    _ptrs_2d_fields(code, Nx, Ny, rho=rho, ux=ux, uy=uy)
+    call("kb_fused_bgk_step", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
+         _t(ux, "ux"), _t(uy, "uy"), _mask(is_solid), Nx, Ny, float(omega), code, _stream())
+
+
+def trt_rates(nu, Lambda=3 / 16):
+    """trt_rates(nu; Lambda) -> (s_plus, s_minus) -- src/kernels/fused_trt_2d.jl:129"""
+    sp, sm = C.c_double(), C.c_double()
+    call("kb_trt_rates", float(nu), float(Lambda), C.byref(sp), C.byref(sm))
+    return sp.value, sm.value
+
+
+def fused_trt_step_(f_out, f_in, rho, ux, uy, is_solid, Nx, Ny, nu, Lambda=3 / 16):
+    """fused_trt_step! -- src/kernels/fused_trt_2d.jl:145"""
+    code = _plain(f_in)
+    _match2(f_in, Nx, Ny); _match2(f_out, Nx, Ny)
+    _ptrs_2d_fields(code, Nx, Ny, rho=rho, ux=ux, uy=uy)
+    call("kb_fused_trt_step", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
+         _t(ux, "ux"), _t(uy, "uy"), _mask(is_solid), Nx, Ny, float(nu), float(Lambda), code,
+         _stream())
+
+
+def aa_even_step_(f, is_solid, Nx, Ny, omega):
+    """aa_even_step! -- src/kernels/aa_bgk_2d.jl:125"""
+    code = _plain(f); _match2(f, Nx, Ny)
+    call("kb_aa_even_step", _t(f, "f"), _mask(is_solid), Nx, Ny, float(omega), code, _stream())
+
+
+def aa_odd_step_(f, is_solid, Nx, Ny, omega):
+    """aa_odd_step! -- src/kernels/aa_bgk_2d.jl:138"""
+    code = _plain(f); _match2(f, Nx, Ny)
+    call("kb_aa_odd_step", _t(f, "f"), _mask(is_solid), Nx, Ny, float(omega), code, _stream())
+
+
+def collide_mrt_2d_(f, is_solid, nu, s_e=1.4, s_eps=1.4, s_q=1.2):
+    """collide_mrt_2d! -- src/kernels/collide_mrt_2d.jl:118"""
+    code = _plain(f)
+    Nx, Ny = _dims2(f)
+    call("kb_collide_mrt_2d", _t(f, "f"), _mask(is_solid), Nx, Ny, float(nu), float(s_e),
+         float(s_eps), float(s_q), code, _stream())
+
+
+def stream_fully_periodic_2d_(f_out, f_in, Nx, Ny):
+    """stream_fully_periodic_2d! -- src/kernels/stream_periodic_2d.jl:112"""
+    code = _plain(f_in); _match2(f_in, Nx, Ny); _match2(f_out, Nx, Ny)
+    call("kb_stream_fully_periodic_2d", _t(f_out, "f_out"), _t(f_in, "f_in"), Nx, Ny, code,
+         _stream())
+
+
+def stream_periodic_x_wall_y_2d_(f_out, f_in, Nx, Ny):
+    """stream_periodic_x_wall_y_2d! -- src/kernels/stream_periodic_2d.jl:71"""
+    code = _plain(f_in); _match2(f_in, Nx, Ny); _match2(f_out, Nx, Ny)
+    call("kb_stream_periodic_x_wall_y_2d", _t(f_out, "f_out"), _t(f_in, "f_in"), Nx, Ny, code,
+         _stream())
+
+
+def cavity_step_2d_(f_out, f_in, rho, ux, uy, is_solid, Nx, Ny, omega, u_lid):
+    """One run_cavity_2d step (src/drivers/basic.jl:121-136) in one launch."""
+    code = _plain(f_in)
+    _match2(f_in, Nx, Ny); _match2(f_out, Nx, Ny)
+    _ptrs_2d_fields(code, Nx, Ny, rho=rho, ux=ux, uy=uy)
+    call("kb_cavity_step_2d", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
+         _t(ux, "ux"), _t(uy, "uy"), _mask(is_solid), Nx, Ny, float(omega), float(u_lid), code,
+         _stream())
+
+
+def fused_natconv_step_(f_out, f_in, g_out, g_in, Temp, Nx, Ny, omega_f, omega_T, beta_g,
+                        T_ref_buoy, T_hot, T_cold):
+    """fused_natconv_step! -- src/kernels/fused_thermal_2d.jl:251"""
+    code = _plain(f_in)
+    for t in (f_in, f_out, g_in, g_out):
+        _match2(t, Nx, Ny)
+    _ptrs_2d_fields(code, Nx, Ny, Temp=Temp)
+    call("kb_fused_natconv_step", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(g_out, "g_out"),
+         _t(g_in, "g_in"), _t(Temp, "Temp"), Nx, Ny, float(omega_f), float(omega_T),
+         float(beta_g), float(T_ref_buoy), float(T_hot), float(T_cold), code, _stream())
+
+
+def fused_natconv_vt_step_(f_out, f_in, g_out, g_in, Temp, Nx, Ny, nu_ref, T0_visc, alpha_visc,
+                           omega_T, beta_g, T_ref_buoy, T_hot, T_cold):
+    """fused_natconv_vt_step! -- src/kernels/fused_thermal_2d.jl:268"""
+    code = _plain(f_in)
+    for t in (f_in, f_out, g_in, g_out):
+        _match2(t, Nx, Ny)
+    _ptrs_2d_fields(code, Nx, Ny, Temp=Temp)
+    call("kb_fused_natconv_vt_step", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(g_out, "g_out"),
+         _t(g_in, "g_in"), _t(Temp, "Temp"), Nx, Ny, float(nu_ref), float(T0_visc),
+         float(alpha_visc), float(omega_T), float(beta_g), float(T_ref_buoy), float(T_hot),
+         float(T_cold), code, _stream())
+
+
+def compute_temperature_2d_(Temp, g):
+    """compute_temperature_2d! -- src/kernels/thermal_2d.jl:113"""
+    code = _plain(g)
+    Nx, Ny = _dims2(g)
+    _ptrs_2d_fields(code, Nx, Ny, Temp=Temp)
+    call("kb_compute_temperature_2d", _t(Temp, "Temp"), _t(g, "g"), Nx, Ny, code, _stream())
+
+
+# -------------------------------------------------------------------- D3Q19
+
+def stream_3d_(f_out, f_in, Nx, Ny, Nz):
+    """stream_3d! -- src/kernels/collide_stream_3d.jl:119"""
+    code = _plain(f_in); _match3(f_in, Nx, Ny, Nz); _match3(f_out, Nx, Ny, Nz)
+    call("kb_stream_3d", _t(f_out, "f_out"), _t(f_in, "f_in"), Nx, Ny, Nz, code, _stream())
+
+
+def collide_3d_(f, is_solid, omega):
+    """collide_3d! -- src/kernels/collide_stream_3d.jl:137"""
+    code = _plain(f)
+    Nx, Ny, Nz = _dims3(f)
+    call("kb_collide_3d", _t(f, "f"), _mask(is_solid), Nx, Ny, Nz, float(omega), code, _stream())
+
+
+FACES_3D = {"west": 0, "east": 1, "south": 2, "north": 3, "bottom": 4, "top": 5}
+
+
+def apply_zou_he_velocity_3d_(f, face, u_normal, u_tang1, u_tang2):
+    """_apply_zou_he_velocity_3d! -- src/kernels/boundary_3d.jl:300"""
+    code = _plain(f)
+    Nx, Ny, Nz = _dims3(f)
+    call("kb_apply_zou_he_velocity_3d", _t(f, "f"), Nx, Ny, Nz, FACES_3D[face],
+         float(u_normal), float(u_tang1), float(u_tang2), code, _stream())
+
+
+def apply_zou_he_top_3d_(f, u_wall_x, Nx, Ny, Nz):
+    """apply_zou_he_top_3d! -- src/kernels/boundary_3d.jl:326"""
+    code = _plain(f); _match3(f, Nx, Ny, Nz)
+    call("kb_apply_zou_he_top_3d", _t(f, "f"), float(u_wall_x), Nx, Ny, Nz, code, _stream())
+
+
+def apply_zou_he_pressure_3d_(f, face, rho_out=1.0):
+    """_apply_zou_he_pressure_3d! -- src/kernels/boundary_3d.jl:307"""
+    code = _plain(f)
+    Nx, Ny, Nz = _dims3(f)
+    call("kb_apply_zou_he_pressure_3d", _t(f, "f"), Nx, Ny, Nz, FACES_3D[face], float(rho_out),
+         code, _stream())
+
+
+def compute_macroscopic_3d_(rho, ux, uy, uz, f):
+    """compute_macroscopic_3d! -- src/kernels/macroscopic.jl:75"""
+    code = _plain(f)
+    Nx, Ny, Nz = _dims3(f)
+    _ptrs_3d_fields(code, Nx, Ny, Nz, rho=rho, ux=ux, uy=uy, uz=uz)
+    call("kb_compute_macroscopic_3d", _t(rho, "rho"), _t(ux, "ux"), _t(uy, "uy"), _t(uz, "uz"),
+         _t(f, "f"), Nx, Ny, Nz, code, _stream())
+
+
+def periodic_mask(periodic) -> int:
+    if isinstance(periodic, int):
+        return periodic
+    px, py, pz = periodic
+    return int(bool(px)) | (int(bool(py)) << 1) | (int(bool(pz)) << 2)
+
+
+def fused_trt_step_3d_(f_out, f_in, rho, ux, uy, uz, is_solid, Nx, Ny, Nz, nu, Lambda=3 / 16,
+                       periodic=(False, False, False), deviation=False):
+    """Fused D3Q19 TRT step -- the reference's fused_trt_libb_v2_step_3d!
+    (src/kernels/li_bb_3d_v2.jl:31) without interpolated-wall links, with
+    per-axis periodic wrap.  Moments may be None (then not written)."""
+    code = storage_dtype(f_in, deviation)
+    if storage_dtype(f_out, deviation) != code:
+        raise ValueError("f_in and f_out must have the same storage")
+    _match3(f_in, Nx, Ny, Nz); _match3(f_out, Nx, Ny, Nz)
+    _ptrs_3d_fields(code, Nx, Ny, Nz, rho=rho, ux=ux, uy=uy, uz=uz)
+    call("kb_fused_trt_step_3d", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
+         _t(ux, "ux"), _t(uy, "uy"), _t(uz, "uz"), _mask(is_solid), Nx, Ny, Nz, float(nu),
+         float(Lambda), periodic_mask(periodic), code, _stream())
+
+
+def stream_periodic_xz_movingwall_y_3d_(f_out, f_in, Ub, Ut, Nx, Ny, Nz, rho_w=1.0):
+    """stream_periodic_xz_movingwall_y_3d! -- src/kernels/stream_periodic_3d.jl:178"""
+    code = _plain(f_in); _match3(f_in, Nx, Ny, Nz); _match3(f_out, Nx, Ny, Nz)
+    call("kb_stream_periodic_xz_movingwall_y_3d", _t(f_out, "f_out"), _t(f_in, "f_in"),
+         float(Ub), float(Ut), float(rho_w), Nx, Ny, Nz, code, _stream())
+
+
+# ------------------------------------------------------- precision + FP64 sums
+
+def convert_populations(dst, src, dst_deviation=False, src_deviation=False):
+    """Convert populations between storages (f <-> f - w_q, any precision)."""
+    if dst.shape != src.shape:
+        raise ValueError("src and dst shapes differ")
+    Q = int(src.shape[0])
+    n = src.numel() // Q
+    call("kb_convert_populations", _t(dst, "dst"), storage_dtype(dst, dst_deviation),
+         _t(src, "src"), storage_dtype(src, src_deviation), Q, n, _stream())
+
+
+def mass(f, deviation=False) -> float:
+    """FP64 compensated total mass sum(f) (synchronises the stream)."""
+    out = C.c_double()
+    Q = int(f.shape[0])
+    call("kb_mass", _t(f, "f"), Q, f.numel() // Q, storage_dtype(f, deviation), C.byref(out),
+         _stream())
+    return out.value
+
+
+def residual(ux, uy, ux_prev, uy_prev, uz=None, uz_prev=None, is_solid=None) -> float:
+    """r_u = ||u - u_prev|| / ||u|| over fluid nodes (FP64 sums; synchronises)."""
+    code = KB_F64 if ux.dtype == torch.float64 else KB_F32
+    out = C.c_double()
+    call("kb_residual", _t(ux, "ux"), _t(uy, "uy"), _t(uz, "uz"), _t(ux_prev, "ux_prev"),
+         _t(uy_prev, "uy_prev"), _t(uz_prev, "uz_prev"), _mask(is_solid), ux.numel(), code,
+         C.byref(out), _stream())
+    return out.value
+
+
+def synchronize():
+    """KernelAbstractions.synchronize(backend)."""
+    call("kb_sync", _stream())
+
+
+__all__ = [n for n in dir() if n.endswith("_") and not n.startswith("_")] + [
+    "trt_rates", "convert_populations", "mass", "residual", "synchronize", "storage_dtype",
+    "torch_dtype", "field_dtype", "periodic_mask", "FACES_3D"]
+
+_ = _lib  # keep the module import explicit for readers

@@ -1,0 +1,987 @@
+/*
+ * kb_oracle.c -- CPU FP64 restatement of Kraken.jl's stream-collide path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the parity oracle: the tests, the
+ * smoke check and the CPU-baseline leg of the benchmark load it as a checker.
+ * The product (the CUDA library behind include/krakenb200.h) never links,
+ * calls or falls back to it.
+ *
+ * Every routine restates one Kraken.jl routine operation for operation: the
+ * same left-to-right sums, `inv_rho = 1/rho` followed by a multiply, the same
+ * pre-rounded constants (1/9, 1/36, ...), the same branch structure at the
+ * domain edges.  It must be compiled with -ffp-contract=off so no multiply-add
+ * is fused, which is what the reference's Julia CPU path does.  The citation
+ * above each function names the reference file:line it follows.
+ *
+ * Parity pinning: Julia is not available in this environment, so the
+ * reference cannot be run.  The restatement is pinned instead against the
+ * known answers of the reference's own tests (lattice sums, TRT rates,
+ * TRT == BGK, equilibrium stationarity, mass conservation, Ghia centreline,
+ * Taylor-Green decay, half-way Dirichlet conduction, De Vahl Davis Nu); see
+ * tests/test_oracle_pins.py.
+ *
+ * Layout: Julia column-major arrays, 0-based here.
+ *   2D  f[i + Nx*(j + Ny*q)]            (i fastest, then j, then population q)
+ *   3D  f[i + Nx*(j + Ny*(k + Nz*q))]
+ * Population q is 0-based here; the reference's q is 1-based (q_ref = q + 1).
+ * Masks are one byte per node (Julia Bool).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stddef.h>
+#include <string.h>
+#include <stdlib.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define I2(i, j, q) ((size_t)(i) + (size_t)Nx * ((size_t)(j) + (size_t)Ny * (size_t)(q)))
+#define N2(i, j) ((size_t)(i) + (size_t)Nx * (size_t)(j))
+#define I3(i, j, k, q) \
+    ((size_t)(i) + (size_t)Nx * ((size_t)(j) + (size_t)Ny * ((size_t)(k) + (size_t)Nz * (size_t)(q))))
+#define N3(i, j, k) ((size_t)(i) + (size_t)Nx * ((size_t)(j) + (size_t)Ny * (size_t)(k)))
+
+/* ------------------------------------------------------------------------ */
+/* Lattice constants: src/lattice/d2q9.jl:17-29, src/lattice/d3q19.jl:13-47  */
+/* ------------------------------------------------------------------------ */
+const double or_d2q9_w[9] = {4.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0,
+                             1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0};
+const int or_d2q9_cx[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
+const int or_d2q9_cy[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+const int or_d2q9_opp[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+
+const double or_d3q19_w[19] = {1.0 / 3.0,
+                               1.0 / 18.0, 1.0 / 18.0, 1.0 / 18.0, 1.0 / 18.0, 1.0 / 18.0, 1.0 / 18.0,
+                               1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0,
+                               1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0,
+                               1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0};
+const int or_d3q19_cx[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+const int or_d3q19_cy[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
+const int or_d3q19_cz[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
+const int or_d3q19_opp[19] = {0, 2, 1, 4, 3, 6, 5, 10, 9, 8, 7, 14, 13, 12, 11, 18, 17, 16, 15};
+
+void or_lattice_d2q9(double *w, int *cx, int *cy, int *opp) {
+    for (int q = 0; q < 9; ++q) {
+        w[q] = or_d2q9_w[q]; cx[q] = or_d2q9_cx[q]; cy[q] = or_d2q9_cy[q]; opp[q] = or_d2q9_opp[q];
+    }
+}
+
+void or_lattice_d3q19(double *w, int *cx, int *cy, int *cz, int *opp) {
+    for (int q = 0; q < 19; ++q) {
+        w[q] = or_d3q19_w[q]; cx[q] = or_d3q19_cx[q]; cy[q] = or_d3q19_cy[q];
+        cz[q] = or_d3q19_cz[q]; opp[q] = or_d3q19_opp[q];
+    }
+}
+
+/* equilibrium(::D2Q9, rho, ux, uy, q): src/lattice/d2q9.jl:60-67 */
+double or_equilibrium_d2q9(double rho, double ux, double uy, int q) {
+    double w = or_d2q9_w[q];
+    double cx = (double)or_d2q9_cx[q], cy = (double)or_d2q9_cy[q];
+    double cu = cx * ux + cy * uy;
+    double usq = ux * ux + uy * uy;
+    return w * rho * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * usq);
+}
+
+/* equilibrium(::D3Q19, rho, ux, uy, uz, q): src/lattice/d3q19.jl:67-75 */
+double or_equilibrium_d3q19(double rho, double ux, double uy, double uz, int q) {
+    double w = or_d3q19_w[q];
+    double cx = (double)or_d3q19_cx[q], cy = (double)or_d3q19_cy[q], cz = (double)or_d3q19_cz[q];
+    double cu = cx * ux + cy * uy + cz * uz;
+    double usq = ux * ux + uy * uy + uz * uz;
+    return w * rho * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * usq);
+}
+
+/* ------------------------------------------------------------------------ */
+/* feq_2d / moments_2d: src/kernels/equilibrium_helpers.jl:8-61             */
+/* ------------------------------------------------------------------------ */
+static inline double feq_poly(double w, double rho, double cu, double usq) {
+    return w * rho * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * usq);
+}
+
+static inline void feq2d_all(double rho, double ux, double uy, double usq, double *feq) {
+    feq[0] = 4.0 / 9.0 * rho * (1.0 - 1.5 * usq);
+    feq[1] = feq_poly(1.0 / 9.0, rho, ux, usq);
+    feq[2] = feq_poly(1.0 / 9.0, rho, uy, usq);
+    feq[3] = feq_poly(1.0 / 9.0, rho, -ux, usq);
+    feq[4] = feq_poly(1.0 / 9.0, rho, -uy, usq);
+    feq[5] = feq_poly(1.0 / 36.0, rho, ux + uy, usq);
+    feq[6] = feq_poly(1.0 / 36.0, rho, -ux + uy, usq);
+    feq[7] = feq_poly(1.0 / 36.0, rho, -ux - uy, usq);
+    feq[8] = feq_poly(1.0 / 36.0, rho, ux - uy, usq);
+}
+
+static inline void moments2d(const double *p, double *rho, double *ux, double *uy) {
+    double r = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8];
+    double inv = 1.0 / r;
+    *rho = r;
+    *ux = (p[1] - p[3] + p[5] - p[6] - p[7] + p[8]) * inv;
+    *uy = (p[2] - p[4] + p[5] + p[6] - p[7] - p[8]) * inv;
+}
+
+/* Pull with half-way bounce-back on all four edges.
+ * src/kernels/collide_stream_2d.jl:12-23 (identical in fused_bgk_2d.jl:13-24,
+ * fused_trt_2d.jl:39-51, aa_bgk_2d.jl:17-29, fused_thermal_2d.jl:10-25). */
+static inline void pull2d(const double *f, int Nx, int Ny, int i, int j, double *fp) {
+    int im = i > 0 ? i - 1 : 0, ip = i < Nx - 1 ? i + 1 : Nx - 1;
+    int jm = j > 0 ? j - 1 : 0, jp = j < Ny - 1 ? j + 1 : Ny - 1;
+    fp[0] = f[I2(i, j, 0)];
+    fp[1] = (i > 0) ? f[I2(im, j, 1)] : f[I2(i, j, 3)];
+    fp[2] = (j > 0) ? f[I2(i, jm, 2)] : f[I2(i, j, 4)];
+    fp[3] = (i < Nx - 1) ? f[I2(ip, j, 3)] : f[I2(i, j, 1)];
+    fp[4] = (j < Ny - 1) ? f[I2(i, jp, 4)] : f[I2(i, j, 2)];
+    fp[5] = (i > 0 && j > 0) ? f[I2(im, jm, 5)] : f[I2(i, j, 7)];
+    fp[6] = (i < Nx - 1 && j > 0) ? f[I2(ip, jm, 6)] : f[I2(i, j, 8)];
+    fp[7] = (i < Nx - 1 && j < Ny - 1) ? f[I2(ip, jp, 7)] : f[I2(i, j, 5)];
+    fp[8] = (i > 0 && j < Ny - 1) ? f[I2(im, jp, 8)] : f[I2(i, j, 6)];
+}
+
+/* stream_2d!: src/kernels/collide_stream_2d.jl:5-31, 77-82 */
+void or_stream_2d(double *f_out, const double *f_in, int Nx, int Ny) {
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            double fp[9];
+            pull2d(f_in, Nx, Ny, i, j, fp);
+            for (int q = 0; q < 9; ++q) f_out[I2(i, j, q)] = fp[q];
+        }
+}
+
+/* bounce_back_2d!: src/kernels/equilibrium_helpers.jl:65-70 */
+static inline void swap_pairs_2d(double *p) {
+    double t;
+    t = p[1]; p[1] = p[3]; p[3] = t;
+    t = p[2]; p[2] = p[4]; p[4] = t;
+    t = p[5]; p[5] = p[7]; p[7] = t;
+    t = p[6]; p[6] = p[8]; p[8] = t;
+}
+
+/* collide_2d!: src/kernels/collide_stream_2d.jl:35-61, 96-102 */
+void or_collide_2d(double *f, const uint8_t *solid, int Nx, int Ny, double omega) {
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            double p[9];
+            for (int q = 0; q < 9; ++q) p[q] = f[I2(i, j, q)];
+            if (solid && solid[N2(i, j)]) {
+                swap_pairs_2d(p);
+            } else {
+                double rho, ux, uy, feq[9];
+                moments2d(p, &rho, &ux, &uy);
+                double usq = ux * ux + uy * uy;
+                feq2d_all(rho, ux, uy, usq, feq);
+                for (int q = 0; q < 9; ++q) p[q] = p[q] - omega * (p[q] - feq[q]);
+            }
+            for (int q = 0; q < 9; ++q) f[I2(i, j, q)] = p[q];
+        }
+}
+
+/* apply_zou_he_north_2d!: src/kernels/boundary_2d.jl:13-60 */
+void or_zou_he_north_2d(double *f, double u, int Nx, int Ny) {
+    int j = Ny - 1;
+    for (int i = 0; i < Nx; ++i) {
+        double f1 = f[I2(i, j, 0)], f2 = f[I2(i, j, 1)], f3 = f[I2(i, j, 2)];
+        double f4 = f[I2(i, j, 3)], f6 = f[I2(i, j, 5)], f7 = f[I2(i, j, 6)];
+        double rw = (f1 + f2 + f4 + 2.0 * (f3 + f6 + f7)) / (1.0 + u * 0.0);
+        f[I2(i, j, 4)] = f3;
+        f[I2(i, j, 8)] = f7 - 0.5 * (f2 - f4) + 0.5 * rw * u;
+        f[I2(i, j, 7)] = f6 + 0.5 * (f2 - f4) - 0.5 * rw * u;
+    }
+}
+
+/* apply_zou_he_south_2d!: src/kernels/boundary_2d.jl:135-167 */
+void or_zou_he_south_2d(double *f, double u, int Nx, int Ny) {
+    int j = 0;
+    for (int i = 0; i < Nx; ++i) {
+        double f1 = f[I2(i, j, 0)], f2 = f[I2(i, j, 1)], f4 = f[I2(i, j, 3)];
+        double f5 = f[I2(i, j, 4)], f8 = f[I2(i, j, 7)], f9 = f[I2(i, j, 8)];
+        double rw = f1 + f2 + f4 + 2.0 * (f5 + f8 + f9);
+        f[I2(i, j, 2)] = f5;
+        f[I2(i, j, 5)] = f8 - 0.5 * (f2 - f4) + 0.5 * rw * u;
+        f[I2(i, j, 6)] = f9 + 0.5 * (f2 - f4) - 0.5 * rw * u;
+    }
+}
+
+/* apply_zou_he_west_2d!: src/kernels/boundary_2d.jl:171-202 */
+void or_zou_he_west_2d(double *f, double u_in, int Nx, int Ny) {
+    for (int j = 0; j < Ny; ++j) {
+        double f1 = f[I2(0, j, 0)], f3 = f[I2(0, j, 2)], f4 = f[I2(0, j, 3)];
+        double f5 = f[I2(0, j, 4)], f7 = f[I2(0, j, 6)], f8 = f[I2(0, j, 7)];
+        double rw = (f1 + f3 + f5 + 2.0 * (f4 + f7 + f8)) / (1.0 - u_in);
+        f[I2(0, j, 1)] = f4 + 2.0 / 3.0 * rw * u_in;
+        f[I2(0, j, 5)] = f8 - 0.5 * (f3 - f5) + 1.0 / 6.0 * rw * u_in;
+        f[I2(0, j, 8)] = f7 + 0.5 * (f3 - f5) + 1.0 / 6.0 * rw * u_in;
+    }
+}
+
+/* apply_zou_he_pressure_east_2d!: src/kernels/boundary_2d.jl:206-241 */
+void or_zou_he_pressure_east_2d(double *f, int Nx, int Ny, double rho_out) {
+    int i = Nx - 1;
+    for (int j = 0; j < Ny; ++j) {
+        double f1 = f[I2(i, j, 0)], f2 = f[I2(i, j, 1)], f3 = f[I2(i, j, 2)];
+        double f5 = f[I2(i, j, 4)], f6 = f[I2(i, j, 5)], f9 = f[I2(i, j, 8)];
+        double ux = -1.0 + (f1 + f3 + f5 + 2.0 * (f2 + f6 + f9)) / rho_out;
+        f[I2(i, j, 3)] = f2 - 2.0 / 3.0 * rho_out * ux;
+        f[I2(i, j, 6)] = f9 - 0.5 * (f3 - f5) - 1.0 / 6.0 * rho_out * ux;
+        f[I2(i, j, 7)] = f6 + 0.5 * (f3 - f5) - 1.0 / 6.0 * rho_out * ux;
+    }
+}
+
+/* apply_zou_he_pressure_west_2d!: src/kernels/boundary_2d.jl:264-299 */
+void or_zou_he_pressure_west_2d(double *f, int Nx, int Ny, double rho_in) {
+    (void)Nx;
+    for (int j = 0; j < Ny; ++j) {
+        double f1 = f[I2(0, j, 0)], f3 = f[I2(0, j, 2)], f4 = f[I2(0, j, 3)];
+        double f5 = f[I2(0, j, 4)], f7 = f[I2(0, j, 6)], f8 = f[I2(0, j, 7)];
+        double ux = 1.0 - (f1 + f3 + f5 + 2.0 * (f4 + f7 + f8)) / rho_in;
+        f[I2(0, j, 1)] = f4 + 2.0 / 3.0 * rho_in * ux;
+        f[I2(0, j, 5)] = f8 - 0.5 * (f3 - f5) + 1.0 / 6.0 * rho_in * ux;
+        f[I2(0, j, 8)] = f7 + 0.5 * (f3 - f5) + 1.0 / 6.0 * rho_in * ux;
+    }
+}
+
+/* apply_extrapolate_east_2d!: src/kernels/boundary_2d.jl:303-323 */
+void or_extrapolate_east_2d(double *f, int Nx, int Ny) {
+    for (int j = 0; j < Ny; ++j)
+        for (int q = 0; q < 9; ++q) f[I2(Nx - 1, j, q)] = f[I2(Nx - 2, j, q)];
+}
+
+/* bounce_back_walls_2d_kernel!: src/kernels/boundary_2d.jl:64-90.
+ * wall_id: 1 south, 2 west, 3 east, 4 north (same codes as the reference). */
+void or_bounce_back_wall_2d(double *f, int Nx, int Ny, int wall_id) {
+    if (wall_id == 1) {
+        for (int i = 0; i < Nx; ++i) {
+            f[I2(i, 0, 2)] = f[I2(i, 0, 4)];
+            f[I2(i, 0, 5)] = f[I2(i, 0, 7)];
+            f[I2(i, 0, 6)] = f[I2(i, 0, 8)];
+        }
+    } else if (wall_id == 2) {
+        for (int j = 0; j < Ny; ++j) {
+            f[I2(0, j, 1)] = f[I2(0, j, 3)];
+            f[I2(0, j, 5)] = f[I2(0, j, 7)];
+            f[I2(0, j, 8)] = f[I2(0, j, 6)];
+        }
+    } else if (wall_id == 3) {
+        for (int j = 0; j < Ny; ++j) {
+            f[I2(Nx - 1, j, 3)] = f[I2(Nx - 1, j, 1)];
+            f[I2(Nx - 1, j, 6)] = f[I2(Nx - 1, j, 8)];
+            f[I2(Nx - 1, j, 7)] = f[I2(Nx - 1, j, 5)];
+        }
+    } else if (wall_id == 4) {
+        for (int i = 0; i < Nx; ++i) {
+            f[I2(i, Ny - 1, 4)] = f[I2(i, Ny - 1, 2)];
+            f[I2(i, Ny - 1, 7)] = f[I2(i, Ny - 1, 5)];
+            f[I2(i, Ny - 1, 8)] = f[I2(i, Ny - 1, 6)];
+        }
+    }
+}
+
+/* compute_macroscopic_2d!: src/kernels/macroscopic.jl:5-38 */
+void or_macroscopic_2d(double *rho, double *ux, double *uy, const double *f, int Nx, int Ny) {
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            double p[9];
+            for (int q = 0; q < 9; ++q) p[q] = f[I2(i, j, q)];
+            double r = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8];
+            double inv = 1.0 / r;
+            rho[N2(i, j)] = r;
+            ux[N2(i, j)] = (p[1] - p[3] + p[5] - p[6] - p[7] + p[8]) * inv;
+            uy[N2(i, j)] = (p[2] - p[4] + p[5] + p[6] - p[7] - p[8]) * inv;
+        }
+}
+
+/* fused_bgk_step!: src/kernels/fused_bgk_2d.jl:8-72 */
+void or_fused_bgk_2d(double *f_out, const double *f_in, double *rho_o, double *ux_o, double *uy_o,
+                     const uint8_t *solid, int Nx, int Ny, double omega) {
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            double p[9];
+            pull2d(f_in, Nx, Ny, i, j, p);
+            if (solid && solid[N2(i, j)]) {
+                swap_pairs_2d(p);
+                for (int q = 0; q < 9; ++q) f_out[I2(i, j, q)] = p[q];
+                rho_o[N2(i, j)] = 1.0; ux_o[N2(i, j)] = 0.0; uy_o[N2(i, j)] = 0.0;
+            } else {
+                double rho, ux, uy, feq[9];
+                moments2d(p, &rho, &ux, &uy);
+                double usq = ux * ux + uy * uy;
+                feq2d_all(rho, ux, uy, usq, feq);
+                for (int q = 0; q < 9; ++q) f_out[I2(i, j, q)] = p[q] - omega * (p[q] - feq[q]);
+                rho_o[N2(i, j)] = rho; ux_o[N2(i, j)] = ux; uy_o[N2(i, j)] = uy;
+            }
+        }
+}
+
+/* trt_rates(nu; Lambda): src/kernels/fused_trt_2d.jl:129-133 */
+void or_trt_rates(double nu, double lambda, double *s_plus, double *s_minus) {
+    *s_plus = 1.0 / (3.0 * nu + 0.5);
+    *s_minus = 1.0 / (lambda / (3.0 * nu) + 0.5);
+}
+
+/* TRT collide of one node given pulled p[] (fused_trt_2d.jl:65-94). */
+static inline void trt2d_node(double *p, double sp, double sm, double *rho, double *ux, double *uy) {
+    double feq[9];
+    moments2d(p, rho, ux, uy);
+    double usq = (*ux) * (*ux) + (*uy) * (*uy);
+    feq2d_all(*rho, *ux, *uy, usq, feq);
+    double a = (sp + sm) * 0.5, b = (sp - sm) * 0.5;
+    double o[9];
+    o[0] = p[0] - sp * (p[0] - feq[0]);
+    o[1] = p[1] - a * (p[1] - feq[1]) - b * (p[3] - feq[3]);
+    o[3] = p[3] - a * (p[3] - feq[3]) - b * (p[1] - feq[1]);
+    o[2] = p[2] - a * (p[2] - feq[2]) - b * (p[4] - feq[4]);
+    o[4] = p[4] - a * (p[4] - feq[4]) - b * (p[2] - feq[2]);
+    o[5] = p[5] - a * (p[5] - feq[5]) - b * (p[7] - feq[7]);
+    o[7] = p[7] - a * (p[7] - feq[7]) - b * (p[5] - feq[5]);
+    o[6] = p[6] - a * (p[6] - feq[6]) - b * (p[8] - feq[8]);
+    o[8] = p[8] - a * (p[8] - feq[8]) - b * (p[6] - feq[6]);
+    for (int q = 0; q < 9; ++q) p[q] = o[q];
+}
+
+/* fused_trt_step!: src/kernels/fused_trt_2d.jl:29-101, 145-153.  The caller
+ * passes the rates already rounded to the storage type (as ET(s_plus)). */
+void or_fused_trt_2d(double *f_out, const double *f_in, double *rho_o, double *ux_o, double *uy_o,
+                     const uint8_t *solid, int Nx, int Ny, double sp, double sm) {
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            double p[9];
+            pull2d(f_in, Nx, Ny, i, j, p);
+            if (solid && solid[N2(i, j)]) {
+                swap_pairs_2d(p);
+                for (int q = 0; q < 9; ++q) f_out[I2(i, j, q)] = p[q];
+                rho_o[N2(i, j)] = 1.0; ux_o[N2(i, j)] = 0.0; uy_o[N2(i, j)] = 0.0;
+            } else {
+                double rho, ux, uy;
+                trt2d_node(p, sp, sm, &rho, &ux, &uy);
+                for (int q = 0; q < 9; ++q) f_out[I2(i, j, q)] = p[q];
+                rho_o[N2(i, j)] = rho; ux_o[N2(i, j)] = ux; uy_o[N2(i, j)] = uy;
+            }
+        }
+}
+
+/* aa_even_step!: src/kernels/aa_bgk_2d.jl:14-53.  Single buffer.  Every node
+ * pulls from its neighbours and writes its own slots; the reference runs this
+ * as one parallel kernel, which is race-free because under the A-A layout each
+ * slot read by a node is written only by that same node.  The oracle reads
+ * from a snapshot to express the same data-parallel semantics. */
+void or_aa_even_2d(double *f, const uint8_t *solid, int Nx, int Ny, double omega) {
+    size_t n = (size_t)Nx * Ny * 9;
+    double *src = (double *)malloc(n * sizeof(double));
+    memcpy(src, f, n * sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            double p[9];
+            pull2d(src, Nx, Ny, i, j, p);
+            if (solid && solid[N2(i, j)]) {
+                f[I2(i, j, 1)] = p[3]; f[I2(i, j, 3)] = p[1];
+                f[I2(i, j, 2)] = p[4]; f[I2(i, j, 4)] = p[2];
+                f[I2(i, j, 5)] = p[7]; f[I2(i, j, 7)] = p[5];
+                f[I2(i, j, 6)] = p[8]; f[I2(i, j, 8)] = p[6];
+            } else {
+                double rho, ux, uy, feq[9];
+                moments2d(p, &rho, &ux, &uy);
+                double usq = ux * ux + uy * uy;
+                feq2d_all(rho, ux, uy, usq, feq);
+                for (int q = 0; q < 9; ++q) f[I2(i, j, q)] = p[q] - omega * (p[q] - feq[q]);
+            }
+        }
+    free(src);
+}
+
+/* aa_odd_step!: src/kernels/aa_bgk_2d.jl:57-115.  Read local, collide, push. */
+void or_aa_odd_2d(double *f, const uint8_t *solid, int Nx, int Ny, double omega) {
+    size_t n = (size_t)Nx * Ny * 9;
+    double *src = (double *)malloc(n * sizeof(double));
+    memcpy(src, f, n * sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            double p[9];
+            for (int q = 0; q < 9; ++q) p[q] = src[I2(i, j, q)];
+            if (solid && solid[N2(i, j)]) {
+                f[I2(i, j, 1)] = p[3]; f[I2(i, j, 3)] = p[1];
+                f[I2(i, j, 2)] = p[4]; f[I2(i, j, 4)] = p[2];
+                f[I2(i, j, 5)] = p[7]; f[I2(i, j, 7)] = p[5];
+                f[I2(i, j, 6)] = p[8]; f[I2(i, j, 8)] = p[6];
+                continue;
+            }
+            double rho, ux, uy, feq[9], c[9];
+            moments2d(p, &rho, &ux, &uy);
+            double usq = ux * ux + uy * uy;
+            feq2d_all(rho, ux, uy, usq, feq);
+            for (int q = 0; q < 9; ++q) c[q] = p[q] - omega * (p[q] - feq[q]);
+            int im = i > 0 ? i - 1 : 0, ip = i < Nx - 1 ? i + 1 : Nx - 1;
+            int jm = j > 0 ? j - 1 : 0, jp = j < Ny - 1 ? j + 1 : Ny - 1;
+            f[I2(i, j, 0)] = c[0];
+            f[I2(i < Nx - 1 ? ip : i, j, 1)] = i < Nx - 1 ? c[1] : c[3];
+            f[I2(i, j < Ny - 1 ? jp : j, 2)] = j < Ny - 1 ? c[2] : c[4];
+            f[I2(i > 0 ? im : i, j, 3)] = i > 0 ? c[3] : c[1];
+            f[I2(i, j > 0 ? jm : j, 4)] = j > 0 ? c[4] : c[2];
+            int c6 = i < Nx - 1 && j < Ny - 1;
+            f[I2(c6 ? ip : i, c6 ? jp : j, 5)] = c6 ? c[5] : c[7];
+            int c7 = i > 0 && j < Ny - 1;
+            f[I2(c7 ? im : i, c7 ? jp : j, 6)] = c7 ? c[6] : c[8];
+            int c8 = i > 0 && j > 0;
+            f[I2(c8 ? im : i, c8 ? jm : j, 7)] = c8 ? c[7] : c[5];
+            int c9 = i < Nx - 1 && j > 0;
+            f[I2(c9 ? ip : i, c9 ? jm : j, 8)] = c9 ? c[8] : c[6];
+        }
+    free(src);
+}
+
+/* collide_mrt_2d!: src/kernels/collide_mrt_2d.jl:43-125.  s_nu is passed in
+ * already computed as 1/(3 nu + 0.5) (collide_mrt_2d.jl:122). */
+void or_collide_mrt_2d(double *f, const uint8_t *solid, int Nx, int Ny,
+                       double s_e, double s_eps, double s_q, double s_nu) {
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            double p[9];
+            for (int q = 0; q < 9; ++q) p[q] = f[I2(i, j, q)];
+            if (solid && solid[N2(i, j)]) {
+                swap_pairs_2d(p);
+                for (int q = 0; q < 9; ++q) f[I2(i, j, q)] = p[q];
+                continue;
+            }
+            double f1 = p[0], f2 = p[1], f3 = p[2], f4 = p[3], f5 = p[4];
+            double f6 = p[5], f7 = p[6], f8 = p[7], f9 = p[8];
+            double rho = f1 + f2 + f3 + f4 + f5 + f6 + f7 + f8 + f9;
+            double e = -4.0 * f1 - f2 - f3 - f4 - f5 + 2.0 * (f6 + f7 + f8 + f9);
+            double eps = 4.0 * f1 - 2.0 * (f2 + f3 + f4 + f5) + f6 + f7 + f8 + f9;
+            double jx = f2 - f4 + f6 - f7 - f8 + f9;
+            double qx = -2.0 * f2 + 2.0 * f4 + f6 - f7 - f8 + f9;
+            double jy = f3 - f5 + f6 + f7 - f8 - f9;
+            double qy = -2.0 * f3 + 2.0 * f5 + f6 + f7 - f8 - f9;
+            double pxx = f2 - f3 + f4 - f5;
+            double pxy = f6 - f7 + f8 - f9;
+            double inv = 1.0 / rho;
+            double ux = jx * inv, uy = jy * inv;
+            double usq = ux * ux + uy * uy;
+            double e_eq = -2.0 * rho + 3.0 * rho * usq;
+            double eps_eq = rho - 3.0 * rho * usq;
+            double qx_eq = -rho * ux;
+            double qy_eq = -rho * uy;
+            double pxx_eq = rho * (ux * ux - uy * uy);
+            double pxy_eq = rho * ux * uy;
+            double es = e - s_e * (e - e_eq);
+            double ep = eps - s_eps * (eps - eps_eq);
+            double qxs = qx - s_q * (qx - qx_eq);
+            double qys = qy - s_q * (qy - qy_eq);
+            double ps = pxx - s_nu * (pxx - pxx_eq);
+            double pxys = pxy - s_nu * (pxy - pxy_eq);
+            double r = rho, jxs = jx, jys = jy;
+            const double c9 = 1.0 / 9.0, c36 = 1.0 / 36.0, c18 = 1.0 / 18.0, c6 = 1.0 / 6.0,
+                         c4 = 1.0 / 4.0, c12 = 1.0 / 12.0;
+            f[I2(i, j, 0)] = c9 * r - c9 * es + c9 * ep;
+            f[I2(i, j, 1)] = c9 * r - c36 * es - c18 * ep + c6 * jxs - c6 * qxs + c4 * ps;
+            f[I2(i, j, 2)] = c9 * r - c36 * es - c18 * ep + c6 * jys - c6 * qys - c4 * ps;
+            f[I2(i, j, 3)] = c9 * r - c36 * es - c18 * ep - c6 * jxs + c6 * qxs + c4 * ps;
+            f[I2(i, j, 4)] = c9 * r - c36 * es - c18 * ep - c6 * jys + c6 * qys - c4 * ps;
+            f[I2(i, j, 5)] = c9 * r + c18 * es + c36 * ep + c6 * jxs + c12 * qxs + c6 * jys + c12 * qys + c4 * pxys;
+            f[I2(i, j, 6)] = c9 * r + c18 * es + c36 * ep - c6 * jxs - c12 * qxs + c6 * jys + c12 * qys - c4 * pxys;
+            f[I2(i, j, 7)] = c9 * r + c18 * es + c36 * ep - c6 * jxs - c12 * qxs - c6 * jys - c12 * qys + c4 * pxys;
+            f[I2(i, j, 8)] = c9 * r + c18 * es + c36 * ep + c6 * jxs + c12 * qxs - c6 * jys - c12 * qys - c4 * pxys;
+        }
+}
+
+/* stream_fully_periodic_2d!: src/kernels/stream_periodic_2d.jl:79-117 */
+void or_stream_fully_periodic_2d(double *f_out, const double *f_in, int Nx, int Ny) {
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            int ip = i > 0 ? i - 1 : Nx - 1, im = i < Nx - 1 ? i + 1 : 0;
+            int jp = j > 0 ? j - 1 : Ny - 1, jm = j < Ny - 1 ? j + 1 : 0;
+            f_out[I2(i, j, 0)] = f_in[I2(i, j, 0)];
+            f_out[I2(i, j, 1)] = f_in[I2(ip, j, 1)];
+            f_out[I2(i, j, 2)] = f_in[I2(i, jp, 2)];
+            f_out[I2(i, j, 3)] = f_in[I2(im, j, 3)];
+            f_out[I2(i, j, 4)] = f_in[I2(i, jm, 4)];
+            f_out[I2(i, j, 5)] = f_in[I2(ip, jp, 5)];
+            f_out[I2(i, j, 6)] = f_in[I2(im, jp, 6)];
+            f_out[I2(i, j, 7)] = f_in[I2(im, jm, 7)];
+            f_out[I2(i, j, 8)] = f_in[I2(ip, jm, 8)];
+        }
+}
+
+/* stream_periodic_x_wall_y_2d!: src/kernels/stream_periodic_2d.jl:5-75 */
+void or_stream_periodic_x_wall_y_2d(double *f_out, const double *f_in, int Nx, int Ny) {
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            int jm1 = j > 0 ? j - 1 : j, jp1 = j < Ny - 1 ? j + 1 : j;
+            int iw = i > 0 ? i - 1 : Nx - 1, ie = i < Nx - 1 ? i + 1 : 0;
+            f_out[I2(i, j, 0)] = f_in[I2(i, j, 0)];
+            f_out[I2(i, j, 1)] = f_in[I2(iw, j, 1)];
+            f_out[I2(i, j, 2)] = j > 0 ? f_in[I2(i, jm1, 2)] : f_in[I2(i, j, 4)];
+            f_out[I2(i, j, 3)] = f_in[I2(ie, j, 3)];
+            f_out[I2(i, j, 4)] = j < Ny - 1 ? f_in[I2(i, jp1, 4)] : f_in[I2(i, j, 2)];
+            f_out[I2(i, j, 5)] = j > 0 ? f_in[I2(iw, jm1, 5)] : f_in[I2(i, j, 7)];
+            f_out[I2(i, j, 6)] = j > 0 ? f_in[I2(ie, jm1, 6)] : f_in[I2(i, j, 8)];
+            f_out[I2(i, j, 7)] = j < Ny - 1 ? f_in[I2(ie, jp1, 7)] : f_in[I2(i, j, 5)];
+            f_out[I2(i, j, 8)] = j < Ny - 1 ? f_in[I2(iw, jp1, 8)] : f_in[I2(i, j, 6)];
+        }
+}
+
+/* The path-B cavity driver, run_cavity_2d: src/drivers/basic.jl:112-144.
+ * f_in/f_out ping-pong; on return f_a holds the latest populations. */
+void or_run_cavity_2d(double *f_a, double *f_b, double *rho, double *ux, double *uy,
+                      const uint8_t *solid, int Nx, int Ny, double omega, double u_lid, int steps) {
+    double *fi = f_a, *fo = f_b;
+    size_t n = (size_t)Nx * Ny * 9;
+    for (int s = 0; s < steps; ++s) {
+        or_stream_2d(fo, fi, Nx, Ny);
+        or_zou_he_north_2d(fo, u_lid, Nx, Ny);
+        or_collide_2d(fo, solid, Nx, Ny, omega);
+        or_macroscopic_2d(rho, ux, uy, fo, Nx, Ny);
+        double *t = fi; fi = fo; fo = t;
+    }
+    if (fi != f_a) memcpy(f_a, fi, n * sizeof(double));
+}
+
+/* ------------------------------------------------------------------------ */
+/* D3Q19                                                                     */
+/* ------------------------------------------------------------------------ */
+
+static inline void feq3d_all(double rho, double ux, double uy, double uz, double usq, double *feq) {
+    const double wr = 1.0 / 3.0, wa = 1.0 / 18.0, we = 1.0 / 36.0;
+    feq[0] = wr * rho * (1.0 - 1.5 * usq);
+    feq[1] = feq_poly(wa, rho, ux, usq);
+    feq[2] = feq_poly(wa, rho, -ux, usq);
+    feq[3] = feq_poly(wa, rho, uy, usq);
+    feq[4] = feq_poly(wa, rho, -uy, usq);
+    feq[5] = feq_poly(wa, rho, uz, usq);
+    feq[6] = feq_poly(wa, rho, -uz, usq);
+    feq[7] = feq_poly(we, rho, ux + uy, usq);
+    feq[8] = feq_poly(we, rho, -ux + uy, usq);
+    feq[9] = feq_poly(we, rho, ux - uy, usq);
+    feq[10] = feq_poly(we, rho, -ux - uy, usq);
+    feq[11] = feq_poly(we, rho, ux + uz, usq);
+    feq[12] = feq_poly(we, rho, -ux + uz, usq);
+    feq[13] = feq_poly(we, rho, ux - uz, usq);
+    feq[14] = feq_poly(we, rho, -ux - uz, usq);
+    feq[15] = feq_poly(we, rho, uy + uz, usq);
+    feq[16] = feq_poly(we, rho, -uy + uz, usq);
+    feq[17] = feq_poly(we, rho, uy - uz, usq);
+    feq[18] = feq_poly(we, rho, -uy - uz, usq);
+}
+
+/* moments_3d: src/kernels/equilibrium_helpers_3d.jl:102-112 (also
+ * collide_stream_3d.jl:69-73 and macroscopic.jl:53-59, same order). */
+static inline void moments3d(const double *p, double *rho, double *ux, double *uy, double *uz) {
+    double r = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8] + p[9] +
+               p[10] + p[11] + p[12] + p[13] + p[14] + p[15] + p[16] + p[17] + p[18];
+    double inv = 1.0 / r;
+    *rho = r;
+    *ux = (p[1] - p[2] + p[7] - p[8] + p[9] - p[10] + p[11] - p[12] + p[13] - p[14]) * inv;
+    *uy = (p[3] - p[4] + p[7] + p[8] - p[9] - p[10] + p[15] - p[16] + p[17] - p[18]) * inv;
+    *uz = (p[5] - p[6] + p[11] + p[12] - p[13] - p[14] + p[15] + p[16] - p[17] - p[18]) * inv;
+}
+
+/* Pull with half-way bounce-back, per-axis optionally periodic.
+ * Walls on every axis: src/kernels/collide_stream_3d.jl:5-42 and the DSL brick
+ * PullHalfwayBB_3D{false} (src/kernels/dsl/bricks_3d.jl:70-100).  Periodic z:
+ * PullHalfwayBB_3D{true} (bricks_3d.jl:106-136).  Periodic x and y are the
+ * same wrap rule extended to the other two axes (no reference counterpart; the
+ * reference has no fully periodic D3Q19 pull). */
+static inline void pull3d(const double *f, int Nx, int Ny, int Nz, int i, int j, int k,
+                          int per_x, int per_y, int per_z, double *fp) {
+    /* neighbour index along each axis for c = -1 (source at +1) and c = +1 */
+    int im = i > 0 ? i - 1 : (per_x ? Nx - 1 : 0);
+    int ip = i < Nx - 1 ? i + 1 : (per_x ? 0 : Nx - 1);
+    int jm = j > 0 ? j - 1 : (per_y ? Ny - 1 : 0);
+    int jp = j < Ny - 1 ? j + 1 : (per_y ? 0 : Ny - 1);
+    int km = k > 0 ? k - 1 : (per_z ? Nz - 1 : 0);
+    int kp = k < Nz - 1 ? k + 1 : (per_z ? 0 : Nz - 1);
+    /* "source exists" flags: true when the pull stays inside or wraps */
+    int xm = per_x || i > 0, xp = per_x || i < Nx - 1;
+    int ym = per_y || j > 0, yp = per_y || j < Ny - 1;
+    int zm = per_z || k > 0, zp = per_z || k < Nz - 1;
+    fp[0] = f[I3(i, j, k, 0)];
+    fp[1] = xm ? f[I3(im, j, k, 1)] : f[I3(i, j, k, 2)];
+    fp[2] = xp ? f[I3(ip, j, k, 2)] : f[I3(i, j, k, 1)];
+    fp[3] = ym ? f[I3(i, jm, k, 3)] : f[I3(i, j, k, 4)];
+    fp[4] = yp ? f[I3(i, jp, k, 4)] : f[I3(i, j, k, 3)];
+    fp[5] = zm ? f[I3(i, j, km, 5)] : f[I3(i, j, k, 6)];
+    fp[6] = zp ? f[I3(i, j, kp, 6)] : f[I3(i, j, k, 5)];
+    fp[7] = (xm && ym) ? f[I3(im, jm, k, 7)] : f[I3(i, j, k, 10)];
+    fp[8] = (xp && ym) ? f[I3(ip, jm, k, 8)] : f[I3(i, j, k, 9)];
+    fp[9] = (xm && yp) ? f[I3(im, jp, k, 9)] : f[I3(i, j, k, 8)];
+    fp[10] = (xp && yp) ? f[I3(ip, jp, k, 10)] : f[I3(i, j, k, 7)];
+    fp[11] = (xm && zm) ? f[I3(im, j, km, 11)] : f[I3(i, j, k, 14)];
+    fp[12] = (xp && zm) ? f[I3(ip, j, km, 12)] : f[I3(i, j, k, 13)];
+    fp[13] = (xm && zp) ? f[I3(im, j, kp, 13)] : f[I3(i, j, k, 12)];
+    fp[14] = (xp && zp) ? f[I3(ip, j, kp, 14)] : f[I3(i, j, k, 11)];
+    fp[15] = (ym && zm) ? f[I3(i, jm, km, 15)] : f[I3(i, j, k, 18)];
+    fp[16] = (yp && zm) ? f[I3(i, jp, km, 16)] : f[I3(i, j, k, 17)];
+    fp[17] = (ym && zp) ? f[I3(i, jm, kp, 17)] : f[I3(i, j, k, 16)];
+    fp[18] = (yp && zp) ? f[I3(i, jp, kp, 18)] : f[I3(i, j, k, 15)];
+}
+
+/* stream_3d!: src/kernels/collide_stream_3d.jl:5-42, 119-123 */
+void or_stream_3d(double *f_out, const double *f_in, int Nx, int Ny, int Nz) {
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                double fp[19];
+                pull3d(f_in, Nx, Ny, Nz, i, j, k, 0, 0, 0, fp);
+                for (int q = 0; q < 19; ++q) f_out[I3(i, j, k, q)] = fp[q];
+            }
+}
+
+static inline void swap_pairs_3d(double *p) {
+    static const int a[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16};
+    static const int b[9] = {2, 4, 6, 10, 9, 14, 13, 18, 17};
+    for (int n = 0; n < 9; ++n) { double t = p[a[n]]; p[a[n]] = p[b[n]]; p[b[n]] = t; }
+}
+
+/* collide_3d!: src/kernels/collide_stream_3d.jl:46-103, 137-142 */
+void or_collide_3d(double *f, const uint8_t *solid, int Nx, int Ny, int Nz, double omega) {
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                double p[19];
+                for (int q = 0; q < 19; ++q) p[q] = f[I3(i, j, k, q)];
+                if (solid && solid[N3(i, j, k)]) {
+                    swap_pairs_3d(p);
+                } else {
+                    double rho, ux, uy, uz, feq[19];
+                    moments3d(p, &rho, &ux, &uy, &uz);
+                    double usq = ux * ux + uy * uy + uz * uz;
+                    feq3d_all(rho, ux, uy, uz, usq, feq);
+                    for (int q = 0; q < 19; ++q) p[q] = p[q] - omega * (p[q] - feq[q]);
+                }
+                for (int q = 0; q < 19; ++q) f[I3(i, j, k, q)] = p[q];
+            }
+}
+
+/* compute_macroscopic_3d!: src/kernels/macroscopic.jl:42-80 */
+void or_macroscopic_3d(double *rho, double *ux, double *uy, double *uz, const double *f,
+                       int Nx, int Ny, int Nz) {
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                double p[19];
+                for (int q = 0; q < 19; ++q) p[q] = f[I3(i, j, k, q)];
+                double r, a, b, c;
+                moments3d(p, &r, &a, &b, &c);
+                rho[N3(i, j, k)] = r; ux[N3(i, j, k)] = a; uy[N3(i, j, k)] = b; uz[N3(i, j, k)] = c;
+            }
+}
+
+/* Zou-He velocity face descriptors: src/kernels/boundary_3d.jl:39-137.
+ * Face codes: 0 west, 1 east, 2 south, 3 north, 4 bottom, 5 top.
+ * Population indices are 0-based here (reference 1-based minus one). */
+typedef struct {
+    int normal_axis, sign, q_axis, q_axis_opp, q_diag[4], q_diag_opp[4];
+    int t1p, t1m, t2p, t2m, parallel[9], outgoing[5];
+} or_face3d;
+
+static const or_face3d or_faces[6] = {
+    {1, -1, 1, 2, {7, 9, 11, 13}, {10, 8, 14, 12}, 3, 4, 5, 6, {0, 3, 4, 5, 6, 15, 16, 17, 18}, {2, 8, 10, 12, 14}},
+    {1, 1, 2, 1, {8, 10, 12, 14}, {9, 7, 13, 11}, 3, 4, 5, 6, {0, 3, 4, 5, 6, 15, 16, 17, 18}, {1, 7, 9, 11, 13}},
+    {2, -1, 3, 4, {7, 8, 15, 17}, {10, 9, 18, 16}, 1, 2, 5, 6, {0, 1, 2, 5, 6, 11, 12, 13, 14}, {4, 9, 10, 16, 18}},
+    {2, 1, 4, 3, {9, 10, 16, 18}, {8, 7, 17, 15}, 1, 2, 5, 6, {0, 1, 2, 5, 6, 11, 12, 13, 14}, {3, 7, 8, 15, 17}},
+    {3, -1, 5, 6, {11, 12, 15, 16}, {14, 13, 18, 17}, 1, 2, 3, 4, {0, 1, 2, 3, 4, 7, 8, 9, 10}, {6, 13, 14, 17, 18}},
+    {3, 1, 6, 5, {13, 14, 17, 18}, {12, 11, 16, 15}, 1, 2, 3, 4, {0, 1, 2, 3, 4, 7, 8, 9, 10}, {5, 11, 12, 15, 16}},
+};
+
+/* zou_he_velocity_3d_kernel!: src/kernels/boundary_3d.jl:154-223.
+ * idx_fixed is 0-based. */
+void or_zou_he_velocity_3d(double *f, int Nx, int Ny, int Nz, int face, int idx_fixed,
+                           double u_n, double u_t1, double u_t2) {
+    const or_face3d *F = &or_faces[face];
+    int N1 = F->normal_axis == 1 ? Ny : Nx;
+    int N2v = F->normal_axis == 3 ? Ny : Nz;
+    for (int b = 0; b < N2v; ++b)
+        for (int a = 0; a < N1; ++a) {
+            int i, j, k;
+            if (F->normal_axis == 1) { i = idx_fixed; j = a; k = b; }
+            else if (F->normal_axis == 2) { i = a; j = idx_fixed; k = b; }
+            else { i = a; j = b; k = idx_fixed; }
+            double sum_par = 0.0, sum_out = 0.0;
+            for (int n = 0; n < 9; ++n) sum_par += f[I3(i, j, k, F->parallel[n])];
+            for (int n = 0; n < 5; ++n) sum_out += f[I3(i, j, k, F->outgoing[n])];
+            double sg = (double)F->sign;
+            double denom = 1.0 + sg * u_n;
+            double rw = (sum_par + 2.0 * sum_out) / denom;
+            f[I3(i, j, k, F->q_axis)] = f[I3(i, j, k, F->q_axis_opp)] - sg * (1.0 / 3.0) * rw * u_n;
+            double d1 = f[I3(i, j, k, F->parallel[5])], d2 = f[I3(i, j, k, F->parallel[6])];
+            double d3 = f[I3(i, j, k, F->parallel[7])], d4 = f[I3(i, j, k, F->parallel[8])];
+            double t1 = (f[I3(i, j, k, F->t1p)] - f[I3(i, j, k, F->t1m)]) + (d1 - d2 + d3 - d4);
+            double t2 = (f[I3(i, j, k, F->t2p)] - f[I3(i, j, k, F->t2m)]) + (d1 + d2 - d3 - d4);
+            f[I3(i, j, k, F->q_diag[0])] = f[I3(i, j, k, F->q_diag_opp[0])] - 0.5 * t1 + 0.5 * rw * u_t1 - sg * (1.0 / 6.0) * rw * u_n;
+            f[I3(i, j, k, F->q_diag[1])] = f[I3(i, j, k, F->q_diag_opp[1])] + 0.5 * t1 - 0.5 * rw * u_t1 - sg * (1.0 / 6.0) * rw * u_n;
+            f[I3(i, j, k, F->q_diag[2])] = f[I3(i, j, k, F->q_diag_opp[2])] - 0.5 * t2 + 0.5 * rw * u_t2 - sg * (1.0 / 6.0) * rw * u_n;
+            f[I3(i, j, k, F->q_diag[3])] = f[I3(i, j, k, F->q_diag_opp[3])] + 0.5 * t2 - 0.5 * rw * u_t2 - sg * (1.0 / 6.0) * rw * u_n;
+        }
+}
+
+/* zou_he_pressure_3d_kernel!: src/kernels/boundary_3d.jl:232-288 */
+void or_zou_he_pressure_3d(double *f, int Nx, int Ny, int Nz, int face, int idx_fixed,
+                           double rho_out) {
+    const or_face3d *F = &or_faces[face];
+    int N1 = F->normal_axis == 1 ? Ny : Nx;
+    int N2v = F->normal_axis == 3 ? Ny : Nz;
+    for (int b = 0; b < N2v; ++b)
+        for (int a = 0; a < N1; ++a) {
+            int i, j, k;
+            if (F->normal_axis == 1) { i = idx_fixed; j = a; k = b; }
+            else if (F->normal_axis == 2) { i = a; j = idx_fixed; k = b; }
+            else { i = a; j = b; k = idx_fixed; }
+            double sum_par = 0.0, sum_out = 0.0;
+            for (int n = 0; n < 9; ++n) sum_par += f[I3(i, j, k, F->parallel[n])];
+            for (int n = 0; n < 5; ++n) sum_out += f[I3(i, j, k, F->outgoing[n])];
+            double sg = (double)F->sign;
+            double u_n = -sg * (1.0 - (sum_par + 2.0 * sum_out) / rho_out);
+            f[I3(i, j, k, F->q_axis)] = f[I3(i, j, k, F->q_axis_opp)] - sg * (1.0 / 3.0) * rho_out * u_n;
+            double t1 = f[I3(i, j, k, F->t1p)] - f[I3(i, j, k, F->t1m)];
+            double t2 = f[I3(i, j, k, F->t2p)] - f[I3(i, j, k, F->t2m)];
+            f[I3(i, j, k, F->q_diag[0])] = f[I3(i, j, k, F->q_diag_opp[0])] - 0.5 * t1 - sg * (1.0 / 6.0) * rho_out * u_n;
+            f[I3(i, j, k, F->q_diag[1])] = f[I3(i, j, k, F->q_diag_opp[1])] + 0.5 * t1 - sg * (1.0 / 6.0) * rho_out * u_n;
+            f[I3(i, j, k, F->q_diag[2])] = f[I3(i, j, k, F->q_diag_opp[2])] - 0.5 * t2 - sg * (1.0 / 6.0) * rho_out * u_n;
+            f[I3(i, j, k, F->q_diag[3])] = f[I3(i, j, k, F->q_diag_opp[3])] + 0.5 * t2 - sg * (1.0 / 6.0) * rho_out * u_n;
+        }
+}
+
+/* apply_zou_he_top_3d!: src/kernels/boundary_3d.jl:326-330 */
+void or_zou_he_top_3d(double *f, double u_wall_x, int Nx, int Ny, int Nz) {
+    or_zou_he_velocity_3d(f, Nx, Ny, Nz, 5, Nz - 1, 0.0, u_wall_x, 0.0);
+}
+
+/* run_cavity_3d: src/drivers/basic.jl:153-176 */
+void or_run_cavity_3d(double *f_a, double *f_b, double *rho, double *ux, double *uy, double *uz,
+                      const uint8_t *solid, int Nx, int Ny, int Nz, double omega, double u_lid, int steps) {
+    double *fi = f_a, *fo = f_b;
+    size_t n = (size_t)Nx * Ny * Nz * 19;
+    for (int s = 0; s < steps; ++s) {
+        or_stream_3d(fo, fi, Nx, Ny, Nz);
+        or_zou_he_top_3d(fo, u_lid, Nx, Ny, Nz);
+        or_collide_3d(fo, solid, Nx, Ny, Nz, omega);
+        or_macroscopic_3d(rho, ux, uy, uz, fo, Nx, Ny, Nz);
+        double *t = fi; fi = fo; fo = t;
+    }
+    if (fi != f_a) memcpy(f_a, fi, n * sizeof(double));
+}
+
+/* Fused D3Q19 TRT step: the DSL spec PullHalfwayBB_3D + SolidInert_3D +
+ * Moments_3D + CollideTRTDirect_3D + WriteMoments_3D
+ * (src/kernels/li_bb_3d_v2.jl:13-42 with no LI-BB links flagged;
+ * bricks_3d.jl:64-230, 476-483).  rho/ux/uy/uz may be NULL: the moment write
+ * is then skipped (populations are unaffected). */
+void or_fused_trt_3d(double *f_out, const double *f_in, double *rho_o, double *ux_o, double *uy_o,
+                     double *uz_o, const uint8_t *solid, int Nx, int Ny, int Nz, double sp, double sm,
+                     int per_x, int per_y, int per_z) {
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                double p[19];
+                size_t n = N3(i, j, k);
+                pull3d(f_in, Nx, Ny, Nz, i, j, k, per_x, per_y, per_z, p);
+                if (solid && solid[n]) {
+                    /* SolidInert_3D: feq_3d(q, 1, 0, 0, 0, 0) = w_q (1 - 1.5*0) */
+                    double feq[19];
+                    feq3d_all(1.0, 0.0, 0.0, 0.0, 0.0, feq);
+                    for (int q = 0; q < 19; ++q) f_out[I3(i, j, k, q)] = feq[q];
+                    if (rho_o) { rho_o[n] = 1.0; ux_o[n] = 0.0; uy_o[n] = 0.0; uz_o[n] = 0.0; }
+                    continue;
+                }
+                double rho, ux, uy, uz, feq[19];
+                moments3d(p, &rho, &ux, &uy, &uz);
+                double usq = ux * ux + uy * uy + uz * uz;
+                feq3d_all(rho, ux, uy, uz, usq, feq);
+                double a = (sp + sm) * 0.5, b = (sp - sm) * 0.5;
+                static const int pa[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16};
+                static const int pb[9] = {2, 4, 6, 10, 9, 14, 13, 18, 17};
+                f_out[I3(i, j, k, 0)] = p[0] - sp * (p[0] - feq[0]);
+                for (int m = 0; m < 9; ++m) {
+                    int x = pa[m], y = pb[m];
+                    f_out[I3(i, j, k, x)] = p[x] - a * (p[x] - feq[x]) - b * (p[y] - feq[y]);
+                    f_out[I3(i, j, k, y)] = p[y] - a * (p[y] - feq[y]) - b * (p[x] - feq[x]);
+                }
+                if (rho_o) { rho_o[n] = rho; ux_o[n] = ux; uy_o[n] = uy; uz_o[n] = uz; }
+            }
+}
+
+/* stream_periodic_xz_movingwall_y_3d!: src/kernels/stream_periodic_3d.jl:106-186 */
+void or_stream_periodic_xz_movingwall_y_3d(double *f_out, const double *f_in, double Ub, double Ut,
+                                           double rho_w, int Nx, int Ny, int Nz) {
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                int im = i > 0 ? i - 1 : Nx - 1, ip = i < Nx - 1 ? i + 1 : 0;
+                int km = k > 0 ? k - 1 : Nz - 1, kp = k < Nz - 1 ? k + 1 : 0;
+                int lo = j == 0, hi = j == Ny - 1;
+                int jm1 = j > 0 ? j - 1 : j, jp1 = j < Ny - 1 ? j + 1 : j;
+                double cbot = 1.0 / 6.0 * rho_w * Ub, ctop = 1.0 / 6.0 * rho_w * Ut;
+                f_out[I3(i, j, k, 0)] = f_in[I3(i, j, k, 0)];
+                f_out[I3(i, j, k, 1)] = f_in[I3(im, j, k, 1)];
+                f_out[I3(i, j, k, 2)] = f_in[I3(ip, j, k, 2)];
+                f_out[I3(i, j, k, 3)] = lo ? f_in[I3(i, j, k, 4)] : f_in[I3(i, jm1, k, 3)];
+                f_out[I3(i, j, k, 4)] = hi ? f_in[I3(i, j, k, 3)] : f_in[I3(i, jp1, k, 4)];
+                f_out[I3(i, j, k, 5)] = f_in[I3(i, j, km, 5)];
+                f_out[I3(i, j, k, 6)] = f_in[I3(i, j, kp, 6)];
+                f_out[I3(i, j, k, 7)] = lo ? f_in[I3(i, j, k, 10)] + cbot : f_in[I3(im, jm1, k, 7)];
+                f_out[I3(i, j, k, 8)] = lo ? f_in[I3(i, j, k, 9)] - cbot : f_in[I3(ip, jm1, k, 8)];
+                f_out[I3(i, j, k, 9)] = hi ? f_in[I3(i, j, k, 8)] + ctop : f_in[I3(im, jp1, k, 9)];
+                f_out[I3(i, j, k, 10)] = hi ? f_in[I3(i, j, k, 7)] - ctop : f_in[I3(ip, jp1, k, 10)];
+                f_out[I3(i, j, k, 11)] = f_in[I3(im, j, km, 11)];
+                f_out[I3(i, j, k, 12)] = f_in[I3(ip, j, km, 12)];
+                f_out[I3(i, j, k, 13)] = f_in[I3(im, j, kp, 13)];
+                f_out[I3(i, j, k, 14)] = f_in[I3(ip, j, kp, 14)];
+                f_out[I3(i, j, k, 15)] = lo ? f_in[I3(i, j, k, 18)] : f_in[I3(i, jm1, km, 15)];
+                f_out[I3(i, j, k, 16)] = hi ? f_in[I3(i, j, k, 17)] : f_in[I3(i, jp1, km, 16)];
+                f_out[I3(i, j, k, 17)] = lo ? f_in[I3(i, j, k, 16)] : f_in[I3(i, jm1, kp, 17)];
+                f_out[I3(i, j, k, 18)] = hi ? f_in[I3(i, j, k, 15)] : f_in[I3(i, jp1, kp, 18)];
+            }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Thermal double distribution: src/kernels/fused_thermal_2d.jl             */
+/* ------------------------------------------------------------------------ */
+
+/* apply_thermal_bc_cavity: fused_thermal_2d.jl:37-57 */
+static inline void thermal_bc(double *g, int i, int Nx, double T_hot, double T_cold) {
+    if (i == 0) {
+        g[1] = -g[1] + 2.0 * (1.0 / 9.0) * T_hot;
+        g[5] = -g[5] + 2.0 * (1.0 / 36.0) * T_hot;
+        g[8] = -g[8] + 2.0 * (1.0 / 36.0) * T_hot;
+    }
+    if (i == Nx - 1) {
+        g[3] = -g[3] + 2.0 * (1.0 / 9.0) * T_cold;
+        g[6] = -g[6] + 2.0 * (1.0 / 36.0) * T_cold;
+        g[7] = -g[7] + 2.0 * (1.0 / 36.0) * T_cold;
+    }
+}
+
+/* collide_thermal_node: fused_thermal_2d.jl:76-111 */
+static inline void collide_thermal(double *g, double ux, double uy, double wT) {
+    double Tm = g[0] + g[1] + g[2] + g[3] + g[4] + g[5] + g[6] + g[7] + g[8];
+    const double t3 = 3.0;
+    double geq;
+    geq = 4.0 / 9.0 * Tm;                              g[0] = g[0] - wT * (g[0] - geq);
+    geq = 1.0 / 9.0 * Tm * (1.0 + t3 * ux);            g[1] = g[1] - wT * (g[1] - geq);
+    geq = 1.0 / 9.0 * Tm * (1.0 + t3 * uy);            g[2] = g[2] - wT * (g[2] - geq);
+    geq = 1.0 / 9.0 * Tm * (1.0 - t3 * ux);            g[3] = g[3] - wT * (g[3] - geq);
+    geq = 1.0 / 9.0 * Tm * (1.0 - t3 * uy);            g[4] = g[4] - wT * (g[4] - geq);
+    geq = 1.0 / 36.0 * Tm * (1.0 + t3 * (ux + uy));    g[5] = g[5] - wT * (g[5] - geq);
+    geq = 1.0 / 36.0 * Tm * (1.0 + t3 * (-ux + uy));   g[6] = g[6] - wT * (g[6] - geq);
+    geq = 1.0 / 36.0 * Tm * (1.0 + t3 * (-ux - uy));   g[7] = g[7] - wT * (g[7] - geq);
+    geq = 1.0 / 36.0 * Tm * (1.0 + t3 * (ux - uy));    g[8] = g[8] - wT * (g[8] - geq);
+}
+
+/* collide_boussinesq_node: fused_thermal_2d.jl:115-151 */
+static inline void collide_boussinesq(double *f, double rho, double ux, double uy, double fy, double w) {
+    const double fx = 0.0;
+    double usq = ux * ux + uy * uy;
+    double gp = 1.0 - w / 2.0;
+    const double t3 = 3.0;
+    double feq[9], S[9];
+    feq2d_all(rho, ux, uy, usq, feq);
+    S[0] = 4.0 / 9.0 * ((-ux) * fx + (-uy) * fy) * t3;
+    S[1] = 1.0 / 9.0 * ((1.0 - ux) * fx + (-uy) * fy) * t3 + 1.0 / 9.0 * ux * fx * 9.0;
+    S[2] = 1.0 / 9.0 * ((-ux) * fx + (1.0 - uy) * fy) * t3 + 1.0 / 9.0 * uy * fy * 9.0;
+    S[3] = 1.0 / 9.0 * ((-1.0 - ux) * fx + (-uy) * fy) * t3 + 1.0 / 9.0 * ux * fx * 9.0;
+    S[4] = 1.0 / 9.0 * ((-ux) * fx + (-1.0 - uy) * fy) * t3 + 1.0 / 9.0 * uy * fy * 9.0;
+    S[5] = 1.0 / 36.0 * ((1.0 - ux) * fx + (1.0 - uy) * fy) * t3 + 1.0 / 36.0 * (ux + uy) * (fx + fy) * 9.0;
+    S[6] = 1.0 / 36.0 * ((-1.0 - ux) * fx + (1.0 - uy) * fy) * t3 + 1.0 / 36.0 * (-ux + uy) * (-fx + fy) * 9.0;
+    S[7] = 1.0 / 36.0 * ((-1.0 - ux) * fx + (-1.0 - uy) * fy) * t3 + 1.0 / 36.0 * (-ux - uy) * (-fx - fy) * 9.0;
+    S[8] = 1.0 / 36.0 * ((1.0 - ux) * fx + (-1.0 - uy) * fy) * t3 + 1.0 / 36.0 * (ux - uy) * (fx - fy) * 9.0;
+    for (int q = 0; q < 9; ++q) f[q] = f[q] - w * (f[q] - feq[q]) + gp * S[q];
+}
+
+/* fused_natconv_step! (and _vt_ when visc_var != 0):
+ * src/kernels/fused_thermal_2d.jl:178-238, 251-278. */
+static void natconv_core(double *f_out, const double *f_in, double *g_out, const double *g_in,
+                         double *Temp, int Nx, int Ny, double w_f, double w_T, double beta_g,
+                         double T_ref, double T_hot, double T_cold, int visc_var, double nu_ref,
+                         double T0_visc, double a_visc) {
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            double fp[9], gp[9];
+            pull2d(f_in, Nx, Ny, i, j, fp);
+            pull2d(g_in, Nx, Ny, i, j, gp);
+            thermal_bc(gp, i, Nx, T_hot, T_cold);
+            double Tl = gp[0] + gp[1] + gp[2] + gp[3] + gp[4] + gp[5] + gp[6] + gp[7] + gp[8];
+            Temp[N2(i, j)] = Tl;
+            double fy = beta_g * (Tl - T_ref);
+            double rho = fp[0] + fp[1] + fp[2] + fp[3] + fp[4] + fp[5] + fp[6] + fp[7] + fp[8];
+            double inv = 1.0 / rho;
+            double ux = (fp[1] - fp[3] + fp[5] - fp[6] - fp[7] + fp[8]) * inv;
+            double uy = ((fp[2] - fp[4] + fp[5] + fp[6] - fp[7] - fp[8]) + fy / 2.0) * inv;
+            collide_thermal(gp, ux, uy, w_T);
+            for (int q = 0; q < 9; ++q) g_out[I2(i, j, q)] = gp[q];
+            double w = w_f;
+            if (visc_var) {
+                double nul = nu_ref * exp(a_visc * (Tl - T0_visc));
+                w = 1.0 / (3.0 * nul + 0.5);
+            }
+            collide_boussinesq(fp, rho, ux, uy, fy, w);
+            for (int q = 0; q < 9; ++q) f_out[I2(i, j, q)] = fp[q];
+        }
+}
+
+void or_fused_natconv_2d(double *f_out, const double *f_in, double *g_out, const double *g_in,
+                         double *Temp, int Nx, int Ny, double w_f, double w_T, double beta_g,
+                         double T_ref, double T_hot, double T_cold) {
+    natconv_core(f_out, f_in, g_out, g_in, Temp, Nx, Ny, w_f, w_T, beta_g, T_ref, T_hot, T_cold,
+                 0, 0.0, 0.0, 0.0);
+}
+
+void or_fused_natconv_vt_2d(double *f_out, const double *f_in, double *g_out, const double *g_in,
+                            double *Temp, int Nx, int Ny, double nu_ref, double T0_visc,
+                            double a_visc, double w_T, double beta_g, double T_ref, double T_hot,
+                            double T_cold) {
+    natconv_core(f_out, f_in, g_out, g_in, Temp, Nx, Ny, 0.0, w_T, beta_g, T_ref, T_hot, T_cold,
+                 1, nu_ref, T0_visc, a_visc);
+}
+
+/* compute_temperature_2d!: src/kernels/thermal_2d.jl:113-138 (T = sum g). */
+void or_temperature_2d(double *Temp, const double *g, int Nx, int Ny) {
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            double s = g[I2(i, j, 0)] + g[I2(i, j, 1)] + g[I2(i, j, 2)] + g[I2(i, j, 3)] +
+                       g[I2(i, j, 4)] + g[I2(i, j, 5)] + g[I2(i, j, 6)] + g[I2(i, j, 7)] + g[I2(i, j, 8)];
+            Temp[N2(i, j)] = s;
+        }
+}
+
+/* Steady residual over fluid nodes, r_u = ||u - u_prev||_2 / ||u||_2
+ * (src/drivers/gnf_periodic_steady.jl:186-194), sequential FP64 sums.
+ * ndim = 2 or 3; uz/uz_prev ignored for 2. */
+double or_residual(const double *ux, const double *uy, const double *uz, const double *uxp,
+                   const double *uyp, const double *uzp, const uint8_t *solid, size_t n, int ndim) {
+    double du2 = 0.0, u2 = 0.0;
+    for (size_t m = 0; m < n; ++m) {
+        if (solid && solid[m]) continue;
+        double a = ux[m] - uxp[m], b = uy[m] - uyp[m];
+        double d = a * a + b * b, s = ux[m] * ux[m] + uy[m] * uy[m];
+        if (ndim == 3) { double c = uz[m] - uzp[m]; d += c * c; s += uz[m] * uz[m]; }
+        du2 += d; u2 += s;
+    }
+    return sqrt(du2 / u2);
+}
+
+int or_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void or_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}

@@ -1,0 +1,257 @@
+"""D2Q9 parity: every reference-arithmetic kernel against the oracle.
+
+FP64 runs must be bit-identical to the oracle (the library compiles these
+kernels without multiply-add contraction, the oracle with
+-ffp-contract=off).  Inputs are seeded perturbations of equilibrium on
+ragged grids, with and without solid masks.
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(1, 1), (2, 3), (17, 13), (33, 7), (128, 128)]
+
+
+def _rand_f(Nx, Ny, seed, amp=0.05):
+    rng = np.random.default_rng(seed)
+    w = np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4)
+    return w[:, None, None] * (1.0 + amp * rng.standard_normal((9, Ny, Nx)))
+
+
+def _mask(Nx, Ny, seed, frac=0.15):
+    rng = np.random.default_rng(seed + 99)
+    return (rng.random((Ny, Nx)) < frac).astype(np.uint8)
+
+
+def _g(a, dtype=torch.float64):
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda", dtype)
+
+
+def _h(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+@pytest.mark.parametrize("Nx,Ny", SIZES)
+def test_stream_2d(cuda, pkg, orc, Nx, Ny):
+    f = _rand_f(Nx, Ny, 1)
+    out = np.empty_like(f)
+    orc.stream_2d(out, f)
+    fo = torch.empty((9, Ny, Nx), dtype=torch.float64, device=cuda)
+    pkg.stream_2d_(fo, _g(f), Nx, Ny)
+    assert np.array_equal(_h(fo), out)
+
+
+@pytest.mark.parametrize("Nx,Ny", SIZES)
+@pytest.mark.parametrize("with_mask", [False, True])
+def test_collide_2d(cuda, pkg, orc, Nx, Ny, with_mask):
+    f = _rand_f(Nx, Ny, 2)
+    m = _mask(Nx, Ny, 2) if with_mask else None
+    ref = f.copy()
+    orc.collide_2d(ref, m, 1.37)
+    ft = _g(f)
+    pkg.collide_2d_(ft, _g(m, torch.uint8) if m is not None else None, 1.37)
+    assert np.array_equal(_h(ft), ref)
+
+
+@pytest.mark.parametrize("Nx,Ny", SIZES)
+def test_zou_he_and_walls(cuda, pkg, orc, Nx, Ny):
+    f = _rand_f(Nx, Ny, 3)
+    cases = [
+        (lambda a: orc.zou_he_north_2d(a, 0.1), lambda t: pkg.apply_zou_he_north_2d_(t, 0.1, Nx, Ny)),
+        (lambda a: orc.zou_he_south_2d(a, -0.07), lambda t: pkg.apply_zou_he_south_2d_(t, -0.07, Nx)),
+        (lambda a: orc.zou_he_west_2d(a, 0.05), lambda t: pkg.apply_zou_he_west_2d_(t, 0.05, Nx, Ny)),
+        (lambda a: orc.zou_he_pressure_east_2d(a, 1.01),
+         lambda t: pkg.apply_zou_he_pressure_east_2d_(t, Nx, Ny, 1.01)),
+        (lambda a: orc.zou_he_pressure_west_2d(a, 0.99),
+         lambda t: pkg.apply_zou_he_pressure_west_2d_(t, Nx, Ny, 0.99)),
+    ]
+    if Nx >= 2:
+        cases.append((lambda a: orc.extrapolate_east_2d(a),
+                      lambda t: pkg.apply_extrapolate_east_2d_(t, Nx, Ny)))
+    for wid, side in ((1, "south"), (2, "west"), (3, "east"), (4, "north")):
+        cases.append((lambda a, w=wid: orc.bounce_back_wall_2d(a, w),
+                      lambda t, s=side: pkg.apply_bounce_back_wall_2d_(t, Nx, Ny, s)))
+    for oracle_fn, gpu_fn in cases:
+        ref = f.copy()
+        oracle_fn(ref)
+        ft = _g(f)
+        gpu_fn(ft)
+        assert np.array_equal(_h(ft), ref)
+
+
+@pytest.mark.parametrize("Nx,Ny", SIZES)
+def test_macroscopic_2d(cuda, pkg, orc, Nx, Ny):
+    f = _rand_f(Nx, Ny, 4)
+    r, a, b = orc.macroscopic_2d(f)
+    rt, at, bt = (torch.empty((Ny, Nx), dtype=torch.float64, device=cuda) for _ in range(3))
+    pkg.compute_macroscopic_2d_(rt, at, bt, _g(f))
+    assert np.array_equal(_h(rt), r) and np.array_equal(_h(at), a) and np.array_equal(_h(bt), b)
+
+
+@pytest.mark.parametrize("Nx,Ny", SIZES)
+@pytest.mark.parametrize("with_mask", [False, True])
+@pytest.mark.parametrize("kind", ["bgk", "trt"])
+def test_fused_steps(cuda, pkg, orc, Nx, Ny, with_mask, kind):
+    f = _rand_f(Nx, Ny, 5)
+    m = _mask(Nx, Ny, 5) if with_mask else None
+    fo = np.empty_like(f)
+    mo = [np.empty((Ny, Nx)) for _ in range(3)]
+    ft, fot = _g(f), torch.empty((9, Ny, Nx), dtype=torch.float64, device=cuda)
+    mt = [torch.empty((Ny, Nx), dtype=torch.float64, device=cuda) for _ in range(3)]
+    mg = _g(m, torch.bool) if m is not None else None
+    nu, lam = 0.02, 3 / 16
+    for _ in range(3):
+        if kind == "bgk":
+            orc.fused_bgk_2d(fo, f, *mo, m, 1.6)
+            pkg.fused_bgk_step_(fot, ft, *mt, mg, Nx, Ny, 1.6)
+        else:
+            sp, sm = orc.trt_rates(nu, lam)
+            orc.fused_trt_2d(fo, f, *mo, m, sp, sm)
+            pkg.fused_trt_step_(fot, ft, *mt, mg, Nx, Ny, nu, lam)
+        f, fo = fo, f
+        ft, fot = fot, ft
+    assert np.array_equal(_h(ft), f)
+    for t, a in zip(mt, mo):
+        assert np.array_equal(_h(t), a)
+
+
+@pytest.mark.parametrize("Nx,Ny", SIZES)
+@pytest.mark.parametrize("with_mask", [False, True])
+def test_mrt(cuda, pkg, orc, Nx, Ny, with_mask):
+    f = _rand_f(Nx, Ny, 6)
+    m = _mask(Nx, Ny, 6) if with_mask else None
+    ref = f.copy()
+    orc.collide_mrt_2d(ref, m, 0.05)
+    ft = _g(f)
+    pkg.collide_mrt_2d_(ft, _g(m, torch.bool) if m is not None else None, 0.05)
+    assert np.array_equal(_h(ft), ref)
+
+
+@pytest.mark.parametrize("Nx,Ny", SIZES)
+def test_periodic_streams(cuda, pkg, orc, Nx, Ny):
+    f = _rand_f(Nx, Ny, 7)
+    for ofn, gfn in ((orc.stream_fully_periodic_2d, pkg.stream_fully_periodic_2d_),
+                     (orc.stream_periodic_x_wall_y_2d, pkg.stream_periodic_x_wall_y_2d_)):
+        ref = np.empty_like(f)
+        ofn(ref, f)
+        fo = torch.empty((9, Ny, Nx), dtype=torch.float64, device=cuda)
+        gfn(fo, _g(f), Nx, Ny)
+        assert np.array_equal(_h(fo), ref)
+
+
+@pytest.mark.parametrize("Nx,Ny", SIZES)
+@pytest.mark.parametrize("with_mask", [False, True])
+def test_aa_steps(cuda, pkg, orc, Nx, Ny, with_mask):
+    f = _rand_f(Nx, Ny, 8)
+    m = _mask(Nx, Ny, 8) if with_mask else None
+    ref = f.copy()
+    ft = _g(f)
+    mg = _g(m, torch.bool) if m is not None else None
+    for step in range(4):
+        if step % 2 == 0:
+            orc.aa_odd_2d(ref, m, 1.3)
+            pkg.aa_odd_step_(ft, mg, Nx, Ny, 1.3)
+        else:
+            orc.aa_even_2d(ref, m, 1.3)
+            pkg.aa_even_step_(ft, mg, Nx, Ny, 1.3)
+    assert np.array_equal(_h(ft), ref)
+
+
+def test_cavity_config1_1000_steps(cuda, pkg, orc):
+    """Plain FP64 D2Q9 BGK cavity, 128^2, nu=0.02, u_lid=0.1 (Re=640): rho and
+    u after 1000 steps equal the oracle's four-launch loop bit for bit (the
+    required bound is 1e-12 relative), for the reference's four launches and
+    for the fused single-launch step."""
+    N, nu, u_lid, steps = 128, 0.02, 0.1, 1000
+    cfg = pkg.LBMConfig.d2q9(N, N, nu, u_lid, steps)
+    f = np.empty((9, N, N))
+    for q in range(9):
+        f[q] = pkg.lattice.D2Q9_W[q]
+    rho, ux, uy = orc.run_cavity_2d(f, N, N, pkg.omega(cfg), u_lid, steps)
+    for fused in (False, True):
+        res = pkg.run_cavity_2d(cfg, T=torch.float64, fused=fused)
+        for key, ref in (("rho", rho), ("ux", ux), ("uy", uy)):
+            got = res[key]
+            rel = np.max(np.abs(got - ref)) / np.max(np.abs(ref))
+            assert rel <= 1e-12, (fused, key, rel)
+            assert np.array_equal(got, ref), (fused, key)
+
+
+def test_cavity_float32_close(cuda, pkg, orc):
+    """Float32 storage and arithmetic (the reference's T=Float32 path) stays
+    within FP32 rounding of the FP64 oracle over 500 steps."""
+    N, nu, u_lid, steps = 64, 0.02, 0.1, 500
+    cfg = pkg.LBMConfig.d2q9(N, N, nu, u_lid, steps)
+    f = np.empty((9, N, N))
+    for q in range(9):
+        f[q] = pkg.lattice.D2Q9_W[q]
+    rho, ux, uy = orc.run_cavity_2d(f, N, N, pkg.omega(cfg), u_lid, steps)
+    res = pkg.run_cavity_2d(cfg, T=torch.float32, fused=True)
+    assert np.max(np.abs(res["ux"] - ux)) / np.max(np.abs(ux)) < 1e-4
+    assert np.max(np.abs(res["rho"] - rho)) < 1e-5
+
+
+@pytest.mark.parametrize("vt", [False, True])
+def test_natconv_fp64(cuda, pkg, orc, vt):
+    """Fused thermal DDF step vs the oracle: bit-identical for constant
+    viscosity; the variable-viscosity form calls exp(), whose last bit differs
+    between CUDA and the host libm, so it is held to 1e-13 relative."""
+    N, steps = 48, 200
+    p = pkg.drivers.natconv_parameters(N, 1e5, 0.71)
+    f = np.empty((9, N, N))
+    for q in range(9):
+        f[q] = pkg.lattice.D2Q9_W[q]
+    g = pkg.drivers.natconv_initial_g(N)
+    fo, go, T = np.empty_like(f), np.empty_like(g), np.empty((N, N))
+    ft, gt = _g(f), _g(g)
+    fot, got = torch.empty_like(ft), torch.empty_like(gt)
+    Tt = torch.empty((N, N), dtype=torch.float64, device=cuda)
+    a_visc = -np.log(10.0)
+    for _ in range(steps):
+        if vt:
+            orc.fused_natconv_vt_2d(fo, f, go, g, T, p["nu"], 0.0, a_visc, p["omega_T"],
+                                    p["beta_g"], p["T_ref"], 1.0, 0.0)
+            pkg.fused_natconv_vt_step_(fot, ft, got, gt, Tt, N, N, p["nu"], 0.0, a_visc,
+                                       p["omega_T"], p["beta_g"], p["T_ref"], 1.0, 0.0)
+        else:
+            orc.fused_natconv_2d(fo, f, go, g, T, p["omega_f"], p["omega_T"], p["beta_g"],
+                                 p["T_ref"], 1.0, 0.0)
+            pkg.fused_natconv_step_(fot, ft, got, gt, Tt, N, N, p["omega_f"], p["omega_T"],
+                                    p["beta_g"], p["T_ref"], 1.0, 0.0)
+        f, fo = fo, f
+        g, go = go, g
+        ft, fot = fot, ft
+        gt, got = got, gt
+    if vt:
+        assert np.max(np.abs(_h(ft) - f)) < 1e-13
+        assert np.max(np.abs(_h(gt) - g)) < 1e-13
+    else:
+        assert np.array_equal(_h(ft), f) and np.array_equal(_h(gt), g)
+        assert np.array_equal(_h(Tt), T)
+    Tc = torch.empty_like(Tt)
+    pkg.compute_temperature_2d_(Tc, gt)
+    assert np.max(np.abs(_h(Tc) - orc.temperature_2d(g))) < 1e-13
+
+
+def test_natconv_driver_nu(cuda, pkg, pins):
+    """De Vahl Davis Ra=1e3 on 64^2 (test/test_thermal.jl:388-404) through the
+    b200 driver: Nu within 0.5 % of 1.118."""
+    res = pkg.run_natural_convection_2d(N=64, Ra=1e3, Pr=0.71, max_steps=30000)
+    ref = pins["natconv_ra1e3_nu_ref"]
+    assert abs(res["Nu"] - ref) / ref < 0.005
+
+
+def test_ghia_re100_on_gpu(cuda, pkg, pins):
+    """test/test_cavity.jl:6-40 through the b200 driver."""
+    N, u_lid = 128, 0.1
+    cfg = pkg.LBMConfig.d2q9(N, N, u_lid * N / 100.0, u_lid, 30000)
+    ux = pkg.run_cavity_2d(cfg, fused=True)["ux"]
+    ic = N // 2 - 1
+    err = 0.0
+    for yg, ug in zip(pins["ghia_re100"]["y"], pins["ghia_re100"]["u"]):
+        j = min(max(round(yg * (N - 1)) + 1, 1), N) - 1
+        err = max(err, abs(ux[j, ic] / u_lid - ug))
+    assert err < 0.1

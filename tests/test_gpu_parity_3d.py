@@ -1,0 +1,188 @@
+"""D3Q19 parity: reference-arithmetic kernels bit-identical to the oracle in
+FP64; deviation storages (FP32/FP16/BF16 with FP32 collision) held to
+stated error bounds against the FP64 run."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(1, 1, 1), (3, 2, 5), (17, 5, 6), (33, 9, 4)]
+W19 = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+
+
+def _rand_f(Nx, Ny, Nz, seed, amp=0.05):
+    rng = np.random.default_rng(seed)
+    return W19[:, None, None, None] * (1.0 + amp * rng.standard_normal((19, Nz, Ny, Nx)))
+
+
+def _mask(shape, seed, frac=0.15):
+    rng = np.random.default_rng(seed + 7)
+    return (rng.random(shape) < frac).astype(np.uint8)
+
+
+def _g(a, dtype=torch.float64):
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda", dtype)
+
+
+def _h(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+@pytest.mark.parametrize("Nx,Ny,Nz", SIZES)
+def test_stream_collide_macro_3d(cuda, pkg, orc, Nx, Ny, Nz):
+    f = _rand_f(Nx, Ny, Nz, 1)
+    ref = np.empty_like(f)
+    orc.stream_3d(ref, f)
+    fo = torch.empty((19, Nz, Ny, Nx), dtype=torch.float64, device=cuda)
+    pkg.stream_3d_(fo, _g(f), Nx, Ny, Nz)
+    assert np.array_equal(_h(fo), ref)
+    m = _mask((Nz, Ny, Nx), 1)
+    orc.collide_3d(ref, m, 1.71)
+    pkg.collide_3d_(fo, _g(m, torch.bool), 1.71)
+    assert np.array_equal(_h(fo), ref)
+    mo = orc.macroscopic_3d(ref)
+    mt = [torch.empty((Nz, Ny, Nx), dtype=torch.float64, device=cuda) for _ in range(4)]
+    pkg.compute_macroscopic_3d_(*mt, fo)
+    for t, a in zip(mt, mo):
+        assert np.array_equal(_h(t), a)
+
+
+@pytest.mark.parametrize("Nx,Ny,Nz", SIZES)
+def test_zou_he_3d_all_faces(cuda, pkg, orc, Nx, Ny, Nz):
+    f = _rand_f(Nx, Ny, Nz, 2)
+    for face in ("west", "east", "south", "north", "bottom", "top"):
+        ref = f.copy()
+        orc.zou_he_velocity_3d(ref, face, 0.03, -0.02, 0.05)
+        ft = _g(f)
+        pkg.apply_zou_he_velocity_3d_(ft, face, 0.03, -0.02, 0.05)
+        assert np.array_equal(_h(ft), ref), face
+        ref = f.copy()
+        orc.zou_he_pressure_3d(ref, face, 1.02)
+        ft = _g(f)
+        pkg.apply_zou_he_pressure_3d_(ft, face, 1.02)
+        assert np.array_equal(_h(ft), ref), face
+    ref = f.copy()
+    orc.zou_he_top_3d(ref, 0.1)
+    ft = _g(f)
+    pkg.apply_zou_he_top_3d_(ft, 0.1, Nx, Ny, Nz)
+    assert np.array_equal(_h(ft), ref)
+
+
+@pytest.mark.parametrize("Nx,Ny,Nz", SIZES)
+@pytest.mark.parametrize("per", range(8))
+@pytest.mark.parametrize("with_mask", [False, True])
+def test_fused_trt_3d_fp64_exact(cuda, pkg, orc, Nx, Ny, Nz, per, with_mask):
+    f = _rand_f(Nx, Ny, Nz, 3 + per)
+    m = _mask((Nz, Ny, Nx), per) if with_mask else None
+    pflags = (per & 1, (per >> 1) & 1, (per >> 2) & 1)
+    nu, lam = 0.01, 0.25
+    sp, sm = orc.trt_rates(nu, lam)
+    fo = np.empty_like(f)
+    mo = [np.empty((Nz, Ny, Nx)) for _ in range(4)]
+    ft = _g(f)
+    fot = torch.empty_like(ft)
+    mt = [torch.empty((Nz, Ny, Nx), dtype=torch.float64, device=cuda) for _ in range(4)]
+    mg = _g(m, torch.bool) if m is not None else None
+    for _ in range(3):
+        orc.fused_trt_3d(fo, f, mo, m, sp, sm, pflags)
+        pkg.fused_trt_step_3d_(fot, ft, *mt, mg, Nx, Ny, Nz, nu, lam, periodic=pflags)
+        f, fo = fo, f
+        ft, fot = fot, ft
+    assert np.array_equal(_h(ft), f)
+    for t, a in zip(mt, mo):
+        assert np.array_equal(_h(t), a)
+
+
+def test_fused_trt_3d_no_moments(cuda, pkg, orc):
+    N = 12
+    f = _rand_f(N, N, N, 11)
+    ref = np.empty_like(f)
+    sp, sm = orc.trt_rates(0.02, 3 / 16)
+    orc.fused_trt_3d(ref, f, None, None, sp, sm, (1, 0, 1))
+    fo = torch.empty((19, N, N, N), dtype=torch.float64, device=cuda)
+    pkg.fused_trt_step_3d_(fo, _g(f), None, None, None, None, None, N, N, N, 0.02, 3 / 16,
+                           periodic=(1, 0, 1))
+    assert np.array_equal(_h(fo), ref)
+
+
+@pytest.mark.parametrize("Nx,Ny,Nz", [(5, 4, 3), (16, 8, 6)])
+def test_movingwall_3d(cuda, pkg, orc, Nx, Ny, Nz):
+    f = _rand_f(Nx, Ny, Nz, 12)
+    ref = np.empty_like(f)
+    orc.stream_periodic_xz_movingwall_y_3d(ref, f, 0.02, -0.03, 1.0)
+    fo = torch.empty((19, Nz, Ny, Nx), dtype=torch.float64, device=cuda)
+    pkg.stream_periodic_xz_movingwall_y_3d_(fo, _g(f), 0.02, -0.03, Nx, Ny, Nz)
+    assert np.array_equal(_h(fo), ref)
+
+
+def test_cavity_3d_driver(cuda, pkg, orc):
+    N, nu, u = 12, 0.05, 0.05
+    cfg = pkg.LBMConfig.d3q19(N, N, N, nu, u, 100)
+    res = pkg.run_cavity_3d(cfg)
+    f = np.empty((19, N, N, N))
+    for q in range(19):
+        f[q] = W19[q]
+    rho, ux, uy, uz = orc.run_cavity_3d(f, pkg.omega(cfg), u, 100)
+    for key, ref in (("rho", rho), ("ux", ux), ("uy", uy), ("uz", uz)):
+        assert np.array_equal(res[key], ref), key
+
+
+def test_fused_trt_3d_fp32_plain(cuda, pkg, orc):
+    """Float32 storage with the reference arithmetic: FP32 rounding of FP64."""
+    N, nu, lam, steps = 16, 0.01, 0.25, 20
+    f0 = pkg.drivers.taylor_green_3d_populations(N, 0.05)
+    sp, sm = orc.trt_rates(nu, lam)
+    a, b = f0.copy(), np.empty_like(f0)
+    for _ in range(steps):
+        orc.fused_trt_3d(b, a, None, None, sp, sm, (1, 1, 1))
+        a, b = b, a
+    ft = _g(f0, torch.float32)
+    fo = torch.empty_like(ft)
+    for _ in range(steps):
+        pkg.fused_trt_step_3d_(fo, ft, None, None, None, None, None, N, N, N, nu, lam,
+                               periodic=(1, 1, 1))
+        ft, fo = fo, ft
+    assert np.max(np.abs(_h(ft) - a)) < 2e-6
+
+
+@pytest.mark.parametrize("dtype,bound", [(torch.float32, 2e-5), (torch.float16, 5e-3),
+                                         (torch.bfloat16, 5e-2)])
+def test_deviation_storage_tgv(cuda, pkg, orc, dtype, bound):
+    """Deviation storages on the periodic TRT Taylor-Green vortex (32^3,
+    u0=0.05, 200 steps): relative L2 velocity error vs the FP64 oracle below
+    the stated bound, and the FP64 oracle itself tracks exp(-2 nu k^2 t)."""
+    N, nu, lam, u0, steps = 32, 0.01, 0.25, 0.05, 200
+    f0 = pkg.drivers.taylor_green_3d_populations(N, u0)
+    sp, sm = orc.trt_rates(nu, lam)
+    a, b = f0.copy(), np.empty_like(f0)
+    mo = [np.empty((N, N, N)) for _ in range(4)]
+    for s in range(steps):
+        orc.fused_trt_3d(b, a, mo if s == steps - 1 else None, None, sp, sm, (1, 1, 1))
+        a, b = b, a
+    res = pkg.run_taylor_green_3d(N=N, nu=nu, u0=u0, Lambda=lam, max_steps=steps, storage=dtype,
+                                  deviation=True)
+    ref_u = np.stack(mo[1:])
+    got_u = np.stack([res["ux"], res["uy"], res["uz"]]).astype(np.float64)
+    l2 = math.sqrt(np.sum((got_u - ref_u) ** 2) / np.sum(ref_u ** 2))
+    assert l2 < bound, l2
+    k = 2 * math.pi / N
+    x = np.arange(N)[None, None, :]; y = np.arange(N)[None, :, None]
+    ua = -u0 * np.cos(k * x) * np.sin(k * y) * math.exp(-2 * nu * k * k * steps) * np.ones((N, 1, 1))
+    l2a = math.sqrt(np.sum((mo[1] - ua) ** 2) / np.sum(ua ** 2))
+    assert l2a < 0.02, l2a
+
+
+def test_convert_roundtrip(cuda, pkg):
+    f = _rand_f(8, 8, 8, 20)
+    ft = _g(f)
+    for dt in (torch.float32, torch.float16, torch.bfloat16):
+        d = torch.empty(ft.shape, dtype=dt, device=cuda)
+        pkg.convert_populations(d, ft, dst_deviation=True)
+        back = torch.empty_like(ft)
+        pkg.convert_populations(back, d, src_deviation=True)
+        tol = {torch.float32: 1e-8, torch.float16: 5e-5, torch.bfloat16: 5e-4}[dt]
+        assert np.max(np.abs(_h(back) - f)) < tol
