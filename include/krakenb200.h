@@ -116,13 +116,20 @@ int kb_fused_trt_step(void *f_out, const void *f_in, void *rho, void *ux, void *
                       const uint8_t *is_solid, int Nx, int Ny, double nu, double Lambda, int dtype,
                       void *stream);
 
-/* aa_even_step!(f, is_solid, Nx, Ny, omega) -- src/kernels/aa_bgk_2d.jl:125 */
-int kb_aa_even_step(void *f, const uint8_t *is_solid, int Nx, int Ny, double omega, int dtype,
-                    void *stream);
-
-/* aa_odd_step!(f, is_solid, Nx, Ny, omega) -- src/kernels/aa_bgk_2d.jl:138 */
-int kb_aa_odd_step(void *f, const uint8_t *is_solid, int Nx, int Ny, double omega, int dtype,
-                   void *stream);
+/* In-place A-A streaming on one population buffer, the scheme of
+ * aa_even_step!/aa_odd_step! (src/kernels/aa_bgk_2d.jl:125,138).  Those
+ * reference kernels let neighbouring nodes read and write the same slot in
+ * one launch, so their result depends on execution order; these two do not.
+ * Buffer states: S (slot qb(x) holds the post-collision f_q(x)) and P
+ * (slot q(x) holds the f_q arriving at x).  kb_aa_stream_step_2d takes S to
+ * P, kb_aa_local_step_2d takes P to S; each is one BGK step with half-way
+ * bounce-back and the solid swap.  A pull-format buffer with slots q and qb
+ * swapped is state S, and a stream step followed by a local step equals two
+ * kb_fused_bgk_step calls bit for bit.  rho/ux/uy: all NULL or all set. */
+int kb_aa_stream_step_2d(void *f, void *rho, void *ux, void *uy, const uint8_t *is_solid, int Nx,
+                         int Ny, double omega, int dtype, void *stream);
+int kb_aa_local_step_2d(void *f, void *rho, void *ux, void *uy, const uint8_t *is_solid, int Nx,
+                        int Ny, double omega, int dtype, void *stream);
 
 /* collide_mrt_2d!(f, is_solid, nu; s_e, s_eps, s_q) -- src/kernels/collide_mrt_2d.jl:118 */
 int kb_collide_mrt_2d(void *f, const uint8_t *is_solid, int Nx, int Ny, double nu, double s_e,
@@ -143,6 +150,24 @@ int kb_stream_periodic_x_wall_y_2d(void *f_out, const void *f_in, int Nx, int Ny
 int kb_cavity_step_2d(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
                       const uint8_t *is_solid, int Nx, int Ny, double omega, double u_lid,
                       int dtype, void *stream);
+
+/* Lid-driven cavity step with a moving-wall half-way bounce-back lid: the
+ * fused pull + half-way bounce-back + BGK + moments of fused_bgk_step!
+ * (src/kernels/fused_bgk_2d.jl:8-59) with the lid link rule of
+ * ApplyHalfwayBBPrePhase (src/kernels/dsl/bricks.jl:447-487) on the top row's
+ * north-pointing links, wall velocity (u_lid, 0).  Moments (pre-collision)
+ * are written when rho/ux/uy are given (all or none). */
+int kb_cavity_movingwall_step_2d(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                                 const uint8_t *is_solid, int Nx, int Ny, double omega,
+                                 double u_lid, int dtype, void *stream);
+
+/* One step of the MRT cavity loop of test/test_mrt.jl:19-25 (stream_2d! ->
+ * apply_zou_he_north_2d! -> collide_mrt_2d!(f, is_solid, nu; s_e, s_eps,
+ * s_q) -> compute_macroscopic_2d!) in one launch, same bits.  rho/ux/uy:
+ * all NULL (moments skipped) or all set. */
+int kb_cavity_mrt_step_2d(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                          const uint8_t *is_solid, int Nx, int Ny, double nu, double s_e,
+                          double s_eps, double s_q, double u_lid, int dtype, void *stream);
 
 /* fused_natconv_step!(f_out, f_in, g_out, g_in, Temp, Nx, Ny, omega_f,
  *   omega_T, beta_g, T_ref_buoy, T_hot, T_cold) -- src/kernels/fused_thermal_2d.jl:251 */
@@ -205,11 +230,78 @@ int kb_fused_trt_step_3d(void *f_out, const void *f_in, void *rho, void *ux, voi
                          const uint8_t *is_solid, int Nx, int Ny, int Nz, double nu,
                          double Lambda, int periodic, int dtype, void *stream);
 
+/* Kernel variant for tuning and tests (process-wide, not thread-safe to
+ * change while other threads launch).  kernel 1 = the deviation-storage
+ * kernels of kb_fused_trt_step_3d: 0 automatic (two nodes per thread with
+ * vector accesses and packed FP32x2 arithmetic when Nx is even, else one
+ * node per thread), 1 one node per thread, 2 two nodes per thread.  Every
+ * variant computes the same update.  No reference counterpart. */
+int kb_set_kernel_variant(int kernel, int variant);
+
 /* stream_periodic_xz_movingwall_y_3d!(f_out, f_in, Ub, Ut, Nx, Ny, Nz; rho_w)
  *   -- src/kernels/stream_periodic_3d.jl:178 */
 int kb_stream_periodic_xz_movingwall_y_3d(void *f_out, const void *f_in, double Ub, double Ut,
                                           double rho_w, int Nx, int Ny, int Nz, int dtype,
                                           void *stream);
+
+/* --------------------------------------------- batched cavity sweeps -- */
+
+/* Many lid-driven MRT cavities of different sizes in ONE persistent kernel:
+ * the loop of test/test_mrt.jl:19-25 (stream_2d!, apply_zou_he_north_2d!,
+ * collide_mrt_2d! with s_e = s_eps = 1.4, s_q = 1.2) per case, each run to
+ * the steady residual r_u (src/drivers/gnf_periodic_steady.jl:186-194) or to
+ * max_steps; a .krk Sweep (src/io/krk/parser.jl:362-420) maps to one batch.
+ * Populations are stored as f - w_q in FP16/BF16/FP32 and collide in FP32.
+ * No reference counterpart runs a sweep in one launch.  The handle owns its
+ * device memory until kb_batch_destroy; creation synchronises `stream`. */
+typedef struct kb_batch kb_batch;
+
+int kb_batch_create(kb_batch **out, int n_cases, const int *N, const double *nu,
+                    const double *u_lid, int dtype, void *stream);
+int kb_batch_destroy(kb_batch *b);
+/* Back to rest (f = w_q), all cases live; synchronises `stream`. */
+int kb_batch_reset(kb_batch *b, void *stream);
+/* Queue the run (asynchronous, one cooperative launch).  check_every >= 2;
+ * max_steps a multiple of check_every; tile_nodes (multiple of 32) and
+ * blocks_per_sm <= 0 take the autotuned choice (else 256 / occupancy). */
+int kb_batch_run(kb_batch *b, int max_steps, int check_every, double tol, int tile_nodes,
+                 int blocks_per_sm, void *stream);
+/* Node updates done, live tiles left and the grid-barrier timeout flag
+ * (KB_ERR_TIMEOUT if set); synchronises `stream`. */
+int kb_batch_status(kb_batch *b, long long *updates, int *n_live, int *timed_out, void *stream);
+/* Case c: size, steps run, last residual, state (0 live, 1 converged,
+ * 2 hit max_steps, 3 non-finite) and optionally its final ux, uy (N*N floats,
+ * row j = slow index); synchronises `stream`. */
+int kb_batch_case(kb_batch *b, int c, int *N, int *steps, double *residual, int *state,
+                  float *ux_host, float *uy_host, void *stream);
+/* Time trial_steps of every (tile_nodes, blocks_per_sm) candidate, keep the
+ * fastest for later runs; reports its MLUPS and the fixed schedule's (tile
+ * 256, 1 block per SM).  Resets the batch. */
+int kb_batch_autotune(kb_batch *b, int trial_steps, int *best_tile, int *best_bpsm,
+                      double *best_mlups, double *fixed_mlups, void *stream);
+/* Device pointer to case c's final populations (9 planes of N*N, storage
+ * `dtype`). */
+int kb_batch_populations(kb_batch *b, int c, void **f, int *dtype, void *stream);
+
+/* ---------------------------------------------------------- CUDA graphs -- */
+
+/* Capture every library call issued on `stream` (a non-default stream)
+ * between kb_graph_begin and kb_graph_end into an instantiated graph, then
+ * replay it with kb_graph_launch.  This is the device-side form of
+ * persistent_fused_bgk! / persistent_aa_bgk! (src/kernels/persistent_bgk_2d.jl:
+ * 17-56), which queue Nt launches from the host.  Calls that synchronise or
+ * allocate (kb_mass, kb_residual, kb_batch_create ...) cannot be captured. */
+typedef struct kb_graph kb_graph;
+int kb_graph_begin(void *stream);
+int kb_graph_end(void *stream, kb_graph **out);
+int kb_graph_launch(kb_graph *g, void *stream);
+int kb_graph_destroy(kb_graph *g);
+
+/* Self test of the bounded device wait used by the batched kernel's grid
+ * barrier: one thread waits on a word that nothing changes; after `limit`
+ * polls it gives up, sets the error flag and returns.  *timed_out = 1 and
+ * KB_ERR_TIMEOUT is the expected result.  No reference counterpart. */
+int kb_selftest_bounded_wait(long long limit, int *timed_out, void *stream);
 
 /* ------------------------------------------------- precision utilities -- */
 

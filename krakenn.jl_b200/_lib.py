@@ -42,12 +42,15 @@ SIGNATURES: dict[str, list] = {
     "kb_fused_bgk_step": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _i, _vp],
     "kb_trt_rates": [_d, _d, _dp, _dp],
     "kb_fused_trt_step": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _d, _i, _vp],
-    "kb_aa_even_step": [_vp, _u8p, _i, _i, _d, _i, _vp],
-    "kb_aa_odd_step": [_vp, _u8p, _i, _i, _d, _i, _vp],
+    "kb_aa_stream_step_2d": [_vp, _vp, _vp, _vp, _u8p, _i, _i, _d, _i, _vp],
+    "kb_aa_local_step_2d": [_vp, _vp, _vp, _vp, _u8p, _i, _i, _d, _i, _vp],
     "kb_collide_mrt_2d": [_vp, _u8p, _i, _i, _d, _d, _d, _d, _i, _vp],
     "kb_stream_fully_periodic_2d": [_vp, _cvp, _i, _i, _i, _vp],
     "kb_stream_periodic_x_wall_y_2d": [_vp, _cvp, _i, _i, _i, _vp],
     "kb_cavity_step_2d": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _d, _i, _vp],
+    "kb_cavity_movingwall_step_2d": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _d, _i, _vp],
+    "kb_cavity_mrt_step_2d": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _d, _d, _d, _d, _i,
+                              _vp],
     "kb_fused_natconv_step": [_vp, _cvp, _vp, _cvp, _vp, _i, _i, _d, _d, _d, _d, _d, _d, _i, _vp],
     "kb_fused_natconv_vt_step": [_vp, _cvp, _vp, _cvp, _vp, _i, _i, _d, _d, _d, _d, _d, _d, _d,
                                  _d, _i, _vp],
@@ -60,7 +63,22 @@ SIGNATURES: dict[str, list] = {
     "kb_compute_macroscopic_3d": [_vp, _vp, _vp, _vp, _cvp, _i, _i, _i, _i, _vp],
     "kb_fused_trt_step_3d": [_vp, _cvp, _vp, _vp, _vp, _vp, _u8p, _i, _i, _i, _d, _d, _i, _i,
                              _vp],
+    "kb_set_kernel_variant": [_i, _i],
     "kb_stream_periodic_xz_movingwall_y_3d": [_vp, _cvp, _d, _d, _d, _i, _i, _i, _i, _vp],
+    "kb_batch_create": [C.POINTER(_vp), _i, C.POINTER(_i), _dp, _dp, _i, _vp],
+    "kb_batch_destroy": [_vp],
+    "kb_batch_reset": [_vp, _vp],
+    "kb_batch_run": [_vp, _i, _i, _d, _i, _i, _vp],
+    "kb_batch_status": [_vp, C.POINTER(C.c_longlong), C.POINTER(_i), C.POINTER(_i), _vp],
+    "kb_batch_case": [_vp, _i, C.POINTER(_i), C.POINTER(_i), _dp, C.POINTER(_i),
+                      C.POINTER(C.c_float), C.POINTER(C.c_float), _vp],
+    "kb_batch_autotune": [_vp, _i, C.POINTER(_i), C.POINTER(_i), _dp, _dp, _vp],
+    "kb_batch_populations": [_vp, _i, C.POINTER(_vp), C.POINTER(_i), _vp],
+    "kb_graph_begin": [_vp],
+    "kb_graph_end": [_vp, C.POINTER(_vp)],
+    "kb_graph_launch": [_vp, _vp],
+    "kb_graph_destroy": [_vp],
+    "kb_selftest_bounded_wait": [C.c_longlong, C.POINTER(_i), _vp],
     "kb_convert_populations": [_vp, _i, _cvp, _i, _i, _sz, _vp],
     "kb_mass": [_cvp, _i, _sz, _i, _dp, _vp],
     "kb_residual": [_cvp, _cvp, _cvp, _cvp, _cvp, _cvp, _u8p, _sz, _i, _dp, _vp],

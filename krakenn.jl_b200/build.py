@@ -36,6 +36,8 @@ UNITS = {
     "kb_d3q19.cu": ["--fmad=false"],
     "kb_d3q19_dev.cu": [],
     "kb_reduce.cu": [],
+    "kb_batch.cu": [],
+    "kb_graph.cu": [],
 }
 
 

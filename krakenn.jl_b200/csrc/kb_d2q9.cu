@@ -327,77 +327,81 @@ __global__ void __launch_bounds__(BX) fused_trt_k(T *__restrict__ fo, const T *_
     rho[c] = r; ux[c] = a_; uy[c] = b_;
 }
 
-// aa_even_kernel!: src/kernels/aa_bgk_2d.jl:14-53.  `src` is a snapshot of
-// the buffer taken before the launch (see kb_aa_even_step).
+// In-place A-A streaming (one population buffer), the scheme that
+// aa_even_step!/aa_odd_step! (src/kernels/aa_bgk_2d.jl:14-143) aim at.  The
+// reference's two kernels read and write slots that neighbouring nodes write
+// in the same launch (its even kernel pulls a neighbour's slot that the
+// neighbour overwrites; its odd kernel has two writers for a wall slot), so
+// their result depends on execution order.  These two kernels are race free:
+// every slot is read and written by one thread only.
+//   state S: slot qb(x) = post-collision f_q(x), not yet streamed
+//   state P: slot q(x)  = f_q arriving at x (post-stream, pre-collision)
+// aa_stream (S -> P): gather p_q from slot qb(x - c_q) (half-way bounce-back:
+//   slot q(x) when x - c_q is outside), collide, scatter to slot q(x + c_q)
+//   (slot qb(x) when x + c_q is outside).
+// aa_local (P -> S): read slot q(x), collide, write slot qb(x).
+// A buffer in the pull kernels' format F (slot q(x) = f*_q(x)) is state S
+// after swapping q <-> qb; stream then local is exactly two fused pull-BGK
+// steps (fused_bgk_2d.jl:8-59), bit for bit, including the solid-node swap
+// and the moments (written when rho/ux/uy are given).
+__device__ constexpr int kOpp9[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+
 template <typename T>
-__global__ void __launch_bounds__(BX) aa_even_k(T *__restrict__ f, const T *__restrict__ src,
-                                                 const uint8_t *__restrict__ solid, Grid2<T> g,
-                                                 T omega) {
-    NODE2
-    T p[9];
-    pull_bb(src, g, i, j, p);
-    if (solid && solid[c]) {
-        f[c + 1 * P] = p[3]; f[c + 3 * P] = p[1];
-        f[c + 2 * P] = p[4]; f[c + 4 * P] = p[2];
-        f[c + 5 * P] = p[7]; f[c + 7 * P] = p[5];
-        f[c + 6 * P] = p[8]; f[c + 8 * P] = p[6];
-        return;
+__device__ __forceinline__ void aa_collide(T *p, bool is_solid, T omega, T &r, T &a, T &b) {
+    if (is_solid) {
+        swap_pairs(p);
+        r = T(1); a = T(0); b = T(0);
+    } else {
+        bgk(p, omega, r, a, b);
     }
-    T r, a, b;
-    bgk(p, omega, r, a, b);
-#pragma unroll
-    for (int q = 0; q < 9; ++q) f[c + q * P] = p[q];
 }
 
-// aa_odd_kernel!: src/kernels/aa_bgk_2d.jl:57-115 (read local, collide, push).
 template <typename T>
-__global__ void __launch_bounds__(BX) aa_odd_k(T *__restrict__ f, const T *__restrict__ src,
-                                                const uint8_t *__restrict__ solid, Grid2<T> g,
-                                                T omega) {
+__global__ void __launch_bounds__(BX) aa_stream_k(T *__restrict__ f, T *__restrict__ rho,
+                                                   T *__restrict__ ux, T *__restrict__ uy,
+                                                   const uint8_t *__restrict__ solid, Grid2<T> g,
+                                                   T omega) {
     NODE2
     const int Nx = g.Nx, Ny = g.Ny;
+    const bool w = i > 0, e = i < Nx - 1, s = j > 0, n = j < Ny - 1;
+    // source (x - c_q) exists?  destination (x + c_q) exists?
+    const bool src[9] = {true, w, s, e, n, w && s, e && s, e && n, w && n};
+    const bool dst[9] = {true, e, n, w, s, e && n, w && n, w && s, e && s};
+    const long long off[9] = {0, 1, (long long)Nx, -1, -(long long)Nx, 1 + (long long)Nx,
+                              -1 + (long long)Nx, -1 - (long long)Nx, 1 - (long long)Nx};
     T p[9];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) p[q] = src[c + q * P];
-    if (solid && solid[c]) {
-        f[c + 1 * P] = p[3]; f[c + 3 * P] = p[1];
-        f[c + 2 * P] = p[4]; f[c + 4 * P] = p[2];
-        f[c + 5 * P] = p[7]; f[c + 7 * P] = p[5];
-        f[c + 6 * P] = p[8]; f[c + 8 * P] = p[6];
-        return;
-    }
+    for (int q = 0; q < 9; ++q)
+        p[q] = src[q] ? f[c - off[q] + kOpp9[q] * P] : f[c + q * P];
     T r, a, b;
-    T cc[9];
+    aa_collide(p, solid && solid[c], omega, r, a, b);
 #pragma unroll
-    for (int q = 0; q < 9; ++q) cc[q] = p[q];
-    bgk(cc, omega, r, a, b);
-    const bool w = i > 0, e = i < Nx - 1, s = j > 0, n = j < Ny - 1;
-    f[c] = cc[0];
-    f[(e ? c + 1 : c) + 1 * P] = e ? cc[1] : cc[3];
-    f[(n ? c + Nx : c) + 2 * P] = n ? cc[2] : cc[4];
-    f[(w ? c - 1 : c) + 3 * P] = w ? cc[3] : cc[1];
-    f[(s ? c - Nx : c) + 4 * P] = s ? cc[4] : cc[2];
-    const bool c6 = e && n, c7 = w && n, c8 = w && s, c9 = e && s;
-    f[(c6 ? c + 1 + Nx : c) + 5 * P] = c6 ? cc[5] : cc[7];
-    f[(c7 ? c - 1 + Nx : c) + 6 * P] = c7 ? cc[6] : cc[8];
-    f[(c8 ? c - 1 - Nx : c) + 7 * P] = c8 ? cc[7] : cc[5];
-    f[(c9 ? c + 1 - Nx : c) + 8 * P] = c9 ? cc[8] : cc[6];
+    for (int q = 0; q < 9; ++q) {
+        if (dst[q]) f[c + off[q] + q * P] = p[q];
+        else f[c + kOpp9[q] * P] = p[q];
+    }
+    if (rho) { rho[c] = r; ux[c] = a; uy[c] = b; }
 }
 
-// collide_mrt_2d_kernel!: src/kernels/collide_mrt_2d.jl:43-109
 template <typename T>
-__global__ void __launch_bounds__(BX) mrt_k(T *__restrict__ f, const uint8_t *__restrict__ solid,
-                                             Grid2<T> g, T s_e, T s_eps, T s_q, T s_nu) {
+__global__ void __launch_bounds__(BX) aa_local_k(T *__restrict__ f, T *__restrict__ rho,
+                                                  T *__restrict__ ux, T *__restrict__ uy,
+                                                  const uint8_t *__restrict__ solid, Grid2<T> g,
+                                                  T omega) {
     NODE2
     T p[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) p[q] = f[c + q * P];
-    if (solid && solid[c]) {
-        swap_pairs(p);
+    T r, a, b;
+    aa_collide(p, solid && solid[c], omega, r, a, b);
 #pragma unroll
-        for (int q = 0; q < 9; ++q) f[c + q * P] = p[q];
-        return;
-    }
+    for (int q = 0; q < 9; ++q) f[c + kOpp9[q] * P] = p[q];
+    if (rho) { rho[c] = r; ux[c] = a; uy[c] = b; }
+}
+
+// collide_mrt_2d_kernel! node update: src/kernels/collide_mrt_2d.jl:54-106
+template <typename T>
+__device__ __forceinline__ void mrt_node(T *p, T s_e, T s_eps, T s_q, T s_nu) {
     const T f1 = p[0], f2 = p[1], f3 = p[2], f4 = p[3], f5 = p[4], f6 = p[5], f7 = p[6],
             f8 = p[7], f9 = p[8];
     T rho = f1 + f2 + f3 + f4 + f5 + f6 + f7 + f8 + f9;
@@ -427,15 +431,54 @@ __global__ void __launch_bounds__(BX) mrt_k(T *__restrict__ f, const uint8_t *__
     const T r = rho, jxs = jx, jys = jy;
     const T c9 = T(1.0 / 9.0), c36 = T(1.0 / 36.0), c18 = T(1.0 / 18.0), c6 = T(1.0 / 6.0),
             c4 = T(1.0 / 4.0), c12 = T(1.0 / 12.0);
-    f[c + 0 * P] = c9 * r - c9 * es + c9 * ep;
-    f[c + 1 * P] = c9 * r - c36 * es - c18 * ep + c6 * jxs - c6 * qxs + c4 * ps;
-    f[c + 2 * P] = c9 * r - c36 * es - c18 * ep + c6 * jys - c6 * qys - c4 * ps;
-    f[c + 3 * P] = c9 * r - c36 * es - c18 * ep - c6 * jxs + c6 * qxs + c4 * ps;
-    f[c + 4 * P] = c9 * r - c36 * es - c18 * ep - c6 * jys + c6 * qys - c4 * ps;
-    f[c + 5 * P] = c9 * r + c18 * es + c36 * ep + c6 * jxs + c12 * qxs + c6 * jys + c12 * qys + c4 * pxys;
-    f[c + 6 * P] = c9 * r + c18 * es + c36 * ep - c6 * jxs - c12 * qxs + c6 * jys + c12 * qys - c4 * pxys;
-    f[c + 7 * P] = c9 * r + c18 * es + c36 * ep - c6 * jxs - c12 * qxs - c6 * jys - c12 * qys + c4 * pxys;
-    f[c + 8 * P] = c9 * r + c18 * es + c36 * ep + c6 * jxs + c12 * qxs - c6 * jys - c12 * qys - c4 * pxys;
+    p[0] = c9 * r - c9 * es + c9 * ep;
+    p[1] = c9 * r - c36 * es - c18 * ep + c6 * jxs - c6 * qxs + c4 * ps;
+    p[2] = c9 * r - c36 * es - c18 * ep + c6 * jys - c6 * qys - c4 * ps;
+    p[3] = c9 * r - c36 * es - c18 * ep - c6 * jxs + c6 * qxs + c4 * ps;
+    p[4] = c9 * r - c36 * es - c18 * ep - c6 * jys + c6 * qys - c4 * ps;
+    p[5] = c9 * r + c18 * es + c36 * ep + c6 * jxs + c12 * qxs + c6 * jys + c12 * qys + c4 * pxys;
+    p[6] = c9 * r + c18 * es + c36 * ep - c6 * jxs - c12 * qxs + c6 * jys + c12 * qys - c4 * pxys;
+    p[7] = c9 * r + c18 * es + c36 * ep - c6 * jxs - c12 * qxs - c6 * jys - c12 * qys + c4 * pxys;
+    p[8] = c9 * r + c18 * es + c36 * ep + c6 * jxs + c12 * qxs - c6 * jys - c12 * qys - c4 * pxys;
+}
+
+// collide_mrt_2d_kernel!: src/kernels/collide_mrt_2d.jl:43-109
+template <typename T>
+__global__ void __launch_bounds__(BX) mrt_k(T *__restrict__ f, const uint8_t *__restrict__ solid,
+                                             Grid2<T> g, T s_e, T s_eps, T s_q, T s_nu) {
+    NODE2
+    T p[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p[q] = f[c + q * P];
+    if (solid && solid[c]) swap_pairs(p);
+    else mrt_node(p, s_e, s_eps, s_q, s_nu);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[c + q * P] = p[q];
+}
+
+// One step of the MRT cavity loop of test/test_mrt.jl:19-25 (stream_2d! ->
+// apply_zou_he_north_2d! -> collide_mrt_2d! -> compute_macroscopic_2d!) in
+// one launch; node-local after the pull, so the bits are the same.
+template <typename T>
+__global__ void __launch_bounds__(BX) cavity_mrt_step_k(T *__restrict__ fo, const T *__restrict__ fi,
+                                                         T *__restrict__ rho, T *__restrict__ ux,
+                                                         T *__restrict__ uy,
+                                                         const uint8_t *__restrict__ solid,
+                                                         Grid2<T> g, T s_e, T s_eps, T s_q,
+                                                         T s_nu, T u_lid) {
+    NODE2
+    T p[9];
+    pull_bb(fi, g, i, j, p);
+    if (j == g.Ny - 1) zou_he_north_node(p, u_lid);
+    if (solid && solid[c]) swap_pairs(p);
+    else mrt_node(p, s_e, s_eps, s_q, s_nu);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) fo[c + q * P] = p[q];
+    if (rho) {
+        T r, a, b;
+        macro_node(p, r, a, b);
+        rho[c] = r; ux[c] = a; uy[c] = b;
+    }
 }
 
 // stream_fully_periodic_2d_kernel!: src/kernels/stream_periodic_2d.jl:79-98
@@ -500,6 +543,41 @@ __global__ void __launch_bounds__(BX) cavity_step_k(T *__restrict__ fo, const T 
     T r, a, b;
     macro_node(p, r, a, b);
     rho[c] = r; ux[c] = a; uy[c] = b;
+}
+
+// Lid-driven cavity step with a moving-wall half-way bounce-back lid: the
+// DSL composition PullHalfwayBB -> ApplyHalfwayBBPrePhase -> Moments ->
+// CollideBGK -> WriteMoments; the lid link rule is
+// src/kernels/dsl/bricks.jl:447-487 with the top row's north-pointing links
+// (reference q = 3, 6, 7) cut by a wall moving at (u_lid, 0), corners
+// included.  Moments are the pre-collision ones, as in fused_bgk_step!.
+template <typename T>
+__global__ void __launch_bounds__(BX) cavity_movingwall_k(T *__restrict__ fo, const T *__restrict__ fi,
+                                                           T *__restrict__ rho, T *__restrict__ ux,
+                                                           T *__restrict__ uy,
+                                                           const uint8_t *__restrict__ solid,
+                                                           Grid2<T> g, T omega, T u_lid) {
+    NODE2
+    T p[9];
+    pull_bb(fi, g, i, j, p);
+    T r, a, b;
+    if (solid && solid[c]) {
+        swap_pairs(p);
+        r = T(1); a = T(0); b = T(0);
+    } else {
+        if (j == g.Ny - 1) {
+            const T d5 = -T(2.0 / 3.0) * T(0);
+            const T d8 = -T(1.0 / 6.0) * (u_lid + T(0));
+            const T d9 = -T(1.0 / 6.0) * (-u_lid + T(0));
+            p[4] = fi[c + 2 * P] + d5;
+            p[7] = fi[c + 5 * P] + d8;
+            p[8] = fi[c + 6 * P] + d9;
+        }
+        bgk(p, omega, r, a, b);
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) fo[c + q * P] = p[q];
+    if (rho) { rho[c] = r; ux[c] = a; uy[c] = b; }
 }
 
 // ------------------------------------------------------------ thermal DDF --
@@ -647,27 +725,6 @@ int plain_dtype(const char *what, int dtype) {
         return kb::check_launch(what);                    \
     } while (0)
 
-// Library-owned scratch for the A-A snapshot, one per device, grow-only.
-void *aa_scratch(size_t bytes, int *err) {
-    static void *ptr[64] = {nullptr};
-    static size_t cap[64] = {0};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) { *err = KB_ERR_ARG; return nullptr; }
-    if (cap[dev] < bytes) {
-        if (ptr[dev]) cudaFree(ptr[dev]);
-        ptr[dev] = nullptr; cap[dev] = 0;
-        if (cudaMalloc(&ptr[dev], bytes) != cudaSuccess) {
-            cudaGetLastError();
-            *err = KB_ERR_NOMEM;
-            return nullptr;
-        }
-        cap[dev] = bytes;
-    }
-    *err = KB_OK;
-    return ptr[dev];
-}
-
 }  // namespace
 
 extern "C" {
@@ -798,38 +855,30 @@ int kb_fused_trt_step(void *f_out, const void *f_in, void *rho, void *ux, void *
             (T)sp, (T)sm)));
 }
 
-static int aa_step(bool even, void *f, const uint8_t *is_solid, int Nx, int Ny, double omega,
-                   int dtype, void *stream) {
-    const char *what = even ? "kb_aa_even_step" : "kb_aa_odd_step";
-    KB_REQUIRE(f, "%s: null population pointer", what);
-    if (int e = check_dims(what, Nx, Ny)) return e;
-    if (int e = plain_dtype(what, dtype)) return e;
-    const size_t bytes = (size_t)Nx * Ny * 9 * kb::dtype_bytes(dtype);
-    int err = KB_OK;
-    void *snap = aa_scratch(bytes, &err);
-    if (!snap) return kb::set_error(err, "%s: cannot allocate %zu-byte snapshot", what, bytes);
-    cudaStream_t s = kb::as_stream(stream);
-    if (cudaMemcpyAsync(snap, f, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
-        return kb::set_error(KB_ERR_CUDA, "%s: snapshot copy failed: %s", what,
-                             cudaGetErrorString(cudaGetLastError()));
-    if (dtype == KB_F64) {
-        if (even) aa_even_k<double><<<nodes_grid(Nx, Ny), BX, 0, s>>>((double *)f, (const double *)snap, is_solid, grid2<double>(Nx, Ny), omega);
-        else aa_odd_k<double><<<nodes_grid(Nx, Ny), BX, 0, s>>>((double *)f, (const double *)snap, is_solid, grid2<double>(Nx, Ny), omega);
-    } else {
-        if (even) aa_even_k<float><<<nodes_grid(Nx, Ny), BX, 0, s>>>((float *)f, (const float *)snap, is_solid, grid2<float>(Nx, Ny), (float)omega);
-        else aa_odd_k<float><<<nodes_grid(Nx, Ny), BX, 0, s>>>((float *)f, (const float *)snap, is_solid, grid2<float>(Nx, Ny), (float)omega);
-    }
-    return kb::check_launch(what);
-}
-
-int kb_aa_even_step(void *f, const uint8_t *is_solid, int Nx, int Ny, double omega, int dtype,
-                    void *stream) {
-    return aa_step(true, f, is_solid, Nx, Ny, omega, dtype, stream);
-}
-
-int kb_aa_odd_step(void *f, const uint8_t *is_solid, int Nx, int Ny, double omega, int dtype,
+static int aa_step(bool stream_step, void *f, void *rho, void *ux, void *uy,
+                   const uint8_t *is_solid, int Nx, int Ny, double omega, int dtype,
                    void *stream) {
-    return aa_step(false, f, is_solid, Nx, Ny, omega, dtype, stream);
+    const char *what = stream_step ? "kb_aa_stream_step_2d" : "kb_aa_local_step_2d";
+    KB_REQUIRE(f, "%s: null population pointer", what);
+    const int nm = (rho != nullptr) + (ux != nullptr) + (uy != nullptr);
+    KB_REQUIRE(nm == 0 || nm == 3, "%s: pass all three moment arrays or none", what);
+    if (int e = check_dims(what, Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN(what, dtype,
+        (stream_step
+             ? aa_stream_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+                   (T *)f, (T *)rho, (T *)ux, (T *)uy, is_solid, grid2<T>(Nx, Ny), (T)omega)
+             : aa_local_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+                   (T *)f, (T *)rho, (T *)ux, (T *)uy, is_solid, grid2<T>(Nx, Ny), (T)omega)));
+}
+
+int kb_aa_stream_step_2d(void *f, void *rho, void *ux, void *uy, const uint8_t *is_solid, int Nx,
+                         int Ny, double omega, int dtype, void *stream) {
+    return aa_step(true, f, rho, ux, uy, is_solid, Nx, Ny, omega, dtype, stream);
+}
+
+int kb_aa_local_step_2d(void *f, void *rho, void *ux, void *uy, const uint8_t *is_solid, int Nx,
+                        int Ny, double omega, int dtype, void *stream) {
+    return aa_step(false, f, rho, ux, uy, is_solid, Nx, Ny, omega, dtype, stream);
 }
 
 int kb_collide_mrt_2d(void *f, const uint8_t *is_solid, int Nx, int Ny, double nu, double s_e,
@@ -872,6 +921,36 @@ int kb_cavity_step_2d(void *f_out, const void *f_in, void *rho, void *ux, void *
     if (int e = check_dims("kb_cavity_step_2d", Nx, Ny)) return e;
     KB_DISPATCH_PLAIN("kb_cavity_step_2d", dtype,
         (cavity_step_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, is_solid, grid2<T>(Nx, Ny),
+            (T)omega, (T)u_lid)));
+}
+
+int kb_cavity_mrt_step_2d(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                          const uint8_t *is_solid, int Nx, int Ny, double nu, double s_e,
+                          double s_eps, double s_q, double u_lid, int dtype, void *stream) {
+    KB_REQUIRE(f_out && f_in, "kb_cavity_mrt_step_2d: null population pointer");
+    KB_REQUIRE(f_out != f_in, "kb_cavity_mrt_step_2d: f_out and f_in must differ");
+    const int nm = (rho != nullptr) + (ux != nullptr) + (uy != nullptr);
+    KB_REQUIRE(nm == 0 || nm == 3, "kb_cavity_mrt_step_2d: pass all three moment arrays or none");
+    KB_REQUIRE(nu > 0.0, "kb_cavity_mrt_step_2d: nu must be positive (got %g)", nu);
+    if (int e = check_dims("kb_cavity_mrt_step_2d", Nx, Ny)) return e;
+    const double s_nu = 1.0 / (3.0 * nu + 0.5);
+    KB_DISPATCH_PLAIN("kb_cavity_mrt_step_2d", dtype,
+        (cavity_mrt_step_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, is_solid, grid2<T>(Nx, Ny),
+            (T)s_e, (T)s_eps, (T)s_q, (T)s_nu, (T)u_lid)));
+}
+
+int kb_cavity_movingwall_step_2d(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                                 const uint8_t *is_solid, int Nx, int Ny, double omega,
+                                 double u_lid, int dtype, void *stream) {
+    KB_REQUIRE(f_out && f_in, "kb_cavity_movingwall_step_2d: null population pointer");
+    KB_REQUIRE(f_out != f_in, "kb_cavity_movingwall_step_2d: f_out and f_in must differ");
+    const int nm = (rho != nullptr) + (ux != nullptr) + (uy != nullptr);
+    KB_REQUIRE(nm == 0 || nm == 3, "kb_cavity_movingwall_step_2d: pass all three moment arrays or none");
+    if (int e = check_dims("kb_cavity_movingwall_step_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_cavity_movingwall_step_2d", dtype,
+        (cavity_movingwall_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
             (T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, is_solid, grid2<T>(Nx, Ny),
             (T)omega, (T)u_lid)));
 }

@@ -310,7 +310,18 @@ int face_fixed(const Face &F, int Nx, int Ny, int Nz) {
 
 }  // namespace
 
+namespace {
+int g_trt3d_dev_variant = 0;  // see kb_set_kernel_variant
+}
+
 extern "C" {
+
+int kb_set_kernel_variant(int kernel, int variant) {
+    KB_REQUIRE(kernel == 1, "kb_set_kernel_variant: unknown kernel id %d", kernel);
+    KB_REQUIRE(variant >= 0 && variant <= 2, "kb_set_kernel_variant: variant %d not in 0..2", variant);
+    g_trt3d_dev_variant = variant;
+    return KB_OK;
+}
 
 int kb_stream_3d(void *f_out, const void *f_in, int Nx, int Ny, int Nz, int dtype, void *stream) {
     KB_REQUIRE(f_out && f_in, "kb_stream_3d: null population pointer");
@@ -399,7 +410,7 @@ int kb_fused_trt_step_3d(void *f_out, const void *f_in, void *rho, void *ux, voi
             (float *)uz, is_solid, g, (float)sp, (float)sm);
     } else if (dtype == KB_F32_DEV || dtype == KB_F16_DEV || dtype == KB_BF16_DEV) {
         return launch_trt3d_dev(dtype, f_out, f_in, (float *)rho, (float *)ux, (float *)uy,
-                                (float *)uz, is_solid, g, (float)sp, (float)sm, s);
+                                (float *)uz, is_solid, g, (float)sp, (float)sm, s, g_trt3d_dev_variant);
     } else {
         return kb::set_error(KB_ERR_UNSUPPORTED, "%s: unknown dtype %d", what, dtype);
     }

@@ -7,7 +7,10 @@
 namespace kb {
 namespace d3 {
 
-constexpr int BX = 128;
+#ifndef KB_D3_BLOCK_X
+#define KB_D3_BLOCK_X 128
+#endif
+constexpr int BX = KB_D3_BLOCK_X;  // threads per block along x
 
 struct Grid3 {
     int Nx, Ny, Nz;
@@ -86,7 +89,7 @@ inline int check_dims(const char *what, int Nx, int Ny, int Nz) {
 // (kb_d3q19_dev.cu); `per` = periodic bit mask.
 int launch_trt3d_dev(int dtype, void *f_out, const void *f_in, float *rho, float *ux, float *uy,
                      float *uz, const uint8_t *solid, const Grid3 &g, float sp, float sm,
-                     cudaStream_t s);
+                     cudaStream_t s, int variant);
 
 }  // namespace d3
 }  // namespace kb

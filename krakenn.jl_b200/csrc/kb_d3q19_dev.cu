@@ -26,15 +26,10 @@ struct DevLoad {
     __device__ __forceinline__ float operator()(R r) const { return Dev<R>::ld(r); }
 };
 
-// Pair table: (q, qb) and the velocity of q.
-struct PairC {
-    int q, qb, cx, cy, cz;
-};
-__device__ __constant__ PairC kPairs[9] = {
-    {1, 2, 1, 0, 0},    {3, 4, 0, 1, 0},    {5, 6, 0, 0, 1},
-    {7, 10, 1, 1, 0},   {8, 9, -1, 1, 0},   {11, 14, 1, 0, 1},
-    {12, 13, -1, 0, 1}, {15, 18, 0, 1, 1},  {16, 17, 0, -1, 1},
-};
+// Opposite pairs (q, qb) of D3Q19; c_qb = -c_q.  Indexed only with
+// compile-time constants (fully unrolled loops), so d[] stays in registers.
+__device__ constexpr int kPairQ[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16};
+__device__ constexpr int kPairQb[9] = {2, 4, 6, 10, 9, 14, 13, 18, 17};
 
 template <typename R, bool MOM, bool SOLID>
 __global__ void __launch_bounds__(BX) trt_dev_k(R *__restrict__ fo, const R *__restrict__ fi,
@@ -74,27 +69,210 @@ __global__ void __launch_bounds__(BX) trt_dev_k(R *__restrict__ fo, const R *__r
 
 #pragma unroll
     for (int m = 0; m < 9; ++m) {
-        const PairC pc = kPairs[m];
+        const int q = kPairQ[m], qb = kPairQb[m];
         const float w = m < 3 ? float(1.0 / 18.0) : float(1.0 / 36.0);
-        const float cu = float(pc.cx) * ux + float(pc.cy) * uy + float(pc.cz) * uz;
+        const float cu = float(cx19(q)) * ux + float(cy19(q)) * uy + float(cz19(q)) * uz;
         const float deq_p = w * (drho + rho * (4.5f * cu * cu - usq15));
         const float deq_m = w * rho * 3.0f * cu;
-        const float dq = d[pc.q], dqb = d[pc.qb];
+        const float dq = d[q], dqb = d[qb];
         const float np = 0.5f * (dq + dqb) - deq_p;
         const float nm = 0.5f * (dq - dqb) - deq_m;
         const float even = sp * np, odd = sm * nm;
-        fo[c + pc.q * P] = Dev<R>::st(dq - even - odd);
-        fo[c + pc.qb * P] = Dev<R>::st(dqb - even + odd);
+        fo[c + q * P] = Dev<R>::st(dq - even - odd);
+        fo[c + qb * P] = Dev<R>::st(dqb - even + odd);
     }
     if (MOM) { rho_o[c] = rho; ux_o[c] = ux; uy_o[c] = uy; uz_o[c] = uz; }
 }
 
+// ---------------------------------------------------------------------------
+// Two x-adjacent nodes per thread (even Nx).  Each population of a node pair
+// is one aligned 2-element vector access (half2 / bfloat162 / float2); the
+// x-shifted pulls take the missing neighbour element from the adjacent lane
+// with a warp shuffle (lanes at a warp edge load it directly).  The collision
+// runs on the pair in packed FP32x2 arithmetic (FADD2/FMUL2/FFMA2, sm_100),
+// which halves the instruction count per node with FP32 results.
+template <typename R> struct Vec2;
+template <> struct Vec2<float> {
+    using T = float2;
+    static __device__ __forceinline__ float2 ld(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+    static __device__ __forceinline__ void st(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
+};
+template <> struct Vec2<__half> {
+    static __device__ __forceinline__ float2 ld(const __half *p) {
+        return __half22float2(*reinterpret_cast<const __half2 *>(p));
+    }
+    static __device__ __forceinline__ void st(__half *p, float2 v) {
+        *reinterpret_cast<__half2 *>(p) = __floats2half2_rn(v.x, v.y);
+    }
+};
+template <> struct Vec2<__nv_bfloat16> {
+    static __device__ __forceinline__ float2 ld(const __nv_bfloat16 *p) {
+        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(p));
+    }
+    static __device__ __forceinline__ void st(__nv_bfloat16 *p, float2 v) {
+        *reinterpret_cast<__nv_bfloat162 *>(p) = __floats2bfloat162_rn(v.x, v.y);
+    }
+};
+
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// Pull population q for the node pair (x0, x0+1) of row (j, k).
+//   src_ok:  the (y, z) source row exists (inside, or wrapped)
+//   src:     row x = 0 of population q in the source row
+//   own_opp: row x = 0 of the opposite population in the pair's own row
+template <typename R, int CX>
+__device__ __forceinline__ float2 pull_pair(bool src_ok, const R *__restrict__ src,
+                                            const R *__restrict__ own_opp, int x0, int Nx, bool px,
+                                            int lane, bool valid) {
+    if (!src_ok) return valid ? Vec2<R>::ld(own_opp + x0) : f2(0.f);  // y/z wall: both bounce
+    const float2 a = valid ? Vec2<R>::ld(src + x0) : f2(0.f);
+    if (CX == 0) return a;
+    if (CX == 1) {
+        // node x0 pulls x0-1, node x0+1 pulls x0
+        const float up = __shfl_up_sync(0xffffffffu, a.y, 1);
+        float left = up;
+        if (valid && (lane == 0 || x0 == 0)) {
+            if (x0 > 0) left = Dev<R>::ld(src[x0 - 1]);
+            else left = px ? Dev<R>::ld(src[Nx - 1]) : Dev<R>::ld(own_opp[x0]);
+        }
+        return make_float2(left, a.x);
+    }
+    // CX == -1: node x0 pulls x0+1, node x0+1 pulls x0+2
+    const float dn = __shfl_down_sync(0xffffffffu, a.x, 1);
+    float right = dn;
+    if (valid && (lane == 31 || x0 + 2 >= Nx)) {
+        if (x0 + 2 < Nx) right = Dev<R>::ld(src[x0 + 2]);
+        else right = px ? Dev<R>::ld(src[0]) : Dev<R>::ld(own_opp[x0 + 1]);
+    }
+    return make_float2(a.y, right);
+}
+
+template <typename R, bool MOM, bool SOLID>
+__global__ void __launch_bounds__(BX) trt_dev_x2_k(R *__restrict__ fo, const R *__restrict__ fi,
+                                                    float *__restrict__ rho_o, float *__restrict__ ux_o,
+                                                    float *__restrict__ uy_o, float *__restrict__ uz_o,
+                                                    const uint8_t *__restrict__ solid, Grid3 g,
+                                                    float sp, float sm) {
+    const int lane = threadIdx.x & 31;
+    const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int j = blockIdx.y, k = blockIdx.z;
+    const bool valid = x0 < g.Nx;
+    const int Nx = g.Nx;
+    const size_t P = g.plane;
+    const bool px = g.per & 1, py = (g.per >> 1) & 1, pz = (g.per >> 2) & 1;
+    const long long sy = Nx, sz = (long long)Nx * g.Ny;
+    const long long row = (long long)j * sy + (long long)k * sz;
+    // source rows for c_y = +1 / -1 and c_z = +1 / -1 (offsets added to `row`)
+    const bool ym = py || j > 0, yp = py || j < g.Ny - 1;
+    const bool zm = pz || k > 0, zp = pz || k < g.Nz - 1;
+    const long long oym = (j > 0 ? -1 : (long long)(g.Ny - 1)) * sy;
+    const long long oyp = (j < g.Ny - 1 ? 1 : -(long long)(g.Ny - 1)) * sy;
+    const long long ozm = (k > 0 ? -1 : (long long)(g.Nz - 1)) * sz;
+    const long long ozp = (k < g.Nz - 1 ? 1 : -(long long)(g.Nz - 1)) * sz;
+    const R *f = fi + row;
+
+#define KB_PULL(Q, OPP, CX, OK, OFF) \
+    pull_pair<R, CX>(OK, f + (OFF) + (size_t)(Q) * P, f + (size_t)(OPP) * P, x0, Nx, px, lane, valid)
+    float2 d[19];
+    d[0] = KB_PULL(0, 0, 0, true, 0);
+    d[1] = KB_PULL(1, 2, 1, true, 0);
+    d[2] = KB_PULL(2, 1, -1, true, 0);
+    d[3] = KB_PULL(3, 4, 0, ym, oym);
+    d[4] = KB_PULL(4, 3, 0, yp, oyp);
+    d[5] = KB_PULL(5, 6, 0, zm, ozm);
+    d[6] = KB_PULL(6, 5, 0, zp, ozp);
+    d[7] = KB_PULL(7, 10, 1, ym, oym);
+    d[8] = KB_PULL(8, 9, -1, ym, oym);
+    d[9] = KB_PULL(9, 8, 1, yp, oyp);
+    d[10] = KB_PULL(10, 7, -1, yp, oyp);
+    d[11] = KB_PULL(11, 14, 1, zm, ozm);
+    d[12] = KB_PULL(12, 13, -1, zm, ozm);
+    d[13] = KB_PULL(13, 12, 1, zp, ozp);
+    d[14] = KB_PULL(14, 11, -1, zp, ozp);
+    d[15] = KB_PULL(15, 18, 0, ym && zm, oym + ozm);
+    d[16] = KB_PULL(16, 17, 0, yp && zm, oyp + ozm);
+    d[17] = KB_PULL(17, 16, 0, ym && zp, oym + ozp);
+    d[18] = KB_PULL(18, 15, 0, yp && zp, oyp + ozp);
+#undef KB_PULL
+    if (!valid) return;
+
+    float2 drho = d[0];
+#pragma unroll
+    for (int q = 1; q < 19; ++q) drho = add2(drho, d[q]);
+    const float2 jx = add2(add2(add2(sub2(d[1], d[2]), sub2(d[7], d[8])), add2(sub2(d[9], d[10]), sub2(d[11], d[12]))), sub2(d[13], d[14]));
+    const float2 jy = add2(add2(add2(sub2(d[3], d[4]), add2(d[7], d[8])), sub2(add2(d[15], d[17]), add2(d[9], d[10]))), sub2(sub2(f2(0.f), d[16]), d[18]));
+    const float2 jz = add2(add2(add2(sub2(d[5], d[6]), add2(d[11], d[12])), sub2(add2(d[15], d[16]), add2(d[13], d[14]))), sub2(sub2(f2(0.f), d[17]), d[18]));
+    const float2 rho = add2(f2(1.0f), drho);
+    const float2 inv = make_float2(__frcp_rn(rho.x), __frcp_rn(rho.y));
+    const float2 ux = mul2(jx, inv), uy = mul2(jy, inv), uz = mul2(jz, inv);
+    const float2 usq15 = mul2(f2(1.5f), fma2(ux, ux, fma2(uy, uy, mul2(uz, uz))));
+    const float2 vsp = f2(sp), vsm = f2(sm);
+    const size_t oc = (size_t)row + x0;
+    // rest population: even mode only
+    {
+        const float2 deq0 = mul2(f2(float(1.0 / 3.0)), sub2(drho, mul2(rho, usq15)));
+        float2 o = sub2(d[0], mul2(vsp, sub2(d[0], deq0)));
+        if (SOLID) { const uchar2 m = *reinterpret_cast<const uchar2 *>(solid + oc); if (m.x) o.x = 0.f; if (m.y) o.y = 0.f; }
+        Vec2<R>::st(fo + oc, o);
+    }
+    const uchar2 sm2 = SOLID ? *reinterpret_cast<const uchar2 *>(solid + oc) : make_uchar2(0, 0);
+#pragma unroll
+    for (int m = 0; m < 9; ++m) {
+        const int q = kPairQ[m], qb = kPairQb[m];
+        const float w = m < 3 ? float(1.0 / 18.0) : float(1.0 / 36.0);
+        float2 cu = f2(0.f);
+        if (cx19(q) == 1) cu = add2(cu, ux); else if (cx19(q) == -1) cu = sub2(cu, ux);
+        if (cy19(q) == 1) cu = add2(cu, uy); else if (cy19(q) == -1) cu = sub2(cu, uy);
+        if (cz19(q) == 1) cu = add2(cu, uz); else if (cz19(q) == -1) cu = sub2(cu, uz);
+        const float2 deq_p = mul2(f2(w), fma2(rho, fma2(mul2(f2(4.5f), cu), cu, make_float2(-usq15.x, -usq15.y)), drho));
+        const float2 deq_m = mul2(mul2(f2(3.0f * w), rho), cu);
+        const float2 np = fma2(f2(0.5f), add2(d[q], d[qb]), make_float2(-deq_p.x, -deq_p.y));
+        const float2 nm = fma2(f2(0.5f), sub2(d[q], d[qb]), make_float2(-deq_m.x, -deq_m.y));
+        const float2 ev = mul2(vsp, np), od = mul2(vsm, nm);
+        float2 oq = sub2(sub2(d[q], ev), od);
+        float2 ob = add2(sub2(d[qb], ev), od);
+        if (SOLID) {
+            if (sm2.x) { oq.x = 0.f; ob.x = 0.f; }
+            if (sm2.y) { oq.y = 0.f; ob.y = 0.f; }
+        }
+        Vec2<R>::st(fo + (size_t)q * P + oc, oq);
+        Vec2<R>::st(fo + (size_t)qb * P + oc, ob);
+    }
+    if (MOM) {
+        float2 r = rho, a = ux, b = uy, c = uz;
+        if (SOLID) {
+            if (sm2.x) { r.x = 1.f; a.x = b.x = c.x = 0.f; }
+            if (sm2.y) { r.y = 1.f; a.y = b.y = c.y = 0.f; }
+        }
+        *reinterpret_cast<float2 *>(rho_o + oc) = r;
+        *reinterpret_cast<float2 *>(ux_o + oc) = a;
+        *reinterpret_cast<float2 *>(uy_o + oc) = b;
+        *reinterpret_cast<float2 *>(uz_o + oc) = c;
+    }
+}
+
 template <typename R>
 static void launch_r(void *f_out, const void *f_in, float *rho, float *ux, float *uy, float *uz,
-                     const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s) {
-    const dim3 grid = nodes_grid(g.Nx, g.Ny, g.Nz);
+                     const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s,
+                     bool pairs) {
     R *fo = (R *)f_out;
     const R *fi = (const R *)f_in;
+    if (pairs) {
+        const dim3 grid((g.Nx / 2 + BX - 1) / BX, g.Ny, g.Nz);
+        if (rho) {
+            if (solid) trt_dev_x2_k<R, true, true><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            else trt_dev_x2_k<R, true, false><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+        } else {
+            if (solid) trt_dev_x2_k<R, false, true><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            else trt_dev_x2_k<R, false, false><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+        }
+        return;
+    }
+    const dim3 grid = nodes_grid(g.Nx, g.Ny, g.Nz);
     if (rho) {
         if (solid) trt_dev_k<R, true, true><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
         else trt_dev_k<R, true, false><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
@@ -106,11 +284,17 @@ static void launch_r(void *f_out, const void *f_in, float *rho, float *ux, float
 
 int launch_trt3d_dev(int dtype, void *f_out, const void *f_in, float *rho, float *ux, float *uy,
                      float *uz, const uint8_t *solid, const Grid3 &g, float sp, float sm,
-                     cudaStream_t s) {
+                     cudaStream_t s, int variant) {
+    // variant: 0 automatic (node pairs when Nx is even), 1 one node per
+    // thread, 2 node pairs (needs even Nx)
+    const bool even = g.Nx % 2 == 0;
+    if (variant == 2 && !even)
+        return set_error(KB_ERR_ARG, "kb_fused_trt_step_3d: the node-pair kernel needs an even Nx");
+    const bool pairs = variant == 2 || (variant == 0 && even);
     switch (dtype) {
-        case KB_F32_DEV: launch_r<float>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s); break;
-        case KB_F16_DEV: launch_r<__half>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s); break;
-        case KB_BF16_DEV: launch_r<__nv_bfloat16>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s); break;
+        case KB_F32_DEV: launch_r<float>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
+        case KB_F16_DEV: launch_r<__half>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
+        case KB_BF16_DEV: launch_r<__nv_bfloat16>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
         default: return set_error(KB_ERR_UNSUPPORTED, "kb_fused_trt_step_3d: unknown dtype %d", dtype);
     }
     return check_launch("kb_fused_trt_step_3d");

@@ -98,21 +98,28 @@ def initialize_3d(config: LBMConfig, T=torch.float64, device=None):
                 is_solid=torch.zeros(shape, dtype=torch.bool, device=d))
 
 
-def run_cavity_2d(config: LBMConfig, backend="b200", T=torch.float64, fused=True, state=None):
+def run_cavity_2d(config: LBMConfig, backend="b200", T=torch.float64, fused=True, state=None,
+                  lid="zou_he"):
     """run_cavity_2d -- src/drivers/basic.jl:112-144.
 
-    fused=False issues the reference's four launches per step (stream_2d!,
-    apply_zou_he_north_2d!, collide_2d!, compute_macroscopic_2d!);
-    fused=True issues the single-launch kb_cavity_step_2d, which gives the
-    same bits."""
+    lid="zou_he" (the reference driver): fused=False issues the reference's
+    four launches per step (stream_2d!, apply_zou_he_north_2d!, collide_2d!,
+    compute_macroscopic_2d!); fused=True issues the single-launch
+    kb_cavity_step_2d, which gives the same bits.
+    lid="moving_wall": half-way bounce-back on all four walls with the
+    moving-wall link rule on the lid (kb_cavity_movingwall_step_2d)."""
     _require_backend(backend)
+    if lid not in ("zou_he", "moving_wall"):
+        raise ValueError(f"unknown lid '{lid}'")
     st = state if state is not None else initialize_2d(config, T)
     f_in, f_out = st["f_in"], st["f_out"]
     rho, ux, uy, solid = st["rho"], st["ux"], st["uy"], st["is_solid"]
     Nx, Ny = config.Nx, config.Ny
     w = omega(config)
     for _ in range(config.max_steps):
-        if fused:
+        if lid == "moving_wall":
+            ops.cavity_movingwall_step_2d_(f_out, f_in, rho, ux, uy, solid, Nx, Ny, w, config.u_lid)
+        elif fused:
             ops.cavity_step_2d_(f_out, f_in, rho, ux, uy, solid, Nx, Ny, w, config.u_lid)
         else:
             ops.stream_2d_(f_out, f_in, Nx, Ny)

@@ -231,16 +231,51 @@ def fused_trt_step_(f_out, f_in, rho, ux, uy, is_solid, Nx, Ny, nu, Lambda=3 / 1
          _stream())
 
 
-def aa_even_step_(f, is_solid, Nx, Ny, omega):
-    """aa_even_step! -- src/kernels/aa_bgk_2d.jl:125"""
+def aa_stream_step_2d_(f, rho, ux, uy, is_solid, Nx, Ny, omega):
+    """In-place A-A step, state S -> P (gather from neighbours, collide,
+    scatter); the race-free form of aa_even_step!/aa_odd_step!
+    (src/kernels/aa_bgk_2d.jl:125,138).  Moments may be None."""
     code = _plain(f); _match2(f, Nx, Ny)
-    call("kb_aa_even_step", _t(f, "f"), _mask(is_solid), Nx, Ny, float(omega), code, _stream())
+    _ptrs_2d_fields(code, Nx, Ny, rho=rho, ux=ux, uy=uy)
+    call("kb_aa_stream_step_2d", _t(f, "f"), _t(rho, "rho"), _t(ux, "ux"), _t(uy, "uy"),
+         _mask(is_solid), Nx, Ny, float(omega), code, _stream())
 
 
-def aa_odd_step_(f, is_solid, Nx, Ny, omega):
-    """aa_odd_step! -- src/kernels/aa_bgk_2d.jl:138"""
+def aa_local_step_2d_(f, rho, ux, uy, is_solid, Nx, Ny, omega):
+    """In-place A-A step, state P -> S (read local, collide, write swapped)."""
     code = _plain(f); _match2(f, Nx, Ny)
-    call("kb_aa_odd_step", _t(f, "f"), _mask(is_solid), Nx, Ny, float(omega), code, _stream())
+    _ptrs_2d_fields(code, Nx, Ny, rho=rho, ux=ux, uy=uy)
+    call("kb_aa_local_step_2d", _t(f, "f"), _t(rho, "rho"), _t(ux, "ux"), _t(uy, "uy"),
+         _mask(is_solid), Nx, Ny, float(omega), code, _stream())
+
+
+AA_SWAP_2D = (0, 3, 4, 1, 2, 7, 8, 5, 6)
+
+
+def persistent_aa_bgk_(f, is_solid, Nx, Ny, omega, Nt):
+    """persistent_aa_bgk! (src/kernels/persistent_bgk_2d.jl:182): Nt A-A steps
+    queued without synchronisation on one pull-format buffer f (slot q holds
+    the post-collision f_q), returned in the same format.  Nt must be even."""
+    if Nt % 2:
+        raise ValueError("persistent_aa_bgk_: Nt must be even (pairs of A-A steps)")
+    idx = torch.tensor(AA_SWAP_2D, device=f.device)
+    f.copy_(f.index_select(0, idx))
+    for _ in range(Nt // 2):
+        aa_stream_step_2d_(f, None, None, None, is_solid, Nx, Ny, omega)
+        aa_local_step_2d_(f, None, None, None, is_solid, Nx, Ny, omega)
+    f.copy_(f.index_select(0, idx))
+    return f
+
+
+def persistent_fused_bgk_(f_in, f_out, rho, ux, uy, is_solid, Nx, Ny, omega, Nt):
+    """persistent_fused_bgk! (src/kernels/persistent_bgk_2d.jl:160): Nt fused
+    BGK steps queued with no host synchronisation; returns (a, b) with a the
+    buffer holding the latest populations."""
+    a, b = f_in, f_out
+    for _ in range(Nt):
+        fused_bgk_step_(b, a, rho, ux, uy, is_solid, Nx, Ny, omega)
+        a, b = b, a
+    return a, b
 
 
 def collide_mrt_2d_(f, is_solid, nu, s_e=1.4, s_eps=1.4, s_q=1.2):
@@ -273,6 +308,28 @@ def cavity_step_2d_(f_out, f_in, rho, ux, uy, is_solid, Nx, Ny, omega, u_lid):
     call("kb_cavity_step_2d", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
          _t(ux, "ux"), _t(uy, "uy"), _mask(is_solid), Nx, Ny, float(omega), float(u_lid), code,
          _stream())
+
+
+def cavity_movingwall_step_2d_(f_out, f_in, rho, ux, uy, is_solid, Nx, Ny, omega, u_lid):
+    """Cavity step with a moving-wall half-way bounce-back lid (fused_bgk_step!
+    + the lid link rule of src/kernels/dsl/bricks.jl:447-487); moments may be None."""
+    code = _plain(f_in)
+    _match2(f_in, Nx, Ny); _match2(f_out, Nx, Ny)
+    _ptrs_2d_fields(code, Nx, Ny, rho=rho, ux=ux, uy=uy)
+    call("kb_cavity_movingwall_step_2d", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
+         _t(ux, "ux"), _t(uy, "uy"), _mask(is_solid), Nx, Ny, float(omega), float(u_lid), code,
+         _stream())
+
+
+def cavity_mrt_step_2d_(f_out, f_in, rho, ux, uy, is_solid, Nx, Ny, nu, u_lid, s_e=1.4,
+                        s_eps=1.4, s_q=1.2):
+    """One MRT cavity step (test/test_mrt.jl:19-25) in one launch; moments may be None."""
+    code = _plain(f_in)
+    _match2(f_in, Nx, Ny); _match2(f_out, Nx, Ny)
+    _ptrs_2d_fields(code, Nx, Ny, rho=rho, ux=ux, uy=uy)
+    call("kb_cavity_mrt_step_2d", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
+         _t(ux, "ux"), _t(uy, "uy"), _mask(is_solid), Nx, Ny, float(nu), float(s_e),
+         float(s_eps), float(s_q), float(u_lid), code, _stream())
 
 
 def fused_natconv_step_(f_out, f_in, g_out, g_in, Temp, Nx, Ny, omega_f, omega_T, beta_g,
@@ -355,6 +412,11 @@ def compute_macroscopic_3d_(rho, ux, uy, uz, f):
     _ptrs_3d_fields(code, Nx, Ny, Nz, rho=rho, ux=ux, uy=uy, uz=uz)
     call("kb_compute_macroscopic_3d", _t(rho, "rho"), _t(ux, "ux"), _t(uy, "uy"), _t(uz, "uz"),
          _t(f, "f"), Nx, Ny, Nz, code, _stream())
+
+
+def set_trt3d_variant(variant: int):
+    """0 automatic, 1 one node per thread, 2 two nodes per thread (even Nx)."""
+    call("kb_set_kernel_variant", 1, int(variant))
 
 
 def periodic_mask(periodic) -> int:

@@ -313,6 +313,48 @@ void or_fused_bgk_2d(double *f_out, const double *f_in, double *rho_o, double *u
         }
 }
 
+/* Lid-driven cavity with a moving-wall half-way bounce-back lid: the DSL
+ * composition PullHalfwayBB -> ApplyHalfwayBBPrePhase -> Moments ->
+ * CollideBGK -> WriteMoments (src/kernels/dsl/bricks.jl:447-487 for the lid
+ * link rule; the pull and BGK as fused_bgk_2d.jl:8-59).  The top row's three
+ * north-pointing links (q = 3, 6, 7 in the reference's 1-based numbering) are
+ * cut by a wall moving at (u_lid, 0), corners included:
+ *   fp5 = f_in[3] - (2/3)*0,  fp8 = f_in[6] - (1/6)(u_lid + 0),
+ *   fp9 = f_in[7] - (1/6)(-u_lid + 0). */
+static inline void lid_links(const double *f, int Nx, int Ny, int i, int j, double u, double *fp) {
+    if (j != Ny - 1) return;
+    const double d5 = -(2.0 / 3.0) * 0.0;
+    const double d8 = -(1.0 / 6.0) * (u + 0.0);
+    const double d9 = -(1.0 / 6.0) * (-u + 0.0);
+    fp[4] = f[I2(i, j, 2)] + d5;
+    fp[7] = f[I2(i, j, 5)] + d8;
+    fp[8] = f[I2(i, j, 6)] + d9;
+}
+
+void or_cavity_movingwall_bgk_2d(double *f_out, const double *f_in, double *rho_o, double *ux_o,
+                                 double *uy_o, const uint8_t *solid, int Nx, int Ny, double omega,
+                                 double u_lid) {
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            double p[9];
+            pull2d(f_in, Nx, Ny, i, j, p);
+            if (solid && solid[N2(i, j)]) {
+                swap_pairs_2d(p);
+                for (int q = 0; q < 9; ++q) f_out[I2(i, j, q)] = p[q];
+                rho_o[N2(i, j)] = 1.0; ux_o[N2(i, j)] = 0.0; uy_o[N2(i, j)] = 0.0;
+                continue;
+            }
+            lid_links(f_in, Nx, Ny, i, j, u_lid, p);
+            double rho, ux, uy, feq[9];
+            moments2d(p, &rho, &ux, &uy);
+            double usq = ux * ux + uy * uy;
+            feq2d_all(rho, ux, uy, usq, feq);
+            for (int q = 0; q < 9; ++q) f_out[I2(i, j, q)] = p[q] - omega * (p[q] - feq[q]);
+            rho_o[N2(i, j)] = rho; ux_o[N2(i, j)] = ux; uy_o[N2(i, j)] = uy;
+        }
+}
+
 /* trt_rates(nu; Lambda): src/kernels/fused_trt_2d.jl:129-133 */
 void or_trt_rates(double nu, double lambda, double *s_plus, double *s_minus) {
     *s_plus = 1.0 / (3.0 * nu + 0.5);
@@ -359,77 +401,6 @@ void or_fused_trt_2d(double *f_out, const double *f_in, double *rho_o, double *u
                 rho_o[N2(i, j)] = rho; ux_o[N2(i, j)] = ux; uy_o[N2(i, j)] = uy;
             }
         }
-}
-
-/* aa_even_step!: src/kernels/aa_bgk_2d.jl:14-53.  Single buffer.  Every node
- * pulls from its neighbours and writes its own slots; the reference runs this
- * as one parallel kernel, which is race-free because under the A-A layout each
- * slot read by a node is written only by that same node.  The oracle reads
- * from a snapshot to express the same data-parallel semantics. */
-void or_aa_even_2d(double *f, const uint8_t *solid, int Nx, int Ny, double omega) {
-    size_t n = (size_t)Nx * Ny * 9;
-    double *src = (double *)malloc(n * sizeof(double));
-    memcpy(src, f, n * sizeof(double));
-#pragma omp parallel for schedule(static)
-    for (int j = 0; j < Ny; ++j)
-        for (int i = 0; i < Nx; ++i) {
-            double p[9];
-            pull2d(src, Nx, Ny, i, j, p);
-            if (solid && solid[N2(i, j)]) {
-                f[I2(i, j, 1)] = p[3]; f[I2(i, j, 3)] = p[1];
-                f[I2(i, j, 2)] = p[4]; f[I2(i, j, 4)] = p[2];
-                f[I2(i, j, 5)] = p[7]; f[I2(i, j, 7)] = p[5];
-                f[I2(i, j, 6)] = p[8]; f[I2(i, j, 8)] = p[6];
-            } else {
-                double rho, ux, uy, feq[9];
-                moments2d(p, &rho, &ux, &uy);
-                double usq = ux * ux + uy * uy;
-                feq2d_all(rho, ux, uy, usq, feq);
-                for (int q = 0; q < 9; ++q) f[I2(i, j, q)] = p[q] - omega * (p[q] - feq[q]);
-            }
-        }
-    free(src);
-}
-
-/* aa_odd_step!: src/kernels/aa_bgk_2d.jl:57-115.  Read local, collide, push. */
-void or_aa_odd_2d(double *f, const uint8_t *solid, int Nx, int Ny, double omega) {
-    size_t n = (size_t)Nx * Ny * 9;
-    double *src = (double *)malloc(n * sizeof(double));
-    memcpy(src, f, n * sizeof(double));
-#pragma omp parallel for schedule(static)
-    for (int j = 0; j < Ny; ++j)
-        for (int i = 0; i < Nx; ++i) {
-            double p[9];
-            for (int q = 0; q < 9; ++q) p[q] = src[I2(i, j, q)];
-            if (solid && solid[N2(i, j)]) {
-                f[I2(i, j, 1)] = p[3]; f[I2(i, j, 3)] = p[1];
-                f[I2(i, j, 2)] = p[4]; f[I2(i, j, 4)] = p[2];
-                f[I2(i, j, 5)] = p[7]; f[I2(i, j, 7)] = p[5];
-                f[I2(i, j, 6)] = p[8]; f[I2(i, j, 8)] = p[6];
-                continue;
-            }
-            double rho, ux, uy, feq[9], c[9];
-            moments2d(p, &rho, &ux, &uy);
-            double usq = ux * ux + uy * uy;
-            feq2d_all(rho, ux, uy, usq, feq);
-            for (int q = 0; q < 9; ++q) c[q] = p[q] - omega * (p[q] - feq[q]);
-            int im = i > 0 ? i - 1 : 0, ip = i < Nx - 1 ? i + 1 : Nx - 1;
-            int jm = j > 0 ? j - 1 : 0, jp = j < Ny - 1 ? j + 1 : Ny - 1;
-            f[I2(i, j, 0)] = c[0];
-            f[I2(i < Nx - 1 ? ip : i, j, 1)] = i < Nx - 1 ? c[1] : c[3];
-            f[I2(i, j < Ny - 1 ? jp : j, 2)] = j < Ny - 1 ? c[2] : c[4];
-            f[I2(i > 0 ? im : i, j, 3)] = i > 0 ? c[3] : c[1];
-            f[I2(i, j > 0 ? jm : j, 4)] = j > 0 ? c[4] : c[2];
-            int c6 = i < Nx - 1 && j < Ny - 1;
-            f[I2(c6 ? ip : i, c6 ? jp : j, 5)] = c6 ? c[5] : c[7];
-            int c7 = i > 0 && j < Ny - 1;
-            f[I2(c7 ? im : i, c7 ? jp : j, 6)] = c7 ? c[6] : c[8];
-            int c8 = i > 0 && j > 0;
-            f[I2(c8 ? im : i, c8 ? jm : j, 7)] = c8 ? c[7] : c[5];
-            int c9 = i < Nx - 1 && j > 0;
-            f[I2(c9 ? ip : i, c9 ? jm : j, 8)] = c9 ? c[8] : c[6];
-        }
-    free(src);
 }
 
 /* collide_mrt_2d!: src/kernels/collide_mrt_2d.jl:43-125.  s_nu is passed in

@@ -36,9 +36,8 @@ _SIG = {
     "or_macroscopic_2d": ([_D, _D, _D, _D, _i, _i], None),
     "or_fused_bgk_2d": ([_D, _D, _D, _D, _D, _U8, _i, _i, _d], None),
     "or_trt_rates": ([_d, _d, _D, _D], None),
+    "or_cavity_movingwall_bgk_2d": ([_D, _D, _D, _D, _D, _U8, _i, _i, _d, _d], None),
     "or_fused_trt_2d": ([_D, _D, _D, _D, _D, _U8, _i, _i, _d, _d], None),
-    "or_aa_even_2d": ([_D, _U8, _i, _i, _d], None),
-    "or_aa_odd_2d": ([_D, _U8, _i, _i, _d], None),
     "or_collide_mrt_2d": ([_D, _U8, _i, _i, _d, _d, _d, _d], None),
     "or_stream_fully_periodic_2d": ([_D, _D, _i, _i], None),
     "or_stream_periodic_x_wall_y_2d": ([_D, _D, _i, _i], None),
@@ -153,6 +152,11 @@ def fused_bgk_2d(f_out, f_in, rho, ux, uy, solid, omega):
     lib().or_fused_bgk_2d(_p(f_out), _p(f_in), _p(rho), _p(ux), _p(uy), _m(solid), *_nxny(f_in), omega)
 
 
+def cavity_movingwall_bgk_2d(f_out, f_in, rho, ux, uy, solid, omega, u_lid):
+    lib().or_cavity_movingwall_bgk_2d(_p(f_out), _p(f_in), _p(rho), _p(ux), _p(uy), _m(solid),
+                                      *_nxny(f_in), omega, u_lid)
+
+
 def trt_rates(nu, lam=3 / 16):
     a, b = C.c_double(), C.c_double()
     lib().or_trt_rates(nu, lam, C.byref(a), C.byref(b))
@@ -161,14 +165,6 @@ def trt_rates(nu, lam=3 / 16):
 
 def fused_trt_2d(f_out, f_in, rho, ux, uy, solid, sp, sm):
     lib().or_fused_trt_2d(_p(f_out), _p(f_in), _p(rho), _p(ux), _p(uy), _m(solid), *_nxny(f_in), sp, sm)
-
-
-def aa_even_2d(f, solid, omega):
-    lib().or_aa_even_2d(_p(f), _m(solid), *_nxny(f), omega)
-
-
-def aa_odd_2d(f, solid, omega):
-    lib().or_aa_odd_2d(_p(f), _m(solid), *_nxny(f), omega)
 
 
 def collide_mrt_2d(f, solid, nu, s_e=1.4, s_eps=1.4, s_q=1.2):

@@ -1,0 +1,102 @@
+"""Batched persistent MRT cavity sweep and CUDA-graph capture."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_mrt_cavity(orc, N, nu, u_lid, steps):
+    w = np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4)
+    f = np.empty((9, N, N))
+    for q in range(9):
+        f[q] = w[q]
+    fo = np.empty_like(f)
+    for _ in range(steps):
+        orc.stream_2d(fo, f)
+        orc.zou_he_north_2d(fo, u_lid)
+        orc.collide_mrt_2d(fo, None, nu)
+        f, fo = fo, f
+    _, ux, uy = orc.macroscopic_2d(f)
+    return ux, uy
+
+
+@pytest.mark.parametrize("storage,tol", [("f32", 2e-6), ("f16", 3e-3), ("bf16", 2e-2)])
+def test_batch_matches_single_case_oracle(cuda, pkg, orc, storage, tol):
+    """Each case of a ragged batch (N = 16, 24, 40) after 200 steps matches the
+    FP64 oracle of the reference loop (stream_2d!, apply_zou_he_north_2d!,
+    collide_mrt_2d!) to `tol` (max |u| error relative to u_lid)."""
+    N = np.array([16, 24, 40], np.int32)
+    nu = np.array([0.05, 0.02, 0.1])
+    u = np.array([0.1, 0.05, 0.08])
+    b = pkg.CavityBatch(N, nu, u, storage)
+    b.run(max_steps=200, check_every=100, tol=0.0)
+    st = b.status()
+    assert not st["timed_out"] and st["live_tiles"] == 0
+    assert st["updates"] == int(np.sum(N.astype(np.int64) ** 2)) * 200
+    for c in range(3):
+        r = b.case(c)
+        assert r["steps"] == 200 and r["state"] == "max_steps"
+        ux, uy = _oracle_mrt_cavity(orc, int(N[c]), nu[c], u[c], 200)
+        err = max(np.max(np.abs(r["ux"] - ux)), np.max(np.abs(r["uy"] - uy))) / u[c]
+        assert err < tol, (c, err)
+    b.close()
+
+
+def test_batch_retires_converged_and_nonfinite(cuda, pkg):
+    """A viscous small cavity converges and retires early; a case with
+    nu -> 0 on a coarse grid blows up and is retired as non-finite; a slow
+    case runs to max_steps.  The tile list shrinks as cases retire."""
+    N = np.array([8, 16, 64], np.int32)
+    nu = np.array([0.5, 1e-6, 0.01])
+    u = np.array([0.05, 0.5, 0.1])
+    b = pkg.CavityBatch(N, nu, u, "f32")
+    b.run(max_steps=20000, check_every=50, tol=1e-6)
+    st = b.status()
+    assert not st["timed_out"]
+    r0, r1, r2 = (b.case(c, fields=False) for c in range(3))
+    assert r0["state"] == "converged" and r0["steps"] < 20000 and r0["residual"] < 1e-6
+    assert r1["state"] == "non-finite" and r1["steps"] < 20000
+    assert r2["state"] in ("max_steps", "converged")
+    assert st["updates"] < int(np.sum(N.astype(np.int64) ** 2)) * 20000
+    b.close()
+
+
+def test_batch_autotune_and_rerun(cuda, pkg):
+    N, nu, u, _ = pkg.sweep_cases(24, seed=3, N_values=(32, 48, 64, 96))
+    b = pkg.CavityBatch(N, nu, u, "f16")
+    t = b.autotune(trial_steps=20)
+    assert t["tile_nodes"] in (256, 512, 1024, 2048, 4096) and t["best_mlups"] >= t["fixed_mlups"] > 0
+    b.run(max_steps=100, check_every=50, tol=0.0)
+    st = b.status()
+    assert st["live_tiles"] == 0 and not st["timed_out"]
+    b.close()
+
+
+def test_bounded_wait_times_out(cuda, pkg):
+    """The bounded wait behind the grid barrier gives up on a flag that nothing
+    sets and reports KB_ERR_TIMEOUT; the context stays usable afterwards."""
+    assert pkg.batch.selftest_bounded_wait(20000)
+    x = torch.ones(4, device="cuda")
+    assert float(x.sum()) == 4.0
+
+
+def test_graph_capture_cavity(cuda, pkg, orc):
+    """100 captured fused cavity steps replayed 3 times equal 300 plain steps."""
+    N, nu, u_lid = 64, 0.02, 0.1
+    cfg = pkg.LBMConfig.d2q9(N, N, nu, u_lid, 300)
+    ref = pkg.run_cavity_2d(cfg, fused=True)
+    st = pkg.initialize_2d(cfg)
+    w = pkg.omega(cfg)
+    g = pkg.Graph()
+    with g:
+        a, b = st["f_in"], st["f_out"]
+        for _ in range(100):
+            pkg.cavity_step_2d_(b, a, st["rho"], st["ux"], st["uy"], st["is_solid"], N, N, w, u_lid)
+            a, b = b, a
+    for _ in range(3):
+        g.launch()
+    torch.cuda.synchronize()
+    assert np.array_equal(st["ux"].cpu().numpy(), ref["ux"])
+    assert np.array_equal(st["rho"].cpu().numpy(), ref["rho"])
+    g.close()

@@ -186,3 +186,56 @@ def test_convert_roundtrip(cuda, pkg):
         pkg.convert_populations(back, d, src_deviation=True)
         tol = {torch.float32: 1e-8, torch.float16: 5e-5, torch.bfloat16: 5e-4}[dt]
         assert np.max(np.abs(_h(back) - f)) < tol
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float16, torch.bfloat16])
+@pytest.mark.parametrize("shape,per", [((34, 6, 5), (1, 1, 1)), ((34, 6, 5), (0, 0, 0)),
+                                       ((66, 3, 4), (0, 1, 0)), ((2, 4, 4), (1, 0, 1))])
+@pytest.mark.parametrize("with_mask", [False, True])
+def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask):
+    """The two-nodes-per-thread kernel (vector accesses, warp-shuffled x
+    neighbours, packed FP32x2 collision) and the one-node kernel compute the
+    same update: on ragged even grids, walls or wraps on every axis and solid
+    nodes, both stay within the storage rounding of the FP64 oracle (max
+    abs error of f relative to w_q) and of each other."""
+    Nx, Ny, Nz = shape
+    rng = np.random.default_rng(7)
+    f = W19[:, None, None, None] * (1 + 0.05 * rng.standard_normal((19, Nz, Ny, Nx)))
+    m = _mask((Nz, Ny, Nx), 3) if with_mask else None
+    sp, sm = orc.trt_rates(0.02, 0.25)
+    ref = np.empty_like(f)
+    mo = [np.empty((Nz, Ny, Nx)) for _ in range(4)]
+    orc.fused_trt_3d(ref, f, mo, m, sp, sm, per)
+    tol = {torch.float32: 2e-6, torch.float16: 2e-3, torch.bfloat16: 1.6e-2}[dtype]
+    src = torch.empty((19, Nz, Ny, Nx), dtype=dtype, device=cuda)
+    pkg.convert_populations(src, _g(f), dst_deviation=True)
+    outs = []
+    try:
+        for variant in (1, 2):
+            pkg.set_trt3d_variant(variant)
+            fo = torch.empty_like(src)
+            mt = [torch.empty((Nz, Ny, Nx), dtype=torch.float32, device=cuda) for _ in range(4)]
+            pkg.fused_trt_step_3d_(fo, src, *mt, _g(m, torch.bool) if m is not None else None,
+                                   Nx, Ny, Nz, 0.02, 0.25, periodic=per, deviation=True)
+            back = torch.empty((19, Nz, Ny, Nx), dtype=torch.float64, device=cuda)
+            pkg.convert_populations(back, fo, src_deviation=True)
+            got = _h(back)
+            err = np.max(np.abs(got - ref) / W19[:, None, None, None])
+            assert err < tol, (variant, err)
+            for t, a in zip(mt, mo):
+                assert np.max(np.abs(_h(t) - a)) < 50 * tol
+            outs.append(got)
+    finally:
+        pkg.set_trt3d_variant(0)
+    assert np.max(np.abs(outs[0] - outs[1]) / W19[:, None, None, None]) < 2 * tol
+
+
+def test_pair_kernel_needs_even_nx(cuda, pkg):
+    pkg.set_trt3d_variant(2)
+    try:
+        f = torch.zeros((19, 4, 4, 5), dtype=torch.float16, device=cuda)
+        with pytest.raises(pkg.KrakenArgumentError):
+            pkg.fused_trt_step_3d_(torch.empty_like(f), f, None, None, None, None, None, 5, 4, 4,
+                                   0.02, 0.25, periodic=(1, 1, 1))
+    finally:
+        pkg.set_trt3d_variant(0)

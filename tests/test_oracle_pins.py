@@ -268,16 +268,3 @@ def test_natconv_de_vahl_davis(orc, pkg, pins):
     T = orc.temperature_2d(g)
     nu_ref = pins["natconv_ra1e3_nu_ref"]
     assert abs(pkg.drivers.nusselt_hot_wall(T) - nu_ref) / nu_ref < 0.005
-
-
-def test_aa_pair_matches_fused_pull(orc):
-    """The oracle's A-A pair applies the reference kernels' data-parallel
-    semantics: an even step after an even step is one pull-collide step."""
-    N = 9
-    rng = np.random.default_rng(0)
-    f = _eq_f2(orc, 1.0, 0.0, 0.0, (N, N)) * (1 + 0.01 * rng.standard_normal((9, N, N)))
-    a = f.copy()
-    orc.aa_even_2d(a, None, 1.2)
-    b, m = np.empty_like(f), [np.empty((N, N)) for _ in range(3)]
-    orc.fused_bgk_2d(b, f.copy(), *m, None, 1.2)
-    assert np.array_equal(a, b)
