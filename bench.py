@@ -338,6 +338,12 @@ def run_gpu(args):
                    "sample": (f"{steps} steps of the periodic D3Q19 TRT Taylor-Green on "
                               f"{n}x{n}x{nz} nodes, FP64, C restatement of the reference CPU path, "
                               f"{dt:.1f} s")}
+        extra = None
+        if not args.no_extra and world == 1:
+            extra = {"cavity2d_config1": bench_cavity2d(pkg, steps=20000),
+                     "natconv_config4": bench_natconv(pkg, 512, 1e5, 2000),
+                     "batch_config3_short": bench_batch(pkg, max_steps=2000, check_every=100,
+                                                        autotune=False)}
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
@@ -357,6 +363,7 @@ def run_gpu(args):
             "e2e": e2e,
             "gpu_launches": args.steps,
             "clocks": clocks,
+            "extra": extra,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -365,11 +372,128 @@ def run_gpu(args):
     return 0
 
 
+# ------------------------------------------------------- other workloads --
+
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def bench_cavity2d(pkg, steps=20000, graph_steps=200):
+    """Plain FP64 D2Q9 BGK cavity 128^2, nu=0.02, u_lid=0.1 (Re=640), half-way
+    bounce-back walls and moving-wall lid, from rest; `steps` fused steps
+    replayed from a captured CUDA graph of `graph_steps` steps."""
+    import torch
+    N, nu, u = 128, 0.02, 0.1
+    cfg = pkg.LBMConfig.d2q9(N, N, nu, u, 0)
+    st = pkg.initialize_2d(cfg)
+    w = pkg.omega(cfg)
+    g = pkg.Graph()
+    with g:
+        a, b = st["f_in"], st["f_out"]
+        for _ in range(graph_steps):
+            pkg.cavity_movingwall_step_2d_(b, a, st["rho"], st["ux"], st["uy"], None, N, N, w, u)
+            a, b = b, a
+    g.launch()
+    torch.cuda.synchronize()
+    st2 = pkg.initialize_2d(cfg)
+    st["f_in"].copy_(st2["f_in"])
+    st["f_out"].copy_(st2["f_out"])
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(steps // graph_steps):
+        g.launch()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ux = st["ux"].cpu().numpy()
+    g.close()
+    return {"workload": "D2Q9 BGK cavity 128^2 FP64, nu=0.02, u_lid=0.1, moving-wall lid, "
+                        f"{steps} steps (CUDA graph of {graph_steps} fused steps)",
+            "mlups": round(N * N * steps / (ms * 1e-3) / 1e6, 1), "ms": round(ms, 2),
+            "max_ux_over_ulid": round(float(abs(ux).max() / u), 4),
+            "finite": bool((ux == ux).all())}
+
+
+def bench_batch(pkg, n_cases=256, max_steps=50000, check_every=100, tol=1e-6, storage="f16",
+                autotune=True):
+    """Batched sweep: n_cases D2Q9 MRT cavities, N uniform on {64,...,512}, Re
+    log-uniform [100, 2000], u_lid=0.1, one persistent launch."""
+    import torch
+    N, nu, u, Re = pkg.sweep_cases(n_cases, seed=0)
+    b = pkg.CavityBatch(N, nu, u, storage)
+    tune = b.autotune(trial_steps=200) if autotune else None
+    b.reset()
+    e0, e1 = _events()
+    e0.record()
+    b.run(max_steps=max_steps, check_every=check_every, tol=tol)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    st = b.status()
+    states = {}
+    for c in range(n_cases):
+        r = b.case(c, fields=False)
+        states[r["state"]] = states.get(r["state"], 0) + 1
+    b.close()
+    out = {"workload": f"{n_cases} D2Q9 MRT cavities, N in 64..512 step 32, Re log-uniform "
+                       f"[100,2000], u_lid=0.1, {storage} deviation storage, residual {tol} or "
+                       f"{max_steps} steps, one persistent cooperative launch",
+           "mlups": round(st["updates"] / (ms * 1e-3) / 1e6, 1), "ms": round(ms, 1),
+           "node_updates": st["updates"], "cases": states, "timed_out": st["timed_out"]}
+    if tune:
+        out["autotune"] = tune
+    return out
+
+
+def bench_natconv(pkg, N=512, Ra=1e5, steps=2000):
+    """Thermal DDF natural convection, 512^2, Pr=0.71, FP32 fused step."""
+    import torch
+    p = pkg.drivers.natconv_parameters(N, Ra, 0.71)
+    cfg = pkg.LBMConfig.d2q9(N, N, p["nu"], 0.0, 0)
+    st = pkg.initialize_2d(cfg, torch.float32)
+    gi = torch.from_numpy(pkg.drivers.natconv_initial_g(N)).to("cuda", torch.float32)
+    go = gi.clone()
+    Temp = torch.zeros((N, N), dtype=torch.float32, device="cuda")
+    fi, fo = st["f_in"], st["f_out"]
+    e0, e1 = _events()
+    for s in range(steps + 10):
+        if s == 10:
+            e0.record()
+        pkg.fused_natconv_step_(fo, fi, go, gi, Temp, N, N, p["omega_f"], p["omega_T"],
+                                p["beta_g"], p["T_ref"], 1.0, 0.0)
+        fi, fo = fo, fi
+        gi, go = go, gi
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"workload": f"thermal DDF natural convection {N}^2 FP32, Ra={Ra:g}, Pr=0.71, "
+                        f"{steps} fused steps", "mlups": round(N * N * steps / (ms * 1e-3) / 1e6, 1),
+            "gbs_alg": round(N * N * steps * 144 / (ms * 1e-3) / 1e9, 1)}
+
+
 def _extrude(plane, n):
     import torch
     out = torch.empty((19, n, n, n), dtype=plane.dtype, device=plane.device)
     out.copy_(plane.expand(19, n, n, n))
     return out
+
+
+def run_other(args):
+    """One of the other configurations, printed as its own JSON line."""
+    import torch
+    import __graft_entry__ as graft
+    torch.cuda.set_device(0)
+    pkg = graft.load_package()
+    pkg._lib.load()
+    if args.workload == "cavity2d":
+        r = bench_cavity2d(pkg, steps=max(args.steps, 200) // 200 * 200)
+    elif args.workload == "batch":
+        r = bench_batch(pkg)
+    else:
+        r = {f"Ra={ra:g}": bench_natconv(pkg, 512, ra, max(args.steps, 100)) for ra in (1e4, 1e5, 1e6)}
+    print(json.dumps({"metric": METRIC, "workload": args.workload, "result": r}), flush=True)
+    return 0
 
 
 def main():
@@ -382,11 +506,16 @@ def main():
     ap.add_argument("--grid", type=int, default=N_GRID)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the short measurements of the other configurations")
+    ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "cavity2d", "batch", "natconv"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "tgv3d":
+        return run_other(args)
     return run_gpu(args)
 
 

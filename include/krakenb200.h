@@ -233,9 +233,9 @@ int kb_fused_trt_step_3d(void *f_out, const void *f_in, void *rho, void *ux, voi
 /* Kernel variant for tuning and tests (process-wide, not thread-safe to
  * change while other threads launch).  kernel 1 = the deviation-storage
  * kernels of kb_fused_trt_step_3d: 0 automatic (two nodes per thread with
- * vector accesses and packed FP32x2 arithmetic when Nx is even, else one
- * node per thread), 1 one node per thread, 2 two nodes per thread.  Every
- * variant computes the same update.  No reference counterpart. */
+ * packed FP32x2 arithmetic for FP16/BF16 when Nx >= 64, else one node per
+ * thread), 1 one node per thread, 2 two nodes per thread.  Every variant
+ * computes the same update up to FP32 rounding.  No reference counterpart. */
 int kb_set_kernel_variant(int kernel, int variant);
 
 /* stream_periodic_xz_movingwall_y_3d!(f_out, f_in, Ub, Ut, Nx, Ny, Nz; rho_w)

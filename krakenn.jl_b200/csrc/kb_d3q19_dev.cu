@@ -85,71 +85,18 @@ __global__ void __launch_bounds__(BX) trt_dev_k(R *__restrict__ fo, const R *__r
 }
 
 // ---------------------------------------------------------------------------
-// Two x-adjacent nodes per thread (even Nx).  Each population of a node pair
-// is one aligned 2-element vector access (half2 / bfloat162 / float2); the
-// x-shifted pulls take the missing neighbour element from the adjacent lane
-// with a warp shuffle (lanes at a warp edge load it directly).  The collision
-// runs on the pair in packed FP32x2 arithmetic (FADD2/FMUL2/FFMA2, sm_100),
-// which halves the instruction count per node with FP32 results.
-template <typename R> struct Vec2;
-template <> struct Vec2<float> {
-    using T = float2;
-    static __device__ __forceinline__ float2 ld(const float *p) { return *reinterpret_cast<const float2 *>(p); }
-    static __device__ __forceinline__ void st(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
-};
-template <> struct Vec2<__half> {
-    static __device__ __forceinline__ float2 ld(const __half *p) {
-        return __half22float2(*reinterpret_cast<const __half2 *>(p));
-    }
-    static __device__ __forceinline__ void st(__half *p, float2 v) {
-        *reinterpret_cast<__half2 *>(p) = __floats2half2_rn(v.x, v.y);
-    }
-};
-template <> struct Vec2<__nv_bfloat16> {
-    static __device__ __forceinline__ float2 ld(const __nv_bfloat16 *p) {
-        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(p));
-    }
-    static __device__ __forceinline__ void st(__nv_bfloat16 *p, float2 v) {
-        *reinterpret_cast<__nv_bfloat162 *>(p) = __floats2bfloat162_rn(v.x, v.y);
-    }
-};
-
+// Two nodes per thread: lane l of a warp owns x = x0 + l and x = x0 + l + 32,
+// x0 = 64 * (global warp index along the row).  Every load and store stays a
+// plain coalesced run of 32 elements; the two nodes share the y/z geometry
+// and most address arithmetic (the second node's addresses are the first's
+// plus 32 elements, away from x walls).  The collision runs on the pair in
+// packed FP32x2 arithmetic (FADD2/FMUL2/FFMA2, sm_100), which halves the
+// arithmetic instruction count with FP32 results.
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-
-// Pull population q for the node pair (x0, x0+1) of row (j, k).
-//   src_ok:  the (y, z) source row exists (inside, or wrapped)
-//   src:     row x = 0 of population q in the source row
-//   own_opp: row x = 0 of the opposite population in the pair's own row
-template <typename R, int CX>
-__device__ __forceinline__ float2 pull_pair(bool src_ok, const R *__restrict__ src,
-                                            const R *__restrict__ own_opp, int x0, int Nx, bool px,
-                                            int lane, bool valid) {
-    if (!src_ok) return valid ? Vec2<R>::ld(own_opp + x0) : f2(0.f);  // y/z wall: both bounce
-    const float2 a = valid ? Vec2<R>::ld(src + x0) : f2(0.f);
-    if (CX == 0) return a;
-    if (CX == 1) {
-        // node x0 pulls x0-1, node x0+1 pulls x0
-        const float up = __shfl_up_sync(0xffffffffu, a.y, 1);
-        float left = up;
-        if (valid && (lane == 0 || x0 == 0)) {
-            if (x0 > 0) left = Dev<R>::ld(src[x0 - 1]);
-            else left = px ? Dev<R>::ld(src[Nx - 1]) : Dev<R>::ld(own_opp[x0]);
-        }
-        return make_float2(left, a.x);
-    }
-    // CX == -1: node x0 pulls x0+1, node x0+1 pulls x0+2
-    const float dn = __shfl_down_sync(0xffffffffu, a.x, 1);
-    float right = dn;
-    if (valid && (lane == 31 || x0 + 2 >= Nx)) {
-        if (x0 + 2 < Nx) right = Dev<R>::ld(src[x0 + 2]);
-        else right = px ? Dev<R>::ld(src[0]) : Dev<R>::ld(own_opp[x0 + 1]);
-    }
-    return make_float2(a.y, right);
-}
 
 template <typename R, bool MOM, bool SOLID>
 __global__ void __launch_bounds__(BX) trt_dev_x2_k(R *__restrict__ fo, const R *__restrict__ fi,
@@ -158,47 +105,20 @@ __global__ void __launch_bounds__(BX) trt_dev_x2_k(R *__restrict__ fo, const R *
                                                     const uint8_t *__restrict__ solid, Grid3 g,
                                                     float sp, float sm) {
     const int lane = threadIdx.x & 31;
-    const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int iA = warp * 64 + lane, iB = iA + 32;
+    if (iA >= g.Nx) return;
+    const bool vB = iB < g.Nx;
     const int j = blockIdx.y, k = blockIdx.z;
-    const bool valid = x0 < g.Nx;
-    const int Nx = g.Nx;
     const size_t P = g.plane;
-    const bool px = g.per & 1, py = (g.per >> 1) & 1, pz = (g.per >> 2) & 1;
-    const long long sy = Nx, sz = (long long)Nx * g.Ny;
-    const long long row = (long long)j * sy + (long long)k * sz;
-    // source rows for c_y = +1 / -1 and c_z = +1 / -1 (offsets added to `row`)
-    const bool ym = py || j > 0, yp = py || j < g.Ny - 1;
-    const bool zm = pz || k > 0, zp = pz || k < g.Nz - 1;
-    const long long oym = (j > 0 ? -1 : (long long)(g.Ny - 1)) * sy;
-    const long long oyp = (j < g.Ny - 1 ? 1 : -(long long)(g.Ny - 1)) * sy;
-    const long long ozm = (k > 0 ? -1 : (long long)(g.Nz - 1)) * sz;
-    const long long ozp = (k < g.Nz - 1 ? 1 : -(long long)(g.Nz - 1)) * sz;
-    const R *f = fi + row;
-
-#define KB_PULL(Q, OPP, CX, OK, OFF) \
-    pull_pair<R, CX>(OK, f + (OFF) + (size_t)(Q) * P, f + (size_t)(OPP) * P, x0, Nx, px, lane, valid)
+    const size_t row = (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k);
+    const size_t cA = row + iA, cB = row + (vB ? iB : iA);
+    float a[19], b[19];
+    pull19(fi, P, cA, pull_geometry(g, iA, j, k), a, DevLoad<R>());
+    pull19(fi, P, cB, pull_geometry(g, vB ? iB : iA, j, k), b, DevLoad<R>());
     float2 d[19];
-    d[0] = KB_PULL(0, 0, 0, true, 0);
-    d[1] = KB_PULL(1, 2, 1, true, 0);
-    d[2] = KB_PULL(2, 1, -1, true, 0);
-    d[3] = KB_PULL(3, 4, 0, ym, oym);
-    d[4] = KB_PULL(4, 3, 0, yp, oyp);
-    d[5] = KB_PULL(5, 6, 0, zm, ozm);
-    d[6] = KB_PULL(6, 5, 0, zp, ozp);
-    d[7] = KB_PULL(7, 10, 1, ym, oym);
-    d[8] = KB_PULL(8, 9, -1, ym, oym);
-    d[9] = KB_PULL(9, 8, 1, yp, oyp);
-    d[10] = KB_PULL(10, 7, -1, yp, oyp);
-    d[11] = KB_PULL(11, 14, 1, zm, ozm);
-    d[12] = KB_PULL(12, 13, -1, zm, ozm);
-    d[13] = KB_PULL(13, 12, 1, zp, ozp);
-    d[14] = KB_PULL(14, 11, -1, zp, ozp);
-    d[15] = KB_PULL(15, 18, 0, ym && zm, oym + ozm);
-    d[16] = KB_PULL(16, 17, 0, yp && zm, oyp + ozm);
-    d[17] = KB_PULL(17, 16, 0, ym && zp, oym + ozp);
-    d[18] = KB_PULL(18, 15, 0, yp && zp, oyp + ozp);
-#undef KB_PULL
-    if (!valid) return;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) d[q] = make_float2(a[q], b[q]);
 
     float2 drho = d[0];
 #pragma unroll
@@ -211,15 +131,13 @@ __global__ void __launch_bounds__(BX) trt_dev_x2_k(R *__restrict__ fo, const R *
     const float2 ux = mul2(jx, inv), uy = mul2(jy, inv), uz = mul2(jz, inv);
     const float2 usq15 = mul2(f2(1.5f), fma2(ux, ux, fma2(uy, uy, mul2(uz, uz))));
     const float2 vsp = f2(sp), vsm = f2(sm);
-    const size_t oc = (size_t)row + x0;
-    // rest population: even mode only
+    uchar2 sm2 = make_uchar2(0, 0);
+    if (SOLID) sm2 = make_uchar2(solid[cA], vB ? solid[cB] : 0);
+    float2 o[19];
     {
         const float2 deq0 = mul2(f2(float(1.0 / 3.0)), sub2(drho, mul2(rho, usq15)));
-        float2 o = sub2(d[0], mul2(vsp, sub2(d[0], deq0)));
-        if (SOLID) { const uchar2 m = *reinterpret_cast<const uchar2 *>(solid + oc); if (m.x) o.x = 0.f; if (m.y) o.y = 0.f; }
-        Vec2<R>::st(fo + oc, o);
+        o[0] = sub2(d[0], mul2(vsp, sub2(d[0], deq0)));
     }
-    const uchar2 sm2 = SOLID ? *reinterpret_cast<const uchar2 *>(solid + oc) : make_uchar2(0, 0);
 #pragma unroll
     for (int m = 0; m < 9; ++m) {
         const int q = kPairQ[m], qb = kPairQb[m];
@@ -233,25 +151,22 @@ __global__ void __launch_bounds__(BX) trt_dev_x2_k(R *__restrict__ fo, const R *
         const float2 np = fma2(f2(0.5f), add2(d[q], d[qb]), make_float2(-deq_p.x, -deq_p.y));
         const float2 nm = fma2(f2(0.5f), sub2(d[q], d[qb]), make_float2(-deq_m.x, -deq_m.y));
         const float2 ev = mul2(vsp, np), od = mul2(vsm, nm);
-        float2 oq = sub2(sub2(d[q], ev), od);
-        float2 ob = add2(sub2(d[qb], ev), od);
-        if (SOLID) {
-            if (sm2.x) { oq.x = 0.f; ob.x = 0.f; }
-            if (sm2.y) { oq.y = 0.f; ob.y = 0.f; }
-        }
-        Vec2<R>::st(fo + (size_t)q * P + oc, oq);
-        Vec2<R>::st(fo + (size_t)qb * P + oc, ob);
+        o[q] = sub2(sub2(d[q], ev), od);
+        o[qb] = add2(sub2(d[qb], ev), od);
+    }
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        fo[cA + q * P] = Dev<R>::st(SOLID && sm2.x ? 0.f : o[q].x);
+        if (vB) fo[cB + q * P] = Dev<R>::st(SOLID && sm2.y ? 0.f : o[q].y);
     }
     if (MOM) {
-        float2 r = rho, a = ux, b = uy, c = uz;
-        if (SOLID) {
-            if (sm2.x) { r.x = 1.f; a.x = b.x = c.x = 0.f; }
-            if (sm2.y) { r.y = 1.f; a.y = b.y = c.y = 0.f; }
+        const bool sA = SOLID && sm2.x, sB = SOLID && sm2.y;
+        rho_o[cA] = sA ? 1.f : rho.x; ux_o[cA] = sA ? 0.f : ux.x;
+        uy_o[cA] = sA ? 0.f : uy.x; uz_o[cA] = sA ? 0.f : uz.x;
+        if (vB) {
+            rho_o[cB] = sB ? 1.f : rho.y; ux_o[cB] = sB ? 0.f : ux.y;
+            uy_o[cB] = sB ? 0.f : uy.y; uz_o[cB] = sB ? 0.f : uz.y;
         }
-        *reinterpret_cast<float2 *>(rho_o + oc) = r;
-        *reinterpret_cast<float2 *>(ux_o + oc) = a;
-        *reinterpret_cast<float2 *>(uy_o + oc) = b;
-        *reinterpret_cast<float2 *>(uz_o + oc) = c;
     }
 }
 
@@ -262,7 +177,8 @@ static void launch_r(void *f_out, const void *f_in, float *rho, float *ux, float
     R *fo = (R *)f_out;
     const R *fi = (const R *)f_in;
     if (pairs) {
-        const dim3 grid((g.Nx / 2 + BX - 1) / BX, g.Ny, g.Nz);
+        const int threads_x = (g.Nx + 63) / 64 * 32;  // one warp per 64 nodes of a row
+        const dim3 grid((threads_x + BX - 1) / BX, g.Ny, g.Nz);
         if (rho) {
             if (solid) trt_dev_x2_k<R, true, true><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
             else trt_dev_x2_k<R, true, false><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
@@ -285,12 +201,11 @@ static void launch_r(void *f_out, const void *f_in, float *rho, float *ux, float
 int launch_trt3d_dev(int dtype, void *f_out, const void *f_in, float *rho, float *ux, float *uy,
                      float *uz, const uint8_t *solid, const Grid3 &g, float sp, float sm,
                      cudaStream_t s, int variant) {
-    // variant: 0 automatic (node pairs when Nx is even), 1 one node per
-    // thread, 2 node pairs (needs even Nx)
-    const bool even = g.Nx % 2 == 0;
-    if (variant == 2 && !even)
-        return set_error(KB_ERR_ARG, "kb_fused_trt_step_3d: the node-pair kernel needs an even Nx");
-    const bool pairs = variant == 2 || (variant == 0 && even);
+    // variant: 0 automatic (two nodes per thread for 16-bit storages when a
+    // row holds at least 64 nodes), 1 one node per thread, 2 two nodes per
+    // thread
+    const bool pairs = variant == 2 ||
+                       (variant == 0 && dtype != KB_F32_DEV && g.Nx >= 64);
     switch (dtype) {
         case KB_F32_DEV: launch_r<float>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
         case KB_F16_DEV: launch_r<__half>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;

@@ -486,6 +486,7 @@ def synchronize():
 
 __all__ = [n for n in dir() if n.endswith("_") and not n.startswith("_")] + [
     "trt_rates", "convert_populations", "mass", "residual", "synchronize", "storage_dtype",
+    "set_trt3d_variant", "AA_SWAP_2D",
     "torch_dtype", "field_dtype", "periodic_mask", "FACES_3D"]
 
 _ = _lib  # keep the module import explicit for readers

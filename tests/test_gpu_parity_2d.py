@@ -224,8 +224,9 @@ def test_cavity_zou_he_path_b_diverges_like_oracle(cuda, pkg, orc):
 
 def test_cavity_float32_close(cuda, pkg, orc):
     """Float32 storage and arithmetic (the reference's T=Float32 path) stays
-    within FP32 rounding of the FP64 oracle over 500 steps."""
-    N, nu, u_lid, steps = 64, 0.02, 0.1, 500
+    within FP32 rounding of the FP64 oracle over 500 steps (nu = 0.05, where
+    the reference's Zou-He cavity is stable at 64^2)."""
+    N, nu, u_lid, steps = 64, 0.05, 0.1, 500
     cfg = pkg.LBMConfig.d2q9(N, N, nu, u_lid, steps)
     f = np.empty((9, N, N))
     for q in range(9):

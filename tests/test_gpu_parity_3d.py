@@ -189,15 +189,16 @@ def test_convert_roundtrip(cuda, pkg):
 
 
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float16, torch.bfloat16])
-@pytest.mark.parametrize("shape,per", [((34, 6, 5), (1, 1, 1)), ((34, 6, 5), (0, 0, 0)),
-                                       ((66, 3, 4), (0, 1, 0)), ((2, 4, 4), (1, 0, 1))])
+@pytest.mark.parametrize("shape,per", [((34, 6, 5), (1, 1, 1)), ((33, 6, 5), (0, 0, 0)),
+                                       ((97, 3, 4), (0, 1, 0)), ((64, 4, 4), (1, 0, 1)),
+                                       ((2, 4, 4), (1, 0, 1)), ((130, 2, 3), (1, 1, 0))])
 @pytest.mark.parametrize("with_mask", [False, True])
 def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask):
-    """The two-nodes-per-thread kernel (vector accesses, warp-shuffled x
-    neighbours, packed FP32x2 collision) and the one-node kernel compute the
-    same update: on ragged even grids, walls or wraps on every axis and solid
-    nodes, both stay within the storage rounding of the FP64 oracle (max
-    abs error of f relative to w_q) and of each other."""
+    """The two-nodes-per-thread kernel (nodes x and x+32 of a warp, packed
+    FP32x2 collision) and the one-node kernel compute the same update: on
+    ragged grids, walls or wraps on every axis and solid nodes, both stay
+    within the storage rounding of the FP64 oracle (max abs error of f
+    relative to w_q) and of each other."""
     Nx, Ny, Nz = shape
     rng = np.random.default_rng(7)
     f = W19[:, None, None, None] * (1 + 0.05 * rng.standard_normal((19, Nz, Ny, Nx)))
@@ -228,14 +229,3 @@ def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask):
     finally:
         pkg.set_trt3d_variant(0)
     assert np.max(np.abs(outs[0] - outs[1]) / W19[:, None, None, None]) < 2 * tol
-
-
-def test_pair_kernel_needs_even_nx(cuda, pkg):
-    pkg.set_trt3d_variant(2)
-    try:
-        f = torch.zeros((19, 4, 4, 5), dtype=torch.float16, device=cuda)
-        with pytest.raises(pkg.KrakenArgumentError):
-            pkg.fused_trt_step_3d_(torch.empty_like(f), f, None, None, None, None, None, 5, 4, 4,
-                                   0.02, 0.25, periodic=(1, 1, 1))
-    finally:
-        pkg.set_trt3d_variant(0)
