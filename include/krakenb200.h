@@ -322,6 +322,22 @@ int kb_convert_populations(void *dst, int dst_dtype, const void *src, int src_dt
 int kb_mass(const void *f, int lattice_q, size_t n_nodes, int dtype, double *out_host,
             void *stream);
 
+/* kb_mass without any device allocation.  No counterpart in the reference:
+ * it exists for callers that cannot let the library call cudaMalloc, such as
+ * a host program whose own pool already owns the device memory, or a loop
+ * that must not pay the device-wide synchronisation that cudaMalloc and
+ * cudaFree bring.  The partial sums go to a fixed 256 KiB array in device
+ * memory that the library holds on every GPU that loads it until the
+ * process exits, so at most 1,073,479,680 populations (lattice_q * n_nodes)
+ * fit; a larger call returns KB_ERR_ARG and names kb_mass.  The first call
+ * on a device looks the array's address up (cudaGetSymbolAddress), so make
+ * it before any stream capture.  All calls share the one array and each
+ * call clears what must start at zero, but calls that overlap on the GPU
+ * (other streams, other host threads) race.  Result, flag and
+ * synchronisation as kb_mass. */
+int kb_mass_static(const void *f, int lattice_q, size_t n_nodes, int dtype, double *out_host,
+                   void *stream);
+
 /* Steady residual r_u = ||u - u_prev||_2 / ||u||_2 over fluid nodes (FP64
  * accumulation), written to *out_host; synchronises `stream`.  uz/uz_prev
  * are NULL in 2D.  Fields are double for KB_F64, float otherwise.  The

@@ -81,6 +81,7 @@ SIGNATURES: dict[str, list] = {
     "kb_selftest_bounded_wait": [C.c_longlong, C.POINTER(_i), _vp],
     "kb_convert_populations": [_vp, _i, _cvp, _i, _i, _sz, _vp],
     "kb_mass": [_cvp, _i, _sz, _i, _dp, _vp],
+    "kb_mass_static": [_cvp, _i, _sz, _i, _dp, _vp],
     "kb_residual": [_cvp, _cvp, _cvp, _cvp, _cvp, _cvp, _u8p, _sz, _i, _dp, _vp],
 }
 _RESTYPES = {"kb_version": C.c_char_p, "kb_last_error": C.c_char_p}

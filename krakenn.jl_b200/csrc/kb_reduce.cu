@@ -190,6 +190,40 @@ int finish(const char *what, void *ws, int nres, double *res, int *bad, cudaStre
     return KB_OK;
 }
 
+// ------------------------------------------------------- static scratch --
+// Scratch of kb_mass_static: a fixed array in device memory that exists as
+// soon as the library is loaded on a device, so that entry point never
+// allocates.  Layout: [head: int flag @0, double result @16 | 64 B]
+// [partial sums, one KSum per block].  Every GPU that loads the library
+// holds these bytes until the process exits.
+constexpr size_t kStaticScratchBytes = 256 * 1024;
+constexpr size_t kStaticMaxPartials = (kStaticScratchBytes - kHead) / sizeof(red::KSum);
+// Each thread of kb_mass_static adds up to 256 populations, so one block
+// (256 threads) covers 65536 and one partial sum stands for 65536 items.
+constexpr size_t kStaticItemsPerBlock = 256 * (size_t)red::RT;
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+// Device address of g_static_scratch on the current device, looked up once
+// per device (host code may not use the symbol's name as an address).
+int static_scratch(char **out) {
+    static char *addr[64] = {nullptr};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 64)
+        return set_error(KB_ERR_CUDA, "kb_mass_static: no current device");
+    if (!addr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess || !p)
+            return set_error(KB_ERR_CUDA, "kb_mass_static: cudaGetSymbolAddress failed: %s",
+                             cudaGetErrorString(e));
+        addr[dev] = (char *)p;
+    }
+    *out = addr[dev];
+    return KB_OK;
+}
+
 }  // namespace
 }  // namespace kb
 
@@ -259,6 +293,48 @@ int kb_residual(const void *ux, const void *uy, const void *uz, const void *ux_p
     if (int e = finish("kb_residual", ws, 2, sums, &flag, s)) return e;
     *out_host = sqrt(sums[0] / sums[1]);
     if (flag) return set_error(KB_ERR_NONFINITE, "kb_residual: non-finite velocity found");
+    return KB_OK;
+}
+
+// Allocation-free variant of kb_mass: the partial sums live in the library's
+// fixed device array instead of a cudaMalloc'ed workspace.
+int kb_mass_static(const void *f, int lattice_q, size_t n_nodes, int dtype, double *out_host,
+                   void *stream) {
+    using namespace kb;
+    KB_REQUIRE(f && out_host, "kb_mass_static: null pointer");
+    KB_REQUIRE(lattice_q == 9 || lattice_q == 19, "kb_mass_static: lattice_q must be 9 or 19");
+    KB_REQUIRE(n_nodes > 0, "kb_mass_static: n_nodes must be positive");
+    KB_REQUIRE(dtype_bytes(dtype), "kb_mass_static: unknown dtype %d", dtype);
+    const size_t items = (size_t)lattice_q * n_nodes;
+    const size_t nb = (items + kStaticItemsPerBlock - 1) / kStaticItemsPerBlock;
+    if (nb > kStaticMaxPartials)
+        return set_error(KB_ERR_ARG,
+                         "kb_mass_static: %zu populations exceed the static scratch limit of %zu "
+                         "(%zu KiB); use kb_mass", items, kStaticMaxPartials * kStaticItemsPerBlock,
+                         kStaticScratchBytes / 1024);
+    char *ws = nullptr;
+    if (int e = static_scratch(&ws)) return e;
+    cudaStream_t s = as_stream(stream);
+    int *bad = (int *)ws;
+    double *out = (double *)(ws + 16);
+    red::KSum *part = (red::KSum *)(ws + kHead);
+    // the flag and the result must start at zero; the partials are all written
+    if (cudaMemsetAsync(ws, 0, kHead, s) != cudaSuccess)
+        return set_error(KB_ERR_CUDA, "kb_mass_static: memset failed");
+    const bool dev = dtype == KB_F32_DEV || dtype == KB_F16_DEV || dtype == KB_BF16_DEV;
+    const int blocks = (int)nb;
+    switch (dtype) {
+        case KB_F64: red::mass_pass1<double><<<blocks, red::RT, 0, s>>>((const double *)f, lattice_q, n_nodes, dev, part, bad); break;
+        case KB_F32:
+        case KB_F32_DEV: red::mass_pass1<float><<<blocks, red::RT, 0, s>>>((const float *)f, lattice_q, n_nodes, dev, part, bad); break;
+        case KB_F16_DEV: red::mass_pass1<__half><<<blocks, red::RT, 0, s>>>((const __half *)f, lattice_q, n_nodes, dev, part, bad); break;
+        default: red::mass_pass1<__nv_bfloat16><<<blocks, red::RT, 0, s>>>((const __nv_bfloat16 *)f, lattice_q, n_nodes, dev, part, bad); break;
+    }
+    red::pass2<1><<<1, red::RT, 0, s>>>(part, blocks, out);
+    if (int e = check_launch("kb_mass_static")) return e;
+    int flag = 0;
+    if (int e = finish("kb_mass_static", ws, 1, out_host, &flag, s)) return e;
+    if (flag) return set_error(KB_ERR_NONFINITE, "kb_mass_static: non-finite population found");
     return KB_OK;
 }
 
