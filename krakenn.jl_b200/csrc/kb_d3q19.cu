@@ -117,21 +117,26 @@ __global__ void __launch_bounds__(BX) macroscopic_k(T *__restrict__ rho, T *__re
 
 // Fused TRT step with the reference arithmetic (PullHalfwayBB_3D +
 // SolidInert_3D + Moments_3D + CollideTRTDirect_3D + WriteMoments_3D,
-// src/kernels/dsl/bricks_3d.jl:64-230, 476-483).
-template <typename T>
+// src/kernels/dsl/bricks_3d.jl:64-230, 476-483).  I: element-offset type.
+template <typename T, typename I>
 __global__ void __launch_bounds__(BX) fused_trt_k(T *__restrict__ fo, const T *__restrict__ fi,
                                                    T *__restrict__ rho, T *__restrict__ ux,
                                                    T *__restrict__ uy, T *__restrict__ uz,
                                                    const uint8_t *__restrict__ solid, Grid3 g, T sp,
                                                    T sm) {
-    NODE3
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i >= g.Nx) return;
+    const size_t c = (size_t)i + (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k);
+    const I P = (I)g.plane;
+    T *__restrict__ o0 = fo + c;
     T p[19];
-    pull19(fi, P, c, pull_geometry(g, i, j, k), p, Ident());
+    pull19_at(fi + c, P, pull_geometry<I>(g, i, j, k), p, Ident());
     if (solid && solid[c]) {
         T feq[19];
         feq_all(T(1), T(0), T(0), T(0), T(0), feq);
 #pragma unroll
-        for (int q = 0; q < 19; ++q) fo[c + q * P] = feq[q];
+        for (int q = 0; q < 19; ++q) o0[q * P] = feq[q];
         if (rho) { rho[c] = T(1); ux[c] = T(0); uy[c] = T(0); uz[c] = T(0); }
         return;
     }
@@ -142,12 +147,12 @@ __global__ void __launch_bounds__(BX) fused_trt_k(T *__restrict__ fo, const T *_
     const T a = (sp + sm) * T(0.5), b = (sp - sm) * T(0.5);
     const int pa[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16};
     const int pb[9] = {2, 4, 6, 10, 9, 14, 13, 18, 17};
-    fo[c] = p[0] - sp * (p[0] - feq[0]);
+    o0[0] = p[0] - sp * (p[0] - feq[0]);
 #pragma unroll
     for (int m = 0; m < 9; ++m) {
         const int x = pa[m], y = pb[m];
-        fo[c + x * P] = p[x] - a * (p[x] - feq[x]) - b * (p[y] - feq[y]);
-        fo[c + y * P] = p[y] - a * (p[y] - feq[y]) - b * (p[x] - feq[x]);
+        o0[x * P] = p[x] - a * (p[x] - feq[x]) - b * (p[y] - feq[y]);
+        o0[y * P] = p[y] - a * (p[y] - feq[y]) - b * (p[x] - feq[x]);
     }
     if (rho) { rho[c] = r; ux[c] = a_; uy[c] = b_; uz[c] = d_; }
 }
@@ -318,7 +323,7 @@ extern "C" {
 
 int kb_set_kernel_variant(int kernel, int variant) {
     KB_REQUIRE(kernel == 1, "kb_set_kernel_variant: unknown kernel id %d", kernel);
-    KB_REQUIRE(variant >= 0 && variant <= 2, "kb_set_kernel_variant: variant %d not in 0..2", variant);
+    KB_REQUIRE(variant >= 0 && variant <= 3, "kb_set_kernel_variant: variant %d not in 0..3", variant);
     g_trt3d_dev_variant = variant;
     return KB_OK;
 }
@@ -400,14 +405,25 @@ int kb_fused_trt_step_3d(void *f_out, const void *f_in, void *rho, void *ux, voi
     if (int e = kb_trt_rates(nu, Lambda, &sp, &sm)) return e;
     const Grid3 g = grid3(Nx, Ny, Nz, periodic);
     cudaStream_t s = kb::as_stream(stream);
+    const bool i32 = offsets_fit_int(g, 19);
     if (dtype == KB_F64) {
-        fused_trt_k<double><<<nodes_grid(Nx, Ny, Nz), BX, 0, s>>>(
-            (double *)f_out, (const double *)f_in, (double *)rho, (double *)ux, (double *)uy,
-            (double *)uz, is_solid, g, sp, sm);
+        if (i32)
+            fused_trt_k<double, int><<<nodes_grid(Nx, Ny, Nz), BX, 0, s>>>(
+                (double *)f_out, (const double *)f_in, (double *)rho, (double *)ux, (double *)uy,
+                (double *)uz, is_solid, g, sp, sm);
+        else
+            fused_trt_k<double, long long><<<nodes_grid(Nx, Ny, Nz), BX, 0, s>>>(
+                (double *)f_out, (const double *)f_in, (double *)rho, (double *)ux, (double *)uy,
+                (double *)uz, is_solid, g, sp, sm);
     } else if (dtype == KB_F32) {
-        fused_trt_k<float><<<nodes_grid(Nx, Ny, Nz), BX, 0, s>>>(
-            (float *)f_out, (const float *)f_in, (float *)rho, (float *)ux, (float *)uy,
-            (float *)uz, is_solid, g, (float)sp, (float)sm);
+        if (i32)
+            fused_trt_k<float, int><<<nodes_grid(Nx, Ny, Nz), BX, 0, s>>>(
+                (float *)f_out, (const float *)f_in, (float *)rho, (float *)ux, (float *)uy,
+                (float *)uz, is_solid, g, (float)sp, (float)sm);
+        else
+            fused_trt_k<float, long long><<<nodes_grid(Nx, Ny, Nz), BX, 0, s>>>(
+                (float *)f_out, (const float *)f_in, (float *)rho, (float *)ux, (float *)uy,
+                (float *)uz, is_solid, g, (float)sp, (float)sm);
     } else if (dtype == KB_F32_DEV || dtype == KB_F16_DEV || dtype == KB_BF16_DEV) {
         return launch_trt3d_dev(dtype, f_out, f_in, (float *)rho, (float *)ux, (float *)uy,
                                 (float *)uz, is_solid, g, (float)sp, (float)sm, s, g_trt3d_dev_variant);

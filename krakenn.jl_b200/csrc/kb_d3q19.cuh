@@ -24,55 +24,73 @@ struct Grid3 {
 // own opposite population.  Follows PullHalfwayBB_3D
 // (src/kernels/dsl/bricks_3d.jl:70-136) and stream_3d_kernel!
 // (src/kernels/collide_stream_3d.jl:5-42).
+// I is the element-offset type: int when every offset of the population
+// buffer fits in 31 bits (all addresses are then a per-thread base pointer
+// plus a 32-bit offset), long long otherwise.
+template <typename I>
 struct Pull3 {
-    long long dxm, dxp, dym, dyp, dzm, dzp;  // offset of source for c=+1 (m) / c=-1 (p)
+    I dxm, dxp, dym, dyp, dzm, dzp;  // offset of the source for c=+1 (m) / c=-1 (p)
     bool xm, xp, ym, yp, zm, zp;
 };
 
-__device__ __forceinline__ Pull3 pull_geometry(const Grid3 &g, int i, int j, int k) {
-    Pull3 s;
+template <typename I = long long>
+__device__ __forceinline__ Pull3<I> pull_geometry(const Grid3 &g, int i, int j, int k) {
+    Pull3<I> s;
     const bool px = g.per & 1, py = (g.per >> 1) & 1, pz = (g.per >> 2) & 1;
-    const long long sx = 1, sy = g.Nx, sz = (long long)g.Nx * g.Ny;
+    const I sx = 1, sy = (I)g.Nx, sz = (I)g.Nx * (I)g.Ny;
     s.xm = px || i > 0;
     s.xp = px || i < g.Nx - 1;
     s.ym = py || j > 0;
     s.yp = py || j < g.Ny - 1;
     s.zm = pz || k > 0;
     s.zp = pz || k < g.Nz - 1;
-    s.dxm = (i > 0 ? -1 : (long long)(g.Nx - 1)) * sx;
-    s.dxp = (i < g.Nx - 1 ? 1 : -(long long)(g.Nx - 1)) * sx;
-    s.dym = (j > 0 ? -1 : (long long)(g.Ny - 1)) * sy;
-    s.dyp = (j < g.Ny - 1 ? 1 : -(long long)(g.Ny - 1)) * sy;
-    s.dzm = (k > 0 ? -1 : (long long)(g.Nz - 1)) * sz;
-    s.dzp = (k < g.Nz - 1 ? 1 : -(long long)(g.Nz - 1)) * sz;
+    s.dxm = (i > 0 ? (I)-1 : (I)(g.Nx - 1)) * sx;
+    s.dxp = (i < g.Nx - 1 ? (I)1 : -(I)(g.Nx - 1)) * sx;
+    s.dym = (j > 0 ? (I)-1 : (I)(g.Ny - 1)) * sy;
+    s.dyp = (j < g.Ny - 1 ? (I)1 : -(I)(g.Ny - 1)) * sy;
+    s.dzm = (k > 0 ? (I)-1 : (I)(g.Nz - 1)) * sz;
+    s.dzp = (k < g.Nz - 1 ? (I)1 : -(I)(g.Nz - 1)) * sz;
     return s;
 }
 
-// Pull all 19 populations of node c into p[] (any element type; the
-// conversion Load(x) maps a stored value to the working value).
-template <typename R, typename V, typename Load>
-__device__ __forceinline__ void pull19(const R *__restrict__ f, size_t P, size_t c, const Pull3 &s,
-                                       V *p, Load ld) {
-    const R *f0 = f + c;
+// Pull all 19 populations of the node at f0 (= f + node index) into p[]
+// (any element type; Load(x) maps a stored value to the working value).
+// P is the plane size in elements.
+template <typename R, typename V, typename Load, typename I>
+__device__ __forceinline__ void pull19_at(const R *__restrict__ f0, I P, const Pull3<I> &s, V *p,
+                                          Load ld) {
     p[0] = ld(f0[0]);
-    p[1] = s.xm ? ld(f0[s.dxm + 1 * P]) : ld(f0[2 * P]);
-    p[2] = s.xp ? ld(f0[s.dxp + 2 * P]) : ld(f0[1 * P]);
-    p[3] = s.ym ? ld(f0[s.dym + 3 * P]) : ld(f0[4 * P]);
-    p[4] = s.yp ? ld(f0[s.dyp + 4 * P]) : ld(f0[3 * P]);
-    p[5] = s.zm ? ld(f0[s.dzm + 5 * P]) : ld(f0[6 * P]);
-    p[6] = s.zp ? ld(f0[s.dzp + 6 * P]) : ld(f0[5 * P]);
-    p[7] = (s.xm && s.ym) ? ld(f0[s.dxm + s.dym + 7 * P]) : ld(f0[10 * P]);
-    p[8] = (s.xp && s.ym) ? ld(f0[s.dxp + s.dym + 8 * P]) : ld(f0[9 * P]);
-    p[9] = (s.xm && s.yp) ? ld(f0[s.dxm + s.dyp + 9 * P]) : ld(f0[8 * P]);
-    p[10] = (s.xp && s.yp) ? ld(f0[s.dxp + s.dyp + 10 * P]) : ld(f0[7 * P]);
-    p[11] = (s.xm && s.zm) ? ld(f0[s.dxm + s.dzm + 11 * P]) : ld(f0[14 * P]);
-    p[12] = (s.xp && s.zm) ? ld(f0[s.dxp + s.dzm + 12 * P]) : ld(f0[13 * P]);
-    p[13] = (s.xm && s.zp) ? ld(f0[s.dxm + s.dzp + 13 * P]) : ld(f0[12 * P]);
-    p[14] = (s.xp && s.zp) ? ld(f0[s.dxp + s.dzp + 14 * P]) : ld(f0[11 * P]);
-    p[15] = (s.ym && s.zm) ? ld(f0[s.dym + s.dzm + 15 * P]) : ld(f0[18 * P]);
-    p[16] = (s.yp && s.zm) ? ld(f0[s.dyp + s.dzm + 16 * P]) : ld(f0[17 * P]);
-    p[17] = (s.ym && s.zp) ? ld(f0[s.dym + s.dzp + 17 * P]) : ld(f0[16 * P]);
-    p[18] = (s.yp && s.zp) ? ld(f0[s.dyp + s.dzp + 18 * P]) : ld(f0[15 * P]);
+    p[1] = ld(f0[s.xm ? s.dxm + 1 * P : 2 * P]);
+    p[2] = ld(f0[s.xp ? s.dxp + 2 * P : 1 * P]);
+    p[3] = ld(f0[s.ym ? s.dym + 3 * P : 4 * P]);
+    p[4] = ld(f0[s.yp ? s.dyp + 4 * P : 3 * P]);
+    p[5] = ld(f0[s.zm ? s.dzm + 5 * P : 6 * P]);
+    p[6] = ld(f0[s.zp ? s.dzp + 6 * P : 5 * P]);
+    p[7] = ld(f0[(s.xm && s.ym) ? s.dxm + s.dym + 7 * P : 10 * P]);
+    p[8] = ld(f0[(s.xp && s.ym) ? s.dxp + s.dym + 8 * P : 9 * P]);
+    p[9] = ld(f0[(s.xm && s.yp) ? s.dxm + s.dyp + 9 * P : 8 * P]);
+    p[10] = ld(f0[(s.xp && s.yp) ? s.dxp + s.dyp + 10 * P : 7 * P]);
+    p[11] = ld(f0[(s.xm && s.zm) ? s.dxm + s.dzm + 11 * P : 14 * P]);
+    p[12] = ld(f0[(s.xp && s.zm) ? s.dxp + s.dzm + 12 * P : 13 * P]);
+    p[13] = ld(f0[(s.xm && s.zp) ? s.dxm + s.dzp + 13 * P : 12 * P]);
+    p[14] = ld(f0[(s.xp && s.zp) ? s.dxp + s.dzp + 14 * P : 11 * P]);
+    p[15] = ld(f0[(s.ym && s.zm) ? s.dym + s.dzm + 15 * P : 18 * P]);
+    p[16] = ld(f0[(s.yp && s.zm) ? s.dyp + s.dzm + 16 * P : 17 * P]);
+    p[17] = ld(f0[(s.ym && s.zp) ? s.dym + s.dzp + 17 * P : 16 * P]);
+    p[18] = ld(f0[(s.yp && s.zp) ? s.dyp + s.dzp + 18 * P : 15 * P]);
+}
+
+// Pull with 64-bit offsets from the buffer base f and node index c.
+template <typename R, typename V, typename Load>
+__device__ __forceinline__ void pull19(const R *__restrict__ f, size_t P, size_t c,
+                                       const Pull3<long long> &s, V *p, Load ld) {
+    pull19_at(f + c, (long long)P, s, p, ld);
+}
+
+// True when every element offset of a Q-population buffer on grid g fits
+// in a signed 32-bit int.
+inline bool offsets_fit_int(const Grid3 &g, int Q) {
+    return (double)g.plane * (double)(Q + 1) < 2147483647.0;
 }
 
 inline dim3 nodes_grid(int Nx, int Ny, int Nz) { return dim3((Nx + BX - 1) / BX, Ny, Nz); }

@@ -31,7 +31,83 @@ struct DevLoad {
 __device__ constexpr int kPairQ[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16};
 __device__ constexpr int kPairQb[9] = {2, 4, 6, 10, 9, 14, 13, 18, 17};
 
-template <typename R, bool MOM, bool SOLID>
+// Scalar / packed-pair arithmetic used by the TRT collision below.
+__device__ __forceinline__ float vadd(float a, float b) { return a + b; }
+__device__ __forceinline__ float vsub(float a, float b) { return a - b; }
+__device__ __forceinline__ float vmul(float a, float b) { return a * b; }
+__device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ float vneg(float a) { return -a; }
+__device__ __forceinline__ float vsplat(float a, float) { return a; }
+__device__ __forceinline__ float vrcp(float a) { return __frcp_rn(a); }
+__device__ __forceinline__ float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 vsub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 vmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 vneg(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 vsplat(float a, float2) { return make_float2(a, a); }
+__device__ __forceinline__ float2 vrcp(float2 a) { return make_float2(__frcp_rn(a.x), __frcp_rn(a.y)); }
+
+// TRT collision of D3Q19 deviations d[19] -> o[19] (V = float for one node,
+// float2 for two).  With s_m = d_q + d_qb and t_m = d_q - d_qb of the nine
+// opposite pairs (q, qb), c_qb = -c_q:
+//   drho = d_0 + sum s_m,  j = sum c_q t_m,  rho = 1 + drho,  u = j / rho
+//   even mode: n+ = s_m/2 - w (drho + rho (4.5 cu^2 - 1.5 u^2))
+//   odd mode:  n- = t_m/2 - 3 w rho cu
+//   o_q = d_q - s+ n+ - s- n-,   o_qb = d_qb - s+ n+ + s- n-
+// which is CollideTRTDirect_3D (src/kernels/dsl/bricks_3d.jl:179-229)
+// written on deviations.  Regrouped on s and t only (d_q = (s + t)/2):
+//   X = (1 - s+)/2 s_m + s+ w (base + 4.5 rho cu^2),  base = drho - 1.5 rho u^2
+//   Y = (1 - s-)/2 t_m + 3 s- w rho cu
+//   o_q = X + Y,  o_qb = X - Y
+template <typename V>
+__device__ __forceinline__ void trt_dev_collide(const V *d, V *o, V &rho, V &ux, V &uy, V &uz,
+                                                float sp, float sm) {
+    const V z = vsplat(0.f, d[0]);
+    V sv[9], tv[9];
+#pragma unroll
+    for (int m = 0; m < 9; ++m) {
+        sv[m] = vadd(d[kPairQ[m]], d[kPairQb[m]]);
+        tv[m] = vsub(d[kPairQ[m]], d[kPairQb[m]]);
+    }
+    // pair order: (1,2) x, (3,4) y, (5,6) z, (7,10) +x+y, (8,9) -x+y,
+    // (11,14) +x+z, (12,13) -x+z, (15,18) +y+z, (16,17) -y+z
+    const V drho = vadd(vadd(vadd(d[0], sv[0]), vadd(sv[1], sv[2])),
+                        vadd(vadd(vadd(sv[3], sv[4]), vadd(sv[5], sv[6])), vadd(sv[7], sv[8])));
+    const V jx = vadd(vsub(vadd(tv[0], tv[3]), tv[4]), vsub(tv[5], tv[6]));
+    const V jy = vadd(vadd(vadd(tv[1], tv[3]), tv[4]), vsub(tv[7], tv[8]));
+    const V jz = vadd(vadd(vadd(tv[2], tv[5]), tv[6]), vadd(tv[7], tv[8]));
+    rho = vadd(vsplat(1.f, z), drho);
+    const V inv = vrcp(rho);
+    ux = vmul(jx, inv);
+    uy = vmul(jy, inv);
+    uz = vmul(jz, inv);
+    const V usq15 = vmul(vsplat(1.5f, z), vfma(ux, ux, vfma(uy, uy, vmul(uz, uz))));
+    const V base = vsub(drho, vmul(rho, usq15));
+    // rest population (even mode only): o_0 = (1 - s+) d_0 + s+ w_0 base
+    o[0] = vfma(vsplat(1.0f - sp, z), d[0], vmul(vsplat(sp * float(1.0 / 3.0), z), base));
+    const V ha = vsplat(0.5f * (1.0f - sp), z), hb = vsplat(0.5f * (1.0f - sm), z);
+#pragma unroll
+    for (int cls = 0; cls < 2; ++cls) {
+        const float w = cls == 0 ? float(1.0 / 18.0) : float(1.0 / 36.0);
+        const V A = vmul(vsplat(sp * w, z), base);          // s+ w base
+        const V B = vmul(vsplat(4.5f * sp * w, z), rho);    // 4.5 s+ w rho
+        const V C = vmul(vsplat(3.0f * sm * w, z), rho);    // 3 s- w rho
+#pragma unroll
+        for (int m = (cls == 0 ? 0 : 3); m < (cls == 0 ? 3 : 9); ++m) {
+            const int q = kPairQ[m], qb = kPairQb[m];
+            V cu = z;
+            if (cx19(q) == 1) cu = vadd(cu, ux); else if (cx19(q) == -1) cu = vsub(cu, ux);
+            if (cy19(q) == 1) cu = vadd(cu, uy); else if (cy19(q) == -1) cu = vsub(cu, uy);
+            if (cz19(q) == 1) cu = vadd(cu, uz); else if (cz19(q) == -1) cu = vsub(cu, uz);
+            const V X = vfma(ha, sv[m], vfma(vmul(B, cu), cu, A));
+            const V Y = vfma(hb, tv[m], vmul(C, cu));
+            o[q] = vadd(X, Y);
+            o[qb] = vsub(X, Y);
+        }
+    }
+}
+
+template <typename R, bool MOM, bool SOLID, typename I>
 __global__ void __launch_bounds__(BX) trt_dev_k(R *__restrict__ fo, const R *__restrict__ fi,
                                                  float *__restrict__ rho_o, float *__restrict__ ux_o,
                                                  float *__restrict__ uy_o, float *__restrict__ uz_o,
@@ -41,46 +117,21 @@ __global__ void __launch_bounds__(BX) trt_dev_k(R *__restrict__ fo, const R *__r
     const int j = blockIdx.y, k = blockIdx.z;
     if (i >= g.Nx) return;
     const size_t c = (size_t)i + (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k);
-    const size_t P = g.plane;
+    const I P = (I)g.plane;
+    R *__restrict__ o0 = fo + c;
     if (SOLID && solid[c]) {
 #pragma unroll
-        for (int q = 0; q < 19; ++q) fo[c + q * P] = Dev<R>::st(0.0f);
+        for (int q = 0; q < 19; ++q) o0[q * P] = Dev<R>::st(0.0f);
         if (MOM) { rho_o[c] = 1.0f; ux_o[c] = 0.0f; uy_o[c] = 0.0f; uz_o[c] = 0.0f; }
         return;
     }
     float d[19];
-    pull19(fi, P, c, pull_geometry(g, i, j, k), d, DevLoad<R>());
+    pull19_at(fi + c, P, pull_geometry<I>(g, i, j, k), d, DevLoad<R>());
 
-    float drho = 0.f;
+    float o[19], rho, ux, uy, uz;
+    trt_dev_collide(d, o, rho, ux, uy, uz, sp, sm);
 #pragma unroll
-    for (int q = 0; q < 19; ++q) drho += d[q];
-    const float jx = (d[1] - d[2]) + (d[7] - d[8]) + (d[9] - d[10]) + (d[11] - d[12]) + (d[13] - d[14]);
-    const float jy = (d[3] - d[4]) + (d[7] + d[8]) - (d[9] + d[10]) + (d[15] - d[16]) + (d[17] - d[18]);
-    const float jz = (d[5] - d[6]) + (d[11] + d[12]) - (d[13] + d[14]) + (d[15] + d[16]) - (d[17] + d[18]);
-    const float rho = 1.0f + drho;
-    const float inv = 1.0f / rho;
-    const float ux = jx * inv, uy = jy * inv, uz = jz * inv;
-    const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
-
-    // rest population: only the even mode
-    const float w0 = float(1.0 / 3.0);
-    const float deq0 = w0 * (drho - rho * usq15);
-    fo[c] = Dev<R>::st(d[0] - sp * (d[0] - deq0));
-
-#pragma unroll
-    for (int m = 0; m < 9; ++m) {
-        const int q = kPairQ[m], qb = kPairQb[m];
-        const float w = m < 3 ? float(1.0 / 18.0) : float(1.0 / 36.0);
-        const float cu = float(cx19(q)) * ux + float(cy19(q)) * uy + float(cz19(q)) * uz;
-        const float deq_p = w * (drho + rho * (4.5f * cu * cu - usq15));
-        const float deq_m = w * rho * 3.0f * cu;
-        const float dq = d[q], dqb = d[qb];
-        const float np = 0.5f * (dq + dqb) - deq_p;
-        const float nm = 0.5f * (dq - dqb) - deq_m;
-        const float even = sp * np, odd = sm * nm;
-        fo[c + q * P] = Dev<R>::st(dq - even - odd);
-        fo[c + qb * P] = Dev<R>::st(dqb - even + odd);
-    }
+    for (int q = 0; q < 19; ++q) o0[q * P] = Dev<R>::st(o[q]);
     if (MOM) { rho_o[c] = rho; ux_o[c] = ux; uy_o[c] = uy; uz_o[c] = uz; }
 }
 
@@ -98,8 +149,14 @@ __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
-template <typename R, bool MOM, bool SOLID>
-__global__ void __launch_bounds__(BX) trt_dev_x2_k(R *__restrict__ fo, const R *__restrict__ fi,
+// Resident blocks per SM requested from the compiler for the pair kernels
+// (caps their registers); set by the build.
+#ifndef KB_PAIR_MIN_BLOCKS
+#define KB_PAIR_MIN_BLOCKS 6
+#endif
+
+template <typename R, bool MOM, bool SOLID, typename I>
+__global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_x2_k(R *__restrict__ fo, const R *__restrict__ fi,
                                                     float *__restrict__ rho_o, float *__restrict__ ux_o,
                                                     float *__restrict__ uy_o, float *__restrict__ uz_o,
                                                     const uint8_t *__restrict__ solid, Grid3 g,
@@ -110,54 +167,24 @@ __global__ void __launch_bounds__(BX) trt_dev_x2_k(R *__restrict__ fo, const R *
     if (iA >= g.Nx) return;
     const bool vB = iB < g.Nx;
     const int j = blockIdx.y, k = blockIdx.z;
-    const size_t P = g.plane;
+    const I P = (I)g.plane;
     const size_t row = (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k);
     const size_t cA = row + iA, cB = row + (vB ? iB : iA);
     float a[19], b[19];
-    pull19(fi, P, cA, pull_geometry(g, iA, j, k), a, DevLoad<R>());
-    pull19(fi, P, cB, pull_geometry(g, vB ? iB : iA, j, k), b, DevLoad<R>());
+    pull19_at(fi + cA, P, pull_geometry<I>(g, iA, j, k), a, DevLoad<R>());
+    pull19_at(fi + cB, P, pull_geometry<I>(g, vB ? iB : iA, j, k), b, DevLoad<R>());
     float2 d[19];
 #pragma unroll
     for (int q = 0; q < 19; ++q) d[q] = make_float2(a[q], b[q]);
 
-    float2 drho = d[0];
-#pragma unroll
-    for (int q = 1; q < 19; ++q) drho = add2(drho, d[q]);
-    const float2 jx = add2(add2(add2(sub2(d[1], d[2]), sub2(d[7], d[8])), add2(sub2(d[9], d[10]), sub2(d[11], d[12]))), sub2(d[13], d[14]));
-    const float2 jy = add2(add2(add2(sub2(d[3], d[4]), add2(d[7], d[8])), sub2(add2(d[15], d[17]), add2(d[9], d[10]))), sub2(sub2(f2(0.f), d[16]), d[18]));
-    const float2 jz = add2(add2(add2(sub2(d[5], d[6]), add2(d[11], d[12])), sub2(add2(d[15], d[16]), add2(d[13], d[14]))), sub2(sub2(f2(0.f), d[17]), d[18]));
-    const float2 rho = add2(f2(1.0f), drho);
-    const float2 inv = make_float2(__frcp_rn(rho.x), __frcp_rn(rho.y));
-    const float2 ux = mul2(jx, inv), uy = mul2(jy, inv), uz = mul2(jz, inv);
-    const float2 usq15 = mul2(f2(1.5f), fma2(ux, ux, fma2(uy, uy, mul2(uz, uz))));
-    const float2 vsp = f2(sp), vsm = f2(sm);
+    float2 o[19], rho, ux, uy, uz;
+    trt_dev_collide(d, o, rho, ux, uy, uz, sp, sm);
     uchar2 sm2 = make_uchar2(0, 0);
     if (SOLID) sm2 = make_uchar2(solid[cA], vB ? solid[cB] : 0);
-    float2 o[19];
-    {
-        const float2 deq0 = mul2(f2(float(1.0 / 3.0)), sub2(drho, mul2(rho, usq15)));
-        o[0] = sub2(d[0], mul2(vsp, sub2(d[0], deq0)));
-    }
-#pragma unroll
-    for (int m = 0; m < 9; ++m) {
-        const int q = kPairQ[m], qb = kPairQb[m];
-        const float w = m < 3 ? float(1.0 / 18.0) : float(1.0 / 36.0);
-        float2 cu = f2(0.f);
-        if (cx19(q) == 1) cu = add2(cu, ux); else if (cx19(q) == -1) cu = sub2(cu, ux);
-        if (cy19(q) == 1) cu = add2(cu, uy); else if (cy19(q) == -1) cu = sub2(cu, uy);
-        if (cz19(q) == 1) cu = add2(cu, uz); else if (cz19(q) == -1) cu = sub2(cu, uz);
-        const float2 deq_p = mul2(f2(w), fma2(rho, fma2(mul2(f2(4.5f), cu), cu, make_float2(-usq15.x, -usq15.y)), drho));
-        const float2 deq_m = mul2(mul2(f2(3.0f * w), rho), cu);
-        const float2 np = fma2(f2(0.5f), add2(d[q], d[qb]), make_float2(-deq_p.x, -deq_p.y));
-        const float2 nm = fma2(f2(0.5f), sub2(d[q], d[qb]), make_float2(-deq_m.x, -deq_m.y));
-        const float2 ev = mul2(vsp, np), od = mul2(vsm, nm);
-        o[q] = sub2(sub2(d[q], ev), od);
-        o[qb] = add2(sub2(d[qb], ev), od);
-    }
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
-        fo[cA + q * P] = Dev<R>::st(SOLID && sm2.x ? 0.f : o[q].x);
-        if (vB) fo[cB + q * P] = Dev<R>::st(SOLID && sm2.y ? 0.f : o[q].y);
+        fo[cA + (size_t)(q * P)] = Dev<R>::st(SOLID && sm2.x ? 0.f : o[q].x);
+        if (vB) fo[cB + (size_t)(q * P)] = Dev<R>::st(SOLID && sm2.y ? 0.f : o[q].y);
     }
     if (MOM) {
         const bool sA = SOLID && sm2.x, sB = SOLID && sm2.y;
@@ -170,42 +197,198 @@ __global__ void __launch_bounds__(BX) trt_dev_x2_k(R *__restrict__ fo, const R *
     }
 }
 
-template <typename R>
-static void launch_r(void *f_out, const void *f_in, float *rho, float *ux, float *uy, float *uz,
-                     const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s,
-                     bool pairs) {
+// ---------------------------------------------------------------------------
+// Vector pairs (even Nx): lane t owns the adjacent nodes x0 = 2t, x0 + 1 of
+// its warp's 64-node run, so each population of the pair is ONE aligned
+// 2-element access (half2 / bfloat162 / float2) for loads and stores.  The
+// x-shifted pulls take the missing element from the neighbouring lane by
+// warp shuffle; lane 0 (c_x = +1) and the last lane of the run (c_x = -1)
+// load that element directly, which also covers the periodic wrap and the
+// half-way bounce-back at x walls.  All loads are issued before any shuffle
+// so each thread keeps 19 vector requests in flight.
+template <typename R> struct Vec2;
+template <> struct Vec2<float> {
+    static __device__ __forceinline__ float2 ld(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+    static __device__ __forceinline__ void st(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
+};
+template <> struct Vec2<__half> {
+    static __device__ __forceinline__ float2 ld(const __half *p) {
+        return __half22float2(*reinterpret_cast<const __half2 *>(p));
+    }
+    static __device__ __forceinline__ void st(__half *p, float2 v) {
+        *reinterpret_cast<__half2 *>(p) = __floats2half2_rn(v.x, v.y);
+    }
+};
+template <> struct Vec2<__nv_bfloat16> {
+    static __device__ __forceinline__ float2 ld(const __nv_bfloat16 *p) {
+        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(p));
+    }
+    static __device__ __forceinline__ void st(__nv_bfloat16 *p, float2 v) {
+        *reinterpret_cast<__nv_bfloat162 *>(p) = __floats2bfloat162_rn(v.x, v.y);
+    }
+};
+
+template <typename R, bool MOM, bool SOLID, typename I>
+__global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_v2_k(R *__restrict__ fo, const R *__restrict__ fi,
+                                                    float *__restrict__ rho_o, float *__restrict__ ux_o,
+                                                    float *__restrict__ uy_o, float *__restrict__ uz_o,
+                                                    const uint8_t *__restrict__ solid, Grid3 g,
+                                                    float sp, float sm) {
+    constexpr int CX[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+    constexpr int CY[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
+    constexpr int CZ[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
+    constexpr int OP[19] = {0, 2, 1, 4, 3, 6, 5, 10, 9, 8, 7, 14, 13, 12, 11, 18, 17, 16, 15};
+    const int lane = threadIdx.x & 31;
+    const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int Nx = g.Nx;
+    const bool valid = x0 < Nx;
+    const bool last = x0 + 2 >= Nx;  // no valid neighbour lane to the right
+    const int j = blockIdx.y, k = blockIdx.z;
+    const I P = (I)g.plane;
+    const bool px = g.per & 1, py = (g.per >> 1) & 1, pz = (g.per >> 2) & 1;
+    const I sy = (I)Nx, sz = (I)Nx * (I)g.Ny;
+    const bool ym = py || j > 0, yp = py || j < g.Ny - 1;
+    const bool zm = pz || k > 0, zp = pz || k < g.Nz - 1;
+    const I oym = (j > 0 ? (I)-1 : (I)(g.Ny - 1)) * sy;
+    const I oyp = (j < g.Ny - 1 ? (I)1 : -(I)(g.Ny - 1)) * sy;
+    const I ozm = (k > 0 ? (I)-1 : (I)(g.Nz - 1)) * sz;
+    const I ozp = (k < g.Nz - 1 ? (I)1 : -(I)(g.Nz - 1)) * sz;
+    const size_t row = (size_t)Nx * ((size_t)j + (size_t)g.Ny * k);
+    const R *__restrict__ f0 = fi + row;  // row x = 0 of population 0, this (j, k)
+    const int xv = valid ? x0 : 0;        // invalid lanes read a harmless in-row pair
+
+    // 1. issue every load: the aligned pair and, for x-shifted populations,
+    //    the one edge element this lane may need
+    float2 a[19];
+    float e[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        const bool ok = (CY[q] == 1 ? ym : CY[q] == -1 ? yp : true) &&
+                        (CZ[q] == 1 ? zm : CZ[q] == -1 ? zp : true);
+        const I srow = (CY[q] == 1 ? oym : CY[q] == -1 ? oyp : (I)0) +
+                       (CZ[q] == 1 ? ozm : CZ[q] == -1 ? ozp : (I)0) + (I)q * P;
+        const I orow = (I)OP[q] * P;  // own row, opposite population
+        a[q] = Vec2<R>::ld(f0 + (ok ? srow : orow) + xv);
+        e[q] = 0.f;
+        if (CX[q] == 1) {
+            // element for node x0: x0-1 in the source row, or wrap, or bounce
+            const bool need = ok && (lane == 0);
+            const I off = x0 > 0 ? srow + (I)(xv - 1) : (px ? srow + (I)(Nx - 1) : orow + (I)xv);
+            if (need && valid) e[q] = Dev<R>::ld(f0[off]);
+        } else if (CX[q] == -1) {
+            // element for node x0+1: x0+2 in the source row, or wrap, or bounce
+            const bool need = ok && (lane == 31 || last);
+            const I off = !last ? srow + (I)(xv + 2) : (px ? srow : orow + (I)(xv + 1));
+            if (need && valid) e[q] = Dev<R>::ld(f0[off]);
+        }
+    }
+    // 2. assemble the pulled pair of every population
+    float2 d[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        const bool ok = (CY[q] == 1 ? ym : CY[q] == -1 ? yp : true) &&
+                        (CZ[q] == 1 ? zm : CZ[q] == -1 ? zp : true);
+        if (CX[q] == 1) {
+            const float up = __shfl_up_sync(0xffffffffu, a[q].y, 1);
+            d[q] = ok ? make_float2(lane == 0 ? e[q] : up, a[q].x) : a[q];
+        } else if (CX[q] == -1) {
+            const float dn = __shfl_down_sync(0xffffffffu, a[q].x, 1);
+            d[q] = ok ? make_float2(a[q].y, (lane == 31 || last) ? e[q] : dn) : a[q];
+        } else {
+            d[q] = a[q];
+        }
+    }
+    if (!valid) return;
+
+    float2 o[19], rho, ux, uy, uz;
+    trt_dev_collide(d, o, rho, ux, uy, uz, sp, sm);
+    const size_t oc = row + x0;
+    uchar2 sm2 = make_uchar2(0, 0);
+    if (SOLID) sm2 = *reinterpret_cast<const uchar2 *>(solid + oc);
+    R *__restrict__ o0 = fo + oc;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        float2 v = o[q];
+        if (SOLID) { if (sm2.x) v.x = 0.f; if (sm2.y) v.y = 0.f; }
+        Vec2<R>::st(o0 + (size_t)(q * P), v);
+    }
+    if (MOM) {
+        float2 r = rho, aa = ux, bb = uy, cc = uz;
+        if (SOLID) {
+            if (sm2.x) { r.x = 1.f; aa.x = bb.x = cc.x = 0.f; }
+            if (sm2.y) { r.y = 1.f; aa.y = bb.y = cc.y = 0.f; }
+        }
+        *reinterpret_cast<float2 *>(rho_o + oc) = r;
+        *reinterpret_cast<float2 *>(ux_o + oc) = aa;
+        *reinterpret_cast<float2 *>(uy_o + oc) = bb;
+        *reinterpret_cast<float2 *>(uz_o + oc) = cc;
+    }
+}
+
+template <typename R, typename I>
+static void launch_ri(void *f_out, const void *f_in, float *rho, float *ux, float *uy, float *uz,
+                      const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s,
+                      int kind) {
     R *fo = (R *)f_out;
     const R *fi = (const R *)f_in;
-    if (pairs) {
+    if (kind == 3) {
+        const dim3 grid((g.Nx / 2 + BX - 1) / BX, g.Ny, g.Nz);
+        if (rho) {
+            if (solid) trt_dev_v2_k<R, true, true, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            else trt_dev_v2_k<R, true, false, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+        } else {
+            if (solid) trt_dev_v2_k<R, false, true, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            else trt_dev_v2_k<R, false, false, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+        }
+        return;
+    }
+    if (kind == 2) {
         const int threads_x = (g.Nx + 63) / 64 * 32;  // one warp per 64 nodes of a row
         const dim3 grid((threads_x + BX - 1) / BX, g.Ny, g.Nz);
         if (rho) {
-            if (solid) trt_dev_x2_k<R, true, true><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
-            else trt_dev_x2_k<R, true, false><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            if (solid) trt_dev_x2_k<R, true, true, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            else trt_dev_x2_k<R, true, false, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
         } else {
-            if (solid) trt_dev_x2_k<R, false, true><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
-            else trt_dev_x2_k<R, false, false><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            if (solid) trt_dev_x2_k<R, false, true, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            else trt_dev_x2_k<R, false, false, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
         }
         return;
     }
     const dim3 grid = nodes_grid(g.Nx, g.Ny, g.Nz);
     if (rho) {
-        if (solid) trt_dev_k<R, true, true><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
-        else trt_dev_k<R, true, false><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+        if (solid) trt_dev_k<R, true, true, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+        else trt_dev_k<R, true, false, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
     } else {
-        if (solid) trt_dev_k<R, false, true><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
-        else trt_dev_k<R, false, false><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+        if (solid) trt_dev_k<R, false, true, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+        else trt_dev_k<R, false, false, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
     }
+}
+
+template <typename R>
+static void launch_r(void *f_out, const void *f_in, float *rho, float *ux, float *uy, float *uz,
+                     const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s,
+                     int kind) {
+    if (offsets_fit_int(g, 19))
+        launch_ri<R, int>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, kind);
+    else
+        launch_ri<R, long long>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, kind);
 }
 
 int launch_trt3d_dev(int dtype, void *f_out, const void *f_in, float *rho, float *ux, float *uy,
                      float *uz, const uint8_t *solid, const Grid3 &g, float sp, float sm,
                      cudaStream_t s, int variant) {
-    // variant: 0 automatic (two nodes per thread for 16-bit storages when a
-    // row holds at least 64 nodes), 1 one node per thread, 2 two nodes per
-    // thread
-    const bool pairs = variant == 2 ||
-                       (variant == 0 && dtype != KB_F32_DEV && g.Nx >= 64);
+    // variant: 0 automatic, 1 one node per thread, 2 nodes x and x+32 per
+    // thread, 3 adjacent node pairs with vector accesses (even Nx only).
+    if (variant == 3 && g.Nx % 2 != 0)
+        return set_error(KB_ERR_ARG, "kb_fused_trt_step_3d: the vector-pair kernel needs an even Nx");
+    // automatic choice, from measurements at 256^3 on B200: FP32 deviations
+    // run fastest as vector pairs, FP16/BF16 as x / x+32 pairs
+    int kind = variant;
+    if (variant == 0) {
+        if (dtype == KB_F32_DEV) kind = g.Nx % 2 == 0 ? 3 : 1;
+        else kind = g.Nx >= 64 ? 2 : 1;
+    }
+    const int pairs = kind;
     switch (dtype) {
         case KB_F32_DEV: launch_r<float>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
         case KB_F16_DEV: launch_r<__half>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;

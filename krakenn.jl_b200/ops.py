@@ -415,7 +415,8 @@ def compute_macroscopic_3d_(rho, ux, uy, uz, f):
 
 
 def set_trt3d_variant(variant: int):
-    """0 automatic, 1 one node per thread, 2 two nodes per thread (even Nx)."""
+    """0 automatic, 1 one node per thread, 2 nodes x and x+32 per thread,
+    3 adjacent node pairs with vector accesses (even Nx)."""
     call("kb_set_kernel_variant", 1, int(variant))
 
 

@@ -194,11 +194,12 @@ def test_convert_roundtrip(cuda, pkg):
                                        ((2, 4, 4), (1, 0, 1)), ((130, 2, 3), (1, 1, 0))])
 @pytest.mark.parametrize("with_mask", [False, True])
 def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask):
-    """The two-nodes-per-thread kernel (nodes x and x+32 of a warp, packed
-    FP32x2 collision) and the one-node kernel compute the same update: on
-    ragged grids, walls or wraps on every axis and solid nodes, both stay
-    within the storage rounding of the FP64 oracle (max abs error of f
-    relative to w_q) and of each other."""
+    """The one-node kernel and the two-node kernels (nodes x and x+32 of a
+    warp; adjacent node pairs with vector accesses and shuffled x
+    neighbours; both with the packed FP32x2 collision) compute the same
+    update: on ragged grids, walls or wraps on every axis and solid nodes,
+    all stay within the storage rounding of the FP64 oracle (max abs error
+    of f relative to w_q) and of each other."""
     Nx, Ny, Nz = shape
     rng = np.random.default_rng(7)
     f = W19[:, None, None, None] * (1 + 0.05 * rng.standard_normal((19, Nz, Ny, Nx)))
@@ -212,7 +213,8 @@ def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask):
     pkg.convert_populations(src, _g(f), dst_deviation=True)
     outs = []
     try:
-        for variant in (1, 2):
+        variants = (1, 2, 3) if Nx % 2 == 0 else (1, 2)
+        for variant in variants:
             pkg.set_trt3d_variant(variant)
             fo = torch.empty_like(src)
             mt = [torch.empty((Nz, Ny, Nx), dtype=torch.float32, device=cuda) for _ in range(4)]
@@ -228,4 +230,16 @@ def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask):
             outs.append(got)
     finally:
         pkg.set_trt3d_variant(0)
-    assert np.max(np.abs(outs[0] - outs[1]) / W19[:, None, None, None]) < 2 * tol
+    for o in outs[1:]:
+        assert np.max(np.abs(outs[0] - o) / W19[:, None, None, None]) < 2 * tol
+
+
+def test_vector_pair_kernel_needs_even_nx(cuda, pkg):
+    pkg.set_trt3d_variant(3)
+    try:
+        f = torch.zeros((19, 4, 4, 5), dtype=torch.float16, device=cuda)
+        with pytest.raises(pkg.KrakenArgumentError):
+            pkg.fused_trt_step_3d_(torch.empty_like(f), f, None, None, None, None, None, 5, 4, 4,
+                                   0.02, 0.25, periodic=(1, 1, 1))
+    finally:
+        pkg.set_trt3d_variant(0)
