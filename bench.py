@@ -340,7 +340,8 @@ def run_gpu(args):
                               f"{dt:.1f} s")}
         extra = None
         if not args.no_extra and world == 1:
-            extra = {"cavity2d_config1": bench_cavity2d(pkg, steps=20000),
+            extra = {"tgv_config2_precisions": bench_tgv_precisions(pkg, n, 2000),
+                     "cavity2d_config1": bench_cavity2d(pkg, steps=20000),
                      "natconv_config4": bench_natconv(pkg, 512, 1e5, 2000),
                      "batch_config3_short": bench_batch(pkg, max_steps=2000, check_every=100,
                                                         autotune=False)}
@@ -377,6 +378,62 @@ def run_gpu(args):
 def _events():
     import torch
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def bench_tgv_precisions(pkg, n=N_GRID, steps=2000):
+    """Config 2 accuracy and speed per storage: periodic D3Q19 TRT
+    Taylor-Green n^3, Lambda=1/4, nu=0.01, u0=0.05, `steps` steps.  Reports
+    MLUPS, the HBM roofline fraction and the relative L2 / max velocity
+    error against the FP64 run and against exp(-2 nu k^2 t)."""
+    import numpy as np
+    import torch
+    k = 2 * math.pi / n
+    decay = math.exp(-2 * NU * k * k * steps)
+    x = torch.arange(n, dtype=torch.float64, device="cuda")
+    ua = (-U0 * torch.cos(k * x)[None, None, :] * torch.sin(k * x)[None, :, None]
+          * decay).expand(n, n, n)
+    peak, _ = hbm_peak()
+    plane = torch.from_numpy(pkg.drivers.taylor_green_3d_populations(n, U0, Nz=1)).cuda()
+    out, u64 = {}, None
+    for name in ("f64", "f32", "f32dev", "f16dev", "bf16dev"):
+        tname, dev, bpp, label = STORAGES[name]
+        dt = getattr(torch, tname)
+        f = torch.empty((19, n, n, n), dtype=dt, device="cuda")
+        full = _extrude(plane, n)
+        if name == "f64":
+            f.copy_(full)
+        else:
+            pkg.convert_populations(f, full, dst_deviation=dev)
+        del full
+        g = torch.empty_like(f)
+        fd = torch.float64 if name == "f64" else torch.float32
+        mom = [torch.empty((n, n, n), dtype=fd, device="cuda") for _ in range(4)]
+        e0, e1 = _events()
+        e0.record()
+        for s in range(steps):
+            m = mom if s == steps - 1 else (None,) * 4
+            pkg.fused_trt_step_3d_(g, f, *m, None, n, n, n, NU, LAMBDA, periodic=(1, 1, 1),
+                                   deviation=dev)
+            f, g = g, f
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        u = torch.stack([t.double() for t in mom[1:]])
+        del f, g, mom
+        row = {"mlups": round(n ** 3 / ms / 1e3, 1),
+               "hbm_frac": round(2 * 19 * bpp * n ** 3 / (ms * 1e-3) / 1e9 / peak, 4),
+               "l2_vs_analytic": float(torch.linalg.vector_norm(u[0] - ua) / torch.linalg.vector_norm(ua))}
+        if name == "f64":
+            u64 = u
+        else:
+            d = u - u64
+            row["l2_vs_f64"] = float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(u64))
+            row["max_vs_f64_over_u0"] = float(d.abs().max() / U0)
+        out[name] = row
+        del u
+        torch.cuda.empty_cache()
+    return {"workload": f"D3Q19 TRT periodic Taylor-Green {n}^3, Lambda=1/4, nu={NU}, u0={U0}, "
+                        f"{steps} steps per storage", "storages": out}
 
 
 def bench_cavity2d(pkg, steps=20000, graph_steps=200):
