@@ -342,7 +342,7 @@ def run_gpu(args):
         if not args.no_extra and world == 1:
             extra = {"tgv_config2_precisions": bench_tgv_precisions(pkg, n, 2000),
                      "cavity2d_config1": bench_cavity2d(pkg, steps=20000),
-                     "natconv_config4": bench_natconv(pkg, 512, 1e5, 2000),
+                     "natconv_config4": bench_natconv(pkg, 512, 1e5, 2000)[0],
                      "batch_config3_short": bench_batch(pkg, max_steps=2000, check_every=100,
                                                         autotune=False)}
         line = {
@@ -473,60 +473,165 @@ def bench_cavity2d(pkg, steps=20000, graph_steps=200):
 
 
 def bench_batch(pkg, n_cases=256, max_steps=50000, check_every=100, tol=1e-6, storage="f16",
-                autotune=True):
+                autotune=True, rank=0, world=1, error_cases=0):
     """Batched sweep: n_cases D2Q9 MRT cavities, N uniform on {64,...,512}, Re
-    log-uniform [100, 2000], u_lid=0.1, one persistent launch."""
+    log-uniform [100, 2000], u_lid=0.1, one persistent launch per rank (the
+    cases are split across ranks with no data exchange).  With error_cases
+    > 0, that many cases (spread over the size range) are rerun on the FP64
+    reference-arithmetic MRT cavity step for the same number of steps and
+    their velocity error is reported."""
+    import numpy as np
     import torch
     N, nu, u, Re = pkg.sweep_cases(n_cases, seed=0)
-    b = pkg.CavityBatch(N, nu, u, storage)
+    mine = pkg.sharding.shard_cases(N, world, rank)
+    b = pkg.CavityBatch(N[mine], nu[mine], u[mine], storage)
     tune = b.autotune(trial_steps=200) if autotune else None
     b.reset()
+    if world > 1:
+        barrier(world)
     e0, e1 = _events()
     e0.record()
     b.run(max_steps=max_steps, check_every=check_every, tol=tol)
     e1.record()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
     st = b.status()
-    states = {}
-    for c in range(n_cases):
+    updates = st["updates"]
+    if world > 1:
+        t = torch.tensor([float(updates)], dtype=torch.float64, device="cuda")
+        import torch.distributed as dist
+        dist.all_reduce(t)
+        updates = int(t.item())
+    states, steps = {}, []
+    for c in range(len(mine)):
         r = b.case(c, fields=False)
         states[r["state"]] = states.get(r["state"], 0) + 1
-    b.close()
+        steps.append(r["steps"])
     out = {"workload": f"{n_cases} D2Q9 MRT cavities, N in 64..512 step 32, Re log-uniform "
                        f"[100,2000], u_lid=0.1, {storage} deviation storage, residual {tol} or "
-                       f"{max_steps} steps, one persistent cooperative launch",
-           "mlups": round(st["updates"] / (ms * 1e-3) / 1e6, 1), "ms": round(ms, 1),
-           "node_updates": st["updates"], "cases": states, "timed_out": st["timed_out"]}
+                       f"{max_steps} steps, one persistent cooperative launch per GPU",
+           "mlups": round(updates / (ms * 1e-3) / 1e6, 1), "ms": round(ms, 1),
+           "node_updates": updates, "cases_on_rank0": states, "timed_out": st["timed_out"],
+           "steps_min_median_max": [int(min(steps)), int(np.median(steps)), int(max(steps))]}
     if tune:
         out["autotune"] = tune
+    if error_cases and rank == 0:
+        errs = []
+        pick = np.unique(np.linspace(0, len(mine) - 1, error_cases).round().astype(int))
+        for c in pick:
+            r = b.case(int(c))
+            n = int(r["N"])
+            ux64, uy64 = _fp64_mrt_cavity(pkg, n, float(nu[mine][c]), float(u[mine][c]), r["steps"])
+            d = np.sqrt((r["ux"] - ux64) ** 2 + (r["uy"] - uy64) ** 2)
+            errs.append({"N": n, "Re": round(float(Re[mine][c]), 1), "steps": r["steps"],
+                         "state": r["state"], "residual": r["residual"],
+                         "max_err_over_ulid": float(np.nanmax(d) / u[mine][c]),
+                         "l2_rel": float(np.sqrt(np.nansum(d ** 2) /
+                                                 np.sum(ux64 ** 2 + uy64 ** 2)))})
+        out["per_case_error_vs_fp64"] = errs
+    b.close()
     return out
 
 
-def bench_natconv(pkg, N=512, Ra=1e5, steps=2000):
-    """Thermal DDF natural convection, 512^2, Pr=0.71, FP32 fused step."""
+def _fp64_mrt_cavity(pkg, N, nu, u_lid, steps, graph_steps=200):
+    assert graph_steps % 2 == 0
+    """The plain FP64 single-case path: the fused MRT cavity step with the
+    reference arithmetic (kb_cavity_mrt_step_2d), `steps` steps from rest."""
     import torch
+    cfg = pkg.LBMConfig.d2q9(N, N, nu, u_lid, 0)
+    st = pkg.initialize_2d(cfg)
+    a, b = st["f_in"], st["f_out"]
+    full, rest = divmod(steps, graph_steps)
+    if full:
+        g = pkg.Graph()
+        with g:
+            x, y = a, b
+            for _ in range(graph_steps):
+                pkg.cavity_mrt_step_2d_(y, x, None, None, None, None, N, N, nu, u_lid)
+                x, y = y, x
+        for _ in range(full):
+            g.launch()          # an even number of steps: the state is back in `a`
+        g.close()
+    for _ in range(rest):
+        pkg.cavity_mrt_step_2d_(b, a, None, None, None, None, N, N, nu, u_lid)
+        a, b = b, a
+    pkg.compute_macroscopic_2d_(st["rho"], st["ux"], st["uy"], a)
+    torch.cuda.synchronize()
+    return st["ux"].cpu().numpy(), st["uy"].cpu().numpy()
+
+
+def bench_natconv(pkg, N=512, Ra=1e5, steps=2000, FT=None, graph_steps=500, nu_ref=None):
+    """Thermal DDF natural convection, N^2, Pr=0.71, fused step (FP32 by
+    default), `steps` steps replayed from a CUDA graph; returns MLUPS, the
+    hot-wall Nusselt number and the final fields."""
+    import torch
+    FT = FT or torch.float32
     p = pkg.drivers.natconv_parameters(N, Ra, 0.71)
     cfg = pkg.LBMConfig.d2q9(N, N, p["nu"], 0.0, 0)
-    st = pkg.initialize_2d(cfg, torch.float32)
-    gi = torch.from_numpy(pkg.drivers.natconv_initial_g(N)).to("cuda", torch.float32)
+    st = pkg.initialize_2d(cfg, FT)
+    gi = torch.from_numpy(pkg.drivers.natconv_initial_g(N)).to("cuda", FT)
     go = gi.clone()
-    Temp = torch.zeros((N, N), dtype=torch.float32, device="cuda")
+    Temp = torch.zeros((N, N), dtype=FT, device="cuda")
     fi, fo = st["f_in"], st["f_out"]
+    assert graph_steps % 2 == 0 and steps % graph_steps == 0
+    g = pkg.Graph()
+    with g:
+        a, b, c, d = fi, fo, gi, go
+        for _ in range(graph_steps):
+            pkg.fused_natconv_step_(b, a, d, c, Temp, N, N, p["omega_f"], p["omega_T"],
+                                    p["beta_g"], p["T_ref"], 1.0, 0.0)
+            a, b = b, a
+            c, d = d, c
+    g.launch()                      # warm-up replay (then restart from the initial state)
+    torch.cuda.synchronize()
+    st2 = pkg.initialize_2d(cfg, FT)
+    fi.copy_(st2["f_in"]); fo.copy_(st2["f_out"])
+    gi.copy_(torch.from_numpy(pkg.drivers.natconv_initial_g(N)).to("cuda", FT)); go.copy_(gi)
     e0, e1 = _events()
-    for s in range(steps + 10):
-        if s == 10:
-            e0.record()
-        pkg.fused_natconv_step_(fo, fi, go, gi, Temp, N, N, p["omega_f"], p["omega_T"],
-                                p["beta_g"], p["T_ref"], 1.0, 0.0)
-        fi, fo = fo, fi
-        gi, go = go, gi
+    e0.record()
+    for _ in range(steps // graph_steps):
+        g.launch()
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    return {"workload": f"thermal DDF natural convection {N}^2 FP32, Ra={Ra:g}, Pr=0.71, "
-                        f"{steps} fused steps", "mlups": round(N * N * steps / (ms * 1e-3) / 1e6, 1),
-            "gbs_alg": round(N * N * steps * 144 / (ms * 1e-3) / 1e9, 1)}
+    g.close()
+    T_prev = Temp.clone()
+    pkg.fused_natconv_step_(fo, fi, go, gi, Temp, N, N, p["omega_f"], p["omega_T"], p["beta_g"],
+                            p["T_ref"], 1.0, 0.0)
+    dT = float((Temp - T_prev).abs().max())
+    pkg.compute_temperature_2d_(Temp, go)
+    pkg.compute_macroscopic_2d_(st["rho"], st["ux"], st["uy"], fo)
+    T = Temp.double().cpu().numpy()
+    out = {"workload": f"thermal DDF natural convection {N}^2 {str(FT).split('.')[-1]}, Ra={Ra:g}, "
+                       f"Pr=0.71, {steps} fused steps (CUDA graph of {graph_steps})",
+           "mlups": round(N * N * steps / (ms * 1e-3) / 1e6, 1),
+           "gbs_alg": round(N * N * steps * (144 if FT == torch.float32 else 288) / (ms * 1e-3) / 1e9, 1),
+           "Nu": pkg.drivers.nusselt_hot_wall(T), "max_dT_last_step": dT}
+    if nu_ref is not None:
+        out["Nu_de_vahl_davis"] = nu_ref
+    return out, T, st["ux"].double().cpu().numpy(), st["uy"].double().cpu().numpy()
+
+
+def bench_natconv_validation(pkg, N=512, steps_by_ra=None):
+    """Config 4: Nu, MLUPS and FP32-vs-FP64 errors of T and u for Ra in
+    {1e4, 1e5, 1e6} on N^2."""
+    import json as _json
+    import numpy as np
+    import torch
+    pins = _json.loads((ROOT / "tests" / "golden" / "reference_pins.json").read_text())
+    dvd = pins["de_vahl_davis_nu"]
+    steps_by_ra = steps_by_ra or {1e4: 1280000, 1e5: 2560000, 1e6: 2560000}
+    res = {}
+    for ra, steps in steps_by_ra.items():
+        r32, T32, ux32, uy32 = bench_natconv(pkg, N, ra, steps, torch.float32,
+                                             nu_ref=dvd.get(str(int(ra))))
+        r64, T64, ux64, uy64 = bench_natconv(pkg, N, ra, steps, torch.float64)
+        un = np.sqrt(np.sum(ux64 ** 2 + uy64 ** 2))
+        res[f"Ra={ra:g}"] = {"fp32": r32, "fp64": {k: r64[k] for k in ("mlups", "Nu", "max_dT_last_step")},
+                             "T_max_err_fp32_vs_fp64": float(np.max(np.abs(T32 - T64))),
+                             "u_l2_rel_fp32_vs_fp64": float(np.sqrt(np.sum((ux32 - ux64) ** 2 +
+                                                                           (uy32 - uy64) ** 2)) / un)}
+    return res
 
 
 def _extrude(plane, n):
@@ -540,16 +645,23 @@ def run_other(args):
     """One of the other configurations, printed as its own JSON line."""
     import torch
     import __graft_entry__ as graft
-    torch.cuda.set_device(0)
+    rank, world, _ = dist_setup(args.gpus)
     pkg = graft.load_package()
     pkg._lib.load()
+    r = None
     if args.workload == "cavity2d":
-        r = bench_cavity2d(pkg, steps=max(args.steps, 200) // 200 * 200)
+        if rank == 0:
+            r = bench_cavity2d(pkg, steps=max(args.steps, 200) // 200 * 200)
     elif args.workload == "batch":
-        r = bench_batch(pkg)
-    else:
-        r = {f"Ra={ra:g}": bench_natconv(pkg, 512, ra, max(args.steps, 100)) for ra in (1e4, 1e5, 1e6)}
-    print(json.dumps({"metric": METRIC, "workload": args.workload, "result": r}), flush=True)
+        r = bench_batch(pkg, rank=rank, world=world, error_cases=8 if world == 1 else 0)
+    elif rank == 0:
+        r = bench_natconv_validation(pkg)
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "workload": args.workload, "n_gpus": world,
+                          "result": r}), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
     return 0
 
 
