@@ -97,6 +97,13 @@ int kb_apply_extrapolate_east_2d(void *f, int Nx, int Ny, int dtype, void *strea
  * wall_id: 1 south, 2 west, 3 east, 4 north (the reference's Int32 codes). */
 int kb_apply_bounce_back_wall_2d(void *f, int Nx, int Ny, int wall_id, int dtype, void *stream);
 
+/* f[.., q] = equilibrium(D2Q9(), rho, ux, uy, q) at every node
+ *   -- src/lattice/d2q9.jl:60-67, as the initialisers of src/drivers/basic.jl:265
+ * fill f.  Fields are double (fields_dtype KB_F64) or float (KB_F32), of
+ * Nx*Ny nodes each; populations are KB_F64 or KB_F32. */
+int kb_init_equilibrium_2d(void *f, const void *rho, const void *ux, const void *uy,
+                           int fields_dtype, int Nx, int Ny, int dtype, void *stream);
+
 /* compute_macroscopic_2d!(rho, ux, uy, f) -- src/kernels/macroscopic.jl:32 */
 int kb_compute_macroscopic_2d(void *rho, void *ux, void *uy, const void *f, int Nx, int Ny,
                               int dtype, void *stream);
@@ -347,6 +354,69 @@ int kb_mass_static(const void *f, int lattice_q, size_t n_nodes, int dtype, doub
 int kb_residual(const void *ux, const void *uy, const void *uz, const void *ux_prev,
                 const void *uy_prev, const void *uz_prev, const uint8_t *is_solid,
                 size_t n_nodes, int dtype, double *out_host, void *stream);
+
+/* ------------------------------------------------ learned warm start -- */
+
+/* The reference has no learned component.  These entry points add the warm
+ * start: a 4-level convolutional encoder-decoder that maps a cavity's
+ * (Re, N, wall mask) to its steady (rho, ux, uy).  Its forward, backward and
+ * optimiser kernels are all in this library.  Every 3x3 convolution runs on
+ * the BF16 tcgen05 tensor cores with FP32 accumulation in TMEM.  Activations
+ * are NHWC BF16.  The first network channel of the input is 8. */
+
+/* Plain GEMM on the same tensor-core mainloop: C[M][N] (FP32) = A B^T.  A is
+ * [M][K] BF16 (a_mn = 0) or [K][M] (a_mn = 1); B is [N][K] (b_mn = 0) or
+ * [K][N] (b_mn = 1).  M % 128 == 0, K % 64 == 0, N % 16 == 0.  *err_device
+ * (device int) is set to 1 if a bounded wait inside the kernel gave up. */
+int kb_gemm_bf16(const void *A, const void *B, float *C, int M, int N, int K, int a_mn,
+                 int b_mn, int *err_device, void *stream);
+
+typedef struct kb_surrogate kb_surrogate;
+/* Network for inputs of H x W (multiples of 8) with `base_channels` (a
+ * multiple of 16, 16..128) at the first level and batches of up to
+ * `max_batch` cases.  Weights are He-normal from `seed`.  Allocates all its
+ * device memory here; synchronises `stream`. */
+int kb_surrogate_create(kb_surrogate **out, int max_batch, int H, int W, int base_channels,
+                        unsigned long long seed, void *stream);
+int kb_surrogate_destroy(kb_surrogate *s);
+/* Number of FP32 parameters.  Layout: per layer W[cout][9*cin] (k = tap*cin +
+ * c, tap = (dy+1)*3 + (dx+1)) then b[cout]; kb_surrogate_layer gives each
+ * layer's offsets.  Layers: 0 enc1a, 1 enc1b, 2 enc2a, 3 enc2b, 4 enc3a,
+ * 5 enc3b, 6 bott_a, 7 bott_b, 8 dec3a, 9 dec3b, 10 dec2a, 11 dec2b,
+ * 12 dec1a, 13 dec1b, 14 head. */
+int kb_surrogate_num_params(const kb_surrogate *s, long long *n);
+int kb_surrogate_layer(const kb_surrogate *s, int layer, int *cin, int *cout, int *level,
+                       long long *w_off, long long *b_off);
+/* Output normalisation: the network predicts (x - offset) * scale for
+ * x = (rho, ux, uy). */
+int kb_surrogate_set_normalisation(kb_surrogate *s, const float *scale, const float *offset);
+/* Copy the FP32 parameters out to `get` and/or in from `set` (device
+ * pointers, n_params floats each); `set` also refreshes the BF16 copies. */
+int kb_surrogate_params(kb_surrogate *s, float *get, const float *set, void *stream);
+/* Copy the gradient of the last kb_surrogate_loss_backward to `get`. */
+int kb_surrogate_grads(kb_surrogate *s, float *get, void *stream);
+/* Build the NHWC BF16 input of n lid-driven cavities (device Re values). */
+int kb_surrogate_cavity_inputs(const kb_surrogate *s, void *input, const float *re, int n,
+                               int n_nodes, void *stream);
+/* Forward pass; `out` (device, may be NULL) receives planar [n][3][H][W]
+ * (rho, ux, uy) in physical units. */
+int kb_surrogate_infer(kb_surrogate *s, const void *input, int n, float *out, void *stream);
+/* Forward, mean-squared error against planar [n][3][H][W] targets, backward.
+ * The loss (device float, may be NULL) and the parameter gradient are kept. */
+int kb_surrogate_loss_backward(kb_surrogate *s, const void *input, const float *target, int n,
+                               float *loss_out, void *stream);
+/* One Adam update (bias-corrected, `step` counts from 1) with the last
+ * gradient, then a refresh of the BF16 weight copies. */
+int kb_surrogate_adam(kb_surrogate *s, float lr, float beta1, float beta2, float eps, int step,
+                      void *stream);
+/* kb_surrogate_loss_backward then kb_surrogate_adam (0.9, 0.999, 1e-8). */
+int kb_surrogate_train_step(kb_surrogate *s, const void *input, const float *target, int n,
+                            float lr, int step, float *loss_out, void *stream);
+/* *timed_out = 1 if any tensor-core kernel of this network gave up a bounded
+ * wait since creation; synchronises `stream`. */
+int kb_surrogate_status(kb_surrogate *s, int *timed_out, void *stream);
+/* Algorithmic FLOPs of one forward pass and of one training step for n cases. */
+int kb_surrogate_flops(const kb_surrogate *s, int n, double *forward_flops, double *train_flops);
 
 #ifdef __cplusplus
 }

@@ -39,6 +39,7 @@ SIGNATURES: dict[str, list] = {
     "kb_apply_extrapolate_east_2d": [_vp, _i, _i, _i, _vp],
     "kb_apply_bounce_back_wall_2d": [_vp, _i, _i, _i, _i, _vp],
     "kb_compute_macroscopic_2d": [_vp, _vp, _vp, _cvp, _i, _i, _i, _vp],
+    "kb_init_equilibrium_2d": [_vp, _cvp, _cvp, _cvp, _i, _i, _i, _i, _vp],
     "kb_fused_bgk_step": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _i, _vp],
     "kb_trt_rates": [_d, _d, _dp, _dp],
     "kb_fused_trt_step": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _d, _i, _vp],
@@ -83,6 +84,22 @@ SIGNATURES: dict[str, list] = {
     "kb_mass": [_cvp, _i, _sz, _i, _dp, _vp],
     "kb_mass_static": [_cvp, _i, _sz, _i, _dp, _vp],
     "kb_residual": [_cvp, _cvp, _cvp, _cvp, _cvp, _cvp, _u8p, _sz, _i, _dp, _vp],
+    "kb_gemm_bf16": [_cvp, _cvp, _vp, _i, _i, _i, _i, _i, _vp, _vp],
+    "kb_surrogate_create": [C.POINTER(_vp), _i, _i, _i, _i, C.c_ulonglong, _vp],
+    "kb_surrogate_destroy": [_vp],
+    "kb_surrogate_num_params": [_vp, C.POINTER(C.c_longlong)],
+    "kb_surrogate_layer": [_vp, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i),
+                           C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
+    "kb_surrogate_set_normalisation": [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float)],
+    "kb_surrogate_params": [_vp, _vp, _cvp, _vp],
+    "kb_surrogate_grads": [_vp, _vp, _vp],
+    "kb_surrogate_cavity_inputs": [_vp, _vp, _cvp, _i, _i, _vp],
+    "kb_surrogate_infer": [_vp, _cvp, _i, _vp, _vp],
+    "kb_surrogate_loss_backward": [_vp, _cvp, _cvp, _i, _vp, _vp],
+    "kb_surrogate_adam": [_vp, C.c_float, C.c_float, C.c_float, C.c_float, _i, _vp],
+    "kb_surrogate_train_step": [_vp, _cvp, _cvp, _i, C.c_float, _i, _vp, _vp],
+    "kb_surrogate_status": [_vp, C.POINTER(_i), _vp],
+    "kb_surrogate_flops": [_vp, _i, _dp, _dp],
 }
 _RESTYPES = {"kb_version": C.c_char_p, "kb_last_error": C.c_char_p}
 

@@ -38,6 +38,8 @@ UNITS = {
     "kb_reduce.cu": [],
     "kb_batch.cu": [],
     "kb_graph.cu": [],
+    "kb_umma.cu": [],
+    "kb_surrogate.cu": [],
 }
 
 

@@ -97,6 +97,22 @@ __device__ __forceinline__ void bgk(T *p, T omega, T &rho, T &ux, T &uy) {
     const size_t c = g.at(i, j);                           \
     const size_t P = g.plane;
 
+// equilibrium(::D2Q9, rho, ux, uy, q) (src/lattice/d2q9.jl:60-67) at every
+// node, as the reference's initialisers fill f (src/drivers/basic.jl:265).
+// Fields may be FP32 for FP64 populations (a warm start from a prediction).
+template <typename T, typename F>
+__global__ void __launch_bounds__(BX) equilibrium_k(T *__restrict__ f, const F *__restrict__ rho,
+                                                     const F *__restrict__ ux,
+                                                     const F *__restrict__ uy, Grid2<T> g) {
+    NODE2
+    const T r = (T)rho[c], a = (T)ux[c], b = (T)uy[c];
+    const T usq = a * a + b * b;
+    T feq[9];
+    feq_all(r, a, b, usq, feq);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[c + q * P] = feq[q];
+}
+
 // stream_2d_kernel!: src/kernels/collide_stream_2d.jl:5-31
 template <typename T>
 __global__ void __launch_bounds__(BX) stream_k(T *__restrict__ fo, const T *__restrict__ fi, Grid2<T> g) {
@@ -808,6 +824,21 @@ int kb_apply_bounce_back_wall_2d(void *f, int Nx, int Ny, int wall_id, int dtype
     KB_DISPATCH_PLAIN("kb_apply_bounce_back_wall_2d", dtype,
         (bounce_back_wall_k<T><<<line_grid(n), BX, 0, kb::as_stream(stream)>>>(
             (T *)f, grid2<T>(Nx, Ny), wall_id)));
+}
+
+int kb_init_equilibrium_2d(void *f, const void *rho, const void *ux, const void *uy,
+                           int fields_dtype, int Nx, int Ny, int dtype, void *stream) {
+    KB_REQUIRE(f && rho && ux && uy, "kb_init_equilibrium_2d: null pointer");
+    KB_REQUIRE(fields_dtype == KB_F64 || fields_dtype == KB_F32,
+               "kb_init_equilibrium_2d: fields must be KB_F64 or KB_F32 (got %d)", fields_dtype);
+    if (int e = check_dims("kb_init_equilibrium_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_init_equilibrium_2d", dtype,
+        if (fields_dtype == KB_F64)
+            (equilibrium_k<T, double><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+                (T *)f, (const double *)rho, (const double *)ux, (const double *)uy, grid2<T>(Nx, Ny)));
+        else
+            (equilibrium_k<T, float><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+                (T *)f, (const float *)rho, (const float *)ux, (const float *)uy, grid2<T>(Nx, Ny))));
 }
 
 int kb_compute_macroscopic_2d(void *rho, void *ux, void *uy, const void *f, int Nx, int Ny,

@@ -1,0 +1,721 @@
+// kb_surrogate.cu -- the warm-start network: a 4-level convolutional
+// encoder-decoder (U-Net) with BF16 weights and activations and FP32
+// accumulation, trained and evaluated entirely by this library's kernels.
+//
+// Every 3x3 convolution (forward, data gradient, weight gradient) runs on the
+// tcgen05 mainloop of kb_umma.cuh as an implicit GEMM over NHWC activations:
+//   forward   D[pixel, cout]      = sum_(tap,cin) X(pixel+tap, cin) W[cout, tap, cin]
+//   data grad D[pixel, cin]       = sum_(tap,cout) dY(pixel+tap, cout) W[cout, 8-tap, cin]
+//   weight    D[(tap,cin), cout]  = sum_pixel X(pixel+tap, cin) dY(pixel, cout)  (+ bias row)
+// The decoder's nearest-neighbour upsampling and skip concatenation are
+// folded into the operand loader (ActView), so neither is materialised.
+//
+// Network (C = base channels, resolution H x W at level 0):
+//   enc1a 8->C, enc1b C->C | pool | enc2a C->2C, enc2b | pool | enc3a 2C->4C,
+//   enc3b | pool | bott_a 4C->8C, bott_b 8C->8C | dec3a [up(8C), 4C]->4C, dec3b |
+//   dec2a [up(4C), 2C]->2C, dec2b | dec1a [up(2C), C]->C, dec1b | head C->16
+// ReLU after every convolution except the head; 2x2 average pooling.  The
+// head's channels 0..2 are the normalised (rho, ux, uy); 3..15 are unused.
+//
+// Parameters are one flat FP32 array: per layer W[cout][9*cin] (k = tap*cin +
+// c, tap = (dy+1)*3 + (dx+1)) followed by b[cout].  Adam keeps FP32 moments;
+// the BF16 operand copies (forward and transposed-flipped) are repacked after
+// every update.
+#include <cmath>
+#include <vector>
+
+#include "kb_common.cuh"
+#include "kb_umma.cuh"
+
+namespace kb {
+namespace sur {
+
+using bf16 = __nv_bfloat16;
+using umma::ActView;
+
+enum {
+    T_IN, T_E1A, T_E1B, T_P1, T_E2A, T_E2B, T_P2, T_E3A, T_E3B, T_P3,
+    T_BA, T_BB, T_D3A, T_D3B, T_D2A, T_D2B, T_D1A, T_D1B, T_OUT, T_COUNT
+};
+constexpr int IN_CH = 8, OUT_CH = 16, N_LAYERS = 15;
+
+struct LayerSpec { int in1, in2, out, relu, pooled_in; };
+constexpr LayerSpec kLayers[N_LAYERS] = {
+    {T_IN, -1, T_E1A, 1, 0},  {T_E1A, -1, T_E1B, 1, 0}, {T_P1, -1, T_E2A, 1, 1},
+    {T_E2A, -1, T_E2B, 1, 0}, {T_P2, -1, T_E3A, 1, 1},  {T_E3A, -1, T_E3B, 1, 0},
+    {T_P3, -1, T_BA, 1, 1},   {T_BA, -1, T_BB, 1, 0},   {T_BB, T_E3B, T_D3A, 1, 0},
+    {T_D3A, -1, T_D3B, 1, 0}, {T_D3B, T_E2B, T_D2A, 1, 0}, {T_D2A, -1, T_D2B, 1, 0},
+    {T_D2B, T_E1B, T_D1A, 1, 0}, {T_D1A, -1, T_D1B, 1, 0}, {T_D1B, -1, T_OUT, 0, 0},
+};
+
+// channels (as a multiple of C, or absolute when negative) and level of each tensor
+struct TensorSpec { int mult, level; };
+constexpr TensorSpec kTensors[T_COUNT] = {
+    {-IN_CH, 0}, {1, 0}, {1, 0}, {1, 1}, {2, 1}, {2, 1}, {2, 2}, {4, 2}, {4, 2}, {4, 3},
+    {8, 3}, {8, 3}, {4, 2}, {4, 2}, {2, 1}, {2, 1}, {1, 0}, {1, 0}, {-OUT_CH, 0},
+};
+
+__host__ __device__ inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+// ------------------------------------------------------------------ kernels
+
+// 2x2 average pooling, NHWC BF16, 8 channels per thread.
+__global__ void pool_k(bf16 *__restrict__ out, const bf16 *__restrict__ in, int B, int Ho, int Wo,
+                       int C) {
+    const int cc = C / 8;
+    const long long n = (long long)B * Ho * Wo * cc;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t % cc) * 8;
+        const long long p = t / cc;
+        const int w = (int)(p % Wo), h = (int)((p / Wo) % Ho), b = (int)(p / ((long long)Wo * Ho));
+        float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx) {
+                const size_t q = (((size_t)b * 2 * Ho + 2 * h + dy) * 2 * Wo + 2 * w + dx) * C + c;
+                const uint4 v = *reinterpret_cast<const uint4 *>(in + q);
+                const bf16 *e = reinterpret_cast<const bf16 *>(&v);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) s[i] += __bfloat162float(e[i]);
+            }
+        __align__(16) bf16 o[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) o[i] = __float2bfloat16_rn(0.25f * s[i]);
+        *reinterpret_cast<uint4 *>(out + (size_t)p * C + c) = *reinterpret_cast<const uint4 *>(o);
+    }
+}
+
+// Gradient of nearest upsampling: dst (low resolution, Cl channels) = sum of
+// the 2x2 children of src channels [0, Cl) (src has Cs channels).
+__global__ void upsum_k(bf16 *__restrict__ dst, const bf16 *__restrict__ src, int B, int Hl, int Wl,
+                        int Cl, int Cs) {
+    const int cc = Cl / 8;
+    const long long n = (long long)B * Hl * Wl * cc;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t % cc) * 8;
+        const long long p = t / cc;
+        const int w = (int)(p % Wl), h = (int)((p / Wl) % Hl), b = (int)(p / ((long long)Wl * Hl));
+        float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx) {
+                const size_t q = (((size_t)b * 2 * Hl + 2 * h + dy) * 2 * Wl + 2 * w + dx) * Cs + c;
+                const uint4 v = *reinterpret_cast<const uint4 *>(src + q);
+                const bf16 *e = reinterpret_cast<const bf16 *>(&v);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) s[i] += __bfloat162float(e[i]);
+            }
+        __align__(16) bf16 o[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) o[i] = __float2bfloat16_rn(s[i]);
+        *reinterpret_cast<uint4 *>(dst + (size_t)p * Cl + c) = *reinterpret_cast<const uint4 *>(o);
+    }
+}
+
+// Gradient of a skip tensor S (C channels, H x W) used by a decoder concat
+// (channels [off, off+C) of dcat, Cc channels, already masked) and by a 2x2
+// average pool (dpool at H/2 x W/2, not masked):
+//   dS = dcat[.., off + c] + (S > 0) * dpool(parent) / 4
+__global__ void skip_grad_k(bf16 *__restrict__ dst, const bf16 *__restrict__ dcat,
+                            const bf16 *__restrict__ dpool, const bf16 *__restrict__ S, int B, int H,
+                            int W, int C, int Cc, int off) {
+    const int cc = C / 8;
+    const long long n = (long long)B * H * W * cc;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t % cc) * 8;
+        const long long p = t / cc;
+        const int w = (int)(p % W), h = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
+        const size_t pp = (((size_t)b * (H / 2) + h / 2) * (W / 2) + w / 2) * C + c;
+        const uint4 a = *reinterpret_cast<const uint4 *>(dcat + (size_t)p * Cc + off + c);
+        const uint4 g = *reinterpret_cast<const uint4 *>(dpool + pp);
+        const uint4 s = *reinterpret_cast<const uint4 *>(S + (size_t)p * C + c);
+        const bf16 *ea = reinterpret_cast<const bf16 *>(&a);
+        const bf16 *eg = reinterpret_cast<const bf16 *>(&g);
+        const bf16 *es = reinterpret_cast<const bf16 *>(&s);
+        __align__(16) bf16 o[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            float v = __bfloat162float(ea[i]);
+            if (__bfloat162float(es[i]) > 0.f) v += 0.25f * __bfloat162float(eg[i]);
+            o[i] = __float2bfloat16_rn(v);
+        }
+        *reinterpret_cast<uint4 *>(dst + (size_t)p * C + c) = *reinterpret_cast<const uint4 *>(o);
+    }
+}
+
+// Mean-squared error over channels 0..2 of the head against the normalised
+// target ((t - offset) * scale, target planar [n][3][H][W]); writes the head
+// gradient (BF16, OUT_CH channels, zero beyond 2) and adds the loss to *loss.
+struct Norm { float scale[3], offset[3]; };
+
+__global__ void loss_k(bf16 *__restrict__ grad, float *__restrict__ loss, const float *__restrict__ pred,
+                       const float *__restrict__ target, Norm nm, int M, int HW) {
+    __shared__ float red[8];
+    float acc = 0.f;
+    const float gs = 2.0f / (3.0f * (float)M);
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+        const int b = m / HW, p = m - b * HW;
+        __align__(16) bf16 g[OUT_CH];
+#pragma unroll
+        for (int c = 0; c < OUT_CH; ++c) g[c] = __float2bfloat16_rn(0.f);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float t = (target[((size_t)b * 3 + c) * HW + p] - nm.offset[c]) * nm.scale[c];
+            const float d = pred[(size_t)m * OUT_CH + c] - t;
+            acc += d * d;
+            g[c] = __float2bfloat16_rn(gs * d);
+        }
+        uint4 *dst = reinterpret_cast<uint4 *>(grad + (size_t)m * OUT_CH);
+        dst[0] = reinterpret_cast<const uint4 *>(g)[0];
+        dst[1] = reinterpret_cast<const uint4 *>(g)[1];
+    }
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = 0.f;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[i];
+        atomicAdd(loss, s / (3.0f * (float)M));
+    }
+}
+
+// Head output (normalised, [M][OUT_CH]) -> physical planar [n][3][H][W].
+__global__ void unpack_k(float *__restrict__ out, const float *__restrict__ pred, Norm nm, int M, int HW) {
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+        const int b = m / HW, p = m - b * HW;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            out[((size_t)b * 3 + c) * HW + p] = pred[(size_t)m * OUT_CH + c] / nm.scale[c] + nm.offset[c];
+    }
+}
+
+// Sum the split-K partials of a weight gradient into the flat gradient array:
+// part [splits][9C+1][Cout] -> gW[cout][9C], gb[cout] (row 9C).
+__global__ void wgrad_reduce_k(float *__restrict__ gW, float *__restrict__ gb,
+                               const float *__restrict__ part, int splits, int R, int Cout) {
+    const int n = (R + 1) * Cout;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int r = t / Cout, co = t - r * Cout;
+        float s = 0.f;
+        for (int z = 0; z < splits; ++z) s += part[((size_t)z * (R + 1) + r) * Cout + co];
+        if (r < R) gW[(size_t)co * R + r] = s;
+        else gb[co] = s;
+    }
+}
+
+__global__ void adam_k(float *__restrict__ p, float *__restrict__ m, float *__restrict__ v,
+                       const float *__restrict__ g, long long n, float lr_t, float b1, float b2,
+                       float eps_t) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= lr_t * mi / (sqrtf(vi) + eps_t);
+    }
+}
+
+// W [Cout][9 Cin] FP32 -> wb [Cout][Kp] and wt [Cin][Kpt] BF16 (zero padded):
+//   wt[ci][t*Cout + co] = W[co][(8 - t)*Cin + ci]
+__global__ void pack_k(bf16 *__restrict__ wb, bf16 *__restrict__ wt, const float *__restrict__ W,
+                       int Cin, int Cout, int Kp, int Kpt) {
+    const int n1 = Cout * Kp, n2 = wt ? Cin * Kpt : 0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n1 + n2; t += gridDim.x * blockDim.x) {
+        if (t < n1) {
+            const int co = t / Kp, k = t - co * Kp;
+            wb[t] = __float2bfloat16_rn(k < 9 * Cin ? W[(size_t)co * 9 * Cin + k] : 0.f);
+        } else {
+            const int u = t - n1, ci = u / Kpt, k = u - ci * Kpt;
+            float x = 0.f;
+            if (k < 9 * Cout) {
+                const int tap = k / Cout, co = k - tap * Cout;
+                x = W[(size_t)co * 9 * Cin + (8 - tap) * Cin + ci];
+            }
+            wt[u] = __float2bfloat16_rn(x);
+        }
+    }
+}
+
+// Network input of n lid-driven cavities at H x W (NHWC BF16, IN_CH channels):
+// 0 wall mask (x = 0, x = W-1, y = 0), 1 lid row (y = H-1), 2 (ln Re - ln 100)/ln 32,
+// 3 N/512, 4 x in (-1, 1), 5 y in (-1, 1), 6-7 zero.
+__global__ void cavity_inputs_k(bf16 *__restrict__ in, const float *__restrict__ re, int n, int H,
+                                int W, float n_norm) {
+    const long long total = (long long)n * H * W;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int w = (int)(t % W), h = (int)((t / W) % H), b = (int)(t / ((long long)W * H));
+        __align__(16) bf16 o[IN_CH];
+        o[0] = __float2bfloat16_rn((w == 0 || w == W - 1 || h == 0) ? 1.f : 0.f);
+        o[1] = __float2bfloat16_rn(h == H - 1 ? 1.f : 0.f);
+        o[2] = __float2bfloat16_rn((logf(re[b]) - 4.605170186f) / 3.465735903f);
+        o[3] = __float2bfloat16_rn(n_norm);
+        o[4] = __float2bfloat16_rn(2.f * (w + 0.5f) / W - 1.f);
+        o[5] = __float2bfloat16_rn(2.f * (h + 0.5f) / H - 1.f);
+        o[6] = o[7] = __float2bfloat16_rn(0.f);
+        *reinterpret_cast<uint4 *>(in + (size_t)t * IN_CH) = *reinterpret_cast<const uint4 *>(o);
+    }
+}
+
+inline dim3 ew_grid(long long n) {
+    long long b = (n + 255) / 256;
+    const long long cap = (long long)kb::sm_count() * 16;
+    return dim3((unsigned)(b < 1 ? 1 : (b > cap ? cap : b)));
+}
+
+// ------------------------------------------------------------------ network
+
+struct Layer {
+    int cin1, cin2, up1, cin, cout, level, relu, pooled_in, in1, in2, out;
+    int Kp, Kpt, bn_f, bn_d, bn_w;
+    long long w_off, b_off;
+    bf16 *wb = nullptr, *wt = nullptr;
+    bf16 *dx = nullptr;  // data-gradient output (own buffer for concat inputs)
+};
+
+}  // namespace sur
+}  // namespace kb
+
+using namespace kb::sur;
+
+struct kb_surrogate {
+    int Bmax, H, W, C;
+    std::vector<Layer> L;
+    int tch[T_COUNT];
+    bf16 *act[T_COUNT] = {};
+    bf16 *grad[T_COUNT] = {};
+    float *out_f32 = nullptr;           // head output [Bmax*H*W][OUT_CH]
+    float *params = nullptr, *grads = nullptr, *adam_m = nullptr, *adam_v = nullptr;
+    long long n_params = 0;
+    float *part = nullptr;              // split-K partials
+    size_t part_floats = 0;
+    int *err = nullptr;
+    float *loss = nullptr;
+    Norm norm{{1.f, 1.f, 1.f}, {0.f, 0.f, 0.f}};
+    std::vector<void *> allocs;
+    int H_at(int level) const { return H >> level; }
+    int W_at(int level) const { return W >> level; }
+};
+
+namespace {
+
+int alloc(kb_surrogate *s, void **p, size_t bytes) {
+    if (cudaMalloc(p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return kb::set_error(KB_ERR_NOMEM, "kb_surrogate_create: cudaMalloc of %zu bytes failed", bytes);
+    }
+    s->allocs.push_back(*p);
+    return 0;
+}
+
+ActView view_of(const kb_surrogate *s, const Layer &l, int n) {
+    ActView v{};
+    v.s1 = s->act[l.in1];
+    v.c1 = l.cin1;
+    v.up1 = l.up1;
+    v.s2 = l.in2 >= 0 ? s->act[l.in2] : nullptr;
+    v.c2 = l.cin2;
+    v.B = n;
+    v.H = s->H_at(l.level);
+    v.W = s->W_at(l.level);
+    return v;
+}
+
+// Upper bound of the split count of a layer's weight gradient (any batch).
+int max_wgrad_splits(const Layer &l) {
+    const int R = 9 * l.cin;
+    const int tiles = ((R + 1 + kb::umma::BM - 1) / kb::umma::BM) * (l.cout / l.bn_w);
+    const int want = (2 * kb::sm_count() + tiles - 1) / tiles;
+    return want < 1 ? 1 : want;
+}
+
+// Splits of the pixel (K) range so that about two CTAs per SM run; every
+// split gets at least one K step and the count never exceeds the bound above.
+int wgrad_splits(const Layer &l, int M, int &steps_per_split) {
+    const int nsteps = (M + kb::umma::BK - 1) / kb::umma::BK;
+    int want = max_wgrad_splits(l);
+    if (want > nsteps) want = nsteps;
+    steps_per_split = (nsteps + want - 1) / want;
+    return (nsteps + steps_per_split - 1) / steps_per_split;
+}
+
+int forward(kb_surrogate *s, const void *input, int n, cudaStream_t st) {
+    using namespace kb::umma;
+    s->act[T_IN] = (bf16 *)input;
+    for (int i = 0; i < N_LAYERS; ++i) {
+        const Layer &l = s->L[i];
+        // pooled inputs are produced just before their consumer
+        if (l.pooled_in) {
+            const Layer &src = s->L[i - 1];
+            const int Ho = s->H_at(l.level), Wo = s->W_at(l.level);
+            pool_k<<<ew_grid((long long)n * Ho * Wo * (src.cout / 8)), 256, 0, st>>>(
+                s->act[l.in1], s->act[src.out], n, Ho, Wo, src.cout);
+        }
+        const int M = n * s->H_at(l.level) * s->W_at(l.level);
+        ConvOp op{};
+        op.x = view_of(s, l, n);
+        op.wt = l.wb;
+        op.bias = s->params + l.b_off;
+        op.mask.s1 = nullptr;
+        op.out = l.out == T_OUT ? (void *)s->out_f32 : (void *)s->act[l.out];
+        op.M = M;
+        op.Nout = l.cout;
+        op.Kp = l.Kp;
+        op.bn = l.bn_f;
+        op.relu = l.relu;
+        op.out_f32 = l.out == T_OUT;
+        op.nsteps = l.Kp / BK;
+        const dim3 grid((M + BM - 1) / BM, l.cout / l.bn_f);
+        if (int rc = launch(op, grid, s->err, st)) return rc;
+    }
+    return kb::check_launch("kb_surrogate forward");
+}
+
+int backward(kb_surrogate *s, int n, cudaStream_t st) {
+    using namespace kb::umma;
+    for (int i = N_LAYERS - 1; i >= 0; --i) {
+        const Layer &l = s->L[i];
+        const int Hl = s->H_at(l.level), Wl = s->W_at(l.level);
+        const int M = n * Hl * Wl;
+        const ActView xv = view_of(s, l, n);
+        // weight gradient (split over pixels) and its reduction
+        int sps = 0;
+        const int splits = wgrad_splits(l, M, sps);
+        WgradOp wo{};
+        wo.x = xv;
+        wo.dy = s->grad[l.out];
+        wo.part = s->part;
+        wo.M = M;
+        wo.Nout = l.cout;
+        wo.bn = l.bn_w;
+        wo.steps_per_split = sps;
+        wo.nsteps = (M + BK - 1) / BK;
+        const int R = 9 * l.cin;
+        const dim3 wg((R + 1 + BM - 1) / BM, l.cout / l.bn_w, splits);
+        if (int rc = launch(wo, wg, s->err, st)) return rc;
+        wgrad_reduce_k<<<ew_grid((long long)(R + 1) * l.cout), 256, 0, st>>>(
+            s->grads + l.w_off, s->grads + l.b_off, s->part, splits, R, l.cout);
+        if (i == 0) break;
+        // data gradient
+        ConvOp op{};
+        op.x.s1 = s->grad[l.out];
+        op.x.c1 = l.cout;
+        op.x.up1 = 0;
+        op.x.s2 = nullptr;
+        op.x.c2 = 0;
+        op.x.B = n;
+        op.x.H = Hl;
+        op.x.W = Wl;
+        op.wt = l.wt;
+        op.bias = nullptr;
+        if (l.pooled_in) op.mask.s1 = nullptr;
+        else op.mask = xv;
+        op.out = l.dx;
+        op.M = M;
+        op.Nout = l.cin;
+        op.Kp = l.Kpt;
+        op.bn = l.bn_d;
+        op.relu = 0;
+        op.out_f32 = 0;
+        op.nsteps = l.Kpt / BK;
+        const dim3 grid((M + BM - 1) / BM, l.cin / l.bn_d);
+        if (int rc = launch(op, grid, s->err, st)) return rc;
+        // route the concat's gradient: the upsampled part to the low-resolution tensor
+        if (l.in2 >= 0) {
+            const Layer &lo = s->L[i - 1];  // producer of in1 (bott_b / dec3b / dec2b)
+            const int Hlo = s->H_at(lo.level), Wlo = s->W_at(lo.level);
+            upsum_k<<<ew_grid((long long)n * Hlo * Wlo * (l.cin1 / 8)), 256, 0, st>>>(
+                s->grad[l.in1], l.dx, n, Hlo, Wlo, l.cin1, l.cin);
+        }
+        // a pooled input: finish the skip tensor's gradient (concat part + pool part)
+        if (l.pooled_in) {
+            const int skip = s->L[i - 1].out;  // enc1b / enc2b / enc3b
+            const Layer *dec = nullptr;
+            for (const Layer &d : s->L)
+                if (d.in2 == skip) dec = &d;
+            const int Hs = s->H_at(s->L[i - 1].level), Ws = s->W_at(s->L[i - 1].level);
+            const int Cs = s->L[i - 1].cout;
+            skip_grad_k<<<ew_grid((long long)n * Hs * Ws * (Cs / 8)), 256, 0, st>>>(
+                s->grad[skip], dec->dx, s->grad[l.in1], s->act[skip], n, Hs, Ws, Cs, dec->cin,
+                dec->cin1);
+        }
+    }
+    return kb::check_launch("kb_surrogate backward");
+}
+
+int repack(kb_surrogate *s, cudaStream_t st) {
+    for (int i = 0; i < N_LAYERS; ++i) {
+        const Layer &l = s->L[i];
+        const long long n = (long long)l.cout * l.Kp + (l.wt ? (long long)l.cin * l.Kpt : 0);
+        pack_k<<<ew_grid(n), 256, 0, st>>>(l.wb, l.wt, s->params + l.w_off, l.cin, l.cout, l.Kp, l.Kpt);
+    }
+    return kb::check_launch("kb_surrogate repack");
+}
+
+uint64_t splitmix(uint64_t &x) {
+    uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+}  // namespace
+
+extern "C" {
+
+int kb_surrogate_create(kb_surrogate **out, int max_batch, int H, int W, int base_channels,
+                        unsigned long long seed, void *stream) {
+    KB_REQUIRE(out, "kb_surrogate_create: null handle pointer");
+    *out = nullptr;
+    KB_REQUIRE(max_batch > 0, "kb_surrogate_create: max_batch=%d must be positive", max_batch);
+    KB_REQUIRE(H >= 8 && W >= 8 && H % 8 == 0 && W % 8 == 0,
+               "kb_surrogate_create: H=%d and W=%d must be multiples of 8 (three 2x2 poolings)", H, W);
+    KB_REQUIRE(base_channels >= 16 && base_channels % 16 == 0 && base_channels <= 128,
+               "kb_surrogate_create: base_channels=%d must be a multiple of 16 in [16, 128]",
+               base_channels);
+    cudaStream_t st = kb::as_stream(stream);
+    kb_surrogate *s = new kb_surrogate();
+    s->Bmax = max_batch;
+    s->H = H;
+    s->W = W;
+    s->C = base_channels;
+    for (int t = 0; t < T_COUNT; ++t)
+        s->tch[t] = kTensors[t].mult < 0 ? -kTensors[t].mult : kTensors[t].mult * base_channels;
+    long long off = 0;
+    for (int i = 0; i < N_LAYERS; ++i) {
+        const LayerSpec &sp = kLayers[i];
+        Layer l;
+        l.in1 = sp.in1;
+        l.in2 = sp.in2;
+        l.out = sp.out;
+        l.relu = sp.relu;
+        l.pooled_in = sp.pooled_in;
+        l.cin1 = s->tch[sp.in1];
+        l.cin2 = sp.in2 >= 0 ? s->tch[sp.in2] : 0;
+        l.up1 = sp.in2 >= 0 ? 1 : 0;
+        l.cin = l.cin1 + l.cin2;
+        l.cout = s->tch[sp.out];
+        l.level = kTensors[sp.out].level;
+        l.Kp = round_up(9 * l.cin, kb::umma::BK);
+        l.Kpt = round_up(9 * l.cout, kb::umma::BK);
+        l.bn_f = kb::umma::pick_bn(l.cout);
+        l.bn_w = l.bn_f;
+        l.bn_d = kb::umma::pick_bn(l.cin);
+        l.w_off = off;
+        off += (long long)l.cout * 9 * l.cin;
+        l.b_off = off;
+        off += l.cout;
+        s->L.push_back(l);
+    }
+    s->n_params = off;
+    int rc = 0;
+    auto A = [&](void **p, size_t bytes) {
+        if (!rc) rc = alloc(s, p, bytes);
+    };
+    const size_t pix0 = (size_t)max_batch * H * W;
+    for (int t = 1; t < T_COUNT - 1; ++t) {
+        const size_t px = pix0 >> (2 * kTensors[t].level);
+        A((void **)&s->act[t], px * s->tch[t] * sizeof(bf16));
+        A((void **)&s->grad[t], px * s->tch[t] * sizeof(bf16));
+    }
+    A((void **)&s->out_f32, pix0 * OUT_CH * sizeof(float));
+    A((void **)&s->grad[T_OUT], pix0 * OUT_CH * sizeof(bf16));
+    size_t part = 0;
+    for (int i = 0; i < N_LAYERS && !rc; ++i) {
+        Layer &l = s->L[i];
+        A((void **)&l.wb, (size_t)l.cout * l.Kp * sizeof(bf16));
+        if (i > 0) A((void **)&l.wt, (size_t)l.cin * l.Kpt * sizeof(bf16));
+        const size_t px = pix0 >> (2 * l.level);
+        if (i > 0) {
+            if (l.in2 >= 0) A((void **)&l.dx, px * l.cin * sizeof(bf16));
+            else l.dx = s->grad[l.in1];
+        }
+        const size_t need = (size_t)max_wgrad_splits(l) * (9 * l.cin + 1) * l.cout;
+        if (need > part) part = need;
+    }
+    s->part_floats = part;
+    A((void **)&s->part, part * sizeof(float));
+    A((void **)&s->params, (size_t)s->n_params * sizeof(float));
+    A((void **)&s->grads, (size_t)s->n_params * sizeof(float));
+    A((void **)&s->adam_m, (size_t)s->n_params * sizeof(float));
+    A((void **)&s->adam_v, (size_t)s->n_params * sizeof(float));
+    A((void **)&s->err, sizeof(int));
+    A((void **)&s->loss, sizeof(float));
+    if (rc) {
+        for (void *p : s->allocs) cudaFree(p);
+        delete s;
+        return rc;
+    }
+    // He-normal initialisation on the host (deterministic in `seed`), zero biases
+    std::vector<float> h((size_t)s->n_params, 0.f);
+    uint64_t x = seed;
+    for (int i = 0; i < N_LAYERS; ++i) {
+        const Layer &l = s->L[i];
+        const double sd = std::sqrt(2.0 / (9.0 * l.cin)) * (l.out == T_OUT ? 0.1 : 1.0);
+        for (long long k = 0; k < (long long)l.cout * 9 * l.cin; ++k) {
+            const double u1 = ((splitmix(x) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+            const double u2 = ((splitmix(x) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+            h[l.w_off + k] = (float)(sd * std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2));
+        }
+    }
+    cudaMemcpyAsync(s->params, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(s->adam_m, 0, (size_t)s->n_params * sizeof(float), st);
+    cudaMemsetAsync(s->adam_v, 0, (size_t)s->n_params * sizeof(float), st);
+    cudaMemsetAsync(s->grads, 0, (size_t)s->n_params * sizeof(float), st);
+    cudaMemsetAsync(s->err, 0, sizeof(int), st);
+    repack(s, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        rc = kb::check_launch("kb_surrogate_create");
+        for (void *p : s->allocs) cudaFree(p);
+        delete s;
+        return rc ? rc : KB_ERR_CUDA;
+    }
+    *out = s;
+    return 0;
+}
+
+int kb_surrogate_destroy(kb_surrogate *s) {
+    if (!s) return 0;
+    cudaDeviceSynchronize();
+    for (void *p : s->allocs) cudaFree(p);
+    delete s;
+    return kb::check_launch("kb_surrogate_destroy");
+}
+
+int kb_surrogate_num_params(const kb_surrogate *s, long long *n) {
+    KB_REQUIRE(s && n, "kb_surrogate_num_params: null argument");
+    *n = s->n_params;
+    return 0;
+}
+
+int kb_surrogate_layer(const kb_surrogate *s, int layer, int *cin, int *cout, int *level,
+                       long long *w_off, long long *b_off) {
+    KB_REQUIRE(s, "kb_surrogate_layer: null handle");
+    KB_REQUIRE(layer >= 0 && layer < N_LAYERS, "kb_surrogate_layer: layer %d out of [0, %d)", layer,
+               N_LAYERS);
+    const Layer &l = s->L[layer];
+    if (cin) *cin = l.cin;
+    if (cout) *cout = l.cout;
+    if (level) *level = l.level;
+    if (w_off) *w_off = l.w_off;
+    if (b_off) *b_off = l.b_off;
+    return 0;
+}
+
+int kb_surrogate_set_normalisation(kb_surrogate *s, const float *scale, const float *offset) {
+    KB_REQUIRE(s && scale && offset, "kb_surrogate_set_normalisation: null argument");
+    for (int c = 0; c < 3; ++c) {
+        KB_REQUIRE(scale[c] != 0.f && std::isfinite(scale[c]) && std::isfinite(offset[c]),
+                   "kb_surrogate_set_normalisation: scale %d must be finite and non-zero", c);
+        s->norm.scale[c] = scale[c];
+        s->norm.offset[c] = offset[c];
+    }
+    return 0;
+}
+
+int kb_surrogate_params(kb_surrogate *s, float *get, const float *set, void *stream) {
+    KB_REQUIRE(s, "kb_surrogate_params: null handle");
+    cudaStream_t st = kb::as_stream(stream);
+    const size_t bytes = (size_t)s->n_params * sizeof(float);
+    if (get) cudaMemcpyAsync(get, s->params, bytes, cudaMemcpyDeviceToDevice, st);
+    if (set) {
+        cudaMemcpyAsync(s->params, set, bytes, cudaMemcpyDeviceToDevice, st);
+        if (int rc = repack(s, st)) return rc;
+    }
+    return kb::check_launch("kb_surrogate_params");
+}
+
+int kb_surrogate_grads(kb_surrogate *s, float *get, void *stream) {
+    KB_REQUIRE(s && get, "kb_surrogate_grads: null argument");
+    cudaMemcpyAsync(get, s->grads, (size_t)s->n_params * sizeof(float), cudaMemcpyDeviceToDevice,
+                    kb::as_stream(stream));
+    return kb::check_launch("kb_surrogate_grads");
+}
+
+int kb_surrogate_cavity_inputs(const kb_surrogate *s, void *input, const float *re, int n,
+                               int n_nodes, void *stream) {
+    KB_REQUIRE(s && input && re, "kb_surrogate_cavity_inputs: null argument");
+    KB_REQUIRE(n > 0 && n <= s->Bmax, "kb_surrogate_cavity_inputs: n=%d out of [1, %d]", n, s->Bmax);
+    cavity_inputs_k<<<ew_grid((long long)n * s->H * s->W), 256, 0, kb::as_stream(stream)>>>(
+        (bf16 *)input, re, n, s->H, s->W, (float)n_nodes / 512.f);
+    return kb::check_launch("kb_surrogate_cavity_inputs");
+}
+
+int kb_surrogate_infer(kb_surrogate *s, const void *input, int n, float *out, void *stream) {
+    KB_REQUIRE(s && input, "kb_surrogate_infer: null argument");
+    KB_REQUIRE(n > 0 && n <= s->Bmax, "kb_surrogate_infer: n=%d out of [1, %d]", n, s->Bmax);
+    KB_REQUIRE(((uintptr_t)input % 16) == 0, "kb_surrogate_infer: input must be 16-byte aligned");
+    cudaStream_t st = kb::as_stream(stream);
+    if (int rc = forward(s, input, n, st)) return rc;
+    if (out) {
+        const int M = n * s->H * s->W;
+        unpack_k<<<ew_grid(M), 256, 0, st>>>(out, s->out_f32, s->norm, M, s->H * s->W);
+    }
+    return kb::check_launch("kb_surrogate_infer");
+}
+
+int kb_surrogate_loss_backward(kb_surrogate *s, const void *input, const float *target, int n,
+                               float *loss_out, void *stream) {
+    KB_REQUIRE(s && input && target, "kb_surrogate_loss_backward: null argument");
+    KB_REQUIRE(n > 0 && n <= s->Bmax, "kb_surrogate_loss_backward: n=%d out of [1, %d]", n, s->Bmax);
+    KB_REQUIRE(((uintptr_t)input % 16) == 0, "kb_surrogate_loss_backward: input must be 16-byte aligned");
+    cudaStream_t st = kb::as_stream(stream);
+    if (int rc = forward(s, input, n, st)) return rc;
+    const int M = n * s->H * s->W;
+    cudaMemsetAsync(s->loss, 0, sizeof(float), st);
+    loss_k<<<ew_grid(M), 256, 0, st>>>(s->grad[T_OUT], s->loss, s->out_f32, target, s->norm, M,
+                                        s->H * s->W);
+    if (int rc = backward(s, n, st)) return rc;
+    if (loss_out) cudaMemcpyAsync(loss_out, s->loss, sizeof(float), cudaMemcpyDeviceToDevice, st);
+    return kb::check_launch("kb_surrogate_loss_backward");
+}
+
+int kb_surrogate_adam(kb_surrogate *s, float lr, float beta1, float beta2, float eps, int step,
+                      void *stream) {
+    KB_REQUIRE(s, "kb_surrogate_adam: null handle");
+    KB_REQUIRE(step >= 1, "kb_surrogate_adam: step=%d must be >= 1", step);
+    KB_REQUIRE(lr >= 0.f && beta1 >= 0.f && beta1 < 1.f && beta2 >= 0.f && beta2 < 1.f && eps > 0.f,
+               "kb_surrogate_adam: bad hyper-parameters");
+    cudaStream_t st = kb::as_stream(stream);
+    const double c1 = 1.0 - std::pow((double)beta1, step), c2 = 1.0 - std::pow((double)beta2, step);
+    const float lr_t = (float)(lr * std::sqrt(c2) / c1);
+    const float eps_t = (float)(eps * std::sqrt(c2));
+    adam_k<<<ew_grid(s->n_params), 256, 0, st>>>(s->params, s->adam_m, s->adam_v, s->grads,
+                                                  s->n_params, lr_t, beta1, beta2, eps_t);
+    if (int rc = repack(s, st)) return rc;
+    return kb::check_launch("kb_surrogate_adam");
+}
+
+int kb_surrogate_train_step(kb_surrogate *s, const void *input, const float *target, int n,
+                            float lr, int step, float *loss_out, void *stream) {
+    if (int rc = kb_surrogate_loss_backward(s, input, target, n, loss_out, stream)) return rc;
+    return kb_surrogate_adam(s, lr, 0.9f, 0.999f, 1e-8f, step, stream);
+}
+
+int kb_surrogate_status(kb_surrogate *s, int *timed_out, void *stream) {
+    KB_REQUIRE(s && timed_out, "kb_surrogate_status: null argument");
+    cudaStream_t st = kb::as_stream(stream);
+    cudaMemcpyAsync(timed_out, s->err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return kb::check_launch("kb_surrogate_status");
+    return 0;
+}
+
+int kb_surrogate_flops(const kb_surrogate *s, int n, double *forward_flops, double *train_flops) {
+    KB_REQUIRE(s, "kb_surrogate_flops: null handle");
+    double f = 0.0, t = 0.0;
+    for (int i = 0; i < N_LAYERS; ++i) {
+        const Layer &l = s->L[i];
+        const double px = (double)n * s->H_at(l.level) * s->W_at(l.level);
+        const double one = 2.0 * px * l.cout * 9.0 * l.cin;
+        f += one;
+        t += one * (i == 0 ? 2.0 : 3.0);
+    }
+    if (forward_flops) *forward_flops = f;
+    if (train_flops) *train_flops = t;
+    return 0;
+}
+
+}  // extern "C"

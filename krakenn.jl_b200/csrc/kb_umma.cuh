@@ -1,0 +1,450 @@
+// kb_umma.cuh -- tcgen05 (UMMA) BF16 tensor-core mainloop for sm_100a, and the
+// operand loaders of the warm-start network's convolutions.
+//
+// One CTA = 128 threads (4 warps) computes one 128 x BN tile of D (FP32, in
+// TMEM) over a range of 64-wide K steps:
+//   * all 128 threads stage the A tile (128 x 64 BF16) and the B tile
+//     (BN x 64) of a K step into shared memory, in the canonical no-swizzle
+//     UMMA layout (16-byte rows, 8-row core matrices);
+//   * one thread issues four tcgen05.mma.cta_group::1.kind::f16 (M=128, N=BN,
+//     K=16) and commits them to the stage's mbarrier;
+//   * two stages alternate, so the loads of step k+1 overlap the MMAs of k;
+//   * the epilogue reads the accumulator with tcgen05.ld.32x32b (warp w owns
+//     TMEM lanes 32w..32w+31 = tile rows) and hands 8 columns at a time to the
+//     operation's store().
+//
+// Shared-memory layouts (both with SBO = 128 B between 8-row groups along
+// M/N and LBO = rows*16 B between 8-element groups along K):
+//   K-major : element (r, k) at (k/8)*rows*16 + r*16 + (k%8)*2
+//   MN-major: element (r, k) at (k/8)*rows*16 + (r/8)*128 + (k%8)*16 + (r%8)*2
+// A K-major 16-byte chunk is 8 consecutive k of one row; an MN-major chunk is
+// 8 consecutive rows of one k.  The instruction descriptor's a_major/b_major
+// bits select the layout per operand.
+//
+// Every wait is bounded.  A CTA that gives up records the failure in *err,
+// waits (bounded) for the MMAs it issued, frees its TMEM and returns.
+#pragma once
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace kb {
+namespace umma {
+
+constexpr int BM = 128, BK = 64, NT = 128, THREADS = 128;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor, no swizzle, sm_100 version field = 1.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// Instruction descriptor, kind::f16: D F32, A = B = BF16, M = 128.
+__host__ __device__ constexpr uint32_t idesc_bf16(int N, bool a_mn, bool b_mn) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) |
+           ((b_mn ? 1u : 0u) << 16) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit) {
+    const uint32_t a = smem_u32(bar);
+    for (long long it = 0; it < limit; ++it) {
+        uint32_t done = 0;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (it > 64) __nanosleep(64);
+    }
+    return false;
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
+    uint32_t r[8];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void st_chunk(unsigned char *smem, uint32_t off, uint4 v) {
+    *reinterpret_cast<uint4 *>(smem + off) = v;
+}
+
+struct Smem {
+    alignas(128) unsigned char a[2][BM * BK * 2];  // 2 x 16 KB
+    alignas(128) unsigned char b[2][NT * BK * 2];  // 2 x 16 KB
+    uint64_t bar[3];
+    uint32_t tmem;
+};
+
+__host__ __device__ constexpr uint32_t tmem_cols(int bn) { return bn <= 32 ? 32u : (bn <= 64 ? 64u : 128u); }
+
+// Op interface:
+//   static constexpr bool A_MN, B_MN;
+//   int bn;                                     N tile width (16..128, multiple of 16)
+//   __device__ void k_range(int &k0, int &k1)  K steps of this CTA
+//   __device__ void load_a(unsigned char *s, int kt)   stage the 128 x 64 A tile
+//   __device__ void load_b(unsigned char *s, int kt)   stage the bn x 64 B tile
+//   __device__ void store(int row, int col, const float *v)  8 columns of row
+template <class Op>
+__global__ void __launch_bounds__(THREADS) umma_k(const Op op, int *__restrict__ err, long long spin) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    Smem &S = *reinterpret_cast<Smem *>(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bn = op.bn;
+    const uint32_t cols = tmem_cols(bn);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&S.tmem)), "r"(cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(&S.bar[0], 1);
+        mbar_init(&S.bar[1], 1);
+        mbar_init(&S.bar[2], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = S.tmem;
+    const uint32_t idesc = idesc_bf16(bn, Op::A_MN, Op::B_MN);
+    int k0, k1;
+    op.k_range(k0, k1);
+    uint32_t phase[2] = {0u, 0u};
+    bool ok = true;
+    const uint32_t lbo_a = BM * 16, lbo_b = (uint32_t)bn * 16;
+
+    for (int kt = k0; kt < k1; ++kt) {
+        const int s = (kt - k0) & 1;
+        bool free_stage = true;
+        if (kt - k0 >= 2) {  // the MMAs that read this stage two steps ago
+            free_stage = mbar_wait(&S.bar[s], phase[s], spin);
+            phase[s] ^= 1u;
+        }
+        if (free_stage) {
+            op.load_a(S.a[s], kt);
+            op.load_b(S.b[s], kt);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        // one barrier per step; it also makes a timeout a block-uniform exit
+        if (!__syncthreads_and(free_stage ? 1 : 0)) {
+            ok = false;
+            break;
+        }
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = smem_u32(S.a[s]), sb = smem_u32(S.b[s]);
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk) {
+                const uint64_t da = sdesc(sa + kk * 2 * lbo_a, lbo_a, 128);
+                const uint64_t db = sdesc(sb + kk * 2 * lbo_b, lbo_b, 128);
+                mma_bf16(tmem, da, db, idesc, (kt > k0 || kk > 0) ? 1u : 0u);
+            }
+            mma_commit(&S.bar[s]);
+        }
+    }
+    // One more commit tracks every MMA this thread issued; wait for it on all
+    // paths (also after a timeout) before reading or freeing TMEM.
+    const bool issued = k1 > k0;
+    if (threadIdx.x == 0 && issued) mma_commit(&S.bar[2]);
+    bool drained = !issued || mbar_wait(&S.bar[2], 0u, spin);
+    ok = ok && drained;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __syncthreads();
+    const bool all_ok = __syncthreads_and(ok ? 1 : 0);
+    const int row = warp * 32 + lane;
+    if (!all_ok) {
+        if (threadIdx.x == 0) atomicExch(err, 1);
+    } else if (issued) {
+        for (int c0 = 0; c0 < bn; c0 += 8) {
+            float v[8];
+            tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            op.store(row, c0, v);
+        }
+    } else {
+        const float z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int c0 = 0; c0 < bn; c0 += 8) op.store(row, c0, z);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cols));
+}
+
+inline size_t smem_bytes() { return sizeof(Smem) + 1024; }
+
+// ---------------------------------------------------------------------------
+// Activation view: the input of a 3x3 convolution at resolution H x W, NHWC
+// BF16.  Channels [0, c1) come from s1, stored at (H >> up1) x (W >> up1)
+// (nearest-neighbour upsampling when up1 = 1); channels [c1, c1 + c2) come from
+// s2 at H x W.  This is the decoder's "upsample, then concatenate the skip"
+// without materialising either.
+struct ActView {
+    const __nv_bfloat16 *s1;
+    const __nv_bfloat16 *s2;
+    int c1, c2, up1;
+    int B, H, W;
+    __device__ __forceinline__ int C() const { return c1 + c2; }
+    // 8 channels [c, c+8) of pixel (b, h, w); zero outside the image.
+    __device__ __forceinline__ uint4 chunk(int b, int h, int w, int c) const {
+        if (h < 0 || h >= H || w < 0 || w >= W) return make_uint4(0, 0, 0, 0);
+        if (c < c1) {
+            const int Hs = H >> up1, Ws = W >> up1;
+            const size_t p = ((size_t)b * Hs + (h >> up1)) * Ws + (w >> up1);
+            return __ldg(reinterpret_cast<const uint4 *>(s1 + p * c1 + c));
+        }
+        const size_t p = ((size_t)b * H + h) * W + w;
+        return __ldg(reinterpret_cast<const uint4 *>(s2 + p * c2 + (c - c1)));
+    }
+};
+
+__device__ __forceinline__ void pixel_of(int m, int H, int W, int &b, int &h, int &w) {
+    const int hw = H * W;
+    b = m / hw;
+    const int r = m - b * hw;
+    h = r / W;
+    w = r - h * W;
+}
+
+// Convolution forward (and data gradient): D[m, n] = sum_k X9[m, k] Wt[n, k],
+// k = tap * C + c, tap = (dy + 1) * 3 + (dx + 1), X9[m, k] = X[pixel m shifted
+// by (dy, dx), channel c].  Wt is [Nout][Kp] BF16 with Kp = roundup(9 C, 64).
+// Epilogue: + bias, ReLU, multiply by (mask view > 0), store BF16 or FP32.
+struct ConvOp {
+    static constexpr bool A_MN = false, B_MN = false;
+    ActView x;
+    const __nv_bfloat16 *wt;  // [Nout][Kp]
+    const float *bias;        // [Nout] or null
+    ActView mask;             // mask.s1 == null: no mask
+    void *out;                // [M][Nout] BF16 or FP32
+    int M, Nout, Kp, bn, relu, out_f32, nsteps;
+
+    __device__ void k_range(int &k0, int &k1) const { k0 = 0; k1 = nsteps; }
+
+    __device__ void load_a(unsigned char *s, int kt) const {
+        const int r = threadIdx.x;  // one tile row (pixel) per thread
+        const int m = blockIdx.x * BM + r;
+        const int C = x.C(), K9 = 9 * C;
+        int b = 0, h = 0, w = 0;
+        const bool live = m < M;
+        if (live) pixel_of(m, x.H, x.W, b, h, w);
+#pragma unroll
+        for (int kc = 0; kc < 8; ++kc) {
+            const int k = kt * BK + kc * 8;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (live && k < K9) {
+                const int t = k / C, c = k - t * C;
+                v = x.chunk(b, h + t / 3 - 1, w + t % 3 - 1, c);
+            }
+            st_chunk(s, (uint32_t)(kc * BM * 16 + r * 16), v);
+        }
+    }
+
+    __device__ void load_b(unsigned char *s, int kt) const {
+        const int n0 = blockIdx.y * bn;
+        for (int c = threadIdx.x; c < bn * 8; c += THREADS) {
+            const int r = c % bn, kc = c / bn;
+            const uint4 v =
+                __ldg(reinterpret_cast<const uint4 *>(wt + (size_t)(n0 + r) * Kp + kt * BK + kc * 8));
+            st_chunk(s, (uint32_t)(kc * bn * 16 + r * 16), v);
+        }
+    }
+
+    __device__ void store(int row, int col, const float *v) const {
+        const int m = blockIdx.x * BM + row;
+        if (m >= M) return;
+        const int n = blockIdx.y * bn + col;
+        float o[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            float t = v[i] + (bias ? bias[n + i] : 0.f);
+            o[i] = relu ? fmaxf(t, 0.f) : t;
+        }
+        if (mask.s1) {
+            int b, h, w;
+            pixel_of(m, mask.H, mask.W, b, h, w);
+            const uint4 mv = mask.chunk(b, h, w, n);
+            const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&mv);
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                if (!(__bfloat162float(mb[i]) > 0.f)) o[i] = 0.f;
+        }
+        if (out_f32) {
+            float4 *d = reinterpret_cast<float4 *>((float *)out + (size_t)m * Nout + n);
+            d[0] = make_float4(o[0], o[1], o[2], o[3]);
+            d[1] = make_float4(o[4], o[5], o[6], o[7]);
+        } else {
+            __align__(16) __nv_bfloat162 p[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) p[i] = __floats2bfloat162_rn(o[2 * i], o[2 * i + 1]);
+            *reinterpret_cast<uint4 *>((__nv_bfloat16 *)out + (size_t)m * Nout + n) =
+                *reinterpret_cast<const uint4 *>(p);
+        }
+    }
+};
+
+// Weight gradient, split over pixels:
+//   P[z][r, n] = sum_{m in split z} X9[m, r] dY[m, n],  r = tap * C + c,
+// plus one extra row r = 9C whose A operand is 1, giving the bias gradient
+// sum_m dY[m, n].  Both operands are staged MN-major: a 16-byte chunk is 8
+// consecutive channels of one pixel, which is contiguous in NHWC.
+struct WgradOp {
+    static constexpr bool A_MN = true, B_MN = true;
+    ActView x;
+    const __nv_bfloat16 *dy;  // [M][Nout]
+    float *part;              // [splits][9C + 1][Nout]
+    int M, Nout, bn, steps_per_split, nsteps;
+
+    __device__ void k_range(int &k0, int &k1) const {
+        k0 = blockIdx.z * steps_per_split;
+        k1 = min(nsteps, k0 + steps_per_split);
+    }
+
+    __device__ void load_a(unsigned char *s, int kt) const {
+        const int C = x.C(), R = 9 * C;
+        const int k_lo = threadIdx.x & 7, g = (threadIdx.x >> 3) & 15;
+        const int r = blockIdx.x * BM + g * 8;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int m = kt * BK + i * 8 + k_lo;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (m < M) {
+                if (r < R) {
+                    int b, h, w;
+                    pixel_of(m, x.H, x.W, b, h, w);
+                    const int t = r / C, c = r - t * C;
+                    v = x.chunk(b, h + t / 3 - 1, w + t % 3 - 1, c);
+                } else if (r == R) {
+                    v.x = 0x3F80u;  // bf16 1.0 in element 0 of the chunk
+                }
+            }
+            st_chunk(s, (uint32_t)(i * BM * 16 + g * 128 + k_lo * 16), v);
+        }
+    }
+
+    __device__ void load_b(unsigned char *s, int kt) const {
+        const int groups = bn >> 3, n0 = blockIdx.y * bn;
+        for (int c = threadIdx.x; c < bn * 8; c += THREADS) {
+            const int k_lo = c & 7, g = (c >> 3) % groups, k_hi = (c >> 3) / groups;
+            const int m = kt * BK + k_hi * 8 + k_lo;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (m < M) v = __ldg(reinterpret_cast<const uint4 *>(dy + (size_t)m * Nout + n0 + g * 8));
+            st_chunk(s, (uint32_t)(k_hi * bn * 16 + g * 128 + k_lo * 16), v);
+        }
+    }
+
+    __device__ void store(int row, int col, const float *v) const {
+        const int R = 9 * x.C();
+        const int r = blockIdx.x * BM + row;
+        if (r > R) return;
+        const int n = blockIdx.y * bn + col;
+        float4 *d = reinterpret_cast<float4 *>(part + ((size_t)blockIdx.z * (R + 1) + r) * Nout + n);
+        d[0] = make_float4(v[0], v[1], v[2], v[3]);
+        d[1] = make_float4(v[4], v[5], v[6], v[7]);
+    }
+};
+
+// Plain GEMM for testing both operand majors: C[M][N] = A B^T in FP32, with A
+// stored [M][K] (K-major) or [K][M] (MN-major), B stored [N][K] or [K][N].
+template <bool AMN, bool BMN>
+struct GemmOp {
+    static constexpr bool A_MN = AMN, B_MN = BMN;
+    const __nv_bfloat16 *a, *b;
+    float *c;
+    int M, N, K, bn;
+
+    __device__ void k_range(int &k0, int &k1) const { k0 = 0; k1 = K / BK; }
+
+    __device__ static void load(unsigned char *s, const __nv_bfloat16 *src, int rows, int r0,
+                                int ld_rows, int K, int kt, bool mn) {
+        for (int c = threadIdx.x; c < rows * 8; c += THREADS) {
+            uint32_t off;
+            const __nv_bfloat16 *p;
+            if (!mn) {  // chunk = row r, k chunk kc
+                const int r = c % rows, kc = c / rows;
+                p = src + (size_t)(r0 + r) * K + kt * BK + kc * 8;
+                off = (uint32_t)(kc * rows * 16 + r * 16);
+            } else {    // chunk = 8 rows of one k
+                const int groups = rows >> 3;
+                const int k_lo = c & 7, g = (c >> 3) % groups, k_hi = (c >> 3) / groups;
+                p = src + (size_t)(kt * BK + k_hi * 8 + k_lo) * ld_rows + r0 + g * 8;
+                off = (uint32_t)(k_hi * rows * 16 + g * 128 + k_lo * 16);
+            }
+            st_chunk(s, off, __ldg(reinterpret_cast<const uint4 *>(p)));
+        }
+    }
+    __device__ void load_a(unsigned char *s, int kt) const { load(s, a, BM, blockIdx.x * BM, M, K, kt, AMN); }
+    __device__ void load_b(unsigned char *s, int kt) const { load(s, b, bn, blockIdx.y * bn, N, K, kt, BMN); }
+    __device__ void store(int row, int col, const float *v) const {
+        const int m = blockIdx.x * BM + row, n = blockIdx.y * bn + col;
+        float4 *d = reinterpret_cast<float4 *>(c + (size_t)m * N + n);
+        d[0] = make_float4(v[0], v[1], v[2], v[3]);
+        d[1] = make_float4(v[4], v[5], v[6], v[7]);
+    }
+};
+
+}  // namespace umma
+}  // namespace kb
+
+namespace kb {
+namespace umma {
+
+// Largest multiple of 16 that is <= 128 and divides n (0 if none).
+int pick_bn(int n);
+
+// Launch umma_k<Op> with the dynamic shared memory it needs.  The attribute
+// is set once per device and instantiation.
+template <class Op>
+int launch(const Op &op, dim3 grid, int *err, cudaStream_t stream, long long spin = 1ll << 22) {
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(umma_k<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem_bytes());
+        if (e != cudaSuccess) return kb::check_launch("umma_k: shared-memory attribute");
+        configured[dev] = true;
+    }
+    umma_k<Op><<<grid, THREADS, smem_bytes(), stream>>>(op, err, spin);
+    return 0;
+}
+
+}  // namespace umma
+}  // namespace kb

@@ -1,0 +1,171 @@
+"""The learned warm start on the GPU: the tcgen05 GEMM in both operand
+majors, the network's forward pass and gradients against the FP64 numpy
+oracle, the equilibrium initialiser against the C oracle, and a small
+end-to-end run in which the trained network shortens the time to steady."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import unet_oracle as U
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def sur(pkg):
+    from importlib import import_module
+    return import_module(pkg.__name__ + ".surrogate")
+
+
+def _bf16(shape, gen):
+    return torch.randn(shape, generator=gen).to(torch.bfloat16).cuda()
+
+
+@pytest.mark.parametrize("a_mn,b_mn", [(0, 0), (1, 1), (1, 0), (0, 1)])
+@pytest.mark.parametrize("N,K", [(16, 64), (48, 128), (96, 192), (128, 64), (256, 320)])
+def test_gemm_bf16_both_majors(cuda, pkg, a_mn, b_mn, N, K):
+    """C = A B^T on tcgen05 with FP32 accumulation equals the FP64 product of
+    the same BF16 operands to FP32 summation error."""
+    import ctypes as C
+    from importlib import import_module
+    lib = import_module(pkg.__name__ + "._lib")
+    M = 256
+    g = torch.Generator().manual_seed(N * 1000 + K)
+    A, B = _bf16((M, K), g), _bf16((N, K), g)
+    a = A.t().contiguous() if a_mn else A
+    b = B.t().contiguous() if b_mn else B
+    out = torch.full((M, N), float("nan"), dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    lib.call("kb_gemm_bf16", C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()),
+             C.c_void_p(out.data_ptr()), M, N, K, a_mn, b_mn, C.c_void_p(err.data_ptr()),
+             C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    ref = A.double() @ B.double().t()
+    assert int(err.item()) == 0
+    tol = 1e-5 * float(ref.abs().max())
+    assert float((out.double() - ref).abs().max()) <= tol
+
+
+def test_gemm_bf16_rejects_bad_shapes(cuda, pkg):
+    import ctypes as C
+    from importlib import import_module
+    lib = import_module(pkg.__name__ + "._lib")
+    a = torch.zeros((128, 64), dtype=torch.bfloat16, device="cuda")
+    out = torch.zeros((128, 24), dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    with pytest.raises(lib.KrakenArgumentError):
+        lib.call("kb_gemm_bf16", C.c_void_p(a.data_ptr()), C.c_void_p(a.data_ptr()),
+                 C.c_void_p(out.data_ptr()), 128, 24, 64, 0, 0, C.c_void_p(err.data_ptr()), None)
+
+
+def _net_case(sur, C=16, H=32, W=32, n=2, seed=3):
+    model = sur.Surrogate(max_batch=4, H=H, W=W, base_channels=C, seed=seed)
+    table, npar = U.layer_table(C)
+    assert npar == model.n_params
+    p = model.params().double().cpu().numpy()
+    rng = np.random.default_rng(seed)
+    for cin, cout, wo, bo in table:
+        p[bo:bo + cout] = rng.normal(0.0, 0.05, cout)
+    model.set_params(torch.from_numpy(p))
+    re = np.array([150.0, 2000.0, 400.0, 900.0])[:n]
+    x = model.inputs(re, n_nodes=256)
+    # parameters as the tensor cores see them: weights rounded to BF16, biases FP32
+    pq = p.copy()
+    for cin, cout, wo, bo in table:
+        pq[wo:bo] = torch.from_numpy(p[wo:bo]).to(torch.bfloat16).double().numpy()
+    xo = x.double().cpu().numpy()
+    tgt = np.empty((n, 3, H, W))
+    tgt[:, 0] = 1.0 + 0.02 * rng.normal(size=(n, H, W))
+    tgt[:, 1:] = 0.1 * rng.normal(size=(n, 2, H, W))
+    return model, x, xo, pq, tgt, table
+
+
+def test_network_inputs_match_oracle(cuda, sur):
+    model = sur.Surrogate(max_batch=3, H=16, W=24, base_channels=16)
+    re = [100.0, 640.0, 3200.0]
+    x = model.inputs(re, n_nodes=256).double().cpu().numpy()
+    xo = U.cavity_inputs(re, 16, 24, 256)
+    assert np.max(np.abs(x - xo)) <= 4e-3  # BF16 rounding of the coordinates
+    assert np.array_equal(x[..., :2], xo[..., :2])
+    model.close()
+
+
+def test_network_forward_matches_oracle(cuda, sur):
+    model, x, xo, pq, tgt, _ = _net_case(sur)
+    out = model.infer(x).double().cpu().numpy()
+    ref, _ = U.forward(pq, xo, 16)
+    sc = np.array(model.scale)[None, :, None, None]
+    off = np.array(model.offset)[None, :, None, None]
+    got = (out - off) * sc                      # back to the normalised head output
+    want = np.moveaxis(ref[..., :3], -1, 1)
+    rel = np.linalg.norm(got - want) / np.linalg.norm(want)
+    assert rel < 3e-2, rel
+    assert not model.timed_out()
+    model.close()
+
+
+def test_network_gradients_match_oracle(cuda, sur):
+    """Per-layer parameter gradients of the MSE loss (BF16 activations and
+    gradients, FP32 accumulation) against the FP64 oracle on the same BF16
+    weights: relative L2 error below 0.1 and cosine above 0.99."""
+    model, x, xo, pq, tgt, table = _net_case(sur)
+    loss = model.loss_backward(x, torch.from_numpy(tgt).float())
+    g = model.grads().double().cpu().numpy()
+    lo, go = U.loss_and_grad(pq, xo, tgt, model.scale, model.offset, 16)
+    assert abs(float(loss.item()) - lo) <= 2e-2 * lo
+    for li, (cin, cout, wo, bo) in enumerate(table):
+        a, b = g[wo:bo + cout], go[wo:bo + cout]
+        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+        cos = float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b)))
+        assert rel < 0.1 and cos > 0.99, (li, rel, cos)
+    assert not model.timed_out()
+    model.close()
+
+
+def test_init_equilibrium_matches_oracle(cuda, pkg, orc):
+    Nx, Ny = 17, 13
+    rng = np.random.default_rng(4)
+    rho = 1.0 + 0.01 * rng.normal(size=(Ny, Nx))
+    ux, uy = 0.05 * rng.normal(size=(2, Ny, Nx))
+    f = torch.empty((9, Ny, Nx), dtype=torch.float64, device="cuda")
+    import ctypes as C
+    from importlib import import_module
+    lib = import_module(pkg.__name__ + "._lib")
+    t = [torch.from_numpy(a).cuda() for a in (rho, ux, uy)]
+    lib.call("kb_init_equilibrium_2d", C.c_void_p(f.data_ptr()), *(C.c_void_p(a.data_ptr()) for a in t),
+             lib.KB_F64, Nx, Ny, lib.KB_F64, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    got = f.cpu().numpy()
+    for q in range(9):
+        for j in range(Ny):
+            for i in range(Nx):
+                assert got[q, j, i] == orc.equilibrium_d2q9(rho[j, i], ux[j, i], uy[j, i], q)
+
+
+def test_trained_network_shortens_time_to_steady(cuda, sur):
+    """32 x 32 cavities, Re in [50, 300]: train on 48 steady fields from the
+    batched kernel, then run 4 held-out cases to r_u <= 1e-8 with the plain
+    FP64 MRT step from rest and from the network's prediction.  The warm
+    start needs fewer steps in total and lands on the same field."""
+    N = 32
+    re_tr, re_te = sur.held_out_split(48, 4, re_range=(50.0, 300.0), seed=7)
+    fields, info = sur.steady_cavities(re_tr, N, storage="f32", max_steps=100000, tol=1e-7,
+                                       check_every=200)
+    assert all(s != "non-finite" for _, _, s in info)
+    model = sur.Surrogate(max_batch=16, H=N, W=N, base_channels=16, seed=1)
+    hist = sur.train(model, re_tr, fields, epochs=60, batch=16, lr=2e-3, lr_min=1e-4)
+    assert hist[-1] < 0.1 * hist[0], hist[::10]
+    pred = model.infer(model.inputs(re_te, n_nodes=N))
+    cold = [sur.PlainCavity(N, 0.1 * N / r, 0.1, check_every=100) for r in re_te]
+    warm = [sur.PlainCavity(N, 0.1 * N / r, 0.1, check_every=100, init=pred[c])
+            for c, r in enumerate(re_te)]
+    sur.run_to_steady(cold, tol=1e-8, max_steps=400000, check_every=100)
+    sur.run_to_steady(warm, tol=1e-8, max_steps=400000, check_every=100)
+    sc = sum(c.steps for c in cold)
+    sw = sum(c.steps for c in warm)
+    assert all(c.residual <= 1e-8 for c in cold + warm)
+    assert sw < 0.9 * sc, (sw, sc, [c.steps for c in cold], [c.steps for c in warm])
+    for c, w in zip(cold, warm):
+        d = (c.fields() - w.fields()).abs()
+        assert float(d[1:].max()) / 0.1 < 1e-4
+    assert not model.timed_out()
+    model.close()
