@@ -634,6 +634,97 @@ def bench_natconv_validation(pkg, N=512, steps_by_ra=None):
     return res
 
 
+def bench_warmstart(pkg, N=256, n_train=2000, n_test=64, epochs=40, batch=16, base=32,
+                    data_steps=300000, data_tol=1e-6, tol=1e-8, max_steps=3000000,
+                    check_every=1000, seed=0):
+    """Learned warm start: train the encoder-decoder on n_train steady N^2
+    cavities from the batched kernel (Re log-uniform [100, 3200], u_lid 0.1),
+    then run n_test held-out cases to r_u <= tol with the plain FP64 MRT step
+    from rest (cold) and from the predicted field (warm).  Reports the data,
+    training and inference throughput, the steps and wall time to steady of
+    both starts, and the converged-field difference."""
+    import numpy as np
+    import torch
+    from importlib import import_module
+    sur = import_module(pkg.__name__ + ".surrogate")
+    out = {"workload": f"learned warm start, {N}^2 lid-driven MRT cavities, Re log-uniform "
+                       f"[100,3200], u_lid=0.1; {n_train} training / {n_test} held-out cases; "
+                       f"4-level U-Net, {base} base channels, BF16 tcgen05, batch {batch}, "
+                       f"{epochs} epochs; plain FP64 MRT to r_u <= {tol:g}"}
+    re_tr, re_te = sur.held_out_split(n_train, n_test, seed=seed)
+    e0, e1 = _events()
+    e0.record()
+    fields, info = sur.steady_cavities(re_tr, N, storage="f32", max_steps=data_steps,
+                                       tol=data_tol, check_every=500)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    steps = np.array([s for s, _, _ in info])
+    states = [st for _, _, st in info]
+    out["data"] = {"storage": "f32 f-w, FP32 MRT", "ms": round(ms, 1),
+                   "mlups": round(float(steps.sum()) * N * N / (ms * 1e-3) / 1e6, 1),
+                   "steps_min_median_max": [int(steps.min()), int(np.median(steps)), int(steps.max())],
+                   "states": {k: states.count(k) for k in set(states)}}
+    ok = torch.tensor([st != "non-finite" for st in states])
+    keep = torch.nonzero(ok).flatten()
+    fields = fields.index_select(0, keep.cuda())
+    re_tr = re_tr[keep.numpy()]
+    model = sur.Surrogate(max_batch=batch, H=N, W=N, base_channels=base, seed=seed)
+    e0.record()
+    hist = sur.train(model, re_tr, fields, epochs=epochs, batch=batch, lr=1e-3, lr_min=2e-5)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    nsteps = epochs * (len(re_tr) // batch)
+    _, tfl = model.flops(batch)
+    out["train"] = {"params": model.n_params, "steps": nsteps, "ms": round(ms, 1),
+                    "tflops": round(tfl * nsteps / (ms * 1e-3) / 1e12, 1),
+                    "loss_first_last": [hist[0], hist[-1]], "timed_out": model.timed_out()}
+    del fields
+    torch.cuda.synchronize()
+    # held-out: predicted fields (timed), then cold and warm plain runs
+    e0.record()
+    preds = []
+    for i in range(0, n_test, batch):
+        x = model.inputs(re_te[i:i + batch], n_nodes=N)
+        preds.append(model.infer(x))
+    pred = torch.cat(preds)
+    e1.record()
+    torch.cuda.synchronize()
+    infer_ms = e0.elapsed_time(e1)
+    cold = [sur.PlainCavity(N, 0.1 * N / r, 0.1, check_every=check_every) for r in re_te]
+    t_cold = sur.run_to_steady(cold, tol=tol, max_steps=max_steps, check_every=check_every)
+    warm = [sur.PlainCavity(N, 0.1 * N / r, 0.1, check_every=check_every, init=pred[c])
+            for c, r in enumerate(re_te)]
+    t_warm = sur.run_to_steady(warm, tol=tol, max_steps=max_steps, check_every=check_every)
+    sc = np.array([c.steps for c in cold])
+    sw = np.array([c.steps for c in warm])
+    conv = [c.residual <= tol for c in cold + warm]
+    dmax, drho, pred_err = [], [], []
+    for k, (c, w) in enumerate(zip(cold, warm)):
+        fc, fw = c.fields(), w.fields()
+        dmax.append(float((fc[1:] - fw[1:]).abs().max()) / 0.1)
+        drho.append(float((fc[0] - fw[0]).abs().max()))
+        pe = (pred[k, 1:].double() - fc[1:]).norm() / fc[1:].norm()
+        pred_err.append(float(pe))
+        c.close()
+        w.close()
+    out["held_out"] = {
+        "inference_ms": round(infer_ms, 2),
+        "prediction_l2_rel_u_vs_converged": [float(np.min(pred_err)), float(np.median(pred_err)),
+                                             float(np.max(pred_err))],
+        "cold_steps_total": int(sc.sum()), "warm_steps_total": int(sw.sum()),
+        "steps_ratio": round(float(sc.sum()) / max(1, float(sw.sum())), 3),
+        "per_case_steps_ratio_min_median_max": [float(np.min(sc / sw)), float(np.median(sc / sw)),
+                                                float(np.max(sc / sw))],
+        "cold_wall_s": round(t_cold, 2), "warm_wall_s_incl_inference": round(t_warm + infer_ms * 1e-3, 2),
+        "wall_ratio": round(t_cold / (t_warm + infer_ms * 1e-3), 3),
+        "all_converged": bool(all(conv)),
+        "converged_max_du_over_ulid": max(dmax), "converged_max_drho": max(drho)}
+    model.close()
+    return out
+
+
 def _extrude(plane, n):
     import torch
     out = torch.empty((19, n, n, n), dtype=plane.dtype, device=plane.device)
@@ -654,6 +745,9 @@ def run_other(args):
             r = bench_cavity2d(pkg, steps=max(args.steps, 200) // 200 * 200)
     elif args.workload == "batch":
         r = bench_batch(pkg, rank=rank, world=world, error_cases=8 if world == 1 else 0)
+    elif args.workload == "warmstart":
+        if rank == 0:
+            r = bench_warmstart(pkg)
     elif rank == 0:
         r = bench_natconv_validation(pkg)
     if rank == 0:
@@ -677,7 +771,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the short measurements of the other configurations")
-    ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "cavity2d", "batch", "natconv"])
+    ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "cavity2d", "batch", "natconv", "warmstart"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -4,11 +4,13 @@
 // One CTA = 128 threads (4 warps) computes one 128 x BN tile of D (FP32, in
 // TMEM) over a range of 64-wide K steps:
 //   * all 128 threads stage the A tile (128 x 64 BF16) and the B tile
-//     (BN x 64) of a K step into shared memory, in the canonical no-swizzle
-//     UMMA layout (16-byte rows, 8-row core matrices);
+//     (BN x 64) of a K step into shared memory with 16-byte cp.async copies
+//     (zero-fill for padding), in the canonical no-swizzle UMMA layout
+//     (16-byte rows, 8-row core matrices);
 //   * one thread issues four tcgen05.mma.cta_group::1.kind::f16 (M=128, N=BN,
 //     K=16) and commits them to the stage's mbarrier;
-//   * two stages alternate, so the loads of step k+1 overlap the MMAs of k;
+//   * STAGES shared-memory stages rotate: while the tensor core works on step
+//     k, the copies of steps k+1 .. k+STAGES-1 are in flight;
 //   * the epilogue reads the accumulator with tcgen05.ld.32x32b (warp w owns
 //     TMEM lanes 32w..32w+31 = tile rows) and hands 8 columns at a time to the
 //     operation's store().
@@ -101,14 +103,22 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
     for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void st_chunk(unsigned char *smem, uint32_t off, uint4 v) {
-    *reinterpret_cast<uint4 *>(smem + off) = v;
+// 16-byte asynchronous global->shared copy; valid = false writes zeros (the
+// source pointer must still be a valid address; callers pass a tensor base).
+__device__ __forceinline__ void cp16(uint32_t saddr, const void *g, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr), "l"(g),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
 }
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+constexpr int STAGES = 3;
 struct Smem {
-    alignas(128) unsigned char a[2][BM * BK * 2];  // 2 x 16 KB
-    alignas(128) unsigned char b[2][NT * BK * 2];  // 2 x 16 KB
-    uint64_t bar[3];
+    alignas(128) unsigned char a[STAGES][BM * BK * 2];  // 16 KB per stage
+    alignas(128) unsigned char b[STAGES][NT * BK * 2];  // 16 KB per stage
+    uint64_t bar[STAGES + 1];
     uint32_t tmem;
 };
 
@@ -118,8 +128,8 @@ __host__ __device__ constexpr uint32_t tmem_cols(int bn) { return bn <= 32 ? 32u
 //   static constexpr bool A_MN, B_MN;
 //   int bn;                                     N tile width (16..128, multiple of 16)
 //   __device__ void k_range(int &k0, int &k1)  K steps of this CTA
-//   __device__ void load_a(unsigned char *s, int kt)   stage the 128 x 64 A tile
-//   __device__ void load_b(unsigned char *s, int kt)   stage the bn x 64 B tile
+//   __device__ void load_a(uint32_t s, int kt)  cp.async the 128 x 64 A tile to smem s
+//   __device__ void load_b(uint32_t s, int kt)  cp.async the bn x 64 B tile
 //   __device__ void store(int row, int col, const float *v)  8 columns of row
 template <class Op>
 __global__ void __launch_bounds__(THREADS) umma_k(const Op op, int *__restrict__ err, long long spin) {
@@ -135,9 +145,7 @@ __global__ void __launch_bounds__(THREADS) umma_k(const Op op, int *__restrict__
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (threadIdx.x == 0) {
-        mbar_init(&S.bar[0], 1);
-        mbar_init(&S.bar[1], 1);
-        mbar_init(&S.bar[2], 1);
+        for (int i = 0; i <= STAGES; ++i) mbar_init(&S.bar[i], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -147,47 +155,64 @@ __global__ void __launch_bounds__(THREADS) umma_k(const Op op, int *__restrict__
     const uint32_t idesc = idesc_bf16(bn, Op::A_MN, Op::B_MN);
     int k0, k1;
     op.k_range(k0, k1);
-    uint32_t phase[2] = {0u, 0u};
-    bool ok = true;
+    const int n = k1 - k0;
     const uint32_t lbo_a = BM * 16, lbo_b = (uint32_t)bn * 16;
+    const uint32_t sa0 = smem_u32(S.a[0]), sb0 = smem_u32(S.b[0]);
+    constexpr uint32_t SA = BM * BK * 2, SB = NT * BK * 2;
 
-    for (int kt = k0; kt < k1; ++kt) {
-        const int s = (kt - k0) & 1;
-        bool free_stage = true;
-        if (kt - k0 >= 2) {  // the MMAs that read this stage two steps ago
-            free_stage = mbar_wait(&S.bar[s], phase[s], spin);
-            phase[s] ^= 1u;
+#pragma unroll
+    for (int i = 0; i < STAGES - 1; ++i) {
+        if (i < n) {
+            op.load_a(sa0 + i * SA, k0 + i);
+            op.load_b(sb0 + i * SB, k0 + i);
         }
-        if (free_stage) {
-            op.load_a(S.a[s], kt);
-            op.load_b(S.b[s], kt);
-        }
+        cp_commit();
+    }
+    uint32_t phase_bits = 0;
+    bool ok = true;
+    for (int i = 0; i < n; ++i) {
+        const int s = i % STAGES;
+        cp_wait<STAGES - 2>();  // this thread's copies of step i have landed
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         // one barrier per step; it also makes a timeout a block-uniform exit
-        if (!__syncthreads_and(free_stage ? 1 : 0)) {
+        if (!__syncthreads_and(ok ? 1 : 0)) {
             ok = false;
             break;
         }
         if (threadIdx.x == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t sa = smem_u32(S.a[s]), sb = smem_u32(S.b[s]);
+            const uint32_t sa = sa0 + s * SA, sb = sb0 + s * SB;
 #pragma unroll
             for (int kk = 0; kk < BK / 16; ++kk) {
                 const uint64_t da = sdesc(sa + kk * 2 * lbo_a, lbo_a, 128);
                 const uint64_t db = sdesc(sb + kk * 2 * lbo_b, lbo_b, 128);
-                mma_bf16(tmem, da, db, idesc, (kt > k0 || kk > 0) ? 1u : 0u);
+                mma_bf16(tmem, da, db, idesc, (i > 0 || kk > 0) ? 1u : 0u);
             }
             mma_commit(&S.bar[s]);
         }
+        // refill the stage that step i-1 used, once its MMAs are done
+        const int nx = i + STAGES - 1;
+        if (nx < n) {
+            const int sp = nx % STAGES;
+            if (i >= 1) {
+                ok = mbar_wait(&S.bar[sp], (phase_bits >> sp) & 1u, spin);
+                phase_bits ^= 1u << sp;
+            }
+            if (ok) {
+                op.load_a(sa0 + sp * SA, k0 + nx);
+                op.load_b(sb0 + sp * SB, k0 + nx);
+            }
+        }
+        cp_commit();
     }
+    cp_wait<0>();
     // One more commit tracks every MMA this thread issued; wait for it on all
     // paths (also after a timeout) before reading or freeing TMEM.
-    const bool issued = k1 > k0;
-    if (threadIdx.x == 0 && issued) mma_commit(&S.bar[2]);
-    bool drained = !issued || mbar_wait(&S.bar[2], 0u, spin);
+    const bool issued = n > 0;
+    if (threadIdx.x == 0 && issued) mma_commit(&S.bar[STAGES]);
+    const bool drained = !issued || mbar_wait(&S.bar[STAGES], 0u, spin);
     ok = ok && drained;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    __syncthreads();
     const bool all_ok = __syncthreads_and(ok ? 1 : 0);
     const int row = warp * 32 + lane;
     if (!all_ok) {
@@ -222,6 +247,20 @@ struct ActView {
     int c1, c2, up1;
     int B, H, W;
     __device__ __forceinline__ int C() const { return c1 + c2; }
+    // Address of channels [c, c+8) of pixel (b, h, w); valid = false (and a
+    // harmless address) outside the image.
+    __device__ __forceinline__ const __nv_bfloat16 *chunk_ptr(int b, int h, int w, int c,
+                                                              bool &valid) const {
+        valid = h >= 0 && h < H && w >= 0 && w < W;
+        if (!valid) return s1;
+        if (c < c1) {
+            const int Hs = H >> up1, Ws = W >> up1;
+            const size_t p = ((size_t)b * Hs + (h >> up1)) * Ws + (w >> up1);
+            return s1 + p * c1 + c;
+        }
+        const size_t p = ((size_t)b * H + h) * W + w;
+        return s2 + p * c2 + (c - c1);
+    }
     // 8 channels [c, c+8) of pixel (b, h, w); zero outside the image.
     __device__ __forceinline__ uint4 chunk(int b, int h, int w, int c) const {
         if (h < 0 || h >= H || w < 0 || w >= W) return make_uint4(0, 0, 0, 0);
@@ -234,6 +273,9 @@ struct ActView {
         return __ldg(reinterpret_cast<const uint4 *>(s2 + p * c2 + (c - c1)));
     }
 };
+
+// Source of the weight gradient's bias row: BF16 1.0 followed by seven zeros.
+static __device__ __align__(16) const unsigned short kOneChunk[8] = {0x3F80u, 0, 0, 0, 0, 0, 0, 0};
 
 __device__ __forceinline__ void pixel_of(int m, int H, int W, int &b, int &h, int &w) {
     const int hw = H * W;
@@ -258,7 +300,7 @@ struct ConvOp {
 
     __device__ void k_range(int &k0, int &k1) const { k0 = 0; k1 = nsteps; }
 
-    __device__ void load_a(unsigned char *s, int kt) const {
+    __device__ void load_a(uint32_t s, int kt) const {
         const int r = threadIdx.x;  // one tile row (pixel) per thread
         const int m = blockIdx.x * BM + r;
         const int C = x.C(), K9 = 9 * C;
@@ -268,22 +310,22 @@ struct ConvOp {
 #pragma unroll
         for (int kc = 0; kc < 8; ++kc) {
             const int k = kt * BK + kc * 8;
-            uint4 v = make_uint4(0, 0, 0, 0);
+            bool v = false;
+            const __nv_bfloat16 *p = x.s1;
             if (live && k < K9) {
                 const int t = k / C, c = k - t * C;
-                v = x.chunk(b, h + t / 3 - 1, w + t % 3 - 1, c);
+                p = x.chunk_ptr(b, h + t / 3 - 1, w + t % 3 - 1, c, v);
             }
-            st_chunk(s, (uint32_t)(kc * BM * 16 + r * 16), v);
+            cp16(s + (uint32_t)(kc * BM * 16 + r * 16), p, v);
         }
     }
 
-    __device__ void load_b(unsigned char *s, int kt) const {
+    __device__ void load_b(uint32_t s, int kt) const {
         const int n0 = blockIdx.y * bn;
         for (int c = threadIdx.x; c < bn * 8; c += THREADS) {
             const int r = c % bn, kc = c / bn;
-            const uint4 v =
-                __ldg(reinterpret_cast<const uint4 *>(wt + (size_t)(n0 + r) * Kp + kt * BK + kc * 8));
-            st_chunk(s, (uint32_t)(kc * bn * 16 + r * 16), v);
+            cp16(s + (uint32_t)(kc * bn * 16 + r * 16), wt + (size_t)(n0 + r) * Kp + kt * BK + kc * 8,
+                 true);
         }
     }
 
@@ -337,36 +379,38 @@ struct WgradOp {
         k1 = min(nsteps, k0 + steps_per_split);
     }
 
-    __device__ void load_a(unsigned char *s, int kt) const {
+    __device__ void load_a(uint32_t s, int kt) const {
         const int C = x.C(), R = 9 * C;
         const int k_lo = threadIdx.x & 7, g = (threadIdx.x >> 3) & 15;
         const int r = blockIdx.x * BM + g * 8;
+        const int t = r / C, c = r - t * C;
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const int m = kt * BK + i * 8 + k_lo;
-            uint4 v = make_uint4(0, 0, 0, 0);
+            bool v = false;
+            const void *p = x.s1;
             if (m < M) {
                 if (r < R) {
                     int b, h, w;
                     pixel_of(m, x.H, x.W, b, h, w);
-                    const int t = r / C, c = r - t * C;
-                    v = x.chunk(b, h + t / 3 - 1, w + t % 3 - 1, c);
+                    p = x.chunk_ptr(b, h + t / 3 - 1, w + t % 3 - 1, c, v);
                 } else if (r == R) {
-                    v.x = 0x3F80u;  // bf16 1.0 in element 0 of the chunk
+                    p = kOneChunk;  // bf16 1.0 in element 0: the bias row
+                    v = true;
                 }
             }
-            st_chunk(s, (uint32_t)(i * BM * 16 + g * 128 + k_lo * 16), v);
+            cp16(s + (uint32_t)(i * BM * 16 + g * 128 + k_lo * 16), p, v);
         }
     }
 
-    __device__ void load_b(unsigned char *s, int kt) const {
+    __device__ void load_b(uint32_t s, int kt) const {
         const int groups = bn >> 3, n0 = blockIdx.y * bn;
         for (int c = threadIdx.x; c < bn * 8; c += THREADS) {
             const int k_lo = c & 7, g = (c >> 3) % groups, k_hi = (c >> 3) / groups;
             const int m = kt * BK + k_hi * 8 + k_lo;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (m < M) v = __ldg(reinterpret_cast<const uint4 *>(dy + (size_t)m * Nout + n0 + g * 8));
-            st_chunk(s, (uint32_t)(k_hi * bn * 16 + g * 128 + k_lo * 16), v);
+            const bool v = m < M;
+            cp16(s + (uint32_t)(k_hi * bn * 16 + g * 128 + k_lo * 16),
+                 v ? (const void *)(dy + (size_t)m * Nout + n0 + g * 8) : (const void *)dy, v);
         }
     }
 
@@ -392,8 +436,8 @@ struct GemmOp {
 
     __device__ void k_range(int &k0, int &k1) const { k0 = 0; k1 = K / BK; }
 
-    __device__ static void load(unsigned char *s, const __nv_bfloat16 *src, int rows, int r0,
-                                int ld_rows, int K, int kt, bool mn) {
+    __device__ static void load(uint32_t s, const __nv_bfloat16 *src, int rows, int r0, int ld_rows,
+                                int K, int kt, bool mn) {
         for (int c = threadIdx.x; c < rows * 8; c += THREADS) {
             uint32_t off;
             const __nv_bfloat16 *p;
@@ -407,11 +451,11 @@ struct GemmOp {
                 p = src + (size_t)(kt * BK + k_hi * 8 + k_lo) * ld_rows + r0 + g * 8;
                 off = (uint32_t)(k_hi * rows * 16 + g * 128 + k_lo * 16);
             }
-            st_chunk(s, off, __ldg(reinterpret_cast<const uint4 *>(p)));
+            cp16(s + off, p, true);
         }
     }
-    __device__ void load_a(unsigned char *s, int kt) const { load(s, a, BM, blockIdx.x * BM, M, K, kt, AMN); }
-    __device__ void load_b(unsigned char *s, int kt) const { load(s, b, bn, blockIdx.y * bn, N, K, kt, BMN); }
+    __device__ void load_a(uint32_t s, int kt) const { load(s, a, BM, blockIdx.x * BM, M, K, kt, AMN); }
+    __device__ void load_b(uint32_t s, int kt) const { load(s, b, bn, blockIdx.y * bn, N, K, kt, BMN); }
     __device__ void store(int row, int col, const float *v) const {
         const int m = blockIdx.x * BM + row, n = blockIdx.y * bn + col;
         float4 *d = reinterpret_cast<float4 *>(c + (size_t)m * N + n);

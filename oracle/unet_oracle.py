@@ -96,22 +96,39 @@ def _pool_grad(d):
     return _up(d) * 0.25
 
 
+def bf16(x):
+    """Round to the nearest BFloat16 (ties to even) through FP32, as the GPU
+    rounds its FP32 accumulators when it stores BF16 tensors."""
+    a = np.ascontiguousarray(np.asarray(x, np.float64).astype(np.float32))
+    b = a.view(np.uint32)
+    r = ((b + np.uint32(0x7FFF) + ((b >> np.uint32(16)) & np.uint32(1))) &
+         np.uint32(0xFFFF0000)).astype(np.uint32)
+    return r.view(np.float32).astype(np.float64)
+
+
+def _ident(x):
+    return x
+
+
 def _layer_input(acts, in1, in2):
     return np.concatenate([_up(acts[in1]), acts[in2]], axis=-1) if in2 else acts[in1]
 
 
-def forward(params, x, C):
-    """Returns (head output [B,H,W,16], activations dict, pre-activations)."""
+def forward(params, x, C, round_bf16=False):
+    """Returns (head output [B,H,W,16], activations dict).  With round_bf16
+    every stored activation but the FP32 head output is rounded to BF16, at
+    the points where the CUDA kernels store BF16."""
+    rnd = bf16 if round_bf16 else _ident
     table, n = layer_table(C)
     assert params.size == n
     acts = {"in": np.asarray(x, np.float64)}
     for (in1, in2, o, relu, pooled), (cin, cout, wo, bo) in zip(LAYERS, table):
         if pooled:
-            acts[in1] = _pool(acts[POOL_OF[in1]])
+            acts[in1] = rnd(_pool(acts[POOL_OF[in1]]))
         X = _layer_input(acts, in1, in2)
         Wm = params[wo:wo + cout * 9 * cin].reshape(cout, 9 * cin)
         y = _im2col(X) @ Wm.T + params[bo:bo + cout]
-        acts[o] = np.maximum(y, 0.0) if relu else y
+        acts[o] = rnd(np.maximum(y, 0.0)) if relu else y
     return acts["out"], acts
 
 
@@ -121,23 +138,27 @@ def normalised_target(target, scale, offset):
     return (t - np.asarray(offset)) * np.asarray(scale)
 
 
-def loss_and_grad(params, x, target, scale, offset, C):
-    """Mean-squared error and its gradient with respect to the flat parameters."""
+def loss_and_grad(params, x, target, scale, offset, C, round_bf16=False):
+    """Mean-squared error and its gradient with respect to the flat
+    parameters.  With round_bf16 the activations and the activation gradients
+    are rounded to BF16 where the CUDA kernels store them (the head gradient,
+    each data gradient after its ReLU mask, the upsampling and skip sums);
+    weight gradients stay unrounded, as the kernels keep them in FP32."""
+    rnd = bf16 if round_bf16 else _ident
     table, n = layer_table(C)
-    out, acts = forward(params, x, C)
+    out, acts = forward(params, x, C, round_bf16)
     t = normalised_target(target, scale, offset)
     d = out[..., :3] - t
     M = d.shape[0] * d.shape[1] * d.shape[2]
     loss = float(np.sum(d * d) / (3 * M))
     grads = np.zeros(n)
     g = {"out": np.zeros_like(out)}
-    g["out"][..., :3] = 2.0 * d / (3 * M)
+    g["out"][..., :3] = rnd(2.0 * d / (3 * M))
+    dcat = {}
     for li in range(len(LAYERS) - 1, -1, -1):
         in1, in2, o, relu, pooled = LAYERS[li]
         cin, cout, wo, bo = table[li]
         dy = g[o]
-        if relu:
-            dy = dy * (acts[o] > 0)
         X = _layer_input(acts, in1, in2)
         cols = _im2col(X)
         Wm = params[wo:wo + cout * 9 * cin].reshape(cout, 9 * cin)
@@ -146,15 +167,19 @@ def loss_and_grad(params, x, target, scale, offset, C):
         if li == 0:
             break
         dX = _col2im(dy @ Wm, cin)
+        if not pooled:            # the input is a post-ReLU tensor (or a concat of two)
+            dX = rnd(dX * (X > 0))
+        else:
+            dX = rnd(dX)
         if in2:
             c1 = channels(in1, C)
-            g[in1] = g.get(in1, 0) + _up_grad(dX[..., :c1])
-            g[in2] = g.get(in2, 0) + dX[..., c1:]
+            g[in1] = rnd(_up_grad(dX[..., :c1]))
+            dcat[in2] = dX[..., c1:]
         else:
-            g[in1] = g.get(in1, 0) + dX
+            g[in1] = dX
         if pooled:
             src = POOL_OF[in1]
-            g[src] = g.get(src, 0) + _pool_grad(g[in1])
+            g[src] = rnd(dcat[src] + _pool_grad(g[in1]) * (acts[src] > 0))
     return loss, grads
 
 

@@ -91,33 +91,44 @@ def test_network_inputs_match_oracle(cuda, sur):
 
 
 def test_network_forward_matches_oracle(cuda, sur):
+    """Head output against the FP64 oracle run with BF16 rounding at the same
+    points as the kernels (tight), and against the unrounded FP64 network
+    (loose: 15 layers of BF16 activations)."""
     model, x, xo, pq, tgt, _ = _net_case(sur)
     out = model.infer(x).double().cpu().numpy()
-    ref, _ = U.forward(pq, xo, 16)
     sc = np.array(model.scale)[None, :, None, None]
     off = np.array(model.offset)[None, :, None, None]
     got = (out - off) * sc                      # back to the normalised head output
-    want = np.moveaxis(ref[..., :3], -1, 1)
-    rel = np.linalg.norm(got - want) / np.linalg.norm(want)
-    assert rel < 3e-2, rel
+    for rounded, tol in ((True, 5e-3), (False, 3e-2)):
+        ref, _ = U.forward(pq, xo, 16, round_bf16=rounded)
+        want = np.moveaxis(ref[..., :3], -1, 1)
+        rel = np.linalg.norm(got - want) / np.linalg.norm(want)
+        assert rel < tol, (rounded, rel)
     assert not model.timed_out()
     model.close()
 
 
 def test_network_gradients_match_oracle(cuda, sur):
-    """Per-layer parameter gradients of the MSE loss (BF16 activations and
-    gradients, FP32 accumulation) against the FP64 oracle on the same BF16
-    weights: relative L2 error below 0.1 and cosine above 0.99."""
+    """Per-layer parameter gradients of the MSE loss against the FP64 oracle
+    on the same BF16 weights.  With the oracle rounding activations and their
+    gradients to BF16 where the kernels do, only FP32 summation order differs:
+    relative L2 error below 2e-2 per layer.  Against the unrounded oracle the
+    BF16 noise of 15 layers shows (cosine above 0.98)."""
     model, x, xo, pq, tgt, table = _net_case(sur)
     loss = model.loss_backward(x, torch.from_numpy(tgt).float())
     g = model.grads().double().cpu().numpy()
-    lo, go = U.loss_and_grad(pq, xo, tgt, model.scale, model.offset, 16)
-    assert abs(float(loss.item()) - lo) <= 2e-2 * lo
+    lr_, gr = U.loss_and_grad(pq, xo, tgt, model.scale, model.offset, 16, round_bf16=True)
+    le, ge = U.loss_and_grad(pq, xo, tgt, model.scale, model.offset, 16)
+    assert abs(float(loss.item()) - lr_) <= 1e-3 * lr_
+    assert abs(float(loss.item()) - le) <= 2e-2 * le
+    worst = []
     for li, (cin, cout, wo, bo) in enumerate(table):
-        a, b = g[wo:bo + cout], go[wo:bo + cout]
+        a = g[wo:bo + cout]
+        b, c = gr[wo:bo + cout], ge[wo:bo + cout]
         rel = np.linalg.norm(a - b) / np.linalg.norm(b)
-        cos = float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b)))
-        assert rel < 0.1 and cos > 0.99, (li, rel, cos)
+        cos = float(a @ c / (np.linalg.norm(a) * np.linalg.norm(c)))
+        worst.append((li, round(rel, 5), round(cos, 5)))
+        assert rel < 2e-2 and cos > 0.98, worst
     assert not model.timed_out()
     model.close()
 
