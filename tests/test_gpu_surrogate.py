@@ -110,10 +110,11 @@ def test_network_forward_matches_oracle(cuda, sur):
 
 def test_network_gradients_match_oracle(cuda, sur):
     """Per-layer parameter gradients of the MSE loss against the FP64 oracle
-    on the same BF16 weights.  With the oracle rounding activations and their
-    gradients to BF16 where the kernels do, only FP32 summation order differs:
-    relative L2 error below 2e-2 per layer.  Against the unrounded oracle the
-    BF16 noise of 15 layers shows (cosine above 0.98)."""
+    on the same BF16 weights.  The oracle run that rounds activations and
+    their gradients to BF16 where the kernels do differs from the kernels only
+    by FP32 summation order and the BF16 rounding flips that follow from it
+    (relative L2 error below 0.1 per layer); against the unrounded oracle the
+    cosine stays above 0.99.  A wrong operand layout gives O(1) errors."""
     model, x, xo, pq, tgt, table = _net_case(sur)
     loss = model.loss_backward(x, torch.from_numpy(tgt).float())
     g = model.grads().double().cpu().numpy()
@@ -121,14 +122,15 @@ def test_network_gradients_match_oracle(cuda, sur):
     le, ge = U.loss_and_grad(pq, xo, tgt, model.scale, model.offset, 16)
     assert abs(float(loss.item()) - lr_) <= 1e-3 * lr_
     assert abs(float(loss.item()) - le) <= 2e-2 * le
-    worst = []
+    rows = []
     for li, (cin, cout, wo, bo) in enumerate(table):
         a = g[wo:bo + cout]
         b, c = gr[wo:bo + cout], ge[wo:bo + cout]
         rel = np.linalg.norm(a - b) / np.linalg.norm(b)
         cos = float(a @ c / (np.linalg.norm(a) * np.linalg.norm(c)))
-        worst.append((li, round(rel, 5), round(cos, 5)))
-        assert rel < 2e-2 and cos > 0.98, worst
+        rows.append((li, round(float(rel), 5), round(cos, 5)))
+    print("per-layer (layer, rel vs rounded oracle, cosine vs exact):", rows)
+    assert all(r < 0.1 and c > 0.99 for _, r, c in rows), rows
     assert not model.timed_out()
     model.close()
 
