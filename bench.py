@@ -46,7 +46,10 @@ STORAGES = {
     "f32dev": ("float32", True, 4, "f32 (f-w)"),
     "f16dev": ("float16", True, 2, "f16 (f-w)"),
     "bf16dev": ("bfloat16", True, 2, "bf16 (f-w)"),
+    "f16dev_sr": ("float16", True, 2, "f16 (f-w), stochastic rounding"),
+    "bf16dev_sr": ("bfloat16", True, 2, "bf16 (f-w), stochastic rounding"),
 }
+SR_STORAGES = {"f16dev_sr", "bf16dev_sr"}
 
 
 def _env_int(name, default):
@@ -262,10 +265,12 @@ def run_gpu(args):
     none4 = (None, None, None, None)
     stream = torch.cuda.current_stream()
 
+    sr = args.storage in SR_STORAGES
+
     def step(s, fi, fo):
         m = mom if (s + 1) % CHECK_EVERY == 0 else none4
         pkg.fused_trt_step_3d_(fo, fi, *m, None, n, n, n, NU, LAMBDA, periodic=(1, 1, 1),
-                               deviation=deviation)
+                               deviation=deviation, stochastic_rounding=sr)
 
     a, b = f_in, f_out
     for s in range(args.warmup):
@@ -306,7 +311,7 @@ def run_gpu(args):
             last = s == args.steps - 1
             m = mom if last else none4
             pkg.fused_trt_step_3d_(b, a, *m, None, n, n, n, NU, LAMBDA, periodic=(1, 1, 1),
-                                   deviation=deviation)
+                                   deviation=deviation, stochastic_rounding=sr)
             a, b = b, a
         for h, d in zip(out_host, mom):
             h.copy_(d, non_blocking=True)
@@ -395,7 +400,7 @@ def bench_tgv_precisions(pkg, n=N_GRID, steps=2000):
     peak, _ = hbm_peak()
     plane = torch.from_numpy(pkg.drivers.taylor_green_3d_populations(n, U0, Nz=1)).cuda()
     out, u64 = {}, None
-    for name in ("f64", "f32", "f32dev", "f16dev", "bf16dev"):
+    for name in ("f64", "f32", "f32dev", "f16dev", "bf16dev", "f16dev_sr", "bf16dev_sr"):
         tname, dev, bpp, label = STORAGES[name]
         dt = getattr(torch, tname)
         f = torch.empty((19, n, n, n), dtype=dt, device="cuda")
@@ -413,7 +418,7 @@ def bench_tgv_precisions(pkg, n=N_GRID, steps=2000):
         for s in range(steps):
             m = mom if s == steps - 1 else (None,) * 4
             pkg.fused_trt_step_3d_(g, f, *m, None, n, n, n, NU, LAMBDA, periodic=(1, 1, 1),
-                                   deviation=dev)
+                                   deviation=dev, stochastic_rounding=name in SR_STORAGES)
             f, g = g, f
         e1.record()
         torch.cuda.synchronize()

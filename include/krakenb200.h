@@ -53,7 +53,13 @@ typedef enum {
     KB_F32 = 1,      /* float populations (reference Float32 semantics)    */
     KB_F32_DEV = 2,  /* float deviations f - w_q, FP32 collision           */
     KB_F16_DEV = 3,  /* IEEE half deviations f - w_q, FP32 collision       */
-    KB_BF16_DEV = 4  /* bfloat16 deviations f - w_q, FP32 collision        */
+    KB_BF16_DEV = 4, /* bfloat16 deviations f - w_q, FP32 collision        */
+    /* Same memory format as KB_F16_DEV / KB_BF16_DEV; kernels that write them
+     * round stochastically (sm_100a cvt.rs), so the rounding error has zero
+     * mean.  Only kb_fused_trt_step_3d writes them; everything that reads
+     * populations accepts them. */
+    KB_F16_DEV_SR = 5,
+    KB_BF16_DEV_SR = 6
 } kb_dtype;
 
 /* Library version string ("krakenb200 <semver> sm_100a"). */
@@ -157,6 +163,18 @@ int kb_stream_periodic_x_wall_y_2d(void *f_out, const void *f_in, int Nx, int Ny
 int kb_cavity_step_2d(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
                       const uint8_t *is_solid, int Nx, int Ny, double omega, double u_lid,
                       int dtype, void *stream);
+
+/* One consistent-initialisation iteration for the MRT cavity: the step of
+ * kb_cavity_mrt_step_2d with the collision's velocity held at the given field
+ * (ux, uy; double or float by fields_dtype) and the momentum reset to rho*u.
+ * Repeating it from f = equilibrium(rho, u) makes rho and the
+ * non-equilibrium populations consistent with u (Mei, Luo, Lallemand and
+ * d'Humieres 2006).  The warm start runs a few hundred of these before the
+ * plain steps.  No reference counterpart. */
+int kb_cavity_mrt_init_step_2d(void *f_out, const void *f_in, const void *ux, const void *uy,
+                               int fields_dtype, const uint8_t *is_solid, int Nx, int Ny, double nu,
+                               double s_e, double s_eps, double s_q, double u_lid, int dtype,
+                               void *stream);
 
 /* Lid-driven cavity step with a moving-wall half-way bounce-back lid: the
  * fused pull + half-way bounce-back + BGK + moments of fused_bgk_step!
@@ -320,6 +338,13 @@ int kb_selftest_bounded_wait(long long limit, int *timed_out, void *stream);
  * reference counterpart (the reference stores plain f). */
 int kb_convert_populations(void *dst, int dst_dtype, const void *src, int src_dtype,
                            int lattice_q, size_t n_nodes, void *stream);
+
+/* Set the launch counter that seeds the random bits of the stochastic-rounding
+ * storages on the current device (each launch that writes them advances it by
+ * one).  Runs that start from the same populations and the same counter on
+ * one stream are bit-identical.  Synchronises `stream`.  No reference
+ * counterpart. */
+int kb_set_stochastic_seed(unsigned int seed, void *stream);
 
 /* ---------------------------------------------------- FP64 reductions -- */
 

@@ -19,6 +19,7 @@ KB_ERR_NONFINITE = -5
 KB_ERR_NOMEM = -6
 
 KB_F64, KB_F32, KB_F32_DEV, KB_F16_DEV, KB_BF16_DEV = 0, 1, 2, 3, 4
+KB_F16_DEV_SR, KB_BF16_DEV_SR = 5, 6   # same format, stochastic rounding on store
 
 _vp, _cvp, _u8p = C.c_void_p, C.c_void_p, C.c_void_p
 _i, _d, _sz = C.c_int, C.c_double, C.c_size_t
@@ -49,6 +50,8 @@ SIGNATURES: dict[str, list] = {
     "kb_stream_fully_periodic_2d": [_vp, _cvp, _i, _i, _i, _vp],
     "kb_stream_periodic_x_wall_y_2d": [_vp, _cvp, _i, _i, _i, _vp],
     "kb_cavity_step_2d": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _d, _i, _vp],
+    "kb_cavity_mrt_init_step_2d": [_vp, _cvp, _cvp, _cvp, _i, _u8p, _i, _i, _d, _d, _d, _d, _d,
+                                   _i, _vp],
     "kb_cavity_movingwall_step_2d": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _d, _i, _vp],
     "kb_cavity_mrt_step_2d": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _d, _d, _d, _d, _i,
                               _vp],
@@ -81,6 +84,7 @@ SIGNATURES: dict[str, list] = {
     "kb_graph_destroy": [_vp],
     "kb_selftest_bounded_wait": [C.c_longlong, C.POINTER(_i), _vp],
     "kb_convert_populations": [_vp, _i, _cvp, _i, _i, _sz, _vp],
+    "kb_set_stochastic_seed": [C.c_uint, _vp],
     "kb_mass": [_cvp, _i, _sz, _i, _dp, _vp],
     "kb_mass_static": [_cvp, _i, _sz, _i, _dp, _vp],
     "kb_residual": [_cvp, _cvp, _cvp, _cvp, _cvp, _cvp, _u8p, _sz, _i, _dp, _vp],

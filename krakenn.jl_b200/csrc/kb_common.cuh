@@ -70,8 +70,16 @@ inline size_t dtype_bytes(int dtype) {
         case KB_F32_DEV: return 4;
         case KB_F16_DEV: return 2;
         case KB_BF16_DEV: return 2;
+        case KB_F16_DEV_SR: return 2;
+        case KB_BF16_DEV_SR: return 2;
         default: return 0;
     }
+}
+
+// Memory format of a storage: the stochastic-rounding storages hold the same
+// bits as their round-to-nearest counterparts.
+__host__ __device__ inline int storage_format(int dtype) {
+    return dtype == KB_F16_DEV_SR ? KB_F16_DEV : (dtype == KB_BF16_DEV_SR ? KB_BF16_DEV : dtype);
 }
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }

@@ -415,9 +415,16 @@ __global__ void __launch_bounds__(BX) aa_local_k(T *__restrict__ f, T *__restric
     if (rho) { rho[c] = r; ux[c] = a; uy[c] = b; }
 }
 
-// collide_mrt_2d_kernel! node update: src/kernels/collide_mrt_2d.jl:54-106
-template <typename T>
-__device__ __forceinline__ void mrt_node(T *p, T s_e, T s_eps, T s_q, T s_nu) {
+// collide_mrt_2d_kernel! node update: src/kernels/collide_mrt_2d.jl:54-106.
+// With FIXED_U the equilibria use the prescribed velocity (ux_g, uy_g) and
+// the momentum is reset to rho * u_g: the iteration of Mei, Luo, Lallemand
+// and d'Humieres (2006, "Consistent initial conditions for lattice
+// Boltzmann simulations", Computers & Fluids 35) that makes rho and the
+// non-equilibrium populations consistent with a given velocity field.
+// Without FIXED_U the arithmetic is the reference's, operation for operation.
+template <typename T, bool FIXED_U = false>
+__device__ __forceinline__ void mrt_node(T *p, T s_e, T s_eps, T s_q, T s_nu, T ux_g = T(0),
+                                         T uy_g = T(0)) {
     const T f1 = p[0], f2 = p[1], f3 = p[2], f4 = p[3], f5 = p[4], f6 = p[5], f7 = p[6],
             f8 = p[7], f9 = p[8];
     T rho = f1 + f2 + f3 + f4 + f5 + f6 + f7 + f8 + f9;
@@ -431,6 +438,12 @@ __device__ __forceinline__ void mrt_node(T *p, T s_e, T s_eps, T s_q, T s_nu) {
     T pxy = f6 - f7 + f8 - f9;
     T inv = T(1) / rho;
     T ux = jx * inv, uy = jy * inv;
+    if (FIXED_U) {
+        ux = ux_g;
+        uy = uy_g;
+        jx = rho * ux;
+        jy = rho * uy;
+    }
     T usq = ux * ux + uy * uy;
     T e_eq = -T(2) * rho + T(3) * rho * usq;
     T eps_eq = rho - T(3) * rho * usq;
@@ -495,6 +508,25 @@ __global__ void __launch_bounds__(BX) cavity_mrt_step_k(T *__restrict__ fo, cons
         macro_node(p, r, a, b);
         rho[c] = r; ux[c] = a; uy[c] = b;
     }
+}
+
+// One consistent-initialisation iteration of the MRT cavity: the step above
+// with the collision's velocity held at the given field (mrt_node<FIXED_U>).
+template <typename T, typename F>
+__global__ void __launch_bounds__(BX) cavity_mrt_fixed_u_k(T *__restrict__ fo, const T *__restrict__ fi,
+                                                            const F *__restrict__ ux_g,
+                                                            const F *__restrict__ uy_g,
+                                                            const uint8_t *__restrict__ solid,
+                                                            Grid2<T> g, T s_e, T s_eps, T s_q,
+                                                            T s_nu, T u_lid) {
+    NODE2
+    T p[9];
+    pull_bb(fi, g, i, j, p);
+    if (j == g.Ny - 1) zou_he_north_node(p, u_lid);
+    if (solid && solid[c]) swap_pairs(p);
+    else mrt_node<T, true>(p, s_e, s_eps, s_q, s_nu, (T)ux_g[c], (T)uy_g[c]);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) fo[c + q * P] = p[q];
 }
 
 // stream_fully_periodic_2d_kernel!: src/kernels/stream_periodic_2d.jl:79-98
@@ -970,6 +1002,27 @@ int kb_cavity_mrt_step_2d(void *f_out, const void *f_in, void *rho, void *ux, vo
         (cavity_mrt_step_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
             (T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, is_solid, grid2<T>(Nx, Ny),
             (T)s_e, (T)s_eps, (T)s_q, (T)s_nu, (T)u_lid)));
+}
+
+int kb_cavity_mrt_init_step_2d(void *f_out, const void *f_in, const void *ux, const void *uy,
+                               int fields_dtype, const uint8_t *is_solid, int Nx, int Ny, double nu,
+                               double s_e, double s_eps, double s_q, double u_lid, int dtype,
+                               void *stream) {
+    KB_REQUIRE(f_out && f_in && ux && uy, "kb_cavity_mrt_init_step_2d: null pointer");
+    KB_REQUIRE(f_out != f_in, "kb_cavity_mrt_init_step_2d: f_out and f_in must differ");
+    KB_REQUIRE(fields_dtype == KB_F64 || fields_dtype == KB_F32,
+               "kb_cavity_mrt_init_step_2d: fields must be KB_F64 or KB_F32 (got %d)", fields_dtype);
+    if (int e = check_dims("kb_cavity_mrt_init_step_2d", Nx, Ny)) return e;
+    const double s_nu = 1.0 / (3.0 * nu + 0.5);
+    KB_DISPATCH_PLAIN("kb_cavity_mrt_init_step_2d", dtype,
+        if (fields_dtype == KB_F64)
+            (cavity_mrt_fixed_u_k<T, double><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+                (T *)f_out, (const T *)f_in, (const double *)ux, (const double *)uy, is_solid,
+                grid2<T>(Nx, Ny), (T)s_e, (T)s_eps, (T)s_q, (T)s_nu, (T)u_lid));
+        else
+            (cavity_mrt_fixed_u_k<T, float><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+                (T *)f_out, (const T *)f_in, (const float *)ux, (const float *)uy, is_solid,
+                grid2<T>(Nx, Ny), (T)s_e, (T)s_eps, (T)s_q, (T)s_nu, (T)u_lid)));
 }
 
 int kb_cavity_movingwall_step_2d(void *f_out, const void *f_in, void *rho, void *ux, void *uy,

@@ -424,7 +424,8 @@ int kb_fused_trt_step_3d(void *f_out, const void *f_in, void *rho, void *ux, voi
             fused_trt_k<float, long long><<<nodes_grid(Nx, Ny, Nz), BX, 0, s>>>(
                 (float *)f_out, (const float *)f_in, (float *)rho, (float *)ux, (float *)uy,
                 (float *)uz, is_solid, g, (float)sp, (float)sm);
-    } else if (dtype == KB_F32_DEV || dtype == KB_F16_DEV || dtype == KB_BF16_DEV) {
+    } else if (dtype == KB_F32_DEV || dtype == KB_F16_DEV || dtype == KB_BF16_DEV ||
+               dtype == KB_F16_DEV_SR || dtype == KB_BF16_DEV_SR) {
         return launch_trt3d_dev(dtype, f_out, f_in, (float *)rho, (float *)ux, (float *)uy,
                                 (float *)uz, is_solid, g, (float)sp, (float)sm, s, g_trt3d_dev_variant);
     } else {

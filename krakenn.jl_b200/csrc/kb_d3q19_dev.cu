@@ -26,6 +26,58 @@ struct DevLoad {
     __device__ __forceinline__ float operator()(R r) const { return Dev<R>::ld(r); }
 };
 
+// ---------------------------------------------------------------------------
+// Stochastic rounding of the 16-bit storages (KB_F16_DEV_SR, KB_BF16_DEV_SR).
+// Round-to-nearest storage of slowly varying deviations is biased: an update
+// smaller than half a unit in the last place is lost every step.  sm_100a's
+// cvt.rs.{f16x2,bf16x2}.f32 rounds up with probability equal to the dropped
+// fraction, given 32 random bits per pair, so the rounding error has zero
+// mean.  The bits come from an integer hash (lowbias32, C. Wellons) of the
+// thread index, the population and a launch counter in device memory that a
+// one-thread kernel advances after every such launch (so CUDA-graph replays
+// draw fresh bits and a run is reproducible on one stream).
+__device__ unsigned int g_sr_epoch = 0;
+
+__global__ void sr_advance_k() { g_sr_epoch += 1u; }
+
+__device__ __forceinline__ uint32_t hash32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+// Per-thread key for this launch; the word for population q is hash32(key + q * golden).
+__device__ __forceinline__ uint32_t sr_key() {
+    const uint32_t tid = (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)) * blockDim.x +
+                         threadIdx.x;
+    const uint32_t e = *(volatile const unsigned int *)&g_sr_epoch;
+    return hash32(tid ^ hash32(e + 0x632BE5ABu));
+}
+__device__ __forceinline__ uint32_t sr_bits(uint32_t key, int q) { return hash32(key + (uint32_t)q * 0x9E3779B9u); }
+
+// Two floats -> one packed 16-bit pair, lo in the low half (lower address).
+template <typename R> struct SRPack;
+template <> struct SRPack<__half> {
+    static __device__ __forceinline__ uint32_t pack(float lo, float hi, uint32_t r) {
+        uint32_t d;
+        asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(r));
+        return d;
+    }
+};
+template <> struct SRPack<__nv_bfloat16> {
+    static __device__ __forceinline__ uint32_t pack(float lo, float hi, uint32_t r) {
+        uint32_t d;
+        asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(r));
+        return d;
+    }
+};
+template <> struct SRPack<float> {  // never instantiated with SR: FP32 storage rounds to nearest
+    static __device__ __forceinline__ uint32_t pack(float, float, uint32_t) { return 0u; }
+};
+
 // Opposite pairs (q, qb) of D3Q19; c_qb = -c_q.  Indexed only with
 // compile-time constants (fully unrolled loops), so d[] stays in registers.
 __device__ constexpr int kPairQ[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16};
@@ -107,7 +159,7 @@ __device__ __forceinline__ void trt_dev_collide(const V *d, V *o, V &rho, V &ux,
     }
 }
 
-template <typename R, bool MOM, bool SOLID, typename I>
+template <typename R, bool MOM, bool SOLID, typename I, bool SR>
 __global__ void __launch_bounds__(BX) trt_dev_k(R *__restrict__ fo, const R *__restrict__ fi,
                                                  float *__restrict__ rho_o, float *__restrict__ ux_o,
                                                  float *__restrict__ uy_o, float *__restrict__ uz_o,
@@ -130,8 +182,17 @@ __global__ void __launch_bounds__(BX) trt_dev_k(R *__restrict__ fo, const R *__r
 
     float o[19], rho, ux, uy, uz;
     trt_dev_collide(d, o, rho, ux, uy, uz, sp, sm);
+    if (SR) {
+        const uint32_t key = sr_key();
 #pragma unroll
-    for (int q = 0; q < 19; ++q) o0[q * P] = Dev<R>::st(o[q]);
+        for (int q = 0; q < 19; ++q) {
+            const uint32_t v = SRPack<R>::pack(o[q], 0.f, sr_bits(key, q));
+            reinterpret_cast<unsigned short *>(o0)[q * P] = (unsigned short)(v & 0xFFFFu);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 19; ++q) o0[q * P] = Dev<R>::st(o[q]);
+    }
     if (MOM) { rho_o[c] = rho; ux_o[c] = ux; uy_o[c] = uy; uz_o[c] = uz; }
 }
 
@@ -155,7 +216,7 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 #define KB_PAIR_MIN_BLOCKS 6
 #endif
 
-template <typename R, bool MOM, bool SOLID, typename I>
+template <typename R, bool MOM, bool SOLID, typename I, bool SR>
 __global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_x2_k(R *__restrict__ fo, const R *__restrict__ fi,
                                                     float *__restrict__ rho_o, float *__restrict__ ux_o,
                                                     float *__restrict__ uy_o, float *__restrict__ uz_o,
@@ -181,10 +242,22 @@ __global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_x2_k(R *__rest
     trt_dev_collide(d, o, rho, ux, uy, uz, sp, sm);
     uchar2 sm2 = make_uchar2(0, 0);
     if (SOLID) sm2 = make_uchar2(solid[cA], vB ? solid[cB] : 0);
+    if (SR) {
+        const uint32_t key = sr_key();
+        unsigned short *fs = reinterpret_cast<unsigned short *>(fo);
 #pragma unroll
-    for (int q = 0; q < 19; ++q) {
-        fo[cA + (size_t)(q * P)] = Dev<R>::st(SOLID && sm2.x ? 0.f : o[q].x);
-        if (vB) fo[cB + (size_t)(q * P)] = Dev<R>::st(SOLID && sm2.y ? 0.f : o[q].y);
+        for (int q = 0; q < 19; ++q) {
+            const uint32_t v = SRPack<R>::pack(SOLID && sm2.x ? 0.f : o[q].x,
+                                               SOLID && sm2.y ? 0.f : o[q].y, sr_bits(key, q));
+            fs[cA + (size_t)(q * P)] = (unsigned short)(v & 0xFFFFu);
+            if (vB) fs[cB + (size_t)(q * P)] = (unsigned short)(v >> 16);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            fo[cA + (size_t)(q * P)] = Dev<R>::st(SOLID && sm2.x ? 0.f : o[q].x);
+            if (vB) fo[cB + (size_t)(q * P)] = Dev<R>::st(SOLID && sm2.y ? 0.f : o[q].y);
+        }
     }
     if (MOM) {
         const bool sA = SOLID && sm2.x, sB = SOLID && sm2.y;
@@ -228,7 +301,7 @@ template <> struct Vec2<__nv_bfloat16> {
     }
 };
 
-template <typename R, bool MOM, bool SOLID, typename I>
+template <typename R, bool MOM, bool SOLID, typename I, bool SR>
 __global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_v2_k(R *__restrict__ fo, const R *__restrict__ fi,
                                                     float *__restrict__ rho_o, float *__restrict__ ux_o,
                                                     float *__restrict__ uy_o, float *__restrict__ uz_o,
@@ -306,11 +379,15 @@ __global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_v2_k(R *__rest
     uchar2 sm2 = make_uchar2(0, 0);
     if (SOLID) sm2 = *reinterpret_cast<const uchar2 *>(solid + oc);
     R *__restrict__ o0 = fo + oc;
+    const uint32_t key = SR ? sr_key() : 0u;
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
         float2 v = o[q];
         if (SOLID) { if (sm2.x) v.x = 0.f; if (sm2.y) v.y = 0.f; }
-        Vec2<R>::st(o0 + (size_t)(q * P), v);
+        if (SR)
+            *reinterpret_cast<uint32_t *>(o0 + (size_t)(q * P)) = SRPack<R>::pack(v.x, v.y, sr_bits(key, q));
+        else
+            Vec2<R>::st(o0 + (size_t)(q * P), v);
     }
     if (MOM) {
         float2 r = rho, aa = ux, bb = uy, cc = uz;
@@ -325,7 +402,7 @@ __global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_v2_k(R *__rest
     }
 }
 
-template <typename R, typename I>
+template <typename R, typename I, bool SR>
 static void launch_ri(void *f_out, const void *f_in, float *rho, float *ux, float *uy, float *uz,
                       const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s,
                       int kind) {
@@ -334,11 +411,11 @@ static void launch_ri(void *f_out, const void *f_in, float *rho, float *ux, floa
     if (kind == 3) {
         const dim3 grid((g.Nx / 2 + BX - 1) / BX, g.Ny, g.Nz);
         if (rho) {
-            if (solid) trt_dev_v2_k<R, true, true, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
-            else trt_dev_v2_k<R, true, false, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            if (solid) trt_dev_v2_k<R, true, true, I, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            else trt_dev_v2_k<R, true, false, I, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
         } else {
-            if (solid) trt_dev_v2_k<R, false, true, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
-            else trt_dev_v2_k<R, false, false, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            if (solid) trt_dev_v2_k<R, false, true, I, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            else trt_dev_v2_k<R, false, false, I, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
         }
         return;
     }
@@ -346,32 +423,33 @@ static void launch_ri(void *f_out, const void *f_in, float *rho, float *ux, floa
         const int threads_x = (g.Nx + 63) / 64 * 32;  // one warp per 64 nodes of a row
         const dim3 grid((threads_x + BX - 1) / BX, g.Ny, g.Nz);
         if (rho) {
-            if (solid) trt_dev_x2_k<R, true, true, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
-            else trt_dev_x2_k<R, true, false, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            if (solid) trt_dev_x2_k<R, true, true, I, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            else trt_dev_x2_k<R, true, false, I, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
         } else {
-            if (solid) trt_dev_x2_k<R, false, true, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
-            else trt_dev_x2_k<R, false, false, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            if (solid) trt_dev_x2_k<R, false, true, I, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+            else trt_dev_x2_k<R, false, false, I, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
         }
         return;
     }
     const dim3 grid = nodes_grid(g.Nx, g.Ny, g.Nz);
     if (rho) {
-        if (solid) trt_dev_k<R, true, true, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
-        else trt_dev_k<R, true, false, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+        if (solid) trt_dev_k<R, true, true, I, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+        else trt_dev_k<R, true, false, I, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
     } else {
-        if (solid) trt_dev_k<R, false, true, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
-        else trt_dev_k<R, false, false, I><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+        if (solid) trt_dev_k<R, false, true, I, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+        else trt_dev_k<R, false, false, I, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
     }
 }
 
-template <typename R>
+template <typename R, bool SR = false>
 static void launch_r(void *f_out, const void *f_in, float *rho, float *ux, float *uy, float *uz,
                      const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s,
                      int kind) {
     if (offsets_fit_int(g, 19))
-        launch_ri<R, int>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, kind);
+        launch_ri<R, int, SR>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, kind);
     else
-        launch_ri<R, long long>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, kind);
+        launch_ri<R, long long, SR>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, kind);
+    if (SR) sr_advance_k<<<1, 1, 0, s>>>();
 }
 
 int launch_trt3d_dev(int dtype, void *f_out, const void *f_in, float *rho, float *ux, float *uy,
@@ -388,11 +466,15 @@ int launch_trt3d_dev(int dtype, void *f_out, const void *f_in, float *rho, float
         if (dtype == KB_F32_DEV) kind = g.Nx % 2 == 0 ? 3 : 1;
         else kind = g.Nx >= 64 ? 2 : 1;
     }
+    // the x / x+32 stores of the stochastic-rounding variant scatter 16-bit
+    // halves; the vector-pair kernel stores each packed pair whole
     const int pairs = kind;
     switch (dtype) {
         case KB_F32_DEV: launch_r<float>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
         case KB_F16_DEV: launch_r<__half>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
         case KB_BF16_DEV: launch_r<__nv_bfloat16>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
+        case KB_F16_DEV_SR: launch_r<__half, true>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
+        case KB_BF16_DEV_SR: launch_r<__nv_bfloat16, true>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
         default: return set_error(KB_ERR_UNSUPPORTED, "kb_fused_trt_step_3d: unknown dtype %d", dtype);
     }
     return check_launch("kb_fused_trt_step_3d");
@@ -428,6 +510,8 @@ __device__ __forceinline__ bool is_dev(int dt) {
 }
 
 __global__ void convert_k(void *dst, int ddt, const void *src, int sdt, int Q, size_t n) {
+    ddt = storage_format(ddt);
+    sdt = storage_format(sdt);
     const size_t total = (size_t)Q * n;
     for (size_t m = (size_t)blockIdx.x * blockDim.x + threadIdx.x; m < total;
          m += (size_t)gridDim.x * blockDim.x) {
@@ -442,6 +526,16 @@ __global__ void convert_k(void *dst, int ddt, const void *src, int sdt, int Q, s
 
 }  // namespace conv
 }  // namespace kb
+
+extern "C" int kb_set_stochastic_seed(unsigned int seed, void *stream) {
+    if (cudaMemcpyToSymbolAsync(kb::d3::g_sr_epoch, &seed, sizeof(seed), 0, cudaMemcpyHostToDevice,
+                                kb::as_stream(stream)) != cudaSuccess)
+        return kb::check_launch("kb_set_stochastic_seed");
+    // the host value must outlive the asynchronous copy
+    if (cudaStreamSynchronize(kb::as_stream(stream)) != cudaSuccess)
+        return kb::check_launch("kb_set_stochastic_seed");
+    return 0;
+}
 
 extern "C" int kb_convert_populations(void *dst, int dst_dtype, const void *src, int src_dtype,
                                       int lattice_q, size_t n_nodes, void *stream) {

@@ -246,6 +246,7 @@ int kb_mass(const void *f, int lattice_q, size_t n_nodes, int dtype, double *out
     red::KSum *part = (red::KSum *)(ws + kHead);
     if (cudaMemsetAsync(ws, 0, kHead, s) != cudaSuccess)
         return set_error(KB_ERR_CUDA, "kb_mass: memset failed");
+    dtype = storage_format(dtype);  // the stochastic-rounding storages share the format
     const bool dev = dtype == KB_F32_DEV || dtype == KB_F16_DEV || dtype == KB_BF16_DEV;
     switch (dtype) {
         case KB_F64: red::mass_pass1<double><<<nb, red::RT, 0, s>>>((const double *)f, lattice_q, n_nodes, dev, part, bad); break;
@@ -321,6 +322,7 @@ int kb_mass_static(const void *f, int lattice_q, size_t n_nodes, int dtype, doub
     // the flag and the result must start at zero; the partials are all written
     if (cudaMemsetAsync(ws, 0, kHead, s) != cudaSuccess)
         return set_error(KB_ERR_CUDA, "kb_mass_static: memset failed");
+    dtype = storage_format(dtype);  // the stochastic-rounding storages share the format
     const bool dev = dtype == KB_F32_DEV || dtype == KB_F16_DEV || dtype == KB_BF16_DEV;
     const int blocks = (int)nb;
     switch (dtype) {

@@ -19,7 +19,8 @@ import ctypes as C
 import torch
 
 from . import _lib
-from ._lib import (KB_BF16_DEV, KB_F16_DEV, KB_F32, KB_F32_DEV, KB_F64, call)
+from ._lib import (KB_BF16_DEV, KB_BF16_DEV_SR, KB_F16_DEV, KB_F16_DEV_SR, KB_F32, KB_F32_DEV,
+                   KB_F64, call)
 
 _TORCH_DTYPE = {KB_F64: torch.float64, KB_F32: torch.float32, KB_F32_DEV: torch.float32,
                 KB_F16_DEV: torch.float16, KB_BF16_DEV: torch.bfloat16}
@@ -428,13 +429,19 @@ def periodic_mask(periodic) -> int:
 
 
 def fused_trt_step_3d_(f_out, f_in, rho, ux, uy, uz, is_solid, Nx, Ny, Nz, nu, Lambda=3 / 16,
-                       periodic=(False, False, False), deviation=False):
+                       periodic=(False, False, False), deviation=False, stochastic_rounding=False):
     """Fused D3Q19 TRT step -- the reference's fused_trt_libb_v2_step_3d!
     (src/kernels/li_bb_3d_v2.jl:31) without interpolated-wall links, with
-    per-axis periodic wrap.  Moments may be None (then not written)."""
+    per-axis periodic wrap.  Moments may be None (then not written).  With
+    stochastic_rounding, 16-bit deviation storages are written with
+    unbiased stochastic rounding (KB_F16_DEV_SR / KB_BF16_DEV_SR)."""
     code = storage_dtype(f_in, deviation)
     if storage_dtype(f_out, deviation) != code:
         raise ValueError("f_in and f_out must have the same storage")
+    if stochastic_rounding:
+        if code not in (KB_F16_DEV, KB_BF16_DEV):
+            raise ValueError("stochastic rounding applies to float16/bfloat16 deviation storage")
+        code = KB_F16_DEV_SR if code == KB_F16_DEV else KB_BF16_DEV_SR
     _match3(f_in, Nx, Ny, Nz); _match3(f_out, Nx, Ny, Nz)
     _ptrs_3d_fields(code, Nx, Ny, Nz, rho=rho, ux=ux, uy=uy, uz=uz)
     call("kb_fused_trt_step_3d", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
@@ -459,6 +466,11 @@ def convert_populations(dst, src, dst_deviation=False, src_deviation=False):
     n = src.numel() // Q
     call("kb_convert_populations", _t(dst, "dst"), storage_dtype(dst, dst_deviation),
          _t(src, "src"), storage_dtype(src, src_deviation), Q, n, _stream())
+
+
+def set_stochastic_seed(seed: int):
+    """Seed the random bits of the stochastic-rounding storages (synchronises)."""
+    call("kb_set_stochastic_seed", C.c_uint(seed & 0xFFFFFFFF), _stream())
 
 
 def mass(f, deviation=False) -> float:
@@ -487,7 +499,7 @@ def synchronize():
 
 __all__ = [n for n in dir() if n.endswith("_") and not n.startswith("_")] + [
     "trt_rates", "convert_populations", "mass", "residual", "synchronize", "storage_dtype",
-    "set_trt3d_variant", "AA_SWAP_2D",
+    "set_trt3d_variant", "set_stochastic_seed", "AA_SWAP_2D",
     "torch_dtype", "field_dtype", "periodic_mask", "FACES_3D"]
 
 _ = _lib  # keep the module import explicit for readers

@@ -4,10 +4,12 @@ The reference has no learned component; this module adds one beside the plain
 method and judges it by the plain method.  A convolutional encoder-decoder
 (`kb_surrogate_*`, BF16 tensor-core kernels in libkrakenb200.so) is trained on
 steady cavities that the batched LBM kernel produces, then predicts the
-steady (rho, ux, uy) of unseen cases.  The plain FP64 MRT cavity step
-(`kb_cavity_mrt_step_2d`, the reference arithmetic) then iterates from the
-predicted field's equilibrium populations to the steady residual, and the
-same step from rest is the cold start it is compared with.
+steady (rho, ux, uy) of unseen cases.  The populations are initialised
+from the predicted field (equilibrium plus a few hundred consistent-
+initialisation iterations with the velocity held fixed), then the plain FP64
+MRT cavity step (`kb_cavity_mrt_step_2d`, the reference arithmetic) iterates
+to the steady residual; the same step from rest is the cold start it is
+compared with.
 
 Residual: r_u = ||u^k - u^(k-1)||_2 / ||u^k||_2 over all nodes, the
 definition of src/drivers/gnf_periodic_steady.jl:186-194, checked every
@@ -201,13 +203,23 @@ def steady_cavities(re, N, u_lid=0.1, storage="f32", max_steps=200000, tol=1e-7,
 class PlainCavity:
     """The plain FP64 MRT cavity (kb_cavity_mrt_step_2d) on its own stream,
     advanced `check_every` steps per CUDA-graph replay; the last two steps of
-    a replay write the moments the residual compares."""
+    a replay write the moments the residual compares.
 
-    def __init__(self, N, nu, u_lid, check_every=500, init=None):
+    Cold start: f = w_q (rest).  Warm start from a field `init` = (rho, ux,
+    uy): f = equilibrium(rho, u), then `init_iters` consistent-initialisation
+    iterations (kb_cavity_mrt_init_step_2d) with u held fixed, which give rho
+    and the non-equilibrium populations that go with u.  Without them the
+    missing non-equilibrium part excites the slowest Stokes mode of the
+    cavity and the warm start loses its lead.  The iterations count as steps."""
+
+    def __init__(self, N, nu, u_lid, check_every=500, init=None, init_iters=500):
         if check_every % 2 or check_every < 2:
             raise ValueError("check_every must be even and >= 2")
+        if init_iters % 2:
+            raise ValueError("init_iters must be even")
         self.N, self.nu, self.u_lid, self.G = N, nu, u_lid, check_every
         self.stream = torch.cuda.Stream()
+        self.steps = 0
         with torch.cuda.stream(self.stream):
             st = initialize_2d(LBMConfig.d2q9(N, N, nu, u_lid, 0))
             self.fa, self.fb = st["f_in"], st["f_out"]
@@ -216,6 +228,12 @@ class PlainCavity:
                 code = KB_F64 if init.dtype == torch.float64 else KB_F32
                 call("kb_init_equilibrium_2d", _p(self.fa), _p(rho), _p(ux), _p(uy), code, N, N,
                      KB_F64, _stream())
+                a, b = self.fa, self.fb
+                for _ in range(init_iters):
+                    call("kb_cavity_mrt_init_step_2d", _p(b), _p(a), _p(ux), _p(uy), code, None, N,
+                         N, float(nu), 1.4, 1.4, 1.2, float(u_lid), KB_F64, _stream())
+                    a, b = b, a
+                self.steps = init_iters
             self.m1 = [torch.zeros((N, N), dtype=torch.float64, device="cuda") for _ in range(3)]
             self.m2 = [torch.zeros((N, N), dtype=torch.float64, device="cuda") for _ in range(3)]
             self.graph = Graph()
@@ -228,7 +246,6 @@ class PlainCavity:
                     else:
                         ops.cavity_mrt_step_2d_(y, x, m[0], m[1], m[2], None, N, N, nu, u_lid)
                     x, y = y, x
-        self.steps = 0
         self.residual = float("inf")
 
     def advance(self):

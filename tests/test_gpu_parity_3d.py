@@ -193,7 +193,8 @@ def test_convert_roundtrip(cuda, pkg):
                                        ((97, 3, 4), (0, 1, 0)), ((64, 4, 4), (1, 0, 1)),
                                        ((2, 4, 4), (1, 0, 1)), ((130, 2, 3), (1, 1, 0))])
 @pytest.mark.parametrize("with_mask", [False, True])
-def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask):
+@pytest.mark.parametrize("sr", [False, True])
+def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask, sr):
     """The one-node kernel and the two-node kernels (nodes x and x+32 of a
     warp; adjacent node pairs with vector accesses and shuffled x
     neighbours; both with the packed FP32x2 collision) compute the same
@@ -208,7 +209,11 @@ def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask):
     ref = np.empty_like(f)
     mo = [np.empty((Nz, Ny, Nx)) for _ in range(4)]
     orc.fused_trt_3d(ref, f, mo, m, sp, sm, per)
+    if sr and dtype == torch.float32:
+        pytest.skip("stochastic rounding applies to the 16-bit storages")
     tol = {torch.float32: 2e-6, torch.float16: 2e-3, torch.bfloat16: 1.6e-2}[dtype]
+    if sr:
+        tol *= 2  # one unit in the last place instead of half of one
     src = torch.empty((19, Nz, Ny, Nx), dtype=dtype, device=cuda)
     pkg.convert_populations(src, _g(f), dst_deviation=True)
     outs = []
@@ -219,7 +224,8 @@ def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask):
             fo = torch.empty_like(src)
             mt = [torch.empty((Nz, Ny, Nx), dtype=torch.float32, device=cuda) for _ in range(4)]
             pkg.fused_trt_step_3d_(fo, src, *mt, _g(m, torch.bool) if m is not None else None,
-                                   Nx, Ny, Nz, 0.02, 0.25, periodic=per, deviation=True)
+                                   Nx, Ny, Nz, 0.02, 0.25, periodic=per, deviation=True,
+                                   stochastic_rounding=sr)
             back = torch.empty((19, Nz, Ny, Nx), dtype=torch.float64, device=cuda)
             pkg.convert_populations(back, fo, src_deviation=True)
             got = _h(back)
@@ -243,3 +249,50 @@ def test_vector_pair_kernel_needs_even_nx(cuda, pkg):
                                    0.02, 0.25, periodic=(1, 1, 1))
     finally:
         pkg.set_trt3d_variant(0)
+
+
+def _tgv_run(pkg, n, steps, dtype, deviation, sr=False):
+    plane = torch.from_numpy(pkg.drivers.taylor_green_3d_populations(n, 0.05, Nz=1)).cuda()
+    full = plane.expand(19, n, n, n).contiguous()
+    f = torch.empty((19, n, n, n), dtype=dtype, device="cuda")
+    if dtype == torch.float64:
+        f.copy_(full)
+    else:
+        pkg.convert_populations(f, full, dst_deviation=deviation)
+    g = torch.empty_like(f)
+    fd = torch.float64 if dtype == torch.float64 else torch.float32
+    mom = [torch.empty((n, n, n), dtype=fd, device="cuda") for _ in range(4)]
+    for s in range(steps):
+        m = mom if s == steps - 1 else (None,) * 4
+        pkg.fused_trt_step_3d_(g, f, *m, None, n, n, n, 0.01, 0.25, periodic=(1, 1, 1),
+                               deviation=deviation, stochastic_rounding=sr)
+        f, g = g, f
+    return torch.stack([t.double() for t in mom[1:]]), f
+
+
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
+def test_stochastic_rounding_lowers_tgv_error(cuda, pkg, dtype):
+    """Periodic TGV 64^3 (nu=0.01, u0=0.05, Lambda=1/4), 1500 steps: storing
+    the deviations with stochastic rounding gives a smaller L2 velocity error
+    against the FP64 run than round-to-nearest, whose bias accumulates."""
+    n, steps = 64, 1500
+    u64, _ = _tgv_run(pkg, n, steps, torch.float64, False)
+    nrm = torch.linalg.vector_norm(u64)
+    rn, _ = _tgv_run(pkg, n, steps, dtype, True, sr=False)
+    pkg.set_stochastic_seed(1)
+    st, _ = _tgv_run(pkg, n, steps, dtype, True, sr=True)
+    e_rn = float(torch.linalg.vector_norm(rn - u64) / nrm)
+    e_sr = float(torch.linalg.vector_norm(st - u64) / nrm)
+    assert e_sr < 0.75 * e_rn, (e_sr, e_rn)
+
+
+def test_stochastic_rounding_reproducible_with_seed(cuda, pkg):
+    """Same seed, same populations, one stream: bit-identical runs; another
+    seed draws other bits."""
+    outs = []
+    for seed in (5, 5, 6):
+        pkg.set_stochastic_seed(seed)
+        _, f = _tgv_run(pkg, 32, 20, torch.float16, True, sr=True)
+        outs.append(f.cpu())
+    assert torch.equal(outs[0], outs[1])
+    assert not torch.equal(outs[0], outs[2])
