@@ -187,28 +187,41 @@ def test_init_step_matches_restatement(cuda, pkg, fields):
 def test_trained_network_shortens_time_to_steady(cuda, sur):
     """32 x 32 cavities, Re in [50, 300]: train on 48 steady fields from the
     batched kernel, then run 4 held-out cases to r_u <= 1e-8 with the plain
-    FP64 MRT step from rest and from the network's prediction.  The warm
-    start needs fewer steps in total and lands on the same field."""
+    FP64 MRT step from rest and from the network's prediction.  A perfect
+    prediction (the converged field itself) first shows what the consistent
+    initialisation can gain; the trained network must still need fewer steps
+    than the cold start, and every start lands on the same field."""
     N = 32
     re_tr, re_te = sur.held_out_split(48, 4, re_range=(50.0, 300.0), seed=7)
     fields, info = sur.steady_cavities(re_tr, N, storage="f32", max_steps=100000, tol=1e-7,
                                        check_every=200)
     assert all(s != "non-finite" for _, _, s in info)
-    model = sur.Surrogate(max_batch=16, H=N, W=N, base_channels=16, seed=1)
-    hist = sur.train(model, re_tr, fields, epochs=300, batch=16, lr=2e-3, lr_min=1e-5)
-    assert hist[-1] < 0.1 * hist[0], hist[::10]
-    pred = model.infer(model.inputs(re_te, n_nodes=N))
     cold = [sur.PlainCavity(N, 0.1 * N / r, 0.1, check_every=100) for r in re_te]
+    sur.run_to_steady(cold, tol=1e-8, max_steps=400000, check_every=100)
+    sc = sum(c.steps for c in cold)
+    exact = torch.stack([c.fields() for c in cold])
+    ideal = [sur.PlainCavity(N, 0.1 * N / r, 0.1, check_every=100, init=exact[c])
+             for c, r in enumerate(re_te)]
+    sur.run_to_steady(ideal, tol=1e-8, max_steps=400000, check_every=100)
+    si = sum(c.steps for c in ideal)
+    model = sur.Surrogate(max_batch=16, H=N, W=N, base_channels=16, seed=1)
+    hist = sur.train(model, re_tr, fields, epochs=700, batch=16, lr=2e-3, lr_min=1e-5)
+    pred = model.infer(model.inputs(re_te, n_nodes=N))
+    perr = [float((pred[c, 1:].double() - exact[c, 1:]).norm() / exact[c, 1:].norm())
+            for c in range(len(re_te))]
     warm = [sur.PlainCavity(N, 0.1 * N / r, 0.1, check_every=100, init=pred[c])
             for c, r in enumerate(re_te)]
-    sur.run_to_steady(cold, tol=1e-8, max_steps=400000, check_every=100)
     sur.run_to_steady(warm, tol=1e-8, max_steps=400000, check_every=100)
-    sc = sum(c.steps for c in cold)
     sw = sum(c.steps for c in warm)
-    assert all(c.residual <= 1e-8 for c in cold + warm)
-    assert sw < 0.9 * sc, (sw, sc, [c.steps for c in cold], [c.steps for c in warm])
+    msg = dict(cold=[c.steps for c in cold], ideal=[c.steps for c in ideal],
+               warm=[c.steps for c in warm], pred_err=perr, loss=(hist[0], hist[-1]))
+    print("warm start 32^2:", msg)
+    assert hist[-1] < 0.05 * hist[0], msg
+    assert all(c.residual <= 1e-8 for c in cold + ideal + warm), msg
+    assert si < 0.6 * sc, msg
+    assert sw < 0.95 * sc, msg
     for c, w in zip(cold, warm):
         d = (c.fields() - w.fields()).abs()
-        assert float(d[1:].max()) / 0.1 < 1e-4
+        assert float(d[1:].max()) / 0.1 < 1e-4, msg
     assert not model.timed_out()
     model.close()
