@@ -244,6 +244,7 @@ def run_gpu(args):
     rank, world, local = dist_setup(args.gpus)
     pkg = graft.load_package()
     pkg._lib.load()
+    pkg.set_trt3d_variant(args.trt_variant)
     dev = torch.device("cuda", torch.cuda.current_device())
     tname, deviation, bpp, dlabel = STORAGES[args.storage]
     dtype = getattr(torch, tname)
@@ -771,6 +772,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--storage", default="f32dev", choices=sorted(STORAGES))
+    ap.add_argument("--trt-variant", type=int, default=0,
+                    help="deviation-storage TRT kernel: 0 automatic, 1 node, 2 x/x+32 pairs, "
+                         "3 vector pairs, 4 16-bit quads")
     ap.add_argument("--grid", type=int, default=N_GRID)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")

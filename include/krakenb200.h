@@ -260,8 +260,9 @@ int kb_fused_trt_step_3d(void *f_out, const void *f_in, void *rho, void *ux, voi
  * kernels of kb_fused_trt_step_3d: 0 automatic (KB_F32_DEV: 3 for even Nx,
  * else 1; FP16/BF16: 2 when Nx >= 64, else 1), 1 one node per thread,
  * 2 nodes x and x+32 per thread, 3 adjacent node pairs with 2-element
- * vector accesses (even Nx).
- * Variants 2 and 3 collide in packed FP32x2 arithmetic.  Every variant
+ * vector accesses (even Nx), 4 adjacent node quads with 8-byte accesses
+ * (16-bit storages, Nx % 4 == 0).
+ * Variants 2, 3 and 4 collide in packed FP32x2 arithmetic.  Every variant
  * computes the same update up to FP32 rounding.  No reference counterpart. */
 int kb_set_kernel_variant(int kernel, int variant);
 

@@ -323,7 +323,7 @@ extern "C" {
 
 int kb_set_kernel_variant(int kernel, int variant) {
     KB_REQUIRE(kernel == 1, "kb_set_kernel_variant: unknown kernel id %d", kernel);
-    KB_REQUIRE(variant >= 0 && variant <= 3, "kb_set_kernel_variant: variant %d not in 0..3", variant);
+    KB_REQUIRE(variant >= 0 && variant <= 4, "kb_set_kernel_variant: variant %d not in 0..4", variant);
     g_trt3d_dev_variant = variant;
     return KB_OK;
 }

@@ -402,12 +402,201 @@ __global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_v2_k(R *__rest
     }
 }
 
+// ---------------------------------------------------------------------------
+// Quads, 16-bit storages (Nx % 4 == 0): lane t of a warp owns the four
+// adjacent nodes x0 = 4t .. 4t + 3 of the warp's 128-node run of one row, so
+// each population of the quad is ONE aligned 8-byte load and one 8-byte
+// store, and the pull geometry (y/z source rows, walls, wraps) is computed
+// once for four nodes.  An x-shifted population takes its missing element
+// from the neighbouring lane by one 32-bit shuffle; the first / last lane of
+// the run load it directly, which also covers the periodic wrap and the
+// half-way bounce-back at x walls.  The collision runs as two packed FP32x2
+// streams (nodes 0,1 and 2,3).
+template <typename R> struct Pack16;
+template <> struct Pack16<__half> {
+    static __device__ __forceinline__ float2 unpack(uint32_t w) {
+        return __half22float2(*reinterpret_cast<const __half2 *>(&w));
+    }
+    static __device__ __forceinline__ float lo(uint32_t w) {
+        return __half2float(__ushort_as_half((unsigned short)(w & 0xFFFFu)));
+    }
+    static __device__ __forceinline__ float hi(uint32_t w) {
+        return __half2float(__ushort_as_half((unsigned short)(w >> 16)));
+    }
+    static __device__ __forceinline__ uint32_t pack(float a, float b) {
+        const __half2 h = __floats2half2_rn(a, b);
+        return *reinterpret_cast<const uint32_t *>(&h);
+    }
+};
+template <> struct Pack16<__nv_bfloat16> {
+    static __device__ __forceinline__ float2 unpack(uint32_t w) {
+        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&w));
+    }
+    static __device__ __forceinline__ float lo(uint32_t w) { return __uint_as_float(w << 16); }
+    static __device__ __forceinline__ float hi(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
+    static __device__ __forceinline__ uint32_t pack(float a, float b) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        return *reinterpret_cast<const uint32_t *>(&h);
+    }
+};
+
+// Resident blocks per SM requested for the quad kernel (caps its registers).
+#ifndef KB_QUAD_MIN_BLOCKS
+#define KB_QUAD_MIN_BLOCKS 3
+#endif
+
+template <typename R, bool MOM, bool SOLID, typename I, bool SR>
+__global__ void __launch_bounds__(128, KB_QUAD_MIN_BLOCKS) trt_dev_v4_k(R *__restrict__ fo, const R *__restrict__ fi,
+                                                       float *__restrict__ rho_o, float *__restrict__ ux_o,
+                                                       float *__restrict__ uy_o, float *__restrict__ uz_o,
+                                                       const uint8_t *__restrict__ solid, Grid3 g,
+                                                       float sp, float sm, int warps_per_row) {
+    constexpr int CX[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+    constexpr int CY[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
+    constexpr int CZ[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
+    constexpr int OP[19] = {0, 2, 1, 4, 3, 6, 5, 10, 9, 8, 7, 14, 13, 12, 11, 18, 17, 16, 15};
+    using PK = Pack16<R>;
+    const int lane = threadIdx.x & 31;
+    const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const long long row_id = gw / warps_per_row;          // (j, k) row
+    if (row_id >= (long long)g.Ny * g.Nz) return;         // whole warp: no shuffle partner left
+    const int seg = (int)(gw - row_id * warps_per_row);
+    const int j = (int)(row_id % g.Ny), k = (int)(row_id / g.Ny);
+    const int Nx = g.Nx;
+    const int x0 = seg * 128 + 4 * lane;
+    const bool valid = x0 < Nx;
+    const bool last = x0 + 4 >= Nx;  // no valid neighbour lane to the right
+    const I P = (I)g.plane;
+    const bool px = g.per & 1, py = (g.per >> 1) & 1, pz = (g.per >> 2) & 1;
+    const I sy = (I)Nx, sz = (I)Nx * (I)g.Ny;
+    const bool ym = py || j > 0, yp = py || j < g.Ny - 1;
+    const bool zm = pz || k > 0, zp = pz || k < g.Nz - 1;
+    const I oym = (j > 0 ? (I)-1 : (I)(g.Ny - 1)) * sy;
+    const I oyp = (j < g.Ny - 1 ? (I)1 : -(I)(g.Ny - 1)) * sy;
+    const I ozm = (k > 0 ? (I)-1 : (I)(g.Nz - 1)) * sz;
+    const I ozp = (k < g.Nz - 1 ? (I)1 : -(I)(g.Nz - 1)) * sz;
+    const size_t row = (size_t)Nx * ((size_t)j + (size_t)g.Ny * k);
+    const R *__restrict__ f0 = fi + row;
+    const int xv = valid ? x0 : 0;
+
+    // 1. every load: the aligned quad and, for x-shifted populations, the one
+    //    edge element this lane may need
+    uint2 a[19];
+    float e[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        const bool ok = (CY[q] == 1 ? ym : CY[q] == -1 ? yp : true) &&
+                        (CZ[q] == 1 ? zm : CZ[q] == -1 ? zp : true);
+        const I srow = (CY[q] == 1 ? oym : CY[q] == -1 ? oyp : (I)0) +
+                       (CZ[q] == 1 ? ozm : CZ[q] == -1 ? ozp : (I)0) + (I)q * P;
+        const I orow = (I)OP[q] * P;
+        a[q] = *reinterpret_cast<const uint2 *>(f0 + (ok ? srow : orow) + xv);
+        e[q] = 0.f;
+        if (CX[q] == 1) {  // node x0 pulls x0 - 1
+            const bool need = ok && lane == 0;
+            const I off = x0 > 0 ? srow + (I)(xv - 1) : (px ? srow + (I)(Nx - 1) : orow + (I)xv);
+            if (need && valid) e[q] = Dev<R>::ld(f0[off]);
+        } else if (CX[q] == -1) {  // node x0 + 3 pulls x0 + 4
+            const bool need = ok && (lane == 31 || last);
+            const I off = !last ? srow + (I)(xv + 4) : (px ? srow : orow + (I)(xv + 3));
+            if (need && valid) e[q] = Dev<R>::ld(f0[off]);
+        }
+    }
+    // 2. assemble the pulled quad of every population as two float2
+    float2 d0[19], d1[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        const bool ok = (CY[q] == 1 ? ym : CY[q] == -1 ? yp : true) &&
+                        (CZ[q] == 1 ? zm : CZ[q] == -1 ? zp : true);
+        const float2 l = PK::unpack(a[q].x), h = PK::unpack(a[q].y);  // elements 0,1 | 2,3
+        if (CX[q] == 1) {
+            const uint32_t up = __shfl_up_sync(0xffffffffu, a[q].y, 1);  // lane-1's elements 2,3
+            const float left = lane == 0 ? e[q] : PK::hi(up);
+            d0[q] = ok ? make_float2(left, l.x) : l;
+            d1[q] = ok ? make_float2(l.y, h.x) : h;
+        } else if (CX[q] == -1) {
+            const uint32_t dn = __shfl_down_sync(0xffffffffu, a[q].x, 1);  // lane+1's elements 0,1
+            const float right = (lane == 31 || last) ? e[q] : PK::lo(dn);
+            d0[q] = ok ? make_float2(l.y, h.x) : l;
+            d1[q] = ok ? make_float2(h.y, right) : h;
+        } else {
+            d0[q] = l;
+            d1[q] = h;
+        }
+    }
+    if (!valid) return;
+
+    const size_t oc = row + x0;
+    uchar4 m4 = make_uchar4(0, 0, 0, 0);
+    if (SOLID) m4 = *reinterpret_cast<const uchar4 *>(solid + oc);
+    R *__restrict__ o0 = fo + oc;
+    const uint32_t key = SR ? sr_key() : 0u;
+    uint32_t w0[19];
+    float2 r0, ux0, uy0, uz0, r1, ux1, uy1, uz1;
+    {
+        float2 o[19];
+        trt_dev_collide(d0, o, r0, ux0, uy0, uz0, sp, sm);
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            float2 v = o[q];
+            if (SOLID) { if (m4.x) v.x = 0.f; if (m4.y) v.y = 0.f; }
+            w0[q] = SR ? SRPack<R>::pack(v.x, v.y, sr_bits(key, q)) : PK::pack(v.x, v.y);
+        }
+    }
+    {
+        float2 o[19];
+        trt_dev_collide(d1, o, r1, ux1, uy1, uz1, sp, sm);
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            float2 v = o[q];
+            if (SOLID) { if (m4.z) v.x = 0.f; if (m4.w) v.y = 0.f; }
+            uint32_t w1;
+            if (SR) {
+                const uint32_t r = sr_bits(key, q) * 0x85EBCA77u;
+                w1 = SRPack<R>::pack(v.x, v.y, __funnelshift_l(r, r, 16));
+            } else {
+                w1 = PK::pack(v.x, v.y);
+            }
+            *reinterpret_cast<uint2 *>(o0 + (size_t)(q * P)) = make_uint2(w0[q], w1);
+        }
+    }
+    if (MOM) {
+        float4 r = make_float4(r0.x, r0.y, r1.x, r1.y), aa = make_float4(ux0.x, ux0.y, ux1.x, ux1.y);
+        float4 bb = make_float4(uy0.x, uy0.y, uy1.x, uy1.y), cc = make_float4(uz0.x, uz0.y, uz1.x, uz1.y);
+        if (SOLID) {
+            if (m4.x) { r.x = 1.f; aa.x = bb.x = cc.x = 0.f; }
+            if (m4.y) { r.y = 1.f; aa.y = bb.y = cc.y = 0.f; }
+            if (m4.z) { r.z = 1.f; aa.z = bb.z = cc.z = 0.f; }
+            if (m4.w) { r.w = 1.f; aa.w = bb.w = cc.w = 0.f; }
+        }
+        *reinterpret_cast<float4 *>(rho_o + oc) = r;
+        *reinterpret_cast<float4 *>(ux_o + oc) = aa;
+        *reinterpret_cast<float4 *>(uy_o + oc) = bb;
+        *reinterpret_cast<float4 *>(uz_o + oc) = cc;
+    }
+}
+
 template <typename R, typename I, bool SR>
 static void launch_ri(void *f_out, const void *f_in, float *rho, float *ux, float *uy, float *uz,
                       const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s,
                       int kind) {
     R *fo = (R *)f_out;
     const R *fi = (const R *)f_in;
+    if constexpr (sizeof(R) == 2) {
+        if (kind == 4) {
+            const int wpr = (g.Nx + 127) / 128;  // warps per row
+            const long long warps = (long long)wpr * g.Ny * g.Nz;
+            const dim3 grid((unsigned)((warps + 3) / 4));
+            if (rho) {
+                if (solid) trt_dev_v4_k<R, true, true, I, SR><<<grid, 128, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm, wpr);
+                else trt_dev_v4_k<R, true, false, I, SR><<<grid, 128, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm, wpr);
+            } else {
+                if (solid) trt_dev_v4_k<R, false, true, I, SR><<<grid, 128, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm, wpr);
+                else trt_dev_v4_k<R, false, false, I, SR><<<grid, 128, 0, s>>>(fo, fi, rho, ux, uy, uz, solid, g, sp, sm, wpr);
+            }
+            return;
+        }
+    }
     if (kind == 3) {
         const dim3 grid((g.Nx / 2 + BX - 1) / BX, g.Ny, g.Nz);
         if (rho) {
@@ -456,9 +645,13 @@ int launch_trt3d_dev(int dtype, void *f_out, const void *f_in, float *rho, float
                      float *uz, const uint8_t *solid, const Grid3 &g, float sp, float sm,
                      cudaStream_t s, int variant) {
     // variant: 0 automatic, 1 one node per thread, 2 nodes x and x+32 per
-    // thread, 3 adjacent node pairs with vector accesses (even Nx only).
+    // thread, 3 adjacent node pairs with vector accesses (even Nx only),
+    // 4 adjacent node quads with 8-byte accesses (16-bit storages, Nx % 4 == 0).
     if (variant == 3 && g.Nx % 2 != 0)
         return set_error(KB_ERR_ARG, "kb_fused_trt_step_3d: the vector-pair kernel needs an even Nx");
+    if (variant == 4 && (g.Nx % 4 != 0 || dtype == KB_F32_DEV))
+        return set_error(KB_ERR_ARG,
+                         "kb_fused_trt_step_3d: the quad kernel needs Nx %% 4 == 0 and 16-bit storage");
     // automatic choice, from measurements at 256^3 on B200: FP32 deviations
     // run fastest as vector pairs, FP16/BF16 as x / x+32 pairs
     int kind = variant;

@@ -417,7 +417,8 @@ def compute_macroscopic_3d_(rho, ux, uy, uz, f):
 
 def set_trt3d_variant(variant: int):
     """0 automatic, 1 one node per thread, 2 nodes x and x+32 per thread,
-    3 adjacent node pairs with vector accesses (even Nx)."""
+    3 adjacent node pairs with vector accesses (even Nx), 4 adjacent node
+    quads with 8-byte accesses (16-bit storages, Nx % 4 == 0)."""
     call("kb_set_kernel_variant", 1, int(variant))
 
 

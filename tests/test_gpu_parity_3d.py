@@ -191,13 +191,17 @@ def test_convert_roundtrip(cuda, pkg):
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float16, torch.bfloat16])
 @pytest.mark.parametrize("shape,per", [((34, 6, 5), (1, 1, 1)), ((33, 6, 5), (0, 0, 0)),
                                        ((97, 3, 4), (0, 1, 0)), ((64, 4, 4), (1, 0, 1)),
-                                       ((2, 4, 4), (1, 0, 1)), ((130, 2, 3), (1, 1, 0))])
+                                       ((2, 4, 4), (1, 0, 1)), ((130, 2, 3), (1, 1, 0)),
+                                       ((132, 3, 2), (1, 0, 1)), ((4, 3, 5), (0, 1, 1)),
+                                       ((260, 2, 2), (0, 0, 0))])
 @pytest.mark.parametrize("with_mask", [False, True])
 @pytest.mark.parametrize("sr", [False, True])
 def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask, sr):
-    """The one-node kernel and the two-node kernels (nodes x and x+32 of a
+    """The one-node kernel, the two-node kernels (nodes x and x+32 of a
     warp; adjacent node pairs with vector accesses and shuffled x
-    neighbours; both with the packed FP32x2 collision) compute the same
+    neighbours) and the four-node kernel of the 16-bit storages (adjacent
+    quads, 8-byte accesses), all but the first with the packed FP32x2
+    collision, compute the same
     update: on ragged grids, walls or wraps on every axis and solid nodes,
     all stay within the storage rounding of the FP64 oracle (max abs error
     of f relative to w_q) and of each other."""
@@ -219,6 +223,8 @@ def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask, 
     outs = []
     try:
         variants = (1, 2, 3) if Nx % 2 == 0 else (1, 2)
+        if Nx % 4 == 0 and dtype != torch.float32:
+            variants += (4,)
         for variant in variants:
             pkg.set_trt3d_variant(variant)
             fo = torch.empty_like(src)
@@ -238,6 +244,21 @@ def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask, 
         pkg.set_trt3d_variant(0)
     for o in outs[1:]:
         assert np.max(np.abs(outs[0] - o) / W19[:, None, None, None]) < 2 * tol
+
+
+def test_quad_kernel_needs_nx_multiple_of_4_and_16bit(cuda, pkg):
+    pkg.set_trt3d_variant(4)
+    try:
+        f = torch.zeros((19, 4, 4, 6), dtype=torch.float16, device=cuda)
+        with pytest.raises(pkg.KrakenArgumentError):
+            pkg.fused_trt_step_3d_(torch.empty_like(f), f, None, None, None, None, None, 6, 4, 4,
+                                   0.02, 0.25, periodic=(1, 1, 1))
+        g = torch.zeros((19, 4, 4, 8), dtype=torch.float32, device=cuda)
+        with pytest.raises(pkg.KrakenArgumentError):
+            pkg.fused_trt_step_3d_(torch.empty_like(g), g, None, None, None, None, None, 8, 4, 4,
+                                   0.02, 0.25, periodic=(1, 1, 1), deviation=True)
+    finally:
+        pkg.set_trt3d_variant(0)
 
 
 def test_vector_pair_kernel_needs_even_nx(cuda, pkg):
