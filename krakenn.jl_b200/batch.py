@@ -15,9 +15,10 @@ import ctypes as C
 import numpy as np
 import torch
 
-from ._lib import KB_BF16_DEV, KB_F16_DEV, KB_F32_DEV, call, load
+from ._lib import KB_BF16_DEV, KB_BF16_DEV_SR, KB_F16_DEV, KB_F16_DEV_SR, KB_F32_DEV, call, load
 
-STORAGE = {"f16": KB_F16_DEV, "bf16": KB_BF16_DEV, "f32": KB_F32_DEV}
+STORAGE = {"f16": KB_F16_DEV, "bf16": KB_BF16_DEV, "f32": KB_F32_DEV,
+           "f16sr": KB_F16_DEV_SR, "bf16sr": KB_BF16_DEV_SR}  # *sr: stochastic rounding
 STATE = {0: "live", 1: "converged", 2: "max_steps", 3: "non-finite"}
 
 

@@ -103,10 +103,10 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
 
 // One node of one case: pull (half-way bounce-back), Zou-He lid on the top
 // row, MRT on deviations; returns the pre-collision velocity.
-template <typename R>
+template <typename R, bool SR>
 __device__ __forceinline__ void node_update(const R *__restrict__ src, R *__restrict__ dst, int N,
                                             int i, int j, float s_nu, float u_lid, float &ux,
-                                            float &uy) {
+                                            float &uy, uint32_t key) {
     const long long P = (long long)N * N;
     const long long c = (long long)j * N + i;
     const bool w = i > 0, e = i < N - 1, s = j > 0, n = j < N - 1;
@@ -169,14 +169,27 @@ __device__ __forceinline__ void node_update(const R *__restrict__ src, R *__rest
     o[6] = base_d - c6 * jx - c12 * qxs + c6 * jy + c12 * qys - c4 * pxys;
     o[7] = base_d - c6 * jx - c12 * qxs - c6 * jy - c12 * qys + c4 * pxys;
     o[8] = base_d + c6 * jx + c12 * qxs - c6 * jy - c12 * qys - c4 * pxys;
+    if (SR) {
+        // stochastic rounding: populations (0,1), (2,3), (4,5), (6,7), (8,-)
+        // share one cvt.rs and one 32-bit random word
+        unsigned short *d16 = reinterpret_cast<unsigned short *>(dst);
 #pragma unroll
-    for (int q = 0; q < 9; ++q) dst[c + q * P] = Dev<R>::st(o[q]);
+        for (int q = 0; q < 9; q += 2) {
+            const uint32_t w = SRPack<R>::pack(o[q], q + 1 < 9 ? o[q + 1] : 0.f,
+                                               hash32(key + (uint32_t)q * 0x9E3779B9u));
+            d16[c + q * P] = (unsigned short)(w & 0xFFFFu);
+            if (q + 1 < 9) d16[c + (q + 1) * P] = (unsigned short)(w >> 16);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) dst[c + q * P] = Dev<R>::st(o[q]);
+    }
 }
 
-template <typename R>
+template <typename R, bool SR>
 __global__ void __launch_bounds__(BT) batch_k(BatchState D, int n_cases, int n_tiles_all, int tile_nodes,
                                                int max_steps, int check_every, float tol,
-                                               long long spin_limit) {
+                                               long long spin_limit, uint32_t seed) {
     __shared__ double sh[BT / 32];
     const unsigned nblocks = gridDim.x;
     for (int s = 0;; ++s) {
@@ -195,7 +208,10 @@ __global__ void __launch_bounds__(BT) batch_k(BatchState D, int n_cases, int n_t
             for (int m = T.start + threadIdx.x; m < end; m += BT) {
                 const int j = m / C.N, i = m - j * C.N;
                 float ux, uy;
-                node_update<R>(src + C.f_off, dst + C.f_off, C.N, i, j, C.s_nu, C.u_lid, ux, uy);
+                const uint32_t key =
+                    SR ? hash32((uint32_t)(C.f_off + m) ^ hash32((uint32_t)s * 0x632BE5ABu + seed)) : 0u;
+                node_update<R, SR>(src + C.f_off, dst + C.f_off, C.N, i, j, C.s_nu, C.u_lid, ux, uy,
+                                   key);
                 if (save) { D.uxp[C.m_off + m] = ux; D.uyp[C.m_off + m] = uy; }
                 if (check) {
                     D.ux[C.m_off + m] = ux;
@@ -282,6 +298,7 @@ struct kb_batch {
     kb::batch::Tile *tiles_all = nullptr, *tiles = nullptr;
     char *scal = nullptr;  // n_tiles, bar[2], err, updates, acc, state, steps, res
     int tuned_tile = 0, tuned_bpsm = 0;
+    unsigned runs = 0;  // launches so far; seeds the stochastic-rounding bits
 };
 
 namespace {
@@ -352,7 +369,7 @@ int reset(kb_batch *b, cudaStream_t s) {
     return KB_OK;
 }
 
-template <typename R>
+template <typename R, bool SR = false>
 int launch(kb_batch *b, int max_steps, int check_every, double tol, int blocks_per_sm,
            cudaStream_t s) {
     const ScalLayout L = scal_layout(b->n_cases);
@@ -370,7 +387,7 @@ int launch(kb_batch *b, int max_steps, int check_every, double tol, int blocks_p
     D.steps = (int *)(b->scal + L.steps);
     D.res = (float *)(b->scal + L.res);
     int occ = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_k<R>, BT, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_k<R, SR>, BT, 0);
     if (e != cudaSuccess) return cuda_err("kb_batch_run: occupancy", e);
     const int bpsm = blocks_per_sm < 1 ? occ : (blocks_per_sm < occ ? blocks_per_sm : occ);
     if (bpsm < 1) return kb::set_error(KB_ERR_UNSUPPORTED, "kb_batch_run: kernel does not fit an SM");
@@ -379,9 +396,10 @@ int launch(kb_batch *b, int max_steps, int check_every, double tol, int blocks_p
     // ~ 2^24 waits of >= 128 ns: a barrier that has not opened after a few
     // seconds is declared timed out
     long long spin = 1ll << 24;
-    void *args[] = {&D, &n_cases, &n_all, &tn, &max_steps, &check_every, &tolf, &spin};
+    uint32_t seed = b->runs++;  // fresh random bits for every run of the batch
+    void *args[] = {&D, &n_cases, &n_all, &tn, &max_steps, &check_every, &tolf, &spin, &seed};
     dim3 grid(bpsm * kb::sm_count()), block(BT);
-    e = cudaLaunchCooperativeKernel((void *)batch_k<R>, grid, block, args, 0, s);
+    e = cudaLaunchCooperativeKernel((void *)batch_k<R, SR>, grid, block, args, 0, s);
     if (e != cudaSuccess) return cuda_err("kb_batch_run: cooperative launch", e);
     return KB_OK;
 }
@@ -394,8 +412,10 @@ int kb_batch_create(kb_batch **out, int n_cases, const int *N, const double *nu,
                     const double *u_lid, int dtype, void *stream) {
     KB_REQUIRE(out && N && nu && u_lid, "kb_batch_create: null pointer");
     KB_REQUIRE(n_cases > 0, "kb_batch_create: n_cases must be positive");
-    KB_REQUIRE(dtype == KB_F16_DEV || dtype == KB_BF16_DEV || dtype == KB_F32_DEV,
-               "kb_batch_create: storage must be KB_F16_DEV, KB_BF16_DEV or KB_F32_DEV");
+    KB_REQUIRE(dtype == KB_F16_DEV || dtype == KB_BF16_DEV || dtype == KB_F32_DEV ||
+                   dtype == KB_F16_DEV_SR || dtype == KB_BF16_DEV_SR,
+               "kb_batch_create: storage must be KB_F16_DEV, KB_BF16_DEV, KB_F32_DEV or a "
+               "stochastic-rounding 16-bit storage");
     int coop = 0, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
@@ -474,6 +494,9 @@ int kb_batch_run(kb_batch *b, int max_steps, int check_every, double tol, int ti
     switch (b->dtype) {
         case KB_F16_DEV: return launch<__half>(b, max_steps, check_every, tol, blocks_per_sm, s);
         case KB_BF16_DEV: return launch<__nv_bfloat16>(b, max_steps, check_every, tol, blocks_per_sm, s);
+        case KB_F16_DEV_SR: return launch<__half, true>(b, max_steps, check_every, tol, blocks_per_sm, s);
+        case KB_BF16_DEV_SR:
+            return launch<__nv_bfloat16, true>(b, max_steps, check_every, tol, blocks_per_sm, s);
         default: return launch<float>(b, max_steps, check_every, tol, blocks_per_sm, s);
     }
 }

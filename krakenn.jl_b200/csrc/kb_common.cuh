@@ -63,6 +63,40 @@ template <> struct Dev<__nv_bfloat16> {
     static __device__ __forceinline__ __nv_bfloat16 st(float d) { return __float2bfloat16_rn(d); }
 };
 
+// ------------------------------------------------------ stochastic rounding --
+// 32-bit integer hash (lowbias32, C. Wellons) for the random bits of the
+// stochastic-rounding stores.
+__device__ __forceinline__ uint32_t hash32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+// Two floats -> one packed 16-bit pair (lo in the low half, the lower
+// address), rounded stochastically by sm_100a's cvt.rs with 32 random bits
+// (bits 0-12 / 0-15 drive lo, bits 16-28 / 16-31 hi, for f16 / bf16).
+template <typename R> struct SRPack;
+template <> struct SRPack<__half> {
+    static __device__ __forceinline__ uint32_t pack(float lo, float hi, uint32_t r) {
+        uint32_t d;
+        asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(r));
+        return d;
+    }
+};
+template <> struct SRPack<__nv_bfloat16> {
+    static __device__ __forceinline__ uint32_t pack(float lo, float hi, uint32_t r) {
+        uint32_t d;
+        asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(r));
+        return d;
+    }
+};
+template <> struct SRPack<float> {  // never used with SR: FP32 storage rounds to nearest
+    static __device__ __forceinline__ uint32_t pack(float, float, uint32_t) { return 0u; }
+};
+
 inline size_t dtype_bytes(int dtype) {
     switch (dtype) {
         case KB_F64: return 8;

@@ -40,15 +40,6 @@ __device__ unsigned int g_sr_epoch = 0;
 
 __global__ void sr_advance_k() { g_sr_epoch += 1u; }
 
-__device__ __forceinline__ uint32_t hash32(uint32_t x) {
-    x ^= x >> 16;
-    x *= 0x7feb352du;
-    x ^= x >> 15;
-    x *= 0x846ca68bu;
-    x ^= x >> 16;
-    return x;
-}
-
 // Per-thread key for this launch; the word for population q is hash32(key + q * golden).
 __device__ __forceinline__ uint32_t sr_key() {
     const uint32_t tid = (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)) * blockDim.x +
@@ -57,26 +48,6 @@ __device__ __forceinline__ uint32_t sr_key() {
     return hash32(tid ^ hash32(e + 0x632BE5ABu));
 }
 __device__ __forceinline__ uint32_t sr_bits(uint32_t key, int q) { return hash32(key + (uint32_t)q * 0x9E3779B9u); }
-
-// Two floats -> one packed 16-bit pair, lo in the low half (lower address).
-template <typename R> struct SRPack;
-template <> struct SRPack<__half> {
-    static __device__ __forceinline__ uint32_t pack(float lo, float hi, uint32_t r) {
-        uint32_t d;
-        asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(r));
-        return d;
-    }
-};
-template <> struct SRPack<__nv_bfloat16> {
-    static __device__ __forceinline__ uint32_t pack(float lo, float hi, uint32_t r) {
-        uint32_t d;
-        asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(r));
-        return d;
-    }
-};
-template <> struct SRPack<float> {  // never instantiated with SR: FP32 storage rounds to nearest
-    static __device__ __forceinline__ uint32_t pack(float, float, uint32_t) { return 0u; }
-};
 
 // Opposite pairs (q, qb) of D3Q19; c_qb = -c_q.  Indexed only with
 // compile-time constants (fully unrolled loops), so d[] stays in registers.

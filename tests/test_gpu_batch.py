@@ -21,7 +21,8 @@ def _oracle_mrt_cavity(orc, N, nu, u_lid, steps):
     return ux, uy
 
 
-@pytest.mark.parametrize("storage,tol", [("f32", 2e-6), ("f16", 3e-3), ("bf16", 2e-2)])
+@pytest.mark.parametrize("storage,tol", [("f32", 2e-6), ("f16", 3e-3), ("bf16", 2e-2),
+                                         ("f16sr", 4e-3), ("bf16sr", 3e-2)])
 def test_batch_matches_single_case_oracle(cuda, pkg, orc, storage, tol):
     """Each case of a ragged batch (N = 16, 24, 40) after 200 steps matches the
     FP64 oracle of the reference loop (stream_2d!, apply_zou_he_north_2d!,
