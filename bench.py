@@ -722,10 +722,20 @@ def bench_warmstart(pkg, N=256, n_train=2000, n_test=64, epochs=40, batch=16, ba
         both = conv & conv_c
         dmax = [float((c.fields()[1:] - w.fields()[1:]).abs().max()) / 0.1
                 for c, w, b in zip(cold, cs, both) if b]
+        per_threshold = {}
+        for th in sur.THRESHOLDS:
+            pairs = [(c.reached[th], w.reached[th]) for c, w in zip(cold, cs)
+                     if th in c.reached and th in w.reached]
+            if pairs:
+                a = sum(p[0] for p in pairs)
+                b = sum(p[1] for p in pairs)
+                per_threshold[f"{th:g}"] = {"cases": len(pairs), "cold_steps": a, "steps": b,
+                                            "ratio": round(a / max(1, b), 3)}
         res[name] = {"steps": sw.tolist(), "converged": int(conv.sum()),
                      "wall_s": round(t + (infer_ms * 1e-3 if name == "warm" else 0.0), 2),
                      "steps_ratio_cold_over_this_on_cases_both_converged":
                          round(float(sc[both].sum()) / max(1.0, float(sw[both].sum())), 3),
+                     "per_residual_threshold": per_threshold,
                      "converged_max_du_over_ulid": max(dmax) if dmax else None}
         for c in cs:
             c.close()

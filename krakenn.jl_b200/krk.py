@@ -13,6 +13,7 @@ never a silent fallback.
 """
 from __future__ import annotations
 
+import ast
 import itertools
 import re
 from dataclasses import dataclass, field, replace
@@ -40,6 +41,30 @@ class SimulationSetup:
         return float(self.physics["nu"])
 
 
+_BINOPS = {ast.Add: lambda a, b: a + b, ast.Sub: lambda a, b: a - b,
+           ast.Mult: lambda a, b: a * b, ast.Div: lambda a, b: a / b,
+           ast.Pow: lambda a, b: a ** b}
+_UNOPS = {ast.UAdd: lambda a: +a, ast.USub: lambda a: -a}
+
+
+def _arith(node, env: dict) -> float:
+    """Evaluate a parsed arithmetic expression: numbers, defined names, + - * / ^
+    (written **) and parentheses.  Anything else (calls, attributes, indexing)
+    is rejected."""
+    if isinstance(node, ast.Expression):
+        return _arith(node.body, env)
+    if isinstance(node, ast.Constant) and isinstance(node.value, (int, float)) \
+            and not isinstance(node.value, bool):
+        return float(node.value)
+    if isinstance(node, ast.Name) and node.id in env:
+        return float(env[node.id])
+    if isinstance(node, ast.BinOp) and type(node.op) in _BINOPS:
+        return _BINOPS[type(node.op)](_arith(node.left, env), _arith(node.right, env))
+    if isinstance(node, ast.UnaryOp) and type(node.op) in _UNOPS:
+        return _UNOPS[type(node.op)](_arith(node.operand, env))
+    raise ValueError("unsupported expression element " + type(node).__name__)
+
+
 def _num(s: str, user_vars: dict) -> float:
     s = s.strip()
     try:
@@ -52,8 +77,8 @@ def _num(s: str, user_vars: dict) -> float:
     if re.fullmatch(r"[\w.eE+\-*/() ]+", s):
         env = {k: float(v) for k, v in user_vars.items() if isinstance(v, (int, float))}
         try:
-            return float(eval(s, {"__builtins__": {}}, env))  # noqa: S307 - restricted names
-        except Exception as exc:  # pragma: no cover - message below
+            return _arith(ast.parse(s, mode="eval"), env)
+        except (SyntaxError, ValueError, ZeroDivisionError, OverflowError) as exc:
             raise ValueError(f"cannot evaluate '{s}' in .krk") from exc
     raise ValueError(f"unknown value '{s}' in .krk")
 

@@ -247,15 +247,19 @@ class PlainCavity:
                         ops.cavity_mrt_step_2d_(y, x, m[0], m[1], m[2], None, N, N, nu, u_lid)
                     x, y = y, x
         self.residual = float("inf")
+        self.reached = {}  # residual threshold -> first checked step count at or below it
 
     def advance(self):
         with torch.cuda.stream(self.stream):
             self.graph.launch()
         self.steps += self.G
 
-    def check(self):
+    def check(self, thresholds=()):
         with torch.cuda.stream(self.stream):
             self.residual = ops.residual(self.m2[1], self.m2[2], self.m1[1], self.m1[2])
+        for t in thresholds:
+            if t not in self.reached and self.residual <= t:
+                self.reached[t] = self.steps
         return self.residual
 
     def fields(self):
@@ -266,9 +270,13 @@ class PlainCavity:
         self.graph.close()
 
 
-def run_to_steady(cases, tol=1e-8, max_steps=2_000_000, check_every=500):
+THRESHOLDS = (1e-4, 1e-5, 1e-6, 1e-7, 1e-8)
+
+
+def run_to_steady(cases, tol=1e-8, max_steps=2_000_000, check_every=500, thresholds=THRESHOLDS):
     """Advance PlainCavity objects concurrently (one stream each) until each
-    reaches r_u <= tol, stops being finite or hits max_steps.  Returns the
+    reaches r_u <= tol, stops being finite or hits max_steps, recording the
+    step count at which each residual threshold is first seen.  Returns the
     wall time in seconds (host clock, the GPU work being synchronised)."""
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -278,7 +286,7 @@ def run_to_steady(cases, tol=1e-8, max_steps=2_000_000, check_every=500):
             c.advance()
         nxt = []
         for c in live:
-            r = c.check()
+            r = c.check(thresholds)
             if math.isfinite(r) and r > tol and c.steps < max_steps:
                 nxt.append(c)
         live = nxt

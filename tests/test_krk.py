@@ -70,3 +70,14 @@ Boundary y periodic
 Run 1000 steps
 """)
     assert st.boundaries["x"][0] == "periodic" and st.user_vars["u0"] == 0.01
+
+
+def test_krk_arithmetic_rejects_code(pkg):
+    """Values in a .krk file are numbers, defined names and + - * / ( );
+    anything else (calls, attributes) is an error, never executed."""
+    k = pkg.krk
+    assert k._num("2*nu+1", {"nu": 0.5}) == 2.0
+    assert k._num("-(3/4)", {}) == -0.75
+    for bad in ("__import__('os')", "nu.real", "f(1)", "1/0"):
+        with pytest.raises(ValueError):
+            k._num(bad, {"nu": 0.5})
