@@ -416,6 +416,10 @@ int kb_surrogate_layer(const kb_surrogate *s, int layer, int *cin, int *cout, in
 /* Output normalisation: the network predicts (x - offset) * scale for
  * x = (rho, ux, uy). */
 int kb_surrogate_set_normalisation(kb_surrogate *s, const float *scale, const float *offset);
+/* Weight gw of the gradient term of the training loss (default 0, the
+ * mean-squared error): L = mean over pixels and channels of
+ * e^2 + gw ((e(x+1) - e(x))^2 + (e(y+1) - e(y))^2), e = prediction - target. */
+int kb_surrogate_set_grad_weight(kb_surrogate *s, float weight);
 /* Copy the FP32 parameters out to `get` and/or in from `set` (device
  * pointers, n_params floats each); `set` also refreshes the BF16 copies. */
 int kb_surrogate_params(kb_surrogate *s, float *get, const float *set, void *stream);

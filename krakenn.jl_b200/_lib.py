@@ -95,6 +95,7 @@ SIGNATURES: dict[str, list] = {
     "kb_surrogate_layer": [_vp, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i),
                            C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
     "kb_surrogate_set_normalisation": [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float)],
+    "kb_surrogate_set_grad_weight": [_vp, C.c_float],
     "kb_surrogate_params": [_vp, _vp, _cvp, _vp],
     "kb_surrogate_grads": [_vp, _vp, _vp],
     "kb_surrogate_cavity_inputs": [_vp, _vp, _cvp, _i, _i, _vp],

@@ -144,26 +144,58 @@ __global__ void skip_grad_k(bf16 *__restrict__ dst, const bf16 *__restrict__ dca
     }
 }
 
-// Mean-squared error over channels 0..2 of the head against the normalised
-// target ((t - offset) * scale, target planar [n][3][H][W]); writes the head
-// gradient (BF16, OUT_CH channels, zero beyond 2) and adds the loss to *loss.
+// Loss over channels 0..2 of the head against the normalised target
+// ((t - offset) * scale, target planar [n][3][H][W]), with e = pred - target:
+//   L = 1/(3M) sum_{pixels, c} [ e_c^2 + gw * ((e_c(x+1) - e_c(x))^2 + (e_c(y+1) - e_c(y))^2) ]
+// The gradient term (an H1 seminorm; gw = 0 gives the mean-squared error)
+// weights an error of wavenumber k by about 1 + gw k^2, so it penalises
+// grid-scale error, which the plain method's slow wall mode picks up, far
+// more than smooth error.  Differences are taken only between pixels of the
+// same image.  Writes dL/dpred (BF16, OUT_CH channels, zero beyond 2) and adds
+// L to *loss.
 struct Norm { float scale[3], offset[3]; };
 
+__device__ __forceinline__ float loss_err(const float *__restrict__ pred, const float *__restrict__ target,
+                                          const Norm &nm, int b, int p, int c, int HW) {
+    const float t = (target[((size_t)b * 3 + c) * HW + p] - nm.offset[c]) * nm.scale[c];
+    return pred[((size_t)b * HW + p) * OUT_CH + c] - t;
+}
+
 __global__ void loss_k(bf16 *__restrict__ grad, float *__restrict__ loss, const float *__restrict__ pred,
-                       const float *__restrict__ target, Norm nm, int M, int HW) {
+                       const float *__restrict__ target, Norm nm, int M, int H, int W, float gw) {
     __shared__ float red[8];
     float acc = 0.f;
+    const int HW = H * W;
     const float gs = 2.0f / (3.0f * (float)M);
     for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
         const int b = m / HW, p = m - b * HW;
+        const int y = p / W, x = p - y * W;
         __align__(16) bf16 g[OUT_CH];
 #pragma unroll
         for (int c = 0; c < OUT_CH; ++c) g[c] = __float2bfloat16_rn(0.f);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const float t = (target[((size_t)b * 3 + c) * HW + p] - nm.offset[c]) * nm.scale[c];
-            const float d = pred[(size_t)m * OUT_CH + c] - t;
-            acc += d * d;
+            const float e = loss_err(pred, target, nm, b, p, c, HW);
+            acc += e * e;
+            float d = e;
+            if (gw != 0.f) {
+                // forward differences owned by this pixel enter the loss; the
+                // gradient collects the differences with all four neighbours
+                float lap = 0.f;
+                if (x + 1 < W) {
+                    const float en = loss_err(pred, target, nm, b, p + 1, c, HW);
+                    acc += gw * (en - e) * (en - e);
+                    lap += e - en;
+                }
+                if (y + 1 < H) {
+                    const float en = loss_err(pred, target, nm, b, p + W, c, HW);
+                    acc += gw * (en - e) * (en - e);
+                    lap += e - en;
+                }
+                if (x > 0) lap += e - loss_err(pred, target, nm, b, p - 1, c, HW);
+                if (y > 0) lap += e - loss_err(pred, target, nm, b, p - W, c, HW);
+                d += gw * lap;
+            }
             g[c] = __float2bfloat16_rn(gs * d);
         }
         uint4 *dst = reinterpret_cast<uint4 *>(grad + (size_t)m * OUT_CH);
@@ -174,9 +206,9 @@ __global__ void loss_k(bf16 *__restrict__ grad, float *__restrict__ loss, const 
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
     __syncthreads();
     if (threadIdx.x == 0) {
-        float s = 0.f;
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[i];
-        atomicAdd(loss, s / (3.0f * (float)M));
+        float sum = 0.f;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) sum += red[i];
+        atomicAdd(loss, sum / (3.0f * (float)M));
     }
 }
 
@@ -295,6 +327,7 @@ struct kb_surrogate {
     int *err = nullptr;
     float *loss = nullptr;
     Norm norm{{1.f, 1.f, 1.f}, {0.f, 0.f, 0.f}};
+    float grad_weight = 0.f;  // weight of the gradient (H1) term of the loss
     std::vector<void *> allocs;
     int H_at(int level) const { return H >> level; }
     int W_at(int level) const { return W >> level; }
@@ -616,6 +649,14 @@ int kb_surrogate_set_normalisation(kb_surrogate *s, const float *scale, const fl
     return 0;
 }
 
+int kb_surrogate_set_grad_weight(kb_surrogate *s, float weight) {
+    KB_REQUIRE(s, "kb_surrogate_set_grad_weight: null handle");
+    KB_REQUIRE(weight >= 0.f && std::isfinite(weight),
+               "kb_surrogate_set_grad_weight: weight must be finite and >= 0");
+    s->grad_weight = weight;
+    return 0;
+}
+
 int kb_surrogate_params(kb_surrogate *s, float *get, const float *set, void *stream) {
     KB_REQUIRE(s, "kb_surrogate_params: null handle");
     cudaStream_t st = kb::as_stream(stream);
@@ -667,7 +708,7 @@ int kb_surrogate_loss_backward(kb_surrogate *s, const void *input, const float *
     const int M = n * s->H * s->W;
     cudaMemsetAsync(s->loss, 0, sizeof(float), st);
     loss_k<<<ew_grid(M), 256, 0, st>>>(s->grad[T_OUT], s->loss, s->out_f32, target, s->norm, M,
-                                        s->H * s->W);
+                                        s->H, s->W, s->grad_weight);
     if (int rc = backward(s, n, st)) return rc;
     if (loss_out) cudaMemcpyAsync(loss_out, s->loss, sizeof(float), cudaMemcpyDeviceToDevice, st);
     return kb::check_launch("kb_surrogate_loss_backward");

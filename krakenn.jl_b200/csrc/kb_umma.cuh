@@ -127,10 +127,11 @@ __host__ __device__ constexpr uint32_t tmem_cols(int bn) { return bn <= 32 ? 32u
 // Op interface:
 //   static constexpr bool A_MN, B_MN;
 //   int bn;                                     N tile width (16..128, multiple of 16)
-//   __device__ void k_range(int &k0, int &k1)  K steps of this CTA
-//   __device__ void load_a(uint32_t s, int kt)  cp.async the 128 x 64 A tile to smem s
-//   __device__ void load_b(uint32_t s, int kt)  cp.async the bn x 64 B tile
-//   __device__ void store(int row, int col, const float *v)  8 columns of row
+//   __device__ void k_range(const uint3 &t, int &k0, int &k1)  K steps of tile t
+//   __device__ void load_a(uint32_t s, int kt, const uint3 &t)  cp.async the 128 x 64 A tile
+//   __device__ void load_b(uint32_t s, int kt, const uint3 &t)  cp.async the bn x 64 B tile
+//   __device__ void store(int row, int col, const float *v, const uint3 &t)  8 columns of row
+// (t = the tile's (m, n, split) coordinates; loads are issued by threads 0..127)
 template <class Op>
 __global__ void __launch_bounds__(THREADS) umma_k(const Op op, int *__restrict__ err, long long spin) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -154,7 +155,8 @@ __global__ void __launch_bounds__(THREADS) umma_k(const Op op, int *__restrict__
     const uint32_t tmem = S.tmem;
     const uint32_t idesc = idesc_bf16(bn, Op::A_MN, Op::B_MN);
     int k0, k1;
-    op.k_range(k0, k1);
+    const uint3 tile = blockIdx;
+    op.k_range(tile, k0, k1);
     const int n = k1 - k0;
     const uint32_t lbo_a = BM * 16, lbo_b = (uint32_t)bn * 16;
     const uint32_t sa0 = smem_u32(S.a[0]), sb0 = smem_u32(S.b[0]);
@@ -163,8 +165,8 @@ __global__ void __launch_bounds__(THREADS) umma_k(const Op op, int *__restrict__
 #pragma unroll
     for (int i = 0; i < STAGES - 1; ++i) {
         if (i < n) {
-            op.load_a(sa0 + i * SA, k0 + i);
-            op.load_b(sb0 + i * SB, k0 + i);
+            op.load_a(sa0 + i * SA, k0 + i, tile);
+            op.load_b(sb0 + i * SB, k0 + i, tile);
         }
         cp_commit();
     }
@@ -199,8 +201,8 @@ __global__ void __launch_bounds__(THREADS) umma_k(const Op op, int *__restrict__
                 phase_bits ^= 1u << sp;
             }
             if (ok) {
-                op.load_a(sa0 + sp * SA, k0 + nx);
-                op.load_b(sb0 + sp * SB, k0 + nx);
+                op.load_a(sa0 + sp * SA, k0 + nx, tile);
+                op.load_b(sb0 + sp * SB, k0 + nx, tile);
             }
         }
         cp_commit();
@@ -221,11 +223,11 @@ __global__ void __launch_bounds__(THREADS) umma_k(const Op op, int *__restrict__
         for (int c0 = 0; c0 < bn; c0 += 8) {
             float v[8];
             tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-            op.store(row, c0, v);
+            op.store(row, c0, v, tile);
         }
     } else {
         const float z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (int c0 = 0; c0 < bn; c0 += 8) op.store(row, c0, z);
+        for (int c0 = 0; c0 < bn; c0 += 8) op.store(row, c0, z, tile);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -298,11 +300,11 @@ struct ConvOp {
     void *out;                // [M][Nout] BF16 or FP32
     int M, Nout, Kp, bn, relu, out_f32, nsteps;
 
-    __device__ void k_range(int &k0, int &k1) const { k0 = 0; k1 = nsteps; }
+    __device__ void k_range(const uint3 &t, int &k0, int &k1) const { k0 = 0; k1 = nsteps; }
 
-    __device__ void load_a(uint32_t s, int kt) const {
+    __device__ void load_a(uint32_t s, int kt, const uint3 &t) const {
         const int r = threadIdx.x;  // one tile row (pixel) per thread
-        const int m = blockIdx.x * BM + r;
+        const int m = t.x * BM + r;
         const int C = x.C(), K9 = 9 * C;
         int b = 0, h = 0, w = 0;
         const bool live = m < M;
@@ -313,15 +315,15 @@ struct ConvOp {
             bool v = false;
             const __nv_bfloat16 *p = x.s1;
             if (live && k < K9) {
-                const int t = k / C, c = k - t * C;
-                p = x.chunk_ptr(b, h + t / 3 - 1, w + t % 3 - 1, c, v);
+                const int tap = k / C, c = k - tap * C;
+                p = x.chunk_ptr(b, h + tap / 3 - 1, w + tap % 3 - 1, c, v);
             }
             cp16(s + (uint32_t)(kc * BM * 16 + r * 16), p, v);
         }
     }
 
-    __device__ void load_b(uint32_t s, int kt) const {
-        const int n0 = blockIdx.y * bn;
+    __device__ void load_b(uint32_t s, int kt, const uint3 &t) const {
+        const int n0 = t.y * bn;
         for (int c = threadIdx.x; c < bn * 8; c += THREADS) {
             const int r = c % bn, kc = c / bn;
             cp16(s + (uint32_t)(kc * bn * 16 + r * 16), wt + (size_t)(n0 + r) * Kp + kt * BK + kc * 8,
@@ -329,10 +331,10 @@ struct ConvOp {
         }
     }
 
-    __device__ void store(int row, int col, const float *v) const {
-        const int m = blockIdx.x * BM + row;
+    __device__ void store(int row, int col, const float *v, const uint3 &t) const {
+        const int m = t.x * BM + row;
         if (m >= M) return;
-        const int n = blockIdx.y * bn + col;
+        const int n = t.y * bn + col;
         float o[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
@@ -374,16 +376,16 @@ struct WgradOp {
     float *part;              // [splits][9C + 1][Nout]
     int M, Nout, bn, steps_per_split, nsteps;
 
-    __device__ void k_range(int &k0, int &k1) const {
-        k0 = blockIdx.z * steps_per_split;
+    __device__ void k_range(const uint3 &t, int &k0, int &k1) const {
+        k0 = t.z * steps_per_split;
         k1 = min(nsteps, k0 + steps_per_split);
     }
 
-    __device__ void load_a(uint32_t s, int kt) const {
+    __device__ void load_a(uint32_t s, int kt, const uint3 &t) const {
         const int C = x.C(), R = 9 * C;
         const int k_lo = threadIdx.x & 7, g = (threadIdx.x >> 3) & 15;
-        const int r = blockIdx.x * BM + g * 8;
-        const int t = r / C, c = r - t * C;
+        const int r = t.x * BM + g * 8;
+        const int tap = r / C, c = r - tap * C;
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const int m = kt * BK + i * 8 + k_lo;
@@ -393,7 +395,7 @@ struct WgradOp {
                 if (r < R) {
                     int b, h, w;
                     pixel_of(m, x.H, x.W, b, h, w);
-                    p = x.chunk_ptr(b, h + t / 3 - 1, w + t % 3 - 1, c, v);
+                    p = x.chunk_ptr(b, h + tap / 3 - 1, w + tap % 3 - 1, c, v);
                 } else if (r == R) {
                     p = kOneChunk;  // bf16 1.0 in element 0: the bias row
                     v = true;
@@ -403,8 +405,8 @@ struct WgradOp {
         }
     }
 
-    __device__ void load_b(uint32_t s, int kt) const {
-        const int groups = bn >> 3, n0 = blockIdx.y * bn;
+    __device__ void load_b(uint32_t s, int kt, const uint3 &t) const {
+        const int groups = bn >> 3, n0 = t.y * bn;
         for (int c = threadIdx.x; c < bn * 8; c += THREADS) {
             const int k_lo = c & 7, g = (c >> 3) % groups, k_hi = (c >> 3) / groups;
             const int m = kt * BK + k_hi * 8 + k_lo;
@@ -414,12 +416,12 @@ struct WgradOp {
         }
     }
 
-    __device__ void store(int row, int col, const float *v) const {
+    __device__ void store(int row, int col, const float *v, const uint3 &t) const {
         const int R = 9 * x.C();
-        const int r = blockIdx.x * BM + row;
+        const int r = t.x * BM + row;
         if (r > R) return;
-        const int n = blockIdx.y * bn + col;
-        float4 *d = reinterpret_cast<float4 *>(part + ((size_t)blockIdx.z * (R + 1) + r) * Nout + n);
+        const int n = t.y * bn + col;
+        float4 *d = reinterpret_cast<float4 *>(part + ((size_t)t.z * (R + 1) + r) * Nout + n);
         d[0] = make_float4(v[0], v[1], v[2], v[3]);
         d[1] = make_float4(v[4], v[5], v[6], v[7]);
     }
@@ -434,7 +436,7 @@ struct GemmOp {
     float *c;
     int M, N, K, bn;
 
-    __device__ void k_range(int &k0, int &k1) const { k0 = 0; k1 = K / BK; }
+    __device__ void k_range(const uint3 &t, int &k0, int &k1) const { k0 = 0; k1 = K / BK; }
 
     __device__ static void load(uint32_t s, const __nv_bfloat16 *src, int rows, int r0, int ld_rows,
                                 int K, int kt, bool mn) {
@@ -454,10 +456,10 @@ struct GemmOp {
             cp16(s + off, p, true);
         }
     }
-    __device__ void load_a(uint32_t s, int kt) const { load(s, a, BM, blockIdx.x * BM, M, K, kt, AMN); }
-    __device__ void load_b(uint32_t s, int kt) const { load(s, b, bn, blockIdx.y * bn, N, K, kt, BMN); }
-    __device__ void store(int row, int col, const float *v) const {
-        const int m = blockIdx.x * BM + row, n = blockIdx.y * bn + col;
+    __device__ void load_a(uint32_t s, int kt, const uint3 &t) const { load(s, a, BM, t.x * BM, M, K, kt, AMN); }
+    __device__ void load_b(uint32_t s, int kt, const uint3 &t) const { load(s, b, bn, t.y * bn, N, K, kt, BMN); }
+    __device__ void store(int row, int col, const float *v, const uint3 &t) const {
+        const int m = t.x * BM + row, n = t.y * bn + col;
         float4 *d = reinterpret_cast<float4 *>(c + (size_t)m * N + n);
         d[0] = make_float4(v[0], v[1], v[2], v[3]);
         d[1] = make_float4(v[4], v[5], v[6], v[7]);

@@ -59,6 +59,7 @@ class Surrogate:
         self.set_normalisation(scale, offset)
         self._loss = torch.zeros(1, dtype=torch.float32, device="cuda")
         self.step = 0
+        self.grad_weight = 0.0
 
     def close(self):
         if self._h:
@@ -76,6 +77,11 @@ class Surrogate:
         o = (C.c_float * 3)(*offset)
         call("kb_surrogate_set_normalisation", self._h, s, o)
         self.scale, self.offset = tuple(scale), tuple(offset)
+
+    def set_grad_weight(self, weight):
+        """Weight of the gradient (H1) term of the training loss (0: plain MSE)."""
+        call("kb_surrogate_set_grad_weight", self._h, C.c_float(weight))
+        self.grad_weight = float(weight)
 
     def layers(self):
         out = []
@@ -297,9 +303,12 @@ def run_to_steady(cases, tol=1e-8, max_steps=2_000_000, check_every=500, thresho
 # ----------------------------------------------------------------- train --
 
 def train(model, re, targets, epochs=100, batch=16, lr=1e-3, lr_min=1e-5, seed=0,
-          n_nodes=None, log_every=0):
+          n_nodes=None, log_every=0, grad_weight=None):
     """Adam on minibatches of (input from Re, target field), cosine decay of
-    the learning rate.  Returns the per-epoch mean loss."""
+    the learning rate; grad_weight (if given) sets the loss's gradient term.
+    Returns the per-epoch mean loss."""
+    if grad_weight is not None:
+        model.set_grad_weight(grad_weight)
     re = torch.as_tensor(np.asarray(re), dtype=torch.float32, device="cuda")
     n = re.numel()
     g = torch.Generator(device="cpu").manual_seed(seed)

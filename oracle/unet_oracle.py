@@ -15,7 +15,8 @@ Conventions shared with the CUDA code:
     parameter array holds W then b for each layer in order;
   * ReLU after every convolution but the head, 2x2 average pooling,
     nearest-neighbour upsampling, skip concatenation [upsampled, skip];
-  * loss = mean over pixels and the 3 channels of (pred - (t - off)*scale)^2.
+  * loss = mean over pixels and the 3 channels of e^2 + gw ((e(x+1) - e(x))^2 +
+    (e(y+1) - e(y))^2), e = pred - (t - off)*scale (gw = 0: mean-squared error).
 """
 from __future__ import annotations
 
@@ -138,7 +139,7 @@ def normalised_target(target, scale, offset):
     return (t - np.asarray(offset)) * np.asarray(scale)
 
 
-def loss_and_grad(params, x, target, scale, offset, C, round_bf16=False):
+def loss_and_grad(params, x, target, scale, offset, C, round_bf16=False, grad_weight=0.0):
     """Mean-squared error and its gradient with respect to the flat
     parameters.  With round_bf16 the activations and the activation gradients
     are rounded to BF16 where the CUDA kernels store them (the head gradient,
@@ -150,10 +151,18 @@ def loss_and_grad(params, x, target, scale, offset, C, round_bf16=False):
     t = normalised_target(target, scale, offset)
     d = out[..., :3] - t
     M = d.shape[0] * d.shape[1] * d.shape[2]
-    loss = float(np.sum(d * d) / (3 * M))
+    # e^2 + gw * (forward differences in x and y)^2, within each image
+    dx = d[:, :, 1:] - d[:, :, :-1]
+    dy = d[:, 1:, :] - d[:, :-1, :]
+    loss = float((np.sum(d * d) + grad_weight * (np.sum(dx * dx) + np.sum(dy * dy))) / (3 * M))
+    lap = np.zeros_like(d)                     # sum over neighbours of (e - e_neighbour)
+    lap[:, :, :-1] -= dx
+    lap[:, :, 1:] += dx
+    lap[:, :-1, :] -= dy
+    lap[:, 1:, :] += dy
     grads = np.zeros(n)
     g = {"out": np.zeros_like(out)}
-    g["out"][..., :3] = rnd(2.0 * d / (3 * M))
+    g["out"][..., :3] = rnd(2.0 * (d + grad_weight * lap) / (3 * M))
     dcat = {}
     for li in range(len(LAYERS) - 1, -1, -1):
         in1, in2, o, relu, pooled = LAYERS[li]

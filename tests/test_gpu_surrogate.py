@@ -108,7 +108,8 @@ def test_network_forward_matches_oracle(cuda, sur):
     model.close()
 
 
-def test_network_gradients_match_oracle(cuda, sur):
+@pytest.mark.parametrize("gw", [0.0, 5.0])
+def test_network_gradients_match_oracle(cuda, sur, gw):
     """Per-layer parameter gradients of the MSE loss against the FP64 oracle
     on the same BF16 weights.  The oracle run that rounds activations and
     their gradients to BF16 where the kernels do differs from the kernels only
@@ -116,10 +117,12 @@ def test_network_gradients_match_oracle(cuda, sur):
     (relative L2 error below 0.1 per layer); against the unrounded oracle the
     cosine stays above 0.98.  A wrong operand layout gives O(1) errors."""
     model, x, xo, pq, tgt, table = _net_case(sur)
+    model.set_grad_weight(gw)
     loss = model.loss_backward(x, torch.from_numpy(tgt).float())
     g = model.grads().double().cpu().numpy()
-    lr_, gr = U.loss_and_grad(pq, xo, tgt, model.scale, model.offset, 16, round_bf16=True)
-    le, ge = U.loss_and_grad(pq, xo, tgt, model.scale, model.offset, 16)
+    lr_, gr = U.loss_and_grad(pq, xo, tgt, model.scale, model.offset, 16, round_bf16=True,
+                              grad_weight=gw)
+    le, ge = U.loss_and_grad(pq, xo, tgt, model.scale, model.offset, 16, grad_weight=gw)
     assert abs(float(loss.item()) - lr_) <= 1e-3 * lr_
     assert abs(float(loss.item()) - le) <= 2e-2 * le
     rows = []

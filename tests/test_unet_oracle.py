@@ -31,16 +31,17 @@ def test_layer_table_matches_channel_plan(net):
     assert U.layer_table(32)[1] == 1952912  # parameters of the 32-channel network
 
 
-def test_gradient_matches_central_differences_per_layer(net):
+@pytest.mark.parametrize("gw", [0.0, 5.0])
+def test_gradient_matches_central_differences_per_layer(net, gw):
     p, x, tgt, sc, off, C = net["p"], net["x"], net["tgt"], net["sc"], net["off"], net["C"]
-    _, g = U.loss_and_grad(p, x, tgt, sc, off, C)
+    _, g = U.loss_and_grad(p, x, tgt, sc, off, C, grad_weight=gw)
     rng = np.random.default_rng(1)
     eps = 1e-7
     for li, (cin, cout, wo, bo) in enumerate(net["table"]):
         v = np.zeros_like(p)
         v[wo:bo + cout] = rng.normal(0.0, 1.0, bo + cout - wo)
-        lp, _ = U.loss_and_grad(p + eps * v, x, tgt, sc, off, C)
-        lm, _ = U.loss_and_grad(p - eps * v, x, tgt, sc, off, C)
+        lp, _ = U.loss_and_grad(p + eps * v, x, tgt, sc, off, C, grad_weight=gw)
+        lm, _ = U.loss_and_grad(p - eps * v, x, tgt, sc, off, C, grad_weight=gw)
         fd = (lp - lm) / (2 * eps)
         an = float(g @ v)
         assert abs(fd - an) <= 1e-5 * max(abs(an), 1e-3), (li, fd, an)
