@@ -318,11 +318,21 @@ int face_fixed(const Face &F, int Nx, int Ny, int Nz) {
 namespace {
 int g_trt3d_dev_variant = 0;  // see kb_set_kernel_variant
 }
+namespace kb {
+namespace umma {
+void set_engine(int e);  // kb_umma.cu
+}
+}
 
 extern "C" {
 
 int kb_set_kernel_variant(int kernel, int variant) {
-    KB_REQUIRE(kernel == 1, "kb_set_kernel_variant: unknown kernel id %d", kernel);
+    KB_REQUIRE(kernel == 1 || kernel == 2, "kb_set_kernel_variant: unknown kernel id %d", kernel);
+    if (kernel == 2) {
+        KB_REQUIRE(variant == 0 || variant == 1, "kb_set_kernel_variant: engine %d not in 0..1", variant);
+        kb::umma::set_engine(variant);
+        return KB_OK;
+    }
     KB_REQUIRE(variant >= 0 && variant <= 4, "kb_set_kernel_variant: variant %d not in 0..4", variant);
     g_trt3d_dev_variant = variant;
     return KB_OK;

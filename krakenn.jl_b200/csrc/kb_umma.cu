@@ -7,6 +7,10 @@
 namespace kb {
 namespace umma {
 
+static int g_engine = 0;
+int engine() { return g_engine; }
+void set_engine(int e) { g_engine = e; }
+
 int pick_bn(int n) {
     for (int bn = NT; bn >= 16; bn -= 16)
         if (n % bn == 0) return bn;

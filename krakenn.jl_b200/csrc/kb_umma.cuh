@@ -238,6 +238,188 @@ __global__ void __launch_bounds__(THREADS) umma_k(const Op op, int *__restrict__
 inline size_t smem_bytes() { return sizeof(Smem) + 1024; }
 
 // ---------------------------------------------------------------------------
+// Warp-specialised persistent form of the mainloop.  One CTA per SM loops
+// over the tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... of the grid
+// `tiles` (x fastest):
+//   warps 0-3  producers: cp.async every K step of every tile into a ring of
+//              WS_STAGES shared-memory stages; after a step's copies land
+//              (one step of lag), each producer thread fences them to the
+//              async proxy and arrives on the stage's `full` barrier
+//   warp 8     MMA: lane 0 waits `full`, issues the four tcgen05.mma of the
+//              step into one of two TMEM accumulators, commits to the stage's
+//              `empty` barrier, and after a tile's last step to `acc_full`
+//   warps 4-7  epilogue: warp w reads TMEM lanes 32(w%4)..+31 of the finished
+//              accumulator, calls op.store, and arrives on `acc_empty`
+// so the loads of the next steps and the epilogue of tile j overlap the MMAs
+// of tile j+1.  Every wait is bounded; a role that gives up stops, sets *err,
+// and the others run out of their own bounded waits.
+constexpr int WS_STAGES = 4, WS_THREADS = 288;
+
+struct SmemWS {
+    alignas(128) unsigned char a[WS_STAGES][BM * BK * 2];
+    alignas(128) unsigned char b[WS_STAGES][NT * BK * 2];
+    uint64_t full[WS_STAGES], empty[WS_STAGES], acc_full[2], acc_empty[2], drain;
+    uint32_t tmem;
+};
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ uint3 tile_of(long long T, const uint3 &n) {
+    uint3 t;
+    t.x = (unsigned)(T % n.x);
+    const long long r = T / n.x;
+    t.y = (unsigned)(r % n.y);
+    t.z = (unsigned)(r / n.y);
+    return t;
+}
+
+template <class Op>
+__global__ void __launch_bounds__(WS_THREADS, 1) umma_ws_k(const Op op, const uint3 tiles,
+                                                           int *__restrict__ err, long long spin) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    SmemWS &S = *reinterpret_cast<SmemWS *>(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bn = op.bn;
+    const uint32_t cols = tmem_cols(bn);  // per accumulator; two of them
+    const long long ntiles = (long long)tiles.x * tiles.y * tiles.z;
+    constexpr uint32_t SA = BM * BK * 2, SB = NT * BK * 2;
+
+    if (warp == 8) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&S.tmem)), "r"(2 * cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < WS_STAGES; ++i) {
+            mbar_init(&S.full[i], 128);
+            mbar_init(&S.empty[i], 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&S.acc_full[i], 1);
+            mbar_init(&S.acc_empty[i], 128);
+        }
+        mbar_init(&S.drain, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = S.tmem;
+    bool ok = true;
+
+    if (warp < 4) {
+        // ------------------------------------------------------ producers
+        const uint32_t sa0 = smem_u32(S.a[0]), sb0 = smem_u32(S.b[0]);
+        long long g = 0;
+        for (long long T = blockIdx.x; T < ntiles && ok; T += gridDim.x) {
+            const uint3 t = tile_of(T, tiles);
+            int k0, k1;
+            op.k_range(t, k0, k1);
+            for (int kt = k0; kt < k1; ++kt, ++g) {
+                const int s = (int)(g % WS_STAGES);
+                const long long use = g / WS_STAGES;
+                if (use >= 1) {
+                    ok = mbar_wait(&S.empty[s], (uint32_t)((use - 1) & 1), spin);
+                    if (!ok) break;
+                }
+                op.load_a(sa0 + s * SA, kt, t);
+                op.load_b(sb0 + s * SB, kt, t);
+                cp_commit();
+                if (g >= 1) {
+                    cp_wait<1>();
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    mbar_arrive(&S.full[(g - 1) % WS_STAGES]);
+                }
+            }
+        }
+        cp_wait<0>();
+        if (ok && g >= 1) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(&S.full[(g - 1) % WS_STAGES]);
+        }
+    } else if (warp == 8) {
+        // ------------------------------------------------------ MMA issue
+        if (lane == 0) {
+            const uint32_t idesc = idesc_bf16(bn, Op::A_MN, Op::B_MN);
+            const uint32_t lbo_a = BM * 16, lbo_b = (uint32_t)bn * 16;
+            const uint32_t sa0 = smem_u32(S.a[0]), sb0 = smem_u32(S.b[0]);
+            long long g = 0;
+            int j = 0;
+            bool issued = false;
+            for (long long T = blockIdx.x; T < ntiles && ok; T += gridDim.x, ++j) {
+                const int buf = j & 1;
+                if (j >= 2) {
+                    ok = mbar_wait(&S.acc_empty[buf], (uint32_t)(((j >> 1) - 1) & 1), spin);
+                    if (!ok) break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint3 t = tile_of(T, tiles);
+                int k0, k1;
+                op.k_range(t, k0, k1);
+                const uint32_t acc = tmem + (uint32_t)buf * cols;
+                for (int kt = k0; kt < k1; ++kt, ++g) {
+                    const int s = (int)(g % WS_STAGES);
+                    ok = mbar_wait(&S.full[s], (uint32_t)((g / WS_STAGES) & 1), spin);
+                    if (!ok) break;
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t sa = sa0 + s * SA, sb = sb0 + s * SB;
+#pragma unroll
+                    for (int kk = 0; kk < BK / 16; ++kk) {
+                        const uint64_t da = sdesc(sa + kk * 2 * lbo_a, lbo_a, 128);
+                        const uint64_t db = sdesc(sb + kk * 2 * lbo_b, lbo_b, 128);
+                        mma_bf16(acc, da, db, idesc, (kt > k0 || kk > 0) ? 1u : 0u);
+                    }
+                    mma_commit(&S.empty[s]);
+                    issued = true;
+                }
+                if (!ok) break;
+                mma_commit(&S.acc_full[buf]);
+            }
+            // every MMA issued above is complete once this commit arrives
+            mma_commit(&S.drain);
+            if (!mbar_wait(&S.drain, 0u, spin)) ok = false;
+            (void)issued;
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------------------------------ epilogue
+        const int q = warp & 3;
+        const int row = q * 32 + lane;
+        int j = 0;
+        for (long long T = blockIdx.x; T < ntiles && ok; T += gridDim.x, ++j) {
+            const int buf = j & 1;
+            ok = mbar_wait(&S.acc_full[buf], (uint32_t)((j >> 1) & 1), spin);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint3 t = tile_of(T, tiles);
+            int k0, k1;
+            op.k_range(t, k0, k1);
+            if (k1 > k0) {
+                for (int c0 = 0; c0 < bn; c0 += 8) {
+                    float v[8];
+                    tmem_ld8(tmem + (uint32_t)buf * cols + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
+                    op.store(row, c0, v, t);
+                }
+            } else {
+                const float z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                for (int c0 = 0; c0 < bn; c0 += 8) op.store(row, c0, z, t);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            mbar_arrive(&S.acc_empty[buf]);
+        }
+    }
+    if (!ok) atomicExch(err, 1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 8)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * cols));
+}
+
+inline size_t smem_bytes_ws() { return sizeof(SmemWS) + 1024; }
+
+// ---------------------------------------------------------------------------
 // Activation view: the input of a 3x3 convolution at resolution H x W, NHWC
 // BF16.  Channels [0, c1) come from s1, stored at (H >> up1) x (W >> up1)
 // (nearest-neighbour upsampling when up1 = 1); channels [c1, c1 + c2) come from
@@ -477,8 +659,31 @@ int pick_bn(int n);
 
 // Launch umma_k<Op> with the dynamic shared memory it needs.  The attribute
 // is set once per device and instantiation.
+// Engine choice for the convolutions and the plain GEMM: 0 the warp-
+// specialised persistent kernel (default), 1 one CTA per tile.
+int engine();
+
+template <class Op>
+int launch_ws(const Op &op, dim3 grid, int *err, cudaStream_t stream, long long spin = 1ll << 22) {
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(umma_ws_k<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem_bytes_ws());
+        if (e != cudaSuccess) return kb::check_launch("umma_ws_k: shared-memory attribute");
+        configured[dev] = true;
+    }
+    const long long ntiles = (long long)grid.x * grid.y * grid.z;
+    const long long ctas = ntiles < kb::sm_count() ? ntiles : kb::sm_count();
+    umma_ws_k<Op><<<(unsigned)ctas, WS_THREADS, smem_bytes_ws(), stream>>>(
+        op, make_uint3(grid.x, grid.y, grid.z), err, spin);
+    return 0;
+}
+
 template <class Op>
 int launch(const Op &op, dim3 grid, int *err, cudaStream_t stream, long long spin = 1ll << 22) {
+    if (engine() == 0) return launch_ws(op, grid, err, stream, spin);
     static bool configured[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);

@@ -422,6 +422,12 @@ def set_trt3d_variant(variant: int):
     call("kb_set_kernel_variant", 1, int(variant))
 
 
+def set_umma_engine(engine: int):
+    """Tensor-core engine of the warm-start network and kb_gemm_bf16: 0 the
+    warp-specialised persistent kernel (default), 1 one CTA per output tile."""
+    call("kb_set_kernel_variant", 2, int(engine))
+
+
 def periodic_mask(periodic) -> int:
     if isinstance(periodic, int):
         return periodic
@@ -500,7 +506,7 @@ def synchronize():
 
 __all__ = [n for n in dir() if n.endswith("_") and not n.startswith("_")] + [
     "trt_rates", "convert_populations", "mass", "residual", "synchronize", "storage_dtype",
-    "set_trt3d_variant", "set_stochastic_seed", "AA_SWAP_2D",
+    "set_trt3d_variant", "set_stochastic_seed", "set_umma_engine", "AA_SWAP_2D",
     "torch_dtype", "field_dtype", "periodic_mask", "FACES_3D"]
 
 _ = _lib  # keep the module import explicit for readers

@@ -21,11 +21,13 @@ def _bf16(shape, gen):
     return torch.randn(shape, generator=gen).to(torch.bfloat16).cuda()
 
 
+@pytest.mark.parametrize("engine", [0, 1])
 @pytest.mark.parametrize("a_mn,b_mn", [(0, 0), (1, 1), (1, 0), (0, 1)])
 @pytest.mark.parametrize("N,K", [(16, 64), (48, 128), (96, 192), (128, 64), (256, 320)])
-def test_gemm_bf16_both_majors(cuda, pkg, a_mn, b_mn, N, K):
+def test_gemm_bf16_both_majors(cuda, pkg, a_mn, b_mn, N, K, engine):
     """C = A B^T on tcgen05 with FP32 accumulation equals the FP64 product of
-    the same BF16 operands to FP32 summation error."""
+    the same BF16 operands to FP32 summation error, with the warp-specialised
+    persistent engine (0) and the one-CTA-per-tile engine (1)."""
     import ctypes as C
     from importlib import import_module
     lib = import_module(pkg.__name__ + "._lib")
@@ -36,10 +38,14 @@ def test_gemm_bf16_both_majors(cuda, pkg, a_mn, b_mn, N, K):
     b = B.t().contiguous() if b_mn else B
     out = torch.full((M, N), float("nan"), dtype=torch.float32, device="cuda")
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
-    lib.call("kb_gemm_bf16", C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()),
-             C.c_void_p(out.data_ptr()), M, N, K, a_mn, b_mn, C.c_void_p(err.data_ptr()),
-             C.c_void_p(torch.cuda.current_stream().cuda_stream))
-    torch.cuda.synchronize()
+    pkg.set_umma_engine(engine)
+    try:
+        lib.call("kb_gemm_bf16", C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()),
+                 C.c_void_p(out.data_ptr()), M, N, K, a_mn, b_mn, C.c_void_p(err.data_ptr()),
+                 C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+    finally:
+        pkg.set_umma_engine(0)
     ref = A.double() @ B.double().t()
     assert int(err.item()) == 0
     tol = 1e-5 * float(ref.abs().max())
@@ -134,6 +140,25 @@ def test_network_gradients_match_oracle(cuda, sur, gw):
         rows.append((li, round(float(rel), 5), round(cos, 5)))
     print("per-layer (layer, rel vs rounded oracle, cosine vs exact):", rows)
     assert all(r < 0.1 and c > 0.98 for _, r, c in rows), rows
+    assert not model.timed_out()
+    model.close()
+
+
+def test_engines_agree_bit_for_bit(cuda, pkg, sur):
+    """Both tensor-core engines accumulate the K steps of a tile in the same
+    order, so the network's output and gradients are identical."""
+    model, x, xo, pq, tgt, table = _net_case(sur)
+    outs = []
+    try:
+        for engine in (1, 0):
+            pkg.set_umma_engine(engine)
+            o = model.infer(x).clone()
+            model.loss_backward(x, torch.from_numpy(tgt).float())
+            outs.append((o, model.grads()))
+    finally:
+        pkg.set_umma_engine(0)
+    assert torch.equal(outs[0][0], outs[1][0])
+    assert torch.equal(outs[0][1], outs[1][1])
     assert not model.timed_out()
     model.close()
 
