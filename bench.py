@@ -642,7 +642,7 @@ def bench_natconv_validation(pkg, N=512, steps_by_ra=None):
 
 def bench_warmstart(pkg, N=256, n_train=2000, n_test=64, epochs=40, batch=16, base=32,
                     data_steps=200000, data_tol=1e-6, tol=1e-8, max_steps=2000000,
-                    check_every=1000, init_iters=500, seed=0):
+                    check_every=1000, init_iters=500, grad_weight=200.0, seed=0):
     """Learned warm start: train the encoder-decoder on n_train steady N^2
     cavities from the batched kernel (Re log-uniform [100, 3200], u_lid 0.1),
     then run n_test held-out cases to r_u <= tol with the plain FP64 MRT step
@@ -658,7 +658,8 @@ def bench_warmstart(pkg, N=256, n_train=2000, n_test=64, epochs=40, batch=16, ba
     out = {"workload": f"learned warm start, {N}^2 lid-driven MRT cavities, Re log-uniform "
                        f"[100,3200], u_lid=0.1; {n_train} training / {n_test} held-out cases; "
                        f"4-level U-Net, {base} base channels, BF16 tcgen05, batch {batch}, "
-                       f"{epochs} epochs; plain FP64 MRT to r_u <= {tol:g} (cap {max_steps} steps)"}
+                       f"{epochs} epochs, loss MSE + {grad_weight:g} x gradient term; plain FP64 "
+                       f"MRT to r_u <= {tol:g} (cap {max_steps} steps)"}
     re_tr, re_te = sur.held_out_split(n_train, n_test, seed=seed)
     e0, e1 = _events()
     e0.record()
@@ -679,7 +680,8 @@ def bench_warmstart(pkg, N=256, n_train=2000, n_test=64, epochs=40, batch=16, ba
     re_tr = re_tr[keep.numpy()]
     model = sur.Surrogate(max_batch=batch, H=N, W=N, base_channels=base, seed=seed)
     e0.record()
-    hist = sur.train(model, re_tr, fields, epochs=epochs, batch=batch, lr=1e-3, lr_min=2e-5)
+    hist = sur.train(model, re_tr, fields, epochs=epochs, batch=batch, lr=1e-3, lr_min=2e-5,
+                     grad_weight=grad_weight)
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
