@@ -264,8 +264,8 @@ int kb_fused_trt_step_3d(void *f_out, const void *f_in, void *rho, void *ux, voi
  * (16-bit storages, Nx % 4 == 0).
  * Variants 2, 3 and 4 collide in packed FP32x2 arithmetic.
  * kernel 2 = the tensor-core engine of the warm-start network and
- * kb_gemm_bf16: 0 warp-specialised persistent kernel (default), 1 one CTA
- * per output tile.  Every variant
+ * kb_gemm_bf16: 0 warp-specialised persistent kernel, 1 one CTA per output
+ * tile (default).  Every variant
  * computes the same update up to FP32 rounding.  No reference counterpart. */
 int kb_set_kernel_variant(int kernel, int variant);
 

@@ -660,7 +660,9 @@ int pick_bn(int n);
 // Launch umma_k<Op> with the dynamic shared memory it needs.  The attribute
 // is set once per device and instantiation.
 // Engine choice for the convolutions and the plain GEMM: 0 the warp-
-// specialised persistent kernel (default), 1 one CTA per tile.
+// specialised persistent kernel, 1 one CTA per tile (default: with cp.async
+// operand staging the persistent kernel's four producer warps are
+// instruction-bound, and two independent CTAs per SM load faster).
 int engine();
 
 template <class Op>

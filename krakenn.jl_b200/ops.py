@@ -424,7 +424,7 @@ def set_trt3d_variant(variant: int):
 
 def set_umma_engine(engine: int):
     """Tensor-core engine of the warm-start network and kb_gemm_bf16: 0 the
-    warp-specialised persistent kernel (default), 1 one CTA per output tile."""
+    warp-specialised persistent kernel, 1 one CTA per output tile (default)."""
     call("kb_set_kernel_variant", 2, int(engine))
 
 

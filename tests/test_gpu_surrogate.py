@@ -45,7 +45,7 @@ def test_gemm_bf16_both_majors(cuda, pkg, a_mn, b_mn, N, K, engine):
                  C.c_void_p(torch.cuda.current_stream().cuda_stream))
         torch.cuda.synchronize()
     finally:
-        pkg.set_umma_engine(0)
+        pkg.set_umma_engine(1)
     ref = A.double() @ B.double().t()
     assert int(err.item()) == 0
     tol = 1e-5 * float(ref.abs().max())
@@ -159,7 +159,7 @@ def test_engines_agree_bit_for_bit(cuda, pkg, sur):
             model.loss_backward(x, torch.from_numpy(tgt).float())
             outs.append((o, model.grads()))
     finally:
-        pkg.set_umma_engine(0)
+        pkg.set_umma_engine(1)
     assert torch.equal(outs[0][0], outs[1][0])
     assert torch.equal(outs[0][1], outs[1][1])
     assert not model.timed_out()
