@@ -751,6 +751,62 @@ def bench_warmstart(pkg, N=256, n_train=2000, n_test=64, epochs=40, batch=16, ba
     return out
 
 
+def bench_surrogate(pkg, steps=10, warmup=3, batch=16, N=256, base=32, engine=None):
+    """Throughput of the warm-start network on the tensor cores: `steps` timed
+    training steps (forward, MSE + gradient-term loss, backward, Adam) and
+    forward passes of `batch` cavities at N^2, after `warmup` untimed steps;
+    TFLOP/s against the measured dense BF16 peak."""
+    import numpy as np
+    import torch
+    from importlib import import_module
+    sur = import_module(pkg.__name__ + ".surrogate")
+    if engine is not None:
+        pkg.set_umma_engine(engine)
+    m = sur.Surrogate(max_batch=batch, H=N, W=N, base_channels=base, seed=0)
+    m.set_grad_weight(200.0)
+    re = np.exp(np.random.default_rng(0).uniform(np.log(100.0), np.log(3200.0), batch))
+    x = m.inputs(re, N)
+    tgt = torch.zeros((batch, 3, N, N), device="cuda")
+    tgt[:, 0] = 1.0
+    fwd, trn = m.flops(batch)
+    for _ in range(warmup):
+        m.train_step(x, tgt, 1e-5)
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(steps):
+        m.train_step(x, tgt, 1e-5)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_t = e0.elapsed_time(e1) / steps
+    e0.record()
+    for _ in range(steps):
+        m.infer(x)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_i = e0.elapsed_time(e1) / steps
+    peak = None
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            peak = d.get("bf16_tflops_sustained") or d.get("bf16_tflops")
+        except (ValueError, OSError):
+            peak = None
+    peak = float(peak) if peak else 1390.0
+    out = {"workload": f"warm-start U-Net, {N}^2, batch {batch}, {base} base channels, BF16 "
+                       f"tcgen05, engine {1 if engine is None else engine}",
+           "train_ms": round(ms_t, 3), "train_tflops": round(trn / (ms_t * 1e-3) / 1e12, 1),
+           "infer_ms": round(ms_i, 3), "infer_tflops": round(fwd / (ms_i * 1e-3) / 1e12, 1),
+           "bf16_peak_tflops": peak,
+           "train_frac_of_peak": round(trn / (ms_t * 1e-3) / 1e12 / peak, 4),
+           "timed_out": m.timed_out()}
+    m.close()
+    if engine is not None:
+        pkg.set_umma_engine(1)
+    return out
+
+
 def _extrude(plane, n):
     import torch
     out = torch.empty((19, n, n, n), dtype=plane.dtype, device=plane.device)
@@ -775,6 +831,9 @@ def run_other(args):
     elif args.workload == "warmstart":
         if rank == 0:
             r = bench_warmstart(pkg)
+    elif args.workload == "surrogate":
+        if rank == 0:
+            r = bench_surrogate(pkg, steps=min(args.steps, 50), warmup=args.warmup)
     elif rank == 0:
         r = bench_natconv_validation(pkg)
     if rank == 0:
@@ -803,7 +862,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the short measurements of the other configurations")
-    ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "cavity2d", "batch", "natconv", "warmstart"])
+    ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "cavity2d", "batch", "natconv", "warmstart", "surrogate"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

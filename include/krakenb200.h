@@ -129,6 +129,19 @@ int kb_fused_trt_step(void *f_out, const void *f_in, void *rho, void *ux, void *
                       const uint8_t *is_solid, int Nx, int Ny, double nu, double Lambda, int dtype,
                       void *stream);
 
+/* fused_trt_libb_v2_step!(f_out, f_in, rho, ux, uy, is_solid, q_wall,
+ *   uw_link_x, uw_link_y, Nx, Ny, nu; Lambda) -- src/kernels/li_bb_2d_v2.jl:35-41,
+ * 104-115: pull with half-way bounce-back, rest equilibrium on solid nodes,
+ * Bouzidi interpolated bounce-back of every cut link before the TRT
+ * collision (ApplyLiBBPrePhase, src/kernels/dsl/bricks.jl:516-560).
+ * q_wall / uw_link_x / uw_link_y: per-link arrays laid out like f (9
+ * planes, the population's type).  rho/ux/uy: all or none (NULL).
+ * KB_F64 / KB_F32. */
+int kb_fused_trt_libb_step(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                           const uint8_t *is_solid, const void *q_wall, const void *uw_link_x,
+                           const void *uw_link_y, int Nx, int Ny, double nu, double Lambda,
+                           int dtype, void *stream);
+
 /* In-place A-A streaming on one population buffer, the scheme of
  * aa_even_step!/aa_odd_step! (src/kernels/aa_bgk_2d.jl:125,138).  Those
  * reference kernels let neighbouring nodes read and write the same slot in
@@ -211,6 +224,55 @@ int kb_fused_natconv_vt_step(void *f_out, const void *f_in, void *g_out, const v
 /* compute_temperature_2d!(Temp, g) -- src/kernels/thermal_2d.jl:113 */
 int kb_compute_temperature_2d(void *Temp, const void *g, int Nx, int Ny, int dtype, void *stream);
 
+/* Unfused thermal DDF (the reference's Rayleigh-Benard loop,
+ * src/drivers/thermal.jl:101-130).  Fields have the population's type.
+ * Faces: 0 west, 1 east, 2 south, 3 north. */
+
+/* collide_thermal_2d!(g, ux, uy, omega_T) -- src/kernels/thermal_2d.jl:16-81 */
+int kb_collide_thermal_2d(void *g, const void *ux, const void *uy, int Nx, int Ny, double omega_T,
+                          int dtype, void *stream);
+
+/* collide_thermal_masked_2d!(g, ux, uy, omega_T, is_skip)
+ *   -- src/kernels/thermal_2d.jl:83-109; is_skip NULL skips no node */
+int kb_collide_thermal_masked_2d(void *g, const void *ux, const void *uy, const uint8_t *is_skip,
+                                 int Nx, int Ny, double omega_T, int dtype, void *stream);
+
+/* _fixed_temp_{west,east,south,north}_2d!(g, T_wall, ..., T_c, skip_c)
+ *   -- src/kernels/thermal_2d.jl:174-350.  Half-way anti-bounce-back on one
+ * face of the post-stream array; the face's two corner slots (low / high end
+ * of the face) take T_corner_* and are left alone when skip_* is non-zero.
+ * apply_fixed_temp_<face>_2d!(g, T_wall, ...) is T_corner_* = T_wall,
+ * skip_* = 0.  Call once per step. */
+int kb_apply_fixed_temp_face_2d(void *g, int Nx, int Ny, int face, double T_wall,
+                                double T_corner_lo, double T_corner_hi, int skip_lo, int skip_hi,
+                                int dtype, void *stream);
+
+/* apply_fixed_temp_2d!(g, Nx, Ny; west, east, south, north)
+ *   -- src/kernels/thermal_2d.jl:371-417.  faces: bit n set = face n is
+ * Dirichlet at T_faces[n] (T_faces has 4 entries, W E S N).  A corner slot
+ * shared by two Dirichlet faces is flipped once, with the mean temperature.
+ * One launch. */
+int kb_apply_fixed_temp_2d(void *g, int Nx, int Ny, unsigned faces, const double *T_faces,
+                           int dtype, void *stream);
+
+/* collide_boussinesq_2d!(f, Temp, is_solid, omega, beta_g, T_ref)
+ *   -- src/kernels/thermal_2d.jl:421-473, 573-579 */
+int kb_collide_boussinesq_2d(void *f, const void *Temp, const uint8_t *is_solid, int Nx, int Ny,
+                             double omega, double beta_g, double T_ref, int dtype, void *stream);
+
+/* collide_boussinesq_vt_2d!(f, Temp, is_solid, nu_ref, T_ref, A_arr, beta_g)
+ *   -- src/kernels/thermal_2d.jl:482-559 (Arrhenius nu(T)) */
+int kb_collide_boussinesq_vt_2d(void *f, const void *Temp, const uint8_t *is_solid, int Nx, int Ny,
+                                double nu_ref, double T_ref, double A_arr, double beta_g,
+                                int dtype, void *stream);
+
+/* collide_boussinesq_vt_modified_2d!(f, Temp, is_solid, nu_ref, T0_visc,
+ *   alpha_visc, beta_g, T_ref_buoy) -- src/kernels/thermal_2d.jl:593-670 */
+int kb_collide_boussinesq_vt_modified_2d(void *f, const void *Temp, const uint8_t *is_solid,
+                                         int Nx, int Ny, double nu_ref, double T0_visc,
+                                         double alpha_visc, double beta_g, double T_ref_buoy,
+                                         int dtype, void *stream);
+
 /* --------------------------------------------------------------- D3Q19 -- */
 
 /* stream_3d!(f_out, f_in, Nx, Ny, Nz) -- src/kernels/collide_stream_3d.jl:119 */
@@ -239,6 +301,55 @@ int kb_apply_zou_he_pressure_3d(void *f, int Nx, int Ny, int Nz, int face, doubl
 /* compute_macroscopic_3d!(rho, ux, uy, uz, f) -- src/kernels/macroscopic.jl:75 */
 int kb_compute_macroscopic_3d(void *rho, void *ux, void *uy, void *uz, const void *f, int Nx,
                               int Ny, int Nz, int dtype, void *stream);
+
+/* Unfused thermal DDF in 3D (run_natural_convection_3d,
+ * src/drivers/thermal.jl:455-537).  Fields have the population's type. */
+
+/* collide_thermal_3d!(g, ux, uy, uz, omega_T) -- src/kernels/thermal_3d.jl:12-124 */
+int kb_collide_thermal_3d(void *g, const void *ux, const void *uy, const void *uz, int Nx, int Ny,
+                          int Nz, double omega_T, int dtype, void *stream);
+
+/* compute_temperature_3d!(Temp, g) -- src/kernels/thermal_3d.jl:128-155 */
+int kb_compute_temperature_3d(void *Temp, const void *g, int Nx, int Ny, int Nz, int dtype,
+                              void *stream);
+
+/* _fixed_temp_{west,...,top}_3d!(g, T_wall, ..., T_e, skip_e)
+ *   -- src/kernels/thermal_3d.jl:193-480.  Half-way anti-bounce-back on one
+ * face (0 west .. 5 top) of the post-stream array.  Edge slot n (the face's
+ * first in-plane axis low / high, then the second low / high: (y, z) for
+ * x-faces, (x, z) for y-faces, (x, y) for z-faces) takes T_edge[n] (NULL:
+ * T_wall) and is left alone when bit n of skip_edges is set.
+ * apply_fixed_temp_<face>_3d!(g, T_wall, ...) is T_edge = NULL, skip 0. */
+int kb_apply_fixed_temp_face_3d(void *g, int Nx, int Ny, int Nz, int face, double T_wall,
+                                const double *T_edge, unsigned skip_edges, int dtype,
+                                void *stream);
+
+/* apply_fixed_temp_3d!(g, Nx, Ny, Nz; west, east, south, north, bottom, top)
+ *   -- src/kernels/thermal_3d.jl:494-553.  faces: bit n set = face n is
+ * Dirichlet at T_faces[n] (6 entries).  An edge slot shared by two
+ * Dirichlet faces is flipped once, with the mean temperature.  One launch. */
+int kb_apply_fixed_temp_3d(void *g, int Nx, int Ny, int Nz, unsigned faces, const double *T_faces,
+                           int dtype, void *stream);
+
+/* collide_boussinesq_3d!(f, Temp, is_solid, omega, beta_g, T_ref)
+ *   -- src/kernels/thermal_3d.jl:559-733 (gravity along -y) */
+int kb_collide_boussinesq_3d(void *f, const void *Temp, const uint8_t *is_solid, int Nx, int Ny,
+                             int Nz, double omega, double beta_g, double T_ref, int dtype,
+                             void *stream);
+
+/* fused_trt_libb_v2_step_3d!(f_out, f_in, rho, ux, uy, uz, is_solid, q_wall,
+ *   uw_link_x, uw_link_y, uw_link_z, Nx, Ny, Nz, nu; Lambda)
+ *   -- src/kernels/li_bb_3d_v2.jl:13-42 (bricks PullHalfwayBB_3D,
+ * SolidInert_3D, ApplyLiBBPrePhase_3D, Moments_3D, CollideTRTDirect_3D,
+ * WriteMoments_3D).  q_wall / uw_link_* are per-link arrays laid out like
+ * f (19 planes, the population's type): q_wall > 0 marks a link cut by a
+ * wall at that fraction of the link, uw_link_* the wall velocity there.
+ * periodic as kb_fused_trt_step_3d.  KB_F64 / KB_F32. */
+int kb_fused_trt_libb_step_3d(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                              void *uz, const uint8_t *is_solid, const void *q_wall,
+                              const void *uw_link_x, const void *uw_link_y, const void *uw_link_z,
+                              int Nx, int Ny, int Nz, double nu, double Lambda, int periodic,
+                              int dtype, void *stream);
 
 /* Fused D3Q19 TRT step: the reference's 3D TRT kernel
  * fused_trt_libb_v2_step_3d!(f_out, f_in, rho, ux, uy, uz, is_solid, ...,

@@ -44,6 +44,10 @@ SIGNATURES: dict[str, list] = {
     "kb_fused_bgk_step": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _i, _vp],
     "kb_trt_rates": [_d, _d, _dp, _dp],
     "kb_fused_trt_step": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _d, _i, _vp],
+    "kb_fused_trt_libb_step": [_vp, _cvp, _vp, _vp, _vp, _u8p, _cvp, _cvp, _cvp, _i, _i, _d, _d,
+                               _i, _vp],
+    "kb_fused_trt_libb_step_3d": [_vp, _cvp, _vp, _vp, _vp, _vp, _u8p, _cvp, _cvp, _cvp, _cvp, _i,
+                                  _i, _i, _d, _d, _i, _i, _vp],
     "kb_aa_stream_step_2d": [_vp, _vp, _vp, _vp, _u8p, _i, _i, _d, _i, _vp],
     "kb_aa_local_step_2d": [_vp, _vp, _vp, _vp, _u8p, _i, _i, _d, _i, _vp],
     "kb_collide_mrt_2d": [_vp, _u8p, _i, _i, _d, _d, _d, _d, _i, _vp],
@@ -59,6 +63,19 @@ SIGNATURES: dict[str, list] = {
     "kb_fused_natconv_vt_step": [_vp, _cvp, _vp, _cvp, _vp, _i, _i, _d, _d, _d, _d, _d, _d, _d,
                                  _d, _i, _vp],
     "kb_compute_temperature_2d": [_vp, _cvp, _i, _i, _i, _vp],
+    "kb_collide_thermal_2d": [_vp, _cvp, _cvp, _i, _i, _d, _i, _vp],
+    "kb_collide_thermal_masked_2d": [_vp, _cvp, _cvp, _u8p, _i, _i, _d, _i, _vp],
+    "kb_apply_fixed_temp_face_2d": [_vp, _i, _i, _i, _d, _d, _d, _i, _i, _i, _vp],
+    "kb_apply_fixed_temp_2d": [_vp, _i, _i, C.c_uint, _dp, _i, _vp],
+    "kb_collide_boussinesq_2d": [_vp, _cvp, _u8p, _i, _i, _d, _d, _d, _i, _vp],
+    "kb_collide_boussinesq_vt_2d": [_vp, _cvp, _u8p, _i, _i, _d, _d, _d, _d, _i, _vp],
+    "kb_collide_boussinesq_vt_modified_2d": [_vp, _cvp, _u8p, _i, _i, _d, _d, _d, _d, _d, _i,
+                                             _vp],
+    "kb_collide_thermal_3d": [_vp, _cvp, _cvp, _cvp, _i, _i, _i, _d, _i, _vp],
+    "kb_compute_temperature_3d": [_vp, _cvp, _i, _i, _i, _i, _vp],
+    "kb_apply_fixed_temp_face_3d": [_vp, _i, _i, _i, _i, _d, _dp, C.c_uint, _i, _vp],
+    "kb_apply_fixed_temp_3d": [_vp, _i, _i, _i, C.c_uint, _dp, _i, _vp],
+    "kb_collide_boussinesq_3d": [_vp, _cvp, _u8p, _i, _i, _i, _d, _d, _d, _i, _vp],
     "kb_stream_3d": [_vp, _cvp, _i, _i, _i, _i, _vp],
     "kb_collide_3d": [_vp, _u8p, _i, _i, _i, _d, _i, _vp],
     "kb_apply_zou_he_velocity_3d": [_vp, _i, _i, _i, _i, _d, _d, _d, _i, _vp],

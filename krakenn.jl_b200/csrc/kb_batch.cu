@@ -26,6 +26,11 @@ namespace kb {
 namespace batch {
 
 constexpr int BT = 256;  // threads per block
+// Blocks per SM the register allocation is sized for (__launch_bounds__):
+// more resident warps keep more population loads in flight.
+#ifndef KB_BATCH_MIN_BLOCKS
+#define KB_BATCH_MIN_BLOCKS 4
+#endif
 
 struct CaseDesc {
     int N;
@@ -186,8 +191,122 @@ __device__ __forceinline__ void node_update(const R *__restrict__ src, R *__rest
     }
 }
 
+// Two x-adjacent nodes (i even, i+1) of one case per thread: N is even, so a
+// pair never straddles a row, and each population of the pair is one aligned
+// 2-element access except the x-shifted pulls.  The MRT collision runs on the
+// pair in packed FP32x2 arithmetic.
+template <typename R> struct Pair2;
+template <> struct Pair2<float> {
+    static __device__ __forceinline__ float2 ld(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+    static __device__ __forceinline__ void st(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
+};
+template <> struct Pair2<__half> {
+    static __device__ __forceinline__ float2 ld(const __half *p) {
+        return __half22float2(*reinterpret_cast<const __half2 *>(p));
+    }
+    static __device__ __forceinline__ void st(__half *p, float2 v) {
+        *reinterpret_cast<__half2 *>(p) = __floats2half2_rn(v.x, v.y);
+    }
+};
+template <> struct Pair2<__nv_bfloat16> {
+    static __device__ __forceinline__ float2 ld(const __nv_bfloat16 *p) {
+        return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(p));
+    }
+    static __device__ __forceinline__ void st(__nv_bfloat16 *p, float2 v) {
+        *reinterpret_cast<__nv_bfloat162 *>(p) = __floats2bfloat162_rn(v.x, v.y);
+    }
+};
+
 template <typename R, bool SR>
-__global__ void __launch_bounds__(BT) batch_k(BatchState D, int n_cases, int n_tiles_all, int tile_nodes,
+__device__ __forceinline__ void node_update_pair(const R *__restrict__ src, R *__restrict__ dst, int N,
+                                                 int i, int j, float s_nu, float u_lid, float2 &ux,
+                                                 float2 &uy, uint32_t key) {
+    const long long P = (long long)N * N;
+    const long long c = (long long)j * N + i;  // node A = (i, j), node B = (i + 1, j)
+    const bool w = i > 0, e = i + 1 < N - 1, s = j > 0, n = j < N - 1;
+    float2 d[9];
+    d[0] = Pair2<R>::ld(src + c);
+    d[2] = s ? Pair2<R>::ld(src + c - N + 2 * P) : Pair2<R>::ld(src + c + 4 * P);
+    d[4] = n ? Pair2<R>::ld(src + c + N + 4 * P) : Pair2<R>::ld(src + c + 2 * P);
+    d[1] = make_float2(w ? ldv(src, c - 1 + P) : ldv(src, c + 3 * P), ldv(src, c + P));
+    d[3] = make_float2(ldv(src, c + 1 + 3 * P), e ? ldv(src, c + 2 + 3 * P) : ldv(src, c + 1 + P));
+    d[5] = make_float2((w && s) ? ldv(src, c - 1 - N + 5 * P) : ldv(src, c + 7 * P),
+                       s ? ldv(src, c - N + 5 * P) : ldv(src, c + 1 + 7 * P));
+    d[6] = make_float2(s ? ldv(src, c + 1 - N + 6 * P) : ldv(src, c + 8 * P),
+                       (e && s) ? ldv(src, c + 2 - N + 6 * P) : ldv(src, c + 1 + 8 * P));
+    d[7] = make_float2(n ? ldv(src, c + 1 + N + 7 * P) : ldv(src, c + 5 * P),
+                       (e && n) ? ldv(src, c + 2 + N + 7 * P) : ldv(src, c + 1 + 5 * P));
+    d[8] = make_float2((w && n) ? ldv(src, c - 1 + N + 8 * P) : ldv(src, c + 6 * P),
+                       n ? ldv(src, c + N + 8 * P) : ldv(src, c + 1 + 6 * P));
+    const float2 z = make_float2(0.f, 0.f);
+    if (!n) {
+        // Zou-He velocity lid on deviations, as node_update
+        const float2 rw = vadd(vsplat(1.0f, z),
+                               vadd(vadd(d[0], vadd(d[1], d[3])),
+                                    vmul(vsplat(2.0f, z), vadd(d[2], vadd(d[5], d[6])))));
+        const float2 h = vmul(vsplat(0.5f, z), vsub(d[1], d[3]));
+        const float2 m = vmul(vsplat(0.5f * u_lid, z), rw);
+        d[4] = d[2];
+        d[8] = vadd(vsub(d[6], h), m);
+        d[7] = vsub(vadd(d[5], h), m);
+    }
+    const float2 drho = vadd(vadd(vadd(d[0], d[1]), vadd(d[2], d[3])),
+                             vadd(vadd(d[4], d[5]), vadd(vadd(d[6], d[7]), d[8])));
+    const float2 dg = vadd(vadd(d[5], d[6]), vadd(d[7], d[8]));
+    const float2 da = vadd(vadd(d[1], d[2]), vadd(d[3], d[4]));
+    const float2 e_d = vadd(vsub(vmul(vsplat(-4.0f, z), d[0]), da), vmul(vsplat(2.0f, z), dg));
+    const float2 eps_d = vadd(vsub(vmul(vsplat(4.0f, z), d[0]), vmul(vsplat(2.0f, z), da)), dg);
+    const float2 t13 = vsub(d[1], d[3]), t24 = vsub(d[2], d[4]);
+    const float2 jx = vadd(t13, vsub(vsub(vadd(d[5], d[8]), d[6]), d[7]));
+    const float2 qx = vadd(vmul(vsplat(-2.0f, z), t13), vsub(vsub(vadd(d[5], d[8]), d[6]), d[7]));
+    const float2 jy = vadd(t24, vsub(vsub(vadd(d[5], d[6]), d[7]), d[8]));
+    const float2 qy = vadd(vmul(vsplat(-2.0f, z), t24), vsub(vsub(vadd(d[5], d[6]), d[7]), d[8]));
+    const float2 pxx = vsub(vadd(d[1], d[3]), vadd(d[2], d[4]));
+    const float2 pxy = vsub(vadd(d[5], d[7]), vadd(d[6], d[8]));
+    const float2 rho = vadd(vsplat(1.0f, z), drho);
+    const float2 inv = vrcp(rho);
+    ux = vmul(jx, inv);
+    uy = vmul(jy, inv);
+    const float2 r3u = vmul(vmul(vsplat(3.0f, z), rho), vfma(ux, ux, vmul(uy, uy)));
+    const float s_e = 1.4f, s_eps = 1.4f, s_q = 1.2f;
+    const float2 es = vsub(e_d, vmul(vsplat(s_e, z), vsub(vadd(e_d, vmul(vsplat(2.0f, z), drho)), r3u)));
+    const float2 ep = vsub(eps_d, vmul(vsplat(s_eps, z), vadd(vsub(eps_d, drho), r3u)));
+    const float2 qxs = vsub(qx, vmul(vsplat(s_q, z), vadd(qx, jx)));
+    const float2 qys = vsub(qy, vmul(vsplat(s_q, z), vadd(qy, jy)));
+    const float2 ps = vsub(pxx, vmul(vsplat(s_nu, z), vsub(pxx, vmul(rho, vsub(vmul(ux, ux), vmul(uy, uy))))));
+    const float2 pxys = vsub(pxy, vmul(vsplat(s_nu, z), vsub(pxy, vmul(rho, vmul(ux, uy)))));
+    const float c9 = 1.0f / 9.0f, c36 = 1.0f / 36.0f, c18 = 1.0f / 18.0f, c6 = 1.0f / 6.0f,
+                c4 = 0.25f, c12 = 1.0f / 12.0f;
+    const float2 base_a = vsub(vsub(vmul(vsplat(c9, z), drho), vmul(vsplat(c36, z), es)), vmul(vsplat(c18, z), ep));
+    const float2 base_d = vadd(vadd(vmul(vsplat(c9, z), drho), vmul(vsplat(c18, z), es)), vmul(vsplat(c36, z), ep));
+    const float2 ax = vsub(vmul(vsplat(c6, z), jx), vmul(vsplat(c6, z), qxs));   // c6 jx - c6 qx*
+    const float2 ay = vsub(vmul(vsplat(c6, z), jy), vmul(vsplat(c6, z), qys));
+    const float2 bx = vadd(vmul(vsplat(c6, z), jx), vmul(vsplat(c12, z), qxs));  // c6 jx + c12 qx*
+    const float2 by = vadd(vmul(vsplat(c6, z), jy), vmul(vsplat(c12, z), qys));
+    const float2 p4 = vmul(vsplat(c4, z), ps), x4 = vmul(vsplat(c4, z), pxys);
+    float2 o[9];
+    o[0] = vmul(vsplat(c9, z), vadd(vsub(drho, es), ep));
+    o[1] = vadd(vadd(base_a, ax), p4);
+    o[2] = vsub(vadd(base_a, ay), p4);
+    o[3] = vadd(vsub(base_a, ax), p4);
+    o[4] = vsub(vsub(base_a, ay), p4);
+    o[5] = vadd(vadd(vadd(base_d, bx), by), x4);
+    o[6] = vsub(vadd(vsub(base_d, bx), by), x4);
+    o[7] = vadd(vsub(vsub(base_d, bx), by), x4);
+    o[8] = vsub(vsub(vadd(base_d, bx), by), x4);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        if (SR) {
+            *reinterpret_cast<uint32_t *>(dst + c + q * P) =
+                SRPack<R>::pack(o[q].x, o[q].y, hash32(key + (uint32_t)q * 0x9E3779B9u));
+        } else {
+            Pair2<R>::st(dst + c + q * P, o[q]);
+        }
+    }
+}
+
+template <typename R, bool SR>
+__global__ void __launch_bounds__(BT, KB_BATCH_MIN_BLOCKS) batch_k(BatchState D, int n_cases, int n_tiles_all, int tile_nodes,
                                                int max_steps, int check_every, float tol,
                                                long long spin_limit, uint32_t seed) {
     __shared__ double sh[BT / 32];
@@ -205,21 +324,51 @@ __global__ void __launch_bounds__(BT) batch_k(BatchState D, int n_cases, int n_t
             const int NN = C.N * C.N;
             const int end = min(T.start + tile_nodes, NN);
             double du2 = 0.0, u2 = 0.0;
-            for (int m = T.start + threadIdx.x; m < end; m += BT) {
+            if (C.N & 1) {
+                // odd N: rows start at odd offsets, so one node per thread
+                for (int m = T.start + threadIdx.x; m < end; m += BT) {
+                    const int j = m / C.N, i = m - j * C.N;
+                    float ux, uy;
+                    const uint32_t key =
+                        SR ? hash32((uint32_t)(C.f_off + m) ^ hash32((uint32_t)s * 0x632BE5ABu + seed)) : 0u;
+                    node_update<R, SR>(src + C.f_off, dst + C.f_off, C.N, i, j, C.s_nu, C.u_lid, ux, uy,
+                                       key);
+                    const long long mo = C.m_off + m;
+                    if (save) { D.uxp[mo] = ux; D.uyp[mo] = uy; }
+                    if (check) {
+                        D.ux[mo] = ux;
+                        D.uy[mo] = uy;
+                        const double a = (double)ux - (double)D.uxp[mo];
+                        const double b = (double)uy - (double)D.uyp[mo];
+                        du2 += a * a + b * b;
+                        u2 += (double)ux * ux + (double)uy * uy;
+                    }
+                }
+            } else
+            // node pairs (m, m + 1): tiles start at multiples of 32, N is even
+            // and case offsets are multiples of 64, so every pair is aligned
+            for (int m = T.start + 2 * threadIdx.x; m < end; m += 2 * BT) {
                 const int j = m / C.N, i = m - j * C.N;
-                float ux, uy;
+                float2 ux, uy;
                 const uint32_t key =
                     SR ? hash32((uint32_t)(C.f_off + m) ^ hash32((uint32_t)s * 0x632BE5ABu + seed)) : 0u;
-                node_update<R, SR>(src + C.f_off, dst + C.f_off, C.N, i, j, C.s_nu, C.u_lid, ux, uy,
-                                   key);
-                if (save) { D.uxp[C.m_off + m] = ux; D.uyp[C.m_off + m] = uy; }
+                node_update_pair<R, SR>(src + C.f_off, dst + C.f_off, C.N, i, j, C.s_nu, C.u_lid,
+                                        ux, uy, key);
+                const long long mo = C.m_off + m;
+                if (save) {
+                    *reinterpret_cast<float2 *>(D.uxp + mo) = ux;
+                    *reinterpret_cast<float2 *>(D.uyp + mo) = uy;
+                }
                 if (check) {
-                    D.ux[C.m_off + m] = ux;
-                    D.uy[C.m_off + m] = uy;
-                    const double a = (double)ux - (double)D.uxp[C.m_off + m];
-                    const double b = (double)uy - (double)D.uyp[C.m_off + m];
-                    du2 += a * a + b * b;
-                    u2 += (double)ux * ux + (double)uy * uy;
+                    *reinterpret_cast<float2 *>(D.ux + mo) = ux;
+                    *reinterpret_cast<float2 *>(D.uy + mo) = uy;
+                    const float2 px = *reinterpret_cast<const float2 *>(D.uxp + mo);
+                    const float2 py = *reinterpret_cast<const float2 *>(D.uyp + mo);
+                    const double a0 = (double)ux.x - px.x, b0 = (double)uy.x - py.x;
+                    const double a1 = (double)ux.y - px.y, b1 = (double)uy.y - py.y;
+                    du2 += a0 * a0 + b0 * b0 + a1 * a1 + b1 * b1;
+                    u2 += (double)ux.x * ux.x + (double)uy.x * uy.x + (double)ux.y * ux.y +
+                          (double)uy.y * uy.y;
                 }
             }
             if (check) {

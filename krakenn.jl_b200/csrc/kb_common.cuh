@@ -63,6 +63,23 @@ template <> struct Dev<__nv_bfloat16> {
     static __device__ __forceinline__ __nv_bfloat16 st(float d) { return __float2bfloat16_rn(d); }
 };
 
+// Scalar / packed-pair (float2, sm_100 FADD2/FMUL2/FFMA2) arithmetic for the
+// collisions written once for one node (float) or two nodes (float2).
+__device__ __forceinline__ float vadd(float a, float b) { return a + b; }
+__device__ __forceinline__ float vsub(float a, float b) { return a - b; }
+__device__ __forceinline__ float vmul(float a, float b) { return a * b; }
+__device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ float vneg(float a) { return -a; }
+__device__ __forceinline__ float vsplat(float a, float) { return a; }
+__device__ __forceinline__ float vrcp(float a) { return __frcp_rn(a); }
+__device__ __forceinline__ float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 vsub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 vmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 vneg(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 vsplat(float a, float2) { return make_float2(a, a); }
+__device__ __forceinline__ float2 vrcp(float2 a) { return make_float2(__frcp_rn(a.x), __frcp_rn(a.y)); }
+
 // ------------------------------------------------------ stochastic rounding --
 // 32-bit integer hash (lowbias32, C. Wellons) for the random bits of the
 // stochastic-rounding stores.

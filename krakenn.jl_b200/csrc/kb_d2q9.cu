@@ -343,6 +343,83 @@ __global__ void __launch_bounds__(BX) fused_trt_k(T *__restrict__ fo, const T *_
     rho[c] = r; ux[c] = a_; uy[c] = b_;
 }
 
+// _libb_branch (src/kernels/li_bb_2d.jl:70-83): Bouzidi interpolated
+// bounce-back of one cut link at wall distance q_w in (0, 1].
+template <typename T>
+__device__ __forceinline__ T libb_branch(T q_w, T f_here, T f_back, T f_bar_here, T d) {
+    if (q_w <= T(0.5)) return T(2) * q_w * f_here + (T(1) - T(2) * q_w) * f_back + d;
+    const T inv = T(1) / (T(2) * q_w);
+    return inv * f_here + (T(1) - inv) * f_bar_here + d * inv;
+}
+
+// ApplyLiBBPrePhase (src/kernels/dsl/bricks.jl:516-560): for each cut link q
+// (q_wall[q] > 0) the pulled population of the opposite direction, which
+// came from a solid node, is replaced by the Bouzidi estimate from the
+// node's own previous post-collision populations.  Pairs in the reference
+// order; the second link of a pair sees the first one's substitution.
+// qw/ux/uy point at the node in planes of stride P.
+template <typename T>
+__device__ __forceinline__ void libb_prephase_2d(const T *__restrict__ f0, const T *__restrict__ qw,
+                                                 const T *__restrict__ uwx,
+                                                 const T *__restrict__ uwy, size_t P, T *p) {
+    const T c23 = T(2.0 / 3.0), c16 = T(1.0 / 6.0);
+    T q;
+    if ((q = qw[1 * P]) > T(0)) p[3] = libb_branch(q, f0[1 * P], p[1], f0[3 * P], -c23 * uwx[1 * P]);
+    if ((q = qw[3 * P]) > T(0)) p[1] = libb_branch(q, f0[3 * P], p[3], f0[1 * P], c23 * uwx[3 * P]);
+    if ((q = qw[2 * P]) > T(0)) p[4] = libb_branch(q, f0[2 * P], p[2], f0[4 * P], -c23 * uwy[2 * P]);
+    if ((q = qw[4 * P]) > T(0)) p[2] = libb_branch(q, f0[4 * P], p[4], f0[2 * P], c23 * uwy[4 * P]);
+    if ((q = qw[5 * P]) > T(0))
+        p[7] = libb_branch(q, f0[5 * P], p[5], f0[7 * P], -c16 * (uwx[5 * P] + uwy[5 * P]));
+    if ((q = qw[7 * P]) > T(0))
+        p[5] = libb_branch(q, f0[7 * P], p[7], f0[5 * P], c16 * (uwx[7 * P] + uwy[7 * P]));
+    if ((q = qw[6 * P]) > T(0))
+        p[8] = libb_branch(q, f0[6 * P], p[6], f0[8 * P], -c16 * (-uwx[6 * P] + uwy[6 * P]));
+    if ((q = qw[8 * P]) > T(0))
+        p[6] = libb_branch(q, f0[8 * P], p[8], f0[6 * P], c16 * (-uwx[8 * P] + uwy[8 * P]));
+}
+
+// fused_trt_libb_v2_step! (src/kernels/li_bb_2d_v2.jl:35-41, 104-115):
+// PullHalfwayBB -> SolidInert | ApplyLiBBPrePhase -> Moments ->
+// CollideTRTDirect -> WriteMoments.  Moments are written when rho != NULL.
+template <typename T>
+__global__ void __launch_bounds__(BX) fused_trt_libb_k(T *__restrict__ fo, const T *__restrict__ fi,
+                                                        T *__restrict__ rho, T *__restrict__ ux,
+                                                        T *__restrict__ uy,
+                                                        const uint8_t *__restrict__ solid,
+                                                        const T *__restrict__ qw,
+                                                        const T *__restrict__ uwx,
+                                                        const T *__restrict__ uwy, Grid2<T> g, T sp,
+                                                        T sm) {
+    NODE2
+    T feq[9];
+    if (solid && solid[c]) {
+        // SolidInert (bricks.jl:133-150): rest equilibrium w_q
+        feq_all(T(1), T(0), T(0), T(0), feq);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) fo[c + q * P] = feq[q];
+        if (rho) { rho[c] = T(1); ux[c] = T(0); uy[c] = T(0); }
+        return;
+    }
+    T p[9];
+    pull_bb(fi, g, i, j, p);
+    libb_prephase_2d(fi + c, qw + c, uwx + c, uwy + c, P, p);
+    T r, a_, b_;
+    moments(p, r, a_, b_);
+    const T usq = a_ * a_ + b_ * b_;
+    feq_all(r, a_, b_, usq, feq);
+    const T a = (sp + sm) * T(0.5), b = (sp - sm) * T(0.5);
+    fo[c + 0 * P] = p[0] - sp * (p[0] - feq[0]);
+    fo[c + 1 * P] = p[1] - a * (p[1] - feq[1]) - b * (p[3] - feq[3]);
+    fo[c + 3 * P] = p[3] - a * (p[3] - feq[3]) - b * (p[1] - feq[1]);
+    fo[c + 2 * P] = p[2] - a * (p[2] - feq[2]) - b * (p[4] - feq[4]);
+    fo[c + 4 * P] = p[4] - a * (p[4] - feq[4]) - b * (p[2] - feq[2]);
+    fo[c + 5 * P] = p[5] - a * (p[5] - feq[5]) - b * (p[7] - feq[7]);
+    fo[c + 7 * P] = p[7] - a * (p[7] - feq[7]) - b * (p[5] - feq[5]);
+    fo[c + 6 * P] = p[6] - a * (p[6] - feq[6]) - b * (p[8] - feq[8]);
+    fo[c + 8 * P] = p[8] - a * (p[8] - feq[8]) - b * (p[6] - feq[6]);
+    if (rho) { rho[c] = r; ux[c] = a_; uy[c] = b_; }
+}
+
 // In-place A-A streaming (one population buffer), the scheme that
 // aa_even_step!/aa_odd_step! (src/kernels/aa_bgk_2d.jl:14-143) aim at.  The
 // reference's two kernels read and write slots that neighbouring nodes write
@@ -726,6 +803,132 @@ __global__ void __launch_bounds__(BX) temperature_k(T *__restrict__ Temp, const 
               gg[c + 6 * P] + gg[c + 7 * P] + gg[c + 8 * P];
 }
 
+// ------------------------------------------------- unfused thermal DDF (2D) --
+// collide_thermal_2d_kernel!: src/kernels/thermal_2d.jl:16-62
+template <typename T>
+__global__ void __launch_bounds__(BX) collide_thermal_k(T *__restrict__ gg, const T *__restrict__ ux,
+                                                         const T *__restrict__ uy, Grid2<T> g, T wT) {
+    NODE2
+    T p[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p[q] = gg[c + q * P];
+    collide_thermal(p, ux[c], uy[c], wT);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) gg[c + q * P] = p[q];
+}
+
+// collide_thermal_masked_2d_kernel!: src/kernels/thermal_2d.jl:83-102.  The
+// equilibrium is written per population from (w_q, c_q) as the reference's
+// loop writes it; skipped nodes are left untouched.
+template <typename T>
+__global__ void __launch_bounds__(BX) collide_thermal_masked_k(T *__restrict__ gg,
+                                                                const T *__restrict__ ux,
+                                                                const T *__restrict__ uy,
+                                                                const uint8_t *__restrict__ skip,
+                                                                Grid2<T> g, T wT) {
+    NODE2
+    if (skip && skip[c]) return;
+    const T a = ux[c], b = uy[c];
+    T p[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p[q] = gg[c + q * P];
+    const T Tm = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8];
+    const T t3 = T(3);
+    const int cx[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
+    const int cy[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const T w = q == 0 ? T(4) / T(9) : (q <= 4 ? T(1) / T(9) : T(1) / T(36));
+        const T geq = w * Tm * (T(1) + t3 * (T(cx[q]) * a + T(cy[q]) * b));
+        gg[c + q * P] = p[q] - wT * (p[q] - geq);
+    }
+}
+
+// Half-way anti-bounce-back on one face: _fixed_temp_{west,east,south,north}_2d!
+// (src/kernels/thermal_2d.jl:151-350).  Slots are 0-based (reference q - 1).
+// The face's main slot always flips; each of its two corner slots uses the
+// corner temperature and is left alone when its skip flag is set.
+template <typename T>
+struct FixedTempFace2 {
+    int face;     // 0 west, 1 east, 2 south, 3 north
+    T T_wall;
+    T T_c[2];     // corner temperature at the low / high end of the face
+    int skip[2];  // corner slot owned by the adjacent face
+};
+
+template <typename T>
+struct FixedTempSet2 {
+    int n;
+    FixedTempFace2<T> f[4];
+};
+
+// _abb_slot (thermal_2d.jl:163-166).  A skipped corner slot is not written
+// at all: in the one-launch multi-face form the face that owns it may be
+// writing it at the same time.
+template <typename T>
+__device__ __forceinline__ void abb_slot(T *gq, T w2, T T_face, bool on_corner, T T_corner, bool skip) {
+    if (on_corner && skip) return;
+    const T T_link = on_corner ? T_corner : T_face;
+    *gq = -*gq + w2 * T_link;
+}
+
+template <typename T>
+__global__ void fixed_temp_k(T *__restrict__ gg, Grid2<T> g, FixedTempSet2<T> S) {
+    const FixedTempFace2<T> F = S.f[blockIdx.y];
+    const int n = threadIdx.x + blockIdx.x * blockDim.x;
+    const bool xface = F.face < 2;
+    const int len = xface ? g.Ny : g.Nx;
+    if (n >= len) return;
+    const int i = xface ? (F.face == 0 ? 0 : g.Nx - 1) : n;
+    const int j = xface ? n : (F.face == 2 ? 0 : g.Ny - 1);
+    const size_t c = g.at(i, j), P = g.plane;
+    // main slot, low-corner slot, high-corner slot per face
+    const int qm[4] = {1, 3, 2, 4}, ql[4] = {5, 6, 5, 8}, qh[4] = {8, 7, 6, 7};
+    const T wa = T(2) * T(1.0 / 9.0), we = T(2) * T(1.0 / 36.0);
+    const bool lo = n == 0, hi = n == len - 1;
+    T *m = gg + c + qm[F.face] * P, *l = gg + c + ql[F.face] * P, *h = gg + c + qh[F.face] * P;
+    *m = -*m + wa * F.T_wall;
+    abb_slot(l, we, F.T_wall, lo, F.T_c[0], F.skip[0] != 0);
+    abb_slot(h, we, F.T_wall, hi, F.T_c[1], F.skip[1] != 0);
+}
+
+// collide_boussinesq_2d_kernel! (src/kernels/thermal_2d.jl:421-473) and its
+// nu(T) forms: MODE 1 Arrhenius (:482-539), MODE 2 modified Arrhenius
+// (:593-650).  a, b: (omega) for MODE 0, (nu_ref, T_ref, A_arr) for MODE 1,
+// (nu_ref, T0_visc, alpha_visc) for MODE 2.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(BX) boussinesq_k(T *__restrict__ f, const T *__restrict__ Temp,
+                                                    const uint8_t *__restrict__ solid, Grid2<T> g,
+                                                    T omega, T nu_ref, T Ta, T Aa, T beta_g,
+                                                    T T_ref) {
+    NODE2
+    T p[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p[q] = f[c + q * P];
+    if (solid && solid[c]) {
+        swap_pairs(p);
+    } else {
+        const T Tl = Temp[c];
+        T w = omega;
+        if (MODE == 1) {
+            const T nul = nu_ref * kb_exp(Aa * (T(1) / Tl - T(1) / Ta));
+            w = T(1) / (T(3) * nul + T(0.5));
+        } else if (MODE == 2) {
+            const T nul = nu_ref * kb_exp(Aa * (Tl - Ta));
+            w = T(1) / (T(3) * nul + T(0.5));
+        }
+        const T fy = beta_g * (Tl - T_ref);
+        const T fx = T(0);
+        const T rho = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8];
+        const T inv = T(1) / rho;
+        const T a = ((p[1] - p[3] + p[5] - p[6] - p[7] + p[8]) + fx / T(2)) * inv;
+        const T b = ((p[2] - p[4] + p[5] + p[6] - p[7] - p[8]) + fy / T(2)) * inv;
+        collide_boussinesq(p, rho, a, b, fy, w);
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[c + q * P] = p[q];
+}
+
 }  // namespace d2
 }  // namespace kb
 
@@ -918,6 +1121,26 @@ int kb_fused_trt_step(void *f_out, const void *f_in, void *rho, void *ux, void *
             (T)sp, (T)sm)));
 }
 
+int kb_fused_trt_libb_step(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                           const uint8_t *is_solid, const void *q_wall, const void *uw_link_x,
+                           const void *uw_link_y, int Nx, int Ny, double nu, double Lambda,
+                           int dtype, void *stream) {
+    const char *what = "kb_fused_trt_libb_step";
+    KB_REQUIRE(f_out && f_in, "%s: null population pointer", what);
+    KB_REQUIRE(q_wall && uw_link_x && uw_link_y, "%s: null q_wall / uw_link pointer", what);
+    KB_REQUIRE(f_out != f_in, "%s: f_out and f_in must differ", what);
+    const int nm = (rho != nullptr) + (ux != nullptr) + (uy != nullptr);
+    KB_REQUIRE(nm == 0 || nm == 3, "%s: pass all three moment arrays or none", what);
+    if (int e = check_dims(what, Nx, Ny)) return e;
+    double sp, sm;
+    if (int e = kb_trt_rates(nu, Lambda, &sp, &sm)) return e;
+    KB_DISPATCH_PLAIN(what,
+        dtype, (fused_trt_libb_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+                   (T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, is_solid,
+                   (const T *)q_wall, (const T *)uw_link_x, (const T *)uw_link_y,
+                   grid2<T>(Nx, Ny), (T)sp, (T)sm)));
+}
+
 static int aa_step(bool stream_step, void *f, void *rho, void *ux, void *uy,
                    const uint8_t *is_solid, int Nx, int Ny, double omega, int dtype,
                    void *stream) {
@@ -1073,6 +1296,142 @@ int kb_compute_temperature_2d(void *Temp, const void *g, int Nx, int Ny, int dty
     KB_DISPATCH_PLAIN("kb_compute_temperature_2d", dtype,
         (temperature_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
             (T *)Temp, (const T *)g, grid2<T>(Nx, Ny))));
+}
+
+int kb_collide_thermal_2d(void *g, const void *ux, const void *uy, int Nx, int Ny, double omega_T,
+                          int dtype, void *stream) {
+    KB_REQUIRE(g && ux && uy, "kb_collide_thermal_2d: null pointer");
+    if (int e = check_dims("kb_collide_thermal_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_collide_thermal_2d", dtype,
+        (collide_thermal_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)g, (const T *)ux, (const T *)uy, grid2<T>(Nx, Ny), (T)omega_T)));
+}
+
+int kb_collide_thermal_masked_2d(void *g, const void *ux, const void *uy, const uint8_t *is_skip,
+                                 int Nx, int Ny, double omega_T, int dtype, void *stream) {
+    KB_REQUIRE(g && ux && uy, "kb_collide_thermal_masked_2d: null pointer");
+    if (int e = check_dims("kb_collide_thermal_masked_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_collide_thermal_masked_2d", dtype,
+        (collide_thermal_masked_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)g, (const T *)ux, (const T *)uy, is_skip, grid2<T>(Nx, Ny), (T)omega_T)));
+}
+
+}  // extern "C"
+
+namespace {
+
+template <typename T>
+T corner_temp(double Ta, bool has_b, double Tb) {
+    // _corner_temp (thermal_2d.jl:356-357): the mean of the two wall
+    // temperatures, in the population type
+    return has_b ? (T(Ta) + T(Tb)) / T(2) : T(Ta);
+}
+
+template <typename T>
+int launch_fixed_temp_2d(T *g, int Nx, int Ny, const FixedTempSet2<T> &S, cudaStream_t s,
+                         const char *what) {
+    if (S.n == 0) return KB_OK;
+    const int len = Nx > Ny ? Nx : Ny;
+    fixed_temp_k<T><<<dim3(line_grid(len), S.n), BX, 0, s>>>(g, grid2<T>(Nx, Ny), S);
+    return kb::check_launch(what);
+}
+
+// _apply_fixed_temp_faces_2d! (thermal_2d.jl:371-392) for every face in
+// `faces`: the x-faces own the corner slots they share with a Dirichlet
+// y-face (mean temperature), the y-faces skip them.  No slot is written by
+// two faces, so all faces run in one launch.
+template <typename T>
+int fixed_temp_all_2d(T *g, int Nx, int Ny, unsigned faces, const double *Tf, cudaStream_t s) {
+    const bool hw = faces & 1u, he = faces & 2u, hs = faces & 4u, hn = faces & 8u;
+    FixedTempSet2<T> S{};
+    S.n = 0;
+    for (int face = 0; face < 4; ++face) {
+        if (!(faces & (1u << face))) continue;
+        FixedTempFace2<T> F{};
+        F.face = face;
+        F.T_wall = T(Tf[face]);
+        if (face < 2) {
+            F.T_c[0] = corner_temp<T>(Tf[face], hs, Tf[2]);
+            F.T_c[1] = corner_temp<T>(Tf[face], hn, Tf[3]);
+            F.skip[0] = F.skip[1] = 0;
+        } else {
+            F.T_c[0] = F.T_c[1] = T(Tf[face]);
+            F.skip[0] = hw;
+            F.skip[1] = he;
+        }
+        S.f[S.n++] = F;
+    }
+    return launch_fixed_temp_2d(g, Nx, Ny, S, s, "kb_apply_fixed_temp_2d");
+}
+
+}  // namespace
+
+extern "C" {
+
+int kb_apply_fixed_temp_face_2d(void *g, int Nx, int Ny, int face, double T_wall,
+                                double T_corner_lo, double T_corner_hi, int skip_lo, int skip_hi,
+                                int dtype, void *stream) {
+    KB_REQUIRE(g, "kb_apply_fixed_temp_face_2d: null population pointer");
+    KB_REQUIRE(face >= 0 && face < 4, "kb_apply_fixed_temp_face_2d: face %d not in 0..3", face);
+    if (int e = check_dims("kb_apply_fixed_temp_face_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_apply_fixed_temp_face_2d", dtype, {
+        FixedTempSet2<T> S{};
+        S.n = 1;
+        S.f[0].face = face;
+        S.f[0].T_wall = (T)T_wall;
+        S.f[0].T_c[0] = (T)T_corner_lo;
+        S.f[0].T_c[1] = (T)T_corner_hi;
+        S.f[0].skip[0] = skip_lo != 0;
+        S.f[0].skip[1] = skip_hi != 0;
+        if (int r = launch_fixed_temp_2d((T *)g, Nx, Ny, S, kb::as_stream(stream),
+                                         "kb_apply_fixed_temp_face_2d"))
+            return r;
+    });
+}
+
+int kb_apply_fixed_temp_2d(void *g, int Nx, int Ny, unsigned faces, const double *T_faces,
+                           int dtype, void *stream) {
+    KB_REQUIRE(g, "kb_apply_fixed_temp_2d: null population pointer");
+    KB_REQUIRE(faces < 16u, "kb_apply_fixed_temp_2d: face mask 0x%x has bits beyond 0..3", faces);
+    KB_REQUIRE(faces == 0u || T_faces, "kb_apply_fixed_temp_2d: null temperature array");
+    if (int e = check_dims("kb_apply_fixed_temp_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_apply_fixed_temp_2d", dtype, {
+        if (int r = fixed_temp_all_2d((T *)g, Nx, Ny, faces, T_faces, kb::as_stream(stream)))
+            return r;
+    });
+}
+
+int kb_collide_boussinesq_2d(void *f, const void *Temp, const uint8_t *is_solid, int Nx, int Ny,
+                             double omega, double beta_g, double T_ref, int dtype, void *stream) {
+    KB_REQUIRE(f && Temp, "kb_collide_boussinesq_2d: null pointer");
+    if (int e = check_dims("kb_collide_boussinesq_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_collide_boussinesq_2d", dtype,
+        (boussinesq_k<T, 0><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, (const T *)Temp, is_solid, grid2<T>(Nx, Ny), (T)omega, T(0), T(0), T(0),
+            (T)beta_g, (T)T_ref)));
+}
+
+int kb_collide_boussinesq_vt_2d(void *f, const void *Temp, const uint8_t *is_solid, int Nx, int Ny,
+                                double nu_ref, double T_ref, double A_arr, double beta_g,
+                                int dtype, void *stream) {
+    KB_REQUIRE(f && Temp, "kb_collide_boussinesq_vt_2d: null pointer");
+    if (int e = check_dims("kb_collide_boussinesq_vt_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_collide_boussinesq_vt_2d", dtype,
+        (boussinesq_k<T, 1><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, (const T *)Temp, is_solid, grid2<T>(Nx, Ny), T(0), (T)nu_ref, (T)T_ref,
+            (T)A_arr, (T)beta_g, (T)T_ref)));
+}
+
+int kb_collide_boussinesq_vt_modified_2d(void *f, const void *Temp, const uint8_t *is_solid,
+                                         int Nx, int Ny, double nu_ref, double T0_visc,
+                                         double alpha_visc, double beta_g, double T_ref_buoy,
+                                         int dtype, void *stream) {
+    KB_REQUIRE(f && Temp, "kb_collide_boussinesq_vt_modified_2d: null pointer");
+    if (int e = check_dims("kb_collide_boussinesq_vt_modified_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_collide_boussinesq_vt_modified_2d", dtype,
+        (boussinesq_k<T, 2><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, (const T *)Temp, is_solid, grid2<T>(Nx, Ny), T(0), (T)nu_ref, (T)T0_visc,
+            (T)alpha_visc, (T)beta_g, (T)T_ref_buoy)));
 }
 
 }  // extern "C"

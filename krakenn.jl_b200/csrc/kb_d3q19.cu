@@ -157,6 +157,94 @@ __global__ void __launch_bounds__(BX) fused_trt_k(T *__restrict__ fo, const T *_
     if (rho) { rho[c] = r; ux[c] = a_; uy[c] = b_; uz[c] = d_; }
 }
 
+// _libb_branch (src/kernels/li_bb_2d.jl:70-83), shared by D3Q19.
+template <typename T>
+__device__ __forceinline__ T libb_branch(T q_w, T f_here, T f_back, T f_bar_here, T d) {
+    if (q_w <= T(0.5)) return T(2) * q_w * f_here + (T(1) - T(2) * q_w) * f_back + d;
+    const T inv = T(1) / (T(2) * q_w);
+    return inv * f_here + (T(1) - inv) * f_bar_here + d * inv;
+}
+
+// ApplyLiBBPrePhase_3D (src/kernels/dsl/bricks_3d.jl:367-475): each cut
+// link q (q_wall[q] > 0) replaces the pulled population of the opposite
+// direction with the Bouzidi estimate; the wall-velocity term of each link
+// is written as the reference writes it.  All pointers are at the node,
+// planes of stride P.
+template <typename T, typename I>
+__device__ __forceinline__ void libb_prephase_3d(const T *__restrict__ f0, const T *__restrict__ qw,
+                                                 const T *__restrict__ wx, const T *__restrict__ wy,
+                                                 const T *__restrict__ wz, I P, T *p) {
+    const T c3 = T(1.0 / 3.0), c6 = T(1.0 / 6.0);
+    T q;
+#define KB_LIBB(QA, QB, DELTA) \
+    if ((q = qw[(QA) * P]) > T(0)) p[QB] = libb_branch(q, f0[(QA) * P], p[QA], f0[(QB) * P], DELTA)
+    KB_LIBB(1, 2, -c3 * wx[1 * P]);
+    KB_LIBB(2, 1, c3 * wx[2 * P]);
+    KB_LIBB(3, 4, -c3 * wy[3 * P]);
+    KB_LIBB(4, 3, c3 * wy[4 * P]);
+    KB_LIBB(5, 6, -c3 * wz[5 * P]);
+    KB_LIBB(6, 5, c3 * wz[6 * P]);
+    KB_LIBB(7, 10, -c6 * (wx[7 * P] + wy[7 * P]));
+    KB_LIBB(10, 7, c6 * (wx[10 * P] + wy[10 * P]));
+    KB_LIBB(8, 9, -c6 * (-wx[8 * P] + wy[8 * P]));
+    KB_LIBB(9, 8, -c6 * (wx[9 * P] - wy[9 * P]));
+    KB_LIBB(11, 14, -c6 * (wx[11 * P] + wz[11 * P]));
+    KB_LIBB(14, 11, c6 * (wx[14 * P] + wz[14 * P]));
+    KB_LIBB(12, 13, -c6 * (-wx[12 * P] + wz[12 * P]));
+    KB_LIBB(13, 12, -c6 * (wx[13 * P] - wz[13 * P]));
+    KB_LIBB(15, 18, -c6 * (wy[15 * P] + wz[15 * P]));
+    KB_LIBB(18, 15, c6 * (wy[18 * P] + wz[18 * P]));
+    KB_LIBB(16, 17, -c6 * (-wy[16 * P] + wz[16 * P]));
+    KB_LIBB(17, 16, -c6 * (wy[17 * P] - wz[17 * P]));
+#undef KB_LIBB
+}
+
+// fused_trt_libb_v2_step_3d! (src/kernels/li_bb_3d_v2.jl:13-42): the fused
+// TRT step above with ApplyLiBBPrePhase_3D on fluid nodes.
+template <typename T, typename I>
+__global__ void __launch_bounds__(BX) fused_trt_libb_k(T *__restrict__ fo, const T *__restrict__ fi,
+                                                        T *__restrict__ rho, T *__restrict__ ux,
+                                                        T *__restrict__ uy, T *__restrict__ uz,
+                                                        const uint8_t *__restrict__ solid,
+                                                        const T *__restrict__ qw,
+                                                        const T *__restrict__ wx,
+                                                        const T *__restrict__ wy,
+                                                        const T *__restrict__ wz, Grid3 g, T sp,
+                                                        T sm) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i >= g.Nx) return;
+    const size_t c = (size_t)i + (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k);
+    const I P = (I)g.plane;
+    T *__restrict__ o0 = fo + c;
+    T feq[19];
+    if (solid && solid[c]) {
+        feq_all(T(1), T(0), T(0), T(0), T(0), feq);
+#pragma unroll
+        for (int q = 0; q < 19; ++q) o0[q * P] = feq[q];
+        if (rho) { rho[c] = T(1); ux[c] = T(0); uy[c] = T(0); uz[c] = T(0); }
+        return;
+    }
+    T p[19];
+    pull19_at(fi + c, P, pull_geometry<I>(g, i, j, k), p, Ident());
+    libb_prephase_3d(fi + c, qw + c, wx + c, wy + c, wz + c, P, p);
+    T r, a_, b_, d_;
+    moments(p, r, a_, b_, d_);
+    const T usq = a_ * a_ + b_ * b_ + d_ * d_;
+    feq_all(r, a_, b_, d_, usq, feq);
+    const T a = (sp + sm) * T(0.5), b = (sp - sm) * T(0.5);
+    const int pa[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16};
+    const int pb[9] = {2, 4, 6, 10, 9, 14, 13, 18, 17};
+    o0[0] = p[0] - sp * (p[0] - feq[0]);
+#pragma unroll
+    for (int m = 0; m < 9; ++m) {
+        const int x = pa[m], y = pb[m];
+        o0[x * P] = p[x] - a * (p[x] - feq[x]) - b * (p[y] - feq[y]);
+        o0[y * P] = p[y] - a * (p[y] - feq[y]) - b * (p[x] - feq[x]);
+    }
+    if (rho) { rho[c] = r; ux[c] = a_; uy[c] = b_; uz[c] = d_; }
+}
+
 // Zou-He face descriptors: src/kernels/boundary_3d.jl:39-137 (0-based).
 struct Face {
     int normal_axis, sign, q_axis, q_axis_opp, q_diag[4], q_diag_opp[4];
@@ -265,6 +353,159 @@ __global__ void __launch_bounds__(BX) movingwall_k(T *__restrict__ fo, const T *
     fo[c + 18 * P] = hi ? f0[15 * P] : f0[jp + kp + 18 * P];
 }
 
+// ------------------------------------------------- unfused thermal DDF (3D) --
+// D3Q19 velocities in the reference order (0-based q = reference q - 1).
+__device__ constexpr int kCx[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+__device__ constexpr int kCy[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
+__device__ constexpr int kCz[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
+
+// c_q . v written as the reference writes it: the signed first component,
+// then the second added or subtracted (one component for the axis links).
+template <typename T>
+__device__ __forceinline__ T cdot(int q, T x, T y, T z) {
+    const T v[3] = {x, y, z};
+    const int cc[3] = {kCx[q], kCy[q], kCz[q]};
+    T r = T(0);
+    bool first = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (cc[a] == 0) continue;
+        if (first) { r = cc[a] > 0 ? v[a] : -v[a]; first = false; }
+        else r = cc[a] > 0 ? r + v[a] : r - v[a];
+    }
+    return r;
+}
+
+// collide_thermal_3d_kernel!: src/kernels/thermal_3d.jl:12-104
+template <typename T>
+__global__ void __launch_bounds__(BX) collide_thermal_k(T *__restrict__ gg, const T *__restrict__ ux,
+                                                         const T *__restrict__ uy,
+                                                         const T *__restrict__ uz, Grid3 g, T wT) {
+    NODE3
+    T p[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) p[q] = gg[c + q * P];
+    T Tm = p[0];
+#pragma unroll
+    for (int q = 1; q < 19; ++q) Tm = Tm + p[q];
+    const T a = ux[c], b = uy[c], d = uz[c], t3 = T(3);
+    gg[c] = p[0] - wT * (p[0] - T(1.0 / 3.0) * Tm);
+#pragma unroll
+    for (int q = 1; q < 19; ++q) {
+        const T w = q < 7 ? T(1.0 / 18.0) : T(1.0 / 36.0);
+        const T geq = w * Tm * (T(1) + t3 * cdot(q, a, b, d));
+        gg[c + q * P] = p[q] - wT * (p[q] - geq);
+    }
+}
+
+// compute_temperature_3d_kernel!: src/kernels/thermal_3d.jl:128-135
+template <typename T>
+__global__ void __launch_bounds__(BX) temperature_k(T *__restrict__ Temp, const T *__restrict__ gg, Grid3 g) {
+    NODE3
+    T s = gg[c];
+#pragma unroll
+    for (int q = 1; q < 19; ++q) s = s + gg[c + q * P];
+    Temp[c] = s;
+}
+
+// Half-way anti-bounce-back on one face: _fixed_temp_{west,...,top}_3d!
+// (src/kernels/thermal_3d.jl:154-480).  Per face: the main slot, and four
+// edge slots, each on the edge where the link also leaves through the
+// neighbouring face (order: the face's first in-plane axis low / high, then
+// the second low / high).  An edge slot uses the edge temperature and is left
+// alone when its skip bit is set.
+template <typename T>
+struct FixedTempFace3 {
+    int face;      // 0 west, 1 east, 2 south, 3 north, 4 bottom, 5 top
+    T T_wall;
+    T T_e[4];
+    unsigned skip;  // bit n: edge slot n is owned by the adjacent face
+};
+
+template <typename T>
+struct FixedTempSet3 {
+    int n;
+    FixedTempFace3<T> f[6];
+};
+
+template <typename T>
+__global__ void fixed_temp_k(T *__restrict__ gg, Grid3 g, FixedTempSet3<T> S) {
+    const FixedTempFace3<T> F = S.f[blockIdx.z];
+    const int a = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y;
+    const int axis = F.face >> 1, high = F.face & 1;
+    // in-plane axes: (y, z) for x-faces, (x, z) for y-faces, (x, y) for z-faces
+    const int Na = axis == 0 ? g.Ny : g.Nx, Nb = axis == 2 ? g.Ny : g.Nz;
+    if (a >= Na || b >= Nb) return;
+    int i, j, k;
+    if (axis == 0) { i = high ? g.Nx - 1 : 0; j = a; k = b; }
+    else if (axis == 1) { i = a; j = high ? g.Ny - 1 : 0; k = b; }
+    else { i = a; j = b; k = high ? g.Nz - 1 : 0; }
+    const size_t c = (size_t)i + (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k), P = g.plane;
+    const int qm[6] = {1, 2, 3, 4, 5, 6};
+    const int qe[6][4] = {{7, 9, 11, 13}, {8, 10, 12, 14}, {7, 8, 15, 17},
+                          {9, 10, 16, 18}, {11, 12, 15, 16}, {13, 14, 17, 18}};
+    const bool on[4] = {a == 0, a == Na - 1, b == 0, b == Nb - 1};
+    const T wa = T(2) * T(1.0 / 18.0), we = T(2) * T(1.0 / 36.0);
+    T *m = gg + c + qm[F.face] * P;
+    *m = -*m + wa * F.T_wall;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        T *s = gg + c + qe[F.face][e] * P;
+        const T T_link = on[e] ? F.T_e[e] : F.T_wall;
+        if (!(on[e] && ((F.skip >> e) & 1u))) *s = -*s + we * T_link;
+    }
+}
+
+// collide_boussinesq_3d_kernel!: src/kernels/thermal_3d.jl:559-722 (Guo
+// force F = (0, beta_g (T - T_ref), 0)).
+template <typename T>
+__global__ void __launch_bounds__(BX) boussinesq_k(T *__restrict__ f, const T *__restrict__ Temp,
+                                                    const uint8_t *__restrict__ solid, Grid3 g, T w,
+                                                    T beta_g, T T_ref) {
+    NODE3
+    T p[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) p[q] = f[c + q * P];
+    if (solid && solid[c]) {
+        swap_pairs(p);
+    } else {
+        const T fy = beta_g * (Temp[c] - T_ref);
+        const T fx = T(0), fz = T(0);
+        T rho = p[0];
+#pragma unroll
+        for (int q = 1; q < 19; ++q) rho = rho + p[q];
+        const T inv = T(1) / rho;
+        const T ux = ((p[1] - p[2] + p[7] - p[8] + p[9] - p[10] + p[11] - p[12] + p[13] - p[14]) +
+                      fx / T(2)) * inv;
+        const T uy = ((p[3] - p[4] + p[7] + p[8] - p[9] - p[10] + p[15] - p[16] + p[17] - p[18]) +
+                      fy / T(2)) * inv;
+        const T uz = ((p[5] - p[6] + p[11] + p[12] - p[13] - p[14] + p[15] + p[16] - p[17] - p[18]) +
+                      fz / T(2)) * inv;
+        const T usq = ux * ux + uy * uy + uz * uz;
+        const T gpf = T(1) - w / T(2), t3 = T(3), t9 = T(9);
+        T feq[19];
+        feq_all(rho, ux, uy, uz, usq, feq);
+        // Guo source S_q = w_q ((c_q - u) . F) 3 + w_q (c_q . u)(c_q . F) 9
+        {
+            const T wr = T(1.0 / 3.0);
+            const T S0 = wr * ((-ux) * fx + (-uy) * fy + (-uz) * fz) * t3;
+            p[0] = p[0] - w * (p[0] - feq[0]) + gpf * S0;
+        }
+#pragma unroll
+        for (int q = 1; q < 19; ++q) {
+            const T wq = q < 7 ? T(1.0 / 18.0) : T(1.0 / 36.0);
+            const T ax = kCx[q] > 0 ? T(1) - ux : (kCx[q] < 0 ? -T(1) - ux : -ux);
+            const T ay = kCy[q] > 0 ? T(1) - uy : (kCy[q] < 0 ? -T(1) - uy : -uy);
+            const T az = kCz[q] > 0 ? T(1) - uz : (kCz[q] < 0 ? -T(1) - uz : -uz);
+            const T S = wq * (ax * fx + ay * fy + az * fz) * t3 +
+                        wq * cdot(q, ux, uy, uz) * cdot(q, fx, fy, fz) * t9;
+            p[q] = p[q] - w * (p[q] - feq[q]) + gpf * S;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 19; ++q) f[c + q * P] = p[q];
+}
+
 }  // namespace d3
 }  // namespace kb
 
@@ -317,6 +558,21 @@ int face_fixed(const Face &F, int Nx, int Ny, int Nz) {
 
 namespace {
 int g_trt3d_dev_variant = 0;  // see kb_set_kernel_variant
+
+template <typename T>
+void launch_trt_libb_3d(void *f_out, const void *f_in, void *rho, void *ux, void *uy, void *uz,
+                        const uint8_t *solid, const void *qw, const void *wx, const void *wy,
+                        const void *wz, const Grid3 &g, double sp, double sm, cudaStream_t s) {
+    const dim3 grid = nodes_grid(g.Nx, g.Ny, g.Nz);
+    if (offsets_fit_int(g, 19))
+        fused_trt_libb_k<T, int><<<grid, BX, 0, s>>>(
+            (T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, (T *)uz, solid, (const T *)qw,
+            (const T *)wx, (const T *)wy, (const T *)wz, g, (T)sp, (T)sm);
+    else
+        fused_trt_libb_k<T, long long><<<grid, BX, 0, s>>>(
+            (T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, (T *)uz, solid, (const T *)qw,
+            (const T *)wx, (const T *)wy, (const T *)wz, g, (T)sp, (T)sm);
+}
 }
 namespace kb {
 namespace umma {
@@ -444,6 +700,29 @@ int kb_fused_trt_step_3d(void *f_out, const void *f_in, void *rho, void *ux, voi
     return kb::check_launch(what);
 }
 
+int kb_fused_trt_libb_step_3d(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                              void *uz, const uint8_t *is_solid, const void *q_wall,
+                              const void *uw_link_x, const void *uw_link_y, const void *uw_link_z,
+                              int Nx, int Ny, int Nz, double nu, double Lambda, int periodic,
+                              int dtype, void *stream) {
+    const char *what = "kb_fused_trt_libb_step_3d";
+    KB_REQUIRE(f_out && f_in, "%s: null population pointer", what);
+    KB_REQUIRE(q_wall && uw_link_x && uw_link_y && uw_link_z, "%s: null q_wall / uw_link pointer",
+               what);
+    KB_REQUIRE(f_out != f_in, "%s: f_out and f_in must differ", what);
+    const int nm = (rho != nullptr) + (ux != nullptr) + (uy != nullptr) + (uz != nullptr);
+    KB_REQUIRE(nm == 0 || nm == 4, "%s: pass all four moment arrays or none", what);
+    KB_REQUIRE(periodic >= 0 && periodic < 8, "%s: periodic mask %d not in 0..7", what, periodic);
+    if (int e = check_dims(what, Nx, Ny, Nz)) return e;
+    double sp, sm;
+    if (int e = kb_trt_rates(nu, Lambda, &sp, &sm)) return e;
+    const Grid3 g = grid3(Nx, Ny, Nz, periodic);
+    cudaStream_t s = kb::as_stream(stream);
+    KB3_DISPATCH_PLAIN(what, dtype,
+        launch_trt_libb_3d<T>(f_out, f_in, rho, ux, uy, uz, is_solid, q_wall, uw_link_x,
+                              uw_link_y, uw_link_z, g, sp, sm, s));
+}
+
 int kb_stream_periodic_xz_movingwall_y_3d(void *f_out, const void *f_in, double Ub, double Ut,
                                           double rho_w, int Nx, int Ny, int Nz, int dtype,
                                           void *stream) {
@@ -453,6 +732,133 @@ int kb_stream_periodic_xz_movingwall_y_3d(void *f_out, const void *f_in, double 
     KB3_DISPATCH_PLAIN("kb_stream_periodic_xz_movingwall_y_3d", dtype,
         (movingwall_k<T><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
             (T *)f_out, (const T *)f_in, grid3(Nx, Ny, Nz), (T)Ub, (T)Ut, (T)rho_w)));
+}
+
+int kb_collide_thermal_3d(void *g, const void *ux, const void *uy, const void *uz, int Nx, int Ny,
+                          int Nz, double omega_T, int dtype, void *stream) {
+    KB_REQUIRE(g && ux && uy && uz, "kb_collide_thermal_3d: null pointer");
+    if (int e = check_dims("kb_collide_thermal_3d", Nx, Ny, Nz)) return e;
+    KB3_DISPATCH_PLAIN("kb_collide_thermal_3d", dtype,
+        (collide_thermal_k<T><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
+            (T *)g, (const T *)ux, (const T *)uy, (const T *)uz, grid3(Nx, Ny, Nz), (T)omega_T)));
+}
+
+int kb_compute_temperature_3d(void *Temp, const void *g, int Nx, int Ny, int Nz, int dtype,
+                              void *stream) {
+    KB_REQUIRE(Temp && g, "kb_compute_temperature_3d: null pointer");
+    if (int e = check_dims("kb_compute_temperature_3d", Nx, Ny, Nz)) return e;
+    KB3_DISPATCH_PLAIN("kb_compute_temperature_3d", dtype,
+        (temperature_k<T><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
+            (T *)Temp, (const T *)g, grid3(Nx, Ny, Nz))));
+}
+
+int kb_collide_boussinesq_3d(void *f, const void *Temp, const uint8_t *is_solid, int Nx, int Ny,
+                             int Nz, double omega, double beta_g, double T_ref, int dtype,
+                             void *stream) {
+    KB_REQUIRE(f && Temp, "kb_collide_boussinesq_3d: null pointer");
+    if (int e = check_dims("kb_collide_boussinesq_3d", Nx, Ny, Nz)) return e;
+    KB3_DISPATCH_PLAIN("kb_collide_boussinesq_3d", dtype,
+        (boussinesq_k<T><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, (const T *)Temp, is_solid, grid3(Nx, Ny, Nz), (T)omega, (T)beta_g, (T)T_ref)));
+}
+
+}  // extern "C"
+
+namespace {
+
+template <typename T>
+int launch_fixed_temp_3d(T *g, int Nx, int Ny, int Nz, const FixedTempSet3<T> &S, cudaStream_t s,
+                         const char *what) {
+    if (S.n == 0) return KB_OK;
+    int Na = 1, Nb = 1;
+    for (int n = 0; n < S.n; ++n) {
+        const int axis = S.f[n].face >> 1;
+        const int a = axis == 0 ? Ny : Nx, b = axis == 2 ? Ny : Nz;
+        Na = a > Na ? a : Na;
+        Nb = b > Nb ? b : Nb;
+    }
+    fixed_temp_k<T><<<dim3((Na + BX - 1) / BX, Nb, S.n), BX, 0, s>>>(g, grid3(Nx, Ny, Nz), S);
+    return kb::check_launch(what);
+}
+
+template <typename T>
+T edge_temp(double Ta, bool has_b, double Tb) {
+    // _corner_temp (thermal_2d.jl:356-357): the mean of the two wall temperatures
+    return has_b ? (T(Ta) + T(Tb)) / T(2) : T(Ta);
+}
+
+// _apply_fixed_temp_faces_3d! (thermal_3d.jl:494-533): x-faces apply all
+// their edge slots (mean temperature where the other face is Dirichlet);
+// y-faces skip the edges they share with a Dirichlet x-face; z-faces skip
+// every edge shared with a Dirichlet face.  No slot is written twice, so all
+// faces run in one launch.
+template <typename T>
+int fixed_temp_all_3d(T *g, int Nx, int Ny, int Nz, unsigned faces, const double *Tf,
+                      cudaStream_t s) {
+    bool h[6];
+    for (int n = 0; n < 6; ++n) h[n] = (faces >> n) & 1u;
+    FixedTempSet3<T> S{};
+    S.n = 0;
+    for (int face = 0; face < 6; ++face) {
+        if (!h[face]) continue;
+        FixedTempFace3<T> F{};
+        F.face = face;
+        F.T_wall = T(Tf[face]);
+        if (face < 2) {
+            F.T_e[0] = edge_temp<T>(Tf[face], h[2], Tf[2]);
+            F.T_e[1] = edge_temp<T>(Tf[face], h[3], Tf[3]);
+            F.T_e[2] = edge_temp<T>(Tf[face], h[4], Tf[4]);
+            F.T_e[3] = edge_temp<T>(Tf[face], h[5], Tf[5]);
+            F.skip = 0u;
+        } else if (face < 4) {
+            F.T_e[0] = F.T_e[1] = T(Tf[face]);
+            F.T_e[2] = edge_temp<T>(Tf[face], h[4], Tf[4]);
+            F.T_e[3] = edge_temp<T>(Tf[face], h[5], Tf[5]);
+            F.skip = (h[0] ? 1u : 0u) | (h[1] ? 2u : 0u);
+        } else {
+            F.T_e[0] = F.T_e[1] = F.T_e[2] = F.T_e[3] = T(Tf[face]);
+            F.skip = (h[0] ? 1u : 0u) | (h[1] ? 2u : 0u) | (h[2] ? 4u : 0u) | (h[3] ? 8u : 0u);
+        }
+        S.f[S.n++] = F;
+    }
+    return launch_fixed_temp_3d(g, Nx, Ny, Nz, S, s, "kb_apply_fixed_temp_3d");
+}
+
+}  // namespace
+
+extern "C" {
+
+int kb_apply_fixed_temp_face_3d(void *g, int Nx, int Ny, int Nz, int face, double T_wall,
+                                const double *T_edge, unsigned skip_edges, int dtype,
+                                void *stream) {
+    KB_REQUIRE(g, "kb_apply_fixed_temp_face_3d: null population pointer");
+    KB_REQUIRE(face >= 0 && face < 6, "kb_apply_fixed_temp_face_3d: face %d not in 0..5", face);
+    KB_REQUIRE(skip_edges < 16u, "kb_apply_fixed_temp_face_3d: skip mask 0x%x beyond 4 edges",
+               skip_edges);
+    if (int e = check_dims("kb_apply_fixed_temp_face_3d", Nx, Ny, Nz)) return e;
+    KB3_DISPATCH_PLAIN("kb_apply_fixed_temp_face_3d", dtype, {
+        FixedTempSet3<T> S{};
+        S.n = 1;
+        S.f[0].face = face;
+        S.f[0].T_wall = (T)T_wall;
+        for (int n = 0; n < 4; ++n) S.f[0].T_e[n] = T_edge ? (T)T_edge[n] : (T)T_wall;
+        S.f[0].skip = skip_edges;
+        if (int r = launch_fixed_temp_3d((T *)g, Nx, Ny, Nz, S, kb::as_stream(stream),
+                                         "kb_apply_fixed_temp_face_3d"))
+            return r;
+    });
+}
+
+int kb_apply_fixed_temp_3d(void *g, int Nx, int Ny, int Nz, unsigned faces, const double *T_faces,
+                           int dtype, void *stream) {
+    KB_REQUIRE(g, "kb_apply_fixed_temp_3d: null population pointer");
+    KB_REQUIRE(faces < 64u, "kb_apply_fixed_temp_3d: face mask 0x%x has bits beyond 0..5", faces);
+    KB_REQUIRE(faces == 0u || T_faces, "kb_apply_fixed_temp_3d: null temperature array");
+    if (int e = check_dims("kb_apply_fixed_temp_3d", Nx, Ny, Nz)) return e;
+    KB3_DISPATCH_PLAIN("kb_apply_fixed_temp_3d", dtype, {
+        if (int r = fixed_temp_all_3d((T *)g, Nx, Ny, Nz, faces, T_faces, kb::as_stream(stream)))
+            return r;
+    });
 }
 
 }  // extern "C"

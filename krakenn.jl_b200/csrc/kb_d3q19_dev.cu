@@ -54,22 +54,6 @@ __device__ __forceinline__ uint32_t sr_bits(uint32_t key, int q) { return hash32
 __device__ constexpr int kPairQ[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16};
 __device__ constexpr int kPairQb[9] = {2, 4, 6, 10, 9, 14, 13, 18, 17};
 
-// Scalar / packed-pair arithmetic used by the TRT collision below.
-__device__ __forceinline__ float vadd(float a, float b) { return a + b; }
-__device__ __forceinline__ float vsub(float a, float b) { return a - b; }
-__device__ __forceinline__ float vmul(float a, float b) { return a * b; }
-__device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a, b, c); }
-__device__ __forceinline__ float vneg(float a) { return -a; }
-__device__ __forceinline__ float vsplat(float a, float) { return a; }
-__device__ __forceinline__ float vrcp(float a) { return __frcp_rn(a); }
-__device__ __forceinline__ float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 vsub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
-__device__ __forceinline__ float2 vmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 vneg(float2 a) { return make_float2(-a.x, -a.y); }
-__device__ __forceinline__ float2 vsplat(float a, float2) { return make_float2(a, a); }
-__device__ __forceinline__ float2 vrcp(float2 a) { return make_float2(__frcp_rn(a.x), __frcp_rn(a.y)); }
-
 // TRT collision of D3Q19 deviations d[19] -> o[19] (V = float for one node,
 // float2 for two).  With s_m = d_q + d_qb and t_m = d_q - d_qb of the nine
 // opposite pairs (q, qb), c_qb = -c_q:

@@ -288,3 +288,174 @@ def run_natural_convection_2d(N=128, Ra=1e4, Pr=0.71, Rc=1.0, T_hot=1.0, T_cold=
     return dict(rho=st["rho"].cpu().numpy(), ux=st["ux"].cpu().numpy(),
                 uy=st["uy"].cpu().numpy(), Temp=T_cpu, Nu=nusselt_hot_wall(T_cpu, T_hot, T_cold),
                 Ra=Ra, Pr=Pr, Rc=Rc, nu=p["nu"], alpha=p["alpha"])
+
+
+# ------------------------------------------------ unfused thermal DDF drivers
+
+def _step_loop(step, max_steps: int, graph: bool):
+    """Run `step(parity)` for parity = 0, 1, 0, ... max_steps times.  With
+    `graph`, one two-step cycle (which returns the ping-pong buffers to their
+    places) is captured once as a CUDA graph and replayed, so the short
+    boundary and collision launches of each step cost one graph launch."""
+    if not graph or max_steps < 4:
+        for s in range(max_steps):
+            step(s & 1)
+        return
+    from .batch import Graph
+    g = Graph()
+    with g:
+        step(0)
+        step(1)
+    try:
+        for _ in range(max_steps // 2):
+            g.launch()
+        if max_steps & 1:
+            step(0)
+    finally:
+        g.close()
+
+
+def rayleigh_benard_initial_g(Nx, Ny, T_hot=1.0, T_cold=0.0, orientation="vertical"):
+    """Thermal populations g = w_q T_init of run_rayleigh_benard_2d
+    (src/drivers/thermal.jl:79-98): the half-way conduction profile across
+    the heated gap, plus the sin-sin seed for the vertical orientation."""
+    dT = T_hot - T_cold
+    i = np.arange(1, Nx + 1, dtype=np.float64)[None, :]
+    j = np.arange(1, Ny + 1, dtype=np.float64)[:, None]
+    if orientation == "vertical":
+        # the seed is separable: libm sin per row / column value
+        si = np.array([math.sin(2 * math.pi * a / Nx) for a in range(1, Nx + 1)])[None, :]
+        sj = np.array([math.sin(math.pi * b / Ny) for b in range(1, Ny + 1)])[:, None]
+        T0 = (T_hot - dT * (j - 0.5) / Ny) + ((0.01 * dT) * si) * sj
+    else:
+        T0 = np.broadcast_to(T_hot - dT * (i - 0.5) / Nx, (Ny, Nx))
+    return np.stack([L.D2Q9_W[q] * T0 for q in range(9)])
+
+
+def rayleigh_benard_parameters(Nx, Ny, Ra, Pr, T_hot=1.0, T_cold=0.0, nu=None, alpha=None,
+                               orientation="vertical"):
+    """Parameters of run_rayleigh_benard_2d (src/drivers/thermal.jl:36-70)."""
+    if orientation not in ("vertical", "horizontal"):
+        raise ValueError(f"run_rayleigh_benard_2d: orientation '{orientation}' is not supported; "
+                         "use 'vertical' (hot south / cold north, periodic x) or 'horizontal' "
+                         "(hot west / cold east, solid walls)")
+    dT = T_hot - T_cold
+    if dT == 0:
+        raise ValueError("run_rayleigh_benard_2d: T_hot and T_cold are equal; the buoyancy "
+                         "scaling is undefined")
+    H = Ny if orientation == "vertical" else Nx
+    nu_v = 0.05 if nu is None else float(nu)
+    alpha_v = nu_v / Pr if alpha is None else float(alpha)
+    if nu_v <= 0 or alpha_v <= 0:
+        raise ValueError("run_rayleigh_benard_2d: nu and alpha must be positive")
+    Pr_v = Pr if alpha is None else nu_v / alpha_v
+    return dict(nu=nu_v, alpha=alpha_v, Pr=Pr_v, H=H,
+                beta_g=Ra * nu_v * alpha_v / (dT * H ** 3),
+                omega_f=1.0 / (3.0 * nu_v + 0.5), omega_T=1.0 / (3.0 * alpha_v + 0.5),
+                T_ref=(T_hot + T_cold) / 2)
+
+
+def run_rayleigh_benard_2d(Nx=128, Ny=32, Ra=2000.0, Pr=1.0, T_hot=1.0, T_cold=0.0,
+                           max_steps=20000, nu=None, alpha=None, orientation="vertical",
+                           backend="b200", FT=torch.float64, graph=True):
+    """run_rayleigh_benard_2d -- src/drivers/thermal.jl:31-144: the unfused
+    DDF loop (stream f and g, fixed-temperature faces, T, moments, thermal
+    BGK, Boussinesq BGK) on the B200 kernels."""
+    _require_backend(backend)
+    p = rayleigh_benard_parameters(Nx, Ny, Ra, Pr, T_hot, T_cold, nu, alpha, orientation)
+    cfg = LBMConfig.d2q9(Nx, Ny, p["nu"], 0.0, max_steps)
+    st = initialize_2d(cfg, FT)
+    f = [st["f_in"], st["f_out"]]
+    g0 = torch.from_numpy(rayleigh_benard_initial_g(Nx, Ny, T_hot, T_cold, orientation))
+    g = [g0.to("cuda", FT), g0.to("cuda", FT)]
+    Temp = torch.zeros((Ny, Nx), dtype=FT, device="cuda")
+    rho, ux, uy, solid = st["rho"], st["ux"], st["uy"], st["is_solid"]
+    stream = ops.stream_periodic_x_wall_y_2d_ if orientation == "vertical" else ops.stream_2d_
+
+    def step(par):
+        fi, fo, gi, go = f[par], f[1 - par], g[par], g[1 - par]
+        stream(fo, fi, Nx, Ny)
+        stream(go, gi, Nx, Ny)
+        if orientation == "vertical":
+            ops.apply_fixed_temp_south_2d_(go, T_hot, Nx)
+            ops.apply_fixed_temp_north_2d_(go, T_cold, Nx, Ny)
+        else:
+            ops.apply_fixed_temp_west_2d_(go, T_hot, Ny)
+            ops.apply_fixed_temp_east_2d_(go, T_cold, Nx, Ny)
+        ops.compute_temperature_2d_(Temp, go)
+        ops.compute_macroscopic_2d_(rho, ux, uy, fo)
+        ops.collide_thermal_2d_(go, ux, uy, p["omega_T"])
+        ops.collide_boussinesq_2d_(fo, Temp, solid, p["omega_f"], p["beta_g"], p["T_ref"])
+
+    _step_loop(step, max_steps, graph)
+    fin, gin = f[max_steps & 1], g[max_steps & 1]
+    ops.compute_macroscopic_2d_(rho, ux, uy, fin)
+    ops.compute_temperature_2d_(Temp, gin)
+    return dict(rho=rho.cpu().numpy(), ux=ux.cpu().numpy(), uy=uy.cpu().numpy(),
+                Temp=Temp.cpu().numpy(), f=fin, g=gin, Ra=Ra, Pr=p["Pr"], nu=p["nu"],
+                alpha=p["alpha"], T_hot=T_hot, T_cold=T_cold, orientation=orientation)
+
+
+def natconv_3d_initial_g(N, T_hot=1.0, T_cold=0.0):
+    """g = w_q T_init, linear in x between the half-way walls
+    (src/drivers/thermal.jl:481-490)."""
+    dT = T_hot - T_cold
+    i = np.arange(1, N + 1, dtype=np.float64)
+    T0 = np.broadcast_to(T_hot - dT * (i - 0.5) / N, (N, N, N))
+    return np.stack([L.D3Q19_W[q] * T0 for q in range(19)])
+
+
+def natconv_3d_parameters(N, Ra, Pr, T_hot=1.0, T_cold=0.0):
+    """Parameters of run_natural_convection_3d (src/drivers/thermal.jl:458-469)."""
+    dT = T_hot - T_cold
+    nu = 0.05
+    alpha = nu / Pr
+    return dict(nu=nu, alpha=alpha, beta_g=Ra * nu * alpha / (dT * float(N) ** 3),
+                omega_f=1.0 / (3.0 * nu + 0.5), omega_T=1.0 / (3.0 * alpha + 0.5),
+                T_ref=(T_hot + T_cold) / 2)
+
+
+def nusselt_hot_wall_3d(Temp: np.ndarray, T_hot=1.0, T_cold=0.0) -> float:
+    """Hot-wall Nusselt number of run_natural_convection_3d
+    (src/drivers/thermal.jl:524-533); Temp is (Nz, Ny, Nx)."""
+    Nz, Ny, Nx = Temp.shape
+    dT = T_hot - T_cold
+    dTdx = (-8 * T_hot + 9 * Temp[:, :, 0] - Temp[:, :, 1]) / 3.0
+    nu_arr = -float(Nx) * dTdx / dT
+    return float(np.sum(nu_arr[1:-1, 1:-1]) / max((Ny - 2) * (Nz - 2), 1))
+
+
+def run_natural_convection_3d(N=32, Ra=1e3, Pr=0.71, T_hot=1.0, T_cold=0.0, max_steps=10000,
+                              backend="b200", FT=torch.float64, graph=True):
+    """run_natural_convection_3d -- src/drivers/thermal.jl:455-537: D3Q19
+    flow and thermal DDF, hot west / cold east half-way walls, adiabatic
+    bounce-back elsewhere, Boussinesq force along y."""
+    _require_backend(backend)
+    p = natconv_3d_parameters(N, Ra, Pr, T_hot, T_cold)
+    cfg = LBMConfig.d3q19(N, N, N, p["nu"], 0.0, max_steps)
+    st = initialize_3d(cfg, FT)
+    f = [st["f_in"], st["f_out"]]
+    g0 = torch.from_numpy(np.ascontiguousarray(natconv_3d_initial_g(N, T_hot, T_cold)))
+    g = [g0.to("cuda", FT), g0.to("cuda", FT)]
+    Temp = torch.zeros((N, N, N), dtype=FT, device="cuda")
+    rho, ux, uy, uz, solid = st["rho"], st["ux"], st["uy"], st["uz"], st["is_solid"]
+
+    def step(par):
+        fi, fo, gi, go = f[par], f[1 - par], g[par], g[1 - par]
+        ops.stream_3d_(fo, fi, N, N, N)
+        ops.stream_3d_(go, gi, N, N, N)
+        ops.apply_fixed_temp_west_3d_(go, T_hot, N, N)
+        ops.apply_fixed_temp_east_3d_(go, T_cold, N, N, N)
+        ops.compute_temperature_3d_(Temp, go)
+        ops.compute_macroscopic_3d_(rho, ux, uy, uz, fo)
+        ops.collide_thermal_3d_(go, ux, uy, uz, p["omega_T"])
+        ops.collide_boussinesq_3d_(fo, Temp, solid, p["omega_f"], p["beta_g"], p["T_ref"])
+
+    _step_loop(step, max_steps, graph)
+    fin, gin = f[max_steps & 1], g[max_steps & 1]
+    ops.compute_macroscopic_3d_(rho, ux, uy, uz, fin)
+    ops.compute_temperature_3d_(Temp, gin)
+    T_cpu = Temp.cpu().numpy()
+    return dict(rho=rho.cpu().numpy(), ux=ux.cpu().numpy(), uy=uy.cpu().numpy(),
+                uz=uz.cpu().numpy(), Temp=T_cpu, Nu=nusselt_hot_wall_3d(T_cpu, T_hot, T_cold),
+                f=fin, g=gin, Ra=Ra, Pr=Pr, nu=p["nu"], alpha=p["alpha"])

@@ -232,6 +232,22 @@ def fused_trt_step_(f_out, f_in, rho, ux, uy, is_solid, Nx, Ny, nu, Lambda=3 / 1
          _stream())
 
 
+def fused_trt_libb_v2_step_(f_out, f_in, rho, ux, uy, is_solid, q_wall, uw_link_x, uw_link_y,
+                            Nx, Ny, nu, Lambda=3 / 16):
+    """fused_trt_libb_v2_step! -- src/kernels/li_bb_2d_v2.jl:104 (TRT with
+    Bouzidi interpolated bounce-back on the links flagged in q_wall)"""
+    code = _plain(f_in)
+    _match2(f_in, Nx, Ny); _match2(f_out, Nx, Ny)
+    for name, t in (("q_wall", q_wall), ("uw_link_x", uw_link_x), ("uw_link_y", uw_link_y)):
+        if t is None or t.dtype != f_in.dtype or tuple(t.shape) != tuple(f_in.shape):
+            raise ValueError(f"{name} must be a {f_in.dtype} tensor shaped like f")
+    _ptrs_2d_fields(code, Nx, Ny, rho=rho, ux=ux, uy=uy)
+    call("kb_fused_trt_libb_step", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
+         _t(ux, "ux"), _t(uy, "uy"), _mask(is_solid), _t(q_wall, "q_wall"),
+         _t(uw_link_x, "uw_link_x"), _t(uw_link_y, "uw_link_y"), Nx, Ny, float(nu),
+         float(Lambda), code, _stream())
+
+
 def aa_stream_step_2d_(f, rho, ux, uy, is_solid, Nx, Ny, omega):
     """In-place A-A step, state S -> P (gather from neighbours, collide,
     scatter); the race-free form of aa_even_step!/aa_odd_step!
@@ -366,6 +382,106 @@ def compute_temperature_2d_(Temp, g):
     call("kb_compute_temperature_2d", _t(Temp, "Temp"), _t(g, "g"), Nx, Ny, code, _stream())
 
 
+FACES_2D = {"west": 0, "east": 1, "south": 2, "north": 3}
+
+
+def collide_thermal_2d_(g, ux, uy, omega_T):
+    """collide_thermal_2d! -- src/kernels/thermal_2d.jl:76"""
+    code = _plain(g)
+    Nx, Ny = _dims2(g)
+    _ptrs_2d_fields(code, Nx, Ny, ux=ux, uy=uy)
+    call("kb_collide_thermal_2d", _t(g, "g"), _t(ux, "ux"), _t(uy, "uy"), Nx, Ny,
+         float(omega_T), code, _stream())
+
+
+def collide_thermal_masked_2d_(g, ux, uy, omega_T, is_skip):
+    """collide_thermal_masked_2d! -- src/kernels/thermal_2d.jl:104"""
+    code = _plain(g)
+    Nx, Ny = _dims2(g)
+    _ptrs_2d_fields(code, Nx, Ny, ux=ux, uy=uy)
+    call("kb_collide_thermal_masked_2d", _t(g, "g"), _t(ux, "ux"), _t(uy, "uy"), _mask(is_skip),
+         Nx, Ny, float(omega_T), code, _stream())
+
+
+def _fixed_temp_face_2d_(g, face, T_wall, T_corner, skip):
+    code = _plain(g)
+    Nx, Ny = _dims2(g)
+    call("kb_apply_fixed_temp_face_2d", _t(g, "g"), Nx, Ny, FACES_2D[face], float(T_wall),
+         float(T_corner[0]), float(T_corner[1]), int(bool(skip[0])), int(bool(skip[1])), code,
+         _stream())
+
+
+def apply_fixed_temp_south_2d_(g, T_wall, Nx):
+    """apply_fixed_temp_south_2d! -- src/kernels/thermal_2d.jl:219"""
+    _match2(g, Nx, _dims2(g)[1])
+    _fixed_temp_face_2d_(g, "south", T_wall, (T_wall, T_wall), (False, False))
+
+
+def apply_fixed_temp_north_2d_(g, T_wall, Nx, Ny):
+    """apply_fixed_temp_north_2d! -- src/kernels/thermal_2d.jl:248"""
+    _match2(g, Nx, Ny)
+    _fixed_temp_face_2d_(g, "north", T_wall, (T_wall, T_wall), (False, False))
+
+
+def apply_fixed_temp_west_2d_(g, T_wall, Ny):
+    """apply_fixed_temp_west_2d! -- src/kernels/thermal_2d.jl:311"""
+    _match2(g, _dims2(g)[0], Ny)
+    _fixed_temp_face_2d_(g, "west", T_wall, (T_wall, T_wall), (False, False))
+
+
+def apply_fixed_temp_east_2d_(g, T_wall, Nx, Ny):
+    """apply_fixed_temp_east_2d! -- src/kernels/thermal_2d.jl:340"""
+    _match2(g, Nx, Ny)
+    _fixed_temp_face_2d_(g, "east", T_wall, (T_wall, T_wall), (False, False))
+
+
+def _face_temps(temps, names):
+    mask, T = 0, (C.c_double * len(names))()
+    for n, name in enumerate(names):
+        if temps.get(name) is not None:
+            mask |= 1 << n
+            T[n] = float(temps[name])
+    return mask, T
+
+
+def apply_fixed_temp_2d_(g, Nx, Ny, west=None, east=None, south=None, north=None):
+    """apply_fixed_temp_2d! -- src/kernels/thermal_2d.jl:413 (corner slots of two
+    Dirichlet faces flipped once, with the mean temperature)"""
+    code = _plain(g)
+    _match2(g, Nx, Ny)
+    mask, T = _face_temps(dict(west=west, east=east, south=south, north=north), list(FACES_2D))
+    call("kb_apply_fixed_temp_2d", _t(g, "g"), Nx, Ny, mask, T, code, _stream())
+
+
+def collide_boussinesq_2d_(f, Temp, is_solid, omega, beta_g, T_ref):
+    """collide_boussinesq_2d! -- src/kernels/thermal_2d.jl:573"""
+    code = _plain(f)
+    Nx, Ny = _dims2(f)
+    _ptrs_2d_fields(code, Nx, Ny, Temp=Temp)
+    call("kb_collide_boussinesq_2d", _t(f, "f"), _t(Temp, "Temp"), _mask(is_solid), Nx, Ny,
+         float(omega), float(beta_g), float(T_ref), code, _stream())
+
+
+def collide_boussinesq_vt_2d_(f, Temp, is_solid, nu_ref, T_ref, A_arr, beta_g):
+    """collide_boussinesq_vt_2d! -- src/kernels/thermal_2d.jl:553"""
+    code = _plain(f)
+    Nx, Ny = _dims2(f)
+    _ptrs_2d_fields(code, Nx, Ny, Temp=Temp)
+    call("kb_collide_boussinesq_vt_2d", _t(f, "f"), _t(Temp, "Temp"), _mask(is_solid), Nx, Ny,
+         float(nu_ref), float(T_ref), float(A_arr), float(beta_g), code, _stream())
+
+
+def collide_boussinesq_vt_modified_2d_(f, Temp, is_solid, nu_ref, T0_visc, alpha_visc, beta_g,
+                                       T_ref_buoy):
+    """collide_boussinesq_vt_modified_2d! -- src/kernels/thermal_2d.jl:664"""
+    code = _plain(f)
+    Nx, Ny = _dims2(f)
+    _ptrs_2d_fields(code, Nx, Ny, Temp=Temp)
+    call("kb_collide_boussinesq_vt_modified_2d", _t(f, "f"), _t(Temp, "Temp"), _mask(is_solid),
+         Nx, Ny, float(nu_ref), float(T0_visc), float(alpha_visc), float(beta_g),
+         float(T_ref_buoy), code, _stream())
+
+
 # -------------------------------------------------------------------- D3Q19
 
 def stream_3d_(f_out, f_in, Nx, Ny, Nz):
@@ -415,6 +531,87 @@ def compute_macroscopic_3d_(rho, ux, uy, uz, f):
          _t(f, "f"), Nx, Ny, Nz, code, _stream())
 
 
+def collide_thermal_3d_(g, ux, uy, uz, omega_T):
+    """collide_thermal_3d! -- src/kernels/thermal_3d.jl:119"""
+    code = _plain(g)
+    Nx, Ny, Nz = _dims3(g)
+    _ptrs_3d_fields(code, Nx, Ny, Nz, ux=ux, uy=uy, uz=uz)
+    call("kb_collide_thermal_3d", _t(g, "g"), _t(ux, "ux"), _t(uy, "uy"), _t(uz, "uz"), Nx, Ny,
+         Nz, float(omega_T), code, _stream())
+
+
+def compute_temperature_3d_(Temp, g):
+    """compute_temperature_3d! -- src/kernels/thermal_3d.jl:150"""
+    code = _plain(g)
+    Nx, Ny, Nz = _dims3(g)
+    _ptrs_3d_fields(code, Nx, Ny, Nz, Temp=Temp)
+    call("kb_compute_temperature_3d", _t(Temp, "Temp"), _t(g, "g"), Nx, Ny, Nz, code, _stream())
+
+
+def _fixed_temp_face_3d_(g, face, T_wall, T_edge=None, skip=0):
+    code = _plain(g)
+    Nx, Ny, Nz = _dims3(g)
+    te = None if T_edge is None else (C.c_double * 4)(*[float(t) for t in T_edge])
+    call("kb_apply_fixed_temp_face_3d", _t(g, "g"), Nx, Ny, Nz, FACES_3D[face], float(T_wall), te,
+         int(skip), code, _stream())
+
+
+def apply_fixed_temp_west_3d_(g, T_wall, Ny, Nz):
+    """apply_fixed_temp_west_3d! -- src/kernels/thermal_3d.jl:225"""
+    _match3(g, _dims3(g)[0], Ny, Nz)
+    _fixed_temp_face_3d_(g, "west", T_wall)
+
+
+def apply_fixed_temp_east_3d_(g, T_wall, Nx, Ny, Nz):
+    """apply_fixed_temp_east_3d! -- src/kernels/thermal_3d.jl:273"""
+    _match3(g, Nx, Ny, Nz)
+    _fixed_temp_face_3d_(g, "east", T_wall)
+
+
+def apply_fixed_temp_south_3d_(g, T_wall, Nx, Nz):
+    """apply_fixed_temp_south_3d! -- src/kernels/thermal_3d.jl:321"""
+    _match3(g, Nx, _dims3(g)[1], Nz)
+    _fixed_temp_face_3d_(g, "south", T_wall)
+
+
+def apply_fixed_temp_north_3d_(g, T_wall, Nx, Ny, Nz):
+    """apply_fixed_temp_north_3d! -- src/kernels/thermal_3d.jl:369"""
+    _match3(g, Nx, Ny, Nz)
+    _fixed_temp_face_3d_(g, "north", T_wall)
+
+
+def apply_fixed_temp_bottom_3d_(g, T_wall, Nx, Ny):
+    """apply_fixed_temp_bottom_3d! -- src/kernels/thermal_3d.jl:417"""
+    _match3(g, Nx, Ny, _dims3(g)[2])
+    _fixed_temp_face_3d_(g, "bottom", T_wall)
+
+
+def apply_fixed_temp_top_3d_(g, T_wall, Nx, Ny, Nz):
+    """apply_fixed_temp_top_3d! -- src/kernels/thermal_3d.jl:465"""
+    _match3(g, Nx, Ny, Nz)
+    _fixed_temp_face_3d_(g, "top", T_wall)
+
+
+def apply_fixed_temp_3d_(g, Nx, Ny, Nz, west=None, east=None, south=None, north=None,
+                         bottom=None, top=None):
+    """apply_fixed_temp_3d! -- src/kernels/thermal_3d.jl:547 (edge slots of two
+    Dirichlet faces flipped once, with the mean temperature)"""
+    code = _plain(g)
+    _match3(g, Nx, Ny, Nz)
+    mask, T = _face_temps(dict(west=west, east=east, south=south, north=north, bottom=bottom,
+                               top=top), list(FACES_3D))
+    call("kb_apply_fixed_temp_3d", _t(g, "g"), Nx, Ny, Nz, mask, T, code, _stream())
+
+
+def collide_boussinesq_3d_(f, Temp, is_solid, omega, beta_g, T_ref):
+    """collide_boussinesq_3d! -- src/kernels/thermal_3d.jl:727"""
+    code = _plain(f)
+    Nx, Ny, Nz = _dims3(f)
+    _ptrs_3d_fields(code, Nx, Ny, Nz, Temp=Temp)
+    call("kb_collide_boussinesq_3d", _t(f, "f"), _t(Temp, "Temp"), _mask(is_solid), Nx, Ny, Nz,
+         float(omega), float(beta_g), float(T_ref), code, _stream())
+
+
 def set_trt3d_variant(variant: int):
     """0 automatic, 1 one node per thread, 2 nodes x and x+32 per thread,
     3 adjacent node pairs with vector accesses (even Nx), 4 adjacent node
@@ -454,6 +651,23 @@ def fused_trt_step_3d_(f_out, f_in, rho, ux, uy, uz, is_solid, Nx, Ny, Nz, nu, L
     call("kb_fused_trt_step_3d", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
          _t(ux, "ux"), _t(uy, "uy"), _t(uz, "uz"), _mask(is_solid), Nx, Ny, Nz, float(nu),
          float(Lambda), periodic_mask(periodic), code, _stream())
+
+
+def fused_trt_libb_v2_step_3d_(f_out, f_in, rho, ux, uy, uz, is_solid, q_wall, uw_link_x,
+                               uw_link_y, uw_link_z, Nx, Ny, Nz, nu, Lambda=3 / 16,
+                               periodic=(False, False, False)):
+    """fused_trt_libb_v2_step_3d! -- src/kernels/li_bb_3d_v2.jl:31"""
+    code = _plain(f_in)
+    _match3(f_in, Nx, Ny, Nz); _match3(f_out, Nx, Ny, Nz)
+    for name, t in (("q_wall", q_wall), ("uw_link_x", uw_link_x), ("uw_link_y", uw_link_y),
+                    ("uw_link_z", uw_link_z)):
+        if t is None or t.dtype != f_in.dtype or tuple(t.shape) != tuple(f_in.shape):
+            raise ValueError(f"{name} must be a {f_in.dtype} tensor shaped like f")
+    _ptrs_3d_fields(code, Nx, Ny, Nz, rho=rho, ux=ux, uy=uy, uz=uz)
+    call("kb_fused_trt_libb_step_3d", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
+         _t(ux, "ux"), _t(uy, "uy"), _t(uz, "uz"), _mask(is_solid), _t(q_wall, "q_wall"),
+         _t(uw_link_x, "uw_link_x"), _t(uw_link_y, "uw_link_y"), _t(uw_link_z, "uw_link_z"),
+         Nx, Ny, Nz, float(nu), float(Lambda), periodic_mask(periodic), code, _stream())
 
 
 def stream_periodic_xz_movingwall_y_3d_(f_out, f_in, Ub, Ut, Nx, Ny, Nz, rho_w=1.0):

@@ -956,3 +956,307 @@ void or_set_threads(int n) {
     (void)n;
 #endif
 }
+
+/* ------------------------------------------------------------------------ */
+/* Unfused thermal DDF: src/kernels/thermal_2d.jl, src/kernels/thermal_3d.jl */
+/* ------------------------------------------------------------------------ */
+
+/* collide_thermal_2d!: thermal_2d.jl:16-81 */
+void or_collide_thermal_2d(double *g, const double *ux, const double *uy, int Nx, int Ny,
+                           double wT) {
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            double p[9];
+            for (int q = 0; q < 9; ++q) p[q] = g[I2(i, j, q)];
+            collide_thermal(p, ux[N2(i, j)], uy[N2(i, j)], wT);
+            for (int q = 0; q < 9; ++q) g[I2(i, j, q)] = p[q];
+        }
+}
+
+/* collide_thermal_masked_2d!: thermal_2d.jl:83-109 (per-population loop
+ * with w_q and c_q selected per q, skipped nodes untouched) */
+void or_collide_thermal_masked_2d(double *g, const double *ux, const double *uy,
+                                  const uint8_t *skip, int Nx, int Ny, double wT) {
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            if (skip && skip[N2(i, j)]) continue;
+            double a = ux[N2(i, j)], b = uy[N2(i, j)];
+            double Tm = g[I2(i, j, 0)] + g[I2(i, j, 1)] + g[I2(i, j, 2)] + g[I2(i, j, 3)] +
+                        g[I2(i, j, 4)] + g[I2(i, j, 5)] + g[I2(i, j, 6)] + g[I2(i, j, 7)] +
+                        g[I2(i, j, 8)];
+            for (int q = 0; q < 9; ++q) {
+                double w = q == 0 ? 4.0 / 9.0 : (q <= 4 ? 1.0 / 9.0 : 1.0 / 36.0);
+                double geq = w * Tm * (1.0 + 3.0 * ((double)or_d2q9_cx[q] * a +
+                                                    (double)or_d2q9_cy[q] * b));
+                g[I2(i, j, q)] -= wT * (g[I2(i, j, q)] - geq);
+            }
+        }
+}
+
+/* _abb_slot: thermal_2d.jl:163-166 */
+static inline double abb_slot(double gq, double w2, double T_face, int on_corner, double T_corner,
+                              int skip) {
+    double T_link = on_corner ? T_corner : T_face;
+    return (on_corner && skip) ? gq : -gq + w2 * T_link;
+}
+
+/* _fixed_temp_{west,east,south,north}_2d!: thermal_2d.jl:174-292
+ * face 0 west, 1 east, 2 south, 3 north; Tc/skip at the low / high end. */
+void or_fixed_temp_face_2d(double *g, int Nx, int Ny, int face, double T_wall, double Tc_lo,
+                           double Tc_hi, int skip_lo, int skip_hi) {
+    const double wa = 2.0 * (1.0 / 9.0), we = 2.0 * (1.0 / 36.0);
+    if (face == 2) {          /* south, j = 0: slots 3, 6, 7 (reference) */
+        for (int i = 0; i < Nx; ++i) {
+            g[I2(i, 0, 2)] = -g[I2(i, 0, 2)] + wa * T_wall;
+            g[I2(i, 0, 5)] = abb_slot(g[I2(i, 0, 5)], we, T_wall, i == 0, Tc_lo, skip_lo);
+            g[I2(i, 0, 6)] = abb_slot(g[I2(i, 0, 6)], we, T_wall, i == Nx - 1, Tc_hi, skip_hi);
+        }
+    } else if (face == 3) {   /* north, j = Ny-1: slots 5, 9, 8 */
+        int j = Ny - 1;
+        for (int i = 0; i < Nx; ++i) {
+            g[I2(i, j, 4)] = -g[I2(i, j, 4)] + wa * T_wall;
+            g[I2(i, j, 8)] = abb_slot(g[I2(i, j, 8)], we, T_wall, i == 0, Tc_lo, skip_lo);
+            g[I2(i, j, 7)] = abb_slot(g[I2(i, j, 7)], we, T_wall, i == Nx - 1, Tc_hi, skip_hi);
+        }
+    } else if (face == 0) {   /* west, i = 0: slots 2, 6, 9 */
+        for (int j = 0; j < Ny; ++j) {
+            g[I2(0, j, 1)] = -g[I2(0, j, 1)] + wa * T_wall;
+            g[I2(0, j, 5)] = abb_slot(g[I2(0, j, 5)], we, T_wall, j == 0, Tc_lo, skip_lo);
+            g[I2(0, j, 8)] = abb_slot(g[I2(0, j, 8)], we, T_wall, j == Ny - 1, Tc_hi, skip_hi);
+        }
+    } else {                  /* east, i = Nx-1: slots 4, 7, 8 */
+        int i = Nx - 1;
+        for (int j = 0; j < Ny; ++j) {
+            g[I2(i, j, 3)] = -g[I2(i, j, 3)] + wa * T_wall;
+            g[I2(i, j, 6)] = abb_slot(g[I2(i, j, 6)], we, T_wall, j == 0, Tc_lo, skip_lo);
+            g[I2(i, j, 7)] = abb_slot(g[I2(i, j, 7)], we, T_wall, j == Ny - 1, Tc_hi, skip_hi);
+        }
+    }
+}
+
+/* _corner_temp: thermal_2d.jl:356-357 */
+static inline double corner_temp(double Ta, int has_b, double Tb) {
+    return has_b ? (Ta + Tb) / 2.0 : Ta;
+}
+
+/* _apply_fixed_temp_faces_2d!: thermal_2d.jl:371-392, faces in the order
+ * west, east, south, north; bit n of `faces` = face n Dirichlet at T[n]. */
+void or_fixed_temp_2d(double *g, int Nx, int Ny, unsigned faces, const double *T) {
+    int hw = faces & 1u, he = (faces >> 1) & 1u, hs = (faces >> 2) & 1u, hn = (faces >> 3) & 1u;
+    if (hw) or_fixed_temp_face_2d(g, Nx, Ny, 0, T[0], corner_temp(T[0], hs, T[2]),
+                                  corner_temp(T[0], hn, T[3]), 0, 0);
+    if (he) or_fixed_temp_face_2d(g, Nx, Ny, 1, T[1], corner_temp(T[1], hs, T[2]),
+                                  corner_temp(T[1], hn, T[3]), 0, 0);
+    if (hs) or_fixed_temp_face_2d(g, Nx, Ny, 2, T[2], T[2], T[2], hw, he);
+    if (hn) or_fixed_temp_face_2d(g, Nx, Ny, 3, T[3], T[3], T[3], hw, he);
+}
+
+/* collide_boussinesq_2d! (thermal_2d.jl:421-473) and the nu(T) kernels:
+ * mode 1 collide_boussinesq_vt_2d! (:482-539, Arrhenius), mode 2
+ * collide_boussinesq_vt_modified_2d! (:593-650). */
+void or_collide_boussinesq_2d(double *f, const double *Temp, const uint8_t *solid, int Nx, int Ny,
+                              int mode, double omega, double nu_ref, double Ta, double Aa,
+                              double beta_g, double T_ref) {
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            double p[9];
+            for (int q = 0; q < 9; ++q) p[q] = f[I2(i, j, q)];
+            if (solid && solid[N2(i, j)]) {
+                swap_pairs_2d(p);
+            } else {
+                double Tl = Temp[N2(i, j)];
+                double w = omega;
+                if (mode == 1) {
+                    double nul = nu_ref * exp(Aa * (1.0 / Tl - 1.0 / Ta));
+                    w = 1.0 / (3.0 * nul + 0.5);
+                } else if (mode == 2) {
+                    double nul = nu_ref * exp(Aa * (Tl - Ta));
+                    w = 1.0 / (3.0 * nul + 0.5);
+                }
+                double fy = beta_g * (Tl - T_ref);
+                double fx = 0.0;
+                double rho = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8];
+                double inv = 1.0 / rho;
+                double ux = ((p[1] - p[3] + p[5] - p[6] - p[7] + p[8]) + fx / 2.0) * inv;
+                double uy = ((p[2] - p[4] + p[5] + p[6] - p[7] - p[8]) + fy / 2.0) * inv;
+                collide_boussinesq(p, rho, ux, uy, fy, w);
+            }
+            for (int q = 0; q < 9; ++q) f[I2(i, j, q)] = p[q];
+        }
+}
+
+/* collide_thermal_3d!: thermal_3d.jl:12-124 */
+void or_collide_thermal_3d(double *g, const double *ux, const double *uy, const double *uz,
+                           int Nx, int Ny, int Nz, double wT) {
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                double p[19];
+                for (int q = 0; q < 19; ++q) p[q] = g[I3(i, j, k, q)];
+                double Tm = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8] + p[9] +
+                            p[10] + p[11] + p[12] + p[13] + p[14] + p[15] + p[16] + p[17] + p[18];
+                double a = ux[N3(i, j, k)], b = uy[N3(i, j, k)], c = uz[N3(i, j, k)];
+                const double t3 = 3.0, wa = 1.0 / 18.0, we = 1.0 / 36.0;
+                double geq[19];
+                geq[0] = 1.0 / 3.0 * Tm;
+                geq[1] = wa * Tm * (1.0 + t3 * a);
+                geq[2] = wa * Tm * (1.0 - t3 * a);
+                geq[3] = wa * Tm * (1.0 + t3 * b);
+                geq[4] = wa * Tm * (1.0 - t3 * b);
+                geq[5] = wa * Tm * (1.0 + t3 * c);
+                geq[6] = wa * Tm * (1.0 - t3 * c);
+                geq[7] = we * Tm * (1.0 + t3 * (a + b));
+                geq[8] = we * Tm * (1.0 + t3 * (-a + b));
+                geq[9] = we * Tm * (1.0 + t3 * (a - b));
+                geq[10] = we * Tm * (1.0 + t3 * (-a - b));
+                geq[11] = we * Tm * (1.0 + t3 * (a + c));
+                geq[12] = we * Tm * (1.0 + t3 * (-a + c));
+                geq[13] = we * Tm * (1.0 + t3 * (a - c));
+                geq[14] = we * Tm * (1.0 + t3 * (-a - c));
+                geq[15] = we * Tm * (1.0 + t3 * (b + c));
+                geq[16] = we * Tm * (1.0 + t3 * (-b + c));
+                geq[17] = we * Tm * (1.0 + t3 * (b - c));
+                geq[18] = we * Tm * (1.0 + t3 * (-b - c));
+                for (int q = 0; q < 19; ++q) g[I3(i, j, k, q)] = p[q] - wT * (p[q] - geq[q]);
+            }
+}
+
+/* compute_temperature_3d!: thermal_3d.jl:128-155 */
+void or_temperature_3d(double *Temp, const double *g, int Nx, int Ny, int Nz) {
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                double s = g[I3(i, j, k, 0)];
+                for (int q = 1; q < 19; ++q) s = s + g[I3(i, j, k, q)];
+                Temp[N3(i, j, k)] = s;
+            }
+}
+
+/* _fixed_temp_<face>_3d!: thermal_3d.jl:193-480.  For each face, the main
+ * slot and the four edge slots with the test that puts a node on that edge,
+ * as listed in the reference kernels (0-based slots). */
+void or_fixed_temp_face_3d(double *g, int Nx, int Ny, int Nz, int face, double T_wall,
+                           const double *T_e, unsigned skip) {
+    static const int main_q[6] = {1, 2, 3, 4, 5, 6};
+    static const int edge_q[6][4] = {{7, 9, 11, 13}, {8, 10, 12, 14}, {7, 8, 15, 17},
+                                     {9, 10, 16, 18}, {11, 12, 15, 16}, {13, 14, 17, 18}};
+    const double wa = 2.0 * (1.0 / 18.0), we = 2.0 * (1.0 / 36.0);
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                int on_face, e[4];
+                switch (face) {
+                case 0: on_face = i == 0; e[0] = j == 0; e[1] = j == Ny - 1; e[2] = k == 0; e[3] = k == Nz - 1; break;
+                case 1: on_face = i == Nx - 1; e[0] = j == 0; e[1] = j == Ny - 1; e[2] = k == 0; e[3] = k == Nz - 1; break;
+                case 2: on_face = j == 0; e[0] = i == 0; e[1] = i == Nx - 1; e[2] = k == 0; e[3] = k == Nz - 1; break;
+                case 3: on_face = j == Ny - 1; e[0] = i == 0; e[1] = i == Nx - 1; e[2] = k == 0; e[3] = k == Nz - 1; break;
+                case 4: on_face = k == 0; e[0] = i == 0; e[1] = i == Nx - 1; e[2] = j == 0; e[3] = j == Ny - 1; break;
+                default: on_face = k == Nz - 1; e[0] = i == 0; e[1] = i == Nx - 1; e[2] = j == 0; e[3] = j == Ny - 1; break;
+                }
+                if (!on_face) continue;
+                size_t m = I3(i, j, k, main_q[face]);
+                g[m] = -g[m] + wa * T_wall;
+                for (int n = 0; n < 4; ++n) {
+                    size_t s = I3(i, j, k, edge_q[face][n]);
+                    g[s] = abb_slot(g[s], we, T_wall, e[n], T_e[n], (skip >> n) & 1u);
+                }
+            }
+}
+
+/* _apply_fixed_temp_faces_3d!: thermal_3d.jl:494-533, faces in the order
+ * west, east, south, north, bottom, top. */
+void or_fixed_temp_3d(double *g, int Nx, int Ny, int Nz, unsigned faces, const double *T) {
+    int h[6];
+    for (int n = 0; n < 6; ++n) h[n] = (faces >> n) & 1u;
+    for (int face = 0; face < 6; ++face) {
+        if (!h[face]) continue;
+        double Te[4];
+        unsigned skip = 0;
+        double t = T[face];
+        if (face < 2) {
+            Te[0] = corner_temp(t, h[2], T[2]); Te[1] = corner_temp(t, h[3], T[3]);
+            Te[2] = corner_temp(t, h[4], T[4]); Te[3] = corner_temp(t, h[5], T[5]);
+        } else if (face < 4) {
+            Te[0] = t; Te[1] = t;
+            Te[2] = corner_temp(t, h[4], T[4]); Te[3] = corner_temp(t, h[5], T[5]);
+            skip = (unsigned)h[0] | ((unsigned)h[1] << 1);
+        } else {
+            Te[0] = Te[1] = Te[2] = Te[3] = t;
+            skip = (unsigned)h[0] | ((unsigned)h[1] << 1) | ((unsigned)h[2] << 2) | ((unsigned)h[3] << 3);
+        }
+        or_fixed_temp_face_3d(g, Nx, Ny, Nz, face, t, Te, skip);
+    }
+}
+
+/* collide_boussinesq_3d!: thermal_3d.jl:559-733, population by population
+ * as the reference writes them (F = (0, beta_g (T - T_ref), 0)). */
+void or_collide_boussinesq_3d(double *f, const double *Temp, const uint8_t *solid, int Nx, int Ny,
+                              int Nz, double omega, double beta_g, double T_ref) {
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                double p[19];
+                for (int q = 0; q < 19; ++q) p[q] = f[I3(i, j, k, q)];
+                if (solid && solid[N3(i, j, k)]) {
+                    swap_pairs_3d(p);
+                } else {
+                    double fy = beta_g * (Temp[N3(i, j, k)] - T_ref);
+                    double fx = 0.0, fz = 0.0;
+                    double rho = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8] +
+                                 p[9] + p[10] + p[11] + p[12] + p[13] + p[14] + p[15] + p[16] +
+                                 p[17] + p[18];
+                    double inv = 1.0 / rho;
+                    double ux = ((p[1] - p[2] + p[7] - p[8] + p[9] - p[10] + p[11] - p[12] + p[13] - p[14]) + fx / 2.0) * inv;
+                    double uy = ((p[3] - p[4] + p[7] + p[8] - p[9] - p[10] + p[15] - p[16] + p[17] - p[18]) + fy / 2.0) * inv;
+                    double uz = ((p[5] - p[6] + p[11] + p[12] - p[13] - p[14] + p[15] + p[16] - p[17] - p[18]) + fz / 2.0) * inv;
+                    double usq = ux * ux + uy * uy + uz * uz;
+                    const double wr = 1.0 / 3.0, wa = 1.0 / 18.0, we = 1.0 / 36.0;
+                    const double t3 = 3.0, t45 = 4.5, t15 = 1.5, t9 = 9.0;
+                    double gp = 1.0 - omega / 2.0;
+                    double feq, S, cu, cf;
+#define OR_FEQ(w) ((w) * rho * (1.0 + t3 * cu + t45 * cu * cu - t15 * usq))
+#define OR_UPD(q) p[q] = p[q] - omega * (p[q] - feq) + gp * S
+                    feq = wr * rho * (1.0 - t15 * usq);
+                    S = wr * ((-ux) * fx + (-uy) * fy + (-uz) * fz) * t3; OR_UPD(0);
+                    cu = ux; feq = OR_FEQ(wa);
+                    S = wa * ((1.0 - ux) * fx + (-uy) * fy + (-uz) * fz) * t3 + wa * cu * fx * t9; OR_UPD(1);
+                    cu = -ux; feq = OR_FEQ(wa);
+                    S = wa * ((-1.0 - ux) * fx + (-uy) * fy + (-uz) * fz) * t3 + wa * cu * (-fx) * t9; OR_UPD(2);
+                    cu = uy; feq = OR_FEQ(wa);
+                    S = wa * ((-ux) * fx + (1.0 - uy) * fy + (-uz) * fz) * t3 + wa * cu * fy * t9; OR_UPD(3);
+                    cu = -uy; feq = OR_FEQ(wa);
+                    S = wa * ((-ux) * fx + (-1.0 - uy) * fy + (-uz) * fz) * t3 + wa * cu * (-fy) * t9; OR_UPD(4);
+                    cu = uz; feq = OR_FEQ(wa);
+                    S = wa * ((-ux) * fx + (-uy) * fy + (1.0 - uz) * fz) * t3 + wa * cu * fz * t9; OR_UPD(5);
+                    cu = -uz; feq = OR_FEQ(wa);
+                    S = wa * ((-ux) * fx + (-uy) * fy + (-1.0 - uz) * fz) * t3 + wa * cu * (-fz) * t9; OR_UPD(6);
+                    cu = ux + uy; cf = fx + fy; feq = OR_FEQ(we);
+                    S = we * ((1.0 - ux) * fx + (1.0 - uy) * fy + (-uz) * fz) * t3 + we * cu * cf * t9; OR_UPD(7);
+                    cu = -ux + uy; cf = -fx + fy; feq = OR_FEQ(we);
+                    S = we * ((-1.0 - ux) * fx + (1.0 - uy) * fy + (-uz) * fz) * t3 + we * cu * cf * t9; OR_UPD(8);
+                    cu = ux - uy; cf = fx - fy; feq = OR_FEQ(we);
+                    S = we * ((1.0 - ux) * fx + (-1.0 - uy) * fy + (-uz) * fz) * t3 + we * cu * cf * t9; OR_UPD(9);
+                    cu = -ux - uy; cf = -fx - fy; feq = OR_FEQ(we);
+                    S = we * ((-1.0 - ux) * fx + (-1.0 - uy) * fy + (-uz) * fz) * t3 + we * cu * cf * t9; OR_UPD(10);
+                    cu = ux + uz; cf = fx + fz; feq = OR_FEQ(we);
+                    S = we * ((1.0 - ux) * fx + (-uy) * fy + (1.0 - uz) * fz) * t3 + we * cu * cf * t9; OR_UPD(11);
+                    cu = -ux + uz; cf = -fx + fz; feq = OR_FEQ(we);
+                    S = we * ((-1.0 - ux) * fx + (-uy) * fy + (1.0 - uz) * fz) * t3 + we * cu * cf * t9; OR_UPD(12);
+                    cu = ux - uz; cf = fx - fz; feq = OR_FEQ(we);
+                    S = we * ((1.0 - ux) * fx + (-uy) * fy + (-1.0 - uz) * fz) * t3 + we * cu * cf * t9; OR_UPD(13);
+                    cu = -ux - uz; cf = -fx - fz; feq = OR_FEQ(we);
+                    S = we * ((-1.0 - ux) * fx + (-uy) * fy + (-1.0 - uz) * fz) * t3 + we * cu * cf * t9; OR_UPD(14);
+                    cu = uy + uz; cf = fy + fz; feq = OR_FEQ(we);
+                    S = we * ((-ux) * fx + (1.0 - uy) * fy + (1.0 - uz) * fz) * t3 + we * cu * cf * t9; OR_UPD(15);
+                    cu = -uy + uz; cf = -fy + fz; feq = OR_FEQ(we);
+                    S = we * ((-ux) * fx + (-1.0 - uy) * fy + (1.0 - uz) * fz) * t3 + we * cu * cf * t9; OR_UPD(16);
+                    cu = uy - uz; cf = fy - fz; feq = OR_FEQ(we);
+                    S = we * ((-ux) * fx + (1.0 - uy) * fy + (-1.0 - uz) * fz) * t3 + we * cu * cf * t9; OR_UPD(17);
+                    cu = -uy - uz; cf = -fy - fz; feq = OR_FEQ(we);
+                    S = we * ((-ux) * fx + (-1.0 - uy) * fy + (-1.0 - uz) * fz) * t3 + we * cu * cf * t9; OR_UPD(18);
+#undef OR_FEQ
+#undef OR_UPD
+                }
+                for (int q = 0; q < 19; ++q) f[I3(i, j, k, q)] = p[q];
+            }
+}

@@ -54,6 +54,16 @@ _SIG = {
     "or_fused_natconv_2d": ([_D, _D, _D, _D, _D, _i, _i, _d, _d, _d, _d, _d, _d], None),
     "or_fused_natconv_vt_2d": ([_D, _D, _D, _D, _D, _i, _i, _d, _d, _d, _d, _d, _d, _d, _d], None),
     "or_temperature_2d": ([_D, _D, _i, _i], None),
+    "or_collide_thermal_2d": ([_D, _D, _D, _i, _i, _d], None),
+    "or_collide_thermal_masked_2d": ([_D, _D, _D, _U8, _i, _i, _d], None),
+    "or_fixed_temp_face_2d": ([_D, _i, _i, _i, _d, _d, _d, _i, _i], None),
+    "or_fixed_temp_2d": ([_D, _i, _i, C.c_uint, _D], None),
+    "or_collide_boussinesq_2d": ([_D, _D, _U8, _i, _i, _i, _d, _d, _d, _d, _d, _d], None),
+    "or_collide_thermal_3d": ([_D, _D, _D, _D, _i, _i, _i, _d], None),
+    "or_temperature_3d": ([_D, _D, _i, _i, _i], None),
+    "or_fixed_temp_face_3d": ([_D, _i, _i, _i, _i, _d, _D, C.c_uint], None),
+    "or_fixed_temp_3d": ([_D, _i, _i, _i, C.c_uint, _D], None),
+    "or_collide_boussinesq_3d": ([_D, _D, _U8, _i, _i, _i, _d, _d, _d], None),
     "or_residual": ([_D, _D, _D, _D, _D, _D, _U8, C.c_size_t, _i], _d),
     "or_max_threads": ([], _i),
     "or_set_threads": ([_i], None),
@@ -206,6 +216,57 @@ def temperature_2d(g):
     return T
 
 
+FACES_2D = {"west": 0, "east": 1, "south": 2, "north": 3}
+FACES_3D = {"west": 0, "east": 1, "south": 2, "north": 3, "bottom": 4, "top": 5}
+
+
+def collide_thermal_2d(g, ux, uy, w_T):
+    lib().or_collide_thermal_2d(_p(g), _p(ux), _p(uy), *_nxny(g), float(w_T))
+
+
+def collide_thermal_masked_2d(g, ux, uy, w_T, is_skip):
+    lib().or_collide_thermal_masked_2d(_p(g), _p(ux), _p(uy), _m(is_skip), *_nxny(g), float(w_T))
+
+
+def fixed_temp_face_2d(g, face, T_wall, T_corner=None, skip=(False, False)):
+    """_fixed_temp_<face>_2d!; T_corner defaults to (T_wall, T_wall)."""
+    tc = (T_wall, T_wall) if T_corner is None else T_corner
+    lib().or_fixed_temp_face_2d(_p(g), *_nxny(g), FACES_2D[face], float(T_wall), float(tc[0]),
+                                float(tc[1]), int(bool(skip[0])), int(bool(skip[1])))
+
+
+def _face_set(temps, names):
+    mask, T = 0, np.zeros(len(names))
+    for n, name in enumerate(names):
+        if temps.get(name) is not None:
+            mask |= 1 << n
+            T[n] = float(temps[name])
+    return mask, T
+
+
+def fixed_temp_2d(g, **temps):
+    """apply_fixed_temp_2d!(g, Nx, Ny; west, east, south, north)"""
+    mask, T = _face_set(temps, list(FACES_2D))
+    lib().or_fixed_temp_2d(_p(g), *_nxny(g), mask, _p(T))
+
+
+def collide_boussinesq_2d(f, Temp, solid, omega, beta_g, T_ref):
+    lib().or_collide_boussinesq_2d(_p(f), _p(Temp), _m(solid), *_nxny(f), 0, float(omega), 0.0,
+                                   0.0, 0.0, float(beta_g), float(T_ref))
+
+
+def collide_boussinesq_vt_2d(f, Temp, solid, nu_ref, T_ref, A_arr, beta_g):
+    lib().or_collide_boussinesq_2d(_p(f), _p(Temp), _m(solid), *_nxny(f), 1, 0.0, float(nu_ref),
+                                   float(T_ref), float(A_arr), float(beta_g), float(T_ref))
+
+
+def collide_boussinesq_vt_modified_2d(f, Temp, solid, nu_ref, T0_visc, alpha_visc, beta_g,
+                                      T_ref_buoy):
+    lib().or_collide_boussinesq_2d(_p(f), _p(Temp), _m(solid), *_nxny(f), 2, 0.0, float(nu_ref),
+                                   float(T0_visc), float(alpha_visc), float(beta_g),
+                                   float(T_ref_buoy))
+
+
 # ---- D3Q19 -----------------------------------------------------------------
 def _n3(f):
     return int(f.shape[3]), int(f.shape[2]), int(f.shape[1])
@@ -282,3 +343,31 @@ def equilibrium_d2q9(rho, ux, uy, q):
 
 def equilibrium_d3q19(rho, ux, uy, uz, q):
     return lib().or_equilibrium_d3q19(rho, ux, uy, uz, q)
+
+
+def collide_thermal_3d(g, ux, uy, uz, w_T):
+    lib().or_collide_thermal_3d(_p(g), _p(ux), _p(uy), _p(uz), *_n3(g), float(w_T))
+
+
+def temperature_3d(g):
+    Nx, Ny, Nz = _n3(g)
+    T = np.empty((Nz, Ny, Nx))
+    lib().or_temperature_3d(_p(T), _p(g), Nx, Ny, Nz)
+    return T
+
+
+def fixed_temp_face_3d(g, face, T_wall, T_edge=None, skip=0):
+    """_fixed_temp_<face>_3d!; T_edge defaults to T_wall on all four edges."""
+    te = np.full(4, float(T_wall)) if T_edge is None else np.asarray(T_edge, dtype=np.float64)
+    lib().or_fixed_temp_face_3d(_p(g), *_n3(g), FACES_3D[face], float(T_wall), _p(te), int(skip))
+
+
+def fixed_temp_3d(g, **temps):
+    """apply_fixed_temp_3d!(g, Nx, Ny, Nz; west, east, south, north, bottom, top)"""
+    mask, T = _face_set(temps, list(FACES_3D))
+    lib().or_fixed_temp_3d(_p(g), *_n3(g), mask, _p(T))
+
+
+def collide_boussinesq_3d(f, Temp, solid, omega, beta_g, T_ref):
+    lib().or_collide_boussinesq_3d(_p(f), _p(Temp), _m(solid), *_n3(f), float(omega),
+                                   float(beta_g), float(T_ref))
