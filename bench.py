@@ -807,6 +807,77 @@ def bench_surrogate(pkg, steps=10, warmup=3, batch=16, N=256, base=32, engine=No
     return out
 
 
+def bench_libb(pkg, N=256, R=40.0, steps=50, warmup=5):
+    """TRT + interpolated bounce-back around a sphere of radius R at the
+    centre of a periodic N^3 box (moving fluid, stationary wall): MLUPS of the
+    reference-layout step (dense per-link arrays) and of the compact cut-link
+    table, per storage, against the HBM roofline of 2*19*b bytes per node."""
+    import torch
+    peak, _ = hbm_peak()
+    c = (N - 1) / 2.0
+    qw64, solid = pkg.libb.precompute_q_wall_sphere_3d_torch(N, N, N, c, c, c, R, device="cuda")
+    m = solid.to(torch.uint8)
+    n_links = int((qw64 > 0).sum().item())
+    nodes = N ** 3
+    W = torch.tensor([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12, dtype=torch.float64, device="cuda")
+    out = {"workload": f"D3Q19 TRT + LI-BB, sphere R={R} in a periodic {N}^3 box, nu=0.01, "
+                       f"Lambda=3/16, {steps} steps", "solid_nodes": int(solid.sum().item()),
+           "cut_links": n_links, "peak_gbs": peak, "runs": {}}
+
+    def timeit(step, fa, fb):
+        for _ in range(warmup):
+            step(fa, fb)
+            fa, fb = fb, fa
+        torch.cuda.synchronize()
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(steps):
+            step(fa, fb)
+            fa, fb = fb, fa
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def record(name, ms, b):
+        gbs = 2 * 19 * b * nodes / (ms * 1e-3) / 1e9
+        out["runs"][name] = {"ms": round(ms, 4), "mlups": round(nodes / ms / 1e3, 1),
+                             "gbs": round(gbs, 1), "hbm_frac": round(gbs / peak, 4)}
+
+    per = (True, True, True)
+    for dt, b in ((torch.float64, 8), (torch.float32, 4)):
+        qw = qw64.to(dt)
+        zeros = torch.zeros_like(qw)
+        f0 = (W.view(19, 1, 1, 1) * torch.ones((19, N, N, N), dtype=torch.float64, device="cuda")).to(dt)
+        fa, fb = f0.clone(), torch.empty_like(f0)
+        name = "f64" if dt == torch.float64 else "f32"
+        ms = timeit(lambda x, y: pkg.fused_trt_libb_v2_step_3d_(
+            y, x, None, None, None, None, m, qw, zeros, zeros, zeros, N, N, N, 0.01,
+            periodic=per), fa, fb)
+        record(f"{name}_dense", ms, b)
+        links = pkg.libb.CutLinks(m, qw, zeros, zeros, zeros)
+        ms = timeit(lambda x, y: pkg.fused_trt_libb_links_step_3d_(
+            y, x, None, None, None, None, links, 0.01, periodic=per), fa, fb)
+        record(f"{name}_table", ms, b)
+        ms = timeit(lambda x, y: pkg.fused_trt_step_3d_(
+            y, x, None, None, None, None, m, N, N, N, 0.01, 3 / 16, periodic=per), fa, fb)
+        record(f"{name}_no_links", ms, b)
+        if dt == torch.float32:
+            for sname, sdt, sb in (("f32dev", torch.float32, 4), ("f16dev", torch.float16, 2),
+                                   ("bf16dev", torch.bfloat16, 2)):
+                ga = torch.zeros((19, N, N, N), dtype=sdt, device="cuda")
+                gb = torch.empty_like(ga)
+                ms = timeit(lambda x, y: pkg.fused_trt_libb_links_step_3d_(
+                    y, x, None, None, None, None, links, 0.01, periodic=per,
+                    deviation=True), ga, gb)
+                record(f"{sname}_table", ms, sb)
+                del ga, gb
+        out["nodes_with_links"] = links.nodes_with_links()
+        links.close()
+        del qw, zeros, f0, fa, fb
+        torch.cuda.empty_cache()
+    return out
+
+
 def _extrude(plane, n):
     import torch
     out = torch.empty((19, n, n, n), dtype=plane.dtype, device=plane.device)
@@ -834,6 +905,9 @@ def run_other(args):
     elif args.workload == "surrogate":
         if rank == 0:
             r = bench_surrogate(pkg, steps=min(args.steps, 50), warmup=args.warmup)
+    elif args.workload == "libb":
+        if rank == 0:
+            r = bench_libb(pkg, steps=min(max(args.steps, 20), 200), warmup=args.warmup)
     elif rank == 0:
         r = bench_natconv_validation(pkg)
     if rank == 0:
@@ -862,7 +936,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the short measurements of the other configurations")
-    ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "cavity2d", "batch", "natconv", "warmstart", "surrogate"])
+    ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "cavity2d", "batch", "natconv", "warmstart", "surrogate",
+                             "libb"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -129,6 +129,18 @@ int kb_fused_trt_step(void *f_out, const void *f_in, void *rho, void *ux, void *
                       const uint8_t *is_solid, int Nx, int Ny, double nu, double Lambda, int dtype,
                       void *stream);
 
+/* collide_guo_2d!(f, is_solid, omega, Fx, Fy) -- src/kernels/collide_guo_2d.jl:5-90:
+ * in-place BGK with the Guo source of a constant body force. */
+int kb_collide_guo_2d(void *f, const uint8_t *is_solid, int Nx, int Ny, double omega, double Fx,
+                      double Fy, int dtype, void *stream);
+
+/* collide_guo_field_2d!(f, is_solid, Fx_field, Fy_field, omega)
+ *   -- src/kernels/collide_guo_2d.jl:93-162: per-node force (fields of the
+ * population's type). */
+int kb_collide_guo_field_2d(void *f, const uint8_t *is_solid, const void *Fx_field,
+                            const void *Fy_field, int Nx, int Ny, double omega, int dtype,
+                            void *stream);
+
 /* fused_trt_libb_v2_step!(f_out, f_in, rho, ux, uy, is_solid, q_wall,
  *   uw_link_x, uw_link_y, Nx, Ny, nu; Lambda) -- src/kernels/li_bb_2d_v2.jl:35-41,
  * 104-115: pull with half-way bounce-back, rest equilibrium on solid nodes,
@@ -350,6 +362,40 @@ int kb_fused_trt_libb_step_3d(void *f_out, const void *f_in, void *rho, void *ux
                               const void *uw_link_x, const void *uw_link_y, const void *uw_link_z,
                               int Nx, int Ny, int Nz, double nu, double Lambda, int periodic,
                               int dtype, void *stream);
+
+/* collide_guo_3d!(f, is_solid, omega, Fx, Fy, Fz) -- src/kernels/collide_guo_3d.jl:5-196 */
+int kb_collide_guo_3d(void *f, const uint8_t *is_solid, int Nx, int Ny, int Nz, double omega,
+                      double Fx, double Fy, double Fz, int dtype, void *stream);
+
+/* collide_guo_field_3d!(f, is_solid, Fx_field, Fy_field, Fz_field, omega)
+ *   -- src/kernels/collide_guo_3d.jl:199-332 */
+int kb_collide_guo_field_3d(void *f, const uint8_t *is_solid, const void *Fx_field,
+                            const void *Fy_field, const void *Fz_field, int Nx, int Ny, int Nz,
+                            double omega, int dtype, void *stream);
+
+/* Compact cut-link table (no counterpart in the reference; a B200 layout of
+ * the inputs of fused_trt_libb_v2_step_3d!).  kb_libb_links_create gathers
+ * the cut links of the dense arrays (q_wall, uw_link_x/y/z, dtype KB_F64 or
+ * KB_F32, laid out like f) and the solid mask into one class byte per node
+ * (fluid / solid / fluid with cut links) plus one record per node with cut
+ * links, in node order.  It allocates the table, synchronises `stream` and
+ * keeps no pointer to its inputs.  With the table, a step reads one byte per
+ * node instead of the mask and 19 q_wall values. */
+typedef struct kb_libb_links kb_libb_links;
+int kb_libb_links_create(kb_libb_links **out, const uint8_t *is_solid, const void *q_wall,
+                         const void *uw_link_x, const void *uw_link_y, const void *uw_link_z,
+                         int Nx, int Ny, int Nz, int dtype, void *stream);
+int kb_libb_links_destroy(kb_libb_links *links);
+/* Number of nodes with cut links and the dtype of the stored link data. */
+int kb_libb_links_info(const kb_libb_links *links, long long *nodes_with_links, int *dtype);
+
+/* fused_trt_libb_v2_step_3d! with the compact table: KB_F64 / KB_F32
+ * populations (table of the same dtype) give the same bits as
+ * kb_fused_trt_libb_step_3d; the deviation storages (KB_F32 table) apply
+ * the Bouzidi pre-phase to f - w and collide in FP32. */
+int kb_fused_trt_libb_links_step_3d(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                                    void *uz, const kb_libb_links *links, double nu,
+                                    double Lambda, int periodic, int dtype, void *stream);
 
 /* Fused D3Q19 TRT step: the reference's 3D TRT kernel
  * fused_trt_libb_v2_step_3d!(f_out, f_in, rho, ux, uy, uz, is_solid, ...,

@@ -44,10 +44,18 @@ SIGNATURES: dict[str, list] = {
     "kb_fused_bgk_step": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _i, _vp],
     "kb_trt_rates": [_d, _d, _dp, _dp],
     "kb_fused_trt_step": [_vp, _cvp, _vp, _vp, _vp, _u8p, _i, _i, _d, _d, _i, _vp],
+    "kb_collide_guo_2d": [_vp, _u8p, _i, _i, _d, _d, _d, _i, _vp],
+    "kb_collide_guo_field_2d": [_vp, _u8p, _cvp, _cvp, _i, _i, _d, _i, _vp],
+    "kb_collide_guo_3d": [_vp, _u8p, _i, _i, _i, _d, _d, _d, _d, _i, _vp],
+    "kb_collide_guo_field_3d": [_vp, _u8p, _cvp, _cvp, _cvp, _i, _i, _i, _d, _i, _vp],
     "kb_fused_trt_libb_step": [_vp, _cvp, _vp, _vp, _vp, _u8p, _cvp, _cvp, _cvp, _i, _i, _d, _d,
                                _i, _vp],
     "kb_fused_trt_libb_step_3d": [_vp, _cvp, _vp, _vp, _vp, _vp, _u8p, _cvp, _cvp, _cvp, _cvp, _i,
                                   _i, _i, _d, _d, _i, _i, _vp],
+    "kb_libb_links_create": [_vp, _u8p, _cvp, _cvp, _cvp, _cvp, _i, _i, _i, _i, _vp],
+    "kb_libb_links_destroy": [_vp],
+    "kb_libb_links_info": [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_int)],
+    "kb_fused_trt_libb_links_step_3d": [_vp, _cvp, _vp, _vp, _vp, _vp, _vp, _d, _d, _i, _i, _vp],
     "kb_aa_stream_step_2d": [_vp, _vp, _vp, _vp, _u8p, _i, _i, _d, _i, _vp],
     "kb_aa_local_step_2d": [_vp, _vp, _vp, _vp, _u8p, _i, _i, _d, _i, _vp],
     "kb_collide_mrt_2d": [_vp, _u8p, _i, _i, _d, _d, _d, _d, _i, _vp],

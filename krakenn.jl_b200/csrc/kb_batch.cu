@@ -25,11 +25,14 @@
 namespace kb {
 namespace batch {
 
-constexpr int BT = 256;  // threads per block
+#ifndef KB_BATCH_THREADS
+#define KB_BATCH_THREADS 256
+#endif
+constexpr int BT = KB_BATCH_THREADS;  // threads per block
 // Blocks per SM the register allocation is sized for (__launch_bounds__):
 // more resident warps keep more population loads in flight.
 #ifndef KB_BATCH_MIN_BLOCKS
-#define KB_BATCH_MIN_BLOCKS 4
+#define KB_BATCH_MIN_BLOCKS 6
 #endif
 
 struct CaseDesc {
@@ -700,7 +703,7 @@ int kb_batch_autotune(kb_batch *b, int trial_steps, int *best_tile, int *best_bp
     KB_REQUIRE(trial_steps >= 2 && trial_steps % 2 == 0, "kb_batch_autotune: trial_steps must be even and >= 2");
     cudaStream_t s = kb::as_stream(stream);
     const int tiles[] = {256, 512, 1024, 2048, 4096};
-    const int bpsms[] = {1, 2, 4, 8};
+    const int bpsms[] = {1, 2, 4, 8, 16};  // clamped to the occupancy limit at launch
     double best = -1.0, fixed = -1.0;
     int bt = 256, bb = 1;
     cudaEvent_t e0, e1;

@@ -737,9 +737,12 @@ __device__ __forceinline__ void collide_thermal(T *g, T ux, T uy, T wT) {
     geq = c5 * Tm * (T(1) + t3 * (ux - uy));   g[8] = g[8] - wT * (g[8] - geq);
 }
 
+// BGK with the Guo source of the body force (fx, fy): collide_guo_2d_kernel!
+// (src/kernels/collide_guo_2d.jl:5-81); with fx = 0 and fy the buoyancy it is
+// collide_boussinesq_node (fused_thermal_2d.jl:115-151).  ux, uy are the
+// force-corrected velocities.
 template <typename T>
-__device__ __forceinline__ void collide_boussinesq(T *f, T rho, T ux, T uy, T fy, T w) {
-    const T fx = T(0);
+__device__ __forceinline__ void collide_guo(T *f, T rho, T ux, T uy, T fx, T fy, T w) {
     const T usq = ux * ux + uy * uy;
     const T gp = T(1) - w / T(2);
     const T t3 = T(3), c0 = T(4.0 / 9.0), c1 = T(1.0 / 9.0), c5 = T(1.0 / 36.0), n9 = T(9);
@@ -789,7 +792,7 @@ __global__ void __launch_bounds__(BX) natconv_k(T *__restrict__ fo, const T *__r
         const T nul = nu_ref * kb_exp(a_visc * (Tl - T0_visc));
         w = T(1) / (T(3) * nul + T(0.5));
     }
-    collide_boussinesq(fp, rho, ux, uy, fy, w);
+    collide_guo(fp, rho, ux, uy, T(0), fy, w);
 #pragma unroll
     for (int q = 0; q < 9; ++q) fo[c + q * P] = fp[q];
 }
@@ -923,7 +926,32 @@ __global__ void __launch_bounds__(BX) boussinesq_k(T *__restrict__ f, const T *_
         const T inv = T(1) / rho;
         const T a = ((p[1] - p[3] + p[5] - p[6] - p[7] + p[8]) + fx / T(2)) * inv;
         const T b = ((p[2] - p[4] + p[5] + p[6] - p[7] - p[8]) + fy / T(2)) * inv;
-        collide_boussinesq(p, rho, a, b, fy, w);
+        collide_guo(p, rho, a, b, fx, fy, w);
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[c + q * P] = p[q];
+}
+
+// collide_guo_2d_kernel! (src/kernels/collide_guo_2d.jl:5-81; FIELD false,
+// constant force) and collide_guo_field_2d_kernel! (:93-155; FIELD true,
+// per-node force).  Solid nodes swap opposite pairs.
+template <typename T, bool FIELD>
+__global__ void __launch_bounds__(BX) guo_k(T *__restrict__ f, const uint8_t *__restrict__ solid,
+                                             const T *__restrict__ Fxf, const T *__restrict__ Fyf,
+                                             Grid2<T> g, T omega, T Fx, T Fy) {
+    NODE2
+    T p[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p[q] = f[c + q * P];
+    if (solid && solid[c]) {
+        swap_pairs(p);
+    } else {
+        const T fx = FIELD ? Fxf[c] : Fx, fy = FIELD ? Fyf[c] : Fy;
+        const T rho = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8];
+        const T inv = T(1) / rho;
+        const T a = ((p[1] - p[3] + p[5] - p[6] - p[7] + p[8]) + fx / T(2)) * inv;
+        const T b = ((p[2] - p[4] + p[5] + p[6] - p[7] - p[8]) + fy / T(2)) * inv;
+        collide_guo(p, rho, a, b, fx, fy, omega);
     }
 #pragma unroll
     for (int q = 0; q < 9; ++q) f[c + q * P] = p[q];
@@ -1432,6 +1460,30 @@ int kb_collide_boussinesq_vt_modified_2d(void *f, const void *Temp, const uint8_
         (boussinesq_k<T, 2><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
             (T *)f, (const T *)Temp, is_solid, grid2<T>(Nx, Ny), T(0), (T)nu_ref, (T)T0_visc,
             (T)alpha_visc, (T)beta_g, (T)T_ref_buoy)));
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int kb_collide_guo_2d(void *f, const uint8_t *is_solid, int Nx, int Ny, double omega, double Fx,
+                      double Fy, int dtype, void *stream) {
+    KB_REQUIRE(f, "kb_collide_guo_2d: null population pointer");
+    if (int e = check_dims("kb_collide_guo_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_collide_guo_2d", dtype,
+        (guo_k<T, false><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, is_solid, nullptr, nullptr, grid2<T>(Nx, Ny), (T)omega, (T)Fx, (T)Fy)));
+}
+
+int kb_collide_guo_field_2d(void *f, const uint8_t *is_solid, const void *Fx_field,
+                            const void *Fy_field, int Nx, int Ny, double omega, int dtype,
+                            void *stream) {
+    KB_REQUIRE(f && Fx_field && Fy_field, "kb_collide_guo_field_2d: null pointer");
+    if (int e = check_dims("kb_collide_guo_field_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_collide_guo_field_2d", dtype,
+        (guo_k<T, true><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, is_solid, (const T *)Fx_field, (const T *)Fy_field, grid2<T>(Nx, Ny),
+            (T)omega, T(0), T(0))));
 }
 
 }  // extern "C"

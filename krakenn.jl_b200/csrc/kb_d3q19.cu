@@ -3,6 +3,8 @@
 // Compiled with --fmad=false so double (float) runs round exactly as the
 // reference's CPU Float64 (Float32) path.  The deviation-storage variants of
 // the fused TRT step live in kb_d3q19_dev.cu.
+#include <vector>
+
 #include "kb_d3q19.cuh"
 
 namespace kb {
@@ -157,48 +159,6 @@ __global__ void __launch_bounds__(BX) fused_trt_k(T *__restrict__ fo, const T *_
     if (rho) { rho[c] = r; ux[c] = a_; uy[c] = b_; uz[c] = d_; }
 }
 
-// _libb_branch (src/kernels/li_bb_2d.jl:70-83), shared by D3Q19.
-template <typename T>
-__device__ __forceinline__ T libb_branch(T q_w, T f_here, T f_back, T f_bar_here, T d) {
-    if (q_w <= T(0.5)) return T(2) * q_w * f_here + (T(1) - T(2) * q_w) * f_back + d;
-    const T inv = T(1) / (T(2) * q_w);
-    return inv * f_here + (T(1) - inv) * f_bar_here + d * inv;
-}
-
-// ApplyLiBBPrePhase_3D (src/kernels/dsl/bricks_3d.jl:367-475): each cut
-// link q (q_wall[q] > 0) replaces the pulled population of the opposite
-// direction with the Bouzidi estimate; the wall-velocity term of each link
-// is written as the reference writes it.  All pointers are at the node,
-// planes of stride P.
-template <typename T, typename I>
-__device__ __forceinline__ void libb_prephase_3d(const T *__restrict__ f0, const T *__restrict__ qw,
-                                                 const T *__restrict__ wx, const T *__restrict__ wy,
-                                                 const T *__restrict__ wz, I P, T *p) {
-    const T c3 = T(1.0 / 3.0), c6 = T(1.0 / 6.0);
-    T q;
-#define KB_LIBB(QA, QB, DELTA) \
-    if ((q = qw[(QA) * P]) > T(0)) p[QB] = libb_branch(q, f0[(QA) * P], p[QA], f0[(QB) * P], DELTA)
-    KB_LIBB(1, 2, -c3 * wx[1 * P]);
-    KB_LIBB(2, 1, c3 * wx[2 * P]);
-    KB_LIBB(3, 4, -c3 * wy[3 * P]);
-    KB_LIBB(4, 3, c3 * wy[4 * P]);
-    KB_LIBB(5, 6, -c3 * wz[5 * P]);
-    KB_LIBB(6, 5, c3 * wz[6 * P]);
-    KB_LIBB(7, 10, -c6 * (wx[7 * P] + wy[7 * P]));
-    KB_LIBB(10, 7, c6 * (wx[10 * P] + wy[10 * P]));
-    KB_LIBB(8, 9, -c6 * (-wx[8 * P] + wy[8 * P]));
-    KB_LIBB(9, 8, -c6 * (wx[9 * P] - wy[9 * P]));
-    KB_LIBB(11, 14, -c6 * (wx[11 * P] + wz[11 * P]));
-    KB_LIBB(14, 11, c6 * (wx[14 * P] + wz[14 * P]));
-    KB_LIBB(12, 13, -c6 * (-wx[12 * P] + wz[12 * P]));
-    KB_LIBB(13, 12, -c6 * (wx[13 * P] - wz[13 * P]));
-    KB_LIBB(15, 18, -c6 * (wy[15 * P] + wz[15 * P]));
-    KB_LIBB(18, 15, c6 * (wy[18 * P] + wz[18 * P]));
-    KB_LIBB(16, 17, -c6 * (-wy[16 * P] + wz[16 * P]));
-    KB_LIBB(17, 16, -c6 * (wy[17 * P] - wz[17 * P]));
-#undef KB_LIBB
-}
-
 // fused_trt_libb_v2_step_3d! (src/kernels/li_bb_3d_v2.jl:13-42): the fused
 // TRT step above with ApplyLiBBPrePhase_3D on fluid nodes.
 template <typename T, typename I>
@@ -227,7 +187,7 @@ __global__ void __launch_bounds__(BX) fused_trt_libb_k(T *__restrict__ fo, const
     }
     T p[19];
     pull19_at(fi + c, P, pull_geometry<I>(g, i, j, k), p, Ident());
-    libb_prephase_3d(fi + c, qw + c, wx + c, wy + c, wz + c, P, p);
+    libb_prephase_3d(fi + c, P, LinkDense<T, I>{qw + c, wx + c, wy + c, wz + c, P}, p);
     T r, a_, b_, d_;
     moments(p, r, a_, b_, d_);
     const T usq = a_ * a_ + b_ * b_ + d_ * d_;
@@ -243,6 +203,112 @@ __global__ void __launch_bounds__(BX) fused_trt_libb_k(T *__restrict__ fo, const
         o0[y * P] = p[y] - a * (p[y] - feq[y]) - b * (p[x] - feq[x]);
     }
     if (rho) { rho[c] = r; ux[c] = a_; uy[c] = b_; uz[c] = d_; }
+}
+
+// The same step with the compact cut-link table: one class byte per node
+// replaces the solid mask and the 18 q_wall reads; link data are read only
+// at nodes with cut links.  Bit-identical to fused_trt_libb_k.
+template <typename T, typename I>
+__global__ void __launch_bounds__(BX) fused_trt_links_k(T *__restrict__ fo, const T *__restrict__ fi,
+                                                         T *__restrict__ rho, T *__restrict__ ux,
+                                                         T *__restrict__ uy, T *__restrict__ uz,
+                                                         LinkTable3 L, Grid3 g, T sp, T sm) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i >= g.Nx) return;
+    const size_t c = (size_t)i + (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k);
+    const I P = (I)g.plane;
+    T *__restrict__ o0 = fo + c;
+    T feq[19];
+    const uint8_t cl = L.cls[c];
+    if (cl == 1) {
+        feq_all(T(1), T(0), T(0), T(0), T(0), feq);
+#pragma unroll
+        for (int q = 0; q < 19; ++q) o0[q * P] = feq[q];
+        if (rho) { rho[c] = T(1); ux[c] = T(0); uy[c] = T(0); uz[c] = T(0); }
+        return;
+    }
+    T p[19];
+    pull19_at(fi + c, P, pull_geometry<I>(g, i, j, k), p, Ident());
+    if (cl == 2) libb_prephase_3d(fi + c, P, link_record<T>(L, L.rec[c]), p);
+    T r, a_, b_, d_;
+    moments(p, r, a_, b_, d_);
+    const T usq = a_ * a_ + b_ * b_ + d_ * d_;
+    feq_all(r, a_, b_, d_, usq, feq);
+    const T a = (sp + sm) * T(0.5), b = (sp - sm) * T(0.5);
+    const int pa[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16};
+    const int pb[9] = {2, 4, 6, 10, 9, 14, 13, 18, 17};
+    o0[0] = p[0] - sp * (p[0] - feq[0]);
+#pragma unroll
+    for (int m = 0; m < 9; ++m) {
+        const int x = pa[m], y = pb[m];
+        o0[x * P] = p[x] - a * (p[x] - feq[x]) - b * (p[y] - feq[y]);
+        o0[y * P] = p[y] - a * (p[y] - feq[y]) - b * (p[x] - feq[x]);
+    }
+    if (rho) { rho[c] = r; ux[c] = a_; uy[c] = b_; uz[c] = d_; }
+}
+
+// Cut-link table construction.  Pass 1 classifies every node and counts the
+// nodes with cut links per block of LT nodes; the host scans the counts;
+// pass 2 ranks the nodes inside each block, so records follow node order.
+constexpr int LT = 1024;
+
+template <typename T>
+__device__ __forceinline__ uint8_t link_class(const uint8_t *solid, const T *qw, size_t n,
+                                              size_t nodes) {
+    if (solid && solid[n]) return 1;
+    bool any = false;
+    for (int q = 1; q < 19; ++q) any |= qw[q * nodes + n] > T(0);
+    return any ? 2 : 0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(LT) links_count_k(uint8_t *cls, int *counts, const uint8_t *solid,
+                                                    const T *qw, size_t nodes) {
+    __shared__ int total;
+    if (threadIdx.x == 0) total = 0;
+    __syncthreads();
+    const size_t n = (size_t)blockIdx.x * LT + threadIdx.x;
+    int mine = 0;
+    if (n < nodes) {
+        const uint8_t c = link_class(solid, qw, n, nodes);
+        cls[n] = c;
+        mine = c == 2;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, mine);
+    if ((threadIdx.x & 31) == 0 && bal) atomicAdd(&total, __popc(bal));
+    __syncthreads();
+    if (threadIdx.x == 0) counts[blockIdx.x] = total;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(LT) links_fill_k(int *rec, T *tq, T *tx, T *ty, T *tz,
+                                                   const uint8_t *cls, const int *offsets,
+                                                   const T *qw, const T *wx, const T *wy,
+                                                   const T *wz, size_t nodes, long long n_rec) {
+    __shared__ int warp_base[LT / 32];
+    const size_t n = (size_t)blockIdx.x * LT + threadIdx.x;
+    const int mine = n < nodes && cls[n] == 2;
+    const unsigned bal = __ballot_sync(0xffffffffu, mine);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) warp_base[warp] = __popc(bal);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int w = 0; w < LT / 32; ++w) { const int v = warp_base[w]; warp_base[w] = acc; acc += v; }
+    }
+    __syncthreads();
+    if (!mine) return;
+    const long long r = (long long)offsets[blockIdx.x] + warp_base[warp] +
+                        __popc(bal & ((1u << lane) - 1u));
+    rec[n] = (int)r;
+    for (int q = 1; q < 19; ++q) {
+        const long long t = (long long)(q - 1) * n_rec + r;
+        tq[t] = qw[q * nodes + n];
+        tx[t] = wx[q * nodes + n];
+        ty[t] = wy[q * nodes + n];
+        tz[t] = wz[q * nodes + n];
+    }
 }
 
 // Zou-He face descriptors: src/kernels/boundary_3d.jl:39-137 (0-based).
@@ -456,12 +522,17 @@ __global__ void fixed_temp_k(T *__restrict__ gg, Grid3 g, FixedTempSet3<T> S) {
     }
 }
 
-// collide_boussinesq_3d_kernel!: src/kernels/thermal_3d.jl:559-722 (Guo
-// force F = (0, beta_g (T - T_ref), 0)).
-template <typename T>
+// BGK with the Guo source of a body force: MODE 0 collide_boussinesq_3d_kernel!
+// (src/kernels/thermal_3d.jl:559-722, F = (0, beta_g (T - T_ref), 0)),
+// MODE 1 collide_guo_3d_kernel! (src/kernels/collide_guo_3d.jl:5-186, constant
+// F), MODE 2 collide_guo_field_3d_kernel! (:199-323, per-node F).  The three
+// share the reference's operation order.
+template <typename T, int MODE>
 __global__ void __launch_bounds__(BX) boussinesq_k(T *__restrict__ f, const T *__restrict__ Temp,
                                                     const uint8_t *__restrict__ solid, Grid3 g, T w,
-                                                    T beta_g, T T_ref) {
+                                                    T beta_g, T T_ref, const T *__restrict__ Fxf,
+                                                    const T *__restrict__ Fyf,
+                                                    const T *__restrict__ Fzf, T Fx, T Fy, T Fz) {
     NODE3
     T p[19];
 #pragma unroll
@@ -469,8 +540,9 @@ __global__ void __launch_bounds__(BX) boussinesq_k(T *__restrict__ f, const T *_
     if (solid && solid[c]) {
         swap_pairs(p);
     } else {
-        const T fy = beta_g * (Temp[c] - T_ref);
-        const T fx = T(0), fz = T(0);
+        const T fx = MODE == 0 ? T(0) : (MODE == 1 ? Fx : Fxf[c]);
+        const T fy = MODE == 0 ? beta_g * (Temp[c] - T_ref) : (MODE == 1 ? Fy : Fyf[c]);
+        const T fz = MODE == 0 ? T(0) : (MODE == 1 ? Fz : Fzf[c]);
         T rho = p[0];
 #pragma unroll
         for (int q = 1; q < 19; ++q) rho = rho + p[q];
@@ -758,8 +830,30 @@ int kb_collide_boussinesq_3d(void *f, const void *Temp, const uint8_t *is_solid,
     KB_REQUIRE(f && Temp, "kb_collide_boussinesq_3d: null pointer");
     if (int e = check_dims("kb_collide_boussinesq_3d", Nx, Ny, Nz)) return e;
     KB3_DISPATCH_PLAIN("kb_collide_boussinesq_3d", dtype,
-        (boussinesq_k<T><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
-            (T *)f, (const T *)Temp, is_solid, grid3(Nx, Ny, Nz), (T)omega, (T)beta_g, (T)T_ref)));
+        (boussinesq_k<T, 0><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, (const T *)Temp, is_solid, grid3(Nx, Ny, Nz), (T)omega, (T)beta_g, (T)T_ref,
+            nullptr, nullptr, nullptr, T(0), T(0), T(0))));
+}
+
+int kb_collide_guo_3d(void *f, const uint8_t *is_solid, int Nx, int Ny, int Nz, double omega,
+                      double Fx, double Fy, double Fz, int dtype, void *stream) {
+    KB_REQUIRE(f, "kb_collide_guo_3d: null population pointer");
+    if (int e = check_dims("kb_collide_guo_3d", Nx, Ny, Nz)) return e;
+    KB3_DISPATCH_PLAIN("kb_collide_guo_3d", dtype,
+        (boussinesq_k<T, 1><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, nullptr, is_solid, grid3(Nx, Ny, Nz), (T)omega, T(0), T(0), nullptr,
+            nullptr, nullptr, (T)Fx, (T)Fy, (T)Fz)));
+}
+
+int kb_collide_guo_field_3d(void *f, const uint8_t *is_solid, const void *Fx_field,
+                            const void *Fy_field, const void *Fz_field, int Nx, int Ny, int Nz,
+                            double omega, int dtype, void *stream) {
+    KB_REQUIRE(f && Fx_field && Fy_field && Fz_field, "kb_collide_guo_field_3d: null pointer");
+    if (int e = check_dims("kb_collide_guo_field_3d", Nx, Ny, Nz)) return e;
+    KB3_DISPATCH_PLAIN("kb_collide_guo_field_3d", dtype,
+        (boussinesq_k<T, 2><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f, nullptr, is_solid, grid3(Nx, Ny, Nz), (T)omega, T(0), T(0),
+            (const T *)Fx_field, (const T *)Fy_field, (const T *)Fz_field, T(0), T(0), T(0))));
 }
 
 }  // extern "C"
@@ -859,6 +953,166 @@ int kb_apply_fixed_temp_3d(void *g, int Nx, int Ny, int Nz, unsigned faces, cons
         if (int r = fixed_temp_all_3d((T *)g, Nx, Ny, Nz, faces, T_faces, kb::as_stream(stream)))
             return r;
     });
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------- compact cut links --
+struct kb_libb_links {
+    int Nx = 0, Ny = 0, Nz = 0, dtype = KB_F64;
+    uint8_t *cls = nullptr;
+    int *rec = nullptr;
+    void *qw = nullptr, *wx = nullptr, *wy = nullptr, *wz = nullptr;
+    long long n_rec = 0;
+};
+
+namespace {
+
+kb::d3::LinkTable3 table_view(const kb_libb_links *L) {
+    return kb::d3::LinkTable3{L->cls, L->rec, L->qw, L->wx, L->wy, L->wz, L->n_rec};
+}
+
+template <typename T>
+int build_links(kb_libb_links *L, const uint8_t *solid, const T *qw, const T *wx, const T *wy,
+                const T *wz, cudaStream_t s) {
+    const size_t nodes = (size_t)L->Nx * L->Ny * L->Nz;
+    const size_t nblk = (nodes + kb::d3::LT - 1) / kb::d3::LT;
+    int *counts = nullptr;
+    cudaError_t e = cudaMalloc(&L->cls, nodes);
+    if (e == cudaSuccess) e = cudaMalloc(&L->rec, nodes * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&counts, nblk * sizeof(int));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(counts);
+        return kb::set_error(KB_ERR_NOMEM, "kb_libb_links_create: device allocation failed: %s",
+                             cudaGetErrorString(e));
+    }
+    kb::d3::links_count_k<T><<<(unsigned)nblk, kb::d3::LT, 0, s>>>(L->cls, counts, solid, qw, nodes);
+    std::vector<int> h(nblk);
+    e = cudaMemcpyAsync(h.data(), counts, nblk * sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        cudaFree(counts);
+        return kb::set_error(KB_ERR_CUDA, "kb_libb_links_create: %s", cudaGetErrorString(e));
+    }
+    long long acc = 0;
+    for (size_t b = 0; b < nblk; ++b) { const int v = h[b]; h[b] = (int)acc; acc += v; }
+    if (acc > 2147483647LL) {
+        cudaFree(counts);
+        return kb::set_error(KB_ERR_ARG, "kb_libb_links_create: %lld nodes with cut links "
+                             "exceed the 2^31 record limit", acc);
+    }
+    L->n_rec = acc;
+    e = cudaMemcpyAsync(counts, h.data(), nblk * sizeof(int), cudaMemcpyHostToDevice, s);
+    if (acc > 0 && e == cudaSuccess) {
+        const size_t bytes = (size_t)acc * 18 * sizeof(T);
+        e = cudaMalloc(&L->qw, bytes);
+        if (e == cudaSuccess) e = cudaMalloc(&L->wx, bytes);
+        if (e == cudaSuccess) e = cudaMalloc(&L->wy, bytes);
+        if (e == cudaSuccess) e = cudaMalloc(&L->wz, bytes);
+        if (e == cudaSuccess)
+            kb::d3::links_fill_k<T><<<(unsigned)nblk, kb::d3::LT, 0, s>>>(
+                L->rec, (T *)L->qw, (T *)L->wx, (T *)L->wy, (T *)L->wz, L->cls, counts, qw, wx,
+                wy, wz, nodes, acc);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(counts);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return kb::set_error(KB_ERR_NOMEM, "kb_libb_links_create: %s", cudaGetErrorString(e));
+    }
+    return kb::check_launch("kb_libb_links_create");
+}
+
+template <typename T>
+void launch_links_3d(void *f_out, const void *f_in, void *rho, void *ux, void *uy, void *uz,
+                     const kb::d3::LinkTable3 &L, const Grid3 &g, double sp, double sm,
+                     cudaStream_t s) {
+    const dim3 grid = nodes_grid(g.Nx, g.Ny, g.Nz);
+    if (offsets_fit_int(g, 19))
+        fused_trt_links_k<T, int><<<grid, BX, 0, s>>>(
+            (T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, (T *)uz, L, g, (T)sp, (T)sm);
+    else
+        fused_trt_links_k<T, long long><<<grid, BX, 0, s>>>(
+            (T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, (T *)uz, L, g, (T)sp, (T)sm);
+}
+
+}  // namespace
+
+extern "C" {
+
+int kb_libb_links_destroy(kb_libb_links *L) {
+    if (!L) return KB_OK;
+    cudaFree(L->cls); cudaFree(L->rec);
+    cudaFree(L->qw); cudaFree(L->wx); cudaFree(L->wy); cudaFree(L->wz);
+    delete L;
+    return KB_OK;
+}
+
+int kb_libb_links_create(kb_libb_links **out, const uint8_t *is_solid, const void *q_wall,
+                         const void *uw_link_x, const void *uw_link_y, const void *uw_link_z,
+                         int Nx, int Ny, int Nz, int dtype, void *stream) {
+    const char *what = "kb_libb_links_create";
+    KB_REQUIRE(out, "%s: null handle pointer", what);
+    *out = nullptr;
+    KB_REQUIRE(q_wall && uw_link_x && uw_link_y && uw_link_z, "%s: null q_wall / uw_link pointer",
+               what);
+    KB_REQUIRE(dtype == KB_F64 || dtype == KB_F32,
+               "%s: link arrays must be KB_F64 or KB_F32 (dtype %d)", what, dtype);
+    if (int e = check_dims(what, Nx, Ny, Nz)) return e;
+    kb_libb_links *L = new kb_libb_links();
+    L->Nx = Nx; L->Ny = Ny; L->Nz = Nz; L->dtype = dtype;
+    cudaStream_t s = kb::as_stream(stream);
+    const int r = dtype == KB_F64
+        ? build_links(L, is_solid, (const double *)q_wall, (const double *)uw_link_x,
+                      (const double *)uw_link_y, (const double *)uw_link_z, s)
+        : build_links(L, is_solid, (const float *)q_wall, (const float *)uw_link_x,
+                      (const float *)uw_link_y, (const float *)uw_link_z, s);
+    if (r) { kb_libb_links_destroy(L); return r; }
+    *out = L;
+    return KB_OK;
+}
+
+int kb_libb_links_info(const kb_libb_links *L, long long *nodes_with_links, int *dtype) {
+    KB_REQUIRE(L, "kb_libb_links_info: null handle");
+    if (nodes_with_links) *nodes_with_links = L->n_rec;
+    if (dtype) *dtype = L->dtype;
+    return KB_OK;
+}
+
+int kb_fused_trt_libb_links_step_3d(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                                    void *uz, const kb_libb_links *L, double nu, double Lambda,
+                                    int periodic, int dtype, void *stream) {
+    const char *what = "kb_fused_trt_libb_links_step_3d";
+    KB_REQUIRE(f_out && f_in, "%s: null population pointer", what);
+    KB_REQUIRE(L, "%s: null cut-link table", what);
+    KB_REQUIRE(f_out != f_in, "%s: f_out and f_in must differ", what);
+    const int nm = (rho != nullptr) + (ux != nullptr) + (uy != nullptr) + (uz != nullptr);
+    KB_REQUIRE(nm == 0 || nm == 4, "%s: pass all four moment arrays or none", what);
+    KB_REQUIRE(periodic >= 0 && periodic < 8, "%s: periodic mask %d not in 0..7", what, periodic);
+    double sp, sm;
+    if (int e = kb_trt_rates(nu, Lambda, &sp, &sm)) return e;
+    const Grid3 g = grid3(L->Nx, L->Ny, L->Nz, periodic);
+    cudaStream_t s = kb::as_stream(stream);
+    const kb::d3::LinkTable3 T3 = table_view(L);
+    if (dtype == KB_F64 || dtype == KB_F32) {
+        if (L->dtype != dtype)
+            return kb::set_error(KB_ERR_UNSUPPORTED, "%s: populations of dtype %d need a cut-link "
+                                 "table of the same dtype (table has %d)", what, dtype, L->dtype);
+        if (dtype == KB_F64) launch_links_3d<double>(f_out, f_in, rho, ux, uy, uz, T3, g, sp, sm, s);
+        else launch_links_3d<float>(f_out, f_in, rho, ux, uy, uz, T3, g, sp, sm, s);
+        return kb::check_launch(what);
+    }
+    if (dtype == KB_F32_DEV || dtype == KB_F16_DEV || dtype == KB_BF16_DEV ||
+        dtype == KB_F16_DEV_SR || dtype == KB_BF16_DEV_SR) {
+        if (L->dtype != KB_F32)
+            return kb::set_error(KB_ERR_UNSUPPORTED, "%s: deviation storages collide in FP32 and "
+                                 "need a KB_F32 cut-link table", what);
+        return kb::d3::launch_trt3d_dev_links(dtype, f_out, f_in, (float *)rho, (float *)ux,
+                                              (float *)uy, (float *)uz, T3, g, (float)sp,
+                                              (float)sm, s);
+    }
+    return kb::set_error(KB_ERR_UNSUPPORTED, "%s: unknown dtype %d", what, dtype);
 }
 
 }  // extern "C"

@@ -103,6 +103,97 @@ inline int check_dims(const char *what, int Nx, int Ny, int Nz) {
     return KB_OK;
 }
 
+// _libb_branch (src/kernels/li_bb_2d.jl:70-83), shared by D3Q19.
+template <typename T>
+__device__ __forceinline__ T libb_branch(T q_w, T f_here, T f_back, T f_bar_here, T d) {
+    if (q_w <= T(0.5)) return T(2) * q_w * f_here + (T(1) - T(2) * q_w) * f_back + d;
+    const T inv = T(1) / (T(2) * q_w);
+    return inv * f_here + (T(1) - inv) * f_bar_here + d * inv;
+}
+
+// ApplyLiBBPrePhase_3D (src/kernels/dsl/bricks_3d.jl:367-475): each cut
+// link q (q_wall[q] > 0) replaces the pulled population of the opposite
+// direction with the Bouzidi estimate; the wall-velocity term of each link
+// is written as the reference writes it.  f0 points at the node (planes of
+// stride P); the link data come through `lk` (LinkDense: the reference's
+// dense per-link arrays; LinkRecord: one record of the compact table).
+struct LoadSame {
+    template <typename V> __device__ __forceinline__ V operator()(V v) const { return v; }
+};
+
+template <typename T, typename I, typename Links, typename F = T, typename Load = LoadSame>
+__device__ __forceinline__ void libb_prephase_3d(const F *__restrict__ f0, I P, const Links &lk,
+                                                 T *p, Load ld = Load()) {
+    const T c3 = T(1.0 / 3.0), c6 = T(1.0 / 6.0);
+    T q;
+#define KB_LIBB(QA, QB, DELTA) \
+    if ((q = lk.q(QA)) > T(0)) \
+        p[QB] = libb_branch(q, (T)ld(f0[(QA) * P]), p[QA], (T)ld(f0[(QB) * P]), DELTA)
+    KB_LIBB(1, 2, -c3 * lk.x(1));
+    KB_LIBB(2, 1, c3 * lk.x(2));
+    KB_LIBB(3, 4, -c3 * lk.y(3));
+    KB_LIBB(4, 3, c3 * lk.y(4));
+    KB_LIBB(5, 6, -c3 * lk.z(5));
+    KB_LIBB(6, 5, c3 * lk.z(6));
+    KB_LIBB(7, 10, -c6 * (lk.x(7) + lk.y(7)));
+    KB_LIBB(10, 7, c6 * (lk.x(10) + lk.y(10)));
+    KB_LIBB(8, 9, -c6 * (-lk.x(8) + lk.y(8)));
+    KB_LIBB(9, 8, -c6 * (lk.x(9) - lk.y(9)));
+    KB_LIBB(11, 14, -c6 * (lk.x(11) + lk.z(11)));
+    KB_LIBB(14, 11, c6 * (lk.x(14) + lk.z(14)));
+    KB_LIBB(12, 13, -c6 * (-lk.x(12) + lk.z(12)));
+    KB_LIBB(13, 12, -c6 * (lk.x(13) - lk.z(13)));
+    KB_LIBB(15, 18, -c6 * (lk.y(15) + lk.z(15)));
+    KB_LIBB(18, 15, c6 * (lk.y(18) + lk.z(18)));
+    KB_LIBB(16, 17, -c6 * (-lk.y(16) + lk.z(16)));
+    KB_LIBB(17, 16, -c6 * (lk.y(17) - lk.z(17)));
+#undef KB_LIBB
+}
+
+// The reference's dense per-link arrays (19 planes laid out like f).
+template <typename T, typename I>
+struct LinkDense {
+    const T *qw, *wx, *wy, *wz;  // at the node
+    I P;
+    __device__ __forceinline__ T q(int a) const { return qw[a * P]; }
+    __device__ __forceinline__ T x(int a) const { return wx[a * P]; }
+    __device__ __forceinline__ T y(int a) const { return wy[a * P]; }
+    __device__ __forceinline__ T z(int a) const { return wz[a * P]; }
+};
+
+// Compact cut-link table (kb_libb_links): the cut links of a grid gathered
+// from the dense per-link arrays.  cls holds one byte per node (0 fluid,
+// 1 solid, 2 fluid with cut links), so a step reads one byte per node, as it
+// would read the solid mask, and touches link data only at wall nodes.
+struct LinkTable3 {
+    const uint8_t *cls;
+    const int *rec;                  // record of each cls == 2 node
+    const void *qw, *wx, *wy, *wz;   // link q = 1..18 of record r at [(q - 1) * n_rec + r]
+    long long n_rec;
+};
+
+// One record of the table, read like LinkDense.
+template <typename T>
+struct LinkRecord {
+    const T *qw, *wx, *wy, *wz;  // at the record
+    long long n;                 // n_rec
+    __device__ __forceinline__ T q(int a) const { return qw[(a - 1) * n]; }
+    __device__ __forceinline__ T x(int a) const { return wx[(a - 1) * n]; }
+    __device__ __forceinline__ T y(int a) const { return wy[(a - 1) * n]; }
+    __device__ __forceinline__ T z(int a) const { return wz[(a - 1) * n]; }
+};
+
+template <typename T>
+__device__ __forceinline__ LinkRecord<T> link_record(const LinkTable3 &L, int r) {
+    return LinkRecord<T>{(const T *)L.qw + r, (const T *)L.wx + r, (const T *)L.wy + r,
+                         (const T *)L.wz + r, L.n_rec};
+}
+
+// Deviation-storage step with the compact cut-link table (kb_d3q19_dev.cu).
+int launch_trt3d_dev_links(int dtype, void *f_out, const void *f_in, float *rho, float *ux,
+                           float *uy, float *uz, const LinkTable3 &L, const Grid3 &g, float sp,
+                           float sm, cudaStream_t s);
+
 // Launchers of the fused TRT step for the deviation storages
 // (kb_d3q19_dev.cu); `per` = periodic bit mask.
 int launch_trt3d_dev(int dtype, void *f_out, const void *f_in, float *rho, float *ux, float *uy,

@@ -151,6 +151,50 @@ __global__ void __launch_bounds__(BX) trt_dev_k(R *__restrict__ fo, const R *__r
     if (MOM) { rho_o[c] = rho; ux_o[c] = ux; uy_o[c] = uy; uz_o[c] = uz; }
 }
 
+// One node per thread with the compact cut-link table (kb_libb_links): the
+// class byte replaces the solid mask; nodes with cut links apply the
+// Bouzidi pre-phase on the deviations.  _libb_branch is affine with weights
+// summing to one and maps a population to its opposite, which has the same
+// lattice weight, so it applies to d = f - w unchanged.
+template <typename R, bool MOM, typename I, bool SR>
+__global__ void __launch_bounds__(BX) trt_dev_links_k(R *__restrict__ fo, const R *__restrict__ fi,
+                                                       float *__restrict__ rho_o,
+                                                       float *__restrict__ ux_o,
+                                                       float *__restrict__ uy_o,
+                                                       float *__restrict__ uz_o, LinkTable3 L,
+                                                       Grid3 g, float sp, float sm) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i >= g.Nx) return;
+    const size_t c = (size_t)i + (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k);
+    const I P = (I)g.plane;
+    R *__restrict__ o0 = fo + c;
+    const uint8_t cl = L.cls[c];
+    if (cl == 1) {
+#pragma unroll
+        for (int q = 0; q < 19; ++q) o0[q * P] = Dev<R>::st(0.0f);
+        if (MOM) { rho_o[c] = 1.0f; ux_o[c] = 0.0f; uy_o[c] = 0.0f; uz_o[c] = 0.0f; }
+        return;
+    }
+    float d[19];
+    pull19_at(fi + c, P, pull_geometry<I>(g, i, j, k), d, DevLoad<R>());
+    if (cl == 2) libb_prephase_3d(fi + c, P, link_record<float>(L, L.rec[c]), d, DevLoad<R>());
+    float o[19], rho, ux, uy, uz;
+    trt_dev_collide(d, o, rho, ux, uy, uz, sp, sm);
+    if (SR) {
+        const uint32_t key = sr_key();
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            const uint32_t v = SRPack<R>::pack(o[q], 0.f, sr_bits(key, q));
+            reinterpret_cast<unsigned short *>(o0)[q * P] = (unsigned short)(v & 0xFFFFu);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 19; ++q) o0[q * P] = Dev<R>::st(o[q]);
+    }
+    if (MOM) { rho_o[c] = rho; ux_o[c] = ux; uy_o[c] = uy; uz_o[c] = uz; }
+}
+
 // ---------------------------------------------------------------------------
 // Two nodes per thread: lane l of a warp owns x = x0 + l and x = x0 + l + 32,
 // x0 = 64 * (global warp index along the row).  Every load and store stays a
@@ -626,6 +670,37 @@ int launch_trt3d_dev(int dtype, void *f_out, const void *f_in, float *rho, float
         default: return set_error(KB_ERR_UNSUPPORTED, "kb_fused_trt_step_3d: unknown dtype %d", dtype);
     }
     return check_launch("kb_fused_trt_step_3d");
+}
+
+template <typename R, bool SR>
+static void launch_links_r(void *f_out, const void *f_in, float *rho, float *ux, float *uy,
+                           float *uz, const LinkTable3 &L, const Grid3 &g, float sp, float sm,
+                           cudaStream_t s) {
+    const dim3 grid((g.Nx + BX - 1) / BX, g.Ny, g.Nz);
+    R *fo = (R *)f_out;
+    const R *fi = (const R *)f_in;
+    if (offsets_fit_int(g, 19)) {
+        if (rho) trt_dev_links_k<R, true, int, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
+        else trt_dev_links_k<R, false, int, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
+    } else {
+        if (rho) trt_dev_links_k<R, true, long long, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
+        else trt_dev_links_k<R, false, long long, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
+    }
+    if (SR) sr_advance_k<<<1, 1, 0, s>>>();
+}
+
+int launch_trt3d_dev_links(int dtype, void *f_out, const void *f_in, float *rho, float *ux,
+                           float *uy, float *uz, const LinkTable3 &L, const Grid3 &g, float sp,
+                           float sm, cudaStream_t s) {
+    switch (dtype) {
+        case KB_F32_DEV: launch_links_r<float, false>(f_out, f_in, rho, ux, uy, uz, L, g, sp, sm, s); break;
+        case KB_F16_DEV: launch_links_r<__half, false>(f_out, f_in, rho, ux, uy, uz, L, g, sp, sm, s); break;
+        case KB_BF16_DEV: launch_links_r<__nv_bfloat16, false>(f_out, f_in, rho, ux, uy, uz, L, g, sp, sm, s); break;
+        case KB_F16_DEV_SR: launch_links_r<__half, true>(f_out, f_in, rho, ux, uy, uz, L, g, sp, sm, s); break;
+        case KB_BF16_DEV_SR: launch_links_r<__nv_bfloat16, true>(f_out, f_in, rho, ux, uy, uz, L, g, sp, sm, s); break;
+        default: return set_error(KB_ERR_UNSUPPORTED, "kb_fused_trt_libb_links_step_3d: unknown dtype %d", dtype);
+    }
+    return check_launch("kb_fused_trt_libb_links_step_3d");
 }
 
 }  // namespace d3

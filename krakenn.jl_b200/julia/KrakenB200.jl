@@ -151,4 +151,122 @@ function compute_macroscopic_3d!(ρ, ux, uy, uz, f::CuArray{T,4}) where {T}
         _ptr(ρ), _ptr(ux), _ptr(uy), _ptr(uz), _ptr(f), Nx, Ny, Nz, kb_dtype(T), _stream()))
 end
 
+"collide_thermal_2d!(g, ux, uy, ω_T) -- src/kernels/thermal_2d.jl:76"
+function collide_thermal_2d!(g::CuArray{T,3}, ux, uy, ω_T) where {T}
+    Nx, Ny = size(g, 1), size(g, 2)
+    _check("kb_collide_thermal_2d", ccall((:kb_collide_thermal_2d, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Cint, Cint, Cdouble, Cint, Ptr{Cvoid}),
+        _ptr(g), _ptr(ux), _ptr(uy), Nx, Ny, ω_T, kb_dtype(T), _stream()))
+end
+
+# One face of half-way anti-bounce-back; face 0 west, 1 east, 2 south, 3 north.
+function _fixed_temp_face_2d!(g::CuArray{T,3}, face, T_wall, T_c, skip_c) where {T}
+    Nx, Ny = size(g, 1), size(g, 2)
+    _check("kb_apply_fixed_temp_face_2d", ccall((:kb_apply_fixed_temp_face_2d, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Cint, Cint, Cdouble, Cdouble, Cdouble, Cint, Cint, Cint, Ptr{Cvoid}),
+        _ptr(g), Nx, Ny, face, T_wall, T_c[1], T_c[2], skip_c[1], skip_c[2], kb_dtype(T),
+        _stream()))
+end
+
+"apply_fixed_temp_west_2d!(g, T_wall, Ny) -- src/kernels/thermal_2d.jl:311"
+apply_fixed_temp_west_2d!(g::CuArray, T_wall, Ny) =
+    _fixed_temp_face_2d!(g, 0, T_wall, (T_wall, T_wall), (false, false))
+"apply_fixed_temp_east_2d!(g, T_wall, Nx, Ny) -- src/kernels/thermal_2d.jl:340"
+apply_fixed_temp_east_2d!(g::CuArray, T_wall, Nx, Ny) =
+    _fixed_temp_face_2d!(g, 1, T_wall, (T_wall, T_wall), (false, false))
+"apply_fixed_temp_south_2d!(g, T_wall, Nx) -- src/kernels/thermal_2d.jl:219"
+apply_fixed_temp_south_2d!(g::CuArray, T_wall, Nx) =
+    _fixed_temp_face_2d!(g, 2, T_wall, (T_wall, T_wall), (false, false))
+"apply_fixed_temp_north_2d!(g, T_wall, Nx, Ny) -- src/kernels/thermal_2d.jl:248"
+apply_fixed_temp_north_2d!(g::CuArray, T_wall, Nx, Ny) =
+    _fixed_temp_face_2d!(g, 3, T_wall, (T_wall, T_wall), (false, false))
+
+"apply_fixed_temp_2d!(g, Nx, Ny; west, east, south, north) -- src/kernels/thermal_2d.jl:413"
+function apply_fixed_temp_2d!(g::CuArray{T,3}, Nx, Ny; west=nothing, east=nothing,
+                              south=nothing, north=nothing) where {T}
+    temps = (west, east, south, north)
+    mask = UInt32(0); Tf = zeros(Float64, 4)
+    for (n, t) in enumerate(temps)
+        t === nothing && continue
+        mask |= UInt32(1) << (n - 1); Tf[n] = Float64(t)
+    end
+    _check("kb_apply_fixed_temp_2d", ccall((:kb_apply_fixed_temp_2d, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Cint, Cuint, Ptr{Cdouble}, Cint, Ptr{Cvoid}),
+        _ptr(g), Nx, Ny, mask, Tf, kb_dtype(T), _stream()))
+end
+
+"collide_boussinesq_2d!(f, Temp, is_solid, ω, β_g, T_ref) -- src/kernels/thermal_2d.jl:573"
+function collide_boussinesq_2d!(f::CuArray{T,3}, Temp, is_solid, ω, β_g, T_ref) where {T}
+    Nx, Ny = size(f, 1), size(f, 2)
+    _check("kb_collide_boussinesq_2d", ccall((:kb_collide_boussinesq_2d, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{UInt8}, Cint, Cint, Cdouble, Cdouble, Cdouble, Cint,
+         Ptr{Cvoid}),
+        _ptr(f), _ptr(Temp), _mask(is_solid), Nx, Ny, ω, β_g, T_ref, kb_dtype(T), _stream()))
+end
+
+"fused_trt_libb_v2_step!(f_out, f_in, ρ, ux, uy, is_solid, q_wall, uw_x, uw_y, Nx, Ny, ν; Λ) -- src/kernels/li_bb_2d_v2.jl:104"
+function fused_trt_libb_v2_step!(f_out::CuArray{T,3}, f_in::CuArray{T,3}, ρ, ux, uy, is_solid,
+                                 q_wall, uw_link_x, uw_link_y, Nx, Ny, ν;
+                                 Λ::Real=3/16) where {T}
+    _check("kb_fused_trt_libb_step", ccall((:kb_fused_trt_libb_step, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{UInt8}, Ptr{Cvoid},
+         Ptr{Cvoid}, Ptr{Cvoid}, Cint, Cint, Cdouble, Cdouble, Cint, Ptr{Cvoid}),
+        _ptr(f_out), _ptr(f_in), _ptr(ρ), _ptr(ux), _ptr(uy), _mask(is_solid), _ptr(q_wall),
+        _ptr(uw_link_x), _ptr(uw_link_y), Nx, Ny, ν, Λ, kb_dtype(T), _stream()))
+end
+
+"fused_trt_libb_v2_step_3d!(...) -- src/kernels/li_bb_3d_v2.jl:31"
+function fused_trt_libb_v2_step_3d!(f_out::CuArray{T,4}, f_in::CuArray{T,4}, ρ, ux, uy, uz,
+                                    is_solid, q_wall, uw_link_x, uw_link_y, uw_link_z,
+                                    Nx, Ny, Nz, ν; Λ::Real=3/16) where {T}
+    _check("kb_fused_trt_libb_step_3d", ccall((:kb_fused_trt_libb_step_3d, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{UInt8},
+         Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Cint, Cint, Cint, Cdouble, Cdouble,
+         Cint, Cint, Ptr{Cvoid}),
+        _ptr(f_out), _ptr(f_in), _ptr(ρ), _ptr(ux), _ptr(uy), _ptr(uz), _mask(is_solid),
+        _ptr(q_wall), _ptr(uw_link_x), _ptr(uw_link_y), _ptr(uw_link_z), Nx, Ny, Nz, ν, Λ, 0,
+        kb_dtype(T), _stream()))
+end
+
+"collide_thermal_3d!(g, ux, uy, uz, ω_T) -- src/kernels/thermal_3d.jl:119"
+function collide_thermal_3d!(g::CuArray{T,4}, ux, uy, uz, ω_T) where {T}
+    Nx, Ny, Nz = size(g, 1), size(g, 2), size(g, 3)
+    _check("kb_collide_thermal_3d", ccall((:kb_collide_thermal_3d, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Cint, Cint, Cint, Cdouble, Cint,
+         Ptr{Cvoid}),
+        _ptr(g), _ptr(ux), _ptr(uy), _ptr(uz), Nx, Ny, Nz, ω_T, kb_dtype(T), _stream()))
+end
+
+"compute_temperature_3d!(Temp, g) -- src/kernels/thermal_3d.jl:150"
+function compute_temperature_3d!(Temp, g::CuArray{T,4}) where {T}
+    Nx, Ny, Nz = size(Temp)
+    _check("kb_compute_temperature_3d", ccall((:kb_compute_temperature_3d, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Cint, Cint, Cint, Ptr{Cvoid}),
+        _ptr(Temp), _ptr(g), Nx, Ny, Nz, kb_dtype(T), _stream()))
+end
+
+"apply_fixed_temp_3d!(g, Nx, Ny, Nz; west, east, south, north, bottom, top) -- src/kernels/thermal_3d.jl:547"
+function apply_fixed_temp_3d!(g::CuArray{T,4}, Nx, Ny, Nz; west=nothing, east=nothing,
+                              south=nothing, north=nothing, bottom=nothing,
+                              top=nothing) where {T}
+    temps = (west, east, south, north, bottom, top)
+    mask = UInt32(0); Tf = zeros(Float64, 6)
+    for (n, t) in enumerate(temps)
+        t === nothing && continue
+        mask |= UInt32(1) << (n - 1); Tf[n] = Float64(t)
+    end
+    _check("kb_apply_fixed_temp_3d", ccall((:kb_apply_fixed_temp_3d, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Cint, Cint, Cuint, Ptr{Cdouble}, Cint, Ptr{Cvoid}),
+        _ptr(g), Nx, Ny, Nz, mask, Tf, kb_dtype(T), _stream()))
+end
+
+"collide_boussinesq_3d!(f, Temp, is_solid, ω, β_g, T_ref) -- src/kernels/thermal_3d.jl:727"
+function collide_boussinesq_3d!(f::CuArray{T,4}, Temp, is_solid, ω, β_g, T_ref) where {T}
+    Nx, Ny, Nz = size(f, 1), size(f, 2), size(f, 3)
+    _check("kb_collide_boussinesq_3d", ccall((:kb_collide_boussinesq_3d, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{UInt8}, Cint, Cint, Cint, Cdouble, Cdouble, Cdouble, Cint,
+         Ptr{Cvoid}),
+        _ptr(f), _ptr(Temp), _mask(is_solid), Nx, Ny, Nz, ω, β_g, T_ref, kb_dtype(T), _stream()))
+end
+
 end # module

@@ -232,6 +232,25 @@ def fused_trt_step_(f_out, f_in, rho, ux, uy, is_solid, Nx, Ny, nu, Lambda=3 / 1
          _stream())
 
 
+def collide_guo_2d_(f, is_solid, omega, Fx, Fy):
+    """collide_guo_2d! -- src/kernels/collide_guo_2d.jl:84"""
+    code = _plain(f)
+    Nx, Ny = _dims2(f)
+    call("kb_collide_guo_2d", _t(f, "f"), _mask(is_solid), Nx, Ny, float(omega), float(Fx),
+         float(Fy), code, _stream())
+
+
+def collide_guo_field_2d_(f, is_solid, Fx_field, Fy_field, omega):
+    """collide_guo_field_2d! -- src/kernels/collide_guo_2d.jl:157"""
+    code = _plain(f)
+    Nx, Ny = _dims2(f)
+    for name, t in (("Fx_field", Fx_field), ("Fy_field", Fy_field)):
+        if t is None or t.dtype != f.dtype or tuple(t.shape) != (Ny, Nx):
+            raise ValueError(f"{name} must be a {f.dtype} tensor of shape (Ny, Nx)")
+    call("kb_collide_guo_field_2d", _t(f, "f"), _mask(is_solid), _t(Fx_field, "Fx_field"),
+         _t(Fy_field, "Fy_field"), Nx, Ny, float(omega), code, _stream())
+
+
 def fused_trt_libb_v2_step_(f_out, f_in, rho, ux, uy, is_solid, q_wall, uw_link_x, uw_link_y,
                             Nx, Ny, nu, Lambda=3 / 16):
     """fused_trt_libb_v2_step! -- src/kernels/li_bb_2d_v2.jl:104 (TRT with
@@ -603,6 +622,26 @@ def apply_fixed_temp_3d_(g, Nx, Ny, Nz, west=None, east=None, south=None, north=
     call("kb_apply_fixed_temp_3d", _t(g, "g"), Nx, Ny, Nz, mask, T, code, _stream())
 
 
+def collide_guo_3d_(f, is_solid, omega, Fx, Fy, Fz):
+    """collide_guo_3d! -- src/kernels/collide_guo_3d.jl:190"""
+    code = _plain(f)
+    Nx, Ny, Nz = _dims3(f)
+    call("kb_collide_guo_3d", _t(f, "f"), _mask(is_solid), Nx, Ny, Nz, float(omega), float(Fx),
+         float(Fy), float(Fz), code, _stream())
+
+
+def collide_guo_field_3d_(f, is_solid, Fx_field, Fy_field, Fz_field, omega):
+    """collide_guo_field_3d! -- src/kernels/collide_guo_3d.jl:327"""
+    code = _plain(f)
+    Nx, Ny, Nz = _dims3(f)
+    for name, t in (("Fx_field", Fx_field), ("Fy_field", Fy_field), ("Fz_field", Fz_field)):
+        if t is None or t.dtype != f.dtype or tuple(t.shape) != (Nz, Ny, Nx):
+            raise ValueError(f"{name} must be a {f.dtype} tensor of shape (Nz, Ny, Nx)")
+    call("kb_collide_guo_field_3d", _t(f, "f"), _mask(is_solid), _t(Fx_field, "Fx_field"),
+         _t(Fy_field, "Fy_field"), _t(Fz_field, "Fz_field"), Nx, Ny, Nz, float(omega), code,
+         _stream())
+
+
 def collide_boussinesq_3d_(f, Temp, is_solid, omega, beta_g, T_ref):
     """collide_boussinesq_3d! -- src/kernels/thermal_3d.jl:727"""
     code = _plain(f)
@@ -668,6 +707,25 @@ def fused_trt_libb_v2_step_3d_(f_out, f_in, rho, ux, uy, uz, is_solid, q_wall, u
          _t(ux, "ux"), _t(uy, "uy"), _t(uz, "uz"), _mask(is_solid), _t(q_wall, "q_wall"),
          _t(uw_link_x, "uw_link_x"), _t(uw_link_y, "uw_link_y"), _t(uw_link_z, "uw_link_z"),
          Nx, Ny, Nz, float(nu), float(Lambda), periodic_mask(periodic), code, _stream())
+
+
+def fused_trt_libb_links_step_3d_(f_out, f_in, rho, ux, uy, uz, links, nu, Lambda=3 / 16,
+                                  periodic=(False, False, False), deviation=False,
+                                  stochastic_rounding=False):
+    """fused_trt_libb_v2_step_3d! with a compact cut-link table
+    (`libb.CutLinks`); any storage (float16/bfloat16 and deviation=True hold
+    f - w; stochastic_rounding as in fused_trt_step_3d_)."""
+    code = storage_dtype(f_in, deviation)
+    if stochastic_rounding:
+        if code not in (KB_F16_DEV, KB_BF16_DEV):
+            raise ValueError("stochastic rounding applies to float16/bfloat16 deviation storage")
+        code = KB_F16_DEV_SR if code == KB_F16_DEV else KB_BF16_DEV_SR
+    Nx, Ny, Nz = links.Nx, links.Ny, links.Nz
+    _match3(f_in, Nx, Ny, Nz); _match3(f_out, Nx, Ny, Nz)
+    _ptrs_3d_fields(code, Nx, Ny, Nz, rho=rho, ux=ux, uy=uy, uz=uz)
+    call("kb_fused_trt_libb_links_step_3d", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
+         _t(ux, "ux"), _t(uy, "uy"), _t(uz, "uz"), links.handle, float(nu), float(Lambda),
+         periodic_mask(periodic), code, _stream())
 
 
 def stream_periodic_xz_movingwall_y_3d_(f_out, f_in, Ub, Ut, Nx, Ny, Nz, rho_w=1.0):

@@ -1190,8 +1190,35 @@ void or_fixed_temp_3d(double *g, int Nx, int Ny, int Nz, unsigned faces, const d
 
 /* collide_boussinesq_3d!: thermal_3d.jl:559-733, population by population
  * as the reference writes them (F = (0, beta_g (T - T_ref), 0)). */
+/* Shared by collide_boussinesq_3d! (mode 0: F = (0, beta_g (T - T_ref), 0)) and
+ * collide_guo_3d! / collide_guo_field_3d! (src/kernels/collide_guo_3d.jl:5-186,
+ * 199-323; mode 1 constant F, mode 2 per-node fields): the same expressions. */
+static void guo_3d_core(double *f, const double *Temp, const uint8_t *solid, int Nx, int Ny,
+                        int Nz, double omega, double beta_g, double T_ref, int mode, double Fx,
+                        double Fy, double Fz, const double *Fxf, const double *Fyf,
+                        const double *Fzf);
+
 void or_collide_boussinesq_3d(double *f, const double *Temp, const uint8_t *solid, int Nx, int Ny,
                               int Nz, double omega, double beta_g, double T_ref) {
+    guo_3d_core(f, Temp, solid, Nx, Ny, Nz, omega, beta_g, T_ref, 0, 0.0, 0.0, 0.0, NULL, NULL,
+                NULL);
+}
+
+void or_collide_guo_3d(double *f, const uint8_t *solid, int Nx, int Ny, int Nz, double omega,
+                       double Fx, double Fy, double Fz) {
+    guo_3d_core(f, NULL, solid, Nx, Ny, Nz, omega, 0.0, 0.0, 1, Fx, Fy, Fz, NULL, NULL, NULL);
+}
+
+void or_collide_guo_field_3d(double *f, const uint8_t *solid, const double *Fxf,
+                             const double *Fyf, const double *Fzf, int Nx, int Ny, int Nz,
+                             double omega) {
+    guo_3d_core(f, NULL, solid, Nx, Ny, Nz, omega, 0.0, 0.0, 2, 0.0, 0.0, 0.0, Fxf, Fyf, Fzf);
+}
+
+static void guo_3d_core(double *f, const double *Temp, const uint8_t *solid, int Nx, int Ny,
+                        int Nz, double omega, double beta_g, double T_ref, int mode, double Fx,
+                        double Fy, double Fz, const double *Fxf, const double *Fyf,
+                        const double *Fzf) {
     for (int k = 0; k < Nz; ++k)
         for (int j = 0; j < Ny; ++j)
             for (int i = 0; i < Nx; ++i) {
@@ -1200,8 +1227,10 @@ void or_collide_boussinesq_3d(double *f, const double *Temp, const uint8_t *soli
                 if (solid && solid[N3(i, j, k)]) {
                     swap_pairs_3d(p);
                 } else {
-                    double fy = beta_g * (Temp[N3(i, j, k)] - T_ref);
-                    double fx = 0.0, fz = 0.0;
+                    size_t nn = N3(i, j, k);
+                    double fx = mode == 0 ? 0.0 : (mode == 1 ? Fx : Fxf[nn]);
+                    double fy = mode == 0 ? beta_g * (Temp[nn] - T_ref) : (mode == 1 ? Fy : Fyf[nn]);
+                    double fz = mode == 0 ? 0.0 : (mode == 1 ? Fz : Fzf[nn]);
                     double rho = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8] +
                                  p[9] + p[10] + p[11] + p[12] + p[13] + p[14] + p[15] + p[16] +
                                  p[17] + p[18];
@@ -1259,4 +1288,167 @@ void or_collide_boussinesq_3d(double *f, const double *Temp, const uint8_t *soli
                 }
                 for (int q = 0; q < 19; ++q) f[I3(i, j, k, q)] = p[q];
             }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Interpolated bounce-back: src/kernels/li_bb_2d_v2.jl, li_bb_3d_v2.jl     */
+/* ------------------------------------------------------------------------ */
+
+/* _libb_branch: src/kernels/li_bb_2d.jl:70-83 */
+static inline double libb_branch(double q_w, double f_here, double f_back, double f_bar_here,
+                                 double d) {
+    if (q_w <= 0.5) return 2.0 * q_w * f_here + (1.0 - 2.0 * q_w) * f_back + d;
+    double inv = 1.0 / (2.0 * q_w);
+    return inv * f_here + (1.0 - inv) * f_bar_here + d * inv;
+}
+
+/* fused_trt_libb_v2_step!: li_bb_2d_v2.jl:35-41 (PullHalfwayBB, SolidInert,
+ * ApplyLiBBPrePhase of dsl/bricks.jl:516-560, Moments, CollideTRTDirect,
+ * WriteMoments).  Rates are passed already rounded to the storage type. */
+void or_fused_trt_libb_2d(double *f_out, const double *f_in, double *rho_o, double *ux_o,
+                          double *uy_o, const uint8_t *solid, const double *qw,
+                          const double *uwx, const double *uwy, int Nx, int Ny, double sp,
+                          double sm) {
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            size_t n = N2(i, j);
+            if (solid && solid[n]) {
+                double feq[9];
+                feq2d_all(1.0, 0.0, 0.0, 0.0, feq);
+                for (int q = 0; q < 9; ++q) f_out[I2(i, j, q)] = feq[q];
+                if (rho_o) { rho_o[n] = 1.0; ux_o[n] = 0.0; uy_o[n] = 0.0; }
+                continue;
+            }
+            double p[9];
+            pull2d(f_in, Nx, Ny, i, j, p);
+#define QW(q) qw[I2(i, j, q)]
+#define FI(q) f_in[I2(i, j, q)]
+#define UX(q) uwx[I2(i, j, q)]
+#define UY(q) uwy[I2(i, j, q)]
+            /* reference q 2/4 (east/west), 3/5, 6/8, 7/9 */
+            if (QW(1) > 0.0) p[3] = libb_branch(QW(1), FI(1), p[1], FI(3), -(2.0 / 3.0) * UX(1));
+            if (QW(3) > 0.0) p[1] = libb_branch(QW(3), FI(3), p[3], FI(1), (2.0 / 3.0) * UX(3));
+            if (QW(2) > 0.0) p[4] = libb_branch(QW(2), FI(2), p[2], FI(4), -(2.0 / 3.0) * UY(2));
+            if (QW(4) > 0.0) p[2] = libb_branch(QW(4), FI(4), p[4], FI(2), (2.0 / 3.0) * UY(4));
+            if (QW(5) > 0.0)
+                p[7] = libb_branch(QW(5), FI(5), p[5], FI(7), -(1.0 / 6.0) * (UX(5) + UY(5)));
+            if (QW(7) > 0.0)
+                p[5] = libb_branch(QW(7), FI(7), p[7], FI(5), (1.0 / 6.0) * (UX(7) + UY(7)));
+            if (QW(6) > 0.0)
+                p[8] = libb_branch(QW(6), FI(6), p[6], FI(8), -(1.0 / 6.0) * (-UX(6) + UY(6)));
+            if (QW(8) > 0.0)
+                p[6] = libb_branch(QW(8), FI(8), p[8], FI(6), (1.0 / 6.0) * (-UX(8) + UY(8)));
+#undef QW
+#undef FI
+#undef UX
+#undef UY
+            double rho, ux, uy;
+            trt2d_node(p, sp, sm, &rho, &ux, &uy);
+            for (int q = 0; q < 9; ++q) f_out[I2(i, j, q)] = p[q];
+            if (rho_o) { rho_o[n] = rho; ux_o[n] = ux; uy_o[n] = uy; }
+        }
+}
+
+/* fused_trt_libb_v2_step_3d!: li_bb_3d_v2.jl:13-42, ApplyLiBBPrePhase_3D of
+ * dsl/bricks_3d.jl:367-475, with the periodic pull of or_fused_trt_3d. */
+void or_fused_trt_libb_3d(double *f_out, const double *f_in, double *rho_o, double *ux_o,
+                          double *uy_o, double *uz_o, const uint8_t *solid, const double *qw,
+                          const double *uwx, const double *uwy, const double *uwz, int Nx,
+                          int Ny, int Nz, double sp, double sm, int per_x, int per_y,
+                          int per_z) {
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                size_t n = N3(i, j, k);
+                double feq[19];
+                if (solid && solid[n]) {
+                    feq3d_all(1.0, 0.0, 0.0, 0.0, 0.0, feq);
+                    for (int q = 0; q < 19; ++q) f_out[I3(i, j, k, q)] = feq[q];
+                    if (rho_o) { rho_o[n] = 1.0; ux_o[n] = 0.0; uy_o[n] = 0.0; uz_o[n] = 0.0; }
+                    continue;
+                }
+                double p[19];
+                pull3d(f_in, Nx, Ny, Nz, i, j, k, per_x, per_y, per_z, p);
+#define QW(q) qw[I3(i, j, k, q)]
+#define FI(q) f_in[I3(i, j, k, q)]
+#define UX(q) uwx[I3(i, j, k, q)]
+#define UY(q) uwy[I3(i, j, k, q)]
+#define UZ(q) uwz[I3(i, j, k, q)]
+#define LINK(a, b, d) if (QW(a) > 0.0) p[b] = libb_branch(QW(a), FI(a), p[a], FI(b), d)
+                const double c3 = 1.0 / 3.0, c6 = 1.0 / 6.0;
+                LINK(1, 2, -c3 * UX(1));
+                LINK(2, 1, c3 * UX(2));
+                LINK(3, 4, -c3 * UY(3));
+                LINK(4, 3, c3 * UY(4));
+                LINK(5, 6, -c3 * UZ(5));
+                LINK(6, 5, c3 * UZ(6));
+                LINK(7, 10, -c6 * (UX(7) + UY(7)));
+                LINK(10, 7, c6 * (UX(10) + UY(10)));
+                LINK(8, 9, -c6 * (-UX(8) + UY(8)));
+                LINK(9, 8, -c6 * (UX(9) - UY(9)));
+                LINK(11, 14, -c6 * (UX(11) + UZ(11)));
+                LINK(14, 11, c6 * (UX(14) + UZ(14)));
+                LINK(12, 13, -c6 * (-UX(12) + UZ(12)));
+                LINK(13, 12, -c6 * (UX(13) - UZ(13)));
+                LINK(15, 18, -c6 * (UY(15) + UZ(15)));
+                LINK(18, 15, c6 * (UY(18) + UZ(18)));
+                LINK(16, 17, -c6 * (-UY(16) + UZ(16)));
+                LINK(17, 16, -c6 * (UY(17) - UZ(17)));
+#undef LINK
+#undef QW
+#undef FI
+#undef UX
+#undef UY
+#undef UZ
+                double rho, ux, uy, uz;
+                moments3d(p, &rho, &ux, &uy, &uz);
+                double usq = ux * ux + uy * uy + uz * uz;
+                feq3d_all(rho, ux, uy, uz, usq, feq);
+                double a = (sp + sm) * 0.5, b = (sp - sm) * 0.5;
+                static const int pa[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16};
+                static const int pb[9] = {2, 4, 6, 10, 9, 14, 13, 18, 17};
+                f_out[I3(i, j, k, 0)] = p[0] - sp * (p[0] - feq[0]);
+                for (int m = 0; m < 9; ++m) {
+                    int x = pa[m], y = pb[m];
+                    f_out[I3(i, j, k, x)] = p[x] - a * (p[x] - feq[x]) - b * (p[y] - feq[y]);
+                    f_out[I3(i, j, k, y)] = p[y] - a * (p[y] - feq[y]) - b * (p[x] - feq[x]);
+                }
+                if (rho_o) { rho_o[n] = rho; ux_o[n] = ux; uy_o[n] = uy; uz_o[n] = uz; }
+            }
+}
+
+/* collide_guo_2d! (src/kernels/collide_guo_2d.jl:5-81; Fxf == NULL: constant
+ * force) and collide_guo_field_2d! (:93-155, per-node force), population by
+ * population as the reference writes them. */
+void or_collide_guo_2d(double *f, const uint8_t *solid, const double *Fxf, const double *Fyf,
+                       int Nx, int Ny, double omega, double Fx, double Fy) {
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            double p[9];
+            size_t n = N2(i, j);
+            for (int q = 0; q < 9; ++q) p[q] = f[I2(i, j, q)];
+            if (solid && solid[n]) {
+                swap_pairs_2d(p);
+            } else {
+                double fx = Fxf ? Fxf[n] : Fx, fy = Fyf ? Fyf[n] : Fy;
+                double rho = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8];
+                double inv = 1.0 / rho;
+                double ux = ((p[1] - p[3] + p[5] - p[6] - p[7] + p[8]) + fx / 2.0) * inv;
+                double uy = ((p[2] - p[4] + p[5] + p[6] - p[7] - p[8]) + fy / 2.0) * inv;
+                double usq = ux * ux + uy * uy;
+                double gp = 1.0 - omega / 2.0, feq[9], S[9];
+                feq2d_all(rho, ux, uy, usq, feq);
+                S[0] = 4.0 / 9.0 * ((-ux) * fx + (-uy) * fy) * 3.0;
+                S[1] = 1.0 / 9.0 * ((1.0 - ux) * fx + (-uy) * fy) * 3.0 + 1.0 / 9.0 * (ux) * (fx) * 9.0;
+                S[2] = 1.0 / 9.0 * ((-ux) * fx + (1.0 - uy) * fy) * 3.0 + 1.0 / 9.0 * (uy) * (fy) * 9.0;
+                S[3] = 1.0 / 9.0 * ((-1.0 - ux) * fx + (-uy) * fy) * 3.0 + 1.0 / 9.0 * (-ux) * (-fx) * 9.0;
+                S[4] = 1.0 / 9.0 * ((-ux) * fx + (-1.0 - uy) * fy) * 3.0 + 1.0 / 9.0 * (-uy) * (-fy) * 9.0;
+                S[5] = 1.0 / 36.0 * ((1.0 - ux) * fx + (1.0 - uy) * fy) * 3.0 + 1.0 / 36.0 * (ux + uy) * (fx + fy) * 9.0;
+                S[6] = 1.0 / 36.0 * ((-1.0 - ux) * fx + (1.0 - uy) * fy) * 3.0 + 1.0 / 36.0 * (-ux + uy) * (-fx + fy) * 9.0;
+                S[7] = 1.0 / 36.0 * ((-1.0 - ux) * fx + (-1.0 - uy) * fy) * 3.0 + 1.0 / 36.0 * (-ux - uy) * (-fx - fy) * 9.0;
+                S[8] = 1.0 / 36.0 * ((1.0 - ux) * fx + (-1.0 - uy) * fy) * 3.0 + 1.0 / 36.0 * (ux - uy) * (fx - fy) * 9.0;
+                for (int q = 0; q < 9; ++q) p[q] = p[q] - omega * (p[q] - feq[q]) + gp * S[q];
+            }
+            for (int q = 0; q < 9; ++q) f[I2(i, j, q)] = p[q];
+        }
 }

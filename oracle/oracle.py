@@ -64,6 +64,12 @@ _SIG = {
     "or_fixed_temp_face_3d": ([_D, _i, _i, _i, _i, _d, _D, C.c_uint], None),
     "or_fixed_temp_3d": ([_D, _i, _i, _i, C.c_uint, _D], None),
     "or_collide_boussinesq_3d": ([_D, _D, _U8, _i, _i, _i, _d, _d, _d], None),
+    "or_collide_guo_2d": ([_D, _U8, _D, _D, _i, _i, _d, _d, _d], None),
+    "or_collide_guo_3d": ([_D, _U8, _i, _i, _i, _d, _d, _d, _d], None),
+    "or_collide_guo_field_3d": ([_D, _U8, _D, _D, _D, _i, _i, _i, _d], None),
+    "or_fused_trt_libb_2d": ([_D, _D, _D, _D, _D, _U8, _D, _D, _D, _i, _i, _d, _d], None),
+    "or_fused_trt_libb_3d": ([_D, _D, _D, _D, _D, _D, _U8, _D, _D, _D, _D, _i, _i, _i, _d, _d,
+                              _i, _i, _i], None),
     "or_residual": ([_D, _D, _D, _D, _D, _D, _U8, C.c_size_t, _i], _d),
     "or_max_threads": ([], _i),
     "or_set_threads": ([_i], None),
@@ -371,3 +377,39 @@ def fixed_temp_3d(g, **temps):
 def collide_boussinesq_3d(f, Temp, solid, omega, beta_g, T_ref):
     lib().or_collide_boussinesq_3d(_p(f), _p(Temp), _m(solid), *_n3(f), float(omega),
                                    float(beta_g), float(T_ref))
+
+
+def fused_trt_libb_2d(f_out, f_in, rho, ux, uy, solid, q_wall, uw_x, uw_y, sp, sm):
+    """fused_trt_libb_v2_step! with the rates already rounded to the storage type"""
+    lib().or_fused_trt_libb_2d(_p(f_out), _p(f_in), _p(rho), _p(ux), _p(uy), _m(solid),
+                               _p(q_wall), _p(uw_x), _p(uw_y), *_nxny(f_in), float(sp), float(sm))
+
+
+def fused_trt_libb_3d(f_out, f_in, moments, solid, q_wall, uw_x, uw_y, uw_z, sp, sm,
+                      periodic=(0, 0, 0)):
+    """fused_trt_libb_v2_step_3d!; moments = (rho, ux, uy, uz) arrays or None"""
+    m = moments if moments is not None else (None,) * 4
+    lib().or_fused_trt_libb_3d(_p(f_out), _p(f_in), *map(_p, m), _m(solid), _p(q_wall),
+                               _p(uw_x), _p(uw_y), _p(uw_z), *_n3(f_in), float(sp), float(sm),
+                               *[int(bool(x)) for x in periodic])
+
+
+def collide_guo_2d(f, solid, omega, Fx, Fy):
+    """collide_guo_2d!(f, is_solid, omega, Fx, Fy)"""
+    lib().or_collide_guo_2d(_p(f), _m(solid), None, None, *_nxny(f), float(omega), float(Fx),
+                            float(Fy))
+
+
+def collide_guo_field_2d(f, solid, Fx_field, Fy_field, omega):
+    lib().or_collide_guo_2d(_p(f), _m(solid), _p(Fx_field), _p(Fy_field), *_nxny(f),
+                            float(omega), 0.0, 0.0)
+
+
+def collide_guo_3d(f, solid, omega, Fx, Fy, Fz):
+    lib().or_collide_guo_3d(_p(f), _m(solid), *_n3(f), float(omega), float(Fx), float(Fy),
+                            float(Fz))
+
+
+def collide_guo_field_3d(f, solid, Fx_field, Fy_field, Fz_field, omega):
+    lib().or_collide_guo_field_3d(_p(f), _m(solid), _p(Fx_field), _p(Fy_field), _p(Fz_field),
+                                  *_n3(f), float(omega))
