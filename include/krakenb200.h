@@ -114,6 +114,11 @@ int kb_init_equilibrium_2d(void *f, const void *rho, const void *ux, const void 
 int kb_compute_macroscopic_2d(void *rho, void *ux, void *uy, const void *f, int Nx, int Ny,
                               int dtype, void *stream);
 
+/* compute_macroscopic_forced_2d!(rho, ux, uy, f, Fx, Fy)
+ *   -- src/kernels/macroscopic.jl:84-118: u = (sum c f + F/2) / rho */
+int kb_compute_macroscopic_forced_2d(void *rho, void *ux, void *uy, const void *f, int Nx, int Ny,
+                                     double Fx, double Fy, int dtype, void *stream);
+
 /* fused_bgk_step!(f_out, f_in, rho, ux, uy, is_solid, Nx, Ny, omega)
  *   -- src/kernels/fused_bgk_2d.jl:67 */
 int kb_fused_bgk_step(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
@@ -313,6 +318,25 @@ int kb_apply_zou_he_pressure_3d(void *f, int Nx, int Ny, int Nz, int face, doubl
 /* compute_macroscopic_3d!(rho, ux, uy, uz, f) -- src/kernels/macroscopic.jl:75 */
 int kb_compute_macroscopic_3d(void *rho, void *ux, void *uy, void *uz, const void *f, int Nx,
                               int Ny, int Nz, int dtype, void *stream);
+
+/* compute_macroscopic_forced_3d!(rho, ux, uy, uz, f, Fx, Fy, Fz)
+ *   -- src/kernels/macroscopic.jl:121-160 */
+int kb_compute_macroscopic_forced_3d(void *rho, void *ux, void *uy, void *uz, const void *f,
+                                     int Nx, int Ny, int Nz, double Fx, double Fy, double Fz,
+                                     int dtype, void *stream);
+
+/* compute_macroscopic_forced_field_3d!(rho, ux, uy, uz, f, Fx, Fy, Fz) with
+ * per-node force fields -- src/kernels/macroscopic.jl:164-200 */
+int kb_compute_macroscopic_forced_field_3d(void *rho, void *ux, void *uy, void *uz, const void *f,
+                                           const void *Fx_field, const void *Fy_field,
+                                           const void *Fz_field, int Nx, int Ny, int Nz,
+                                           int dtype, void *stream);
+
+/* stream_periodic_xz_wall_y_3d!(f_out, f_in, Nx, Ny, Nz)
+ *   -- src/kernels/stream_periodic_3d.jl:24-92: x and z wrap, half-way
+ * bounce-back on the y faces */
+int kb_stream_periodic_xz_wall_y_3d(void *f_out, const void *f_in, int Nx, int Ny, int Nz,
+                                    int dtype, void *stream);
 
 /* Unfused thermal DDF in 3D (run_natural_convection_3d,
  * src/drivers/thermal.jl:455-537).  Fields have the population's type. */

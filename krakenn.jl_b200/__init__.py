@@ -10,7 +10,8 @@ from . import _lib, batch, drivers, krk, lattice, libb, ops, sharding, surrogate
 from ._lib import KrakenArgumentError, KrakenError, version  # noqa: F401
 from .drivers import (LBMConfig, initialize_2d, initialize_3d, omega, reynolds,  # noqa: F401
                       run_cavity_2d, run_cavity_3d, run_natural_convection_2d,
-                      run_natural_convection_3d, run_rayleigh_benard_2d,
+                      run_couette_2d, run_natural_convection_3d, run_poiseuille_2d,
+                      run_rayleigh_benard_2d,
                       run_taylor_green_2d, run_taylor_green_3d)
 from .batch import CavityBatch, Graph, sweep_cases  # noqa: F401
 from .ops import *  # noqa: F401,F403

@@ -932,6 +932,24 @@ __global__ void __launch_bounds__(BX) boussinesq_k(T *__restrict__ f, const T *_
     for (int q = 0; q < 9; ++q) f[c + q * P] = p[q];
 }
 
+// compute_macroscopic_forced_2d_kernel! (src/kernels/macroscopic.jl:84-99):
+// the velocity carries the half-force correction (sum c f + F/2) / rho.
+template <typename T>
+__global__ void __launch_bounds__(BX) macroscopic_forced_k(T *__restrict__ rho, T *__restrict__ ux,
+                                                            T *__restrict__ uy,
+                                                            const T *__restrict__ f, Grid2<T> g,
+                                                            T Fx, T Fy) {
+    NODE2
+    T p[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p[q] = f[c + q * P];
+    const T r = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8];
+    const T inv = T(1) / r;
+    rho[c] = r;
+    ux[c] = ((p[1] - p[3] + p[5] - p[6] - p[7] + p[8]) + Fx / T(2)) * inv;
+    uy[c] = ((p[2] - p[4] + p[5] + p[6] - p[7] - p[8]) + Fy / T(2)) * inv;
+}
+
 // collide_guo_2d_kernel! (src/kernels/collide_guo_2d.jl:5-81; FIELD false,
 // constant force) and collide_guo_field_2d_kernel! (:93-155; FIELD true,
 // per-node force).  Solid nodes swap opposite pairs.
@@ -1484,6 +1502,19 @@ int kb_collide_guo_field_2d(void *f, const uint8_t *is_solid, const void *Fx_fie
         (guo_k<T, true><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
             (T *)f, is_solid, (const T *)Fx_field, (const T *)Fy_field, grid2<T>(Nx, Ny),
             (T)omega, T(0), T(0))));
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int kb_compute_macroscopic_forced_2d(void *rho, void *ux, void *uy, const void *f, int Nx, int Ny,
+                                     double Fx, double Fy, int dtype, void *stream) {
+    KB_REQUIRE(rho && ux && uy && f, "kb_compute_macroscopic_forced_2d: null pointer");
+    if (int e = check_dims("kb_compute_macroscopic_forced_2d", Nx, Ny)) return e;
+    KB_DISPATCH_PLAIN("kb_compute_macroscopic_forced_2d", dtype,
+        (macroscopic_forced_k<T><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
+            (T *)rho, (T *)ux, (T *)uy, (const T *)f, grid2<T>(Nx, Ny), (T)Fx, (T)Fy)));
 }
 
 }  // extern "C"

@@ -117,6 +117,32 @@ __global__ void __launch_bounds__(BX) macroscopic_k(T *__restrict__ rho, T *__re
     rho[c] = r; ux[c] = a; uy[c] = b; uz[c] = d;
 }
 
+// compute_macroscopic_forced_3d_kernel! (src/kernels/macroscopic.jl:121-141;
+// FIELD false, constant force) and compute_macroscopic_forced_field_3d_kernel!
+// (:164-192; FIELD true, per-node force).
+template <typename T, bool FIELD>
+__global__ void __launch_bounds__(BX) macroscopic_forced_k(T *__restrict__ rho, T *__restrict__ ux,
+                                                            T *__restrict__ uy, T *__restrict__ uz,
+                                                            const T *__restrict__ f, Grid3 g,
+                                                            T Fx, T Fy, T Fz,
+                                                            const T *__restrict__ Fxf,
+                                                            const T *__restrict__ Fyf,
+                                                            const T *__restrict__ Fzf) {
+    NODE3
+    T p[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) p[q] = f[c + q * P];
+    T r = p[0];
+#pragma unroll
+    for (int q = 1; q < 19; ++q) r = r + p[q];
+    const T inv = T(1) / r;
+    const T fx = FIELD ? Fxf[c] : Fx, fy = FIELD ? Fyf[c] : Fy, fz = FIELD ? Fzf[c] : Fz;
+    rho[c] = r;
+    ux[c] = ((p[1] - p[2] + p[7] - p[8] + p[9] - p[10] + p[11] - p[12] + p[13] - p[14]) + fx / T(2)) * inv;
+    uy[c] = ((p[3] - p[4] + p[7] + p[8] - p[9] - p[10] + p[15] - p[16] + p[17] - p[18]) + fy / T(2)) * inv;
+    uz[c] = ((p[5] - p[6] + p[11] + p[12] - p[13] - p[14] + p[15] + p[16] - p[17] - p[18]) + fz / T(2)) * inv;
+}
+
 // Fused TRT step with the reference arithmetic (PullHalfwayBB_3D +
 // SolidInert_3D + Moments_3D + CollideTRTDirect_3D + WriteMoments_3D,
 // src/kernels/dsl/bricks_3d.jl:64-230, 476-483).  I: element-offset type.
@@ -1113,6 +1139,45 @@ int kb_fused_trt_libb_links_step_3d(void *f_out, const void *f_in, void *rho, vo
                                               (float)sm, s);
     }
     return kb::set_error(KB_ERR_UNSUPPORTED, "%s: unknown dtype %d", what, dtype);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int kb_compute_macroscopic_forced_3d(void *rho, void *ux, void *uy, void *uz, const void *f,
+                                     int Nx, int Ny, int Nz, double Fx, double Fy, double Fz,
+                                     int dtype, void *stream) {
+    KB_REQUIRE(rho && ux && uy && uz && f, "kb_compute_macroscopic_forced_3d: null pointer");
+    if (int e = check_dims("kb_compute_macroscopic_forced_3d", Nx, Ny, Nz)) return e;
+    KB3_DISPATCH_PLAIN("kb_compute_macroscopic_forced_3d", dtype,
+        (macroscopic_forced_k<T, false><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
+            (T *)rho, (T *)ux, (T *)uy, (T *)uz, (const T *)f, grid3(Nx, Ny, Nz), (T)Fx, (T)Fy,
+            (T)Fz, nullptr, nullptr, nullptr)));
+}
+
+int kb_compute_macroscopic_forced_field_3d(void *rho, void *ux, void *uy, void *uz, const void *f,
+                                           const void *Fx_field, const void *Fy_field,
+                                           const void *Fz_field, int Nx, int Ny, int Nz,
+                                           int dtype, void *stream) {
+    KB_REQUIRE(rho && ux && uy && uz && f && Fx_field && Fy_field && Fz_field,
+               "kb_compute_macroscopic_forced_field_3d: null pointer");
+    if (int e = check_dims("kb_compute_macroscopic_forced_field_3d", Nx, Ny, Nz)) return e;
+    KB3_DISPATCH_PLAIN("kb_compute_macroscopic_forced_field_3d", dtype,
+        (macroscopic_forced_k<T, true><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
+            (T *)rho, (T *)ux, (T *)uy, (T *)uz, (const T *)f, grid3(Nx, Ny, Nz), T(0), T(0),
+            T(0), (const T *)Fx_field, (const T *)Fy_field, (const T *)Fz_field)));
+}
+
+int kb_stream_periodic_xz_wall_y_3d(void *f_out, const void *f_in, int Nx, int Ny, int Nz,
+                                    int dtype, void *stream) {
+    KB_REQUIRE(f_out && f_in, "kb_stream_periodic_xz_wall_y_3d: null population pointer");
+    KB_REQUIRE(f_out != f_in, "kb_stream_periodic_xz_wall_y_3d: f_out and f_in must differ");
+    if (int e = check_dims("kb_stream_periodic_xz_wall_y_3d", Nx, Ny, Nz)) return e;
+    // the pull of stream_3d with x and z wrapped (periodic mask x | z)
+    KB3_DISPATCH_PLAIN("kb_stream_periodic_xz_wall_y_3d", dtype,
+        (stream_k<T><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
+            (T *)f_out, (const T *)f_in, grid3(Nx, Ny, Nz, 5))));
 }
 
 }  // extern "C"

@@ -149,6 +149,50 @@ def run_cavity_3d(config: LBMConfig, backend="b200", T=torch.float64):
                 uy=st["uy"].cpu().numpy(), uz=st["uz"].cpu().numpy(), config=config)
 
 
+def run_poiseuille_2d(Nx=4, Ny=32, nu=0.1, Fx=1e-5, max_steps=10000, backend="b200",
+                      T=torch.float64, graph=True):
+    """run_poiseuille_2d -- src/drivers/basic.jl:185-203: periodic x, half-way
+    bounce-back walls in y, Guo body force Fx."""
+    _require_backend(backend)
+    cfg = LBMConfig.d2q9(Nx, Ny, nu, 0.0, max_steps)
+    st = initialize_2d(cfg, T)
+    f = [st["f_in"], st["f_out"]]
+    w = omega(cfg)
+
+    def step(par):
+        fi, fo = f[par], f[1 - par]
+        ops.stream_periodic_x_wall_y_2d_(fo, fi, Nx, Ny)
+        ops.collide_guo_2d_(fo, st["is_solid"], w, Fx, 0.0)
+        ops.compute_macroscopic_2d_(st["rho"], st["ux"], st["uy"], fo)
+
+    _step_loop(step, max_steps, graph)
+    return dict(rho=st["rho"].cpu().numpy(), ux=st["ux"].cpu().numpy(),
+                uy=st["uy"].cpu().numpy(), f=f[max_steps & 1], config=cfg)
+
+
+def run_couette_2d(Nx=4, Ny=32, nu=0.1, u_wall=0.05, max_steps=10000, backend="b200",
+                   T=torch.float64, graph=True):
+    """run_couette_2d -- src/drivers/basic.jl:213-234: periodic x, Zou-He south
+    wall moving at u_wall, resting Zou-He north wall, BGK."""
+    _require_backend(backend)
+    cfg = LBMConfig.d2q9(Nx, Ny, nu, 0.0, max_steps)
+    st = initialize_2d(cfg, T)
+    f = [st["f_in"], st["f_out"]]
+    w = omega(cfg)
+
+    def step(par):
+        fi, fo = f[par], f[1 - par]
+        ops.stream_periodic_x_wall_y_2d_(fo, fi, Nx, Ny)
+        ops.apply_zou_he_south_2d_(fo, u_wall, Nx)
+        ops.apply_zou_he_north_2d_(fo, 0.0, Nx, Ny)
+        ops.collide_2d_(fo, st["is_solid"], w)
+        ops.compute_macroscopic_2d_(st["rho"], st["ux"], st["uy"], fo)
+
+    _step_loop(step, max_steps, graph)
+    return dict(rho=st["rho"].cpu().numpy(), ux=st["ux"].cpu().numpy(),
+                uy=st["uy"].cpu().numpy(), f=f[max_steps & 1], config=cfg)
+
+
 def taylor_green_2d_populations(N, u0):
     """Host FP64 populations of initialize_taylor_green_2d
     (src/drivers/basic.jl:242-273), shape (9, N, N)."""

@@ -232,6 +232,15 @@ def fused_trt_step_(f_out, f_in, rho, ux, uy, is_solid, Nx, Ny, nu, Lambda=3 / 1
          _stream())
 
 
+def compute_macroscopic_forced_2d_(rho, ux, uy, f, Fx, Fy):
+    """compute_macroscopic_forced_2d! -- src/kernels/macroscopic.jl:112"""
+    code = _plain(f)
+    Nx, Ny = _dims2(f)
+    _ptrs_2d_fields(code, Nx, Ny, rho=rho, ux=ux, uy=uy)
+    call("kb_compute_macroscopic_forced_2d", _t(rho, "rho"), _t(ux, "ux"), _t(uy, "uy"),
+         _t(f, "f"), Nx, Ny, float(Fx), float(Fy), code, _stream())
+
+
 def collide_guo_2d_(f, is_solid, omega, Fx, Fy):
     """collide_guo_2d! -- src/kernels/collide_guo_2d.jl:84"""
     code = _plain(f)
@@ -620,6 +629,31 @@ def apply_fixed_temp_3d_(g, Nx, Ny, Nz, west=None, east=None, south=None, north=
     mask, T = _face_temps(dict(west=west, east=east, south=south, north=north, bottom=bottom,
                                top=top), list(FACES_3D))
     call("kb_apply_fixed_temp_3d", _t(g, "g"), Nx, Ny, Nz, mask, T, code, _stream())
+
+
+def compute_macroscopic_forced_3d_(rho, ux, uy, uz, f, Fx, Fy, Fz):
+    """compute_macroscopic_forced_3d! (src/kernels/macroscopic.jl:155); tensors
+    Fx, Fy, Fz select compute_macroscopic_forced_field_3d! (:195)"""
+    import torch as _torch
+    code = _plain(f)
+    Nx, Ny, Nz = _dims3(f)
+    _ptrs_3d_fields(code, Nx, Ny, Nz, rho=rho, ux=ux, uy=uy, uz=uz)
+    if isinstance(Fx, _torch.Tensor):
+        _ptrs_3d_fields(code, Nx, Ny, Nz, Fx=Fx, Fy=Fy, Fz=Fz)
+        call("kb_compute_macroscopic_forced_field_3d", _t(rho, "rho"), _t(ux, "ux"), _t(uy, "uy"),
+             _t(uz, "uz"), _t(f, "f"), _t(Fx, "Fx"), _t(Fy, "Fy"), _t(Fz, "Fz"), Nx, Ny, Nz,
+             code, _stream())
+    else:
+        call("kb_compute_macroscopic_forced_3d", _t(rho, "rho"), _t(ux, "ux"), _t(uy, "uy"),
+             _t(uz, "uz"), _t(f, "f"), Nx, Ny, Nz, float(Fx), float(Fy), float(Fz), code,
+             _stream())
+
+
+def stream_periodic_xz_wall_y_3d_(f_out, f_in, Nx, Ny, Nz):
+    """stream_periodic_xz_wall_y_3d! -- src/kernels/stream_periodic_3d.jl:88"""
+    code = _plain(f_in); _match3(f_in, Nx, Ny, Nz); _match3(f_out, Nx, Ny, Nz)
+    call("kb_stream_periodic_xz_wall_y_3d", _t(f_out, "f_out"), _t(f_in, "f_in"), Nx, Ny, Nz,
+         code, _stream())
 
 
 def collide_guo_3d_(f, is_solid, omega, Fx, Fy, Fz):

@@ -1452,3 +1452,54 @@ void or_collide_guo_2d(double *f, const uint8_t *solid, const double *Fxf, const
             for (int q = 0; q < 9; ++q) f[I2(i, j, q)] = p[q];
         }
 }
+
+/* compute_macroscopic_forced_2d!: src/kernels/macroscopic.jl:84-99 */
+void or_macroscopic_forced_2d(double *rho, double *ux, double *uy, const double *f, int Nx, int Ny,
+                              double Fx, double Fy) {
+    for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+            const double *p[9];
+            for (int q = 0; q < 9; ++q) p[q] = &f[I2(i, j, q)];
+            double r = *p[0] + *p[1] + *p[2] + *p[3] + *p[4] + *p[5] + *p[6] + *p[7] + *p[8];
+            double inv = 1.0 / r;
+            rho[N2(i, j)] = r;
+            ux[N2(i, j)] = ((*p[1] - *p[3] + *p[5] - *p[6] - *p[7] + *p[8]) + Fx / 2.0) * inv;
+            uy[N2(i, j)] = ((*p[2] - *p[4] + *p[5] + *p[6] - *p[7] - *p[8]) + Fy / 2.0) * inv;
+        }
+}
+
+/* compute_macroscopic_forced_3d! / _field_3d!: src/kernels/macroscopic.jl:121-192
+ * (Fxf == NULL: constant force). */
+void or_macroscopic_forced_3d(double *rho, double *ux, double *uy, double *uz, const double *f,
+                              int Nx, int Ny, int Nz, double Fx, double Fy, double Fz,
+                              const double *Fxf, const double *Fyf, const double *Fzf) {
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                double p[19];
+                size_t n = N3(i, j, k);
+                for (int q = 0; q < 19; ++q) p[q] = f[I3(i, j, k, q)];
+                double r = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8] + p[9] +
+                           p[10] + p[11] + p[12] + p[13] + p[14] + p[15] + p[16] + p[17] + p[18];
+                double inv = 1.0 / r;
+                double fx = Fxf ? Fxf[n] : Fx, fy = Fyf ? Fyf[n] : Fy, fz = Fzf ? Fzf[n] : Fz;
+                rho[n] = r;
+                ux[n] = ((p[1] - p[2] + p[7] - p[8] + p[9] - p[10] + p[11] - p[12] + p[13] - p[14]) + fx / 2.0) * inv;
+                uy[n] = ((p[3] - p[4] + p[7] + p[8] - p[9] - p[10] + p[15] - p[16] + p[17] - p[18]) + fy / 2.0) * inv;
+                uz[n] = ((p[5] - p[6] + p[11] + p[12] - p[13] - p[14] + p[15] + p[16] - p[17] - p[18]) + fz / 2.0) * inv;
+            }
+}
+
+/* stream_periodic_xz_wall_y_3d!: src/kernels/stream_periodic_3d.jl:24-84 (pull
+ * with x and z wrapped, half-way bounce-back at the y faces); the general
+ * per-axis form. */
+void or_stream_periodic_3d(double *f_out, const double *f_in, int Nx, int Ny, int Nz, int px,
+                           int py, int pz) {
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                double fp[19];
+                pull3d(f_in, Nx, Ny, Nz, i, j, k, px, py, pz, fp);
+                for (int q = 0; q < 19; ++q) f_out[I3(i, j, k, q)] = fp[q];
+            }
+}

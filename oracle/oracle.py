@@ -64,6 +64,9 @@ _SIG = {
     "or_fixed_temp_face_3d": ([_D, _i, _i, _i, _i, _d, _D, C.c_uint], None),
     "or_fixed_temp_3d": ([_D, _i, _i, _i, C.c_uint, _D], None),
     "or_collide_boussinesq_3d": ([_D, _D, _U8, _i, _i, _i, _d, _d, _d], None),
+    "or_macroscopic_forced_2d": ([_D, _D, _D, _D, _i, _i, _d, _d], None),
+    "or_macroscopic_forced_3d": ([_D, _D, _D, _D, _D, _i, _i, _i, _d, _d, _d, _D, _D, _D], None),
+    "or_stream_periodic_3d": ([_D, _D, _i, _i, _i, _i, _i, _i], None),
     "or_collide_guo_2d": ([_D, _U8, _D, _D, _i, _i, _d, _d, _d], None),
     "or_collide_guo_3d": ([_D, _U8, _i, _i, _i, _d, _d, _d, _d], None),
     "or_collide_guo_field_3d": ([_D, _U8, _D, _D, _D, _i, _i, _i, _d], None),
@@ -413,3 +416,27 @@ def collide_guo_3d(f, solid, omega, Fx, Fy, Fz):
 def collide_guo_field_3d(f, solid, Fx_field, Fy_field, Fz_field, omega):
     lib().or_collide_guo_field_3d(_p(f), _m(solid), _p(Fx_field), _p(Fy_field), _p(Fz_field),
                                   *_n3(f), float(omega))
+
+
+def macroscopic_forced_2d(f, Fx, Fy):
+    Nx, Ny = _nxny(f)
+    rho, ux, uy = (np.empty((Ny, Nx)) for _ in range(3))
+    lib().or_macroscopic_forced_2d(_p(rho), _p(ux), _p(uy), _p(f), Nx, Ny, float(Fx), float(Fy))
+    return rho, ux, uy
+
+
+def macroscopic_forced_3d(f, Fx, Fy, Fz):
+    """Fx, Fy, Fz scalars or per-node arrays (compute_macroscopic_forced_field_3d!)"""
+    Nx, Ny, Nz = _n3(f)
+    out = [np.empty((Nz, Ny, Nx)) for _ in range(4)]
+    if isinstance(Fx, np.ndarray):
+        lib().or_macroscopic_forced_3d(*map(_p, out), _p(f), Nx, Ny, Nz, 0.0, 0.0, 0.0, _p(Fx),
+                                       _p(Fy), _p(Fz))
+    else:
+        lib().or_macroscopic_forced_3d(*map(_p, out), _p(f), Nx, Ny, Nz, float(Fx), float(Fy),
+                                       float(Fz), None, None, None)
+    return tuple(out)
+
+
+def stream_periodic_xz_wall_y_3d(f_out, f_in):
+    lib().or_stream_periodic_3d(_p(f_out), _p(f_in), *_n3(f_in), 1, 0, 1)
