@@ -897,8 +897,9 @@ def run_other(args):
         if rank == 0:
             r = bench_cavity2d(pkg, steps=max(args.steps, 200) // 200 * 200)
     elif args.workload == "batch":
-        r = bench_batch(pkg, rank=rank, world=world, error_cases=8 if world == 1 else 0,
-                        storage=args.batch_storage)
+        r = bench_batch(pkg, n_cases=args.cases, max_steps=args.max_steps, rank=rank,
+                        world=world, error_cases=(8 if world == 1 and args.cases == 256 else 0),
+                        storage=args.batch_storage, autotune=not args.no_autotune)
     elif args.workload == "warmstart":
         if rank == 0:
             r = bench_warmstart(pkg)
@@ -907,7 +908,8 @@ def run_other(args):
             r = bench_surrogate(pkg, steps=min(args.steps, 50), warmup=args.warmup)
     elif args.workload == "libb":
         if rank == 0:
-            r = bench_libb(pkg, steps=min(max(args.steps, 20), 200), warmup=args.warmup)
+            r = bench_libb(pkg, N=args.grid, R=40.0 * args.grid / 256,
+                           steps=min(max(args.steps, 20), 200), warmup=args.warmup)
     elif rank == 0:
         r = bench_natconv_validation(pkg)
     if rank == 0:
@@ -932,6 +934,11 @@ def main():
                     help="deviation-storage TRT kernel: 0 automatic, 1 node, 2 x/x+32 pairs, "
                          "3 vector pairs, 4 16-bit quads")
     ap.add_argument("--grid", type=int, default=N_GRID)
+    ap.add_argument("--cases", type=int, default=256, help="--workload batch: number of cavities")
+    ap.add_argument("--max-steps", type=int, default=50000,
+                    help="--workload batch: step cap per cavity")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="--workload batch: skip the schedule autotuner")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
