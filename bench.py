@@ -878,6 +878,63 @@ def bench_libb(pkg, N=256, R=40.0, steps=50, warmup=5):
     return out
 
 
+def bench_output(pkg, n=256, steps=400, every=20):
+    """Cost of field output in a step loop: the periodic D3Q19 TRT Taylor-Green
+    step (n^3, F32 f-w) with rho, ux, uy, uz written every `every` steps and
+    copied to the host (a) not at all, (b) synchronously (the reference's
+    Array() per snapshot), (c) through the asynchronous snapshot pipeline
+    (staging copy, device-to-host on a copy stream, host sink on a thread).
+    Wall-clock ms per step, host synchronised at both ends."""
+    import time
+    import torch
+    plane = torch.from_numpy(pkg.drivers.taylor_green_3d_populations(n, U0, Nz=1)).cuda()
+    f = torch.empty((19, n, n, n), dtype=torch.float32, device="cuda")
+    full = _extrude(plane, n)
+    pkg.convert_populations(f, full, dst_deviation=True)
+    del full
+    g = torch.empty_like(f)
+    mom = [torch.empty((n, n, n), dtype=torch.float32, device="cuda") for _ in range(4)]
+    got = []
+    snaps = pkg.output.AsyncSnapshots(lambda s, t, fl: got.append(s), depth=3)
+
+    def run(mode):
+        nonlocal f, g
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for s in range(steps):
+            out = (s + 1) % every == 0
+            m = mom if out else [None] * 4
+            pkg.fused_trt_step_3d_(g, f, *m, None, n, n, n, NU, 0.25, periodic=(1, 1, 1),
+                                   deviation=True)
+            f, g = g, f
+            if out and mode == "sync":
+                [t.cpu() for t in mom]
+            elif out and mode == "async":
+                snaps.submit(s + 1, {"rho": mom[0], "velocity": tuple(mom[1:])})
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        return (t1 - t0) * 1e3 / steps
+
+    run("none")
+    run("async")   # allocates the pinned ring once; the timed runs reuse it
+    res = {m: round(run(m), 4) for m in ("none", "sync", "async", "none")}
+    snaps.close()
+    snap_mb = 4 * n ** 3 * 4 / 1e6
+    host = torch.empty(mom[0].shape, dtype=torch.float32, pin_memory=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(10):
+        host.copy_(mom[0], non_blocking=True)
+    torch.cuda.synchronize()
+    d2h = 10 * mom[0].numel() * 4 / (time.perf_counter() - t0) / 1e9
+    return {"workload": f"D3Q19 TRT Taylor-Green {n}^3 f32dev, rho/u ({snap_mb:.0f} MB) every "
+                        f"{every} of {steps} steps", "ms_per_step": res,
+            "pinned_d2h_gbs": round(d2h, 1),
+            "async_snapshots_delivered": len(got),
+            "sync_overhead_ms_per_snapshot": round((res["sync"] - res["none"]) * every, 3),
+            "async_overhead_ms_per_snapshot": round((res["async"] - res["none"]) * every, 3)}
+
+
 def _extrude(plane, n):
     import torch
     out = torch.empty((19, n, n, n), dtype=plane.dtype, device=plane.device)
@@ -906,6 +963,9 @@ def run_other(args):
     elif args.workload == "surrogate":
         if rank == 0:
             r = bench_surrogate(pkg, steps=min(args.steps, 50), warmup=args.warmup)
+    elif args.workload == "output":
+        if rank == 0:
+            r = bench_output(pkg, n=args.grid)
     elif args.workload == "libb":
         if rank == 0:
             r = bench_libb(pkg, N=args.grid, R=40.0 * args.grid / 256,
@@ -944,7 +1004,7 @@ def main():
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the short measurements of the other configurations")
     ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "cavity2d", "batch", "natconv", "warmstart", "surrogate",
-                             "libb"])
+                             "libb", "output"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

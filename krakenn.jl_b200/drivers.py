@@ -99,7 +99,7 @@ def initialize_3d(config: LBMConfig, T=torch.float64, device=None):
 
 
 def run_cavity_2d(config: LBMConfig, backend="b200", T=torch.float64, fused=True, state=None,
-                  lid="zou_he"):
+                  lid="zou_he", on_step=None):
     """run_cavity_2d -- src/drivers/basic.jl:112-144.
 
     lid="zou_he" (the reference driver): fused=False issues the reference's
@@ -107,7 +107,9 @@ def run_cavity_2d(config: LBMConfig, backend="b200", T=torch.float64, fused=True
     compute_macroscopic_2d!); fused=True issues the single-launch
     kb_cavity_step_2d, which gives the same bits.
     lid="moving_wall": half-way bounce-back on all four walls with the
-    moving-wall link rule on the lid (kb_cavity_movingwall_step_2d)."""
+    moving-wall link rule on the lid (kb_cavity_movingwall_step_2d).
+    on_step(step, fields): called after every step with the device moment
+    fields (for example an output.StepOutput)."""
     _require_backend(backend)
     if lid not in ("zou_he", "moving_wall"):
         raise ValueError(f"unknown lid '{lid}'")
@@ -116,7 +118,7 @@ def run_cavity_2d(config: LBMConfig, backend="b200", T=torch.float64, fused=True
     rho, ux, uy, solid = st["rho"], st["ux"], st["uy"], st["is_solid"]
     Nx, Ny = config.Nx, config.Ny
     w = omega(config)
-    for _ in range(config.max_steps):
+    for step in range(config.max_steps):
         if lid == "moving_wall":
             ops.cavity_movingwall_step_2d_(f_out, f_in, rho, ux, uy, solid, Nx, Ny, w, config.u_lid)
         elif fused:
@@ -127,24 +129,28 @@ def run_cavity_2d(config: LBMConfig, backend="b200", T=torch.float64, fused=True
             ops.collide_2d_(f_out, solid, w)
             ops.compute_macroscopic_2d_(rho, ux, uy, f_out)
         f_in, f_out = f_out, f_in
+        if on_step is not None:
+            on_step(step + 1, {"rho": rho, "velocity": (ux, uy)})
     st["f_in"], st["f_out"] = f_in, f_out
     return dict(rho=rho.cpu().numpy(), ux=ux.cpu().numpy(), uy=uy.cpu().numpy(), config=config,
                 state=st)
 
 
-def run_cavity_3d(config: LBMConfig, backend="b200", T=torch.float64):
-    """run_cavity_3d -- src/drivers/basic.jl:153-176"""
+def run_cavity_3d(config: LBMConfig, backend="b200", T=torch.float64, on_step=None):
+    """run_cavity_3d -- src/drivers/basic.jl:153-176 (on_step as run_cavity_2d)"""
     _require_backend(backend)
     st = initialize_3d(config, T)
     f_in, f_out = st["f_in"], st["f_out"]
     Nx, Ny, Nz = config.Nx, config.Ny, config.Nz
     w = omega(config)
-    for _ in range(config.max_steps):
+    for step in range(config.max_steps):
         ops.stream_3d_(f_out, f_in, Nx, Ny, Nz)
         ops.apply_zou_he_top_3d_(f_out, config.u_lid, Nx, Ny, Nz)
         ops.collide_3d_(f_out, st["is_solid"], w)
         ops.compute_macroscopic_3d_(st["rho"], st["ux"], st["uy"], st["uz"], f_out)
         f_in, f_out = f_out, f_in
+        if on_step is not None:
+            on_step(step + 1, {"rho": st["rho"], "velocity": (st["ux"], st["uy"], st["uz"])})
     return dict(rho=st["rho"].cpu().numpy(), ux=st["ux"].cpu().numpy(),
                 uy=st["uy"].cpu().numpy(), uz=st["uz"].cpu().numpy(), config=config)
 

@@ -245,9 +245,13 @@ def resolve_backend(setup: SimulationSetup, backend: str | None) -> str:
 
 
 def run_simulation(setup_or_path, backend: str | None = None, max_steps: int | None = None,
-                   T=None, **kwargs):
+                   T=None, output_dir=None, vtk_every=0, callback=None, callback_every=100,
+                   **kwargs):
     """run_simulation -- src/simulation_runner.jl:62-73, 235-443 (dispatch to
-    the driver whose stream-collide path this package implements)."""
+    the driver whose stream-collide path this package implements).  For the
+    cavity drivers, output_dir + vtk_every write VTK snapshots and a .pvd, and
+    callback(step, fields) runs every callback_every steps (:414-426); both
+    run asynchronously (output.StepOutput)."""
     import torch
 
     from . import drivers
@@ -273,14 +277,34 @@ def run_simulation(setup_or_path, backend: str | None = None, max_steps: int | N
                                                      for s in ("south", "east", "west")):
             u = setup.boundaries["north"][1].get("ux", 0.1)
             cfg = drivers.LBMConfig.d2q9(Nx, Ny, setup.nu, u, steps)
-            return drivers.run_cavity_2d(cfg, T=T)
+            hook = _output_hook(setup, Nx, Ny, None, output_dir, vtk_every, callback,
+                                callback_every)
+            try:
+                return drivers.run_cavity_2d(cfg, T=T, on_step=hook)
+            finally:
+                if hook is not None:
+                    hook.close()
     if setup.lattice == "D3Q19":
         if kinds.get("top") == "velocity":
             u = setup.boundaries["top"][1].get("ux", 0.1)
             cfg = drivers.LBMConfig.d3q19(*setup.N, setup.nu, u, steps)
-            return drivers.run_cavity_3d(cfg, T=T)
+            hook = _output_hook(setup, *setup.N, output_dir, vtk_every, callback, callback_every)
+            try:
+                return drivers.run_cavity_3d(cfg, T=T, on_step=hook)
+            finally:
+                if hook is not None:
+                    hook.close()
     raise ValueError(f"setup '{setup.name}' ({setup.lattice}, boundaries {kinds}) is not on the "
                      "b200 stream-collide path")
+
+
+def _output_hook(setup, Nx, Ny, Nz, output_dir, vtk_every, callback, callback_every):
+    if (output_dir is None or not vtk_every) and callback is None:
+        return None
+    from .output import StepOutput
+    dx = setup.L[0] / Nx if setup.L and setup.L[0] else 1.0
+    return StepOutput(Nx, Ny, Nz, dx, output_dir, vtk_every, callback, callback_every,
+                      name=setup.name)
 
 
 __all__ = ["SimulationSetup", "parse_kraken", "parse_kraken_sweep", "load_kraken",
