@@ -86,19 +86,61 @@ def traffic_per_launch(storage):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML
+    (nvidia_ml_py) every 10 ms on the GPU with the CUDA device's PCI bus id,
+    else nvidia-smi every 100 ms.  start() returns once the first sample is
+    in, so the samples cover the whole timed region.  Read-only queries."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index):
         self.index = index
         self.proc = None
         self.lines = []
+        self.samples = []  # (sm_mhz, max_mhz, reason bits) from NVML
         self.t = None
+        self.nvml = None
+        self.stop_flag = threading.Event()
+        self.first = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            p = torch.cuda.get_device_properties(self.index)
+            bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _poll(self, nv, h):
+        getr = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop_flag.is_set():
+            try:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), smax, getr(h)))
+            except Exception:
+                pass
+            self.first.set()
+            self.stop_flag.wait(0.01)
 
     def start(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.nvml = nv
+            self.t = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self.t.start()
+            self.first.wait(5)
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
@@ -106,14 +148,27 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            self.first.wait(5)
         except (OSError, FileNotFoundError):
             self.proc = None
 
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+            self.first.set()
 
     def stop(self):
+        if self.nvml is not None:
+            self.stop_flag.set()
+            self.t.join(timeout=5)
+            sm = [s[0] for s in self.samples]
+            bits = 0
+            for s in self.samples:
+                bits |= int(s[2])
+            return {"sm_mhz": statistics.median(sm) if sm else None,
+                    "sm_max_mhz": self.samples[0][1] if self.samples else None,
+                    "reasons": sorted(k for k, b in self.REASONS.items() if bits & b),
+                    "samples": len(sm), "source": "nvml"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -136,7 +191,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
 def dist_setup(gpus):
@@ -439,7 +494,9 @@ def bench_tgv_precisions(pkg, n=N_GRID, steps=2000):
         del u
         torch.cuda.empty_cache()
     return {"workload": f"D3Q19 TRT periodic Taylor-Green {n}^3, Lambda=1/4, nu={NU}, u0={U0}, "
-                        f"{steps} steps per storage", "storages": out}
+                        f"{steps} steps per storage", "storages": out,
+            "f16dev_over_f32dev_mlups": round(out["f16dev"]["mlups"] / out["f32dev"]["mlups"], 3),
+            "f16dev_sr_over_f32dev_mlups": round(out["f16dev_sr"]["mlups"] / out["f32dev"]["mlups"], 3)}
 
 
 def bench_cavity2d(pkg, steps=20000, graph_steps=200):
@@ -984,7 +1041,7 @@ def run_other(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--storage", default="f32dev", choices=sorted(STORAGES))

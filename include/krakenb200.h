@@ -439,11 +439,14 @@ int kb_fused_trt_step_3d(void *f_out, const void *f_in, void *rho, void *ux, voi
 /* Kernel variant for tuning and tests (process-wide, not thread-safe to
  * change while other threads launch).  kernel 1 = the deviation-storage
  * kernels of kb_fused_trt_step_3d: 0 automatic (KB_F32_DEV: 3 for even Nx,
- * else 1; FP16/BF16: 2 when Nx >= 64, else 1), 1 one node per thread,
- * 2 nodes x and x+32 per thread, 3 adjacent node pairs with 2-element
- * vector accesses (even Nx), 4 adjacent node quads with 8-byte accesses
- * (16-bit storages, Nx % 4 == 0).
- * Variants 2, 3 and 4 collide in packed FP32x2 arithmetic.
+ * else 1; FP16/BF16: 5 when its conditions hold and the rows fill the
+ * 256-node tiles to 90 % or more, else 2 when Nx >= 64, else 1), 1 one node
+ * per thread, 2 nodes x and x+32 per thread, 3 adjacent node pairs with
+ * 2-element vector accesses (even Nx), 4 adjacent node quads with 8-byte accesses
+ * (16-bit storages, Nx % 4 == 0), 5 persistent row tiles of 256 nodes whose
+ * pull source rows are staged in shared memory by tensor-memory-accelerator
+ * copies (16-bit storages, Nx % 8 == 0, 16-byte aligned populations).
+ * Variants 2 to 5 collide in packed FP32x2 arithmetic.
  * kernel 2 = the tensor-core engine of the warm-start network and
  * kb_gemm_bf16: 0 warp-specialised persistent kernel, 1 one CTA per output
  * tile (default).  Every variant
@@ -530,6 +533,11 @@ int kb_convert_populations(void *dst, int dst_dtype, const void *src, int src_dt
  * one stream are bit-identical.  Synchronises `stream`.  No reference
  * counterpart. */
 int kb_set_stochastic_seed(unsigned int seed, void *stream);
+
+/* *timed_out = 1 if a staged step (kernel 1, variant 5) gave up a bounded
+ * wait on its copies since the last call (the flag is then cleared);
+ * synchronises `stream`.  No reference counterpart. */
+int kb_staged_step_status(int *timed_out, void *stream);
 
 /* ---------------------------------------------------- FP64 reductions -- */
 

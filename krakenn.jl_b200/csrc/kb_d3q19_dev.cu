@@ -16,6 +16,11 @@
 //
 // Compiled with FMA contraction on: this is the precision tier, checked by
 // its max/L2 error against the FP64 run, not bit for bit.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+
 #include "kb_d3q19.cuh"
 
 namespace kb {
@@ -221,18 +226,58 @@ __global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_x2_k(R *__rest
                                                     float *__restrict__ uy_o, float *__restrict__ uz_o,
                                                     const uint8_t *__restrict__ solid, Grid3 g,
                                                     float sp, float sm) {
+    constexpr int CX[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+    constexpr int CY[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
+    constexpr int CZ[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int iA = warp * 64 + lane, iB = iA + 32;
+    const int x0 = warp * 64;  // first node of the warp's run (warp-uniform)
+    const int iA = x0 + lane, iB = iA + 32;
     if (iA >= g.Nx) return;
     const bool vB = iB < g.Nx;
     const int j = blockIdx.y, k = blockIdx.z;
     const I P = (I)g.plane;
-    const size_t row = (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k);
-    const size_t cA = row + iA, cB = row + (vB ? iB : iA);
+    const size_t cA = (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k) + iA;
+    const bool px = g.per & 1, py = (g.per >> 1) & 1, pz = (g.per >> 2) & 1;
+    // Fast path: a full 64-node run whose every pull source is a node at a
+    // fixed y/z shift (inside the box or wrapped; block-uniform) and an x
+    // shift of -1, 0 or +1, wrapped only on the two row-end lanes.  Node B's
+    // sources are then node A's plus 32 elements (an immediate offset), and
+    // one address per population serves both nodes.  Runs touching an x
+    // wall, rows at a y or z wall and ragged run ends take the general pull.
+    const bool yz_fast = (py || (j > 0 && j < g.Ny - 1)) && (pz || (k > 0 && k < g.Nz - 1));
+    const bool x_fast = x0 + 64 <= g.Nx && (px || (x0 > 0 && x0 + 64 < g.Nx));
     float a[19], b[19];
-    pull19_at(fi + cA, P, pull_geometry<I>(g, iA, j, k), a, DevLoad<R>());
-    pull19_at(fi + cB, P, pull_geometry<I>(g, vB ? iB : iA, j, k), b, DevLoad<R>());
+    if (yz_fast && x_fast) {
+        const R *__restrict__ b0 = fi + cA;
+        // c_x = +1 sources of node A and c_x = -1 sources of node B, relative
+        // to node A: the x neighbour, or the wrapped one at a row end
+        const R *__restrict__ bAm = b0 + (iA > 0 ? -1 : g.Nx - 1);
+        const R *__restrict__ bBp = b0 + (iB < g.Nx - 1 ? 33 : 33 - g.Nx);
+        const I sy = (I)g.Nx, sz = (I)g.Nx * (I)g.Ny;
+        const I ym = j > 0 ? -sy : (I)(g.Ny - 1) * sy, yp = j < g.Ny - 1 ? sy : -(I)(g.Ny - 1) * sy;
+        const I zm = k > 0 ? -sz : (I)(g.Nz - 1) * sz, zp = k < g.Nz - 1 ? sz : -(I)(g.Nz - 1) * sz;
+        const DevLoad<R> ld;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            const I u = (I)q * P + (CY[q] > 0 ? ym : CY[q] < 0 ? yp : (I)0) +
+                        (CZ[q] > 0 ? zm : CZ[q] < 0 ? zp : (I)0);
+            const R *__restrict__ p = b0 + u;
+            if (CX[q] == 0) {
+                a[q] = ld(p[0]);
+                b[q] = ld(p[32]);
+            } else if (CX[q] > 0) {
+                a[q] = ld(bAm[u]);
+                b[q] = ld(p[31]);
+            } else {
+                a[q] = ld(p[1]);
+                b[q] = ld(bBp[u]);
+            }
+        }
+    } else {
+        pull19_at(fi + cA, P, pull_geometry<I>(g, iA, j, k), a, DevLoad<R>());
+        pull19_at(fi + cA + (vB ? 32 : 0), P, pull_geometry<I>(g, vB ? iB : iA, j, k), b, DevLoad<R>());
+    }
     float2 d[19];
 #pragma unroll
     for (int q = 0; q < 19; ++q) d[q] = make_float2(a[q], b[q]);
@@ -240,31 +285,35 @@ __global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_x2_k(R *__rest
     float2 o[19], rho, ux, uy, uz;
     trt_dev_collide(d, o, rho, ux, uy, uz, sp, sm);
     uchar2 sm2 = make_uchar2(0, 0);
-    if (SOLID) sm2 = make_uchar2(solid[cA], vB ? solid[cB] : 0);
+    if (SOLID) sm2 = make_uchar2(solid[cA], vB ? solid[cA + 32] : 0);
+    R *__restrict__ o0 = fo + cA;  // node B stores at +32 elements
     if (SR) {
         const uint32_t key = sr_key();
-        unsigned short *fs = reinterpret_cast<unsigned short *>(fo);
+        unsigned short *fs = reinterpret_cast<unsigned short *>(o0);
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
             const uint32_t v = SRPack<R>::pack(SOLID && sm2.x ? 0.f : o[q].x,
                                                SOLID && sm2.y ? 0.f : o[q].y, sr_bits(key, q));
-            fs[cA + (size_t)(q * P)] = (unsigned short)(v & 0xFFFFu);
-            if (vB) fs[cB + (size_t)(q * P)] = (unsigned short)(v >> 16);
+            unsigned short *s = fs + (I)q * P;
+            s[0] = (unsigned short)(v & 0xFFFFu);
+            if (vB) s[32] = (unsigned short)(v >> 16);
         }
     } else {
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
-            fo[cA + (size_t)(q * P)] = Dev<R>::st(SOLID && sm2.x ? 0.f : o[q].x);
-            if (vB) fo[cB + (size_t)(q * P)] = Dev<R>::st(SOLID && sm2.y ? 0.f : o[q].y);
+            R *s = o0 + (I)q * P;
+            s[0] = Dev<R>::st(SOLID && sm2.x ? 0.f : o[q].x);
+            if (vB) s[32] = Dev<R>::st(SOLID && sm2.y ? 0.f : o[q].y);
         }
     }
     if (MOM) {
         const bool sA = SOLID && sm2.x, sB = SOLID && sm2.y;
-        rho_o[cA] = sA ? 1.f : rho.x; ux_o[cA] = sA ? 0.f : ux.x;
-        uy_o[cA] = sA ? 0.f : uy.x; uz_o[cA] = sA ? 0.f : uz.x;
+        float *r = rho_o + cA, *x = ux_o + cA, *y = uy_o + cA, *z = uz_o + cA;
+        r[0] = sA ? 1.f : rho.x; x[0] = sA ? 0.f : ux.x;
+        y[0] = sA ? 0.f : uy.x; z[0] = sA ? 0.f : uz.x;
         if (vB) {
-            rho_o[cB] = sB ? 1.f : rho.y; ux_o[cB] = sB ? 0.f : ux.y;
-            uy_o[cB] = sB ? 0.f : uy.y; uz_o[cB] = sB ? 0.f : uz.y;
+            r[32] = sB ? 1.f : rho.y; x[32] = sB ? 0.f : ux.y;
+            y[32] = sB ? 0.f : uy.y; z[32] = sB ? 0.f : uz.y;
         }
     }
 }
@@ -575,6 +624,398 @@ __global__ void __launch_bounds__(128, KB_QUAD_MIN_BLOCKS) trt_dev_v4_k(R *__res
     }
 }
 
+// ---------------------------------------------------------------------------
+// Row tiles staged by the tensor memory accelerator (16-bit storages).
+// A persistent block walks tiles of TT = 256 nodes along x (one row segment
+// at fixed y, z).  A producer warp streams each tile's pull sources into a
+// ring of TSTAGES shared-memory stages with cp.async.bulk.tensor copies,
+// each stage completed by a "full" mbarrier transaction count: for every
+// population q the 256-element run of plane q at the pull source row
+// (y - c_y, z - c_z), wrapped on periodic axes (13 copies: populations that
+// share a source row and are adjacent in q travel in one box), and for the
+// ten populations with c_x != 0 an 8-element halo run holding the one
+// source outside the tile (x0 - 1 for c_x = +1, the element after the
+// tile's last node for c_x = -1): the neighbouring segment, the periodic
+// wrap, or at an x wall the node's own opposite population (half-way
+// bounce-back).  Four consumer warps wait on "full", read, release the stage
+// on its "empty" mbarrier and collide; the loads of the next tiles run
+// meanwhile and no register holds a load in flight.  Consumer thread t owns
+// the adjacent nodes x0 + 2t, x0 + 2t + 1 and reads population q at the
+// fixed shared-memory offset 2t - c_x (no address arithmetic per
+// population); it stores each updated pair as one 4-byte word.  Rows whose
+// pull meets a y or z wall take the direct pull of every population.
+// Needs Nx % 8 == 0 and 16-byte aligned populations (tensor-map rules).
+constexpr int TT = 256;                 // nodes per row tile
+constexpr int THALO = 64;               // halo slot stride (elements, 128 bytes)
+constexpr int TSTAGES = 4;
+constexpr int TCONS = TT / 2;           // consumer threads: one per adjacent node pair
+constexpr int TTHREADS = TCONS + 32;    // + the producer warp
+constexpr int TSTAGE = 19 * TT + 10 * THALO;  // elements per stage (row q at q * TT)
+constexpr size_t TSMEM = 128 + (size_t)TSTAGES * TSTAGE * 2;  // + alignment slack
+constexpr uint32_t TBYTES = 19u * TT * 2u + 10u * 8u * 2u;   // transaction bytes of a staged tile
+constexpr long long TWAIT = 4000000;    // bounded mbarrier wait (polls)
+
+#ifndef KB_TMA_MIN_BLOCKS
+#define KB_TMA_MIN_BLOCKS 3
+#endif
+
+__device__ int g_tma_timeout = 0;  // set when a staged step gave up a bounded wait
+
+// c_x = +1 populations (left tile end) with their y/z shifts; QM are their
+// opposites, the c_x = -1 populations of the right end, with shifts negated.
+__device__ constexpr int kQP[5] = {1, 7, 9, 11, 13}, kQM[5] = {2, 10, 8, 14, 12};
+__device__ constexpr int kEY[5] = {0, 1, -1, 0, 0}, kEZ[5] = {0, 0, 0, 1, -1};
+
+__device__ __forceinline__ uint32_t s_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ bool tbar_wait(uint32_t bar, uint32_t parity) {
+    for (long long it = 0; it < TWAIT; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (it > 32) __nanosleep(128);
+    }
+    return false;
+}
+__device__ __forceinline__ void tbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tma_load4(uint32_t dst, const CUtensorMap *tm, int x, int y, int z,
+                                          int q, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(q), "r"(bar)
+        : "memory");
+}
+
+// Tiles are numbered x-segment fastest, then y, then z.  A block visits
+// tiles b, b + G, b + 2G, ... (G = grid size); a cursor (xt, j, k) advances
+// by G without a division per tile.  staged() says whether every pull
+// source row of a tile exists (interior or wrapped), i.e. it is staged.
+struct TileMap {
+    int ntx, Nx, Ny, Nz, per;
+    int dx, dj, dk;  // G decomposed as (x-segments, rows, planes)
+    __device__ __forceinline__ void at(int t, int &xt, int &j, int &k) const {
+        xt = t % ntx;
+        const int r = t / ntx;
+        j = r % Ny;
+        k = r / Ny;
+    }
+    __device__ __forceinline__ void advance(int &xt, int &j, int &k) const {
+        xt += dx;
+        int c = xt >= ntx;
+        xt -= c ? ntx : 0;
+        j += dj + c;
+        c = j >= Ny;
+        j -= c ? Ny : 0;
+        k += dk + c;
+    }
+    __device__ __forceinline__ bool staged(int j, int k) const {
+        return ((per & 2) || (j > 0 && j < Ny - 1)) && ((per & 4) || (k > 0 && k < Nz - 1));
+    }
+};
+
+// The copies of one staged tile (issued by one elected producer lane).
+// Maps: t1 / t2 / t3 copy 1 / 2 / 3 consecutive planes of a 256-element
+// row run, th an 8-element halo run of one plane.
+struct TileMaps {
+    const CUtensorMap *t1, *t2, *t3, *th;
+};
+__device__ __forceinline__ void tma_issue_tile(const TileMaps &mp, uint32_t dst, uint32_t bar,
+                                               int x0, int j, int k, const TileMap &m) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(TBYTES)
+                 : "memory");
+    const int ym = j > 0 ? j - 1 : m.Ny - 1, yp = j < m.Ny - 1 ? j + 1 : 0;
+    const int zm = k > 0 ? k - 1 : m.Nz - 1, zp = k < m.Nz - 1 ? k + 1 : 0;
+    const uint32_t R = TT * 2;  // bytes per staged row
+    tma_load4(dst + 0 * R, mp.t3, x0, j, k, 0, bar);     // q 0, 1, 2: (0, 0)
+    tma_load4(dst + 3 * R, mp.t1, x0, ym, k, 3, bar);    // q 3: c_y = +1
+    tma_load4(dst + 4 * R, mp.t1, x0, yp, k, 4, bar);    // q 4: c_y = -1
+    tma_load4(dst + 5 * R, mp.t1, x0, j, zm, 5, bar);    // q 5: c_z = +1
+    tma_load4(dst + 6 * R, mp.t1, x0, j, zp, 6, bar);    // q 6: c_z = -1
+    tma_load4(dst + 7 * R, mp.t2, x0, ym, k, 7, bar);    // q 7, 8: c_y = +1
+    tma_load4(dst + 9 * R, mp.t2, x0, yp, k, 9, bar);    // q 9, 10: c_y = -1
+    tma_load4(dst + 11 * R, mp.t2, x0, j, zm, 11, bar);  // q 11, 12: c_z = +1
+    tma_load4(dst + 13 * R, mp.t2, x0, j, zp, 13, bar);  // q 13, 14: c_z = -1
+    tma_load4(dst + 15 * R, mp.t1, x0, ym, zm, 15, bar); // q 15: (+1, +1)
+    tma_load4(dst + 16 * R, mp.t1, x0, yp, zm, 16, bar); // q 16: (-1, +1)
+    tma_load4(dst + 17 * R, mp.t1, x0, ym, zp, 17, bar); // q 17: (+1, -1)
+    tma_load4(dst + 18 * R, mp.t1, x0, yp, zp, 18, bar); // q 18: (-1, -1)
+    // halos: slot e (left, c_x = +1) and 5 + e (right, c_x = -1).  At an x
+    // wall the slot holds the end node's own opposite population from its
+    // own row (node 0 at slot position 0, node Nx - 1 at position 7).
+    const bool px = m.per & 1;
+    const uint32_t hdst = dst + 19 * R;
+    const bool lwall = x0 == 0 && !px, rwall = x0 + TT >= m.Nx && !px;
+    const int xl = lwall ? 0 : (x0 > 0 ? x0 - 8 : m.Nx - 8);       // x0 - 1 (or Nx - 1) at 7
+    const int xr = rwall ? m.Nx - 8 : (x0 + TT < m.Nx ? x0 + TT : 0); // next column (or 0) at 0
+#pragma unroll
+    for (int e = 0; e < 5; ++e) {
+        const int yl = lwall ? j : (kEY[e] > 0 ? ym : kEY[e] < 0 ? yp : j);
+        const int zl = lwall ? k : (kEZ[e] > 0 ? zm : kEZ[e] < 0 ? zp : k);
+        const int yr = rwall ? j : (kEY[e] > 0 ? yp : kEY[e] < 0 ? ym : j);
+        const int zr = rwall ? k : (kEZ[e] > 0 ? zp : kEZ[e] < 0 ? zm : k);
+        tma_load4(hdst + (uint32_t)(e * THALO * 2), mp.th, xl, yl, zl, lwall ? kQM[e] : kQP[e], bar);
+        tma_load4(hdst + (uint32_t)((5 + e) * THALO * 2), mp.th, xr, yr, zr, rwall ? kQP[e] : kQM[e], bar);
+    }
+}
+
+template <typename R, bool MOM, bool SOLID, typename I, bool SR>
+__global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
+    trt_dev_tma_k(const __grid_constant__ CUtensorMap tmap1, const __grid_constant__ CUtensorMap tmap2,
+                  const __grid_constant__ CUtensorMap tmap3, const __grid_constant__ CUtensorMap thalo,
+                  R *__restrict__ fo, const R *__restrict__ fi, float *__restrict__ rho_o,
+                  float *__restrict__ ux_o, float *__restrict__ uy_o, float *__restrict__ uz_o,
+                  const uint8_t *__restrict__ solid, Grid3 g, float sp, float sm) {
+    constexpr int CX[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+    extern __shared__ unsigned char tsm_raw[];
+    __shared__ __align__(8) uint64_t full[TSTAGES], empty[TSTAGES];
+    R *stage0 = reinterpret_cast<R *>(tsm_raw + ((128u - (s_addr(tsm_raw) & 127u)) & 127u));
+    const int t = threadIdx.x;
+    TileMap m;
+    m.ntx = (g.Nx + TT - 1) / TT;
+    m.Nx = g.Nx;
+    m.Ny = g.Ny;
+    m.Nz = g.Nz;
+    m.per = g.per;
+    m.at((int)gridDim.x, m.dx, m.dj, m.dk);
+    if (t == 0) {
+        for (int s = 0; s < TSTAGES; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s_addr(&full[s])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_addr(&empty[s])),
+                         "r"(TCONS / 32));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    int cx, cj, ck;  // this role's current tile
+    m.at((int)blockIdx.x, cx, cj, ck);
+
+    if (t >= TCONS) {
+        // ------------------------------------------------ producer warp --
+        const TileMaps mp{&tmap1, &tmap2, &tmap3, &thalo};
+        if (t == TCONS) {
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap1)) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap2)) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap3)) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&thalo)) : "memory");
+        }
+#pragma unroll 1
+        for (int n = 0; ck < g.Nz; m.advance(cx, cj, ck), ++n) {
+            const int s = n % TSTAGES;
+            // the consumers have released this stage's previous tile
+            if (n >= TSTAGES && !tbar_wait(s_addr(&empty[s]), (uint32_t)(n / TSTAGES - 1) & 1u)) {
+                if (t == TCONS) atomicExch(&g_tma_timeout, 1);
+                break;
+            }
+            if (t == TCONS) {
+                const uint32_t bar = s_addr(&full[s]);
+                if (m.staged(cj, ck))
+                    tma_issue_tile(mp, s_addr(stage0 + s * TSTAGE), bar, cx * TT, cj, ck, m);
+                else  // nothing to copy: the phase completes on the arrival
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], 0;" ::"r"(bar)
+                                 : "memory");
+            }
+            __syncwarp();
+        }
+        return;
+    }
+
+    // ---------------------------------------------------- consumer warps --
+    const I P = (I)g.plane;
+    const uint32_t ekey = SR ? hash32(*(volatile const unsigned int *)&g_sr_epoch + 0x632BE5ABu) : 0u;
+    int it = 0;
+    bool aborted = false;
+#pragma unroll 1
+    for (; ck < g.Nz; m.advance(cx, cj, ck), ++it) {
+        const int s = it % TSTAGES;
+        const int x0 = cx * TT, j = cj, k = ck;
+        const int iA = x0 + 2 * t;
+        const bool live = iA < g.Nx;  // Nx even: both nodes of the pair or neither
+        const size_t cA = (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k) + iA;
+        if (!tbar_wait(s_addr(&full[s]), (uint32_t)(it / TSTAGES) & 1u)) {
+            atomicExch(&g_tma_timeout, 1);
+            aborted = true;
+            break;
+        }
+        float2 d[19];
+        if (m.staged(j, k)) {
+            const R *st = stage0 + s * TSTAGE + 2 * t;
+            const DevLoad<R> ld;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) {
+                const R *r = st + q * TT;  // reads at -1 / +256 fall in the neighbouring rows
+                if (CX[q] == 0) d[q] = Vec2<R>::ld(r);
+                else if (CX[q] > 0) d[q] = make_float2(ld(r[-1]), ld(r[0]));
+                else d[q] = make_float2(ld(r[1]), ld(r[2]));
+            }
+            // the tile ends take the halo slots (the thread holding the
+            // tile's last node: local index min(TT, Nx - x0) - 1, odd)
+            const R *h = stage0 + s * TSTAGE + 19 * TT;
+            if (t == 0) {
+                const int pl = (x0 == 0 && !(g.per & 1)) ? 0 : 7;
+#pragma unroll
+                for (int e = 0; e < 5; ++e) d[kQP[e]].x = ld(h[e * THALO + pl]);
+            }
+            if (t == (min(TT, g.Nx - x0) - 2) >> 1) {
+                const int pr = (x0 + TT >= g.Nx && !(g.per & 1)) ? 7 : 0;
+#pragma unroll
+                for (int e = 0; e < 5; ++e) d[kQM[e]].y = ld(h[(5 + e) * THALO + pr]);
+            }
+        } else if (live) {
+            // rows at a y or z wall: direct pull of both nodes
+            float a[19], b[19];
+            pull19_at(fi + cA, P, pull_geometry<I>(g, iA, j, k), a, DevLoad<R>());
+            pull19_at(fi + cA + 1, P, pull_geometry<I>(g, iA + 1, j, k), b, DevLoad<R>());
+#pragma unroll
+            for (int q = 0; q < 19; ++q) d[q] = make_float2(a[q], b[q]);
+        }
+        __syncwarp();
+        if ((t & 31) == 0) tbar_arrive(s_addr(&empty[s]));  // this warp is done with stage s
+        if (!live) continue;
+        // the rates pass through opaque moves each tile so the collision's
+        // rate-derived constants are formed here, not held across the loop
+        float spl, sml;
+        asm volatile("mov.b32 %0, %1;" : "=f"(spl) : "f"(sp));
+        asm volatile("mov.b32 %0, %1;" : "=f"(sml) : "f"(sm));
+        float2 o[19], rho, ux, uy, uz;
+        trt_dev_collide(d, o, rho, ux, uy, uz, spl, sml);
+        uchar2 sm2 = make_uchar2(0, 0);
+        if (SOLID) sm2 = *reinterpret_cast<const uchar2 *>(solid + cA);
+        // likewise the plane stride, so the 19 plane offsets are not hoisted
+        I Pl;
+        if constexpr (sizeof(I) == 4) asm volatile("mov.b32 %0, %1;" : "=r"(Pl) : "r"((int)P));
+        else asm volatile("mov.b64 %0, %1;" : "=l"(Pl) : "l"((long long)P));
+        R *o0 = fo + cA;
+        if (SR) {
+            const uint32_t key = hash32((uint32_t)cA ^ ekey);
+#pragma unroll
+            for (int q = 0; q < 19; ++q) {
+                const uint32_t v = SRPack<R>::pack(SOLID && sm2.x ? 0.f : o[q].x,
+                                                   SOLID && sm2.y ? 0.f : o[q].y, sr_bits(key, q));
+                *reinterpret_cast<uint32_t *>(o0 + (I)q * Pl) = v;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 19; ++q)
+                Vec2<R>::st(o0 + (I)q * Pl, make_float2(SOLID && sm2.x ? 0.f : o[q].x,
+                                                        SOLID && sm2.y ? 0.f : o[q].y));
+        }
+        if (MOM) {
+            float2 r = rho, a = ux, b = uy, c = uz;
+            if (SOLID && sm2.x) { r.x = 1.f; a.x = b.x = c.x = 0.f; }
+            if (SOLID && sm2.y) { r.y = 1.f; a.y = b.y = c.y = 0.f; }
+            *reinterpret_cast<float2 *>(rho_o + cA) = r;
+            *reinterpret_cast<float2 *>(ux_o + cA) = a;
+            *reinterpret_cast<float2 *>(uy_o + cA) = b;
+            *reinterpret_cast<float2 *>(uz_o + cA) = c;
+        }
+    }
+    // after a timeout: wait (bounded) for copies the producer may still have
+    // in flight, so none lands in shared memory after the block has exited
+    if (aborted && (t & 31) == 0) {
+        for (int n = 0; n < TSTAGES && ck < g.Nz; ++n, m.advance(cx, cj, ck)) {
+            const int i2 = it + n;
+            tbar_wait(s_addr(&full[i2 % TSTAGES]), (uint32_t)(i2 / TSTAGES) & 1u);
+        }
+    }
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 tma_encode_fn() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// The staged kernel's layout and alignment rules: Nx % 8 == 0 (16-byte
+// row pitch of the tensor map), 16-byte aligned input populations, 4-byte
+// aligned output pairs, 8-byte aligned moment pairs, 2-byte aligned mask
+// pairs, tile count within int.
+static bool tma_eligible(const Grid3 &g, const void *f_out, const void *f_in, const float *rho,
+                         const float *ux, const float *uy, const float *uz, const uint8_t *solid) {
+    const auto al = [](const void *p, uintptr_t a) { return ((uintptr_t)p & (a - 1)) == 0; };
+    const double tiles = (double)((g.Nx + TT - 1) / TT) * g.Ny * g.Nz;
+    return g.Nx % 8 == 0 && al(f_in, 16) && al(f_out, 4) && al(rho, 8) && al(ux, 8) &&
+           al(uy, 8) && al(uz, 8) && al(solid, 2) && tiles < 2147483647.0 &&
+           tma_encode_fn() != nullptr;
+}
+
+// Maps of one population buffer: [0..2] 256-element row runs of 1, 2 and 3
+// consecutive planes, [3] 8-element halo runs of one plane.
+struct TmaMaps {
+    CUtensorMap m[4];
+};
+
+template <typename R, bool MOM, bool SOLID, typename I, bool SR>
+static int launch_tma_k(const TmaMaps &mp, R *fo, const R *fi, float *rho, float *ux, float *uy,
+                        float *uz, const uint8_t *solid, const Grid3 &g, float sp, float sm,
+                        cudaStream_t s) {
+    static int occ = -1;  // resident blocks per SM of this instantiation
+    if (occ < 0) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trt_dev_tma_k<R, MOM, SOLID, I, SR>,
+                                                          TTHREADS, TSMEM) != cudaSuccess || n < 1) {
+            cudaGetLastError();
+            n = 1;
+        }
+        occ = n;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long tiles = (long long)((g.Nx + TT - 1) / TT) * g.Ny * g.Nz;
+    const int blocks = (int)std::min<long long>(tiles, (long long)sms * occ);
+    trt_dev_tma_k<R, MOM, SOLID, I, SR><<<blocks, TTHREADS, TSMEM, s>>>(
+        mp.m[0], mp.m[1], mp.m[2], mp.m[3], fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+    return KB_OK;
+}
+
+template <typename R, typename I, bool SR>
+static int launch_tma(void *f_out, const void *f_in, float *rho, float *ux, float *uy, float *uz,
+                      const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s) {
+    // the populations as a 4-D tensor (x, y, z, q) of 16-bit words
+    TmaMaps mp;
+    const cuuint64_t dims[4] = {(cuuint64_t)g.Nx, (cuuint64_t)g.Ny, (cuuint64_t)g.Nz, 19};
+    const cuuint64_t strides[3] = {(cuuint64_t)g.Nx * 2, (cuuint64_t)g.Nx * g.Ny * 2,
+                                   (cuuint64_t)g.plane * 2};
+    const cuuint32_t boxes[4][4] = {{TT, 1, 1, 1}, {TT, 1, 1, 2}, {TT, 1, 1, 3}, {8, 1, 1, 1}};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    for (int n = 0; n < 4; ++n) {
+        const CUresult r = tma_encode_fn()(&mp.m[n], CU_TENSOR_MAP_DATA_TYPE_UINT16, 4,
+                                           const_cast<void *>(f_in), dims, strides, boxes[n], es,
+                                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS)
+            return set_error(KB_ERR_CUDA, "kb_fused_trt_step_3d: cuTensorMapEncodeTiled failed (%d)",
+                             (int)r);
+    }
+    R *fo = (R *)f_out;
+    const R *fi = (const R *)f_in;
+    if (rho) {
+        if (solid) return launch_tma_k<R, true, true, I, SR>(mp, fo, fi, rho, ux, uy, uz, solid, g, sp, sm, s);
+        return launch_tma_k<R, true, false, I, SR>(mp, fo, fi, rho, ux, uy, uz, solid, g, sp, sm, s);
+    }
+    if (solid) return launch_tma_k<R, false, true, I, SR>(mp, fo, fi, rho, ux, uy, uz, solid, g, sp, sm, s);
+    return launch_tma_k<R, false, false, I, SR>(mp, fo, fi, rho, ux, uy, uz, solid, g, sp, sm, s);
+}
+
 template <typename R, typename I, bool SR>
 static void launch_ri(void *f_out, const void *f_in, float *rho, float *ux, float *uy, float *uz,
                       const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s,
@@ -630,14 +1071,24 @@ static void launch_ri(void *f_out, const void *f_in, float *rho, float *ux, floa
 }
 
 template <typename R, bool SR = false>
-static void launch_r(void *f_out, const void *f_in, float *rho, float *ux, float *uy, float *uz,
-                     const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s,
-                     int kind) {
+static int launch_r(void *f_out, const void *f_in, float *rho, float *ux, float *uy, float *uz,
+                    const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s,
+                    int kind) {
+    if constexpr (sizeof(R) == 2) {
+        if (kind == 5) {
+            const int rc = offsets_fit_int(g, 19)
+                               ? launch_tma<R, int, SR>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s)
+                               : launch_tma<R, long long, SR>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s);
+            if (rc == KB_OK && SR) sr_advance_k<<<1, 1, 0, s>>>();
+            return rc;
+        }
+    }
     if (offsets_fit_int(g, 19))
         launch_ri<R, int, SR>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, kind);
     else
         launch_ri<R, long long, SR>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, kind);
     if (SR) sr_advance_k<<<1, 1, 0, s>>>();
+    return KB_OK;
 }
 
 int launch_trt3d_dev(int dtype, void *f_out, const void *f_in, float *rho, float *ux, float *uy,
@@ -645,30 +1096,43 @@ int launch_trt3d_dev(int dtype, void *f_out, const void *f_in, float *rho, float
                      cudaStream_t s, int variant) {
     // variant: 0 automatic, 1 one node per thread, 2 nodes x and x+32 per
     // thread, 3 adjacent node pairs with vector accesses (even Nx only),
-    // 4 adjacent node quads with 8-byte accesses (16-bit storages, Nx % 4 == 0).
+    // 4 adjacent node quads with 8-byte accesses (16-bit storages, Nx % 4 == 0),
+    // 5 row tiles staged by the tensor memory accelerator (16-bit storages,
+    // Nx % 8 == 0, aligned buffers).
     if (variant == 3 && g.Nx % 2 != 0)
         return set_error(KB_ERR_ARG, "kb_fused_trt_step_3d: the vector-pair kernel needs an even Nx");
     if (variant == 4 && (g.Nx % 4 != 0 || dtype == KB_F32_DEV))
         return set_error(KB_ERR_ARG,
                          "kb_fused_trt_step_3d: the quad kernel needs Nx %% 4 == 0 and 16-bit storage");
+    if (variant == 5 && (dtype == KB_F32_DEV || !tma_eligible(g, f_out, f_in, rho, ux, uy, uz, solid)))
+        return set_error(KB_ERR_ARG,
+                         "kb_fused_trt_step_3d: the staged kernel needs 16-bit storage, Nx %% 8 == 0 "
+                         "and 16-byte aligned populations");
     // automatic choice, from measurements at 256^3 on B200: FP32 deviations
-    // run fastest as vector pairs, FP16/BF16 as x / x+32 pairs
+    // run fastest as vector pairs (44.5 GLUPS); FP16/BF16 as staged row
+    // tiles (78.7 GLUPS) where the rows fill the 256-node tiles to 90 % or
+    // more, else as x / x+32 pairs (65.2 GLUPS at 256^3)
     int kind = variant;
     if (variant == 0) {
+        const int ntx = (g.Nx + TT - 1) / TT;
         if (dtype == KB_F32_DEV) kind = g.Nx % 2 == 0 ? 3 : 1;
+        else if (10 * g.Nx >= 9 * ntx * TT && tma_eligible(g, f_out, f_in, rho, ux, uy, uz, solid))
+            kind = 5;
         else kind = g.Nx >= 64 ? 2 : 1;
     }
     // the x / x+32 stores of the stochastic-rounding variant scatter 16-bit
     // halves; the vector-pair kernel stores each packed pair whole
     const int pairs = kind;
+    int rc = KB_OK;
     switch (dtype) {
-        case KB_F32_DEV: launch_r<float>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
-        case KB_F16_DEV: launch_r<__half>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
-        case KB_BF16_DEV: launch_r<__nv_bfloat16>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
-        case KB_F16_DEV_SR: launch_r<__half, true>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
-        case KB_BF16_DEV_SR: launch_r<__nv_bfloat16, true>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
+        case KB_F32_DEV: rc = launch_r<float>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
+        case KB_F16_DEV: rc = launch_r<__half>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
+        case KB_BF16_DEV: rc = launch_r<__nv_bfloat16>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
+        case KB_F16_DEV_SR: rc = launch_r<__half, true>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
+        case KB_BF16_DEV_SR: rc = launch_r<__nv_bfloat16, true>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, pairs); break;
         default: return set_error(KB_ERR_UNSUPPORTED, "kb_fused_trt_step_3d: unknown dtype %d", dtype);
     }
+    if (rc != KB_OK) return rc;
     return check_launch("kb_fused_trt_step_3d");
 }
 
@@ -757,6 +1221,25 @@ extern "C" int kb_set_stochastic_seed(unsigned int seed, void *stream) {
     // the host value must outlive the asynchronous copy
     if (cudaStreamSynchronize(kb::as_stream(stream)) != cudaSuccess)
         return kb::check_launch("kb_set_stochastic_seed");
+    return 0;
+}
+
+extern "C" int kb_staged_step_status(int *timed_out, void *stream) {
+    KB_REQUIRE(timed_out, "kb_staged_step_status: null argument");
+    cudaStream_t s = kb::as_stream(stream);
+    int v = 0;
+    if (cudaMemcpyFromSymbolAsync(&v, kb::d3::g_tma_timeout, sizeof(int), 0, cudaMemcpyDeviceToHost,
+                                  s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return kb::check_launch("kb_staged_step_status");
+    if (v) {
+        const int zero = 0;
+        if (cudaMemcpyToSymbolAsync(kb::d3::g_tma_timeout, &zero, sizeof(int), 0,
+                                    cudaMemcpyHostToDevice, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return kb::check_launch("kb_staged_step_status");
+    }
+    *timed_out = v;
     return 0;
 }
 

@@ -688,7 +688,9 @@ def collide_boussinesq_3d_(f, Temp, is_solid, omega, beta_g, T_ref):
 def set_trt3d_variant(variant: int):
     """0 automatic, 1 one node per thread, 2 nodes x and x+32 per thread,
     3 adjacent node pairs with vector accesses (even Nx), 4 adjacent node
-    quads with 8-byte accesses (16-bit storages, Nx % 4 == 0)."""
+    quads with 8-byte accesses (16-bit storages, Nx % 4 == 0), 5 persistent
+    256-node row tiles staged in shared memory by tensor-memory-accelerator
+    copies (16-bit storages, Nx % 8 == 0, 16-byte aligned buffers)."""
     call("kb_set_kernel_variant", 1, int(variant))
 
 
@@ -786,6 +788,14 @@ def set_stochastic_seed(seed: int):
     call("kb_set_stochastic_seed", C.c_uint(seed & 0xFFFFFFFF), _stream())
 
 
+def staged_step_timed_out() -> bool:
+    """True if a staged step (variant 5) gave up a bounded wait on its copies
+    since the last call; clears the flag (synchronises the stream)."""
+    out = C.c_int(0)
+    call("kb_staged_step_status", C.byref(out), _stream())
+    return bool(out.value)
+
+
 def mass(f, deviation=False) -> float:
     """FP64 compensated total mass sum(f) (synchronises the stream)."""
     out = C.c_double()
@@ -812,7 +822,7 @@ def synchronize():
 
 __all__ = [n for n in dir() if n.endswith("_") and not n.startswith("_")] + [
     "trt_rates", "convert_populations", "mass", "residual", "synchronize", "storage_dtype",
-    "set_trt3d_variant", "set_stochastic_seed", "set_umma_engine", "AA_SWAP_2D",
+    "set_trt3d_variant", "set_stochastic_seed", "staged_step_timed_out", "set_umma_engine", "AA_SWAP_2D",
     "torch_dtype", "field_dtype", "periodic_mask", "FACES_3D"]
 
 _ = _lib  # keep the module import explicit for readers

@@ -193,7 +193,9 @@ def test_convert_roundtrip(cuda, pkg):
                                        ((97, 3, 4), (0, 1, 0)), ((64, 4, 4), (1, 0, 1)),
                                        ((2, 4, 4), (1, 0, 1)), ((130, 2, 3), (1, 1, 0)),
                                        ((132, 3, 2), (1, 0, 1)), ((4, 3, 5), (0, 1, 1)),
-                                       ((260, 2, 2), (0, 0, 0))])
+                                       ((260, 2, 2), (0, 0, 0)), ((200, 4, 3), (0, 0, 0)),
+                                       ((192, 4, 3), (1, 0, 1)), ((520, 3, 3), (1, 1, 1)),
+                                       ((512, 3, 4), (0, 1, 0))])
 @pytest.mark.parametrize("with_mask", [False, True])
 @pytest.mark.parametrize("sr", [False, True])
 def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask, sr):
@@ -225,6 +227,8 @@ def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask, 
         variants = (1, 2, 3) if Nx % 2 == 0 else (1, 2)
         if Nx % 4 == 0 and dtype != torch.float32:
             variants += (4,)
+        if Nx % 8 == 0 and dtype != torch.float32:
+            variants += (5,)
         for variant in variants:
             pkg.set_trt3d_variant(variant)
             fo = torch.empty_like(src)
@@ -244,6 +248,51 @@ def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask, 
         pkg.set_trt3d_variant(0)
     for o in outs[1:]:
         assert np.max(np.abs(outs[0] - o) / W19[:, None, None, None]) < 2 * tol
+    assert not pkg.staged_step_timed_out()
+
+
+def test_staged_kernel_rejects_what_it_cannot_stage(cuda, pkg):
+    """Variant 5 needs 16-bit storage, Nx % 8 == 0 and a 16-byte aligned
+    population buffer (tensor-map rules); anything else is an argument error,
+    not a silent fallback."""
+    pkg.set_trt3d_variant(5)
+    try:
+        for dt, Nx, off in ((torch.float16, 12, 0), (torch.float32, 16, 0), (torch.float16, 16, 1)):
+            buf = torch.zeros(19 * 4 * 4 * Nx + off, dtype=dt, device=cuda)
+            f = buf[off:].view(19, 4, 4, Nx)
+            with pytest.raises(pkg.KrakenArgumentError):
+                pkg.fused_trt_step_3d_(torch.empty((19, 4, 4, Nx), dtype=dt, device=cuda), f,
+                                       None, None, None, None, None, Nx, 4, 4, 0.02, 0.25,
+                                       periodic=(1, 1, 1), deviation=True)
+    finally:
+        pkg.set_trt3d_variant(0)
+
+
+def test_staged_kernel_bit_identical_to_pair_kernel_without_sr(cuda, pkg):
+    """The staged kernel and the x / x+32 pair kernel run the same packed
+    FP32x2 collision on the same inputs, so their round-to-nearest outputs
+    agree bit for bit (the staging changes where the operands come from,
+    not their values), on a 256³-class row length with wraps and walls."""
+    rng = np.random.default_rng(3)
+    Nx, Ny, Nz = 264, 5, 4
+    f = W19[:, None, None, None] * (1 + 0.05 * rng.standard_normal((19, Nz, Ny, Nx)))
+    for per in ((1, 1, 1), (0, 0, 0), (1, 0, 1)):
+        src = torch.empty((19, Nz, Ny, Nx), dtype=torch.float16, device=cuda)
+        pkg.convert_populations(src, _g(f), dst_deviation=True)
+        outs = []
+        try:
+            for variant in (2, 5):
+                pkg.set_trt3d_variant(variant)
+                fo = torch.empty_like(src)
+                mt = [torch.empty((Nz, Ny, Nx), dtype=torch.float32, device=cuda) for _ in range(4)]
+                pkg.fused_trt_step_3d_(fo, src, *mt, None, Nx, Ny, Nz, 0.02, 0.25, periodic=per,
+                                       deviation=True)
+                outs.append((fo.clone(), [m.clone() for m in mt]))
+        finally:
+            pkg.set_trt3d_variant(0)
+        assert torch.equal(outs[0][0], outs[1][0]), per
+        for a, b in zip(outs[0][1], outs[1][1]):
+            assert torch.equal(a, b), per
 
 
 def test_quad_kernel_needs_nx_multiple_of_4_and_16bit(cuda, pkg):
