@@ -992,6 +992,44 @@ def bench_output(pkg, n=256, steps=400, every=20):
             "async_overhead_ms_per_snapshot": round((res["async"] - res["none"]) * every, 3)}
 
 
+def bench_slab(pkg, n, storage, steps, warmup, rank, world):
+    """One periodic n^3 Taylor-Green grid split along z over `world` ranks
+    (strong scaling): per step the fused TRT step on each slab's local array
+    and the exchange of the five crossing populations per face (NCCL
+    point-to-point; with one rank, copies of the slab's own end planes).
+    Timed on the device with CUDA events, max over ranks."""
+    import torch
+    tname, deviation, bpp, _ = STORAGES[storage]
+    dt = getattr(torch, tname)
+    slab = pkg.slab.Slab(n, world, rank, True)
+    plane = torch.from_numpy(pkg.drivers.taylor_green_3d_populations(n, U0, Nz=1)).cuda()
+    a = torch.empty((19, slab.nz_alloc, n, n), dtype=dt, device="cuda")
+    pkg.convert_populations(a, plane.expand(19, slab.nz_alloc, n, n).contiguous(),
+                            dst_deviation=deviation)
+    b = torch.empty_like(a)
+    st = pkg.slab.SlabTRT3D(slab, n, n, nu=NU, Lambda=LAMBDA, periodic_xy=(1, 1),
+                            deviation=deviation, stochastic_rounding=storage in SR_STORAGES)
+    for _ in range(warmup):
+        st.step(b, a)
+        a, b = b, a
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(steps):
+        st.step(b, a)
+        a, b = b, a
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    halo = 2 * 5 * n * n * bpp if world > 1 else 0
+    return {"workload": f"D3Q19 TRT periodic Taylor-Green {n}^3 split along z over {world} "
+                        f"rank(s), {storage}", "scaling": "strong",
+            "mlups": round(n ** 3 * steps / (ms * 1e-3) / 1e6, 1), "ms_per_step": round(ms / steps, 4),
+            "planes_per_rank": slab.nz, "ghost_planes_per_rank": slab.nz_alloc - slab.nz,
+            "halo_bytes_sent_per_rank_per_step": halo}
+
+
 def _extrude(plane, n):
     import torch
     out = torch.empty((19, n, n, n), dtype=plane.dtype, device=plane.device)
@@ -1023,6 +1061,8 @@ def run_other(args):
     elif args.workload == "output":
         if rank == 0:
             r = bench_output(pkg, n=args.grid)
+    elif args.workload == "slab":
+        r = bench_slab(pkg, args.grid, args.storage, max(args.steps, 20), args.warmup, rank, world)
     elif args.workload == "libb":
         if rank == 0:
             r = bench_libb(pkg, N=args.grid, R=40.0 * args.grid / 256,
@@ -1060,7 +1100,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the short measurements of the other configurations")
-    ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "cavity2d", "batch", "natconv", "warmstart", "surrogate",
+    ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "cavity2d", "batch", "natconv", "warmstart", "surrogate", "slab",
                              "libb", "output"])
     args = ap.parse_args()
     if args.warmup < 3:

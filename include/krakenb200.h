@@ -338,6 +338,17 @@ int kb_compute_macroscopic_forced_field_3d(void *rho, void *ux, void *uy, void *
 int kb_stream_periodic_xz_wall_y_3d(void *f_out, const void *f_in, int Nx, int Ny, int Nz,
                                     int dtype, void *stream);
 
+/* Ghost planes of a z-slab of D3Q19 populations f[q][k][j][i] with nz_alloc
+ * planes (a ghost plane at k = 0 if lo, at k = nz_alloc - 1 if hi) whose
+ * neighbouring slabs are the slab itself, i.e. one rank on a periodic z
+ * axis: the c_z = +1 populations (5, 11, 12, 15, 16) of the top real plane
+ * fill the bottom ghost, the c_z = -1 populations (6, 13, 14, 17, 18) of the
+ * first real plane fill the top ghost.  Between ranks the same planes travel
+ * by point-to-point messages.  No reference counterpart: the reference runs
+ * one grid on one device. */
+int kb_slab_fill_ghosts_3d(void *f, int Nx, int Ny, int nz_alloc, int lo, int hi, int dtype,
+                           void *stream);
+
 /* Unfused thermal DDF in 3D (run_natural_convection_3d,
  * src/drivers/thermal.jl:455-537).  Fields have the population's type. */
 

@@ -50,6 +50,7 @@ SIGNATURES: dict[str, list] = {
     "kb_compute_macroscopic_forced_field_3d": [_vp, _vp, _vp, _vp, _cvp, _cvp, _cvp, _cvp, _i, _i,
                                                _i, _i, _vp],
     "kb_stream_periodic_xz_wall_y_3d": [_vp, _cvp, _i, _i, _i, _i, _vp],
+    "kb_slab_fill_ghosts_3d": [_vp, _i, _i, _i, _i, _i, _i, _vp],
     "kb_collide_guo_2d": [_vp, _u8p, _i, _i, _d, _d, _d, _i, _vp],
     "kb_collide_guo_field_2d": [_vp, _u8p, _cvp, _cvp, _i, _i, _d, _i, _vp],
     "kb_collide_guo_3d": [_vp, _u8p, _i, _i, _i, _d, _d, _d, _d, _i, _vp],

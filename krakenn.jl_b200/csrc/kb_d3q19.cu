@@ -1181,3 +1181,46 @@ int kb_stream_periodic_xz_wall_y_3d(void *f_out, const void *f_in, int Nx, int N
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Ghost planes of a z-slab whose neighbours are itself (one rank on a
+// periodic z axis): the five c_z = +1 populations of the top real plane go
+// to the bottom ghost plane, the five c_z = -1 populations of the first real
+// plane to the top ghost plane; blockIdx.y picks one of the ten planes.
+namespace kb {
+namespace d3 {
+
+template <typename W>
+__global__ void slab_ghosts_k(W *f, size_t plane, size_t pop, int nz_alloc, int lo, int hi) {
+    constexpr int CZP[5] = {5, 11, 12, 15, 16}, CZM[5] = {6, 13, 14, 17, 18};
+    const int p = blockIdx.y;
+    if (p < 5 ? !lo : !hi) return;
+    const int q = p < 5 ? CZP[p] : CZM[p - 5];
+    const size_t dst = (size_t)q * pop + (p < 5 ? 0 : (size_t)(nz_alloc - 1) * plane);
+    const size_t src = (size_t)q * pop + (size_t)(p < 5 ? nz_alloc - 1 - hi : lo) * plane;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < plane;
+         i += (size_t)gridDim.x * blockDim.x)
+        f[dst + i] = f[src + i];
+}
+
+}  // namespace d3
+}  // namespace kb
+
+extern "C" int kb_slab_fill_ghosts_3d(void *f, int Nx, int Ny, int nz_alloc, int lo, int hi,
+                                      int dtype, void *stream) {
+    using namespace kb::d3;
+    KB_REQUIRE(f, "kb_slab_fill_ghosts_3d: null population pointer");
+    if (int e = check_dims("kb_slab_fill_ghosts_3d", Nx, Ny, nz_alloc)) return e;
+    KB_REQUIRE(nz_alloc >= 1 + (lo != 0) + (hi != 0),
+               "kb_slab_fill_ghosts_3d: %d planes hold no real plane besides the ghosts", nz_alloc);
+    const size_t plane = (size_t)Nx * Ny, pop = plane * (size_t)nz_alloc;
+    const size_t b = kb::dtype_bytes(dtype);
+    KB_REQUIRE(b != 0, "kb_slab_fill_ghosts_3d: unknown dtype %d", dtype);
+    const dim3 grid((unsigned)std::min<size_t>((plane + 255) / 256, 1024), 10);
+    cudaStream_t s = kb::as_stream(stream);
+    const int l = lo != 0, h = hi != 0;
+    if (b == 8) slab_ghosts_k<unsigned long long><<<grid, 256, 0, s>>>((unsigned long long *)f, plane, pop, nz_alloc, l, h);
+    else if (b == 4) slab_ghosts_k<unsigned int><<<grid, 256, 0, s>>>((unsigned int *)f, plane, pop, nz_alloc, l, h);
+    else slab_ghosts_k<unsigned short><<<grid, 256, 0, s>>>((unsigned short *)f, plane, pop, nz_alloc, l, h);
+    return kb::check_launch("kb_slab_fill_ghosts_3d");
+}

@@ -656,6 +656,15 @@ def stream_periodic_xz_wall_y_3d_(f_out, f_in, Nx, Ny, Nz):
          code, _stream())
 
 
+def slab_fill_ghosts_3d_(f, lo, hi, deviation=False):
+    """Ghost planes of a one-rank z-slab on a periodic z axis from the slab's
+    own end planes (kb_slab_fill_ghosts_3d); f is (19, nz_alloc, Ny, Nx)."""
+    if f.dim() != 4 or f.shape[0] != 19 or not f.is_contiguous():
+        raise ValueError("f must be a contiguous (19, nz_alloc, Ny, Nx) tensor")
+    call("kb_slab_fill_ghosts_3d", _t(f, "f"), f.shape[3], f.shape[2], f.shape[1], int(bool(lo)),
+         int(bool(hi)), storage_dtype(f, deviation), _stream())
+
+
 def collide_guo_3d_(f, is_solid, omega, Fx, Fy, Fz):
     """collide_guo_3d! -- src/kernels/collide_guo_3d.jl:190"""
     code = _plain(f)

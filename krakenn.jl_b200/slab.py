@@ -1,0 +1,197 @@
+"""One D3Q19 grid over several GPUs: slab decomposition along z.
+
+The reference runs one grid on one device and has no distributed backend;
+this module is the B200 extension for grids larger than one GPU (or to
+shorten time to solution).  Rank r of R owns the z-planes [z0, z1) of the
+global Nx x Ny x Nz grid, stored in the library's layout f[q][k][j][i] with
+one ghost plane below and one above wherever a neighbouring slab exists
+(always on a periodic z axis, where the slabs form a ring; not at a global
+z wall).
+
+A pull step of node (i, j, k) reads population q from (i, j, k) - c_q, so
+the planes next to a slab face need, from the neighbouring slab, only the
+five populations that cross that face: c_z = +1 (q = 5, 11, 12, 15, 16)
+from the plane below, c_z = -1 (q = 6, 13, 14, 17, 18) from the plane
+above.  Each population's plane is contiguous in this layout, so the
+exchange after every step sends ten contiguous planes per interior face
+(five each way) with no packing: NCCL point-to-point over NVLink on GPUs,
+gloo on CPU.
+
+The local step is the library's fused step on the whole local array with a
+non-periodic z axis (x and y as on the global grid).  The real planes then
+pull across into the ghost planes, which hold exactly the neighbour's
+populations; the ghost planes themselves are updated with meaningless
+values that nothing reads and the next exchange overwrites; a slab that
+ends at a global z wall keeps the step's own half-way bounce-back there.
+Every storage and kernel variant of kb_fused_trt_step_3d thus runs
+unchanged, and a round-to-nearest storage gives the full-grid result bit
+for bit.  The cost is two ghost planes of work per slab.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+# populations that cross a z face upward (c_z = +1) and downward (c_z = -1)
+CZP = (5, 11, 12, 15, 16)
+CZM = (6, 13, 14, 17, 18)
+
+
+@dataclass(frozen=True)
+class Slab:
+    """Rank `rank`'s part of a grid of `Nz` planes split over `world` ranks."""
+
+    Nz: int
+    world: int
+    rank: int
+    periodic_z: bool
+
+    def __post_init__(self):
+        if self.world < 1 or not 0 <= self.rank < self.world:
+            raise ValueError(f"bad rank {self.rank} of world {self.world}")
+        if self.Nz < self.world:
+            raise ValueError(f"{self.Nz} z-planes cannot be split over {self.world} ranks")
+
+    @property
+    def z0(self) -> int:
+        """First global z-plane of this slab (planes split as evenly as possible)."""
+        q, r = divmod(self.Nz, self.world)
+        return self.rank * q + min(self.rank, r)
+
+    @property
+    def z1(self) -> int:
+        q, r = divmod(self.Nz, self.world)
+        return self.z0 + q + (1 if self.rank < r else 0)
+
+    @property
+    def nz(self) -> int:
+        """Real planes of this slab."""
+        return self.z1 - self.z0
+
+    @property
+    def lo(self) -> bool:
+        """A ghost plane below (a neighbouring slab under this one)."""
+        return self.periodic_z or self.rank > 0
+
+    @property
+    def hi(self) -> bool:
+        """A ghost plane above."""
+        return self.periodic_z or self.rank < self.world - 1
+
+    @property
+    def nz_alloc(self) -> int:
+        """Planes of the local arrays: real planes plus ghosts."""
+        return self.nz + int(self.lo) + int(self.hi)
+
+    @property
+    def k0(self) -> int:
+        """Local index of the first real plane."""
+        return int(self.lo)
+
+    @property
+    def up(self) -> int:
+        return (self.rank + 1) % self.world
+
+    @property
+    def down(self) -> int:
+        return (self.rank - 1) % self.world
+
+    def global_planes(self):
+        """Global z index of every local plane (ghosts included, wrapped)."""
+        return [(self.z0 - self.k0 + k) % self.Nz for k in range(self.nz_alloc)]
+
+    def local_from_global(self, full):
+        """The local array (ghosts filled) cut from a full-grid array whose
+        z axis is dimension -3, e.g. populations (Q, Nz, Ny, Nx) or moments
+        (Nz, Ny, Nx)."""
+        return full[..., self.global_planes(), :, :].clone() if hasattr(full, "clone") else \
+            full[..., self.global_planes(), :, :].copy()
+
+    def real(self, local):
+        """View of the real planes of a local array (z axis dimension -3)."""
+        return local[..., self.k0:self.k0 + self.nz, :, :]
+
+
+def exchange(f, slab: Slab, group=None):
+    """Fill the ghost planes of the local populations `f` (19, nz_alloc, Ny,
+    Nx) from the neighbouring slabs, after a step wrote `f`.  With one rank
+    the ghosts of a periodic z axis are copies of the slab's own end planes.
+    Every rank must call this at the same point of its step sequence."""
+    if slab.world == 1:
+        if not (slab.lo or slab.hi):
+            return
+        if getattr(f, "is_cuda", False):  # one launch for the ten planes
+            import torch
+            from . import ops
+            ops.slab_fill_ghosts_3d_(f, slab.lo, slab.hi,
+                                     deviation=f.dtype in (torch.float16, torch.bfloat16))
+            return
+        exchange_in_process([f], [slab])
+        return
+    import torch.distributed as dist
+    top, bot, ghost_hi = slab.k0 + slab.nz - 1, slab.k0, slab.nz_alloc - 1
+    p2p = []
+    # one fixed order on every rank: upward sends, upward receives,
+    # downward sends, downward receives, each in population order, so the
+    # matching per peer pair is the same even when up == down (two ranks)
+    if slab.hi:
+        p2p += [dist.P2POp(dist.isend, f[q, top], slab.up, group) for q in CZP]
+    if slab.lo:
+        p2p += [dist.P2POp(dist.irecv, f[q, 0], slab.down, group) for q in CZP]
+    if slab.lo:
+        p2p += [dist.P2POp(dist.isend, f[q, bot], slab.down, group) for q in CZM]
+    if slab.hi:
+        p2p += [dist.P2POp(dist.irecv, f[q, ghost_hi], slab.up, group) for q in CZM]
+    if p2p:
+        for req in dist.batch_isend_irecv(p2p):
+            req.wait()
+
+
+def exchange_in_process(fs, slabs):
+    """The exchange of `exchange` for all slabs of one grid held by one
+    process (a list of local arrays, one per slab, e.g. to run a grid in
+    slabs on one GPU or to check the decomposition against the full grid)."""
+    R = len(slabs)
+    for r, (f, s) in enumerate(zip(fs, slabs)):
+        if s.lo:
+            below, sb = fs[(r - 1) % R], slabs[(r - 1) % R]
+            for q in CZP:
+                f[q, 0] = below[q, sb.k0 + sb.nz - 1]
+        if s.hi:
+            above, sa = fs[(r + 1) % R], slabs[(r + 1) % R]
+            for q in CZM:
+                f[q, s.nz_alloc - 1] = above[q, sa.k0]
+
+
+class SlabTRT3D:
+    """The fused D3Q19 TRT step of one slab: kb_fused_trt_step_3d on the
+    local array (z non-periodic), then the ghost exchange of its output.
+
+    `step_fn(f_out, f_in, moments, mask)` replaces the library step (a test
+    plugs the oracle in here); by default the CUDA step runs with the given
+    nu, Lambda, x/y periodicity, storage options.  `moments` is None or four
+    local (nz_alloc, Ny, Nx) arrays whose real planes receive rho, ux, uy,
+    uz."""
+
+    def __init__(self, slab: Slab, Nx, Ny, nu=None, Lambda=3 / 16, periodic_xy=(False, False),
+                 deviation=False, stochastic_rounding=False, mask=None, group=None,
+                 step_fn=None):
+        self.slab, self.Nx, self.Ny = slab, Nx, Ny
+        self.mask, self.group = mask, group
+        if step_fn is None:
+            from . import ops
+            per = (bool(periodic_xy[0]), bool(periodic_xy[1]), False)
+
+            def step_fn(f_out, f_in, moments, mask):
+                m = moments if moments is not None else (None,) * 4
+                ops.fused_trt_step_3d_(f_out, f_in, *m, mask, Nx, Ny, slab.nz_alloc, nu, Lambda,
+                                       periodic=per, deviation=deviation,
+                                       stochastic_rounding=stochastic_rounding)
+        self.step_fn = step_fn
+
+    def shape(self):
+        return (19, self.slab.nz_alloc, self.Ny, self.Nx)
+
+    def step(self, f_out, f_in, moments=None):
+        """One step f_in -> f_out; afterwards f_out's ghosts are current."""
+        self.step_fn(f_out, f_in, moments, self.mask)
+        exchange(f_out, self.slab, self.group)
