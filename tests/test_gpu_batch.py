@@ -45,6 +45,45 @@ def test_batch_matches_single_case_oracle(cuda, pkg, orc, storage, tol):
     b.close()
 
 
+@pytest.mark.parametrize("storage,tol", [("f32", 2e-6), ("f16", 3e-3), ("bf16sr", 3e-2)])
+def test_batch_larger_cases_match_single_case_oracle(cuda, pkg, orc, storage, tol):
+    """Cases of N = 64 .. 128 (several 2048-node tiles per case, tiles that
+    start mid-row for N = 72 and 96) beside N = 66 and the odd N = 65 match the
+    FP64 oracle after 200 steps."""
+    N = np.array([64, 72, 128, 96, 66, 65], np.int32)
+    nu = np.array([0.05, 0.04, 0.02, 0.1, 0.03, 0.05])
+    u = np.array([0.1, 0.07, 0.05, 0.08, 0.1, 0.09])
+    b = pkg.CavityBatch(N, nu, u, storage)
+    b.run(max_steps=200, check_every=100, tol=0.0, tile_nodes=2048)
+    st = b.status()
+    assert not st["timed_out"] and st["live_tiles"] == 0
+    for c in range(len(N)):
+        r = b.case(c)
+        assert r["steps"] == 200 and r["state"] == "max_steps"
+        ux, uy = _oracle_mrt_cavity(orc, int(N[c]), nu[c], u[c], 200)
+        err = max(np.max(np.abs(r["ux"] - ux)), np.max(np.abs(r["uy"] - uy))) / u[c]
+        assert err < tol, (c, err)
+    b.close()
+
+
+@pytest.mark.parametrize("storage", ["f16", "f32"])
+def test_batch_fields_independent_of_tile_size(cuda, pkg, storage):
+    """The tile size only changes which block updates which nodes: runs with
+    256- and 4096-node tiles give the same fields bit for bit."""
+    N = np.array([64, 96, 128, 160, 72], np.int32)
+    nu = np.array([0.05, 0.04, 0.02, 0.1, 0.03])
+    u = np.array([0.1, 0.07, 0.05, 0.08, 0.1])
+    out = []
+    for tn in (256, 4096):
+        b = pkg.CavityBatch(N, nu, u, storage)
+        b.run(max_steps=300, check_every=100, tol=0.0, tile_nodes=tn)
+        assert not b.status()["timed_out"]
+        out.append([b.case(c) for c in range(len(N))])
+        b.close()
+    for a, c in zip(*out):
+        assert np.array_equal(a["ux"], c["ux"]) and np.array_equal(a["uy"], c["uy"])
+
+
 def test_batch_retires_converged_and_nonfinite(cuda, pkg):
     """A viscous small cavity converges and retires early; a case with
     nu -> 0 on a coarse grid blows up and is retired as non-finite; a slow
