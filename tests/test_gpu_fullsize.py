@@ -1,0 +1,92 @@
+"""The D3Q19 TRT step at the bench's full size (256^3 periodic Taylor-Green,
+Lambda = 1/4, nu = 0.01, u0 = 0.05), through size-independent properties:
+the staged row-tile kernel equals the x / x+32 pair kernel bit for bit, the
+total mass stays put, the velocity decays as exp(-2 nu k^2 t), and the FP64
+step equals the oracle bit for bit on full 256 x 256 planes."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+N, NU, LAM, U0 = 256, 0.01, 0.25, 0.05
+
+
+def _tgv(pkg, dtype, deviation, Nz=N):
+    plane = torch.from_numpy(np.ascontiguousarray(
+        pkg.drivers.taylor_green_3d_populations(N, U0, Nz=1))).cuda()
+    f = torch.empty((19, Nz, N, N), dtype=dtype, device="cuda")
+    pkg.convert_populations(f, plane.expand(19, Nz, N, N).contiguous(), dst_deviation=deviation)
+    return f
+
+
+def _run(pkg, f, steps, deviation, sr=False, mom=None, Nz=N):
+    g = torch.empty_like(f)
+    for s in range(steps):
+        m = mom if (mom is not None and s == steps - 1) else (None,) * 4
+        pkg.fused_trt_step_3d_(g, f, *m, None, N, N, Nz, NU, LAM, periodic=(1, 1, 1),
+                               deviation=deviation, stochastic_rounding=sr)
+        f, g = g, f
+    return f
+
+
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
+def test_staged_equals_pair_kernel_at_256cubed(cuda, pkg, dtype):
+    outs = []
+    try:
+        for variant in (5, 2):
+            pkg.set_trt3d_variant(variant)
+            outs.append(_run(pkg, _tgv(pkg, dtype, True), 20, True))
+    finally:
+        pkg.set_trt3d_variant(0)
+    assert torch.equal(outs[0], outs[1])
+    assert not pkg.staged_step_timed_out()
+
+
+@pytest.mark.parametrize("dtype,sr,bound", [(torch.float32, False, 5e-8), (torch.float16, True, 1e-7)])
+def test_mass_conserved_at_256cubed(cuda, pkg, dtype, sr, bound):
+    """The TRT collision conserves mass and the periodic pull moves it, so
+    the FP64 total changes only by rounding: |dm| / N^3 after 50 steps below
+    `bound`.  FP32 round-to-nearest drifts one way (measured 0.19 in
+    1.7e7 over 50 steps, 2.2e-10 per node and step); FP16 with stochastic
+    rounding has zero-mean rounding."""
+    f = _tgv(pkg, dtype, True)
+    m0 = pkg.mass(f, deviation=True)
+    f = _run(pkg, f, 50, True, sr=sr)
+    m1 = pkg.mass(f, deviation=True)
+    assert abs(m1 - m0) / N ** 3 < bound, (m0, m1)
+
+
+def test_velocity_decays_as_analytic_at_256cubed(cuda, pkg):
+    """u(t) / u(0) = exp(-2 nu k^2 t) for the Taylor-Green vortex; after 500
+    steps of FP32 deviations the velocity matches the decayed analytic field
+    to the discretisation error (relative L2 < 2e-3)."""
+    steps = 500
+    f = _tgv(pkg, torch.float32, True)
+    mom = [torch.empty((N, N, N), dtype=torch.float32, device="cuda") for _ in range(4)]
+    _run(pkg, f, steps, True, mom=mom)
+    k = 2 * math.pi / N
+    x = torch.arange(N, dtype=torch.float64, device="cuda")
+    # the moments are those of the last step's input: t = steps - 1
+    decay = math.exp(-2 * NU * k * k * (steps - 1))
+    ux = (-U0 * torch.cos(k * x)[None, None, :] * torch.sin(k * x)[None, :, None] * decay)
+    err = torch.linalg.vector_norm(mom[1].double() - ux) / torch.linalg.vector_norm(ux.expand(N, N, N))
+    assert float(err) < 2e-3, float(err)
+    assert float(mom[3].abs().max()) < 1e-6
+
+
+def test_fp64_equals_oracle_on_full_planes(cuda, pkg, orc):
+    """FP64 step vs the oracle (C restatement of the reference CPU path) on
+    256 x 256 x 32 nodes, 3 steps: bit for bit."""
+    Nz, steps = 32, 3
+    f = _tgv(pkg, torch.float64, False, Nz=Nz)
+    ref = f.cpu().numpy()
+    got = _run(pkg, f, steps, False, Nz=Nz).cpu().numpy()
+    sp, sm = orc.trt_rates(NU, LAM)
+    g = np.empty_like(ref)
+    for _ in range(steps):
+        orc.fused_trt_3d(g, ref, None, None, sp, sm, (1, 1, 1))
+        ref, g = g, ref
+    assert np.array_equal(got, ref)
