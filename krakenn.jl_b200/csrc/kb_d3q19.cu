@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(LT) links_count_k(uint8_t *cls, int *counts, c
 }
 
 template <typename T>
-__global__ void __launch_bounds__(LT) links_fill_k(int *rec, T *tq, T *tx, T *ty, T *tz,
+__global__ void __launch_bounds__(LT) links_fill_k(int *rec, int *node, T *tq, T *tx, T *ty, T *tz,
                                                    const uint8_t *cls, const int *offsets,
                                                    const T *qw, const T *wx, const T *wy,
                                                    const T *wz, size_t nodes, long long n_rec) {
@@ -328,6 +328,7 @@ __global__ void __launch_bounds__(LT) links_fill_k(int *rec, T *tq, T *tx, T *ty
     const long long r = (long long)offsets[blockIdx.x] + warp_base[warp] +
                         __popc(bal & ((1u << lane) - 1u));
     rec[n] = (int)r;
+    node[r] = (int)n;
     for (int q = 1; q < 19; ++q) {
         const long long t = (long long)(q - 1) * n_rec + r;
         tq[t] = qw[q * nodes + n];
@@ -988,6 +989,7 @@ struct kb_libb_links {
     int Nx = 0, Ny = 0, Nz = 0, dtype = KB_F64;
     uint8_t *cls = nullptr;
     int *rec = nullptr;
+    int *node = nullptr;  // node of each record
     void *qw = nullptr, *wx = nullptr, *wy = nullptr, *wz = nullptr;
     long long n_rec = 0;
 };
@@ -995,7 +997,7 @@ struct kb_libb_links {
 namespace {
 
 kb::d3::LinkTable3 table_view(const kb_libb_links *L) {
-    return kb::d3::LinkTable3{L->cls, L->rec, L->qw, L->wx, L->wy, L->wz, L->n_rec};
+    return kb::d3::LinkTable3{L->cls, L->rec, L->qw, L->wx, L->wy, L->wz, L->n_rec, L->node};
 }
 
 template <typename T>
@@ -1032,13 +1034,14 @@ int build_links(kb_libb_links *L, const uint8_t *solid, const T *qw, const T *wx
     e = cudaMemcpyAsync(counts, h.data(), nblk * sizeof(int), cudaMemcpyHostToDevice, s);
     if (acc > 0 && e == cudaSuccess) {
         const size_t bytes = (size_t)acc * 18 * sizeof(T);
-        e = cudaMalloc(&L->qw, bytes);
+        e = cudaMalloc(&L->node, (size_t)acc * sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc(&L->qw, bytes);
         if (e == cudaSuccess) e = cudaMalloc(&L->wx, bytes);
         if (e == cudaSuccess) e = cudaMalloc(&L->wy, bytes);
         if (e == cudaSuccess) e = cudaMalloc(&L->wz, bytes);
         if (e == cudaSuccess)
             kb::d3::links_fill_k<T><<<(unsigned)nblk, kb::d3::LT, 0, s>>>(
-                L->rec, (T *)L->qw, (T *)L->wx, (T *)L->wy, (T *)L->wz, L->cls, counts, qw, wx,
+                L->rec, L->node, (T *)L->qw, (T *)L->wx, (T *)L->wy, (T *)L->wz, L->cls, counts, qw, wx,
                 wy, wz, nodes, acc);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -1069,7 +1072,7 @@ extern "C" {
 
 int kb_libb_links_destroy(kb_libb_links *L) {
     if (!L) return KB_OK;
-    cudaFree(L->cls); cudaFree(L->rec);
+    cudaFree(L->cls); cudaFree(L->rec); cudaFree(L->node);
     cudaFree(L->qw); cudaFree(L->wx); cudaFree(L->wy); cudaFree(L->wz);
     delete L;
     return KB_OK;
@@ -1136,7 +1139,7 @@ int kb_fused_trt_libb_links_step_3d(void *f_out, const void *f_in, void *rho, vo
                                  "need a KB_F32 cut-link table", what);
         return kb::d3::launch_trt3d_dev_links(dtype, f_out, f_in, (float *)rho, (float *)ux,
                                               (float *)uy, (float *)uz, T3, g, (float)sp,
-                                              (float)sm, s);
+                                              (float)sm, s, g_trt3d_dev_variant);
     }
     return kb::set_error(KB_ERR_UNSUPPORTED, "%s: unknown dtype %d", what, dtype);
 }

@@ -170,6 +170,7 @@ struct LinkTable3 {
     const int *rec;                  // record of each cls == 2 node
     const void *qw, *wx, *wy, *wz;   // link q = 1..18 of record r at [(q - 1) * n_rec + r]
     long long n_rec;
+    const int *node;                 // node of each record
 };
 
 // One record of the table, read like LinkDense.
@@ -189,10 +190,12 @@ __device__ __forceinline__ LinkRecord<T> link_record(const LinkTable3 &L, int r)
                          (const T *)L.wz + r, L.n_rec};
 }
 
-// Deviation-storage step with the compact cut-link table (kb_d3q19_dev.cu).
+// Deviation-storage step with the compact cut-link table (kb_d3q19_dev.cu);
+// `variant` follows kernel 1 of kb_set_kernel_variant (0 automatic, 5 the
+// staged row tiles for 16-bit storages, anything else one node per thread).
 int launch_trt3d_dev_links(int dtype, void *f_out, const void *f_in, float *rho, float *ux,
                            float *uy, float *uz, const LinkTable3 &L, const Grid3 &g, float sp,
-                           float sm, cudaStream_t s);
+                           float sm, cudaStream_t s, int variant);
 
 // Launchers of the fused TRT step for the deviation storages
 // (kb_d3q19_dev.cu); `per` = periodic bit mask.

@@ -20,6 +20,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "kb_d3q19.cuh"
 
@@ -658,7 +659,8 @@ constexpr int THALO = 64;               // halo slot stride (elements, 128 bytes
 constexpr int TSTAGES = 4;
 constexpr int TCONS = TT / 2;           // consumer threads: one per adjacent node pair
 constexpr int TTHREADS = TCONS + 32;    // + the producer warp
-constexpr int TSTAGE = 19 * TT + 10 * THALO;  // elements per stage (row q at q * TT)
+constexpr int TCLS = 19 * TT + 10 * THALO;     // element offset of the class-byte run (cut-link steps)
+constexpr int TSTAGE = TCLS + TT / 2;           // elements per stage (row q at q * TT)
 constexpr size_t TSMEM = 128 + (size_t)TSTAGES * TSTAGE * 2;  // + alignment slack
 constexpr uint32_t TBYTES = 19u * TT * 2u + 10u * 8u * 2u;   // transaction bytes of a staged tile
 constexpr long long TWAIT = 4000000;    // bounded mbarrier wait (polls)
@@ -736,11 +738,22 @@ struct TileMap {
 // row run, th an 8-element halo run of one plane.
 struct TileMaps {
     const CUtensorMap *t1, *t2, *t3, *th;
+    const CUtensorMap *tc;  // the row's class bytes of a cut-link table, or null
 };
+__device__ __forceinline__ void tma_load3(uint32_t dst, const CUtensorMap *tm, int x, int y, int z,
+                                          uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(bar)
+        : "memory");
+}
 __device__ __forceinline__ void tma_issue_tile(const TileMaps &mp, uint32_t dst, uint32_t bar,
                                                int x0, int j, int k, const TileMap &m) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(TBYTES)
+    const uint32_t bytes = TBYTES + (mp.tc ? (uint32_t)TT : 0u);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                  : "memory");
+    if (mp.tc) tma_load3(dst + TCLS * 2, mp.tc, x0, j, k, bar);  // own row's class bytes
     const int ym = j > 0 ? j - 1 : m.Ny - 1, yp = j < m.Ny - 1 ? j + 1 : 0;
     const int zm = k > 0 ? k - 1 : m.Nz - 1, zp = k < m.Nz - 1 ? k + 1 : 0;
     const uint32_t R = TT * 2;  // bytes per staged row
@@ -776,13 +789,54 @@ __device__ __forceinline__ void tma_issue_tile(const TileMaps &mp, uint32_t dst,
     }
 }
 
-template <typename R, bool MOM, bool SOLID, typename I, bool SR>
+// The cut nodes of a compact link table (class 2), one thread per record:
+// the same pull, interpolated bounce-back and collision as the one-node
+// kernel trt_dev_links_k.  The staged step stores every other node, so the
+// two kernels write disjoint nodes, read only f_in, and run side by side.
+template <typename R, bool MOM, typename I, bool SR>
+__global__ void __launch_bounds__(BX) trt_dev_cut_k(R *__restrict__ fo, const R *__restrict__ fi,
+                                                     float *__restrict__ rho_o, float *__restrict__ ux_o,
+                                                     float *__restrict__ uy_o, float *__restrict__ uz_o,
+                                                     LinkTable3 L, Grid3 g, float sp, float sm) {
+    const long long r = (long long)blockIdx.x * BX + threadIdx.x;
+    if (r >= L.n_rec) return;
+    const size_t c = (size_t)L.node[r];
+    const size_t row = c / (size_t)g.Nx;
+    const int i = (int)(c - row * (size_t)g.Nx), j = (int)(row % (size_t)g.Ny),
+              k = (int)(row / (size_t)g.Ny);
+    const I P = (I)g.plane;
+    float d[19];
+    pull19_at(fi + c, P, pull_geometry<I>(g, i, j, k), d, DevLoad<R>());
+    libb_prephase_3d(fi + c, P, link_record<float>(L, (int)r), d, DevLoad<R>());
+    float o[19], rho, ux, uy, uz;
+    trt_dev_collide(d, o, rho, ux, uy, uz, sp, sm);
+    R *__restrict__ o0 = fo + c;
+    if (SR) {
+        const uint32_t key =
+            hash32((uint32_t)c ^ hash32(*(volatile const unsigned int *)&g_sr_epoch + 0x632BE5ABu));
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            const uint32_t v = SRPack<R>::pack(o[q], 0.f, sr_bits(key, q));
+            reinterpret_cast<unsigned short *>(o0)[q * P] = (unsigned short)(v & 0xFFFFu);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 19; ++q) o0[q * P] = Dev<R>::st(o[q]);
+    }
+    if (MOM) { rho_o[c] = rho; ux_o[c] = ux; uy_o[c] = uy; uz_o[c] = uz; }
+}
+
+// LINKS: the compact cut-link table (row f1) in place of a solid mask: class
+// 1 nodes are solid; class 2 nodes are left to trt_dev_cut_k.
+template <typename R, bool MOM, bool SOLID, typename I, bool SR, bool LINKS = false>
 __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
     trt_dev_tma_k(const __grid_constant__ CUtensorMap tmap1, const __grid_constant__ CUtensorMap tmap2,
                   const __grid_constant__ CUtensorMap tmap3, const __grid_constant__ CUtensorMap thalo,
+                  const __grid_constant__ CUtensorMap tcls,
                   R *__restrict__ fo, const R *__restrict__ fi, float *__restrict__ rho_o,
                   float *__restrict__ ux_o, float *__restrict__ uy_o, float *__restrict__ uz_o,
-                  const uint8_t *__restrict__ solid, Grid3 g, float sp, float sm) {
+                  const uint8_t *__restrict__ solid, Grid3 g, float sp, float sm, LinkTable3 L) {
+    constexpr bool HS = SOLID || LINKS;  // some nodes are solid
     constexpr int CX[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
     extern __shared__ unsigned char tsm_raw[];
     __shared__ __align__(8) uint64_t full[TSTAGES], empty[TSTAGES];
@@ -809,12 +863,14 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
 
     if (t >= TCONS) {
         // ------------------------------------------------ producer warp --
-        const TileMaps mp{&tmap1, &tmap2, &tmap3, &thalo};
+        const TileMaps mp{&tmap1, &tmap2, &tmap3, &thalo, LINKS ? &tcls : nullptr};
         if (t == TCONS) {
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap1)) : "memory");
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap2)) : "memory");
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap3)) : "memory");
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&thalo)) : "memory");
+            if (LINKS)
+                asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tcls)) : "memory");
         }
 #pragma unroll 1
         for (int n = 0; ck < g.Nz; m.advance(cx, cj, ck), ++n) {
@@ -849,6 +905,7 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
         const int iA = x0 + 2 * t;
         const bool live = iA < g.Nx;  // Nx even: both nodes of the pair or neither
         const size_t cA = (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k) + iA;
+        uchar2 cl = make_uchar2(0, 0);  // LINKS: the pair's class bytes
         if (!tbar_wait(s_addr(&full[s]), (uint32_t)(it / TSTAGES) & 1u)) {
             atomicExch(&g_tma_timeout, 1);
             aborted = true;
@@ -856,6 +913,9 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
         }
         float2 d[19];
         if (m.staged(j, k)) {
+            if (LINKS)
+                cl = *reinterpret_cast<const uchar2 *>(
+                    reinterpret_cast<const unsigned char *>(stage0 + s * TSTAGE + TCLS) + 2 * t);
             const R *st = stage0 + s * TSTAGE + 2 * t;
             const DevLoad<R> ld;
 #pragma unroll
@@ -880,6 +940,7 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
             }
         } else if (live) {
             // rows at a y or z wall: direct pull of both nodes
+            if (LINKS) cl = *reinterpret_cast<const uchar2 *>(L.cls + cA);
             float a[19], b[19];
             pull19_at(fi + cA, P, pull_geometry<I>(g, iA, j, k), a, DevLoad<R>());
             pull19_at(fi + cA + 1, P, pull_geometry<I>(g, iA + 1, j, k), b, DevLoad<R>());
@@ -889,6 +950,12 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
         __syncwarp();
         if ((t & 31) == 0) tbar_arrive(s_addr(&empty[s]));  // this warp is done with stage s
         if (!live) continue;
+        uchar2 sm2 = make_uchar2(0, 0);
+        if (LINKS) {
+            sm2 = make_uchar2(cl.x == 1, cl.y == 1);
+        } else if (SOLID) {
+            sm2 = *reinterpret_cast<const uchar2 *>(solid + cA);
+        }
         // the rates pass through opaque moves each tile so the collision's
         // rate-derived constants are formed here, not held across the loop
         float spl, sml;
@@ -896,31 +963,59 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
         asm volatile("mov.b32 %0, %1;" : "=f"(sml) : "f"(sm));
         float2 o[19], rho, ux, uy, uz;
         trt_dev_collide(d, o, rho, ux, uy, uz, spl, sml);
-        uchar2 sm2 = make_uchar2(0, 0);
-        if (SOLID) sm2 = *reinterpret_cast<const uchar2 *>(solid + cA);
         // likewise the plane stride, so the 19 plane offsets are not hoisted
         I Pl;
         if constexpr (sizeof(I) == 4) asm volatile("mov.b32 %0, %1;" : "=r"(Pl) : "r"((int)P));
         else asm volatile("mov.b64 %0, %1;" : "=l"(Pl) : "l"((long long)P));
         R *o0 = fo + cA;
+        if (LINKS && (cl.x == 2 || cl.y == 2)) {
+            // a pair with a cut node: trt_dev_cut_k writes that node (it runs
+            // beside this kernel), so only the other node is stored here
+            const bool wA = cl.x != 2, wB = cl.y != 2;
+            const uint32_t key = SR ? hash32((uint32_t)cA ^ ekey) : 0u;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) {
+                const float vA = sm2.x ? 0.f : o[q].x, vB = sm2.y ? 0.f : o[q].y;
+                unsigned short *w = reinterpret_cast<unsigned short *>(o0 + (I)q * Pl);
+                if (SR) {
+                    const uint32_t v = SRPack<R>::pack(vA, vB, sr_bits(key, q));
+                    if (wA) w[0] = (unsigned short)(v & 0xFFFFu);
+                    if (wB) w[1] = (unsigned short)(v >> 16);
+                } else {
+                    if (wA) o0[(I)q * Pl] = Dev<R>::st(vA);
+                    if (wB) o0[(I)q * Pl + 1] = Dev<R>::st(vB);
+                }
+            }
+            if (MOM) {
+                if (wA) {
+                    rho_o[cA] = sm2.x ? 1.f : rho.x; ux_o[cA] = sm2.x ? 0.f : ux.x;
+                    uy_o[cA] = sm2.x ? 0.f : uy.x; uz_o[cA] = sm2.x ? 0.f : uz.x;
+                }
+                if (wB) {
+                    rho_o[cA + 1] = sm2.y ? 1.f : rho.y; ux_o[cA + 1] = sm2.y ? 0.f : ux.y;
+                    uy_o[cA + 1] = sm2.y ? 0.f : uy.y; uz_o[cA + 1] = sm2.y ? 0.f : uz.y;
+                }
+            }
+            continue;
+        }
         if (SR) {
             const uint32_t key = hash32((uint32_t)cA ^ ekey);
 #pragma unroll
             for (int q = 0; q < 19; ++q) {
-                const uint32_t v = SRPack<R>::pack(SOLID && sm2.x ? 0.f : o[q].x,
-                                                   SOLID && sm2.y ? 0.f : o[q].y, sr_bits(key, q));
+                const uint32_t v = SRPack<R>::pack(HS && sm2.x ? 0.f : o[q].x,
+                                                   HS && sm2.y ? 0.f : o[q].y, sr_bits(key, q));
                 *reinterpret_cast<uint32_t *>(o0 + (I)q * Pl) = v;
             }
         } else {
 #pragma unroll
             for (int q = 0; q < 19; ++q)
-                Vec2<R>::st(o0 + (I)q * Pl, make_float2(SOLID && sm2.x ? 0.f : o[q].x,
-                                                        SOLID && sm2.y ? 0.f : o[q].y));
+                Vec2<R>::st(o0 + (I)q * Pl, make_float2(HS && sm2.x ? 0.f : o[q].x,
+                                                        HS && sm2.y ? 0.f : o[q].y));
         }
         if (MOM) {
             float2 r = rho, a = ux, b = uy, c = uz;
-            if (SOLID && sm2.x) { r.x = 1.f; a.x = b.x = c.x = 0.f; }
-            if (SOLID && sm2.y) { r.y = 1.f; a.y = b.y = c.y = 0.f; }
+            if (HS && sm2.x) { r.x = 1.f; a.x = b.x = c.x = 0.f; }
+            if (HS && sm2.y) { r.y = 1.f; a.y = b.y = c.y = 0.f; }
             *reinterpret_cast<float2 *>(rho_o + cA) = r;
             *reinterpret_cast<float2 *>(ux_o + cA) = a;
             *reinterpret_cast<float2 *>(uy_o + cA) = b;
@@ -967,17 +1062,17 @@ static bool tma_eligible(const Grid3 &g, const void *f_out, const void *f_in, co
 // Maps of one population buffer: [0..2] 256-element row runs of 1, 2 and 3
 // consecutive planes, [3] 8-element halo runs of one plane.
 struct TmaMaps {
-    CUtensorMap m[4];
+    CUtensorMap m[5];  // [4]: class bytes of a cut-link table (x, y, z) 256-byte runs
 };
 
-template <typename R, bool MOM, bool SOLID, typename I, bool SR>
+template <typename R, bool MOM, bool SOLID, typename I, bool SR, bool LINKS = false>
 static int launch_tma_k(const TmaMaps &mp, R *fo, const R *fi, float *rho, float *ux, float *uy,
                         float *uz, const uint8_t *solid, const Grid3 &g, float sp, float sm,
-                        cudaStream_t s) {
+                        cudaStream_t s, const LinkTable3 &L = LinkTable3{}) {
     static int occ = -1;  // resident blocks per SM of this instantiation
     if (occ < 0) {
         int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trt_dev_tma_k<R, MOM, SOLID, I, SR>,
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trt_dev_tma_k<R, MOM, SOLID, I, SR, LINKS>,
                                                           TTHREADS, TSMEM) != cudaSuccess || n < 1) {
             cudaGetLastError();
             n = 1;
@@ -989,14 +1084,15 @@ static int launch_tma_k(const TmaMaps &mp, R *fo, const R *fi, float *rho, float
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long tiles = (long long)((g.Nx + TT - 1) / TT) * g.Ny * g.Nz;
     const int blocks = (int)std::min<long long>(tiles, (long long)sms * occ);
-    trt_dev_tma_k<R, MOM, SOLID, I, SR><<<blocks, TTHREADS, TSMEM, s>>>(
-        mp.m[0], mp.m[1], mp.m[2], mp.m[3], fo, fi, rho, ux, uy, uz, solid, g, sp, sm);
+    trt_dev_tma_k<R, MOM, SOLID, I, SR, LINKS><<<blocks, TTHREADS, TSMEM, s>>>(
+        mp.m[0], mp.m[1], mp.m[2], mp.m[3], mp.m[4], fo, fi, rho, ux, uy, uz, solid, g, sp, sm, L);
     return KB_OK;
 }
 
 template <typename R, typename I, bool SR>
 static int launch_tma(void *f_out, const void *f_in, float *rho, float *ux, float *uy, float *uz,
-                      const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s) {
+                      const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s,
+                      const LinkTable3 *links = nullptr) {
     // the populations as a 4-D tensor (x, y, z, q) of 16-bit words
     TmaMaps mp;
     const cuuint64_t dims[4] = {(cuuint64_t)g.Nx, (cuuint64_t)g.Ny, (cuuint64_t)g.Nz, 19};
@@ -1014,8 +1110,26 @@ static int launch_tma(void *f_out, const void *f_in, float *rho, float *ux, floa
             return set_error(KB_ERR_CUDA, "kb_fused_trt_step_3d: cuTensorMapEncodeTiled failed (%d)",
                              (int)r);
     }
+    mp.m[4] = mp.m[3];  // unused placeholder unless a cut-link table is staged
+    if (links) {
+        const cuuint64_t cd[3] = {(cuuint64_t)g.Nx, (cuuint64_t)g.Ny, (cuuint64_t)g.Nz};
+        const cuuint64_t cs[2] = {(cuuint64_t)g.Nx, (cuuint64_t)g.Nx * g.Ny};
+        const cuuint32_t cb[3] = {TT, 1, 1};
+        const CUresult r = tma_encode_fn()(&mp.m[4], CU_TENSOR_MAP_DATA_TYPE_UINT8, 3,
+                                           const_cast<uint8_t *>(links->cls), cd, cs, cb, es,
+                                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS)
+            return set_error(KB_ERR_CUDA, "kb_fused_trt_libb_links_step_3d: cuTensorMapEncodeTiled "
+                             "failed (%d)", (int)r);
+    }
     R *fo = (R *)f_out;
     const R *fi = (const R *)f_in;
+    if (links) {
+        if (rho) return launch_tma_k<R, true, false, I, SR, true>(mp, fo, fi, rho, ux, uy, uz, nullptr, g, sp, sm, s, *links);
+        return launch_tma_k<R, false, false, I, SR, true>(mp, fo, fi, rho, ux, uy, uz, nullptr, g, sp, sm, s, *links);
+    }
     if (rho) {
         if (solid) return launch_tma_k<R, true, true, I, SR>(mp, fo, fi, rho, ux, uy, uz, solid, g, sp, sm, s);
         return launch_tma_k<R, true, false, I, SR>(mp, fo, fi, rho, ux, uy, uz, solid, g, sp, sm, s);
@@ -1144,10 +1258,79 @@ int launch_trt3d_dev(int dtype, void *f_out, const void *f_in, float *rho, float
     return check_launch("kb_fused_trt_step_3d");
 }
 
+// One side stream and a fork / join event pair per device, created on first
+// use and kept for the life of the process: the cut-node kernel of a staged
+// cut-link step runs there, beside the staged kernel.
+struct SideStream {
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    bool ok = false;
+};
+static SideStream *side_stream() {
+    static std::mutex mu;
+    static SideStream per_dev[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    SideStream &ss = per_dev[dev];
+    if (!ss.ok) {
+        if (cudaStreamCreateWithFlags(&ss.side, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        ss.ok = true;
+    }
+    return &ss;
+}
+
 template <typename R, bool SR>
-static void launch_links_r(void *f_out, const void *f_in, float *rho, float *ux, float *uy,
-                           float *uz, const LinkTable3 &L, const Grid3 &g, float sp, float sm,
-                           cudaStream_t s) {
+static int launch_links_r(void *f_out, const void *f_in, float *rho, float *ux, float *uy,
+                          float *uz, const LinkTable3 &L, const Grid3 &g, float sp, float sm,
+                          cudaStream_t s, int variant) {
+    if constexpr (sizeof(R) == 2) {
+        // the staged row tiles with the table, under the rules of the plain step
+        const int ntx = (g.Nx + TT - 1) / TT;
+        const bool fill = 10 * g.Nx >= 9 * ntx * TT;
+        // (the class-byte map needs a 16-byte row pitch: Nx % 16 == 0)
+        if ((variant == 5 || (variant == 0 && fill)) && g.Nx % 16 == 0 &&
+            ((uintptr_t)L.cls & 15) == 0 && tma_eligible(g, f_out, f_in, rho, ux, uy, uz, L.cls)) {
+            const bool i32 = offsets_fit_int(g, 19);
+            // the cut nodes on the side stream (forked from s, joined back
+            // before anything that follows on s), or on s itself
+            SideStream *ss = L.n_rec > 0 ? side_stream() : nullptr;
+            cudaStream_t cs = s;
+            if (ss && cudaEventRecord(ss->fork, s) == cudaSuccess &&
+                cudaStreamWaitEvent(ss->side, ss->fork, 0) == cudaSuccess)
+                cs = ss->side;
+            else
+                cudaGetLastError();
+            if (L.n_rec > 0) {
+                const unsigned nb = (unsigned)((L.n_rec + BX - 1) / BX);
+                R *fo = (R *)f_out;
+                const R *fi = (const R *)f_in;
+                if (i32) {
+                    if (rho) trt_dev_cut_k<R, true, int, SR><<<nb, BX, 0, cs>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
+                    else trt_dev_cut_k<R, false, int, SR><<<nb, BX, 0, cs>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
+                } else {
+                    if (rho) trt_dev_cut_k<R, true, long long, SR><<<nb, BX, 0, cs>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
+                    else trt_dev_cut_k<R, false, long long, SR><<<nb, BX, 0, cs>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
+                }
+            }
+            const int rc = i32 ? launch_tma<R, int, SR>(f_out, f_in, rho, ux, uy, uz, nullptr, g, sp, sm, s, &L)
+                               : launch_tma<R, long long, SR>(f_out, f_in, rho, ux, uy, uz, nullptr, g, sp, sm, s, &L);
+            if (cs != s && (cudaEventRecord(ss->join, cs) != cudaSuccess ||
+                            cudaStreamWaitEvent(s, ss->join, 0) != cudaSuccess))
+                return set_error(KB_ERR_CUDA, "kb_fused_trt_libb_links_step_3d: joining the cut-node stream failed");
+            if (rc != KB_OK) return rc;
+            if (SR) sr_advance_k<<<1, 1, 0, s>>>();
+            return KB_OK;
+        }
+    }
     const dim3 grid((g.Nx + BX - 1) / BX, g.Ny, g.Nz);
     R *fo = (R *)f_out;
     const R *fi = (const R *)f_in;
@@ -1159,19 +1342,22 @@ static void launch_links_r(void *f_out, const void *f_in, float *rho, float *ux,
         else trt_dev_links_k<R, false, long long, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
     }
     if (SR) sr_advance_k<<<1, 1, 0, s>>>();
+    return KB_OK;
 }
 
 int launch_trt3d_dev_links(int dtype, void *f_out, const void *f_in, float *rho, float *ux,
                            float *uy, float *uz, const LinkTable3 &L, const Grid3 &g, float sp,
-                           float sm, cudaStream_t s) {
+                           float sm, cudaStream_t s, int variant) {
+    int rc = KB_OK;
     switch (dtype) {
-        case KB_F32_DEV: launch_links_r<float, false>(f_out, f_in, rho, ux, uy, uz, L, g, sp, sm, s); break;
-        case KB_F16_DEV: launch_links_r<__half, false>(f_out, f_in, rho, ux, uy, uz, L, g, sp, sm, s); break;
-        case KB_BF16_DEV: launch_links_r<__nv_bfloat16, false>(f_out, f_in, rho, ux, uy, uz, L, g, sp, sm, s); break;
-        case KB_F16_DEV_SR: launch_links_r<__half, true>(f_out, f_in, rho, ux, uy, uz, L, g, sp, sm, s); break;
-        case KB_BF16_DEV_SR: launch_links_r<__nv_bfloat16, true>(f_out, f_in, rho, ux, uy, uz, L, g, sp, sm, s); break;
+        case KB_F32_DEV: rc = launch_links_r<float, false>(f_out, f_in, rho, ux, uy, uz, L, g, sp, sm, s, variant); break;
+        case KB_F16_DEV: rc = launch_links_r<__half, false>(f_out, f_in, rho, ux, uy, uz, L, g, sp, sm, s, variant); break;
+        case KB_BF16_DEV: rc = launch_links_r<__nv_bfloat16, false>(f_out, f_in, rho, ux, uy, uz, L, g, sp, sm, s, variant); break;
+        case KB_F16_DEV_SR: rc = launch_links_r<__half, true>(f_out, f_in, rho, ux, uy, uz, L, g, sp, sm, s, variant); break;
+        case KB_BF16_DEV_SR: rc = launch_links_r<__nv_bfloat16, true>(f_out, f_in, rho, ux, uy, uz, L, g, sp, sm, s, variant); break;
         default: return set_error(KB_ERR_UNSUPPORTED, "kb_fused_trt_libb_links_step_3d: unknown dtype %d", dtype);
     }
+    if (rc != KB_OK) return rc;
     return check_launch("kb_fused_trt_libb_links_step_3d");
 }
 

@@ -249,3 +249,49 @@ def test_sphere_geometry_on_device_equals_host(cuda, pkg):
     a, sa = pkg.libb.precompute_q_wall_sphere_3d(*args)
     b, sb = pkg.libb.precompute_q_wall_sphere_3d_torch(*args, device="cuda")
     assert np.array_equal(a, _h(b)) and np.array_equal(sa, _h(sb))
+
+
+@pytest.mark.parametrize("dtype,sr,tol", [(torch.float16, False, 2e-3), (torch.bfloat16, False, 1.6e-2),
+                                          (torch.float16, True, 4e-3)])
+def test_staged_cut_link_step_matches_one_node_kernel(cuda, pkg, dtype, sr, tol):
+    """The cut-link step on 16-bit storage through the staged row tiles
+    (variant 5, the automatic choice for full 256-node rows) and through the
+    one-node kernel agree within the storage rounding, and both stay within
+    it of the FP64 table step: a sphere cut through 256-node rows, random
+    populations, walls in y and z, periodic x."""
+    Nx, Ny, Nz = 256, 20, 18
+    qw, solid = pkg.libb.precompute_q_wall_sphere_3d(Nx, Ny, Nz, 128.3, 9.7, 8.9, 7.3)
+    f, _, _, _ = _random_case((Nz, Ny, Nx), 19, W19, 77)
+    zeros = np.zeros_like(qw)
+    per = (True, False, False)
+    m = _g(solid, torch.uint8)
+    links64 = pkg.libb.CutLinks(m, *[_g(a) for a in (qw, zeros, zeros, zeros)])
+    ref = torch.empty_like(_g(f))
+    pkg.fused_trt_libb_links_step_3d_(ref, _g(f), None, None, None, None, links64, 0.04, periodic=per)
+    ref = _h(ref)
+    links64.close()
+    links = pkg.libb.CutLinks(m, *[_g(a, torch.float32) for a in (qw, zeros, zeros, zeros)])
+    assert links.nodes_with_links() > 100
+    src = torch.empty((19, Nz, Ny, Nx), dtype=dtype, device=cuda)
+    pkg.convert_populations(src, _g(f), dst_deviation=True)
+    got = []
+    try:
+        for variant in (5, 1):
+            pkg.set_trt3d_variant(variant)
+            fo = torch.empty_like(src)
+            mt = [torch.empty((Nz, Ny, Nx), dtype=torch.float32, device=cuda) for _ in range(4)]
+            pkg.fused_trt_libb_links_step_3d_(fo, src, *mt, links, 0.04, periodic=per,
+                                              deviation=True, stochastic_rounding=sr)
+            back = torch.empty((19, Nz, Ny, Nx), dtype=torch.float64, device=cuda)
+            pkg.convert_populations(back, fo, src_deviation=True)
+            got.append((_h(back), [_h(t) for t in mt]))
+    finally:
+        pkg.set_trt3d_variant(0)
+    links.close()
+    w = W19[:, None, None, None]
+    for g, _ in got:
+        assert np.max(np.abs(g - ref) / w) < tol
+    assert np.max(np.abs(got[0][0] - got[1][0]) / w) < 2 * tol
+    for a, b in zip(got[0][1], got[1][1]):
+        assert np.max(np.abs(a - b)) < 50 * tol
+    assert not pkg.staged_step_timed_out()
