@@ -29,10 +29,11 @@ namespace batch {
 #define KB_BATCH_THREADS 256
 #endif
 constexpr int BT = KB_BATCH_THREADS;  // threads per block
-// Blocks per SM the register allocation is sized for (__launch_bounds__):
-// more resident warps keep more population loads in flight.
+// Blocks per SM the register allocation is sized for (__launch_bounds__).
+// The pair loop keeps two pairs of pulls in flight per thread; 4 blocks give
+// it the registers for that with a small spill (5 or 6 spill far more).
 #ifndef KB_BATCH_MIN_BLOCKS
-#define KB_BATCH_MIN_BLOCKS 6
+#define KB_BATCH_MIN_BLOCKS 4
 #endif
 
 struct CaseDesc {
@@ -220,27 +221,60 @@ template <> struct Pair2<__nv_bfloat16> {
     }
 };
 
-template <typename R, bool SR>
-__device__ __forceinline__ void node_update_pair(const R *__restrict__ src, R *__restrict__ dst, int N,
-                                                 int i, int j, float s_nu, float u_lid, float2 &ux,
-                                                 float2 &uy, uint32_t key) {
+// The pulls of the pair (i, j), (i + 1, j) as raw stored values v[2q] (node
+// A) and v[2q + 1] (node B), not yet converted: a loop can issue the next
+// pair's loads and convert them only when it collides that pair.
+template <typename R> struct Raw2;
+template <> struct Raw2<float> {
+    static __device__ __forceinline__ void ld(const float *p, float *v) {
+        const float2 t = *reinterpret_cast<const float2 *>(p);
+        v[0] = t.x; v[1] = t.y;
+    }
+};
+template <> struct Raw2<__half> {
+    static __device__ __forceinline__ void ld(const __half *p, __half *v) {
+        const __half2 t = *reinterpret_cast<const __half2 *>(p);
+        v[0] = __low2half(t); v[1] = __high2half(t);
+    }
+};
+template <> struct Raw2<__nv_bfloat16> {
+    static __device__ __forceinline__ void ld(const __nv_bfloat16 *p, __nv_bfloat16 *v) {
+        const __nv_bfloat162 t = *reinterpret_cast<const __nv_bfloat162 *>(p);
+        v[0] = __low2bfloat16(t); v[1] = __high2bfloat16(t);
+    }
+};
+
+template <typename R>
+__device__ __forceinline__ void pair_loads_raw(const R *__restrict__ src, int N, int i, int j, R *v) {
     const long long P = (long long)N * N;
     const long long c = (long long)j * N + i;  // node A = (i, j), node B = (i + 1, j)
     const bool w = i > 0, e = i + 1 < N - 1, s = j > 0, n = j < N - 1;
-    float2 d[9];
-    d[0] = Pair2<R>::ld(src + c);
-    d[2] = s ? Pair2<R>::ld(src + c - N + 2 * P) : Pair2<R>::ld(src + c + 4 * P);
-    d[4] = n ? Pair2<R>::ld(src + c + N + 4 * P) : Pair2<R>::ld(src + c + 2 * P);
-    d[1] = make_float2(w ? ldv(src, c - 1 + P) : ldv(src, c + 3 * P), ldv(src, c + P));
-    d[3] = make_float2(ldv(src, c + 1 + 3 * P), e ? ldv(src, c + 2 + 3 * P) : ldv(src, c + 1 + P));
-    d[5] = make_float2((w && s) ? ldv(src, c - 1 - N + 5 * P) : ldv(src, c + 7 * P),
-                       s ? ldv(src, c - N + 5 * P) : ldv(src, c + 1 + 7 * P));
-    d[6] = make_float2(s ? ldv(src, c + 1 - N + 6 * P) : ldv(src, c + 8 * P),
-                       (e && s) ? ldv(src, c + 2 - N + 6 * P) : ldv(src, c + 1 + 8 * P));
-    d[7] = make_float2(n ? ldv(src, c + 1 + N + 7 * P) : ldv(src, c + 5 * P),
-                       (e && n) ? ldv(src, c + 2 + N + 7 * P) : ldv(src, c + 1 + 5 * P));
-    d[8] = make_float2((w && n) ? ldv(src, c - 1 + N + 8 * P) : ldv(src, c + 6 * P),
-                       n ? ldv(src, c + N + 8 * P) : ldv(src, c + 1 + 6 * P));
+    Raw2<R>::ld(src + c, v + 0);
+    Raw2<R>::ld(s ? src + c - N + 2 * P : src + c + 4 * P, v + 4);
+    Raw2<R>::ld(n ? src + c + N + 4 * P : src + c + 2 * P, v + 8);
+    v[2] = w ? src[c - 1 + P] : src[c + 3 * P];
+    v[3] = src[c + P];
+    v[6] = src[c + 1 + 3 * P];
+    v[7] = e ? src[c + 2 + 3 * P] : src[c + 1 + P];
+    v[10] = (w && s) ? src[c - 1 - N + 5 * P] : src[c + 7 * P];
+    v[11] = s ? src[c - N + 5 * P] : src[c + 1 + 7 * P];
+    v[12] = s ? src[c + 1 - N + 6 * P] : src[c + 8 * P];
+    v[13] = (e && s) ? src[c + 2 - N + 6 * P] : src[c + 1 + 8 * P];
+    v[14] = n ? src[c + 1 + N + 7 * P] : src[c + 5 * P];
+    v[15] = (e && n) ? src[c + 2 + N + 7 * P] : src[c + 1 + 5 * P];
+    v[16] = (w && n) ? src[c - 1 + N + 8 * P] : src[c + 6 * P];
+    v[17] = n ? src[c + N + 8 * P] : src[c + 1 + 6 * P];
+}
+
+// Zou-He lid (top row), MRT collision and stores of the pair whose pulled
+// deviations are d[]; returns the pre-collision velocity.
+template <typename R, bool SR>
+__device__ __forceinline__ void pair_finish(float2 *d, R *__restrict__ dst, int N, int i, int j,
+                                            float s_nu, float u_lid, float2 &ux, float2 &uy,
+                                            uint32_t key) {
+    const long long P = (long long)N * N;
+    const long long c = (long long)j * N + i;
+    const bool n = j < N - 1;
     const float2 z = make_float2(0.f, 0.f);
     if (!n) {
         // Zou-He velocity lid on deviations, as node_update
@@ -347,16 +381,25 @@ __global__ void __launch_bounds__(BT, KB_BATCH_MIN_BLOCKS) batch_k(BatchState D,
                         u2 += (double)ux * ux + (double)uy * uy;
                     }
                 }
-            } else
+            } else {
             // node pairs (m, m + 1): tiles start at multiples of 32, N is even
-            // and case offsets are multiples of 64, so every pair is aligned
-            for (int m = T.start + 2 * threadIdx.x; m < end; m += 2 * BT) {
+            // and case offsets are multiples of 64, so every pair is aligned;
+            // software-pipelined: the next pair's pulls are in flight (as raw
+            // stored values) while this pair collides
+            R vn[18];
+            int m = T.start + 2 * threadIdx.x;
+            if (m < end) pair_loads_raw<R>(src + C.f_off, C.N, m % C.N, m / C.N, vn);
+            for (; m < end; m += 2 * BT) {
                 const int j = m / C.N, i = m - j * C.N;
+                float2 d[9];
+#pragma unroll
+                for (int q = 0; q < 9; ++q) d[q] = make_float2(Dev<R>::ld(vn[2 * q]), Dev<R>::ld(vn[2 * q + 1]));
+                const int mn = m + 2 * BT;
+                if (mn < end) pair_loads_raw<R>(src + C.f_off, C.N, mn % C.N, mn / C.N, vn);
                 float2 ux, uy;
                 const uint32_t key =
                     SR ? hash32((uint32_t)(C.f_off + m) ^ hash32((uint32_t)s * 0x632BE5ABu + seed)) : 0u;
-                node_update_pair<R, SR>(src + C.f_off, dst + C.f_off, C.N, i, j, C.s_nu, C.u_lid,
-                                        ux, uy, key);
+                pair_finish<R, SR>(d, dst + C.f_off, C.N, i, j, C.s_nu, C.u_lid, ux, uy, key);
                 const long long mo = C.m_off + m;
                 if (save) {
                     *reinterpret_cast<float2 *>(D.uxp + mo) = ux;
@@ -373,6 +416,7 @@ __global__ void __launch_bounds__(BT, KB_BATCH_MIN_BLOCKS) batch_k(BatchState D,
                     u2 += (double)ux.x * ux.x + (double)uy.x * uy.x + (double)ux.y * ux.y +
                           (double)uy.y * uy.y;
                 }
+            }
             }
             if (check) {
                 const double a = block_sum(du2, sh);
