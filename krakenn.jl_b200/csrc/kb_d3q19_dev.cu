@@ -963,6 +963,16 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
         asm volatile("mov.b32 %0, %1;" : "=f"(sml) : "f"(sm));
         float2 o[19], rho, ux, uy, uz;
         trt_dev_collide(d, o, rho, ux, uy, uz, spl, sml);
+        // solid nodes store rest equilibrium (d = 0) and rho = 1, u = 0; only
+        // warps that hold one pay for the selects
+        if (HS && __any_sync(__activemask(), (sm2.x | sm2.y) != 0)) {
+#pragma unroll
+            for (int q = 0; q < 19; ++q) o[q] = make_float2(sm2.x ? 0.f : o[q].x, sm2.y ? 0.f : o[q].y);
+            rho = make_float2(sm2.x ? 1.f : rho.x, sm2.y ? 1.f : rho.y);
+            ux = make_float2(sm2.x ? 0.f : ux.x, sm2.y ? 0.f : ux.y);
+            uy = make_float2(sm2.x ? 0.f : uy.x, sm2.y ? 0.f : uy.y);
+            uz = make_float2(sm2.x ? 0.f : uz.x, sm2.y ? 0.f : uz.y);
+        }
         // likewise the plane stride, so the 19 plane offsets are not hoisted
         I Pl;
         if constexpr (sizeof(I) == 4) asm volatile("mov.b32 %0, %1;" : "=r"(Pl) : "r"((int)P));
@@ -975,7 +985,7 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
             const uint32_t key = SR ? hash32((uint32_t)cA ^ ekey) : 0u;
 #pragma unroll
             for (int q = 0; q < 19; ++q) {
-                const float vA = sm2.x ? 0.f : o[q].x, vB = sm2.y ? 0.f : o[q].y;
+                const float vA = o[q].x, vB = o[q].y;
                 unsigned short *w = reinterpret_cast<unsigned short *>(o0 + (I)q * Pl);
                 if (SR) {
                     const uint32_t v = SRPack<R>::pack(vA, vB, sr_bits(key, q));
@@ -987,14 +997,8 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
                 }
             }
             if (MOM) {
-                if (wA) {
-                    rho_o[cA] = sm2.x ? 1.f : rho.x; ux_o[cA] = sm2.x ? 0.f : ux.x;
-                    uy_o[cA] = sm2.x ? 0.f : uy.x; uz_o[cA] = sm2.x ? 0.f : uz.x;
-                }
-                if (wB) {
-                    rho_o[cA + 1] = sm2.y ? 1.f : rho.y; ux_o[cA + 1] = sm2.y ? 0.f : ux.y;
-                    uy_o[cA + 1] = sm2.y ? 0.f : uy.y; uz_o[cA + 1] = sm2.y ? 0.f : uz.y;
-                }
+                if (wA) { rho_o[cA] = rho.x; ux_o[cA] = ux.x; uy_o[cA] = uy.x; uz_o[cA] = uz.x; }
+                if (wB) { rho_o[cA + 1] = rho.y; ux_o[cA + 1] = ux.y; uy_o[cA + 1] = uy.y; uz_o[cA + 1] = uz.y; }
             }
             continue;
         }
@@ -1002,24 +1006,19 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
             const uint32_t key = hash32((uint32_t)cA ^ ekey);
 #pragma unroll
             for (int q = 0; q < 19; ++q) {
-                const uint32_t v = SRPack<R>::pack(HS && sm2.x ? 0.f : o[q].x,
-                                                   HS && sm2.y ? 0.f : o[q].y, sr_bits(key, q));
+                const uint32_t v = SRPack<R>::pack(o[q].x, o[q].y, sr_bits(key, q));
                 *reinterpret_cast<uint32_t *>(o0 + (I)q * Pl) = v;
             }
         } else {
 #pragma unroll
             for (int q = 0; q < 19; ++q)
-                Vec2<R>::st(o0 + (I)q * Pl, make_float2(HS && sm2.x ? 0.f : o[q].x,
-                                                        HS && sm2.y ? 0.f : o[q].y));
+                Vec2<R>::st(o0 + (I)q * Pl, o[q]);
         }
         if (MOM) {
-            float2 r = rho, a = ux, b = uy, c = uz;
-            if (HS && sm2.x) { r.x = 1.f; a.x = b.x = c.x = 0.f; }
-            if (HS && sm2.y) { r.y = 1.f; a.y = b.y = c.y = 0.f; }
-            *reinterpret_cast<float2 *>(rho_o + cA) = r;
-            *reinterpret_cast<float2 *>(ux_o + cA) = a;
-            *reinterpret_cast<float2 *>(uy_o + cA) = b;
-            *reinterpret_cast<float2 *>(uz_o + cA) = c;
+            *reinterpret_cast<float2 *>(rho_o + cA) = rho;
+            *reinterpret_cast<float2 *>(ux_o + cA) = ux;
+            *reinterpret_cast<float2 *>(uy_o + cA) = uy;
+            *reinterpret_cast<float2 *>(uz_o + cA) = uz;
         }
     }
     // after a timeout: wait (bounded) for copies the producer may still have
