@@ -895,7 +895,15 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
 
     // ---------------------------------------------------- consumer warps --
     const I P = (I)g.plane;
-    const uint32_t ekey = SR ? hash32(*(volatile const unsigned int *)&g_sr_epoch + 0x632BE5ABu) : 0u;
+    // stochastic rounding: one full hash per thread and launch; each tile
+    // advances it by a Weyl step and one multiply, and population q's word is
+    // that plus q times a constant (one add).  Every word is uniform, which is
+    // what makes the rounding unbiased; words of one thread are correlated,
+    // not independent.
+    const uint32_t ekey =
+        SR ? hash32(((uint32_t)blockIdx.x * TTHREADS + (uint32_t)t) ^
+                    hash32(*(volatile const unsigned int *)&g_sr_epoch + 0x632BE5ABu))
+           : 0u;
     int it = 0;
     bool aborted = false;
 #pragma unroll 1
@@ -982,13 +990,13 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
             // a pair with a cut node: trt_dev_cut_k writes that node (it runs
             // beside this kernel), so only the other node is stored here
             const bool wA = cl.x != 2, wB = cl.y != 2;
-            const uint32_t key = SR ? hash32((uint32_t)cA ^ ekey) : 0u;
+            const uint32_t key = SR ? (ekey + (uint32_t)it * 0x9E3779B9u) * 0x7FEB352Du : 0u;
 #pragma unroll
             for (int q = 0; q < 19; ++q) {
                 const float vA = o[q].x, vB = o[q].y;
                 unsigned short *w = reinterpret_cast<unsigned short *>(o0 + (I)q * Pl);
                 if (SR) {
-                    const uint32_t v = SRPack<R>::pack(vA, vB, sr_bits(key, q));
+                    const uint32_t v = SRPack<R>::pack(vA, vB, key + (uint32_t)q * 0x2C1B3C6Du);
                     if (wA) w[0] = (unsigned short)(v & 0xFFFFu);
                     if (wB) w[1] = (unsigned short)(v >> 16);
                 } else {
@@ -1003,10 +1011,10 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
             continue;
         }
         if (SR) {
-            const uint32_t key = hash32((uint32_t)cA ^ ekey);
+            const uint32_t key = (ekey + (uint32_t)it * 0x9E3779B9u) * 0x7FEB352Du;
 #pragma unroll
             for (int q = 0; q < 19; ++q) {
-                const uint32_t v = SRPack<R>::pack(o[q].x, o[q].y, sr_bits(key, q));
+                const uint32_t v = SRPack<R>::pack(o[q].x, o[q].y, key + (uint32_t)q * 0x2C1B3C6Du);
                 *reinterpret_cast<uint32_t *>(o0 + (I)q * Pl) = v;
             }
         } else {
