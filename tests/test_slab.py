@@ -155,3 +155,42 @@ def test_slab_split_and_ghosts(pkg, Nz, world):
         pkg.slab.Slab(3, 4, 0, True)
     with pytest.raises(ValueError):
         pkg.slab.Slab(8, 2, 2, True)
+
+
+def _worker_peer_gone(rank, world, port, out):
+    import sys
+    from datetime import timedelta
+    sys.path.insert(0, str(ROOT))
+    import __graft_entry__ as graft
+    pkg = graft.load_package()
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=5))
+    slab = pkg.slab.Slab(8, world, rank, True)
+    f = torch.zeros((19, slab.nz_alloc, 3, 4), dtype=torch.float64)
+    if rank == 1:
+        out.put((rank, "left"))
+        return  # leaves between steps, before its exchange
+    try:
+        pkg.slab.exchange(f, slab)
+        out.put((rank, "no error"))
+    except Exception as e:  # the surviving rank learns of it from the process group
+        out.put((rank, type(e).__name__))
+
+
+def test_slab_exchange_reports_a_missing_peer(pkg):
+    """A rank that leaves between steps makes its neighbour's next exchange
+    end with an error within the process-group timeout, not hang."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker_peer_gone, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        if p.is_alive():
+            p.kill()
+    assert res[1] == "left"
+    assert res[0] != "no error", res
