@@ -404,6 +404,7 @@ def run_gpu(args):
             extra = {"tgv_config2_precisions": bench_tgv_precisions(pkg, n, 2000),
                      "cavity2d_config1": bench_cavity2d(pkg, steps=20000),
                      "natconv_config4": bench_natconv(pkg, 512, 1e5, 2000)[0],
+                     "d2q9_fused_4096": bench_d2q9_large(pkg),
                      "batch_config3_short": bench_batch(pkg, max_steps=2000, check_every=100,
                                                         autotune=False)}
         line = {
@@ -497,6 +498,45 @@ def bench_tgv_precisions(pkg, n=N_GRID, steps=2000):
                         f"{steps} steps per storage", "storages": out,
             "f16dev_over_f32dev_mlups": round(out["f16dev"]["mlups"] / out["f32dev"]["mlups"], 3),
             "f16dev_sr_over_f32dev_mlups": round(out["f16dev_sr"]["mlups"] / out["f32dev"]["mlups"], 3)}
+
+
+def bench_d2q9_large(pkg, n=4096, steps=50, warmup=3):
+    """The 2D fused steps (fused_bgk_step!, fused_trt_step!: pull with half-way
+    bounce-back on the four walls, collision, rho and u written every step as
+    the reference's do) on an n x n grid larger than L2, FP64 and FP32: GLUPS
+    and the fraction of the measured copy bandwidth at 2 * 9 * b bytes per
+    node (the 3 * b bytes of moments count as overhead)."""
+    import torch
+    peak, _ = hbm_peak()
+    w = torch.tensor([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4, dtype=torch.float64, device="cuda")
+    out = {}
+    for name, dt, bpp in (("f64", torch.float64, 8), ("f32", torch.float32, 4)):
+        a = (w[:, None, None] * (1 + 0.01 * torch.rand((9, n, n), dtype=torch.float64,
+                                                        device="cuda"))).to(dt)
+        b = torch.empty_like(a)
+        mom = [torch.empty((n, n), dtype=dt, device="cuda") for _ in range(3)]
+        for kern in ("bgk", "trt"):
+            def step(x, y):
+                if kern == "bgk":
+                    pkg.fused_bgk_step_(y, x, *mom, None, n, n, 1.0 / (3 * 0.02 + 0.5))
+                else:
+                    pkg.fused_trt_step_(y, x, *mom, None, n, n, 0.02, 0.25)
+            for _ in range(warmup):
+                step(a, b)
+                a, b = b, a
+            e0, e1 = _events()
+            e0.record()
+            for _ in range(steps):
+                step(a, b)
+                a, b = b, a
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            out[f"{kern}_{name}"] = {"mlups": round(n * n / ms / 1e3, 1),
+                                     "hbm_frac": round(2 * 9 * bpp * n * n / (ms * 1e-3) / 1e9 / peak, 4)}
+        del a, b, mom
+        torch.cuda.empty_cache()
+    return {"workload": f"D2Q9 fused steps on a walled {n}x{n} grid, {steps} steps each", "runs": out}
 
 
 def bench_cavity2d(pkg, steps=20000, graph_steps=200):
