@@ -405,6 +405,7 @@ def run_gpu(args):
                      "cavity2d_config1": bench_cavity2d(pkg, steps=20000),
                      "natconv_config4": bench_natconv(pkg, 512, 1e5, 2000)[0],
                      "d2q9_fused_4096": bench_d2q9_large(pkg),
+                     "unfused_paths": bench_unfused_paths(pkg),
                      "batch_config3_short": bench_batch(pkg, max_steps=2000, check_every=100,
                                                         autotune=False)}
         line = {
@@ -537,6 +538,59 @@ def bench_d2q9_large(pkg, n=4096, steps=50, warmup=3):
         del a, b, mom
         torch.cuda.empty_cache()
     return {"workload": f"D2Q9 fused steps on a walled {n}x{n} grid, {steps} steps each", "runs": out}
+
+
+def bench_unfused_paths(pkg, n2=4096, n3=256, steps=40, warmup=3):
+    """Throughput of the reference's other step structures: the in-place A-A
+    pair (aa_even_step!/aa_odd_step!, race-free form) on an n2 x n2 walled
+    grid, and the unfused D3Q19 walled cavity step (stream_3d!, Zou-He lid,
+    collide_3d!: three launches, run_cavity_3d) at n3^3.  GLUPS, and the
+    fraction of the measured copy bandwidth at the step's own traffic (A-A:
+    2 * 9 * b per node in one buffer; unfused 3D: 4 * 19 * b per node, the
+    stream and the collide passes each read and write every population)."""
+    import torch
+    peak, _ = hbm_peak()
+    out = {}
+    w9 = torch.tensor([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4, dtype=torch.float64, device="cuda")
+    w19 = torch.tensor([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12, dtype=torch.float64, device="cuda")
+    om = 1.0 / (3 * 0.02 + 0.5)
+
+    def timed(step):
+        for _ in range(warmup):
+            step()
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    for name, dt, bpp in (("f64", torch.float64, 8), ("f32", torch.float32, 4)):
+        f = (w9[:, None, None] * torch.ones((9, n2, n2), dtype=torch.float64, device="cuda")).to(dt)
+        ms = timed(lambda: (pkg.aa_stream_step_2d_(f, None, None, None, None, n2, n2, om),
+                            pkg.aa_local_step_2d_(f, None, None, None, None, n2, n2, om))) / 2
+        out[f"aa_2d_{name}"] = {"mlups": round(n2 * n2 / ms / 1e3, 1),
+                                "hbm_frac": round(2 * 9 * bpp * n2 * n2 / (ms * 1e-3) / 1e9 / peak, 4)}
+        del f
+        a = (w19[:, None, None, None] * torch.ones((19, n3, n3, n3), dtype=torch.float64,
+                                                   device="cuda")).to(dt)
+        b = torch.empty_like(a)
+        bufs = [a, b]
+
+        def step3():
+            pkg.stream_3d_(bufs[1], bufs[0], n3, n3, n3)
+            pkg.apply_zou_he_top_3d_(bufs[1], 0.1, n3, n3, n3)
+            pkg.collide_3d_(bufs[1], None, om)
+            bufs.reverse()
+        ms = timed(step3)
+        out[f"cavity3d_unfused_{name}"] = {
+            "mlups": round(n3 ** 3 / ms / 1e3, 1),
+            "hbm_frac": round(4 * 19 * bpp * n3 ** 3 / (ms * 1e-3) / 1e9 / peak, 4)}
+        del a, b, bufs
+        torch.cuda.empty_cache()
+    return {"workload": f"A-A pair on a walled {n2}^2 D2Q9 grid; unfused D3Q19 cavity step at "
+                        f"{n3}^3; {steps} steps each", "runs": out}
 
 
 def bench_cavity2d(pkg, steps=20000, graph_steps=200):
