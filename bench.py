@@ -542,11 +542,13 @@ def bench_d2q9_large(pkg, n=4096, steps=50, warmup=3):
 
 def bench_unfused_paths(pkg, n2=4096, n3=256, steps=40, warmup=3):
     """Throughput of the reference's other step structures: the in-place A-A
-    pair (aa_even_step!/aa_odd_step!, race-free form) on an n2 x n2 walled
-    grid, and the unfused D3Q19 walled cavity step (stream_3d!, Zou-He lid,
-    collide_3d!: three launches, run_cavity_3d) at n3^3.  GLUPS, and the
+    pair (aa_even_step!/aa_odd_step!, race-free form) and the unfused D2Q9
+    cavity step (stream_2d!, apply_zou_he_north_2d!, collide_2d!) on an
+    n2 x n2 walled grid, and the unfused D3Q19 walled cavity step
+    (stream_3d!, Zou-He lid, collide_3d!: three launches, run_cavity_3d) at
+    n3^3.  GLUPS, and the
     fraction of the measured copy bandwidth at the step's own traffic (A-A:
-    2 * 9 * b per node in one buffer; unfused 3D: 4 * 19 * b per node, the
+    2 * 9 * b per node in one buffer; unfused steps: 4 * Q * b per node, the
     stream and the collide passes each read and write every population)."""
     import torch
     peak, _ = hbm_peak()
@@ -572,7 +574,19 @@ def bench_unfused_paths(pkg, n2=4096, n3=256, steps=40, warmup=3):
                             pkg.aa_local_step_2d_(f, None, None, None, None, n2, n2, om))) / 2
         out[f"aa_2d_{name}"] = {"mlups": round(n2 * n2 / ms / 1e3, 1),
                                 "hbm_frac": round(2 * 9 * bpp * n2 * n2 / (ms * 1e-3) / 1e9 / peak, 4)}
-        del f
+        g = torch.empty_like(f)
+        b2 = [f, g]
+
+        def step2():
+            pkg.stream_2d_(b2[1], b2[0], n2, n2)
+            pkg.apply_zou_he_north_2d_(b2[1], 0.1, n2, n2)
+            pkg.collide_2d_(b2[1], None, om)
+            b2.reverse()
+        ms = timed(step2)
+        out[f"cavity2d_unfused_{name}"] = {
+            "mlups": round(n2 * n2 / ms / 1e3, 1),
+            "hbm_frac": round(4 * 9 * bpp * n2 * n2 / (ms * 1e-3) / 1e9 / peak, 4)}
+        del f, g, b2
         a = (w19[:, None, None, None] * torch.ones((19, n3, n3, n3), dtype=torch.float64,
                                                    device="cuda")).to(dt)
         b = torch.empty_like(a)
@@ -589,8 +603,8 @@ def bench_unfused_paths(pkg, n2=4096, n3=256, steps=40, warmup=3):
             "hbm_frac": round(4 * 19 * bpp * n3 ** 3 / (ms * 1e-3) / 1e9 / peak, 4)}
         del a, b, bufs
         torch.cuda.empty_cache()
-    return {"workload": f"A-A pair on a walled {n2}^2 D2Q9 grid; unfused D3Q19 cavity step at "
-                        f"{n3}^3; {steps} steps each", "runs": out}
+    return {"workload": f"A-A pair and unfused D2Q9 cavity step on a walled {n2}^2 grid; unfused "
+                        f"D3Q19 cavity step at {n3}^3; {steps} steps each", "runs": out}
 
 
 def bench_cavity2d(pkg, steps=20000, graph_steps=200):
