@@ -185,7 +185,7 @@ __device__ __forceinline__ void node_update(const R *__restrict__ src, R *__rest
 #pragma unroll
         for (int q = 0; q < 9; q += 2) {
             const uint32_t w = SRPack<R>::pack(o[q], q + 1 < 9 ? o[q + 1] : 0.f,
-                                               hash32(key + (uint32_t)q * 0x9E3779B9u));
+                                               key * 0x7FEB352Du + (uint32_t)q * 0x2C1B3C6Du);
             d16[c + q * P] = (unsigned short)(w & 0xFFFFu);
             if (q + 1 < 9) d16[c + (q + 1) * P] = (unsigned short)(w >> 16);
         }
@@ -335,7 +335,7 @@ __device__ __forceinline__ void pair_finish(float2 *d, R *__restrict__ dst, int 
     for (int q = 0; q < 9; ++q) {
         if (SR) {
             *reinterpret_cast<uint32_t *>(dst + c + q * P) =
-                SRPack<R>::pack(o[q].x, o[q].y, hash32(key + (uint32_t)q * 0x9E3779B9u));
+                SRPack<R>::pack(o[q].x, o[q].y, key * 0x7FEB352Du + (uint32_t)q * 0x2C1B3C6Du);
         } else {
             Pair2<R>::st(dst + c + q * P, o[q]);
         }

@@ -38,13 +38,11 @@ struct DevLoad {
 // smaller than half a unit in the last place is lost every step.  sm_100a's
 // cvt.rs.{f16x2,bf16x2}.f32 rounds up with probability equal to the dropped
 // fraction, given 32 random bits per pair, so the rounding error has zero
-// mean.  Each thread (node pair) draws a key from an integer hash (lowbias32,
-// C. Wellons) of its index and a launch counter in device memory that a
-// one-thread kernel advances after every such launch (so CUDA-graph replays
-// draw fresh bits and a run is reproducible on one stream).  The word of
-// population q is one multiply-xorshift round of the Weyl sequence
-// key + q * golden: uniform because the key is, and it costs three integer
-// instructions per population instead of a full hash.
+// mean.  Each thread draws a key from an integer hash (lowbias32, C. Wellons)
+// of its index and a launch counter in device memory that a one-thread kernel
+// advances after every such launch (so CUDA-graph replays draw fresh bits and
+// a run is reproducible on one stream); population q's word is derived from
+// the key with one add (sr_bits).
 __device__ unsigned int g_sr_epoch = 0;
 
 __global__ void sr_advance_k() { g_sr_epoch += 1u; }
@@ -56,11 +54,13 @@ __device__ __forceinline__ uint32_t sr_key() {
     const uint32_t e = *(volatile const unsigned int *)&g_sr_epoch;
     return hash32(tid ^ hash32(e + 0x632BE5ABu));
 }
-// Random word for population q.  cvt.rs reads bits 0-12 (low element) and
-// 16-28 (high element); the xorshift folds the product's high bits into them.
+// Random word for population q (cvt.rs reads bits 0-12 for the low element
+// and 16-28 for the high one): the key, a full hash, times an odd constant,
+// plus q times another.  Each word is uniform because the key is, which keeps
+// the rounding unbiased; the words of one key are correlated, not independent.
+// The compiler forms key * M once, so a word costs one add.
 __device__ __forceinline__ uint32_t sr_bits(uint32_t key, int q) {
-    const uint32_t x = (key + (uint32_t)q * 0x9E3779B9u) * 0x7FEB352Du;
-    return x ^ (x >> 15);
+    return key * 0x7FEB352Du + (uint32_t)q * 0x2C1B3C6Du;
 }
 
 // Opposite pairs (q, qb) of D3Q19; c_qb = -c_q.  Indexed only with
