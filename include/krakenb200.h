@@ -447,6 +447,22 @@ int kb_fused_trt_step_3d(void *f_out, const void *f_in, void *rho, void *ux, voi
                          const uint8_t *is_solid, int Nx, int Ny, int Nz, double nu,
                          double Lambda, int periodic, int dtype, void *stream);
 
+/* The same fused TRT step over the z-planes [k_begin, k_end) of an
+ * allocation of Nz_alloc planes whose first and last planes are halo (ghost)
+ * planes of a z-slab: z-pulls read planes k_begin - 1 and k_end as they are
+ * (no wrap, no bounce-back).  All pointers address node (0, 0, 0) of the
+ * whole allocation and every array spans it; only the planes of the range
+ * are written.  Stepping [1, n) and [n, Nz_alloc - 1) gives bit for bit the
+ * result of one step over [1, Nz_alloc - 1), so a slab steps its boundary
+ * planes first, starts their exchange, then steps its interior.  Requires
+ * 1 <= k_begin < k_end <= Nz_alloc - 1; periodic_xy: bit 0 = x, bit 1 = y.
+ * No reference counterpart: the reference steps a whole array
+ * (src/kernels/li_bb_3d_v2.jl:31). */
+int kb_fused_trt_step_3d_zrange(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                                void *uz, const uint8_t *is_solid, int Nx, int Ny, int Nz_alloc,
+                                int k_begin, int k_end, double nu, double Lambda,
+                                int periodic_xy, int dtype, void *stream);
+
 /* Kernel variant for tuning and tests (process-wide, not thread-safe to
  * change while other threads launch).  kernel 1 = the deviation-storage
  * kernels of kb_fused_trt_step_3d: 0 automatic (KB_F32_DEV: 3 for even Nx,

@@ -99,6 +99,8 @@ SIGNATURES: dict[str, list] = {
     "kb_compute_macroscopic_3d": [_vp, _vp, _vp, _vp, _cvp, _i, _i, _i, _i, _vp],
     "kb_fused_trt_step_3d": [_vp, _cvp, _vp, _vp, _vp, _vp, _u8p, _i, _i, _i, _d, _d, _i, _i,
                              _vp],
+    "kb_fused_trt_step_3d_zrange": [_vp, _cvp, _vp, _vp, _vp, _vp, _u8p, _i, _i, _i, _i, _i, _d,
+                                    _d, _i, _i, _vp],
     "kb_set_kernel_variant": [_i, _i],
     "kb_stream_periodic_xz_movingwall_y_3d": [_vp, _cvp, _d, _d, _d, _i, _i, _i, _i, _vp],
     "kb_batch_create": [C.POINTER(_vp), _i, C.POINTER(_i), _dp, _dp, _i, _vp],

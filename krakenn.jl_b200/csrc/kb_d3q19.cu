@@ -756,37 +756,39 @@ int kb_compute_macroscopic_3d(void *rho, void *ux, void *uy, void *uz, const voi
             (T *)rho, (T *)ux, (T *)uy, (T *)uz, (const T *)f, grid3(Nx, Ny, Nz))));
 }
 
-int kb_fused_trt_step_3d(void *f_out, const void *f_in, void *rho, void *ux, void *uy, void *uz,
-                         const uint8_t *is_solid, int Nx, int Ny, int Nz, double nu,
-                         double Lambda, int periodic, int dtype, void *stream) {
-    const char *what = "kb_fused_trt_step_3d";
+}  // extern "C"
+
+namespace {
+// One fused TRT step over the grid g; the pointers address node (0, 0, 0)
+// of g, the population stride is g.plane.
+int trt3d_step(const char *what, void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+               void *uz, const uint8_t *is_solid, const Grid3 &g, double nu, double Lambda,
+               int dtype, void *stream) {
     KB_REQUIRE(f_out && f_in, "%s: null population pointer", what);
     KB_REQUIRE(f_out != f_in, "%s: f_out and f_in must differ", what);
     const int nm = (rho != nullptr) + (ux != nullptr) + (uy != nullptr) + (uz != nullptr);
     KB_REQUIRE(nm == 0 || nm == 4, "%s: pass all four moment arrays or none", what);
-    KB_REQUIRE(periodic >= 0 && periodic < 8, "%s: periodic mask %d not in 0..7", what, periodic);
-    if (int e = check_dims(what, Nx, Ny, Nz)) return e;
     double sp, sm;
     if (int e = kb_trt_rates(nu, Lambda, &sp, &sm)) return e;
-    const Grid3 g = grid3(Nx, Ny, Nz, periodic);
     cudaStream_t s = kb::as_stream(stream);
     const bool i32 = offsets_fit_int(g, 19);
+    const dim3 grid = nodes_grid(g.Nx, g.Ny, g.Nz);
     if (dtype == KB_F64) {
         if (i32)
-            fused_trt_k<double, int><<<nodes_grid(Nx, Ny, Nz), BX, 0, s>>>(
+            fused_trt_k<double, int><<<grid, BX, 0, s>>>(
                 (double *)f_out, (const double *)f_in, (double *)rho, (double *)ux, (double *)uy,
                 (double *)uz, is_solid, g, sp, sm);
         else
-            fused_trt_k<double, long long><<<nodes_grid(Nx, Ny, Nz), BX, 0, s>>>(
+            fused_trt_k<double, long long><<<grid, BX, 0, s>>>(
                 (double *)f_out, (const double *)f_in, (double *)rho, (double *)ux, (double *)uy,
                 (double *)uz, is_solid, g, sp, sm);
     } else if (dtype == KB_F32) {
         if (i32)
-            fused_trt_k<float, int><<<nodes_grid(Nx, Ny, Nz), BX, 0, s>>>(
+            fused_trt_k<float, int><<<grid, BX, 0, s>>>(
                 (float *)f_out, (const float *)f_in, (float *)rho, (float *)ux, (float *)uy,
                 (float *)uz, is_solid, g, (float)sp, (float)sm);
         else
-            fused_trt_k<float, long long><<<nodes_grid(Nx, Ny, Nz), BX, 0, s>>>(
+            fused_trt_k<float, long long><<<grid, BX, 0, s>>>(
                 (float *)f_out, (const float *)f_in, (float *)rho, (float *)ux, (float *)uy,
                 (float *)uz, is_solid, g, (float)sp, (float)sm);
     } else if (dtype == KB_F32_DEV || dtype == KB_F16_DEV || dtype == KB_BF16_DEV ||
@@ -797,6 +799,53 @@ int kb_fused_trt_step_3d(void *f_out, const void *f_in, void *rho, void *ux, voi
         return kb::set_error(KB_ERR_UNSUPPORTED, "%s: unknown dtype %d", what, dtype);
     }
     return kb::check_launch(what);
+}
+
+// bytes of one population word and of one moment value per storage
+size_t pop_bytes(int dtype) {
+    switch (dtype) {
+        case KB_F64: return 8;
+        case KB_F32: case KB_F32_DEV: return 4;
+        case KB_F16_DEV: case KB_BF16_DEV: case KB_F16_DEV_SR: case KB_BF16_DEV_SR: return 2;
+        default: return 0;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int kb_fused_trt_step_3d(void *f_out, const void *f_in, void *rho, void *ux, void *uy, void *uz,
+                         const uint8_t *is_solid, int Nx, int Ny, int Nz, double nu,
+                         double Lambda, int periodic, int dtype, void *stream) {
+    const char *what = "kb_fused_trt_step_3d";
+    KB_REQUIRE(periodic >= 0 && periodic < 8, "%s: periodic mask %d not in 0..7", what, periodic);
+    if (int e = check_dims(what, Nx, Ny, Nz)) return e;
+    return trt3d_step(what, f_out, f_in, rho, ux, uy, uz, is_solid, grid3(Nx, Ny, Nz, periodic),
+                      nu, Lambda, dtype, stream);
+}
+
+int kb_fused_trt_step_3d_zrange(void *f_out, const void *f_in, void *rho, void *ux, void *uy,
+                                void *uz, const uint8_t *is_solid, int Nx, int Ny, int Nz_alloc,
+                                int k_begin, int k_end, double nu, double Lambda,
+                                int periodic_xy, int dtype, void *stream) {
+    const char *what = "kb_fused_trt_step_3d_zrange";
+    KB_REQUIRE(periodic_xy >= 0 && periodic_xy < 4, "%s: periodic mask %d not in 0..3", what,
+               periodic_xy);
+    if (int e = check_dims(what, Nx, Ny, Nz_alloc)) return e;
+    KB_REQUIRE(k_begin >= 1 && k_begin < k_end && k_end <= Nz_alloc - 1,
+               "%s: plane range [%d, %d) must lie in [1, %d) (the first and last allocated planes "
+               "are halo planes)", what, k_begin, k_end, Nz_alloc - 1);
+    const size_t eb = pop_bytes(dtype);
+    KB_REQUIRE(eb != 0, "%s: unknown dtype %d", what, dtype);
+    const size_t mb = (dtype == KB_F64 || dtype == KB_F32) ? eb : 4;  // moment bytes
+    const size_t off = (size_t)k_begin * (size_t)Nx * (size_t)Ny;     // nodes before the range
+    Grid3 g = grid3(Nx, Ny, Nz_alloc, (periodic_xy & 3) | KB_ZHALO);
+    g.Nz = k_end - k_begin;
+    g.zoff = k_begin;
+    const auto at = [off](void *p, size_t b) { return p ? (void *)((char *)p + off * b) : p; };
+    return trt3d_step(what, at(f_out, eb), (const char *)f_in + off * eb, at(rho, mb), at(ux, mb),
+                      at(uy, mb), at(uz, mb), is_solid ? is_solid + off : nullptr, g, nu, Lambda,
+                      dtype, stream);
 }
 
 int kb_fused_trt_libb_step_3d(void *f_out, const void *f_in, void *rho, void *ux, void *uy,

@@ -14,9 +14,14 @@ constexpr int BX = KB_D3_BLOCK_X;  // threads per block along x
 
 struct Grid3 {
     int Nx, Ny, Nz;
-    size_t plane;  // Nx*Ny*Nz nodes in one population plane
-    int per;       // bit 0 x, bit 1 y, bit 2 z periodic
+    size_t plane;  // population stride in nodes: Nx*Ny*Nz, or more for a z-range
+    int per;       // bit 0 x, bit 1 y, bit 2 z periodic; bit 3 z halo (below)
+    int zoff = 0;  // z-range: plane of the allocation that k = 0 is (staged copies)
 };
+// z halo (per bit 3): the grid is a range of z-planes inside a larger
+// allocation whose planes k = -1 and k = Nz exist; z-pulls read them as they
+// are (no wrap, no bounce-back).  The pointers passed start at plane zoff.
+constexpr int KB_ZHALO = 8;
 
 // Signed node offsets of the pull sources of one node, with the flags that
 // say whether the source exists (inside the box, or wrapped on a periodic
@@ -37,19 +42,20 @@ template <typename I = long long>
 __device__ __forceinline__ Pull3<I> pull_geometry(const Grid3 &g, int i, int j, int k) {
     Pull3<I> s;
     const bool px = g.per & 1, py = (g.per >> 1) & 1, pz = (g.per >> 2) & 1;
+    const bool zh = (g.per & KB_ZHALO) != 0;
     const I sx = 1, sy = (I)g.Nx, sz = (I)g.Nx * (I)g.Ny;
     s.xm = px || i > 0;
     s.xp = px || i < g.Nx - 1;
     s.ym = py || j > 0;
     s.yp = py || j < g.Ny - 1;
-    s.zm = pz || k > 0;
-    s.zp = pz || k < g.Nz - 1;
+    s.zm = pz || zh || k > 0;
+    s.zp = pz || zh || k < g.Nz - 1;
     s.dxm = (i > 0 ? (I)-1 : (I)(g.Nx - 1)) * sx;
     s.dxp = (i < g.Nx - 1 ? (I)1 : -(I)(g.Nx - 1)) * sx;
     s.dym = (j > 0 ? (I)-1 : (I)(g.Ny - 1)) * sy;
     s.dyp = (j < g.Ny - 1 ? (I)1 : -(I)(g.Ny - 1)) * sy;
-    s.dzm = (k > 0 ? (I)-1 : (I)(g.Nz - 1)) * sz;
-    s.dzp = (k < g.Nz - 1 ? (I)1 : -(I)(g.Nz - 1)) * sz;
+    s.dzm = (k > 0 || zh ? (I)-1 : (I)(g.Nz - 1)) * sz;
+    s.dzp = (k < g.Nz - 1 || zh ? (I)1 : -(I)(g.Nz - 1)) * sz;
     return s;
 }
 

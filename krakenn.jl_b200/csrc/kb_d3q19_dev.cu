@@ -248,13 +248,14 @@ __global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_x2_k(R *__rest
     const I P = (I)g.plane;
     const size_t cA = (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k) + iA;
     const bool px = g.per & 1, py = (g.per >> 1) & 1, pz = (g.per >> 2) & 1;
+    const bool zh = (g.per & KB_ZHALO) != 0;
     // Fast path: a full 64-node run whose every pull source is a node at a
     // fixed y/z shift (inside the box or wrapped; block-uniform) and an x
     // shift of -1, 0 or +1, wrapped only on the two row-end lanes.  Node B's
     // sources are then node A's plus 32 elements (an immediate offset), and
     // one address per population serves both nodes.  Runs touching an x
     // wall, rows at a y or z wall and ragged run ends take the general pull.
-    const bool yz_fast = (py || (j > 0 && j < g.Ny - 1)) && (pz || (k > 0 && k < g.Nz - 1));
+    const bool yz_fast = (py || (j > 0 && j < g.Ny - 1)) && (pz || zh || (k > 0 && k < g.Nz - 1));
     const bool x_fast = x0 + 64 <= g.Nx && (px || (x0 > 0 && x0 + 64 < g.Nx));
     float a[19], b[19];
     if (yz_fast && x_fast) {
@@ -265,7 +266,8 @@ __global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_x2_k(R *__rest
         const R *__restrict__ bBp = b0 + (iB < g.Nx - 1 ? 33 : 33 - g.Nx);
         const I sy = (I)g.Nx, sz = (I)g.Nx * (I)g.Ny;
         const I ym = j > 0 ? -sy : (I)(g.Ny - 1) * sy, yp = j < g.Ny - 1 ? sy : -(I)(g.Ny - 1) * sy;
-        const I zm = k > 0 ? -sz : (I)(g.Nz - 1) * sz, zp = k < g.Nz - 1 ? sz : -(I)(g.Nz - 1) * sz;
+        const I zm = (k > 0 || zh) ? -sz : (I)(g.Nz - 1) * sz;
+        const I zp = (k < g.Nz - 1 || zh) ? sz : -(I)(g.Nz - 1) * sz;
         const DevLoad<R> ld;
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
@@ -378,11 +380,12 @@ __global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_v2_k(R *__rest
     const bool px = g.per & 1, py = (g.per >> 1) & 1, pz = (g.per >> 2) & 1;
     const I sy = (I)Nx, sz = (I)Nx * (I)g.Ny;
     const bool ym = py || j > 0, yp = py || j < g.Ny - 1;
-    const bool zm = pz || k > 0, zp = pz || k < g.Nz - 1;
+    const bool zh = (g.per & KB_ZHALO) != 0;
+    const bool zm = pz || zh || k > 0, zp = pz || zh || k < g.Nz - 1;
     const I oym = (j > 0 ? (I)-1 : (I)(g.Ny - 1)) * sy;
     const I oyp = (j < g.Ny - 1 ? (I)1 : -(I)(g.Ny - 1)) * sy;
-    const I ozm = (k > 0 ? (I)-1 : (I)(g.Nz - 1)) * sz;
-    const I ozp = (k < g.Nz - 1 ? (I)1 : -(I)(g.Nz - 1)) * sz;
+    const I ozm = (k > 0 || zh ? (I)-1 : (I)(g.Nz - 1)) * sz;
+    const I ozp = (k < g.Nz - 1 || zh ? (I)1 : -(I)(g.Nz - 1)) * sz;
     const size_t row = (size_t)Nx * ((size_t)j + (size_t)g.Ny * k);
     const R *__restrict__ f0 = fi + row;  // row x = 0 of population 0, this (j, k)
     const int xv = valid ? x0 : 0;        // invalid lanes read a harmless in-row pair
@@ -527,11 +530,12 @@ __global__ void __launch_bounds__(128, KB_QUAD_MIN_BLOCKS) trt_dev_v4_k(R *__res
     const bool px = g.per & 1, py = (g.per >> 1) & 1, pz = (g.per >> 2) & 1;
     const I sy = (I)Nx, sz = (I)Nx * (I)g.Ny;
     const bool ym = py || j > 0, yp = py || j < g.Ny - 1;
-    const bool zm = pz || k > 0, zp = pz || k < g.Nz - 1;
+    const bool zh = (g.per & KB_ZHALO) != 0;
+    const bool zm = pz || zh || k > 0, zp = pz || zh || k < g.Nz - 1;
     const I oym = (j > 0 ? (I)-1 : (I)(g.Ny - 1)) * sy;
     const I oyp = (j < g.Ny - 1 ? (I)1 : -(I)(g.Ny - 1)) * sy;
-    const I ozm = (k > 0 ? (I)-1 : (I)(g.Nz - 1)) * sz;
-    const I ozp = (k < g.Nz - 1 ? (I)1 : -(I)(g.Nz - 1)) * sz;
+    const I ozm = (k > 0 || zh ? (I)-1 : (I)(g.Nz - 1)) * sz;
+    const I ozp = (k < g.Nz - 1 || zh ? (I)1 : -(I)(g.Nz - 1)) * sz;
     const size_t row = (size_t)Nx * ((size_t)j + (size_t)g.Ny * k);
     const R *__restrict__ f0 = fi + row;
     const int xv = valid ? x0 : 0;
@@ -711,7 +715,7 @@ __device__ __forceinline__ void tma_load4(uint32_t dst, const CUtensorMap *tm, i
 // by G without a division per tile.  staged() says whether every pull
 // source row of a tile exists (interior or wrapped), i.e. it is staged.
 struct TileMap {
-    int ntx, Nx, Ny, Nz, per;
+    int ntx, Nx, Ny, Nz, per, zoff;
     int dx, dj, dk;  // G decomposed as (x-segments, rows, planes)
     __device__ __forceinline__ void at(int t, int &xt, int &j, int &k) const {
         xt = t % ntx;
@@ -729,7 +733,7 @@ struct TileMap {
         k += dk + c;
     }
     __device__ __forceinline__ bool staged(int j, int k) const {
-        return ((per & 2) || (j > 0 && j < Ny - 1)) && ((per & 4) || (k > 0 && k < Nz - 1));
+        return ((per & 2) || (j > 0 && j < Ny - 1)) && ((per & (4 | KB_ZHALO)) || (k > 0 && k < Nz - 1));
     }
 };
 
@@ -753,9 +757,14 @@ __device__ __forceinline__ void tma_issue_tile(const TileMaps &mp, uint32_t dst,
     const uint32_t bytes = TBYTES + (mp.tc ? (uint32_t)TT : 0u);
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                  : "memory");
-    if (mp.tc) tma_load3(dst + TCLS * 2, mp.tc, x0, j, k, bar);  // own row's class bytes
+    // tensor-map z coordinates: the map spans the whole allocation, this
+    // range starts at plane zoff; with a z halo the neighbours are read as is
+    const bool zh = (m.per & KB_ZHALO) != 0;
     const int ym = j > 0 ? j - 1 : m.Ny - 1, yp = j < m.Ny - 1 ? j + 1 : 0;
-    const int zm = k > 0 ? k - 1 : m.Nz - 1, zp = k < m.Nz - 1 ? k + 1 : 0;
+    const int zm = ((k > 0 || zh) ? k - 1 : m.Nz - 1) + m.zoff;
+    const int zp = ((k < m.Nz - 1 || zh) ? k + 1 : 0) + m.zoff;
+    k += m.zoff;
+    if (mp.tc) tma_load3(dst + TCLS * 2, mp.tc, x0, j, k, bar);  // own row's class bytes
     const uint32_t R = TT * 2;  // bytes per staged row
     tma_load4(dst + 0 * R, mp.t3, x0, j, k, 0, bar);     // q 0, 1, 2: (0, 0)
     tma_load4(dst + 3 * R, mp.t1, x0, ym, k, 3, bar);    // q 3: c_y = +1
@@ -848,6 +857,7 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
     m.Ny = g.Ny;
     m.Nz = g.Nz;
     m.per = g.per;
+    m.zoff = g.zoff;
     m.at((int)gridDim.x, m.dx, m.dj, m.dk);
     if (t == 0) {
         for (int s = 0; s < TSTAGES; ++s) {
@@ -1100,16 +1110,19 @@ template <typename R, typename I, bool SR>
 static int launch_tma(void *f_out, const void *f_in, float *rho, float *ux, float *uy, float *uz,
                       const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s,
                       const LinkTable3 *links = nullptr) {
-    // the populations as a 4-D tensor (x, y, z, q) of 16-bit words
+    // the populations as a 4-D tensor (x, y, z, q) of 16-bit words over the
+    // whole allocation (a z-range starts at its plane g.zoff)
     TmaMaps mp;
-    const cuuint64_t dims[4] = {(cuuint64_t)g.Nx, (cuuint64_t)g.Ny, (cuuint64_t)g.Nz, 19};
+    const size_t nxy = (size_t)g.Nx * (size_t)g.Ny;
+    const void *fbase = (const char *)f_in - (size_t)g.zoff * nxy * 2;
+    const cuuint64_t dims[4] = {(cuuint64_t)g.Nx, (cuuint64_t)g.Ny, (cuuint64_t)(g.plane / nxy), 19};
     const cuuint64_t strides[3] = {(cuuint64_t)g.Nx * 2, (cuuint64_t)g.Nx * g.Ny * 2,
                                    (cuuint64_t)g.plane * 2};
     const cuuint32_t boxes[4][4] = {{TT, 1, 1, 1}, {TT, 1, 1, 2}, {TT, 1, 1, 3}, {8, 1, 1, 1}};
     const cuuint32_t es[4] = {1, 1, 1, 1};
     for (int n = 0; n < 4; ++n) {
         const CUresult r = tma_encode_fn()(&mp.m[n], CU_TENSOR_MAP_DATA_TYPE_UINT16, 4,
-                                           const_cast<void *>(f_in), dims, strides, boxes[n], es,
+                                           const_cast<void *>(fbase), dims, strides, boxes[n], es,
                                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);

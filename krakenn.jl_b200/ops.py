@@ -737,6 +737,32 @@ def fused_trt_step_3d_(f_out, f_in, rho, ux, uy, uz, is_solid, Nx, Ny, Nz, nu, L
          float(Lambda), periodic_mask(periodic), code, _stream())
 
 
+def fused_trt_step_3d_zrange_(f_out, f_in, rho, ux, uy, uz, is_solid, Nx, Ny, Nz_alloc, k_begin,
+                              k_end, nu, Lambda=3 / 16, periodic_xy=(False, False),
+                              deviation=False, stochastic_rounding=False):
+    """fused_trt_step_3d_ over the z-planes [k_begin, k_end) of a slab
+    allocation of Nz_alloc planes; planes k_begin - 1 and k_end are read as
+    halo planes.  Every array spans the whole allocation; only the range is
+    written.  No reference counterpart (the reference steps whole arrays,
+    src/kernels/li_bb_3d_v2.jl:31)."""
+    code = storage_dtype(f_in, deviation)
+    if storage_dtype(f_out, deviation) != code:
+        raise ValueError("f_in and f_out must have the same storage")
+    if stochastic_rounding:
+        if code not in (KB_F16_DEV, KB_BF16_DEV):
+            raise ValueError("stochastic rounding applies to float16/bfloat16 deviation storage")
+        code = KB_F16_DEV_SR if code == KB_F16_DEV else KB_BF16_DEV_SR
+    _match3(f_in, Nx, Ny, Nz_alloc); _match3(f_out, Nx, Ny, Nz_alloc)
+    _ptrs_3d_fields(code, Nx, Ny, Nz_alloc, rho=rho, ux=ux, uy=uy, uz=uz)
+    if is_solid is not None and tuple(is_solid.shape) != (Nz_alloc, Ny, Nx):
+        raise ValueError(f"is_solid must have shape (Nz_alloc, Ny, Nx) = ({Nz_alloc}, {Ny}, {Nx})")
+    px, py = periodic_xy
+    call("kb_fused_trt_step_3d_zrange", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
+         _t(ux, "ux"), _t(uy, "uy"), _t(uz, "uz"), _mask(is_solid), Nx, Ny, Nz_alloc,
+         int(k_begin), int(k_end), float(nu), float(Lambda), int(bool(px)) | 2 * int(bool(py)),
+         code, _stream())
+
+
 def fused_trt_libb_v2_step_3d_(f_out, f_in, rho, ux, uy, uz, is_solid, q_wall, uw_link_x,
                                uw_link_y, uw_link_z, Nx, Ny, Nz, nu, Lambda=3 / 16,
                                periodic=(False, False, False)):

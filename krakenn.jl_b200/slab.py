@@ -127,12 +127,28 @@ def exchange(f, slab: Slab, group=None):
             return
         exchange_in_process([f], [slab])
         return
+    # one fixed order on every rank (exchange_start): upward sends, upward
+    # receives, downward sends, downward receives, each in population order,
+    # so the matching per peer pair is the same even when up == down (two
+    # ranks)
+    for req in exchange_start(f, slab, group):
+        req.wait()
+
+
+def exchange_start(f, slab: Slab, group=None):
+    """`exchange` without the wait: the point-to-point operations are
+    posted and their requests returned (an empty list when there is nothing
+    in flight, e.g. one rank, where the ghosts are filled at once).  Wait on
+    every request before the next step reads `f`'s ghost planes.  On NCCL
+    the transfers run on the communicator's stream after the work already
+    queued on the current stream, so kernels launched afterwards overlap
+    them."""
+    if slab.world == 1:
+        exchange(f, slab, group)
+        return []
     import torch.distributed as dist
     top, bot, ghost_hi = slab.k0 + slab.nz - 1, slab.k0, slab.nz_alloc - 1
     p2p = []
-    # one fixed order on every rank: upward sends, upward receives,
-    # downward sends, downward receives, each in population order, so the
-    # matching per peer pair is the same even when up == down (two ranks)
     if slab.hi:
         p2p += [dist.P2POp(dist.isend, f[q, top], slab.up, group) for q in CZP]
     if slab.lo:
@@ -141,9 +157,7 @@ def exchange(f, slab: Slab, group=None):
         p2p += [dist.P2POp(dist.isend, f[q, bot], slab.down, group) for q in CZM]
     if slab.hi:
         p2p += [dist.P2POp(dist.irecv, f[q, ghost_hi], slab.up, group) for q in CZM]
-    if p2p:
-        for req in dist.batch_isend_irecv(p2p):
-            req.wait()
+    return dist.batch_isend_irecv(p2p) if p2p else []
 
 
 def exchange_in_process(fs, slabs):
@@ -174,7 +188,7 @@ class SlabTRT3D:
 
     def __init__(self, slab: Slab, Nx, Ny, nu=None, Lambda=3 / 16, periodic_xy=(False, False),
                  deviation=False, stochastic_rounding=False, mask=None, group=None,
-                 step_fn=None):
+                 step_fn=None, range_fn=None):
         self.slab, self.Nx, self.Ny = slab, Nx, Ny
         self.mask, self.group = mask, group
         if step_fn is None:
@@ -186,7 +200,15 @@ class SlabTRT3D:
                 ops.fused_trt_step_3d_(f_out, f_in, *m, mask, Nx, Ny, slab.nz_alloc, nu, Lambda,
                                        periodic=per, deviation=deviation,
                                        stochastic_rounding=stochastic_rounding)
-        self.step_fn = step_fn
+
+            def range_fn(f_out, f_in, moments, mask, k_begin, k_end):
+                m = moments if moments is not None else (None,) * 4
+                ops.fused_trt_step_3d_zrange_(f_out, f_in, *m, mask, Nx, Ny, slab.nz_alloc,
+                                              k_begin, k_end, nu, Lambda, periodic_xy=per[:2],
+                                              deviation=deviation,
+                                              stochastic_rounding=stochastic_rounding)
+        self.step_fn, self.range_fn = step_fn, range_fn
+        self._side = None  # CUDA side stream of step_overlapped, made on first use
 
     def shape(self):
         return (19, self.slab.nz_alloc, self.Ny, self.Nx)
@@ -195,3 +217,53 @@ class SlabTRT3D:
         """One step f_in -> f_out; afterwards f_out's ghosts are current."""
         self.step_fn(f_out, f_in, moments, self.mask)
         exchange(f_out, self.slab, self.group)
+
+    def overlapped(self) -> bool:
+        """True when step_overlapped splits the step: the slab has ghost
+        planes on both faces (no global z wall) and a range step exists."""
+        return self.range_fn is not None and self.slab.lo and self.slab.hi
+
+    def step_overlapped(self, f_out, f_in, moments=None):
+        """`step` with the exchange overlapped: the two real planes next to
+        the faces are stepped first, their crossing populations are posted
+        to the neighbours, and the interior planes are stepped while they
+        travel.  Identical real planes to `step` for round-to-nearest
+        storages; the non-crossing populations of f_out's ghost planes are
+        left as they were (nothing reads them).  Falls back to `step` on a
+        slab that ends at a global z wall."""
+        if not self.overlapped():
+            return self.step(f_out, f_in, moments)
+        s = self.slab
+        bot, top = s.k0, s.k0 + s.nz - 1
+
+        def faces():
+            self.range_fn(f_out, f_in, moments, self.mask, bot, bot + 1)
+            if top > bot:
+                self.range_fn(f_out, f_in, moments, self.mask, top, top + 1)
+            return exchange_start(f_out, s, self.group)
+
+        if not getattr(f_out, "is_cuda", False):
+            reqs = faces()
+            if top - bot > 1:
+                self.range_fn(f_out, f_in, moments, self.mask, bot + 1, top)
+            for req in reqs:
+                req.wait()
+            return
+        # on the GPU the face planes and their exchange run on a side stream
+        # beside the interior planes: both read only f_in and write disjoint
+        # planes of f_out, and the current stream joins the side stream
+        # before anything later reads f_out
+        import torch
+        main = torch.cuda.current_stream()
+        if self._side is None or self._side.device != main.device:
+            self._side = torch.cuda.Stream(device=main.device)
+        side = self._side
+        side.wait_stream(main)
+        with torch.cuda.stream(side):
+            reqs = faces()
+        if top - bot > 1:
+            self.range_fn(f_out, f_in, moments, self.mask, bot + 1, top)
+        with torch.cuda.stream(side):
+            for req in reqs:
+                req.wait()
+        main.wait_stream(side)

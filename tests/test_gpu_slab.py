@@ -77,3 +77,95 @@ def test_single_slab_periodic_ring_on_gpu(cuda, pkg):
         st.step(b, a)
         a, b = b, a
     assert torch.equal(s.real(a), full)
+
+
+def _range_cases():
+    out = []
+    for dtype, dev in [(torch.float64, False), (torch.float32, False), (torch.float32, True)]:
+        out.append((dtype, dev, 0))
+    for dtype in (torch.float16, torch.bfloat16):
+        for v in range(6):
+            out.append((dtype, True, v))
+    return out
+
+
+@pytest.mark.parametrize("dtype,deviation,variant", _range_cases())
+@pytest.mark.parametrize("Nx,per_xy", [(256, (1, 1)), (96, (0, 1)), (64, (1, 0))])
+def test_zrange_steps_match_whole_local_step(cuda, pkg, dtype, deviation, variant, Nx, per_xy):
+    """kb_fused_trt_step_3d_zrange over [1, 2), [Nz-2, Nz-1) and the planes
+    between equals one step of the whole local array (z non-periodic) on
+    every plane but the two halo planes, bit for bit, for every kernel
+    variant of the 16-bit storages (the staged row tiles need Nx % 8 == 0
+    and 16-byte rows: every Nx here runs them)."""
+    Ny, Nz = 5, 10
+    full, mask = _setup(pkg, Nx, Ny, Nz, dtype, deviation, seed=21)
+    fd = torch.float64 if dtype == torch.float64 else torch.float32
+    ref = torch.zeros_like(full)
+    got = torch.zeros_like(full)
+    rm = [torch.zeros((Nz, Ny, Nx), dtype=fd, device="cuda") for _ in range(4)]
+    gm = [torch.zeros((Nz, Ny, Nx), dtype=fd, device="cuda") for _ in range(4)]
+    pkg.set_trt3d_variant(variant)
+    try:
+        for m in (mask, None):
+            pkg.fused_trt_step_3d_(ref, full, *rm, m, Nx, Ny, Nz, 0.02, 0.25,
+                                   periodic=(*per_xy, 0), deviation=deviation)
+            for kb, ke in ((1, 2), (Nz - 2, Nz - 1), (2, Nz - 2)):
+                pkg.fused_trt_step_3d_zrange_(got, full, *gm, m, Nx, Ny, Nz, kb, ke, 0.02, 0.25,
+                                              periodic_xy=per_xy, deviation=deviation)
+            torch.cuda.synchronize()
+            assert torch.equal(got[:, 1:Nz - 1], ref[:, 1:Nz - 1])
+            for a, b in zip(gm, rm):
+                assert torch.equal(a[1:Nz - 1], b[1:Nz - 1])
+            # only the range is written
+            assert not got[:, 0].any() and not got[:, Nz - 1].any()
+    finally:
+        pkg.set_trt3d_variant(0)
+
+
+def test_zrange_rejects_halo_planes(cuda, pkg):
+    Nx, Ny, Nz = 64, 4, 6
+    f = torch.zeros((19, Nz, Ny, Nx), dtype=torch.float32, device="cuda")
+    g = torch.zeros_like(f)
+    for kb, ke in ((0, 3), (1, Nz), (3, 3), (4, 2)):
+        with pytest.raises(ValueError):
+            pkg.fused_trt_step_3d_zrange_(g, f, None, None, None, None, None, Nx, Ny, Nz, kb, ke,
+                                          0.02, 0.25)
+
+
+@pytest.mark.parametrize("dtype,deviation", [(torch.float64, False), (torch.float16, True),
+                                             (torch.float32, True)])
+@pytest.mark.parametrize("R", [1, 2, 3])
+def test_overlapped_slab_steps_match_full_grid_on_gpu(cuda, pkg, dtype, deviation, R):
+    """Each slab of a periodic z ring steps its two face planes, then its
+    interior, with range steps (the order of step_overlapped); the exchange
+    in one process then gives the full-grid CUDA step bit for bit.  With one
+    slab, step_overlapped itself runs (its exchange is the one-rank ghost
+    fill)."""
+    Nx, Ny, Nz = 256, 4, 12
+    full, mask = _setup(pkg, Nx, Ny, Nz, dtype, deviation, seed=17)
+    slabs = [pkg.slab.Slab(Nz, R, r, True) for r in range(R)]
+    a = [s.local_from_global(full).contiguous() for s in slabs]
+    b = [torch.zeros_like(x) for x in a]
+    masks = [s.local_from_global(mask).contiguous() for s in slabs]
+    steppers = [pkg.slab.SlabTRT3D(s, Nx, Ny, nu=0.02, Lambda=0.25, periodic_xy=(1, 0),
+                                   deviation=deviation, mask=mk) for s, mk in zip(slabs, masks)]
+    assert all(st.overlapped() for st in steppers)
+    g = torch.empty_like(full)
+    for _ in range(3):
+        pkg.fused_trt_step_3d_(g, full, None, None, None, None, mask, Nx, Ny, Nz, 0.02, 0.25,
+                               periodic=(1, 0, 1), deviation=deviation)
+        full, g = g, full
+        if R == 1:
+            steppers[0].step_overlapped(b[0], a[0])
+        else:
+            for st, x, y in zip(steppers, a, b):
+                s = st.slab
+                bot, top = s.k0, s.k0 + s.nz - 1
+                st.range_fn(y, x, None, st.mask, bot, bot + 1)
+                st.range_fn(y, x, None, st.mask, top, top + 1)
+                st.range_fn(y, x, None, st.mask, bot + 1, top)
+            pkg.slab.exchange_in_process(b, slabs)
+        a, b = b, a
+    torch.cuda.synchronize()
+    for s, x in zip(slabs, a):
+        assert torch.equal(s.real(x), full[:, s.z0:s.z1])
