@@ -406,6 +406,7 @@ def run_gpu(args):
                      "natconv_config4": bench_natconv(pkg, 512, 1e5, 2000)[0],
                      "d2q9_fused_4096": bench_d2q9_large(pkg),
                      "unfused_paths": bench_unfused_paths(pkg),
+                     "thermal_guo_paths": bench_thermal_guo_paths(pkg),
                      "batch_config3_short": bench_batch(pkg, max_steps=2000, check_every=100,
                                                         autotune=False)}
         line = {
@@ -605,6 +606,109 @@ def bench_unfused_paths(pkg, n2=4096, n3=256, steps=40, warmup=3):
         torch.cuda.empty_cache()
     return {"workload": f"A-A pair and unfused D2Q9 cavity step on a walled {n2}^2 grid; unfused "
                         f"D3Q19 cavity step at {n3}^3; {steps} steps each", "runs": out}
+
+
+def bench_thermal_guo_paths(pkg, nx2=4096, ny2=2048, n3=192, steps=20, warmup=3):
+    """Throughput of the reference's unfused multi-launch steps: the
+    Rayleigh-Benard DDF step (run_rayleigh_benard_2d: stream f and g, fixed
+    temperature faces, T, moments, thermal BGK, Boussinesq BGK) on an
+    nx2 x ny2 grid, the 3D natural-convection step (run_natural_convection_3d,
+    D3Q19 f and g) at n3^3, and the Guo-forced Poiseuille steps (stream with
+    x(/z) wrap and y walls, Guo BGK, force-corrected moments) in 2D and 3D.
+    GLUPS and the fraction of the measured copy bandwidth at each step's own
+    traffic: every launch reads its inputs and writes its outputs once,
+    b bytes per value and one mask byte per node (the per-step sums are in
+    the `bytes_per_node` fields)."""
+    import torch
+    peak, _ = hbm_peak()
+    out = {}
+    w9 = torch.tensor([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4, dtype=torch.float64, device="cuda")
+    w19 = torch.tensor([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12, dtype=torch.float64, device="cuda")
+    om, omT, bg = 1.0 / (3 * 0.02 + 0.5), 1.0 / (3 * 0.03 + 0.5), 1e-4
+
+    def timed(step):
+        for _ in range(warmup):
+            step()
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def record(key, nodes, ms, bpn):
+        out[key] = {"mlups": round(nodes / ms / 1e3, 1), "ms_per_step": round(ms, 4),
+                    "bytes_per_node": bpn,
+                    "hbm_frac": round(bpn * nodes / (ms * 1e-3) / 1e9 / peak, 4)}
+
+    for name, dt, b in (("f64", torch.float64, 8), ("f32", torch.float32, 4)):
+        Nx, Ny = nx2, ny2
+        sh = (9, Ny, Nx)
+        f = [(w9[:, None, None] * torch.ones(sh, dtype=torch.float64, device="cuda")).to(dt)
+             for _ in range(2)]
+        g = [(0.5 * w9[:, None, None] * torch.ones(sh, dtype=torch.float64, device="cuda")).to(dt)
+             for _ in range(2)]
+        T, rho, ux, uy = (torch.zeros((Ny, Nx), dtype=dt, device="cuda") for _ in range(4))
+        solid = torch.zeros((Ny, Nx), dtype=torch.bool, device="cuda")
+
+        def rb():
+            pkg.stream_periodic_x_wall_y_2d_(f[1], f[0], Nx, Ny)
+            pkg.stream_periodic_x_wall_y_2d_(g[1], g[0], Nx, Ny)
+            pkg.apply_fixed_temp_south_2d_(g[1], 1.0, Nx)
+            pkg.apply_fixed_temp_north_2d_(g[1], 0.0, Nx, Ny)
+            pkg.compute_temperature_2d_(T, g[1])
+            pkg.compute_macroscopic_2d_(rho, ux, uy, f[1])
+            pkg.collide_thermal_2d_(g[1], ux, uy, omT)
+            pkg.collide_boussinesq_2d_(f[1], T, solid, om, bg, 0.5)
+            f.reverse(); g.reverse()
+        # stream f, g 2*18b; T 10b; moments 12b; thermal BGK 20b; Boussinesq 19b + mask
+        record(f"rayleigh_benard_2d_{name}", Nx * Ny, timed(rb), 97 * b + 1)
+
+        def poiseuille2d():
+            pkg.stream_periodic_x_wall_y_2d_(f[1], f[0], Nx, Ny)
+            pkg.collide_guo_2d_(f[1], solid, om, 1e-6, 0.0)
+            pkg.compute_macroscopic_2d_(rho, ux, uy, f[1])
+            f.reverse()
+        # stream 18b; Guo BGK 18b + mask; moments 12b
+        record(f"poiseuille_guo_2d_{name}", Nx * Ny, timed(poiseuille2d), 48 * b + 1)
+        del f, g, T, rho, ux, uy, solid
+        torch.cuda.empty_cache()
+
+        N = n3
+        sh = (19, N, N, N)
+        f = [(w19[:, None, None, None] * torch.ones(sh, dtype=torch.float64, device="cuda")).to(dt)
+             for _ in range(2)]
+        g = [(0.5 * w19[:, None, None, None] * torch.ones(sh, dtype=torch.float64,
+                                                          device="cuda")).to(dt)
+             for _ in range(2)]
+        T, rho, ux, uy, uz = (torch.zeros((N, N, N), dtype=dt, device="cuda") for _ in range(5))
+        solid = torch.zeros((N, N, N), dtype=torch.bool, device="cuda")
+
+        def nc3():
+            pkg.stream_3d_(f[1], f[0], N, N, N)
+            pkg.stream_3d_(g[1], g[0], N, N, N)
+            pkg.apply_fixed_temp_west_3d_(g[1], 1.0, N, N)
+            pkg.apply_fixed_temp_east_3d_(g[1], 0.0, N, N, N)
+            pkg.compute_temperature_3d_(T, g[1])
+            pkg.compute_macroscopic_3d_(rho, ux, uy, uz, f[1])
+            pkg.collide_thermal_3d_(g[1], ux, uy, uz, omT)
+            pkg.collide_boussinesq_3d_(f[1], T, solid, om, bg, 0.5)
+            f.reverse(); g.reverse()
+        # stream f, g 2*38b; T 20b; moments 23b; thermal BGK 41b; Boussinesq 39b + mask
+        record(f"natural_convection_3d_{name}", N ** 3, timed(nc3), 199 * b + 1)
+
+        def poiseuille3d():
+            pkg.stream_periodic_xz_wall_y_3d_(f[1], f[0], N, N, N)
+            pkg.collide_guo_3d_(f[1], solid, om, 1e-6, 0.0, 0.0)
+            pkg.compute_macroscopic_forced_3d_(rho, ux, uy, uz, f[1], 1e-6, 0.0, 0.0)
+            f.reverse()
+        # stream 38b; Guo BGK 38b + mask; forced moments 23b
+        record(f"poiseuille_guo_3d_{name}", N ** 3, timed(poiseuille3d), 99 * b + 1)
+        del f, g, T, rho, ux, uy, uz, solid
+        torch.cuda.empty_cache()
+    return {"workload": f"unfused thermal DDF and Guo-forced steps: D2Q9 {nx2}x{ny2}, D3Q19 "
+                        f"{n3}^3; {steps} steps each", "runs": out}
 
 
 def bench_cavity2d(pkg, steps=20000, graph_steps=200):
