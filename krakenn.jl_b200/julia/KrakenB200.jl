@@ -120,6 +120,33 @@ function fused_trt_step_3d!(f_out::CuArray{T,4}, f_in::CuArray{T,4}, ρ, ux, uy,
         Nx, Ny, Nz, ν, Λ, per, dtype, _stream()))
 end
 
+"""
+Fused D3Q19 TRT step over the z-planes `k_begin .. k_end-1` (0-based, as in the C
+header) of a z-slab allocation of `Nz_alloc` planes whose planes 0 and `Nz_alloc-1`
+are halo planes, read as they are.  Every array spans the whole allocation; only the
+range is written.  No reference counterpart (the reference steps whole arrays).
+"""
+function fused_trt_step_3d_zrange!(f_out::CuArray{T,4}, f_in::CuArray{T,4}, ρ, ux, uy, uz,
+                                   is_solid, Nx, Ny, Nz_alloc, k_begin, k_end, ν;
+                                   Λ::Real=3/16, periodic_xy=(false, false),
+                                   dtype::Integer=kb_dtype(T)) where {T}
+    per = Int(periodic_xy[1]) | (Int(periodic_xy[2]) << 1)
+    _check("kb_fused_trt_step_3d_zrange", ccall((:kb_fused_trt_step_3d_zrange, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{UInt8},
+         Cint, Cint, Cint, Cint, Cint, Cdouble, Cdouble, Cint, Cint, Ptr{Cvoid}),
+        _ptr(f_out), _ptr(f_in), _ptr(ρ), _ptr(ux), _ptr(uy), _ptr(uz), _mask(is_solid),
+        Nx, Ny, Nz_alloc, k_begin, k_end, ν, Λ, per, dtype, _stream()))
+end
+
+"Ghost planes of one z-slab on a periodic z axis from its own end planes (one launch)."
+function slab_fill_ghosts_3d!(f::CuArray{T,4}, lo::Bool, hi::Bool;
+                              dtype::Integer=kb_dtype(T)) where {T}
+    Nx, Ny, Nz_alloc = size(f, 1), size(f, 2), size(f, 3)
+    _check("kb_slab_fill_ghosts_3d", ccall((:kb_slab_fill_ghosts_3d, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Cint, Cint, Cint, Cint, Cint, Ptr{Cvoid}),
+        _ptr(f), Nx, Ny, Nz_alloc, Int(lo), Int(hi), dtype, _stream()))
+end
+
 "stream_3d!(f_out, f_in, Nx, Ny, Nz) -- src/kernels/collide_stream_3d.jl:119"
 function stream_3d!(f_out::CuArray{T,4}, f_in::CuArray{T,4}, Nx, Ny, Nz) where {T}
     _check("kb_stream_3d", ccall((:kb_stream_3d, LIB), Cint,
