@@ -196,6 +196,50 @@ __device__ __forceinline__ LinkRecord<T> link_record(const LinkTable3 &L, int r)
                          (const T *)L.wz + r, L.n_rec};
 }
 
+// The link data of one record held in registers (read with constant link
+// indices once libb_prephase_3d is inlined).
+template <typename T>
+struct LinkRegs {
+    T qv[19], xv[19], yv[19], zv[19];
+    __device__ __forceinline__ T q(int a) const { return qv[a]; }
+    __device__ __forceinline__ T x(int a) const { return xv[a]; }
+    __device__ __forceinline__ T y(int a) const { return yv[a]; }
+    __device__ __forceinline__ T z(int a) const { return zv[a]; }
+};
+
+// libb_prephase_3d on record r of the compact table with every load issued
+// up front: the node's own populations and the 18 link fractions, then the
+// wall velocities of the cut links.  Read link by link, each cut link is a
+// branch on a load that must return first, so a node waits for up to 18
+// dependent rounds of memory latency; here it waits for two.  The
+// interpolation then runs on registers with the same expressions, so the
+// result equals the link-by-link form.  It pays in a kernel of cut nodes
+// only (trt_dev_cut_k); inside a kernel over every node its ~90 extra live
+// values cut the residency of all nodes (the one-node FP64 table step went
+// from 0.80 to 1.29 ms at 256^3 with it), so those keep the direct form.
+template <typename T, typename I, typename F, typename Load = LoadSame>
+__device__ __forceinline__ void libb_prephase_3d_record(const F *__restrict__ f0, I P,
+                                                        const LinkTable3 &L, int r, T *p,
+                                                        Load ld = Load()) {
+    const LinkRecord<T> rec = link_record<T>(L, r);
+    T own[19];
+    LinkRegs<T> lk;
+    own[0] = lk.qv[0] = lk.xv[0] = lk.yv[0] = lk.zv[0] = T(0);
+#pragma unroll
+    for (int a = 1; a < 19; ++a) {
+        own[a] = (T)ld(f0[(I)a * P]);
+        lk.qv[a] = rec.q(a);
+    }
+#pragma unroll
+    for (int a = 1; a < 19; ++a) {
+        const bool cut = lk.qv[a] > T(0);
+        lk.xv[a] = cut ? rec.x(a) : T(0);
+        lk.yv[a] = cut ? rec.y(a) : T(0);
+        lk.zv[a] = cut ? rec.z(a) : T(0);
+    }
+    libb_prephase_3d(own, (I)1, lk, p, LoadSame());
+}
+
 // Deviation-storage step with the compact cut-link table (kb_d3q19_dev.cu);
 // `variant` follows kernel 1 of kb_set_kernel_variant (0 automatic, 5 the
 // staged row tiles for 16-bit storages, anything else one node per thread).

@@ -802,6 +802,7 @@ __device__ __forceinline__ void tma_issue_tile(const TileMaps &mp, uint32_t dst,
 // the same pull, interpolated bounce-back and collision as the one-node
 // kernel trt_dev_links_k.  The staged step stores every other node, so the
 // two kernels write disjoint nodes, read only f_in, and run side by side.
+// The link data are loaded up front (libb_prephase_3d_record).
 template <typename R, bool MOM, typename I, bool SR>
 __global__ void __launch_bounds__(BX) trt_dev_cut_k(R *__restrict__ fo, const R *__restrict__ fi,
                                                      float *__restrict__ rho_o, float *__restrict__ ux_o,
@@ -816,7 +817,7 @@ __global__ void __launch_bounds__(BX) trt_dev_cut_k(R *__restrict__ fo, const R 
     const I P = (I)g.plane;
     float d[19];
     pull19_at(fi + c, P, pull_geometry<I>(g, i, j, k), d, DevLoad<R>());
-    libb_prephase_3d(fi + c, P, link_record<float>(L, (int)r), d, DevLoad<R>());
+    libb_prephase_3d_record(fi + c, P, L, (int)r, d, DevLoad<R>());
     float o[19], rho, ux, uy, uz;
     trt_dev_collide(d, o, rho, ux, uy, uz, sp, sm);
     R *__restrict__ o0 = fo + c;
