@@ -1247,6 +1247,44 @@ def bench_slab(pkg, n, storage, steps, warmup, rank, world):
             "halo_bytes_sent_per_rank_per_step": halo}
 
 
+def bench_slab2d(pkg, steps, warmup, rank, world, Nx=4096, Ny=4096):
+    """One walled Nx x Ny D2Q9 grid (fused TRT, FP64 and FP32) split along y
+    over `world` ranks (strong scaling): per step the fused step on each
+    slab's local rows and the exchange of the three crossing populations per
+    face (NCCL point-to-point).  Timed on the device with CUDA events, max
+    over ranks."""
+    import torch
+    slab = pkg.slab.Slab(Ny, world, rank, False)
+    w9 = torch.tensor([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4, dtype=torch.float64, device="cuda")
+    out = {}
+    for name, dt, b in (("f64", torch.float64, 8), ("f32", torch.float32, 4)):
+        a = (w9[:, None, None] * torch.ones((9, slab.nz_alloc, Nx), dtype=torch.float64,
+                                           device="cuda")).to(dt)
+        c = torch.empty_like(a)
+        st = pkg.slab.SlabD2Q9(slab, Nx, "trt", nu=NU, Lambda=LAMBDA)
+        for _ in range(warmup):
+            st.step(c, a)
+            a, c = c, a
+        torch.cuda.synchronize()
+        barrier(world)
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(steps):
+            st.step(c, a)
+            a, c = c, a
+        e1.record()
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), world)
+        out[name] = {"mlups": round(Nx * Ny * steps / (ms * 1e-3) / 1e6, 1),
+                     "ms_per_step": round(ms / steps, 4),
+                     "halo_bytes_sent_per_rank_per_step":
+                         (int(slab.lo) + int(slab.hi)) * 3 * Nx * b}
+        del a, c
+        torch.cuda.empty_cache()
+    return {"workload": f"walled D2Q9 TRT {Nx}x{Ny} split along y over {world} rank(s)",
+            "scaling": "strong", "rows_per_rank": slab.nz, "runs": out}
+
+
 def _extrude(plane, n):
     import torch
     out = torch.empty((19, n, n, n), dtype=plane.dtype, device=plane.device)
@@ -1280,6 +1318,8 @@ def run_other(args):
             r = bench_output(pkg, n=args.grid)
     elif args.workload == "slab":
         r = bench_slab(pkg, args.grid, args.storage, max(args.steps, 20), args.warmup, rank, world)
+    elif args.workload == "slab2d":
+        r = bench_slab2d(pkg, max(args.steps, 20), args.warmup, rank, world)
     elif args.workload == "libb":
         if rank == 0:
             r = bench_libb(pkg, N=args.grid, R=40.0 * args.grid / 256,
@@ -1317,7 +1357,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the short measurements of the other configurations")
-    ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "cavity2d", "batch", "natconv", "warmstart", "surrogate", "slab",
+    ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "cavity2d", "batch", "natconv", "warmstart", "surrogate", "slab", "slab2d",
                              "libb", "output"])
     args = ap.parse_args()
     if args.warmup < 3:

@@ -6,7 +6,7 @@ reference's kernel wrappers (`ops`) and step-loop drivers (`drivers`).
 The directory name is not a Python identifier; load it with
 `__graft_entry__.load_package()` (registered as module `krakenn_b200`).
 """
-from . import _lib, batch, drivers, krk, lattice, libb, ops, output, sharding, slab, surrogate  # noqa: F401
+from . import _lib, batch, checkpoint, drivers, krk, lattice, libb, ops, output, sharding, slab, surrogate  # noqa: F401
 from ._lib import KrakenArgumentError, KrakenError, version  # noqa: F401
 from .drivers import (LBMConfig, initialize_2d, initialize_3d, omega, reynolds,  # noqa: F401
                       run_cavity_2d, run_cavity_3d, run_natural_convection_2d,

@@ -1,4 +1,4 @@
-"""One D3Q19 grid over several GPUs: slab decomposition along z.
+"""One grid over several GPUs: D3Q19 slabs along z, D2Q9 slabs along y.
 
 The reference runs one grid on one device and has no distributed backend;
 this module is the B200 extension for grids larger than one GPU (or to
@@ -26,6 +26,12 @@ ends at a global z wall keeps the step's own half-way bounce-back there.
 Every storage and kernel variant of kb_fused_trt_step_3d thus runs
 unchanged, and a round-to-nearest storage gives the full-grid result bit
 for bit.  The cost is two ghost planes of work per slab.
+
+A D2Q9 grid splits the same way along y (`SlabD2Q9`): `Slab` then counts
+rows, the local arrays are (9, ny_alloc, Nx), and three populations cross
+each face, c_y = +1 (q = 2, 5, 6) and c_y = -1 (q = 4, 7, 8), each one
+contiguous row.  The fused 2D steps wall all four sides, so the split is of
+a walled y axis.
 """
 from __future__ import annotations
 
@@ -34,6 +40,9 @@ from dataclasses import dataclass
 # populations that cross a z face upward (c_z = +1) and downward (c_z = -1)
 CZP = (5, 11, 12, 15, 16)
 CZM = (6, 13, 14, 17, 18)
+# D2Q9 populations that cross a y face upward (c_y = +1) and downward
+CYP = (2, 5, 6)
+CYM = (4, 7, 8)
 
 
 @dataclass(frozen=True)
@@ -99,43 +108,48 @@ class Slab:
         """Global z index of every local plane (ghosts included, wrapped)."""
         return [(self.z0 - self.k0 + k) % self.Nz for k in range(self.nz_alloc)]
 
-    def local_from_global(self, full):
+    def local_from_global(self, full, axis=-3):
         """The local array (ghosts filled) cut from a full-grid array whose
-        z axis is dimension -3, e.g. populations (Q, Nz, Ny, Nx) or moments
-        (Nz, Ny, Nx)."""
-        return full[..., self.global_planes(), :, :].clone() if hasattr(full, "clone") else \
-            full[..., self.global_planes(), :, :].copy()
+        split axis is dimension `axis`: -3 for z in (Q, Nz, Ny, Nx) or
+        (Nz, Ny, Nx), -2 for y in the D2Q9 (Q, Ny, Nx) or (Ny, Nx)."""
+        idx = (Ellipsis, self.global_planes()) + (slice(None),) * (-axis - 1)
+        return full[idx].clone() if hasattr(full, "clone") else full[idx].copy()
 
-    def real(self, local):
-        """View of the real planes of a local array (z axis dimension -3)."""
-        return local[..., self.k0:self.k0 + self.nz, :, :]
+    def real(self, local, axis=-3):
+        """View of the real planes (rows) of a local array."""
+        idx = (Ellipsis, slice(self.k0, self.k0 + self.nz)) + (slice(None),) * (-axis - 1)
+        return local[idx]
 
 
-def exchange(f, slab: Slab, group=None):
+def exchange(f, slab: Slab, group=None, cross=(CZP, CZM)):
     """Fill the ghost planes of the local populations `f` (19, nz_alloc, Ny,
     Nx) from the neighbouring slabs, after a step wrote `f`.  With one rank
     the ghosts of a periodic z axis are copies of the slab's own end planes.
-    Every rank must call this at the same point of its step sequence."""
+    Every rank must call this at the same point of its step sequence.
+    `cross` names the populations that cross a face upward and downward
+    (CZP, CZM for D3Q19 z-slabs; CYP, CYM for D2Q9 y-slabs, f (9, ny_alloc,
+    Nx))."""
     if slab.world == 1:
         if not (slab.lo or slab.hi):
             return
-        if getattr(f, "is_cuda", False):  # one launch for the ten planes
+        if getattr(f, "is_cuda", False) and f.dim() == 4 and cross == (CZP, CZM):
+            # one launch for the ten planes
             import torch
             from . import ops
             ops.slab_fill_ghosts_3d_(f, slab.lo, slab.hi,
                                      deviation=f.dtype in (torch.float16, torch.bfloat16))
             return
-        exchange_in_process([f], [slab])
+        exchange_in_process([f], [slab], cross)
         return
     # one fixed order on every rank (exchange_start): upward sends, upward
     # receives, downward sends, downward receives, each in population order,
     # so the matching per peer pair is the same even when up == down (two
     # ranks)
-    for req in exchange_start(f, slab, group):
+    for req in exchange_start(f, slab, group, cross):
         req.wait()
 
 
-def exchange_start(f, slab: Slab, group=None):
+def exchange_start(f, slab: Slab, group=None, cross=(CZP, CZM)):
     """`exchange` without the wait: the point-to-point operations are
     posted and their requests returned (an empty list when there is nothing
     in flight, e.g. one rank, where the ghosts are filled at once).  Wait on
@@ -144,23 +158,24 @@ def exchange_start(f, slab: Slab, group=None):
     queued on the current stream, so kernels launched afterwards overlap
     them."""
     if slab.world == 1:
-        exchange(f, slab, group)
+        exchange(f, slab, group, cross)
         return []
     import torch.distributed as dist
     top, bot, ghost_hi = slab.k0 + slab.nz - 1, slab.k0, slab.nz_alloc - 1
+    cp, cm = cross
     p2p = []
     if slab.hi:
-        p2p += [dist.P2POp(dist.isend, f[q, top], slab.up, group) for q in CZP]
+        p2p += [dist.P2POp(dist.isend, f[q, top], slab.up, group) for q in cp]
     if slab.lo:
-        p2p += [dist.P2POp(dist.irecv, f[q, 0], slab.down, group) for q in CZP]
+        p2p += [dist.P2POp(dist.irecv, f[q, 0], slab.down, group) for q in cp]
     if slab.lo:
-        p2p += [dist.P2POp(dist.isend, f[q, bot], slab.down, group) for q in CZM]
+        p2p += [dist.P2POp(dist.isend, f[q, bot], slab.down, group) for q in cm]
     if slab.hi:
-        p2p += [dist.P2POp(dist.irecv, f[q, ghost_hi], slab.up, group) for q in CZM]
+        p2p += [dist.P2POp(dist.irecv, f[q, ghost_hi], slab.up, group) for q in cm]
     return dist.batch_isend_irecv(p2p) if p2p else []
 
 
-def exchange_in_process(fs, slabs):
+def exchange_in_process(fs, slabs, cross=(CZP, CZM)):
     """The exchange of `exchange` for all slabs of one grid held by one
     process (a list of local arrays, one per slab, e.g. to run a grid in
     slabs on one GPU or to check the decomposition against the full grid)."""
@@ -168,11 +183,11 @@ def exchange_in_process(fs, slabs):
     for r, (f, s) in enumerate(zip(fs, slabs)):
         if s.lo:
             below, sb = fs[(r - 1) % R], slabs[(r - 1) % R]
-            for q in CZP:
+            for q in cross[0]:
                 f[q, 0] = below[q, sb.k0 + sb.nz - 1]
         if s.hi:
             above, sa = fs[(r + 1) % R], slabs[(r + 1) % R]
-            for q in CZM:
+            for q in cross[1]:
                 f[q, s.nz_alloc - 1] = above[q, sa.k0]
 
 
@@ -267,3 +282,63 @@ class SlabTRT3D:
             for req in reqs:
                 req.wait()
         main.wait_stream(side)
+
+
+class SlabD2Q9:
+    """One y-slab of a walled D2Q9 grid: the library's fused 2D step on the
+    local array (9, ny_alloc, Nx), then the exchange of the three crossing
+    populations per face (CYP up, CYM down).  The fused 2D steps wall every
+    side of their grid, so the real rows pull across into the ghost rows
+    (the neighbour's populations) and a slab at a global y wall keeps the
+    step's own wall; the real rows equal the full-grid step bit for bit.
+
+    kind: "bgk" (fused_bgk_step!, omega), "trt" (fused_trt_step!, nu and
+    Lambda), "cavity" (the one-launch run_cavity_2d step, omega and u_lid;
+    the lid is the top slab's top row) or "movingwall" (the moving-wall
+    half-way bounce-back lid).  `step_fn(f_out, f_in, moments, mask)`
+    replaces the library step (a test plugs the oracle in here).
+    `moments` is None or three local (ny_alloc, Nx) arrays rho, ux, uy; the
+    2D fused steps always write them, so the slab keeps scratch ones."""
+
+    KINDS = ("bgk", "trt", "cavity", "movingwall")
+
+    def __init__(self, slab: Slab, Nx, kind="bgk", omega=None, nu=None, Lambda=3 / 16,
+                 u_lid=0.0, mask=None, group=None, step_fn=None):
+        if slab.periodic_z:
+            raise ValueError("the fused D2Q9 steps wall the y axis: a y-slab split cannot be "
+                             "periodic")
+        if kind not in self.KINDS:
+            raise ValueError(f"kind must be one of {self.KINDS}")
+        self.slab, self.Nx, self.kind = slab, Nx, kind
+        self.mask, self.group = mask, group
+        self._scratch = None
+        if step_fn is None:
+            from . import ops
+            ny = slab.nz_alloc
+
+            def step_fn(f_out, f_in, moments, mask):
+                rho, ux, uy = moments
+                if kind == "bgk":
+                    ops.fused_bgk_step_(f_out, f_in, rho, ux, uy, mask, Nx, ny, omega)
+                elif kind == "trt":
+                    ops.fused_trt_step_(f_out, f_in, rho, ux, uy, mask, Nx, ny, nu, Lambda)
+                elif kind == "cavity":
+                    ops.cavity_step_2d_(f_out, f_in, rho, ux, uy, mask, Nx, ny, omega, u_lid)
+                else:
+                    ops.cavity_movingwall_step_2d_(f_out, f_in, rho, ux, uy, mask, Nx, ny,
+                                                   omega, u_lid)
+        self.step_fn = step_fn
+
+    def shape(self):
+        return (9, self.slab.nz_alloc, self.Nx)
+
+    def step(self, f_out, f_in, moments=None):
+        """One step f_in -> f_out; afterwards f_out's ghost rows are current."""
+        if moments is None:
+            if self._scratch is None or self._scratch[0].dtype != f_in.dtype:
+                import torch
+                self._scratch = [torch.empty((self.slab.nz_alloc, self.Nx), dtype=f_in.dtype,
+                                             device=f_in.device) for _ in range(3)]
+            moments = self._scratch
+        self.step_fn(f_out, f_in, moments, self.mask)
+        exchange(f_out, self.slab, self.group, (CYP, CYM))

@@ -219,3 +219,125 @@ def test_slab_exchange_reports_a_missing_peer(pkg):
             p.kill()
     assert res[1] == "left"
     assert res[0] != "no error", res
+
+
+# ------------------------------------------------------------ D2Q9 y-slabs
+
+W9 = np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4)
+
+
+def _fields2(Nx, Ny, with_mask, seed=13):
+    rng = np.random.default_rng(seed)
+    f = W9[:, None, None] * (1 + 0.05 * rng.standard_normal((9, Ny, Nx)))
+    m = (rng.random((Ny, Nx)) < 0.1).astype(np.uint8) if with_mask else None
+    return f, m
+
+
+def _oracle_step2(orc, kind):
+    om, u_lid = 1.0 / (3 * 0.02 + 0.5), 0.1
+    sp, sm = orc.trt_rates(0.02, 0.25)
+
+    def step(f_out, f_in, moments, mask):
+        a, b = f_out.numpy(), f_in.numpy()
+        rho, ux, uy = (t.numpy() for t in moments)
+        if kind == "bgk":
+            orc.fused_bgk_2d(a, b, rho, ux, uy, mask, om)
+        elif kind == "trt":
+            orc.fused_trt_2d(a, b, rho, ux, uy, mask, sp, sm)
+        else:
+            orc.cavity_movingwall_bgk_2d(a, b, rho, ux, uy, mask, om, u_lid)
+    return step
+
+
+def _full2(orc, Nx, Ny, kind, steps, with_mask):
+    f, m = _fields2(Nx, Ny, with_mask)
+    g = np.empty_like(f)
+    mom = [torch.zeros((Ny, Nx), dtype=torch.float64) for _ in range(3)]
+    step = _oracle_step2(orc, kind)
+    a, b = torch.from_numpy(f), torch.from_numpy(g)
+    for _ in range(steps):
+        step(b, a, mom, m)
+        a, b = b, a
+    return a.numpy(), [t.numpy() for t in mom]
+
+
+def _worker2(rank, world, port, cfg, out):
+    import sys
+    sys.path.insert(0, str(ROOT))
+    import __graft_entry__ as graft
+    pkg, orc = graft.load_package(), graft.load_oracle()
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        Nx, Ny, kind, steps, with_mask = cfg
+        slab = pkg.slab.Slab(Ny, world, rank, False)
+        f, m = _fields2(Nx, Ny, with_mask)
+        ml = np.ascontiguousarray(slab.local_from_global(m, axis=-2)) if m is not None else None
+        st = pkg.slab.SlabD2Q9(slab, Nx, kind, mask=ml, step_fn=_oracle_step2(orc, kind))
+        a = torch.from_numpy(np.ascontiguousarray(slab.local_from_global(f, axis=-2)))
+        b = torch.zeros_like(a)
+        mom = [torch.zeros((slab.nz_alloc, Nx), dtype=torch.float64) for _ in range(3)]
+        for _ in range(steps):
+            st.step(b, a, mom)
+            a, b = b, a
+        out.put((rank, slab.z0, slab.z1, slab.real(a, axis=-2).numpy().copy(),
+                 [slab.real(t, axis=-2).numpy().copy() for t in mom]))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,cfg", [
+    (2, (7, 10, "bgk", 4, True)),
+    (3, (6, 11, "trt", 3, True)),
+    (3, (8, 9, "movingwall", 4, False)),
+])
+def test_d2q9_y_slabs_over_gloo_ranks_match_full_grid(orc, world, cfg):
+    """D2Q9 y-slabs on gloo ranks, the oracle's fused step as the local step,
+    against the full-grid oracle bit for bit (populations and moments)."""
+    Nx, Ny, kind, steps, with_mask = cfg
+    ref, ref_mom = _full2(orc, Nx, Ny, kind, steps, with_mask)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker2, args=(r, world, port, cfg, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=180) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    covered = []
+    for rank, y0, y1, got, mom in res:
+        assert np.array_equal(got, ref[:, y0:y1]), rank
+        for a, b in zip(mom, ref_mom):
+            assert np.array_equal(a, b[y0:y1]), rank
+        covered += list(range(y0, y1))
+    assert sorted(covered) == list(range(Ny))
+
+
+@pytest.mark.parametrize("R", [1, 2, 4])
+@pytest.mark.parametrize("kind", ["bgk", "trt", "movingwall"])
+def test_d2q9_y_slabs_in_one_process_match_full_grid(pkg, orc, R, kind):
+    Nx, Ny, steps = 6, 12, 3
+    ref, _ = _full2(orc, Nx, Ny, kind, steps, True)
+    f, m = _fields2(Nx, Ny, True)
+    slabs = [pkg.slab.Slab(Ny, R, r, False) for r in range(R)]
+    a = [torch.from_numpy(np.ascontiguousarray(s.local_from_global(f, axis=-2))) for s in slabs]
+    b = [torch.zeros_like(x) for x in a]
+    masks = [np.ascontiguousarray(s.local_from_global(m, axis=-2)) for s in slabs]
+    step = _oracle_step2(orc, kind)
+    mom = [[torch.zeros((s.nz_alloc, Nx), dtype=torch.float64) for _ in range(3)] for s in slabs]
+    for _ in range(steps):
+        for x, y, mk, mm in zip(a, b, masks, mom):
+            step(y, x, mm, mk)
+        pkg.slab.exchange_in_process(b, slabs, (pkg.slab.CYP, pkg.slab.CYM))
+        a, b = b, a
+    for s, x in zip(slabs, a):
+        assert np.array_equal(s.real(x, axis=-2).numpy(), ref[:, s.z0:s.z1])
+
+
+def test_d2q9_slab_rejects_periodic_split(pkg):
+    with pytest.raises(ValueError):
+        pkg.slab.SlabD2Q9(pkg.slab.Slab(8, 2, 0, True), 4, "bgk", omega=1.0)
