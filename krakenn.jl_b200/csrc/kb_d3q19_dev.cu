@@ -1090,6 +1090,12 @@ static int launch_tma_k(const TmaMaps &mp, R *fo, const R *fi, float *rho, float
     static int occ = -1;  // resident blocks per SM of this instantiation
     if (occ < 0) {
         int n = 0;
+        // the stage ring may exceed the 48 KB default of dynamic shared memory
+        if (cudaFuncSetAttribute(trt_dev_tma_k<R, MOM, SOLID, I, SR, LINKS>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TSMEM) !=
+            cudaSuccess)
+            return set_error(KB_ERR_CUDA, "kb_fused_trt_step_3d: %zu bytes of shared memory per "
+                             "block refused", TSMEM);
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trt_dev_tma_k<R, MOM, SOLID, I, SR, LINKS>,
                                                           TTHREADS, TSMEM) != cudaSuccess || n < 1) {
             cudaGetLastError();
