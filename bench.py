@@ -230,34 +230,56 @@ def max_over_ranks(x, world):
 
 # ---------------------------------------------------------------- CPU arm --
 
-def cpu_reference_mlups(n, steps_cap, budget_s, threads):
-    """The oracle port (C restatement of the reference's CPU path, OpenMP)
-    on a periodic n^3 D3Q19 TRT Taylor-Green vortex.  Returns (MLUPS,
-    steps, seconds, nz) timed after one warm-up step; the z extent is cut to
-    keep one step near budget_s/steps_cap seconds on slow hosts."""
+# Precision of the reference's CPU path that a GPU storage is timed against:
+# FP64 for FP64; the reference's T = Float32 path (its narrowest) for the
+# FP32 storages and the 16-bit deviation storages.
+CPU_PRECISION = {"f64": "f64", "f32": "f32", "f32dev": "f32", "f16dev": "f32", "bf16dev": "f32",
+                 "f16dev_sr": "f32", "bf16dev_sr": "f32"}
+
+
+def tgv_config(n, storage, world):
+    """The `config` of the TGV bench line, shared by the GPU and reference arms."""
+    return {"workload": f"D3Q19 TRT periodic Taylor-Green {n}^3, Lambda=1/4, nu={NU}, "
+                        f"u0={U0}, rho0=1", "grid": [n, n, n], "storage": storage,
+            "moments": f"written every {CHECK_EVERY} steps",
+            "l2": "inputs larger than L2 (no flush)",
+            "parallelism": f"replicas x{world}" if world > 1 else "none"}
+
+
+def cpu_reference_mlups(n, steps_cap, budget_s, threads, precision="f32", warmup=1):
+    """The oracle port (C restatement of the reference's CPU path, OpenMP) on
+    a periodic n^3 D3Q19 TRT Taylor-Green vortex, in FP64 or in the
+    reference's Float32 arithmetic.  Returns (MLUPS, steps, seconds, nz) timed
+    after `warmup` untimed steps; the z extent is cut to keep one step near
+    budget_s/steps_cap seconds on slow hosts (the first warm-up step sizes
+    it)."""
     import numpy as np
     import __graft_entry__ as graft
     orc = graft.load_oracle()
     pkg = graft.load_package()
     orc.set_threads(threads)
+    dt_np = np.float64 if precision == "f64" else np.float32
+    step = orc.fused_trt_3d if precision == "f64" else orc.fused_trt_3d_f32
     nz = n
-    plane = pkg.drivers.taylor_green_3d_populations(n, U0, Nz=1)
+    plane = pkg.drivers.taylor_green_3d_populations(n, U0, Nz=1).astype(dt_np)
     f = np.ascontiguousarray(np.broadcast_to(plane, (19, nz, n, n)))
     g = np.empty_like(f)
     sp, sm = orc.trt_rates(NU, LAMBDA)
     t0 = time.perf_counter()
-    orc.fused_trt_3d(g, f, None, None, sp, sm, (1, 1, 1))
+    step(g, f, None, None, sp, sm, (1, 1, 1))
     t1 = time.perf_counter() - t0
     per_step_budget = budget_s / max(1, steps_cap)
     if t1 > per_step_budget and nz > 8:
         nz = max(8, int(nz * per_step_budget / t1))
         f = np.ascontiguousarray(np.broadcast_to(plane, (19, nz, n, n)))
         g = np.empty_like(f)
-        orc.fused_trt_3d(g, f, None, None, sp, sm, (1, 1, 1))
+    for _ in range(max(0, warmup - 1) if nz == n else max(1, warmup)):
+        step(g, f, None, None, sp, sm, (1, 1, 1))
+        f, g = g, f
     steps = 0
     t0 = time.perf_counter()
     while steps < steps_cap:
-        orc.fused_trt_3d(g, f, None, None, sp, sm, (1, 1, 1))
+        step(g, f, None, None, sp, sm, (1, 1, 1))
         f, g = g, f
         steps += 1
         if time.perf_counter() - t0 > budget_s:
@@ -266,22 +288,29 @@ def cpu_reference_mlups(n, steps_cap, budget_s, threads):
     return steps * n * n * nz / dt / 1e6, steps, dt, nz
 
 
+def _cpu_sample(n, nz, steps, warmup, precision, threads):
+    arith = "FP64" if precision == "f64" else "FP32 (the reference's T=Float32 path)"
+    return (f"periodic D3Q19 TRT Taylor-Green {n}x{n}x{nz} (z cut to bound the run), {steps} "
+            f"steps after {warmup} warm-up, {arith}, C restatement of the reference CPU path "
+            f"(Julia reference not runnable here), OpenMP {threads} threads")
+
+
 def run_reference(args):
     rank, world, _ = dist_setup(args.gpus)
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    mlups, steps, dt, nz = cpu_reference_mlups(N_GRID, max(1, args.steps), 150.0, threads)
-    sample = (f"periodic D3Q19 TRT Taylor-Green {N_GRID}x{N_GRID}x{nz} (z cut to bound the run), "
-              f"{steps} steps after 1 warm-up, FP64, C restatement of the reference CPU path "
-              f"(Julia reference not runnable here), OpenMP {threads} threads")
+    prec = CPU_PRECISION[args.storage]
+    warmup = max(1, args.warmup)
+    mlups, steps, dt, nz = cpu_reference_mlups(N_GRID, max(1, args.steps), 150.0, threads,
+                                               prec, warmup)
+    sample = _cpu_sample(N_GRID, nz, steps, warmup, prec, threads)
     line = {"impl": "reference", "metric": METRIC, "value": round(mlups, 3), "unit": "MLUPS",
-            "n_gpus": args.gpus, "steps": steps, "warmup": 1, "ms_per_step": round(1e3 * dt / steps, 3),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": f"D3Q19 TRT periodic Taylor-Green {N_GRID}^3, Lambda=1/4, "
-                                   f"nu={NU}, u0={U0}", "grid": [N_GRID, N_GRID, N_GRID],
-                       "storage": "f64", "parallelism": "host OpenMP"},
+            "n_gpus": args.gpus, "steps": steps, "warmup": warmup,
+            "ms_per_step": round(1e3 * dt / steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": prec, "data": "synthetic",
+            "config": tgv_config(N_GRID, args.storage, world),
             "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": threads,
                              "kind": "port", "sample": sample},
             "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0,
@@ -391,17 +420,22 @@ def run_gpu(args):
 
     line = None
     if rank == 0:
-        cpu = None
+        cpu = cpu64 = None
         if not args.no_cpu_baseline and world == 1:
             threads = os.cpu_count() or 1
-            mlups, steps, dt, nz = cpu_reference_mlups(n, 20, 20.0, threads)
+            prec = CPU_PRECISION[args.storage]
+            mlups, steps, dt, nz = cpu_reference_mlups(n, 20, 15.0, threads, prec, 3)
             cpu = {"value": round(mlups, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
-                   "sample": (f"{steps} steps of the periodic D3Q19 TRT Taylor-Green on "
-                              f"{n}x{n}x{nz} nodes, FP64, C restatement of the reference CPU path, "
-                              f"{dt:.1f} s")}
+                   "sample": _cpu_sample(n, nz, steps, 3, prec, threads) + f", {dt:.1f} s"}
+            if prec != "f64" and not args.no_extra:
+                mlups, steps, dt, nz = cpu_reference_mlups(n, 20, 15.0, threads, "f64", 3)
+                cpu64 = {"value": round(mlups, 3), "unit": "MLUPS", "cores": threads,
+                         "kind": "port",
+                         "sample": _cpu_sample(n, nz, steps, 3, "f64", threads) + f", {dt:.1f} s"}
         extra = None
         if not args.no_extra and world == 1:
-            extra = {"tgv_config2_precisions": bench_tgv_precisions(pkg, n, 2000),
+            extra = {"cpu_baseline_f64": cpu64,
+                     "tgv_config2_precisions": bench_tgv_precisions(pkg, n, 2000),
                      "cavity2d_config1": bench_cavity2d(pkg, steps=20000),
                      "natconv_config4": bench_natconv(pkg, 512, 1e5, 2000)[0],
                      "d2q9_fused_4096": bench_d2q9_large(pkg),
@@ -414,11 +448,7 @@ def run_gpu(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dlabel,
             "data": "synthetic",
-            "config": {"workload": f"D3Q19 TRT periodic Taylor-Green {n}^3, Lambda=1/4, nu={NU}, "
-                                   f"u0={U0}, rho0=1", "grid": [n, n, n], "storage": args.storage,
-                       "moments": f"written every {CHECK_EVERY} steps",
-                       "l2": "inputs larger than L2 (no flush)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "config": tgv_config(n, args.storage, world),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
@@ -835,33 +865,60 @@ def _fp64_mrt_cavity(pkg, N, nu, u_lid, steps, graph_steps=200):
     return st["ux"].cpu().numpy(), st["uy"].cpu().numpy()
 
 
-def bench_natconv(pkg, N=512, Ra=1e5, steps=2000, FT=None, graph_steps=500, nu_ref=None):
-    """Thermal DDF natural convection, N^2, Pr=0.71, fused step (FP32 by
-    default), `steps` steps replayed from a CUDA graph; returns MLUPS, the
-    hot-wall Nusselt number and the final fields."""
+NATCONV_STORAGES = {
+    # name: (torch dtype name, deviation, stochastic rounding, bytes per population)
+    "f64": ("float64", False, False, 8), "f32": ("float32", False, False, 4),
+    "f32dev": ("float32", True, False, 4), "f16dev_sr": ("float16", True, True, 2),
+    "bf16dev_sr": ("bfloat16", True, True, 2),
+}
+
+
+def bench_natconv(pkg, N=512, Ra=1e5, steps=2000, FT=None, graph_steps=500, nu_ref=None,
+                  storage=None):
+    """Thermal DDF natural convection, N^2, Pr=0.71, fused step, `steps` steps
+    replayed from a CUDA graph; returns MLUPS, the hot-wall Nusselt number
+    and the final fields.  storage: f64 / f32 (the reference's arithmetic,
+    f and g stored whole) or f32dev / f16dev_sr / bf16dev_sr (f - w_q and
+    g - w_q T_ref, FP32 step; stochastic rounding for the 16-bit ones)."""
+    import numpy as np
     import torch
-    FT = FT or torch.float32
+    if storage is None:
+        storage = "f64" if FT == torch.float64 else "f32"
+    tname, dev, sr, bpp = NATCONV_STORAGES[storage]
+    FT = getattr(torch, tname)
+    fd = torch.float64 if storage == "f64" else torch.float32
     p = pkg.drivers.natconv_parameters(N, Ra, 0.71)
-    cfg = pkg.LBMConfig.d2q9(N, N, p["nu"], 0.0, 0)
-    st = pkg.initialize_2d(cfg, FT)
-    gi = torch.from_numpy(pkg.drivers.natconv_initial_g(N)).to("cuda", FT)
-    go = gi.clone()
-    Temp = torch.zeros((N, N), dtype=FT, device="cuda")
-    fi, fo = st["f_in"], st["f_out"]
+    f0 = torch.from_numpy(np.stack([pkg.lattice.D2Q9_W[q] * np.ones((N, N)) for q in range(9)]))
+    g0 = torch.from_numpy(pkg.drivers.natconv_initial_g(N))
+
+    def load(fi, fo, gi, go):
+        if dev:
+            pkg.convert_populations(fi, f0.cuda(), dst_deviation=True)
+            gi.copy_(pkg.thermal_deviation(g0.cuda(), p["T_ref"]).to(FT))
+        else:
+            fi.copy_(f0.to(FT)); gi.copy_(g0.to(FT))
+        fo.copy_(fi); go.copy_(gi)
+
+    fi = torch.empty((9, N, N), dtype=FT, device="cuda")
+    fo, gi, go = torch.empty_like(fi), torch.empty_like(fi), torch.empty_like(fi)
+    load(fi, fo, gi, go)
+    Temp = torch.zeros((N, N), dtype=fd, device="cuda")
     assert graph_steps % 2 == 0 and steps % graph_steps == 0
+
+    def step(b, a, d, c):
+        pkg.fused_natconv_step_(b, a, d, c, Temp, N, N, p["omega_f"], p["omega_T"], p["beta_g"],
+                                p["T_ref"], 1.0, 0.0, deviation=dev, stochastic_rounding=sr)
+
     g = pkg.Graph()
     with g:
         a, b, c, d = fi, fo, gi, go
         for _ in range(graph_steps):
-            pkg.fused_natconv_step_(b, a, d, c, Temp, N, N, p["omega_f"], p["omega_T"],
-                                    p["beta_g"], p["T_ref"], 1.0, 0.0)
+            step(b, a, d, c)
             a, b = b, a
             c, d = d, c
     g.launch()                      # warm-up replay (then restart from the initial state)
     torch.cuda.synchronize()
-    st2 = pkg.initialize_2d(cfg, FT)
-    fi.copy_(st2["f_in"]); fo.copy_(st2["f_out"])
-    gi.copy_(torch.from_numpy(pkg.drivers.natconv_initial_g(N)).to("cuda", FT)); go.copy_(gi)
+    load(fi, fo, gi, go)
     e0, e1 = _events()
     e0.record()
     for _ in range(steps // graph_steps):
@@ -871,41 +928,54 @@ def bench_natconv(pkg, N=512, Ra=1e5, steps=2000, FT=None, graph_steps=500, nu_r
     ms = e0.elapsed_time(e1)
     g.close()
     T_prev = Temp.clone()
-    pkg.fused_natconv_step_(fo, fi, go, gi, Temp, N, N, p["omega_f"], p["omega_T"], p["beta_g"],
-                            p["T_ref"], 1.0, 0.0)
+    step(fo, fi, go, gi)
     dT = float((Temp - T_prev).abs().max())
-    pkg.compute_temperature_2d_(Temp, go)
-    pkg.compute_macroscopic_2d_(st["rho"], st["ux"], st["uy"], fo)
-    T = Temp.double().cpu().numpy()
-    out = {"workload": f"thermal DDF natural convection {N}^2 {str(FT).split('.')[-1]}, Ra={Ra:g}, "
+    # final fields of the populations in fi / gi (moments without the Guo
+    # half-force term, as compute_macroscopic_2d!)
+    fb = torch.empty((9, N, N), dtype=torch.float64, device="cuda")
+    if dev:
+        pkg.convert_populations(fb, fi, src_deviation=True)
+        gb = pkg.thermal_deviation(gi, p["T_ref"], to_deviation=False)
+    else:
+        fb.copy_(fi); gb = gi.double()
+    rho = fb.sum(0)
+    ux = (fb[1] - fb[3] + fb[5] - fb[6] - fb[7] + fb[8]) / rho
+    uy = (fb[2] - fb[4] + fb[5] + fb[6] - fb[7] - fb[8]) / rho
+    T = gb.sum(0).cpu().numpy()
+    out = {"workload": f"thermal DDF natural convection {N}^2 {storage}, Ra={Ra:g}, "
                        f"Pr=0.71, {steps} fused steps (CUDA graph of {graph_steps})",
            "mlups": round(N * N * steps / (ms * 1e-3) / 1e6, 1),
-           "gbs_alg": round(N * N * steps * (144 if FT == torch.float32 else 288) / (ms * 1e-3) / 1e9, 1),
+           "gbs_alg": round(N * N * steps * 36 * bpp / (ms * 1e-3) / 1e9, 1),
            "Nu": pkg.drivers.nusselt_hot_wall(T), "max_dT_last_step": dT}
     if nu_ref is not None:
         out["Nu_de_vahl_davis"] = nu_ref
-    return out, T, st["ux"].double().cpu().numpy(), st["uy"].double().cpu().numpy()
+    return out, T, ux.cpu().numpy(), uy.cpu().numpy()
 
 
-def bench_natconv_validation(pkg, N=512, steps_by_ra=None):
-    """Config 4: Nu, MLUPS and FP32-vs-FP64 errors of T and u for Ra in
-    {1e4, 1e5, 1e6} on N^2."""
+def bench_natconv_validation(pkg, N=512, steps_by_ra=None,
+                             storages=("f32", "f32dev", "f16dev_sr")):
+    """Config 4: Nu, MLUPS and the errors of T and u against the FP64 run for
+    Ra in {1e4, 1e5, 1e6} on N^2, per storage: FP32 with f and g whole (the
+    reference's arithmetic), FP32 deviations, FP16 deviations with
+    stochastic rounding."""
     import json as _json
     import numpy as np
-    import torch
     pins = _json.loads((ROOT / "tests" / "golden" / "reference_pins.json").read_text())
     dvd = pins["de_vahl_davis_nu"]
     steps_by_ra = steps_by_ra or {1e4: 1280000, 1e5: 2560000, 1e6: 2560000}
     res = {}
     for ra, steps in steps_by_ra.items():
-        r32, T32, ux32, uy32 = bench_natconv(pkg, N, ra, steps, torch.float32,
+        r64, T64, ux64, uy64 = bench_natconv(pkg, N, ra, steps, storage="f64",
                                              nu_ref=dvd.get(str(int(ra))))
-        r64, T64, ux64, uy64 = bench_natconv(pkg, N, ra, steps, torch.float64)
         un = np.sqrt(np.sum(ux64 ** 2 + uy64 ** 2))
-        res[f"Ra={ra:g}"] = {"fp32": r32, "fp64": {k: r64[k] for k in ("mlups", "Nu", "max_dT_last_step")},
-                             "T_max_err_fp32_vs_fp64": float(np.max(np.abs(T32 - T64))),
-                             "u_l2_rel_fp32_vs_fp64": float(np.sqrt(np.sum((ux32 - ux64) ** 2 +
-                                                                           (uy32 - uy64) ** 2)) / un)}
+        row = {"fp64": r64}
+        for st in storages:
+            r, T, ux, uy = bench_natconv(pkg, N, ra, steps, storage=st)
+            r["T_max_err_vs_fp64"] = float(np.max(np.abs(T - T64)))
+            r["u_l2_rel_vs_fp64"] = float(np.sqrt(np.sum((ux - ux64) ** 2 + (uy - uy64) ** 2)) / un)
+            r["Nu_rel_err_vs_fp64"] = float(abs(r["Nu"] - r64["Nu"]) / r64["Nu"])
+            row[st] = r
+        res[f"Ra={ra:g}"] = row
     return res
 
 

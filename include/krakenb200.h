@@ -5,8 +5,8 @@
  * stream-collide path; the comment above it cites the reference function
  * (file:line, paths inside the Kraken.jl repository) whose argument meaning
  * and error behaviour it keeps.  A Julia backend binds these with `ccall`
- * (see INTEGRATION.md); the Python host layer in krakenn.jl_b200/ binds them
- * with ctypes.
+ * (krakenn.jl_b200/julia/KrakenB200.jl); the Python host layer in
+ * krakenn.jl_b200/ binds them with ctypes.
  *
  * Conventions shared by every entry point
  *   - Arrays are raw DEVICE pointers owned by the caller, in Julia
@@ -225,7 +225,11 @@ int kb_cavity_mrt_step_2d(void *f_out, const void *f_in, void *rho, void *ux, vo
                           double s_eps, double s_q, double u_lid, int dtype, void *stream);
 
 /* fused_natconv_step!(f_out, f_in, g_out, g_in, Temp, Nx, Ny, omega_f,
- *   omega_T, beta_g, T_ref_buoy, T_hot, T_cold) -- src/kernels/fused_thermal_2d.jl:251 */
+ *   omega_T, beta_g, T_ref_buoy, T_hot, T_cold) -- src/kernels/fused_thermal_2d.jl:251
+ * KB_F64 / KB_F32 keep the reference arithmetic (f, g and Temp of that type).
+ * The deviation storages (KB_F32_DEV, KB_F16_DEV, KB_BF16_DEV and the
+ * stochastic-rounding 16-bit codes) hold f - w_q and g - w_q * T_ref_buoy in
+ * that type and step in FP32; Temp is then float.  Same for the _vt_ step. */
 int kb_fused_natconv_step(void *f_out, const void *f_in, void *g_out, const void *g_in,
                           void *Temp, int Nx, int Ny, double omega_f, double omega_T,
                           double beta_g, double T_ref_buoy, double T_hot, double T_cold,
@@ -560,6 +564,11 @@ int kb_convert_populations(void *dst, int dst_dtype, const void *src, int src_dt
  * one stream are bit-identical.  Synchronises `stream`.  No reference
  * counterpart. */
 int kb_set_stochastic_seed(unsigned int seed, void *stream);
+/* The current value of that counter on the current device, so that a
+ * checkpoint can record it and a resumed run can restore it with
+ * kb_set_stochastic_seed and draw the same random bits as an uninterrupted
+ * run.  Synchronises `stream`.  No reference counterpart. */
+int kb_get_stochastic_seed(unsigned int *seed, void *stream);
 
 /* *timed_out = 1 if a staged step (kernel 1, variant 5) gave up a bounded
  * wait on its copies since the last call (the flag is then cleared);
@@ -585,7 +594,9 @@ int kb_mass(const void *f, int lattice_q, size_t n_nodes, int dtype, double *out
  * process exits, so at most 1,073,479,680 populations (lattice_q * n_nodes)
  * fit; a larger call returns KB_ERR_ARG and names kb_mass.  The first call
  * on a device looks the array's address up (cudaGetSymbolAddress), so make
- * it before any stream capture.  All calls share the one array and each
+ * it before any stream capture; the address is kept for the life of the
+ * process, so do not use this entry point on a device after
+ * cudaDeviceReset.  All calls share the one array and each
  * call clears what must start at zero, but calls that overlap on the GPU
  * (other streams, other host threads) race.  Result, flag and
  * synchronisation as kb_mass. */

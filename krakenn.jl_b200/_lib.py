@@ -119,6 +119,7 @@ SIGNATURES: dict[str, list] = {
     "kb_selftest_bounded_wait": [C.c_longlong, C.POINTER(_i), _vp],
     "kb_convert_populations": [_vp, _i, _cvp, _i, _i, _sz, _vp],
     "kb_set_stochastic_seed": [C.c_uint, _vp],
+    "kb_get_stochastic_seed": [C.POINTER(C.c_uint), _vp],
     "kb_staged_step_status": [_vp, _vp],
     "kb_mass": [_cvp, _i, _sz, _i, _dp, _vp],
     "kb_mass_static": [_cvp, _i, _sz, _i, _dp, _vp],

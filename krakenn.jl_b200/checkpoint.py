@@ -25,7 +25,14 @@ file raises `CheckpointError` naming the object.
 (any storage; 16-bit deviation storages are held as float32 values, which
 round-trips them exactly), optional moments, the grid and storage as the
 identity and the relaxation parameters, so a run resumed from a checkpoint
-continues bit for bit.
+continues bit for bit.  A stochastic-rounding run also records, in
+`run_control`, the device counter that seeds its random rounding bits, and
+its identity says so; restoring it sets the counter back, so the resumed run
+draws the bits the uninterrupted run would have drawn.
+
+Durability: the archive is closed, then the temporary file and (after the
+renames) its directory are fsync'ed, so after a crash `path` is either the
+previous complete checkpoint or the new complete one.
 """
 from __future__ import annotations
 
@@ -207,8 +214,8 @@ def write_checkpoint(path, snap: StateSnapshot, keep_previous=True):
                     meta["crc32"][member] = zlib.crc32(data)
                     z.writestr(member, data)
             z.writestr("meta.json", json.dumps(meta, allow_nan=True))
-            z.fp.flush()
-            os.fsync(z.fp.fileno())
+        # the central directory is written on close: sync the whole file after it
+        _fsync_path(tmp)
     except Exception as err:
         if os.path.exists(tmp):
             os.remove(tmp)
@@ -216,7 +223,31 @@ def write_checkpoint(path, snap: StateSnapshot, keep_previous=True):
     if keep_previous and os.path.exists(path):
         os.replace(path, path + ".prev")
     os.replace(tmp, path)
+    _fsync_dir(os.path.dirname(os.path.abspath(path)))
     return path
+
+
+def _fsync_path(p):
+    fd = os.open(p, os.O_RDONLY)
+    try:
+        os.fsync(fd)
+    finally:
+        os.close(fd)
+
+
+def _fsync_dir(d):
+    """Make the renames durable (a directory fsync; skipped where the platform
+    cannot open a directory)."""
+    try:
+        fd = os.open(d, os.O_RDONLY)
+    except OSError:
+        return
+    try:
+        os.fsync(fd)
+    except OSError:
+        pass
+    finally:
+        os.close(fd)
 
 
 def _open(path):
@@ -288,41 +319,65 @@ def _host(t):
     return t.detach().cpu().numpy().copy()
 
 
-def lbm_identity(f, deviation=False):
+def lbm_identity(f, deviation=False, stochastic_rounding=False):
     """The identity of a plain LBM state: lattice, grid and storage of its
-    populations (Q, [Nz,] Ny, Nx)."""
+    populations (Q, [Nz,] Ny, Nx), and whether its stores round
+    stochastically."""
     q = int(f.shape[0])
     dims = [int(d) for d in f.shape[1:]][::-1]  # Nx, Ny[, Nz]
     ident = {"lattice": {9: "D2Q9", 19: "D3Q19"}.get(q, f"Q{q}"), "Nx": dims[0], "Ny": dims[1],
-             "storage": str(f.dtype).replace("torch.", ""), "deviation": bool(deviation)}
+             "storage": str(f.dtype).replace("torch.", ""), "deviation": bool(deviation),
+             "stochastic_rounding": bool(stochastic_rounding)}
     if len(dims) == 3:
         ident["Nz"] = dims[2]
     return ident
 
 
-def snapshot_lbm(f, cycle, moments=None, parameters=None, deviation=False, run_control=None):
+# checkpoints written before the stochastic-rounding key existed
+_LBM_IDENTITY_DEFAULTS = {"stochastic_rounding": False}
+
+
+def snapshot_lbm(f, cycle, moments=None, parameters=None, deviation=False, run_control=None,
+                 stochastic_rounding=False):
     """StateSnapshot of a plain LBM state: the populations `f` (any storage),
     optional moments {name: tensor}, the relaxation `parameters` (e.g. nu,
-    Lambda, omega, u_lid) and the global `cycle`."""
+    Lambda, omega, u_lid) and the global `cycle`.  With stochastic_rounding,
+    run_control["sr_epoch"] holds the device counter that seeds the rounding
+    bits (read from the library; synchronises the current stream)."""
     fields = {"f": _host(f)}
     for name, t in (moments or {}).items():
         fields[f"moments/{name}"] = _host(t)
+    rc = dict(run_control or {})
+    if stochastic_rounding:
+        from . import ops
+        rc["sr_epoch"] = ops.get_stochastic_seed()
     return StateSnapshot(LBM_SOLVER, LBM_SCHEMA, cycle, fields=fields,
-                         identity=lbm_identity(f, deviation),
-                         run_control=dict(run_control or {}),
+                         identity=lbm_identity(f, deviation, stochastic_rounding),
+                         run_control=rc,
                          parameters=dict(parameters or {}))
 
 
-def restore_lbm(snap: StateSnapshot, like, deviation=False):
+def restore_lbm(snap: StateSnapshot, like, deviation=False, stochastic_rounding=False):
     """Populations of `snap` as a tensor with the dtype, device and shape of
     `like`, after check_compatible against `like`'s identity; returns
-    (f, cycle, moments {name: tensor on like's device})."""
+    (f, cycle, moments {name: tensor on like's device}).  A stochastic-rounding
+    state also sets the library's rounding-bit counter back to the recorded
+    one, so the resumed run continues bit for bit."""
     import torch
     check_compatible(snap, solver=LBM_SOLVER, schema_version=LBM_SCHEMA,
-                     identity=lbm_identity(like, deviation))
+                     identity=lbm_identity(like, deviation, stochastic_rounding),
+                     identity_defaults=_LBM_IDENTITY_DEFAULTS)
+    if stochastic_rounding:
+        epoch = snap.run_control.get("sr_epoch")
+        if not isinstance(epoch, int) or isinstance(epoch, bool):
+            raise CheckpointError("run_control/sr_epoch: a stochastic-rounding checkpoint must "
+                                  f"record the rounding-bit counter, found {epoch!r}")
     f = torch.from_numpy(snap.fields["f"]).to(like.device).to(like.dtype)
     mom = {k.split("/", 1)[1]: torch.from_numpy(v).to(like.device)
            for k, v in snap.fields.items() if k.startswith("moments/")}
+    if stochastic_rounding:
+        from . import ops
+        ops.set_stochastic_seed(epoch)
     return f, snap.cycle, mom
 
 
@@ -332,9 +387,9 @@ def save_checkpoint_lbm(path, f, cycle, keep_previous=True, **kw):
     return write_checkpoint(path, snapshot_lbm(f, cycle, **kw), keep_previous=keep_previous)
 
 
-def load_checkpoint_lbm(path, like, deviation=False):
+def load_checkpoint_lbm(path, like, deviation=False, stochastic_rounding=False):
     """read_checkpoint then restore_lbm."""
-    return restore_lbm(read_checkpoint(path), like, deviation)
+    return restore_lbm(read_checkpoint(path), like, deviation, stochastic_rounding)
 
 
 __all__ = ["CheckpointError", "StateSnapshot", "validate_content", "check_finite",

@@ -79,6 +79,17 @@ __device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __
 __device__ __forceinline__ float2 vneg(float2 a) { return make_float2(-a.x, -a.y); }
 __device__ __forceinline__ float2 vsplat(float a, float2) { return make_float2(a, a); }
 __device__ __forceinline__ float2 vrcp(float2 a) { return make_float2(__frcp_rn(a.x), __frcp_rn(a.y)); }
+// 1/a from the hardware approximation (PTX rcp.approx.ftz.f32, within about
+// one unit in the last place).  The deviation-storage collisions divide by
+// rho = 1 + drho, which is never near zero or subnormal; the IEEE-rounded
+// reciprocal (vrcp) would add a refinement and a range check per node to a
+// kernel that is instruction bound at 16-bit storage.
+__device__ __forceinline__ float vrcp_fast(float a) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+}
+__device__ __forceinline__ float2 vrcp_fast(float2 a) { return make_float2(vrcp_fast(a.x), vrcp_fast(a.y)); }
 
 // ------------------------------------------------------ stochastic rounding --
 // 32-bit integer hash (lowbias32, C. Wellons) for the random bits of the

@@ -11,6 +11,17 @@
 #include "kb_common.cuh"
 
 namespace kb {
+namespace d3 {
+// The deviation-storage form of the fused thermal DDF step lives in the
+// precision-tier unit (kb_d3q19_dev.cu, compiled with FMA contraction).
+int launch_natconv_dev(int dtype, bool vt, void *f_out, const void *f_in, void *g_out,
+                       const void *g_in, float *Temp, int Nx, int Ny, double w_f, double w_T,
+                       double beta_g, double T_ref, double T_hot, double T_cold, double nu_ref,
+                       double T0_visc, double a_visc, cudaStream_t s);
+}  // namespace d3
+}  // namespace kb
+
+namespace kb {
 namespace d2 {
 
 constexpr int BX = 128;
@@ -1315,6 +1326,10 @@ int kb_fused_natconv_step(void *f_out, const void *f_in, void *g_out, const void
     KB_REQUIRE(f_out && f_in && g_out && g_in && Temp, "kb_fused_natconv_step: null pointer");
     KB_REQUIRE(f_out != f_in && g_out != g_in, "kb_fused_natconv_step: in and out must differ");
     if (int e = check_dims("kb_fused_natconv_step", Nx, Ny)) return e;
+    if (dtype != KB_F64 && dtype != KB_F32)
+        return kb::d3::launch_natconv_dev(dtype, false, f_out, f_in, g_out, g_in, (float *)Temp, Nx,
+                                          Ny, omega_f, omega_T, beta_g, T_ref_buoy, T_hot, T_cold,
+                                          0.0, 0.0, 0.0, kb::as_stream(stream));
     KB_DISPATCH_PLAIN("kb_fused_natconv_step", dtype,
         (natconv_k<T, false><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
             (T *)f_out, (const T *)f_in, (T *)g_out, (const T *)g_in, (T *)Temp, grid2<T>(Nx, Ny),
@@ -1329,6 +1344,10 @@ int kb_fused_natconv_vt_step(void *f_out, const void *f_in, void *g_out, const v
     KB_REQUIRE(f_out && f_in && g_out && g_in && Temp, "kb_fused_natconv_vt_step: null pointer");
     KB_REQUIRE(f_out != f_in && g_out != g_in, "kb_fused_natconv_vt_step: in and out must differ");
     if (int e = check_dims("kb_fused_natconv_vt_step", Nx, Ny)) return e;
+    if (dtype != KB_F64 && dtype != KB_F32)
+        return kb::d3::launch_natconv_dev(dtype, true, f_out, f_in, g_out, g_in, (float *)Temp, Nx,
+                                          Ny, 0.0, omega_T, beta_g, T_ref_buoy, T_hot, T_cold,
+                                          nu_ref, T0_visc, alpha_visc, kb::as_stream(stream));
     KB_DISPATCH_PLAIN("kb_fused_natconv_vt_step", dtype,
         (natconv_k<T, true><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
             (T *)f_out, (const T *)f_in, (T *)g_out, (const T *)g_in, (T *)Temp, grid2<T>(Nx, Ny),

@@ -249,6 +249,14 @@ int launch_trt3d_dev_links(int dtype, void *f_out, const void *f_in, float *rho,
 
 // Launchers of the fused TRT step for the deviation storages
 // (kb_d3q19_dev.cu); `per` = periodic bit mask.
+// Fused thermal DDF natural-convection step on deviation storage (f - w_q,
+// g - w_q T_ref; KB_F32_DEV / KB_F16_DEV / KB_BF16_DEV and the stochastic-
+// rounding 16-bit storages); Temp is float.  vt: temperature-dependent
+// viscosity.
+int launch_natconv_dev(int dtype, bool vt, void *f_out, const void *f_in, void *g_out,
+                       const void *g_in, float *Temp, int Nx, int Ny, double w_f, double w_T,
+                       double beta_g, double T_ref, double T_hot, double T_cold, double nu_ref,
+                       double T0_visc, double a_visc, cudaStream_t s);
 int launch_trt3d_dev(int dtype, void *f_out, const void *f_in, float *rho, float *ux, float *uy,
                      float *uz, const uint8_t *solid, const Grid3 &g, float sp, float sm,
                      cudaStream_t s, int variant);

@@ -44,8 +44,25 @@ struct DevLoad {
 // a run is reproducible on one stream); population q's word is derived from
 // the key with one add (sr_bits).
 __device__ unsigned int g_sr_epoch = 0;
+// Consumer warps of the current staged launch that have finished; the last
+// one advances g_sr_epoch (sr_epoch_done), so that kernel needs no
+// sr_advance_k launch after it.
+__device__ unsigned int g_sr_done = 0;
 
 __global__ void sr_advance_k() { g_sr_epoch += 1u; }
+
+// Called once by lane 0 of each of `warps` warps of a persistent launch, after
+// every lane of the warp has read g_sr_epoch: the last warp to arrive
+// advances the epoch and resets the count.  All reads of the epoch by this
+// launch happen before its advance, as with a separate sr_advance_k.
+__device__ __forceinline__ void sr_epoch_done(unsigned int warps) {
+    __threadfence();
+    if (atomicAdd(&g_sr_done, 1u) == warps - 1u) {
+        g_sr_done = 0u;
+        g_sr_epoch += 1u;
+        __threadfence();
+    }
+}
 
 // Per-thread key for this launch.
 __device__ __forceinline__ uint32_t sr_key() {
@@ -98,7 +115,7 @@ __device__ __forceinline__ void trt_dev_collide(const V *d, V *o, V &rho, V &ux,
     const V jy = vadd(vadd(vadd(tv[1], tv[3]), tv[4]), vsub(tv[7], tv[8]));
     const V jz = vadd(vadd(vadd(tv[2], tv[5]), tv[6]), vadd(tv[7], tv[8]));
     rho = vadd(vsplat(1.f, z), drho);
-    const V inv = vrcp(rho);
+    const V inv = vrcp_fast(rho);
     ux = vmul(jx, inv);
     uy = vmul(jy, inv);
     uz = vmul(jz, inv);
@@ -650,7 +667,9 @@ __global__ void __launch_bounds__(128, KB_QUAD_MIN_BLOCKS) trt_dev_v4_k(R *__res
 // source outside the tile (x0 - 1 for c_x = +1, the element after the
 // tile's last node for c_x = -1): the neighbouring segment, the periodic
 // wrap, or at an x wall the node's own opposite population (half-way
-// bounce-back).  Four consumer warps wait on "full", read, release the stage
+// bounce-back).  A tile that spans a whole periodic row needs no halo run:
+// its x wrap is read from the other end of the staged rows.  Four consumer
+// warps wait on "full", read, release the stage
 // on its "empty" mbarrier and collide; the loads of the next tiles run
 // meanwhile and no register holds a load in flight.  Consumer thread t owns
 // the adjacent nodes x0 + 2t, x0 + 2t + 1 and reads population q at the
@@ -666,7 +685,8 @@ constexpr int TTHREADS = TCONS + 32;    // + the producer warp
 constexpr int TCLS = 19 * TT + 10 * THALO;     // element offset of the class-byte run (cut-link steps)
 constexpr int TSTAGE = TCLS + TT / 2;           // elements per stage (row q at q * TT)
 constexpr size_t TSMEM = 128 + (size_t)TSTAGES * TSTAGE * 2;  // + alignment slack
-constexpr uint32_t TBYTES = 19u * TT * 2u + 10u * 8u * 2u;   // transaction bytes of a staged tile
+constexpr uint32_t TROWBYTES = 19u * TT * 2u;                 // the 19 row runs of a tile
+constexpr uint32_t TBYTES = TROWBYTES + 10u * 8u * 2u;           // + the 10 halo runs
 constexpr long long TWAIT = 4000000;    // bounded mbarrier wait (polls)
 
 #ifndef KB_TMA_MIN_BLOCKS
@@ -753,8 +773,8 @@ __device__ __forceinline__ void tma_load3(uint32_t dst, const CUtensorMap *tm, i
         : "memory");
 }
 __device__ __forceinline__ void tma_issue_tile(const TileMaps &mp, uint32_t dst, uint32_t bar,
-                                               int x0, int j, int k, const TileMap &m) {
-    const uint32_t bytes = TBYTES + (mp.tc ? (uint32_t)TT : 0u);
+                                               int x0, int j, int k, const TileMap &m, bool halos) {
+    const uint32_t bytes = (halos ? TBYTES : TROWBYTES) + (mp.tc ? (uint32_t)TT : 0u);
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                  : "memory");
     // tensor-map z coordinates: the map spans the whole allocation, this
@@ -779,6 +799,7 @@ __device__ __forceinline__ void tma_issue_tile(const TileMaps &mp, uint32_t dst,
     tma_load4(dst + 16 * R, mp.t1, x0, yp, zm, 16, bar); // q 16: (-1, +1)
     tma_load4(dst + 17 * R, mp.t1, x0, ym, zp, 17, bar); // q 17: (+1, -1)
     tma_load4(dst + 18 * R, mp.t1, x0, yp, zp, 18, bar); // q 18: (-1, -1)
+    if (!halos) return;  // a periodic row in one tile: the wrap sources are in the rows
     // halos: slot e (left, c_x = +1) and 5 + e (right, c_x = -1).  At an x
     // wall the slot holds the end node's own opposite population from its
     // own row (node 0 at slot position 0, node Nx - 1 at position 7).
@@ -884,6 +905,9 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
                 asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tcls)) : "memory");
         }
 #pragma unroll 1
+        // one tile spans a periodic row: its x wrap reads the staged rows, so
+        // no halo runs are copied
+        const bool halos = !((g.per & 1) && m.ntx == 1);
         for (int n = 0; ck < g.Nz; m.advance(cx, cj, ck), ++n) {
             const int s = n % TSTAGES;
             // the consumers have released this stage's previous tile
@@ -894,7 +918,7 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
             if (t == TCONS) {
                 const uint32_t bar = s_addr(&full[s]);
                 if (m.staged(cj, ck))
-                    tma_issue_tile(mp, s_addr(stage0 + s * TSTAGE), bar, cx * TT, cj, ck, m);
+                    tma_issue_tile(mp, s_addr(stage0 + s * TSTAGE), bar, cx * TT, cj, ck, m, halos);
                 else  // nothing to copy: the phase completes on the arrival
                     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], 0;" ::"r"(bar)
                                  : "memory");
@@ -915,6 +939,7 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
         SR ? hash32(((uint32_t)blockIdx.x * TTHREADS + (uint32_t)t) ^
                     hash32(*(volatile const unsigned int *)&g_sr_epoch + 0x632BE5ABu))
            : 0u;
+    const bool wrapx = (g.per & 1) && m.ntx == 1;  // as the producer's !halos
     int it = 0;
     bool aborted = false;
 #pragma unroll 1
@@ -945,17 +970,30 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
                 else d[q] = make_float2(ld(r[1]), ld(r[2]));
             }
             // the tile ends take the halo slots (the thread holding the
-            // tile's last node: local index min(TT, Nx - x0) - 1, odd)
+            // tile's last node: local index min(TT, Nx - x0) - 1, odd), or,
+            // when the tile is a whole periodic row, the other end of the
+            // staged row itself (x = Nx - 1 feeds node 0, x = 0 feeds Nx - 1)
             const R *h = stage0 + s * TSTAGE + 19 * TT;
+            const R *rows = stage0 + s * TSTAGE;
             if (t == 0) {
-                const int pl = (x0 == 0 && !(g.per & 1)) ? 0 : 7;
+                if (wrapx) {
 #pragma unroll
-                for (int e = 0; e < 5; ++e) d[kQP[e]].x = ld(h[e * THALO + pl]);
+                    for (int e = 0; e < 5; ++e) d[kQP[e]].x = ld(rows[kQP[e] * TT + g.Nx - 1]);
+                } else {
+                    const int pl = (x0 == 0 && !(g.per & 1)) ? 0 : 7;
+#pragma unroll
+                    for (int e = 0; e < 5; ++e) d[kQP[e]].x = ld(h[e * THALO + pl]);
+                }
             }
             if (t == (min(TT, g.Nx - x0) - 2) >> 1) {
-                const int pr = (x0 + TT >= g.Nx && !(g.per & 1)) ? 7 : 0;
+                if (wrapx) {
 #pragma unroll
-                for (int e = 0; e < 5; ++e) d[kQM[e]].y = ld(h[(5 + e) * THALO + pr]);
+                    for (int e = 0; e < 5; ++e) d[kQM[e]].y = ld(rows[kQM[e] * TT]);
+                } else {
+                    const int pr = (x0 + TT >= g.Nx && !(g.per & 1)) ? 7 : 0;
+#pragma unroll
+                    for (int e = 0; e < 5; ++e) d[kQM[e]].y = ld(h[(5 + e) * THALO + pr]);
+                }
             }
         } else if (live) {
             // rows at a y or z wall: direct pull of both nodes
@@ -1048,6 +1086,12 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
             tbar_wait(s_addr(&full[i2 % TSTAGES]), (uint32_t)(i2 / TSTAGES) & 1u);
         }
     }
+    // stochastic rounding: this launch's last consumer warp advances the
+    // epoch (the cut-link step keeps sr_advance_k, after its side kernel)
+    if (SR && !LINKS) {
+        __syncwarp();
+        if ((t & 31) == 0) sr_epoch_done(gridDim.x * (TCONS / 32));
+    }
 }
 
 static PFN_cuTensorMapEncodeTiled_v12000 tma_encode_fn() {
@@ -1087,8 +1131,14 @@ template <typename R, bool MOM, bool SOLID, typename I, bool SR, bool LINKS = fa
 static int launch_tma_k(const TmaMaps &mp, R *fo, const R *fi, float *rho, float *ux, float *uy,
                         float *uz, const uint8_t *solid, const Grid3 &g, float sp, float sm,
                         cudaStream_t s, const LinkTable3 &L = LinkTable3{}) {
-    static int occ = -1;  // resident blocks per SM of this instantiation
-    if (occ < 0) {
+    // resident blocks per SM of this instantiation, per device (the shared
+    // memory opt-in below is a per-device attribute too)
+    static int occ_dev[64] = {};
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return set_error(KB_ERR_CUDA, "kb_fused_trt_step_3d: no usable current device");
+    int &occ = occ_dev[dev];
+    if (occ <= 0) {
         int n = 0;
         // the stage ring may exceed the 48 KB default of dynamic shared memory
         if (cudaFuncSetAttribute(trt_dev_tma_k<R, MOM, SOLID, I, SR, LINKS>,
@@ -1103,8 +1153,6 @@ static int launch_tma_k(const TmaMaps &mp, R *fo, const R *fi, float *rho, float
         }
         occ = n;
     }
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long tiles = (long long)((g.Nx + TT - 1) / TT) * g.Ny * g.Nz;
     const int blocks = (int)std::min<long long>(tiles, (long long)sms * occ);
@@ -1228,7 +1276,7 @@ static int launch_r(void *f_out, const void *f_in, float *rho, float *ux, float 
             const int rc = offsets_fit_int(g, 19)
                                ? launch_tma<R, int, SR>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s)
                                : launch_tma<R, long long, SR>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s);
-            if (rc == KB_OK && SR) sr_advance_k<<<1, 1, 0, s>>>();
+            // (the staged kernel advances the stochastic-rounding epoch itself)
             return rc;
         }
     }
@@ -1388,6 +1436,156 @@ int launch_trt3d_dev_links(int dtype, void *f_out, const void *f_in, float *rho,
     return check_launch("kb_fused_trt_libb_links_step_3d");
 }
 
+// ---------------------------------------------------------------------------
+// Thermal DDF natural convection on deviation storage: the fused step of
+// src/kernels/fused_thermal_2d.jl:37-151, 178-238 (pull with half-way
+// bounce-back of f and g, anti-bounce-back hot west / cold east walls for g,
+// temperature, Boussinesq force fy = beta_g (T - T_ref), thermal BGK of g,
+// Guo-forced BGK of f) with f stored as d = f - w_q and g as
+// e = g - w_q T_ref, and every step computed in FP32 on those deviations:
+//   T = T_ref + sum e,   fy = beta_g sum e,   rho = 1 + sum d,
+//   u = (sum c d + (0, fy / 2)) / rho
+//   e* = e - wT (e - w (dT + 3 T c.u))                 [g_eq - w T_ref]
+//   d* = d - w_f (d - w (drho + rho (3 c.u + 4.5 (c.u)^2 - 1.5 u^2)))
+//        + (1 - w_f / 2) S_q                            [f_eq - w]
+//   anti-bounce-back: e_q = -e_qb + 2 w_q (T_wall - T_ref)
+// so neither the O(w) background of f nor the w T_ref background of g is
+// rounded.  D2Q9 order: 0 rest, 1 +x, 2 +y, 3 -x, 4 -y, 5 +x+y, 6 -x+y,
+// 7 -x-y, 8 +x-y.  VT: the temperature-dependent viscosity of
+// fused_natconv_vt_step! (nu = nu_ref exp(a (T - T0)), :155-161).
+template <typename R, bool VT, bool SR>
+__global__ void __launch_bounds__(BX) natconv_dev_k(R *__restrict__ fo, const R *__restrict__ fi,
+                                                     R *__restrict__ go, const R *__restrict__ gi,
+                                                     float *__restrict__ Temp, int Nx, int Ny,
+                                                     float w_f, float w_T, float beta_g,
+                                                     float T_ref, float T_hot, float T_cold,
+                                                     float nu_ref, float T0_visc, float a_visc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= Nx) return;
+    const size_t P = (size_t)Nx * Ny;
+    const size_t c = (size_t)i + (size_t)Nx * j;
+    const bool w = i > 0, e = i < Nx - 1, s = j > 0, n = j < Ny - 1;
+    // pull with half-way bounce-back; source offsets per population (the
+    // opposite population of the node itself at a wall)
+    const size_t src[9] = {c,
+                           w ? c - 1 + 1 * P : c + 3 * P,
+                           s ? c - Nx + 2 * P : c + 4 * P,
+                           e ? c + 1 + 3 * P : c + 1 * P,
+                           n ? c + Nx + 4 * P : c + 2 * P,
+                           (w && s) ? c - 1 - Nx + 5 * P : c + 7 * P,
+                           (e && s) ? c + 1 - Nx + 6 * P : c + 8 * P,
+                           (e && n) ? c + 1 + Nx + 7 * P : c + 5 * P,
+                           (w && n) ? c - 1 + Nx + 8 * P : c + 6 * P};
+    float d[9], t[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        d[q] = Dev<R>::ld(fi[src[q]]);
+        t[q] = Dev<R>::ld(gi[src[q]]);
+    }
+    const float wa = 1.0f / 9.0f, wd = 1.0f / 36.0f;
+    if (i == 0) {  // hot wall (thermal_bc, fused_thermal_2d.jl:37-52)
+        const float h = 2.0f * (T_hot - T_ref);
+        t[1] = -t[1] + wa * h;
+        t[5] = -t[5] + wd * h;
+        t[8] = -t[8] + wd * h;
+    }
+    if (i == Nx - 1) {  // cold wall
+        const float h = 2.0f * (T_cold - T_ref);
+        t[3] = -t[3] + wa * h;
+        t[6] = -t[6] + wd * h;
+        t[7] = -t[7] + wd * h;
+    }
+    const float dT = ((t[0] + t[1]) + (t[2] + t[3])) + ((t[4] + t[5]) + ((t[6] + t[7]) + t[8]));
+    const float Tl = T_ref + dT;
+    Temp[c] = Tl;
+    const float fy = beta_g * dT;
+    const float drho = ((d[0] + d[1]) + (d[2] + d[3])) + ((d[4] + d[5]) + ((d[6] + d[7]) + d[8]));
+    const float rho = 1.0f + drho;
+    const float inv = vrcp_fast(rho);
+    const float ux = (((d[1] - d[3]) + (d[5] - d[6])) + (d[8] - d[7])) * inv;
+    const float uy = ((((d[2] - d[4]) + (d[5] + d[6])) - (d[7] + d[8])) + 0.5f * fy) * inv;
+    // velocity projections c_q . u
+    const float cu[9] = {0.f, ux, uy, -ux, -uy, ux + uy, uy - ux, -ux - uy, ux - uy};
+    const float wq[9] = {4.0f / 9.0f, wa, wa, wa, wa, wd, wd, wd, wd};
+    // thermal BGK on e
+    float eo[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const float eeq = wq[q] * fmaf(3.0f * Tl, cu[q], dT);
+        eo[q] = t[q] - w_T * (t[q] - eeq);
+    }
+    float wf = w_f;
+    if (VT) wf = 1.0f / (3.0f * (nu_ref * expf(a_visc * (Tl - T0_visc))) + 0.5f);
+    // Guo-forced BGK on d (collide_guo with fx = 0): the source
+    // S_q = w_q (3 (c_q - u) . F + 9 (c_q . u)(c_q . F)), F = (0, fy)
+    const float usq15 = 1.5f * fmaf(ux, ux, uy * uy);
+    const float cy[9] = {0.f, 0.f, 1.f, 0.f, -1.f, 1.f, 1.f, -1.f, -1.f};
+    const float gsrc = 1.0f - 0.5f * wf;
+    float dout[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const float deq = wq[q] * fmaf(rho, fmaf(cu[q], fmaf(4.5f, cu[q], 3.0f), -usq15), drho);
+        const float S = wq[q] * fy * fmaf(9.0f * cu[q], cy[q], 3.0f * (cy[q] - uy));
+        dout[q] = d[q] - wf * (d[q] - deq) + gsrc * S;
+    }
+    if (SR) {
+        const uint32_t key =
+            hash32((uint32_t)c ^ hash32(*(volatile const unsigned int *)&g_sr_epoch + 0x632BE5ABu));
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            const uint32_t v = SRPack<R>::pack(dout[q], eo[q], sr_bits(key, q));
+            reinterpret_cast<unsigned short *>(fo)[c + q * P] = (unsigned short)(v & 0xFFFFu);
+            reinterpret_cast<unsigned short *>(go)[c + q * P] = (unsigned short)(v >> 16);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            fo[c + q * P] = Dev<R>::st(dout[q]);
+            go[c + q * P] = Dev<R>::st(eo[q]);
+        }
+    }
+}
+
+template <typename R, bool SR>
+static void launch_natconv_dev_r(bool vt, void *f_out, const void *f_in, void *g_out,
+                                 const void *g_in, float *Temp, int Nx, int Ny, float w_f,
+                                 float w_T, float beta_g, float T_ref, float T_hot, float T_cold,
+                                 float nu_ref, float T0_visc, float a_visc, cudaStream_t s) {
+    const dim3 grid((Nx + BX - 1) / BX, Ny);
+    R *fo = (R *)f_out, *go = (R *)g_out;
+    const R *fi = (const R *)f_in, *gi = (const R *)g_in;
+    if (vt)
+        natconv_dev_k<R, true, SR><<<grid, BX, 0, s>>>(fo, fi, go, gi, Temp, Nx, Ny, w_f, w_T, beta_g,
+                                                      T_ref, T_hot, T_cold, nu_ref, T0_visc, a_visc);
+    else
+        natconv_dev_k<R, false, SR><<<grid, BX, 0, s>>>(fo, fi, go, gi, Temp, Nx, Ny, w_f, w_T, beta_g,
+                                                       T_ref, T_hot, T_cold, nu_ref, T0_visc, a_visc);
+    if (SR) sr_advance_k<<<1, 1, 0, s>>>();
+}
+
+int launch_natconv_dev(int dtype, bool vt, void *f_out, const void *f_in, void *g_out,
+                       const void *g_in, float *Temp, int Nx, int Ny, double w_f, double w_T,
+                       double beta_g, double T_ref, double T_hot, double T_cold, double nu_ref,
+                       double T0_visc, double a_visc, cudaStream_t s) {
+    const float a[10] = {(float)w_f, (float)w_T, (float)beta_g, (float)T_ref, (float)T_hot,
+                         (float)T_cold, (float)nu_ref, (float)T0_visc, (float)a_visc, 0.f};
+#define KB_NATCONV_DEV(R, SR)                                                                   \
+    launch_natconv_dev_r<R, SR>(vt, f_out, f_in, g_out, g_in, Temp, Nx, Ny, a[0], a[1], a[2], a[3], \
+                                a[4], a[5], a[6], a[7], a[8], s)
+    switch (dtype) {
+        case KB_F32_DEV: KB_NATCONV_DEV(float, false); break;
+        case KB_F16_DEV: KB_NATCONV_DEV(__half, false); break;
+        case KB_BF16_DEV: KB_NATCONV_DEV(__nv_bfloat16, false); break;
+        case KB_F16_DEV_SR: KB_NATCONV_DEV(__half, true); break;
+        case KB_BF16_DEV_SR: KB_NATCONV_DEV(__nv_bfloat16, true); break;
+        default:
+            return set_error(KB_ERR_UNSUPPORTED, "kb_fused_natconv_step: unknown dtype %d", dtype);
+    }
+#undef KB_NATCONV_DEV
+    return check_launch("kb_fused_natconv_step");
+}
+
 }  // namespace d3
 
 // ------------------------------------------------------ storage conversion --
@@ -1436,12 +1634,26 @@ __global__ void convert_k(void *dst, int ddt, const void *src, int sdt, int Q, s
 }  // namespace kb
 
 extern "C" int kb_set_stochastic_seed(unsigned int seed, void *stream) {
+    const unsigned int zero = 0u;
     if (cudaMemcpyToSymbolAsync(kb::d3::g_sr_epoch, &seed, sizeof(seed), 0, cudaMemcpyHostToDevice,
+                                kb::as_stream(stream)) != cudaSuccess ||
+        cudaMemcpyToSymbolAsync(kb::d3::g_sr_done, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice,
                                 kb::as_stream(stream)) != cudaSuccess)
         return kb::check_launch("kb_set_stochastic_seed");
     // the host value must outlive the asynchronous copy
     if (cudaStreamSynchronize(kb::as_stream(stream)) != cudaSuccess)
         return kb::check_launch("kb_set_stochastic_seed");
+    return 0;
+}
+
+extern "C" int kb_get_stochastic_seed(unsigned int *seed, void *stream) {
+    KB_REQUIRE(seed, "kb_get_stochastic_seed: null argument");
+    unsigned int v = 0u;
+    if (cudaMemcpyFromSymbolAsync(&v, kb::d3::g_sr_epoch, sizeof(v), 0, cudaMemcpyDeviceToHost,
+                                  kb::as_stream(stream)) != cudaSuccess ||
+        cudaStreamSynchronize(kb::as_stream(stream)) != cudaSuccess)
+        return kb::check_launch("kb_get_stochastic_seed");
+    *seed = v;
     return 0;
 }
 

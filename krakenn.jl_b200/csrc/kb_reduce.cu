@@ -205,7 +205,10 @@ constexpr size_t kStaticItemsPerBlock = 256 * (size_t)red::RT;
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
 // Device address of g_static_scratch on the current device, looked up once
-// per device (host code may not use the symbol's name as an address).
+// per device (host code may not use the symbol's name as an address).  The
+// cached address belongs to the device's current context: after a
+// cudaDeviceReset it is stale, and the process must not call
+// kb_mass_static on that device again.
 int static_scratch(char **out) {
     static char *addr[64] = {nullptr};
     int dev = 0;
@@ -236,6 +239,8 @@ int kb_mass(const void *f, int lattice_q, size_t n_nodes, int dtype, double *out
     KB_REQUIRE(lattice_q == 9 || lattice_q == 19, "kb_mass: lattice_q must be 9 or 19");
     KB_REQUIRE(n_nodes > 0, "kb_mass: n_nodes must be positive");
     KB_REQUIRE(dtype_bytes(dtype), "kb_mass: unknown dtype %d", dtype);
+    KB_REQUIRE(n_nodes <= SIZE_MAX / (size_t)lattice_q,
+               "kb_mass: lattice_q * n_nodes overflows size_t (n_nodes = %zu)", n_nodes);
     const int nb = reduction_blocks((size_t)lattice_q * n_nodes);
     int err;
     char *ws = (char *)reduce_workspace(kHead + sizeof(red::KSum) * nb, &err);
@@ -306,6 +311,9 @@ int kb_mass_static(const void *f, int lattice_q, size_t n_nodes, int dtype, doub
     KB_REQUIRE(lattice_q == 9 || lattice_q == 19, "kb_mass_static: lattice_q must be 9 or 19");
     KB_REQUIRE(n_nodes > 0, "kb_mass_static: n_nodes must be positive");
     KB_REQUIRE(dtype_bytes(dtype), "kb_mass_static: unknown dtype %d", dtype);
+    // (a product that wrapped around would pass the limit check below)
+    KB_REQUIRE(n_nodes <= SIZE_MAX / (size_t)lattice_q,
+               "kb_mass_static: lattice_q * n_nodes overflows size_t (n_nodes = %zu)", n_nodes);
     const size_t items = (size_t)lattice_q * n_nodes;
     const size_t nb = (items + kStaticItemsPerBlock - 1) / kStaticItemsPerBlock;
     if (nb > kStaticMaxPartials)

@@ -249,10 +249,12 @@ def taylor_green_3d_populations(N, u0, rho0=1.0, Nz=None):
 
 
 def run_taylor_green_3d(N=64, nu=0.01, u0=0.05, Lambda=0.25, max_steps=100, backend="b200",
-                        storage=torch.float64, deviation=None, moments_every=0):
+                        storage=torch.float64, deviation=None, moments_every=0,
+                        stochastic_rounding=False):
     """Periodic D3Q19 TRT Taylor-Green vortex (no reference driver: the
     reference has no fully periodic D3Q19 pull).  Returns host fields after
-    max_steps."""
+    max_steps.  stochastic_rounding: 16-bit deviation storages round their
+    stores stochastically."""
     _require_backend(backend)
     if deviation is None:
         deviation = storage in (torch.float16, torch.bfloat16)
@@ -272,7 +274,8 @@ def run_taylor_green_3d(N=64, nu=0.01, u0=0.05, Lambda=0.25, max_steps=100, back
         want = last or (moments_every and (s + 1) % moments_every == 0)
         m = (rho, ux, uy, uz) if want else (None, None, None, None)
         ops.fused_trt_step_3d_(f_out, f_in, *m, None, N, N, N, nu, Lambda,
-                               periodic=(True, True, True), deviation=deviation)
+                               periodic=(True, True, True), deviation=deviation,
+                               stochastic_rounding=stochastic_rounding)
         f_in, f_out = f_out, f_in
     return dict(rho=rho.cpu().numpy(), ux=ux.cpu().numpy(), uy=uy.cpu().numpy(),
                 uz=uz.cpu().numpy(), f=f_in, k=2 * math.pi / N)

@@ -19,6 +19,13 @@ import ctypes as C
 import torch
 
 from . import _lib
+
+
+def _arg_error(msg: str) -> _lib.KrakenArgumentError:
+    """A refused argument, raised before any call into the library: the same
+    exception (a ValueError) and status code (KB_ERR_ARG) as an argument the
+    library itself refuses."""
+    return _lib.KrakenArgumentError("argument check", _lib.KB_ERR_ARG, msg)
 from ._lib import (KB_BF16_DEV, KB_BF16_DEV_SR, KB_F16_DEV, KB_F16_DEV_SR, KB_F32, KB_F32_DEV,
                    KB_F64, call)
 
@@ -30,7 +37,7 @@ def storage_dtype(t: torch.Tensor, deviation: bool = False) -> int:
     """kb_dtype code of a population tensor."""
     if t.dtype == torch.float64:
         if deviation:
-            raise ValueError("float64 storage holds f, not a deviation")
+            raise _arg_error("float64 storage holds f, not a deviation")
         return KB_F64
     if t.dtype == torch.float32:
         return KB_F32_DEV if deviation else KB_F32
@@ -38,7 +45,7 @@ def storage_dtype(t: torch.Tensor, deviation: bool = False) -> int:
         return KB_F16_DEV
     if t.dtype == torch.bfloat16:
         return KB_BF16_DEV
-    raise ValueError(f"unsupported population dtype {t.dtype}")
+    raise _arg_error(f"unsupported population dtype {t.dtype}")
 
 
 def torch_dtype(code: int) -> torch.dtype:
@@ -54,11 +61,11 @@ def _t(t: torch.Tensor | None, name: str):
     if t is None:
         return None
     if not isinstance(t, torch.Tensor):
-        raise TypeError(f"{name} must be a torch tensor")
+        raise _arg_error(f"{name} must be a torch tensor")
     if not t.is_cuda:
-        raise ValueError(f"{name} must live on a CUDA device (the B200 path has no CPU fallback)")
+        raise _arg_error(f"{name} must live on a CUDA device (the B200 path has no CPU fallback)")
     if not t.is_contiguous():
-        raise ValueError(f"{name} must be contiguous")
+        raise _arg_error(f"{name} must be contiguous")
     return C.c_void_p(t.data_ptr())
 
 
@@ -66,7 +73,7 @@ def _mask(m: torch.Tensor | None):
     if m is None:
         return None
     if m.dtype not in (torch.bool, torch.uint8):
-        raise ValueError("is_solid must be a bool or uint8 tensor")
+        raise _arg_error("is_solid must be a bool or uint8 tensor")
     return _t(m, "is_solid")
 
 
@@ -77,7 +84,7 @@ def _stream():
 def _plain(f: torch.Tensor) -> int:
     code = storage_dtype(f)
     if code not in (KB_F64, KB_F32):
-        raise ValueError("this reference kernel takes float64 or float32 populations")
+        raise _arg_error("this reference kernel takes float64 or float32 populations")
     return code
 
 
@@ -85,43 +92,43 @@ def _same(code: int, *fields):
     want = field_dtype(code)
     for name, t in fields:
         if t is not None and t.dtype != want:
-            raise ValueError(f"{name} must be {want} for this population storage")
+            raise _arg_error(f"{name} must be {want} for this population storage")
 
 
 def _dims2(f: torch.Tensor):
     if f.dim() != 3 or f.shape[0] != 9:
-        raise ValueError("D2Q9 populations must have shape (9, Ny, Nx)")
+        raise _arg_error("D2Q9 populations must have shape (9, Ny, Nx)")
     return int(f.shape[2]), int(f.shape[1])
 
 
 def _dims3(f: torch.Tensor):
     if f.dim() != 4 or f.shape[0] != 19:
-        raise ValueError("D3Q19 populations must have shape (19, Nz, Ny, Nx)")
+        raise _arg_error("D3Q19 populations must have shape (19, Nz, Ny, Nx)")
     return int(f.shape[3]), int(f.shape[2]), int(f.shape[1])
 
 
 def _match2(f, Nx, Ny):
     if _dims2(f) != (Nx, Ny):
-        raise ValueError(f"population shape {tuple(f.shape)} does not match Nx={Nx}, Ny={Ny}")
+        raise _arg_error(f"population shape {tuple(f.shape)} does not match Nx={Nx}, Ny={Ny}")
 
 
 def _match3(f, Nx, Ny, Nz):
     if _dims3(f) != (Nx, Ny, Nz):
-        raise ValueError(f"population shape {tuple(f.shape)} does not match "
+        raise _arg_error(f"population shape {tuple(f.shape)} does not match "
                          f"Nx={Nx}, Ny={Ny}, Nz={Nz}")
 
 
 def _ptrs_2d_fields(code, Nx, Ny, **fields):
     for name, t in fields.items():
         if t is not None and tuple(t.shape) != (Ny, Nx):
-            raise ValueError(f"{name} must have shape (Ny, Nx) = ({Ny}, {Nx})")
+            raise _arg_error(f"{name} must have shape (Ny, Nx) = ({Ny}, {Nx})")
     _same(code, *fields.items())
 
 
 def _ptrs_3d_fields(code, Nx, Ny, Nz, **fields):
     for name, t in fields.items():
         if t is not None and tuple(t.shape) != (Nz, Ny, Nx):
-            raise ValueError(f"{name} must have shape (Nz, Ny, Nx) = ({Nz}, {Ny}, {Nx})")
+            raise _arg_error(f"{name} must have shape (Nz, Ny, Nx) = ({Nz}, {Ny}, {Nx})")
     _same(code, *fields.items())
 
 
@@ -152,7 +159,7 @@ def apply_zou_he_south_2d_(f, u_wall_x, Nx):
     code = _plain(f)
     nx, ny = _dims2(f)
     if nx != Nx:
-        raise ValueError("Nx does not match the population shape")
+        raise _arg_error("Nx does not match the population shape")
     call("kb_apply_zou_he_south_2d", _t(f, "f"), float(u_wall_x), Nx, ny, code, _stream())
 
 
@@ -187,7 +194,7 @@ def apply_bounce_back_wall_2d_(f, Nx, Ny, side):
     """apply_bounce_back_wall_2d! -- src/kernels/boundary_2d.jl:117"""
     code = _plain(f); _match2(f, Nx, Ny)
     if side not in _SIDES:
-        raise ValueError(f"apply_bounce_back_wall_2d!: unknown side {side}")
+        raise _arg_error(f"apply_bounce_back_wall_2d!: unknown side {side}")
     call("kb_apply_bounce_back_wall_2d", _t(f, "f"), Nx, Ny, _SIDES[side], code, _stream())
 
 
@@ -255,7 +262,7 @@ def collide_guo_field_2d_(f, is_solid, Fx_field, Fy_field, omega):
     Nx, Ny = _dims2(f)
     for name, t in (("Fx_field", Fx_field), ("Fy_field", Fy_field)):
         if t is None or t.dtype != f.dtype or tuple(t.shape) != (Ny, Nx):
-            raise ValueError(f"{name} must be a {f.dtype} tensor of shape (Ny, Nx)")
+            raise _arg_error(f"{name} must be a {f.dtype} tensor of shape (Ny, Nx)")
     call("kb_collide_guo_field_2d", _t(f, "f"), _mask(is_solid), _t(Fx_field, "Fx_field"),
          _t(Fy_field, "Fy_field"), Nx, Ny, float(omega), code, _stream())
 
@@ -268,7 +275,7 @@ def fused_trt_libb_v2_step_(f_out, f_in, rho, ux, uy, is_solid, q_wall, uw_link_
     _match2(f_in, Nx, Ny); _match2(f_out, Nx, Ny)
     for name, t in (("q_wall", q_wall), ("uw_link_x", uw_link_x), ("uw_link_y", uw_link_y)):
         if t is None or t.dtype != f_in.dtype or tuple(t.shape) != tuple(f_in.shape):
-            raise ValueError(f"{name} must be a {f_in.dtype} tensor shaped like f")
+            raise _arg_error(f"{name} must be a {f_in.dtype} tensor shaped like f")
     _ptrs_2d_fields(code, Nx, Ny, rho=rho, ux=ux, uy=uy)
     call("kb_fused_trt_libb_step", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
          _t(ux, "ux"), _t(uy, "uy"), _mask(is_solid), _t(q_wall, "q_wall"),
@@ -302,7 +309,7 @@ def persistent_aa_bgk_(f, is_solid, Nx, Ny, omega, Nt):
     queued without synchronisation on one pull-format buffer f (slot q holds
     the post-collision f_q), returned in the same format.  Nt must be even."""
     if Nt % 2:
-        raise ValueError("persistent_aa_bgk_: Nt must be even (pairs of A-A steps)")
+        raise _arg_error("persistent_aa_bgk_: Nt must be even (pairs of A-A steps)")
     idx = torch.tensor(AA_SWAP_2D, device=f.device)
     f.copy_(f.index_select(0, idx))
     for _ in range(Nt // 2):
@@ -377,10 +384,38 @@ def cavity_mrt_step_2d_(f_out, f_in, rho, ux, uy, is_solid, Nx, Ny, nu, u_lid, s
          float(s_eps), float(s_q), float(u_lid), code, _stream())
 
 
+def _natconv_code(f_in, g_in, deviation, stochastic_rounding):
+    """kb_dtype of a natural-convection step: the reference's FP64 / FP32, or
+    (deviation) f - w_q and g - w_q T_ref in float32 / float16 / bfloat16."""
+    if g_in.dtype != f_in.dtype:
+        raise _arg_error("f and g populations must have the same dtype")
+    if not deviation:
+        if stochastic_rounding:
+            raise _arg_error("stochastic rounding applies to float16/bfloat16 deviation storage")
+        return _plain(f_in)
+    code = storage_dtype(f_in, True)
+    if stochastic_rounding:
+        if code not in (KB_F16_DEV, KB_BF16_DEV):
+            raise _arg_error("stochastic rounding applies to float16/bfloat16 deviation storage")
+        code = KB_F16_DEV_SR if code == KB_F16_DEV else KB_BF16_DEV_SR
+    return code
+
+
+def thermal_deviation(g, T_ref, to_deviation=True):
+    """g - w_q T_ref (to_deviation) or its inverse, for the thermal DDF
+    populations of a D2Q9 natural-convection step on deviation storage; g of
+    shape (9, Ny, Nx).  Returns a float64 tensor on g's device."""
+    w = torch.tensor([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4, dtype=torch.float64, device=g.device)
+    shift = (w * float(T_ref))[:, None, None]
+    return g.double() - shift if to_deviation else g.double() + shift
+
+
 def fused_natconv_step_(f_out, f_in, g_out, g_in, Temp, Nx, Ny, omega_f, omega_T, beta_g,
-                        T_ref_buoy, T_hot, T_cold):
-    """fused_natconv_step! -- src/kernels/fused_thermal_2d.jl:251"""
-    code = _plain(f_in)
+                        T_ref_buoy, T_hot, T_cold, deviation=False, stochastic_rounding=False):
+    """fused_natconv_step! -- src/kernels/fused_thermal_2d.jl:251.  With
+    deviation, f holds f - w_q and g holds g - w_q T_ref_buoy (float32,
+    float16 or bfloat16) and the step runs in FP32; Temp is float32."""
+    code = _natconv_code(f_in, g_in, deviation, stochastic_rounding)
     for t in (f_in, f_out, g_in, g_out):
         _match2(t, Nx, Ny)
     _ptrs_2d_fields(code, Nx, Ny, Temp=Temp)
@@ -390,9 +425,11 @@ def fused_natconv_step_(f_out, f_in, g_out, g_in, Temp, Nx, Ny, omega_f, omega_T
 
 
 def fused_natconv_vt_step_(f_out, f_in, g_out, g_in, Temp, Nx, Ny, nu_ref, T0_visc, alpha_visc,
-                           omega_T, beta_g, T_ref_buoy, T_hot, T_cold):
-    """fused_natconv_vt_step! -- src/kernels/fused_thermal_2d.jl:268"""
-    code = _plain(f_in)
+                           omega_T, beta_g, T_ref_buoy, T_hot, T_cold, deviation=False,
+                           stochastic_rounding=False):
+    """fused_natconv_vt_step! -- src/kernels/fused_thermal_2d.jl:268 (storages
+    as fused_natconv_step_)"""
+    code = _natconv_code(f_in, g_in, deviation, stochastic_rounding)
     for t in (f_in, f_out, g_in, g_out):
         _match2(t, Nx, Ny)
     _ptrs_2d_fields(code, Nx, Ny, Temp=Temp)
@@ -660,7 +697,7 @@ def slab_fill_ghosts_3d_(f, lo, hi, deviation=False):
     """Ghost planes of a one-rank z-slab on a periodic z axis from the slab's
     own end planes (kb_slab_fill_ghosts_3d); f is (19, nz_alloc, Ny, Nx)."""
     if f.dim() != 4 or f.shape[0] != 19 or not f.is_contiguous():
-        raise ValueError("f must be a contiguous (19, nz_alloc, Ny, Nx) tensor")
+        raise _arg_error("f must be a contiguous (19, nz_alloc, Ny, Nx) tensor")
     call("kb_slab_fill_ghosts_3d", _t(f, "f"), f.shape[3], f.shape[2], f.shape[1], int(bool(lo)),
          int(bool(hi)), storage_dtype(f, deviation), _stream())
 
@@ -679,7 +716,7 @@ def collide_guo_field_3d_(f, is_solid, Fx_field, Fy_field, Fz_field, omega):
     Nx, Ny, Nz = _dims3(f)
     for name, t in (("Fx_field", Fx_field), ("Fy_field", Fy_field), ("Fz_field", Fz_field)):
         if t is None or t.dtype != f.dtype or tuple(t.shape) != (Nz, Ny, Nx):
-            raise ValueError(f"{name} must be a {f.dtype} tensor of shape (Nz, Ny, Nx)")
+            raise _arg_error(f"{name} must be a {f.dtype} tensor of shape (Nz, Ny, Nx)")
     call("kb_collide_guo_field_3d", _t(f, "f"), _mask(is_solid), _t(Fx_field, "Fx_field"),
          _t(Fy_field, "Fy_field"), _t(Fz_field, "Fz_field"), Nx, Ny, Nz, float(omega), code,
          _stream())
@@ -725,10 +762,10 @@ def fused_trt_step_3d_(f_out, f_in, rho, ux, uy, uz, is_solid, Nx, Ny, Nz, nu, L
     unbiased stochastic rounding (KB_F16_DEV_SR / KB_BF16_DEV_SR)."""
     code = storage_dtype(f_in, deviation)
     if storage_dtype(f_out, deviation) != code:
-        raise ValueError("f_in and f_out must have the same storage")
+        raise _arg_error("f_in and f_out must have the same storage")
     if stochastic_rounding:
         if code not in (KB_F16_DEV, KB_BF16_DEV):
-            raise ValueError("stochastic rounding applies to float16/bfloat16 deviation storage")
+            raise _arg_error("stochastic rounding applies to float16/bfloat16 deviation storage")
         code = KB_F16_DEV_SR if code == KB_F16_DEV else KB_BF16_DEV_SR
     _match3(f_in, Nx, Ny, Nz); _match3(f_out, Nx, Ny, Nz)
     _ptrs_3d_fields(code, Nx, Ny, Nz, rho=rho, ux=ux, uy=uy, uz=uz)
@@ -747,15 +784,15 @@ def fused_trt_step_3d_zrange_(f_out, f_in, rho, ux, uy, uz, is_solid, Nx, Ny, Nz
     src/kernels/li_bb_3d_v2.jl:31)."""
     code = storage_dtype(f_in, deviation)
     if storage_dtype(f_out, deviation) != code:
-        raise ValueError("f_in and f_out must have the same storage")
+        raise _arg_error("f_in and f_out must have the same storage")
     if stochastic_rounding:
         if code not in (KB_F16_DEV, KB_BF16_DEV):
-            raise ValueError("stochastic rounding applies to float16/bfloat16 deviation storage")
+            raise _arg_error("stochastic rounding applies to float16/bfloat16 deviation storage")
         code = KB_F16_DEV_SR if code == KB_F16_DEV else KB_BF16_DEV_SR
     _match3(f_in, Nx, Ny, Nz_alloc); _match3(f_out, Nx, Ny, Nz_alloc)
     _ptrs_3d_fields(code, Nx, Ny, Nz_alloc, rho=rho, ux=ux, uy=uy, uz=uz)
     if is_solid is not None and tuple(is_solid.shape) != (Nz_alloc, Ny, Nx):
-        raise ValueError(f"is_solid must have shape (Nz_alloc, Ny, Nx) = ({Nz_alloc}, {Ny}, {Nx})")
+        raise _arg_error(f"is_solid must have shape (Nz_alloc, Ny, Nx) = ({Nz_alloc}, {Ny}, {Nx})")
     px, py = periodic_xy
     call("kb_fused_trt_step_3d_zrange", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
          _t(ux, "ux"), _t(uy, "uy"), _t(uz, "uz"), _mask(is_solid), Nx, Ny, Nz_alloc,
@@ -772,7 +809,7 @@ def fused_trt_libb_v2_step_3d_(f_out, f_in, rho, ux, uy, uz, is_solid, q_wall, u
     for name, t in (("q_wall", q_wall), ("uw_link_x", uw_link_x), ("uw_link_y", uw_link_y),
                     ("uw_link_z", uw_link_z)):
         if t is None or t.dtype != f_in.dtype or tuple(t.shape) != tuple(f_in.shape):
-            raise ValueError(f"{name} must be a {f_in.dtype} tensor shaped like f")
+            raise _arg_error(f"{name} must be a {f_in.dtype} tensor shaped like f")
     _ptrs_3d_fields(code, Nx, Ny, Nz, rho=rho, ux=ux, uy=uy, uz=uz)
     call("kb_fused_trt_libb_step_3d", _t(f_out, "f_out"), _t(f_in, "f_in"), _t(rho, "rho"),
          _t(ux, "ux"), _t(uy, "uy"), _t(uz, "uz"), _mask(is_solid), _t(q_wall, "q_wall"),
@@ -789,7 +826,7 @@ def fused_trt_libb_links_step_3d_(f_out, f_in, rho, ux, uy, uz, links, nu, Lambd
     code = storage_dtype(f_in, deviation)
     if stochastic_rounding:
         if code not in (KB_F16_DEV, KB_BF16_DEV):
-            raise ValueError("stochastic rounding applies to float16/bfloat16 deviation storage")
+            raise _arg_error("stochastic rounding applies to float16/bfloat16 deviation storage")
         code = KB_F16_DEV_SR if code == KB_F16_DEV else KB_BF16_DEV_SR
     Nx, Ny, Nz = links.Nx, links.Ny, links.Nz
     _match3(f_in, Nx, Ny, Nz); _match3(f_out, Nx, Ny, Nz)
@@ -811,7 +848,7 @@ def stream_periodic_xz_movingwall_y_3d_(f_out, f_in, Ub, Ut, Nx, Ny, Nz, rho_w=1
 def convert_populations(dst, src, dst_deviation=False, src_deviation=False):
     """Convert populations between storages (f <-> f - w_q, any precision)."""
     if dst.shape != src.shape:
-        raise ValueError("src and dst shapes differ")
+        raise _arg_error("src and dst shapes differ")
     Q = int(src.shape[0])
     n = src.numel() // Q
     call("kb_convert_populations", _t(dst, "dst"), storage_dtype(dst, dst_deviation),
@@ -821,6 +858,13 @@ def convert_populations(dst, src, dst_deviation=False, src_deviation=False):
 def set_stochastic_seed(seed: int):
     """Seed the random bits of the stochastic-rounding storages (synchronises)."""
     call("kb_set_stochastic_seed", C.c_uint(seed & 0xFFFFFFFF), _stream())
+
+
+def get_stochastic_seed() -> int:
+    """The launch counter that seeds the stochastic-rounding bits (synchronises)."""
+    out = C.c_uint(0)
+    call("kb_get_stochastic_seed", C.byref(out), _stream())
+    return int(out.value)
 
 
 def staged_step_timed_out() -> bool:
@@ -857,7 +901,7 @@ def synchronize():
 
 __all__ = [n for n in dir() if n.endswith("_") and not n.startswith("_")] + [
     "trt_rates", "convert_populations", "mass", "residual", "synchronize", "storage_dtype",
-    "set_trt3d_variant", "set_stochastic_seed", "staged_step_timed_out", "set_umma_engine", "AA_SWAP_2D",
+    "set_trt3d_variant", "set_stochastic_seed", "get_stochastic_seed", "thermal_deviation", "staged_step_timed_out", "set_umma_engine", "AA_SWAP_2D",
     "torch_dtype", "field_dtype", "periodic_mask", "FACES_3D"]
 
 _ = _lib  # keep the module import explicit for readers

@@ -780,6 +780,101 @@ void or_fused_trt_3d(double *f_out, const double *f_in, double *rho_o, double *u
             }
 }
 
+/* The same fused D3Q19 TRT step in single precision: the reference's
+ * T = Float32 path, where every constant is T(literal) and every operation
+ * rounds to Float32 (feq_3d: src/kernels/equilibrium_helpers_3d.jl:26-101,
+ * moments_3d: :102-112, CollideTRTDirect_3D: src/kernels/dsl/bricks_3d.jl:
+ * 179-229).  Same operation order as or_fused_trt_3d.  Used as the timed CPU
+ * baseline of the FP32 storages; parity is held by the FP64 restatement. */
+static inline float feq_poly_f32(float w, float rho, float cu, float usq) {
+    return w * rho * (1.0f + 3.0f * cu + 4.5f * cu * cu - 1.5f * usq);
+}
+
+void or_fused_trt_3d_f32(float *f_out, const float *f_in, float *rho_o, float *ux_o,
+                         float *uy_o, float *uz_o, const uint8_t *solid, int Nx, int Ny, int Nz,
+                         float sp, float sm, int per_x, int per_y, int per_z) {
+    const float wr = (float)(1.0 / 3.0), wa = (float)(1.0 / 18.0), we = (float)(1.0 / 36.0);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                float p[19];
+                size_t n = N3(i, j, k);
+                int im = i > 0 ? i - 1 : (per_x ? Nx - 1 : 0);
+                int ip = i < Nx - 1 ? i + 1 : (per_x ? 0 : Nx - 1);
+                int jm = j > 0 ? j - 1 : (per_y ? Ny - 1 : 0);
+                int jp = j < Ny - 1 ? j + 1 : (per_y ? 0 : Ny - 1);
+                int km = k > 0 ? k - 1 : (per_z ? Nz - 1 : 0);
+                int kp = k < Nz - 1 ? k + 1 : (per_z ? 0 : Nz - 1);
+                int xm = per_x || i > 0, xp = per_x || i < Nx - 1;
+                int ym = per_y || j > 0, yp = per_y || j < Ny - 1;
+                int zm = per_z || k > 0, zp = per_z || k < Nz - 1;
+                p[0] = f_in[I3(i, j, k, 0)];
+                p[1] = xm ? f_in[I3(im, j, k, 1)] : f_in[I3(i, j, k, 2)];
+                p[2] = xp ? f_in[I3(ip, j, k, 2)] : f_in[I3(i, j, k, 1)];
+                p[3] = ym ? f_in[I3(i, jm, k, 3)] : f_in[I3(i, j, k, 4)];
+                p[4] = yp ? f_in[I3(i, jp, k, 4)] : f_in[I3(i, j, k, 3)];
+                p[5] = zm ? f_in[I3(i, j, km, 5)] : f_in[I3(i, j, k, 6)];
+                p[6] = zp ? f_in[I3(i, j, kp, 6)] : f_in[I3(i, j, k, 5)];
+                p[7] = (xm && ym) ? f_in[I3(im, jm, k, 7)] : f_in[I3(i, j, k, 10)];
+                p[8] = (xp && ym) ? f_in[I3(ip, jm, k, 8)] : f_in[I3(i, j, k, 9)];
+                p[9] = (xm && yp) ? f_in[I3(im, jp, k, 9)] : f_in[I3(i, j, k, 8)];
+                p[10] = (xp && yp) ? f_in[I3(ip, jp, k, 10)] : f_in[I3(i, j, k, 7)];
+                p[11] = (xm && zm) ? f_in[I3(im, j, km, 11)] : f_in[I3(i, j, k, 14)];
+                p[12] = (xp && zm) ? f_in[I3(ip, j, km, 12)] : f_in[I3(i, j, k, 13)];
+                p[13] = (xm && zp) ? f_in[I3(im, j, kp, 13)] : f_in[I3(i, j, k, 12)];
+                p[14] = (xp && zp) ? f_in[I3(ip, j, kp, 14)] : f_in[I3(i, j, k, 11)];
+                p[15] = (ym && zm) ? f_in[I3(i, jm, km, 15)] : f_in[I3(i, j, k, 18)];
+                p[16] = (yp && zm) ? f_in[I3(i, jp, km, 16)] : f_in[I3(i, j, k, 17)];
+                p[17] = (ym && zp) ? f_in[I3(i, jm, kp, 17)] : f_in[I3(i, j, k, 16)];
+                p[18] = (yp && zp) ? f_in[I3(i, jp, kp, 18)] : f_in[I3(i, j, k, 15)];
+                if (solid && solid[n]) {
+                    for (int q = 0; q < 19; ++q)
+                        f_out[I3(i, j, k, q)] = q == 0 ? wr * 1.0f * (1.0f - 1.5f * 0.0f)
+                                                       : feq_poly_f32(q < 7 ? wa : we, 1.0f, 0.0f, 0.0f);
+                    if (rho_o) { rho_o[n] = 1.0f; ux_o[n] = 0.0f; uy_o[n] = 0.0f; uz_o[n] = 0.0f; }
+                    continue;
+                }
+                float r = p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7] + p[8] + p[9] +
+                          p[10] + p[11] + p[12] + p[13] + p[14] + p[15] + p[16] + p[17] + p[18];
+                float inv = 1.0f / r;
+                float ux = (p[1] - p[2] + p[7] - p[8] + p[9] - p[10] + p[11] - p[12] + p[13] - p[14]) * inv;
+                float uy = (p[3] - p[4] + p[7] + p[8] - p[9] - p[10] + p[15] - p[16] + p[17] - p[18]) * inv;
+                float uz = (p[5] - p[6] + p[11] + p[12] - p[13] - p[14] + p[15] + p[16] - p[17] - p[18]) * inv;
+                float usq = ux * ux + uy * uy + uz * uz;
+                float feq[19];
+                feq[0] = wr * r * (1.0f - 1.5f * usq);
+                feq[1] = feq_poly_f32(wa, r, ux, usq);
+                feq[2] = feq_poly_f32(wa, r, -ux, usq);
+                feq[3] = feq_poly_f32(wa, r, uy, usq);
+                feq[4] = feq_poly_f32(wa, r, -uy, usq);
+                feq[5] = feq_poly_f32(wa, r, uz, usq);
+                feq[6] = feq_poly_f32(wa, r, -uz, usq);
+                feq[7] = feq_poly_f32(we, r, ux + uy, usq);
+                feq[8] = feq_poly_f32(we, r, -ux + uy, usq);
+                feq[9] = feq_poly_f32(we, r, ux - uy, usq);
+                feq[10] = feq_poly_f32(we, r, -ux - uy, usq);
+                feq[11] = feq_poly_f32(we, r, ux + uz, usq);
+                feq[12] = feq_poly_f32(we, r, -ux + uz, usq);
+                feq[13] = feq_poly_f32(we, r, ux - uz, usq);
+                feq[14] = feq_poly_f32(we, r, -ux - uz, usq);
+                feq[15] = feq_poly_f32(we, r, uy + uz, usq);
+                feq[16] = feq_poly_f32(we, r, -uy + uz, usq);
+                feq[17] = feq_poly_f32(we, r, uy - uz, usq);
+                feq[18] = feq_poly_f32(we, r, -uy - uz, usq);
+                float a = (sp + sm) * 0.5f, b = (sp - sm) * 0.5f;
+                static const int pa[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16};
+                static const int pb[9] = {2, 4, 6, 10, 9, 14, 13, 18, 17};
+                f_out[I3(i, j, k, 0)] = p[0] - sp * (p[0] - feq[0]);
+                for (int m = 0; m < 9; ++m) {
+                    int x = pa[m], y = pb[m];
+                    f_out[I3(i, j, k, x)] = p[x] - a * (p[x] - feq[x]) - b * (p[y] - feq[y]);
+                    f_out[I3(i, j, k, y)] = p[y] - a * (p[y] - feq[y]) - b * (p[x] - feq[x]);
+                }
+                if (rho_o) { rho_o[n] = r; ux_o[n] = ux; uy_o[n] = uy; uz_o[n] = uz; }
+            }
+}
+
 /* stream_periodic_xz_movingwall_y_3d!: src/kernels/stream_periodic_3d.jl:106-186 */
 void or_stream_periodic_xz_movingwall_y_3d(double *f_out, const double *f_in, double Ub, double Ut,
                                            double rho_w, int Nx, int Ny, int Nz) {

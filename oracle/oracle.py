@@ -18,6 +18,7 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "_build" / "libkboracle.so"
 
 _D = C.POINTER(C.c_double)
+_F = C.POINTER(C.c_float)
 _U8 = C.c_void_p
 _i, _d = C.c_int, C.c_double
 
@@ -50,6 +51,8 @@ _SIG = {
     "or_zou_he_top_3d": ([_D, _d, _i, _i, _i], None),
     "or_run_cavity_3d": ([_D, _D, _D, _D, _D, _D, _U8, _i, _i, _i, _d, _d, _i], None),
     "or_fused_trt_3d": ([_D, _D, _D, _D, _D, _D, _U8, _i, _i, _i, _d, _d, _i, _i, _i], None),
+    "or_fused_trt_3d_f32": ([_F, _F, _F, _F, _F, _F, _U8, _i, _i, _i, C.c_float, C.c_float, _i,
+                             _i, _i], None),
     "or_stream_periodic_xz_movingwall_y_3d": ([_D, _D, _d, _d, _d, _i, _i, _i], None),
     "or_fused_natconv_2d": ([_D, _D, _D, _D, _D, _i, _i, _d, _d, _d, _d, _d, _d], None),
     "or_fused_natconv_vt_2d": ([_D, _D, _D, _D, _D, _i, _i, _d, _d, _d, _d, _d, _d, _d, _d], None),
@@ -334,6 +337,26 @@ def fused_trt_3d(f_out, f_in, moments, solid, sp, sm, periodic=(0, 0, 0)):
     m = moments if moments is not None else (None,) * 4
     lib().or_fused_trt_3d(_p(f_out), _p(f_in), *map(_p, m), _m(solid), Nx, Ny, Nz, sp, sm,
                           int(bool(periodic[0])), int(bool(periodic[1])), int(bool(periodic[2])))
+
+
+def _pf(a):
+    if a is None:
+        return None
+    if a.dtype != np.float32 or not a.flags.c_contiguous:
+        raise ValueError("single-precision oracle arrays must be C-contiguous float32")
+    return a.ctypes.data_as(_F)
+
+
+def fused_trt_3d_f32(f_out, f_in, moments, solid, sp, sm, periodic=(0, 0, 0)):
+    """fused_trt_3d in single precision (the reference's T = Float32 path):
+    float32 arrays, rates rounded to float32.  The timed CPU baseline of the
+    FP32 storages."""
+    Nx, Ny, Nz = _n3(f_in)
+    m = moments if moments is not None else (None,) * 4
+    lib().or_fused_trt_3d_f32(_pf(f_out), _pf(f_in), *map(_pf, m), _m(solid), Nx, Ny, Nz,
+                              float(np.float32(sp)), float(np.float32(sm)),
+                              int(bool(periodic[0])), int(bool(periodic[1])),
+                              int(bool(periodic[2])))
 
 
 def stream_periodic_xz_movingwall_y_3d(f_out, f_in, Ub, Ut, rho_w=1.0):
