@@ -442,7 +442,7 @@ def run_gpu(args):
                      "unfused_paths": bench_unfused_paths(pkg),
                      "thermal_guo_paths": bench_thermal_guo_paths(pkg),
                      "batch_config3_short": bench_batch(pkg, max_steps=2000, check_every=100,
-                                                        autotune=False)}
+                                                        autotune=True)}
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
@@ -778,28 +778,38 @@ def bench_cavity2d(pkg, steps=20000, graph_steps=200):
 
 
 def bench_batch(pkg, n_cases=256, max_steps=50000, check_every=100, tol=1e-6, storage="f16",
-                autotune=True, rank=0, world=1, error_cases=0):
+                autotune=True, rank=0, world=1, error_cases=0, graph=True):
     """Batched sweep: n_cases D2Q9 MRT cavities, N uniform on {64,...,512}, Re
     log-uniform [100, 2000], u_lid=0.1, one persistent launch per rank (the
-    cases are split across ranks with no data exchange).  With error_cases
-    > 0, that many cases (spread over the size range) are rerun on the FP64
-    reference-arithmetic MRT cavity step for the same number of steps and
-    their velocity error is reported."""
+    cases are split across ranks with no data exchange), replayed from a
+    captured CUDA graph (graph=True).  autotune: the schedule is tuned first,
+    and the tuned and the untuned (fixed) schedules' throughputs are
+    reported.  With error_cases > 0, that many cases (spread over the size
+    range) are rerun on the FP64 reference-arithmetic MRT cavity step for the
+    same number of steps and their velocity error is reported; every case that
+    went non-finite is rerun there too, to tell whether the physics or the
+    storage diverges."""
     import numpy as np
     import torch
     N, nu, u, Re = pkg.sweep_cases(n_cases, seed=0)
     mine = pkg.sharding.shard_cases(N, world, rank)
     b = pkg.CavityBatch(N[mine], nu[mine], u[mine], storage)
     tune = b.autotune(trial_steps=200) if autotune else None
+    g = b.capture(max_steps=max_steps, check_every=check_every, tol=tol) if graph else None
     b.reset()
     if world > 1:
         barrier(world)
     e0, e1 = _events()
     e0.record()
-    b.run(max_steps=max_steps, check_every=check_every, tol=tol)
+    if g is not None:
+        g.launch()
+    else:
+        b.run(max_steps=max_steps, check_every=check_every, tol=tol)
     e1.record()
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1), world)
+    if g is not None:
+        g.close()
     st = b.status()
     updates = st["updates"]
     if world > 1:
@@ -816,10 +826,30 @@ def bench_batch(pkg, n_cases=256, max_steps=50000, check_every=100, tol=1e-6, st
                        f"[100,2000], u_lid=0.1, {storage} deviation storage, residual {tol} or "
                        f"{max_steps} steps, one persistent cooperative launch per GPU",
            "mlups": round(updates / (ms * 1e-3) / 1e6, 1), "ms": round(ms, 1),
+           "hbm_frac_36B": round(updates * 36 / (ms * 1e-3) / 1e9 / hbm_peak()[0], 4)
+           if storage in ("f16", "bf16", "f16sr", "bf16sr") else None,
+           "launch": "one cooperative kernel replayed from a captured CUDA graph" if graph
+           else "one cooperative kernel",
            "node_updates": updates, "cases_on_rank0": states, "timed_out": st["timed_out"],
            "steps_min_median_max": [int(min(steps)), int(np.median(steps)), int(max(steps))]}
     if tune:
+        tune["tuned_over_fixed"] = round(tune["best_mlups"] / tune["fixed_mlups"], 3)
+        tune["fixed_schedule"] = "256-node tiles, blocks per SM at the occupancy limit (untuned default)"
         out["autotune"] = tune
+    if rank == 0:
+        nonfinite = []
+        for c in range(len(mine)):
+            r = b.case(c, fields=False)
+            if r["state"] != "non-finite":
+                continue
+            n = int(r["N"])
+            ux64, uy64 = _fp64_mrt_cavity(pkg, n, float(nu[mine][c]), float(u[mine][c]),
+                                          max(200, (r["steps"] + 199) // 200 * 200))
+            nonfinite.append({"N": n, "Re": round(float(Re[mine][c]), 1),
+                              "steps_in_batch": r["steps"],
+                              "fp64_single_case_finite": bool(np.isfinite(ux64).all() and
+                                                             np.isfinite(uy64).all())})
+        out["non_finite_cases_on_fp64_path"] = nonfinite
     if error_cases and rank == 0:
         errs = []
         pick = np.unique(np.linspace(0, len(mine) - 1, error_cases).round().astype(int))
@@ -980,10 +1010,13 @@ def bench_natconv_validation(pkg, N=512, steps_by_ra=None,
 
 
 def bench_warmstart(pkg, N=256, n_train=2000, n_test=64, epochs=40, batch=16, base=32,
-                    data_steps=200000, data_tol=1e-6, tol=1e-8, max_steps=2000000,
+                    data_steps=400000, data_tol=1e-8, tol=1e-8, max_steps=2000000,
                     check_every=1000, init_iters=500, grad_weight=200.0, seed=0):
-    """Learned warm start: train the encoder-decoder on n_train steady N^2
-    cavities from the batched kernel (Re log-uniform [100, 3200], u_lid 0.1),
+    """Learned warm start: train the encoder-decoder on the steady N^2 cavities
+    among n_train run by the batched kernel (Re log-uniform [100, 3200], u_lid
+    0.1) to r_u <= data_tol within data_steps: only the cases that reached it
+    are training targets (an unconverged field is a transient, not a steady
+    solution),
     then run n_test held-out cases to r_u <= tol with the plain FP64 MRT step
     from rest (cold), from the network's prediction (warm) and, as the bound
     of the method, from the cold run's own converged field (ideal).  Warm and
@@ -1013,8 +1046,9 @@ def bench_warmstart(pkg, N=256, n_train=2000, n_test=64, epochs=40, batch=16, ba
                    "mlups": round(float(steps.sum()) * N * N / (ms * 1e-3) / 1e6, 1),
                    "steps_min_median_max": [int(steps.min()), int(np.median(steps)), int(steps.max())],
                    "states": {k: states.count(k) for k in set(states)}}
-    ok = torch.tensor([st != "non-finite" for st in states])
+    ok = torch.tensor([st == "converged" for st in states])
     keep = torch.nonzero(ok).flatten()
+    out["data"]["training_targets"] = int(ok.sum())
     fields = fields.index_select(0, keep.cuda())
     re_tr = re_tr[keep.numpy()]
     model = sur.Surrogate(max_batch=batch, H=N, W=N, base_channels=base, seed=seed)

@@ -520,9 +520,11 @@ int kb_batch_status(kb_batch *b, long long *updates, int *n_live, int *timed_out
  * row j = slow index); synchronises `stream`. */
 int kb_batch_case(kb_batch *b, int c, int *N, int *steps, double *residual, int *state,
                   float *ux_host, float *uy_host, void *stream);
-/* Time trial_steps of every (tile_nodes, blocks_per_sm) candidate, keep the
- * fastest for later runs; reports its MLUPS and the fixed schedule's (tile
- * 256, 1 block per SM).  Resets the batch. */
+/* Time trial_steps of every (tile_nodes, blocks_per_sm) candidate (tiles of
+ * 256 ... 4096 nodes, 1 ... the occupancy limit of blocks per SM), keep the
+ * fastest for later runs; reports its MLUPS and that of the fixed schedule
+ * kb_batch_run takes untuned (256-node tiles, as many blocks per SM as fit).
+ * Resets the batch. */
 int kb_batch_autotune(kb_batch *b, int trial_steps, int *best_tile, int *best_bpsm,
                       double *best_mlups, double *fixed_mlups, void *stream);
 /* Device pointer to case c's final populations (9 planes of N*N, storage

@@ -86,6 +86,16 @@ class CavityBatch:
         call("kb_batch_run", self._h, int(max_steps), int(check_every), float(tol),
              int(tile_nodes), int(blocks_per_sm), _stream())
 
+    def capture(self, max_steps=50000, check_every=100, tol=1e-6):
+        """The sweep's one cooperative launch (kb_batch_run with the current
+        schedule) captured in a CUDA graph.  Each .launch() of the returned
+        Graph advances the batch from its state at that moment; reset() first
+        to replay the whole sweep.  close() the graph when done."""
+        g = Graph()
+        with g:
+            self.run(max_steps, check_every, tol)
+        return g
+
     def status(self):
         up, live, tout = C.c_longlong(), C.c_int(), C.c_int()
         call("kb_batch_status", self._h, C.byref(up), C.byref(live), C.byref(tout), _stream())

@@ -600,6 +600,24 @@ int launch(kb_batch *b, int max_steps, int check_every, double tol, int blocks_p
     return KB_OK;
 }
 
+// Resident blocks per SM of the batched kernel for a storage.
+int batch_occupancy(int dtype) {
+    int occ = 0;
+    cudaError_t e;
+    switch (dtype) {
+        case KB_F16_DEV: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_k<__half, false>, BT, 0); break;
+        case KB_BF16_DEV: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_k<__nv_bfloat16, false>, BT, 0); break;
+        case KB_F16_DEV_SR: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_k<__half, true>, BT, 0); break;
+        case KB_BF16_DEV_SR: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_k<__nv_bfloat16, true>, BT, 0); break;
+        default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_k<float, false>, BT, 0); break;
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return occ;
+}
+
 }  // namespace
 
 extern "C" {
@@ -746,15 +764,19 @@ int kb_batch_autotune(kb_batch *b, int trial_steps, int *best_tile, int *best_bp
     KB_REQUIRE(b, "kb_batch_autotune: null handle");
     KB_REQUIRE(trial_steps >= 2 && trial_steps % 2 == 0, "kb_batch_autotune: trial_steps must be even and >= 2");
     cudaStream_t s = kb::as_stream(stream);
+    // the candidates: tile sizes x every residency up to the occupancy limit;
+    // the fixed schedule is what kb_batch_run takes untuned (256-node tiles,
+    // as many blocks per SM as fit)
+    const int occ = batch_occupancy(b->dtype);
+    if (occ < 1) return kb::set_error(KB_ERR_UNSUPPORTED, "kb_batch_autotune: kernel does not fit an SM");
     const int tiles[] = {256, 512, 1024, 2048, 4096};
-    const int bpsms[] = {1, 2, 4, 8, 16};  // clamped to the occupancy limit at launch
     double best = -1.0, fixed = -1.0;
-    int bt = 256, bb = 1;
+    int bt = 256, bb = occ;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     for (int tn : tiles)
-        for (int bp : bpsms) {
+        for (int bp = 1; bp <= occ; ++bp) {
             if (int r = build_tiles(b, tn)) return r;
             if (int r = reset(b, s)) return r;
             cudaEventRecord(e0, s);
@@ -768,7 +790,7 @@ int kb_batch_autotune(kb_batch *b, int trial_steps, int *best_tile, int *best_bp
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
             const double mlups = (double)up / (ms * 1e-3) / 1e6;
-            if (tn == 256 && bp == 1) fixed = mlups;
+            if (tn == 256 && bp == occ) fixed = mlups;
             if (mlups > best) { best = mlups; bt = tn; bb = bp; }
         }
     cudaEventDestroy(e0);

@@ -257,8 +257,11 @@ def test_trained_network_shortens_time_to_steady(cuda, sur):
     assert all(c.residual <= 1e-8 for c in cold + ideal + warm), msg
     assert total(ideal, 1e-8) < 0.6 * total(cold, 1e-8), msg
     assert total(warm, 1e-4) < total(cold, 1e-4), msg
+    # the warm-started runs converge to the cold runs' steady field: velocity
+    # difference at most 1e-6 of the lid speed
     for c, w in zip(cold, warm):
         d = (c.fields() - w.fields()).abs()
-        assert float(d[1:].max()) / 0.1 < 1e-4, msg
+        assert float(d[1:].max()) / 0.1 < 1e-6, msg
+    assert all(c.reached[1e-8] > 0 for c in cold + warm), msg
     assert not model.timed_out()
     model.close()
