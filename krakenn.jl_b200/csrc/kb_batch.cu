@@ -301,7 +301,7 @@ __device__ __forceinline__ void pair_finish(float2 *d, R *__restrict__ dst, int 
     const float2 pxx = vsub(vadd(d[1], d[3]), vadd(d[2], d[4]));
     const float2 pxy = vsub(vadd(d[5], d[7]), vadd(d[6], d[8]));
     const float2 rho = vadd(vsplat(1.0f, z), drho);
-    const float2 inv = vrcp(rho);
+    const float2 inv = vrcp_fast(rho);
     ux = vmul(jx, inv);
     uy = vmul(jy, inv);
     const float2 r3u = vmul(vmul(vsplat(3.0f, z), rho), vfma(ux, ux, vmul(uy, uy)));
@@ -386,16 +386,21 @@ __global__ void __launch_bounds__(BT, KB_BATCH_MIN_BLOCKS) batch_k(BatchState D,
             // and case offsets are multiples of 64, so every pair is aligned;
             // software-pipelined: the next pair's pulls are in flight (as raw
             // stored values) while this pair collides
+            // (i, j) of node m advance by the stride 2 BT with one division
+            // per tile, not per pair: 2 BT = dj rows + di columns (di even)
             R vn[18];
             int m = T.start + 2 * threadIdx.x;
-            if (m < end) pair_loads_raw<R>(src + C.f_off, C.N, m % C.N, m / C.N, vn);
+            int j = m / C.N, i = m - j * C.N;
+            const int dj = (2 * BT) / C.N, di = 2 * BT - dj * C.N;
+            if (m < end) pair_loads_raw<R>(src + C.f_off, C.N, i, j, vn);
             for (; m < end; m += 2 * BT) {
-                const int j = m / C.N, i = m - j * C.N;
                 float2 d[9];
 #pragma unroll
                 for (int q = 0; q < 9; ++q) d[q] = make_float2(Dev<R>::ld(vn[2 * q]), Dev<R>::ld(vn[2 * q + 1]));
+                int in = i + di, jn = j + dj;
+                if (in >= C.N) { in -= C.N; ++jn; }
                 const int mn = m + 2 * BT;
-                if (mn < end) pair_loads_raw<R>(src + C.f_off, C.N, mn % C.N, mn / C.N, vn);
+                if (mn < end) pair_loads_raw<R>(src + C.f_off, C.N, in, jn, vn);
                 float2 ux, uy;
                 const uint32_t key =
                     SR ? hash32((uint32_t)(C.f_off + m) ^ hash32((uint32_t)s * 0x632BE5ABu + seed)) : 0u;
@@ -416,6 +421,8 @@ __global__ void __launch_bounds__(BT, KB_BATCH_MIN_BLOCKS) batch_k(BatchState D,
                     u2 += (double)ux.x * ux.x + (double)uy.x * uy.x + (double)ux.y * ux.y +
                           (double)uy.y * uy.y;
                 }
+                i = in;
+                j = jn;
             }
             }
             if (check) {

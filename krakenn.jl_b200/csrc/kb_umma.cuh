@@ -491,16 +491,18 @@ struct ConvOp {
         int b = 0, h = 0, w = 0;
         const bool live = m < M;
         if (live) pixel_of(m, x.H, x.W, b, h, w);
+        // (tap, c) of the step's first chunk by one division; the next chunks
+        // step c by 8 and carry into tap (C is a multiple of 8)
+        int tap = (kt * BK) / C, c = kt * BK - tap * C;
 #pragma unroll
         for (int kc = 0; kc < 8; ++kc) {
             const int k = kt * BK + kc * 8;
             bool v = false;
             const __nv_bfloat16 *p = x.s1;
-            if (live && k < K9) {
-                const int tap = k / C, c = k - tap * C;
-                p = x.chunk_ptr(b, h + tap / 3 - 1, w + tap % 3 - 1, c, v);
-            }
+            if (live && k < K9) p = x.chunk_ptr(b, h + tap / 3 - 1, w + tap % 3 - 1, c, v);
             cp16(s + (uint32_t)(kc * BM * 16 + r * 16), p, v);
+            c += 8;
+            if (c >= C) { c -= C; ++tap; }
         }
     }
 
@@ -568,6 +570,12 @@ struct WgradOp {
         const int k_lo = threadIdx.x & 7, g = (threadIdx.x >> 3) & 15;
         const int r = t.x * BM + g * 8;
         const int tap = r / C, c = r - tap * C;
+        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+        // pixel of the step's first chunk by one pixel_of; the next chunks
+        // are 8 pixels on (one row carry when the image is at least 8 wide;
+        // the deepest levels of a small image may be narrower)
+        int b, h, w;
+        pixel_of(kt * BK + k_lo, x.H, x.W, b, h, w);
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const int m = kt * BK + i * 8 + k_lo;
@@ -575,15 +583,18 @@ struct WgradOp {
             const void *p = x.s1;
             if (m < M) {
                 if (r < R) {
-                    int b, h, w;
-                    pixel_of(m, x.H, x.W, b, h, w);
-                    p = x.chunk_ptr(b, h + tap / 3 - 1, w + tap % 3 - 1, c, v);
+                    p = x.chunk_ptr(b, h + dy, w + dx, c, v);
                 } else if (r == R) {
                     p = kOneChunk;  // bf16 1.0 in element 0: the bias row
                     v = true;
                 }
             }
             cp16(s + (uint32_t)(i * BM * 16 + g * 128 + k_lo * 16), p, v);
+            w += 8;
+            while (w >= x.W) {
+                w -= x.W;
+                if (++h == x.H) { h = 0; ++b; }
+            }
         }
     }
 
