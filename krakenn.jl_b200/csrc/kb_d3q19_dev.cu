@@ -721,25 +721,11 @@ __device__ __forceinline__ bool tbar_wait(uint32_t bar, uint32_t parity) {
 __device__ __forceinline__ void tbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
-// KB_TMA_ELECT: the producer warp runs its tile loop converged, with the warp
-// index made provably uniform, and every copy is issued by the lane that
-// elect.sync picks inside the copy's own asm; otherwise one lane issues the
-// copies in a branch of its own.
-#ifndef KB_TMA_ELECT
-#define KB_TMA_ELECT 0
-#endif
-#if KB_TMA_ELECT
-#define KB_ELECT_PRED "{\n\t.reg .pred pe;\n\telect.sync _|pe, 0xffffffff;\n\t@pe "
-#define KB_ELECT_END ";\n\t}"
-#else
-#define KB_ELECT_PRED ""
-#define KB_ELECT_END ";"
-#endif
 __device__ __forceinline__ void tma_load4(uint32_t dst, const CUtensorMap *tm, int x, int y, int z,
                                           int q, uint32_t bar) {
     asm volatile(
-        KB_ELECT_PRED "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4, %5}], [%6]" KB_ELECT_END ::"r"(dst),
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
         "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(q), "r"(bar)
         : "memory");
 }
@@ -781,16 +767,15 @@ struct TileMaps {
 __device__ __forceinline__ void tma_load3(uint32_t dst, const CUtensorMap *tm, int x, int y, int z,
                                           uint32_t bar) {
     asm volatile(
-        KB_ELECT_PRED "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4}], [%5]" KB_ELECT_END ::"r"(dst),
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
         "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(bar)
         : "memory");
 }
 __device__ __forceinline__ void tma_issue_tile(const TileMaps &mp, uint32_t dst, uint32_t bar,
                                                int x0, int j, int k, const TileMap &m, bool halos) {
     const uint32_t bytes = (halos ? TBYTES : TROWBYTES) + (mp.tc ? (uint32_t)TT : 0u);
-    asm volatile(KB_ELECT_PRED "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1" KB_ELECT_END
-                 ::"r"(bar), "r"(bytes)
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                  : "memory");
     // tensor-map z coordinates: the map spans the whole allocation, this
     // range starts at plane zoff; with a z halo the neighbours are read as is
@@ -908,9 +893,7 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
     int cx, cj, ck;  // this role's current tile
     m.at((int)blockIdx.x, cx, cj, ck);
 
-    // the warp index, provably uniform across the warp (a shuffle from lane 0)
-    const int warp_u = __shfl_sync(0xffffffffu, t >> 5, 0);
-    if (warp_u == TCONS / 32) {
+    if (t >= TCONS) {
         // ------------------------------------------------ producer warp --
         const TileMaps mp{&tmap1, &tmap2, &tmap3, &thalo, LINKS ? &tcls : nullptr};
         if (t == TCONS) {
@@ -929,20 +912,19 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
             const int s = n % TSTAGES;
             // the consumers have released this stage's previous tile; every
             // lane of the warp leaves the loop together on a timeout (the
-            // warp-synchronous copy issue below needs all of them)
+            // __syncwarp below needs all of them)
             if (n >= TSTAGES &&
                 !__all_sync(0xffffffffu,
                             tbar_wait(s_addr(&empty[s]), (uint32_t)(n / TSTAGES - 1) & 1u))) {
                 if (t == TCONS) atomicExch(&g_tma_timeout, 1);
                 break;
             }
-            if (KB_TMA_ELECT || t == TCONS) {
+            if (t == TCONS) {
                 const uint32_t bar = s_addr(&full[s]);
                 if (m.staged(cj, ck))
                     tma_issue_tile(mp, s_addr(stage0 + s * TSTAGE), bar, cx * TT, cj, ck, m, halos);
                 else  // nothing to copy: the phase completes on the arrival
-                    asm volatile(KB_ELECT_PRED "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], 0"
-                                 KB_ELECT_END ::"r"(bar)
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], 0;" ::"r"(bar)
                                  : "memory");
             }
             __syncwarp();
