@@ -508,10 +508,15 @@ struct ConvOp {
 
     __device__ void load_b(uint32_t s, int kt, const uint3 &t) const {
         const int n0 = t.y * bn;
+        // chunk c = kc * bn + r; stepping c by THREADS steps (kc, r) with a carry
+        int kc = threadIdx.x / bn, r = threadIdx.x - kc * bn;
+        const int dk = THREADS / bn, dr = THREADS - dk * bn;
         for (int c = threadIdx.x; c < bn * 8; c += THREADS) {
-            const int r = c % bn, kc = c / bn;
             cp16(s + (uint32_t)(kc * bn * 16 + r * 16), wt + (size_t)(n0 + r) * Kp + kt * BK + kc * 8,
                  true);
+            kc += dk;
+            r += dr;
+            if (r >= bn) { r -= bn; ++kc; }
         }
     }
 
@@ -600,12 +605,19 @@ struct WgradOp {
 
     __device__ void load_b(uint32_t s, int kt, const uint3 &t) const {
         const int groups = bn >> 3, n0 = t.y * bn;
+        // chunk c: k_lo = c % 8 and (c / 8) = k_hi * groups + g; stepping c by
+        // THREADS steps (k_hi, g) with a carry
+        const int k_lo = threadIdx.x & 7;
+        int k_hi = (threadIdx.x >> 3) / groups, g = (threadIdx.x >> 3) - k_hi * groups;
+        const int dq = THREADS >> 3, dk = dq / groups, dg = dq - dk * groups;
         for (int c = threadIdx.x; c < bn * 8; c += THREADS) {
-            const int k_lo = c & 7, g = (c >> 3) % groups, k_hi = (c >> 3) / groups;
             const int m = kt * BK + k_hi * 8 + k_lo;
             const bool v = m < M;
             cp16(s + (uint32_t)(k_hi * bn * 16 + g * 128 + k_lo * 16),
                  v ? (const void *)(dy + (size_t)m * Nout + n0 + g * 8) : (const void *)dy, v);
+            k_hi += dk;
+            g += dg;
+            if (g >= groups) { g -= groups; ++k_hi; }
         }
     }
 
