@@ -1170,7 +1170,7 @@ def bench_surrogate(pkg, steps=10, warmup=3, batch=16, N=256, base=32, engine=No
             peak = None
     peak = float(peak) if peak else 1390.0
     out = {"workload": f"warm-start U-Net, {N}^2, batch {batch}, {base} base channels, BF16 "
-                       f"tcgen05, engine {1 if engine is None else engine}",
+                       f"tcgen05, engine {2 if engine is None else engine}",
            "train_ms": round(ms_t, 3), "train_tflops": round(trn / (ms_t * 1e-3) / 1e12, 1),
            "infer_ms": round(ms_i, 3), "infer_tflops": round(fwd / (ms_i * 1e-3) / 1e12, 1),
            "bf16_peak_tflops": peak,
@@ -1178,7 +1178,7 @@ def bench_surrogate(pkg, steps=10, warmup=3, batch=16, N=256, base=32, engine=No
            "timed_out": m.timed_out()}
     m.close()
     if engine is not None:
-        pkg.set_umma_engine(1)
+        pkg.set_umma_engine(2)
     return out
 
 

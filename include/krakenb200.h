@@ -479,8 +479,10 @@ int kb_fused_trt_step_3d_zrange(void *f_out, const void *f_in, void *rho, void *
  * copies (16-bit storages, Nx % 8 == 0, 16-byte aligned populations).
  * Variants 2 to 5 collide in packed FP32x2 arithmetic.
  * kernel 2 = the tensor-core engine of the warm-start network and
- * kb_gemm_bf16: 0 warp-specialised persistent kernel, 1 one CTA per output
- * tile (default).  Every variant
+ * kb_gemm_bf16: 0 warp-specialised persistent kernel with cp.async operand
+ * staging, 1 one CTA per output tile with cp.async staging, 2 (default)
+ * persistent kernel with tensor-memory-accelerator operand staging in
+ * swizzled layouts (shapes it cannot tile run on engine 1).  Every variant
  * computes the same update up to FP32 rounding.  No reference counterpart. */
 int kb_set_kernel_variant(int kernel, int variant);
 

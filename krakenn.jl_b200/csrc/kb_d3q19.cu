@@ -684,7 +684,7 @@ extern "C" {
 int kb_set_kernel_variant(int kernel, int variant) {
     KB_REQUIRE(kernel == 1 || kernel == 2, "kb_set_kernel_variant: unknown kernel id %d", kernel);
     if (kernel == 2) {
-        KB_REQUIRE(variant == 0 || variant == 1, "kb_set_kernel_variant: engine %d not in 0..1", variant);
+        KB_REQUIRE(variant >= 0 && variant <= 2, "kb_set_kernel_variant: engine %d not in 0..2", variant);
         kb::umma::set_engine(variant);
         return KB_OK;
     }

@@ -25,7 +25,7 @@
 #include <vector>
 
 #include "kb_common.cuh"
-#include "kb_umma.cuh"
+#include "kb_umma_tma.cuh"
 
 namespace kb {
 namespace sur {
@@ -82,6 +82,22 @@ __global__ void pool_k(bf16 *__restrict__ out, const bf16 *__restrict__ in, int 
 #pragma unroll
         for (int i = 0; i < 8; ++i) o[i] = __float2bfloat16_rn(0.25f * s[i]);
         *reinterpret_cast<uint4 *>(out + (size_t)p * C + c) = *reinterpret_cast<const uint4 *>(o);
+    }
+}
+
+// Nearest upsampling, NHWC BF16, 8 channels per thread: dst [B][H][W][C] from
+// src [B][H/2][W/2][C] (the decoder input that the TMA engine copies by boxes).
+__global__ void upsample_k(bf16 *__restrict__ dst, const bf16 *__restrict__ src, int B, int H, int W,
+                           int C) {
+    const int cc = C / 8;
+    const long long n = (long long)B * H * W * cc;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t % cc) * 8;
+        const long long p = t / cc;
+        const int w = (int)(p % W), h = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
+        const size_t q = (((size_t)b * (H / 2) + h / 2) * (W / 2) + w / 2) * C + c;
+        *reinterpret_cast<uint4 *>(dst + (size_t)p * C + c) = *reinterpret_cast<const uint4 *>(src + q);
     }
 }
 
@@ -306,6 +322,19 @@ struct Layer {
     long long w_off, b_off;
     bf16 *wb = nullptr, *wt = nullptr;
     bf16 *dx = nullptr;  // data-gradient output (own buffer for concat inputs)
+    bf16 *up = nullptr;  // decoder layers: in1 upsampled to this level (TMA engine)
+};
+
+// The TMA engine's operations of one layer for a batch of n images (the maps
+// bound the image index by n, so images beyond the batch read as zeros).
+// f / d / w: the forward, data-gradient and weight-gradient shapes tile into
+// TMA boxes (otherwise that operation runs on the one-CTA-per-tile engine).
+struct TmaPlan {
+    int n = -1;
+    bool f = false, d = false, w = false;
+    int wsplits = 0;
+    kb::umma::ConvTma fwd, dgr;
+    kb::umma::WgradTma wg;
 };
 
 }  // namespace sur
@@ -328,6 +357,9 @@ struct kb_surrogate {
     float *loss = nullptr;
     Norm norm{{1.f, 1.f, 1.f}, {0.f, 0.f, 0.f}};
     float grad_weight = 0.f;  // weight of the gradient (H1) term of the loss
+    std::vector<TmaPlan> tp;            // per layer, TMA engine
+    bf16 *ones = nullptr;               // [64][64] BF16, column 0 = 1: the bias row's A block
+    int up_batch = -1;                  // batch of the decoder inputs last upsampled
     std::vector<void *> allocs;
     int H_at(int level) const { return H >> level; }
     int W_at(int level) const { return W >> level; }
@@ -375,9 +407,130 @@ int wgrad_splits(const Layer &l, int M, int &steps_per_split) {
     return (nsteps + steps_per_split - 1) / steps_per_split;
 }
 
+// Decoder input in1 of layer l upsampled to the layer's level (l.up).
+void upsample(kb_surrogate *s, const Layer &l, int n, cudaStream_t st) {
+    const int H = s->H_at(l.level), W = s->W_at(l.level);
+    upsample_k<<<ew_grid((long long)n * H * W * (l.cin1 / 8)), 256, 0, st>>>(l.up, s->act[l.in1], n, H,
+                                                                              W, l.cin1);
+}
+
+// Build (or keep) the TMA engine's operations of layer i for n images.
+int prepare_tma(kb_surrogate *s, int i, int n) {
+    using namespace kb::umma;
+    const Layer &l = s->L[i];
+    TmaPlan &p = s->tp[i];
+    if (p.n == n) return 0;
+    p.n = -1;
+    p.f = p.d = p.w = false;
+    const char *what = "kb_surrogate (TMA engine)";
+    const int H = s->H_at(l.level), W = s->W_at(l.level), M = n * H * W;
+    const bf16 *x1 = l.in2 >= 0 ? l.up : s->act[l.in1];
+    const bf16 *x2 = l.in2 >= 0 ? s->act[l.in2] : nullptr;
+    PixBox b128{}, b64{};
+    const bool g128 = pix_box(BM, H, W, b128), g64 = pix_box(BK, H, W, b64);
+    int rc = 0;
+    // forward: boxes of e input channels x 128 pixels, weights e x bn_f
+    const int ef = chunk_of(l.cin1, l.cin2);
+    if (ef && g128) {
+        ConvTma &c = p.fwd;
+        c = ConvTma{};
+        if ((rc = nhwc_map(&c.x1, x1, l.cin1, W, H, n, ef, b128, what))) return rc;
+        if (x2 && (rc = nhwc_map(&c.x2, x2, l.cin2, W, H, n, ef, b128, what))) return rc;
+        if (!x2) c.x2 = c.x1;
+        const cuuint64_t d[2] = {(cuuint64_t)l.Kp, (cuuint64_t)l.cout}, sd[1] = {(cuuint64_t)l.Kp * 2};
+        const cuuint32_t bx[2] = {(cuuint32_t)ef, (cuuint32_t)l.bn_f};
+        if ((rc = bf16_map(&c.w, l.wb, 2, d, sd, bx, 2 * ef, what))) return rc;
+        c.e = ef;
+        c.c1 = l.cin1;
+        c.C = l.cin;
+        c.H = H;
+        c.W = W;
+        c.nck = l.cin / ef;
+        c.a_bytes = round1k((uint32_t)(BM * 2 * ef));
+        c.b_bytes = round1k((uint32_t)(l.bn_f * 2 * ef));
+        c.tx = (uint32_t)(BM * 2 * ef + l.bn_f * 2 * ef);
+        c.bias = s->params + l.b_off;
+        c.mask.s1 = nullptr;
+        c.out = l.out == T_OUT ? (void *)s->out_f32 : (void *)s->act[l.out];
+        c.M = M;
+        c.Nout = l.cout;
+        c.bn = l.bn_f;
+        c.relu = l.relu;
+        c.out_f32 = l.out == T_OUT;
+        p.f = true;
+    }
+    // data gradient: boxes of e output-gradient channels, weights wt [cin][Kpt]
+    const int ed = chunk_of(l.cout);
+    if (i > 0 && ed && g128) {
+        ConvTma &c = p.dgr;
+        c = ConvTma{};
+        if ((rc = nhwc_map(&c.x1, s->grad[l.out], l.cout, W, H, n, ed, b128, what))) return rc;
+        c.x2 = c.x1;
+        const cuuint64_t d[2] = {(cuuint64_t)l.Kpt, (cuuint64_t)l.cin}, sd[1] = {(cuuint64_t)l.Kpt * 2};
+        const cuuint32_t bx[2] = {(cuuint32_t)ed, (cuuint32_t)l.bn_d};
+        if ((rc = bf16_map(&c.w, l.wt, 2, d, sd, bx, 2 * ed, what))) return rc;
+        c.e = ed;
+        c.c1 = l.cout;
+        c.C = l.cout;
+        c.H = H;
+        c.W = W;
+        c.nck = l.cout / ed;
+        c.a_bytes = round1k((uint32_t)(BM * 2 * ed));
+        c.b_bytes = round1k((uint32_t)(l.bn_d * 2 * ed));
+        c.tx = (uint32_t)(BM * 2 * ed + l.bn_d * 2 * ed);
+        c.bias = nullptr;
+        if (l.pooled_in) c.mask.s1 = nullptr;
+        else c.mask = view_of(s, l, n);
+        c.out = l.dx;
+        c.M = M;
+        c.Nout = l.cin;
+        c.bn = l.bn_d;
+        c.relu = 0;
+        c.out_f32 = 0;
+        p.d = true;
+    }
+    // weight gradient: blocks of ea input channels / eb output-gradient
+    // channels x 64 pixels
+    const int ea = chunk_of(l.cin1, l.cin2), eb = chunk_of(l.bn_w);
+    if (ea && eb && g64) {
+        WgradTma &w = p.wg;
+        w = WgradTma{};
+        if ((rc = nhwc_map(&w.x1, x1, l.cin1, W, H, n, ea, b64, what))) return rc;
+        if (x2 && (rc = nhwc_map(&w.x2, x2, l.cin2, W, H, n, ea, b64, what))) return rc;
+        if (!x2) w.x2 = w.x1;
+        const cuuint64_t d[2] = {(cuuint64_t)ea, 64}, sd[1] = {128};
+        const cuuint32_t bx[2] = {(cuuint32_t)ea, 64};
+        if ((rc = bf16_map(&w.ones, s->ones, 2, d, sd, bx, 2 * ea, what))) return rc;
+        if ((rc = nhwc_map(&w.dy, s->grad[l.out], l.cout, W, H, n, eb, b64, what))) return rc;
+        int sps = 0;
+        p.wsplits = wgrad_splits(l, M, sps);
+        w.part = s->part;
+        w.bn = l.bn_w;
+        w.ea = ea;
+        w.eb = eb;
+        w.c1 = l.cin1;
+        w.C = l.cin;
+        w.H = H;
+        w.W = W;
+        w.Nout = l.cout;
+        w.steps_per_split = sps;
+        w.nsteps = (M + BK - 1) / BK;
+        w.py = W < BK && H * W >= BK ? BK / W : 0;
+        w.pb = H * W < BK ? BK / (H * W) : 0;
+        w.na = BM / ea;
+        w.nb = l.bn_w / eb;
+        w.a_bytes = BM * BK * 2;
+        w.b_bytes = round1k((uint32_t)(l.bn_w * BK * 2));
+        p.w = true;
+    }
+    p.n = n;
+    return 0;
+}
+
 int forward(kb_surrogate *s, const void *input, int n, cudaStream_t st) {
     using namespace kb::umma;
     s->act[T_IN] = (bf16 *)input;
+    const bool tma = engine() == 2;
     for (int i = 0; i < N_LAYERS; ++i) {
         const Layer &l = s->L[i];
         // pooled inputs are produced just before their consumer
@@ -388,6 +541,15 @@ int forward(kb_surrogate *s, const void *input, int n, cudaStream_t st) {
                 s->act[l.in1], s->act[src.out], n, Ho, Wo, src.cout);
         }
         const int M = n * s->H_at(l.level) * s->W_at(l.level);
+        const dim3 grid((M + BM - 1) / BM, l.cout / l.bn_f);
+        if (tma) {
+            if (l.in2 >= 0) upsample(s, l, n, st);
+            if (int rc = prepare_tma(s, i, n)) return rc;
+            if (s->tp[i].f) {
+                if (int rc = launch_tma(s->tp[i].fwd, grid, s->err, st)) return rc;
+                continue;
+            }
+        }
         ConvOp op{};
         op.x = view_of(s, l, n);
         op.wt = l.wb;
@@ -401,61 +563,81 @@ int forward(kb_surrogate *s, const void *input, int n, cudaStream_t st) {
         op.relu = l.relu;
         op.out_f32 = l.out == T_OUT;
         op.nsteps = l.Kp / BK;
-        const dim3 grid((M + BM - 1) / BM, l.cout / l.bn_f);
         if (int rc = launch(op, grid, s->err, st)) return rc;
     }
+    s->up_batch = tma ? n : -1;
     return kb::check_launch("kb_surrogate forward");
 }
 
 int backward(kb_surrogate *s, int n, cudaStream_t st) {
     using namespace kb::umma;
+    const bool tma = engine() == 2;
+    if (tma && s->up_batch != n) {
+        // the forward pass ran on another engine: upsample the decoder inputs
+        for (const Layer &l : s->L)
+            if (l.in2 >= 0) upsample(s, l, n, st);
+        s->up_batch = n;
+    }
     for (int i = N_LAYERS - 1; i >= 0; --i) {
         const Layer &l = s->L[i];
         const int Hl = s->H_at(l.level), Wl = s->W_at(l.level);
         const int M = n * Hl * Wl;
         const ActView xv = view_of(s, l, n);
+        if (tma)
+            if (int rc = prepare_tma(s, i, n)) return rc;
+        const TmaPlan &tp = s->tp[i];
+        const int R = 9 * l.cin;
         // weight gradient (split over pixels) and its reduction
         int sps = 0;
-        const int splits = wgrad_splits(l, M, sps);
-        WgradOp wo{};
-        wo.x = xv;
-        wo.dy = s->grad[l.out];
-        wo.part = s->part;
-        wo.M = M;
-        wo.Nout = l.cout;
-        wo.bn = l.bn_w;
-        wo.steps_per_split = sps;
-        wo.nsteps = (M + BK - 1) / BK;
-        const int R = 9 * l.cin;
-        const dim3 wg((R + 1 + BM - 1) / BM, l.cout / l.bn_w, splits);
-        if (int rc = launch(wo, wg, s->err, st)) return rc;
+        int splits = wgrad_splits(l, M, sps);
+        if (tma && tp.w) {
+            splits = tp.wsplits;
+            const dim3 wg((R + 1 + BM - 1) / BM, l.cout / l.bn_w, splits);
+            if (int rc = launch_tma(tp.wg, wg, s->err, st)) return rc;
+        } else {
+            WgradOp wo{};
+            wo.x = xv;
+            wo.dy = s->grad[l.out];
+            wo.part = s->part;
+            wo.M = M;
+            wo.Nout = l.cout;
+            wo.bn = l.bn_w;
+            wo.steps_per_split = sps;
+            wo.nsteps = (M + BK - 1) / BK;
+            const dim3 wg((R + 1 + BM - 1) / BM, l.cout / l.bn_w, splits);
+            if (int rc = launch(wo, wg, s->err, st)) return rc;
+        }
         wgrad_reduce_k<<<ew_grid((long long)(R + 1) * l.cout), 256, 0, st>>>(
             s->grads + l.w_off, s->grads + l.b_off, s->part, splits, R, l.cout);
         if (i == 0) break;
         // data gradient
-        ConvOp op{};
-        op.x.s1 = s->grad[l.out];
-        op.x.c1 = l.cout;
-        op.x.up1 = 0;
-        op.x.s2 = nullptr;
-        op.x.c2 = 0;
-        op.x.B = n;
-        op.x.H = Hl;
-        op.x.W = Wl;
-        op.wt = l.wt;
-        op.bias = nullptr;
-        if (l.pooled_in) op.mask.s1 = nullptr;
-        else op.mask = xv;
-        op.out = l.dx;
-        op.M = M;
-        op.Nout = l.cin;
-        op.Kp = l.Kpt;
-        op.bn = l.bn_d;
-        op.relu = 0;
-        op.out_f32 = 0;
-        op.nsteps = l.Kpt / BK;
         const dim3 grid((M + BM - 1) / BM, l.cin / l.bn_d);
-        if (int rc = launch(op, grid, s->err, st)) return rc;
+        if (tma && tp.d) {
+            if (int rc = launch_tma(tp.dgr, grid, s->err, st)) return rc;
+        } else {
+            ConvOp op{};
+            op.x.s1 = s->grad[l.out];
+            op.x.c1 = l.cout;
+            op.x.up1 = 0;
+            op.x.s2 = nullptr;
+            op.x.c2 = 0;
+            op.x.B = n;
+            op.x.H = Hl;
+            op.x.W = Wl;
+            op.wt = l.wt;
+            op.bias = nullptr;
+            if (l.pooled_in) op.mask.s1 = nullptr;
+            else op.mask = xv;
+            op.out = l.dx;
+            op.M = M;
+            op.Nout = l.cin;
+            op.Kp = l.Kpt;
+            op.bn = l.bn_d;
+            op.relu = 0;
+            op.out_f32 = 0;
+            op.nsteps = l.Kpt / BK;
+            if (int rc = launch(op, grid, s->err, st)) return rc;
+        }
         // route the concat's gradient: the upsampled part to the low-resolution tensor
         if (l.in2 >= 0) {
             const Layer &lo = s->L[i - 1];  // producer of in1 (bott_b / dec3b / dec2b)
@@ -566,6 +748,7 @@ int kb_surrogate_create(kb_surrogate **out, int max_batch, int H, int W, int bas
             if (l.in2 >= 0) A((void **)&l.dx, px * l.cin * sizeof(bf16));
             else l.dx = s->grad[l.in1];
         }
+        if (l.in2 >= 0) A((void **)&l.up, px * l.cin1 * sizeof(bf16));
         const size_t need = (size_t)max_wgrad_splits(l) * (9 * l.cin + 1) * l.cout;
         if (need > part) part = need;
     }
@@ -577,6 +760,8 @@ int kb_surrogate_create(kb_surrogate **out, int max_batch, int H, int W, int bas
     A((void **)&s->adam_v, (size_t)s->n_params * sizeof(float));
     A((void **)&s->err, sizeof(int));
     A((void **)&s->loss, sizeof(float));
+    A((void **)&s->ones, 64 * 64 * sizeof(bf16));
+    s->tp.resize(N_LAYERS);
     if (rc) {
         for (void *p : s->allocs) cudaFree(p);
         delete s;
@@ -595,6 +780,12 @@ int kb_surrogate_create(kb_surrogate **out, int max_batch, int H, int W, int bas
         }
     }
     cudaMemcpyAsync(s->params, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, st);
+    static const std::vector<unsigned short> ones = [] {
+        std::vector<unsigned short> o(64 * 64, 0);
+        for (int k = 0; k < 64; ++k) o[k * 64] = 0x3F80u;  // BF16 1.0
+        return o;
+    }();
+    cudaMemcpyAsync(s->ones, ones.data(), ones.size() * sizeof(unsigned short), cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(s->adam_m, 0, (size_t)s->n_params * sizeof(float), st);
     cudaMemsetAsync(s->adam_v, 0, (size_t)s->n_params * sizeof(float), st);
     cudaMemsetAsync(s->grads, 0, (size_t)s->n_params * sizeof(float), st);

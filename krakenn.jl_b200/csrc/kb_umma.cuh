@@ -469,18 +469,55 @@ __device__ __forceinline__ void pixel_of(int m, int H, int W, int &b, int &h, in
     w = r - h * W;
 }
 
+// Epilogue of a convolution tile: + bias, ReLU, multiply by (mask view > 0),
+// store BF16 or FP32 rows of [M][Nout].
+struct ConvStore {
+    const float *bias;  // [Nout] or null
+    ActView mask;       // mask.s1 == null: no mask
+    void *out;          // [M][Nout] BF16 or FP32
+    int M, Nout, bn, relu, out_f32;
+
+    __device__ void store(int row, int col, const float *v, const uint3 &t) const {
+        const int m = t.x * BM + row;
+        if (m >= M) return;
+        const int n = t.y * bn + col;
+        float o[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            float t = v[i] + (bias ? bias[n + i] : 0.f);
+            o[i] = relu ? fmaxf(t, 0.f) : t;
+        }
+        if (mask.s1) {
+            int b, h, w;
+            pixel_of(m, mask.H, mask.W, b, h, w);
+            const uint4 mv = mask.chunk(b, h, w, n);
+            const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&mv);
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                if (!(__bfloat162float(mb[i]) > 0.f)) o[i] = 0.f;
+        }
+        if (out_f32) {
+            float4 *d = reinterpret_cast<float4 *>((float *)out + (size_t)m * Nout + n);
+            d[0] = make_float4(o[0], o[1], o[2], o[3]);
+            d[1] = make_float4(o[4], o[5], o[6], o[7]);
+        } else {
+            __align__(16) __nv_bfloat162 p[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) p[i] = __floats2bfloat162_rn(o[2 * i], o[2 * i + 1]);
+            *reinterpret_cast<uint4 *>((__nv_bfloat16 *)out + (size_t)m * Nout + n) =
+                *reinterpret_cast<const uint4 *>(p);
+        }
+    }
+};
+
 // Convolution forward (and data gradient): D[m, n] = sum_k X9[m, k] Wt[n, k],
 // k = tap * C + c, tap = (dy + 1) * 3 + (dx + 1), X9[m, k] = X[pixel m shifted
 // by (dy, dx), channel c].  Wt is [Nout][Kp] BF16 with Kp = roundup(9 C, 64).
-// Epilogue: + bias, ReLU, multiply by (mask view > 0), store BF16 or FP32.
-struct ConvOp {
+struct ConvOp : ConvStore {
     static constexpr bool A_MN = false, B_MN = false;
     ActView x;
     const __nv_bfloat16 *wt;  // [Nout][Kp]
-    const float *bias;        // [Nout] or null
-    ActView mask;             // mask.s1 == null: no mask
-    void *out;                // [M][Nout] BF16 or FP32
-    int M, Nout, Kp, bn, relu, out_f32, nsteps;
+    int Kp, nsteps;
 
     __device__ void k_range(const uint3 &t, int &k0, int &k1) const { k0 = 0; k1 = nsteps; }
 
@@ -517,38 +554,6 @@ struct ConvOp {
             kc += dk;
             r += dr;
             if (r >= bn) { r -= bn; ++kc; }
-        }
-    }
-
-    __device__ void store(int row, int col, const float *v, const uint3 &t) const {
-        const int m = t.x * BM + row;
-        if (m >= M) return;
-        const int n = t.y * bn + col;
-        float o[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            float t = v[i] + (bias ? bias[n + i] : 0.f);
-            o[i] = relu ? fmaxf(t, 0.f) : t;
-        }
-        if (mask.s1) {
-            int b, h, w;
-            pixel_of(m, mask.H, mask.W, b, h, w);
-            const uint4 mv = mask.chunk(b, h, w, n);
-            const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&mv);
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-                if (!(__bfloat162float(mb[i]) > 0.f)) o[i] = 0.f;
-        }
-        if (out_f32) {
-            float4 *d = reinterpret_cast<float4 *>((float *)out + (size_t)m * Nout + n);
-            d[0] = make_float4(o[0], o[1], o[2], o[3]);
-            d[1] = make_float4(o[4], o[5], o[6], o[7]);
-        } else {
-            __align__(16) __nv_bfloat162 p[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) p[i] = __floats2bfloat162_rn(o[2 * i], o[2 * i + 1]);
-            *reinterpret_cast<uint4 *>((__nv_bfloat16 *)out + (size_t)m * Nout + n) =
-                *reinterpret_cast<const uint4 *>(p);
         }
     }
 };
@@ -683,9 +688,10 @@ int pick_bn(int n);
 // Launch umma_k<Op> with the dynamic shared memory it needs.  The attribute
 // is set once per device and instantiation.
 // Engine choice for the convolutions and the plain GEMM: 0 the warp-
-// specialised persistent kernel, 1 one CTA per tile (default: with cp.async
-// operand staging the persistent kernel's four producer warps are
-// instruction-bound, and two independent CTAs per SM load faster).
+// specialised persistent kernel with cp.async staging, 1 one CTA per tile
+// with cp.async staging, 2 (default) the TMA-staged persistent kernel of
+// kb_umma_tma.cuh.  Under engine 2 an operation whose shapes the TMA boxes
+// cannot tile runs on engine 1 (launch() below).
 int engine();
 
 template <class Op>
@@ -708,7 +714,7 @@ int launch_ws(const Op &op, dim3 grid, int *err, cudaStream_t stream, long long 
 
 template <class Op>
 int launch(const Op &op, dim3 grid, int *err, cudaStream_t stream, long long spin = 1ll << 22) {
-    if (engine() == 0) return launch_ws(op, grid, err, stream, spin);
+    if (engine() == 0) return launch_ws(op, grid, err, stream, spin);  // 1 and 2: one CTA per tile
     static bool configured[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);

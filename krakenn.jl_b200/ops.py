@@ -742,7 +742,9 @@ def set_trt3d_variant(variant: int):
 
 def set_umma_engine(engine: int):
     """Tensor-core engine of the warm-start network and kb_gemm_bf16: 0 the
-    warp-specialised persistent kernel, 1 one CTA per output tile (default)."""
+    warp-specialised persistent kernel with cp.async staging, 1 one CTA per
+    output tile with cp.async staging, 2 (default) the persistent kernel with
+    TMA staging into swizzled layouts (shapes it cannot tile run on 1)."""
     call("kb_set_kernel_variant", 2, int(engine))
 
 
