@@ -21,6 +21,7 @@
 // c, tap = (dy+1)*3 + (dx+1)) followed by b[cout].  Adam keeps FP32 moments;
 // the BF16 operand copies (forward and transposed-flipped) are repacked after
 // every update.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -327,14 +328,18 @@ struct Layer {
 
 // The TMA engine's operations of one layer for a batch of n images (the maps
 // bound the image index by n, so images beyond the batch read as zeros).
-// f / d / w: the forward, data-gradient and weight-gradient shapes tile into
-// TMA boxes (otherwise that operation runs on the one-CTA-per-tile engine).
+// f / d / w: how the forward, data-gradient and weight-gradient operations
+// run -- row strips where rows are wide enough and one output-channel tile
+// holds the layer, else per-tap boxes where the shapes tile into boxes, else
+// the one-CTA-per-tile engine.
 struct TmaPlan {
     int n = -1;
-    bool f = false, d = false, w = false;
+    int f = 0, d = 0, w = 0;  // 0: per-tile engine, 1: TMA per-tap boxes, 2: TMA row strips
     int wsplits = 0;
     kb::umma::ConvTma fwd, dgr;
+    kb::umma::ConvStrip sfwd, sdgr;
     kb::umma::WgradTma wg;
+    kb::umma::WgradStrip swg;
 };
 
 }  // namespace sur
@@ -358,7 +363,7 @@ struct kb_surrogate {
     Norm norm{{1.f, 1.f, 1.f}, {0.f, 0.f, 0.f}};
     float grad_weight = 0.f;  // weight of the gradient (H1) term of the loss
     std::vector<TmaPlan> tp;            // per layer, TMA engine
-    bf16 *ones = nullptr;               // [64][64] BF16, column 0 = 1: the bias row's A block
+    bf16 *ones = nullptr;               // [72][64] BF16, column 0 = 1: the bias row's A block
     int up_batch = -1;                  // batch of the decoder inputs last upsampled
     std::vector<void *> allocs;
     int H_at(int level) const { return H >> level; }
@@ -414,6 +419,65 @@ void upsample(kb_surrogate *s, const Layer &l, int n, cudaStream_t st) {
                                                                               W, l.cin1);
 }
 
+// Row-strip weight gradient of a layer: TMEM columns of its accumulators
+// (all taps, all channel chunks and the bias row of one output tile), or 0
+// when the layer does not take that form.
+uint32_t strip_wgrad_cols(const Layer &l, int W) {
+    using namespace kb::umma;
+    const int ea = chunk_of(l.cin1, l.cin2), bn = l.bn_w;
+    if (!ea || !chunk_of(bn) || W % BK || l.cout != bn || (bn & (bn - 1))) return 0;
+    const int nmt = 3 * (l.cin / ea) * (ea == 64 ? 2 : 1);
+    const uint32_t need = (uint32_t)((nmt + 1) * bn);
+    uint32_t cols = 32;
+    while (cols < need) cols <<= 1;
+    return cols <= 512 ? cols : 0;
+}
+
+// Row-strip convolution (forward or data gradient): input channels c1 + c2
+// in chunks of e, weights [Nout][Kp] resident, Nout one tile of bn.
+int conv_strip(kb::umma::ConvStrip &c, const bf16 *x1, int c1, const bf16 *x2, int c2, const bf16 *wmat,
+               int Kp, int bn, int e, int H, int W, int n, const char *what) {
+    using namespace kb::umma;
+    int rc;
+    const PixBox strip{BM + 2, 1, 1};
+    if ((rc = nhwc_map(&c.x1, x1, c1, W, H, n, e, strip, what))) return rc;
+    if (x2 && (rc = nhwc_map(&c.x2, x2, c2, W, H, n, e, strip, what))) return rc;
+    if (!x2) c.x2 = c.x1;
+    const cuuint64_t d[2] = {(cuuint64_t)Kp, (cuuint64_t)bn}, sd[1] = {(cuuint64_t)Kp * 2};
+    const cuuint32_t bx[2] = {(cuuint32_t)e, (cuuint32_t)bn};
+    if ((rc = bf16_map(&c.w, wmat, 2, d, sd, bx, 2 * e, what))) return rc;
+    const int C = c1 + c2;
+    c.e = e;
+    c.c1 = c1;
+    c.C = C;
+    c.H = H;
+    c.W = W;
+    c.nck = C / e;
+    c.strip_bytes = round1k((uint32_t)((BM + 2) * 2 * e));
+    c.tx = (uint32_t)(c.nck * (BM + 2) * 2 * e);
+    c.a_bytes = (uint32_t)c.nck * c.strip_bytes;
+    c.b_bytes = 0;
+    c.res_bytes = (uint32_t)(9 * c.nck * bn * 2 * e);
+    c.acc_cols = tmem_cols(bn);
+    c.nbuf = 2;
+    c.ncols = bn;
+    c.cps = tma_fit(c);
+    return c.cps ? 0 : kb::set_error(KB_ERR_ARG, "%s: row-strip convolution does not fit", what);
+}
+
+// Whether a row-strip convolution of these shapes fits the engine.
+bool conv_strip_fits(int C, int e, int bn, int W) {
+    using namespace kb::umma;
+    if (!e || W % BM) return false;
+    TmaBase b{};
+    const int nck = C / e;
+    b.a_bytes = (uint32_t)nck * round1k((uint32_t)((BM + 2) * 2 * e));
+    b.res_bytes = (uint32_t)(9 * nck * bn * 2 * e);
+    b.acc_cols = tmem_cols(bn);
+    b.nbuf = 2;
+    return tma_fit(b) > 0;
+}
+
 // Build (or keep) the TMA engine's operations of layer i for n images.
 int prepare_tma(kb_surrogate *s, int i, int n) {
     using namespace kb::umma;
@@ -421,7 +485,7 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
     TmaPlan &p = s->tp[i];
     if (p.n == n) return 0;
     p.n = -1;
-    p.f = p.d = p.w = false;
+    p.f = p.d = p.w = 0;
     const char *what = "kb_surrogate (TMA engine)";
     const int H = s->H_at(l.level), W = s->W_at(l.level), M = n * H * W;
     const bf16 *x1 = l.in2 >= 0 ? l.up : s->act[l.in1];
@@ -429,9 +493,22 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
     PixBox b128{}, b64{};
     const bool g128 = pix_box(BM, H, W, b128), g64 = pix_box(BK, H, W, b64);
     int rc = 0;
-    // forward: boxes of e input channels x 128 pixels, weights e x bn_f
+    // forward: row strips, or boxes of e input channels x 128 pixels (weights e x bn_f)
     const int ef = chunk_of(l.cin1, l.cin2);
-    if (ef && g128) {
+    if (ef && l.cout == l.bn_f && conv_strip_fits(l.cin, ef, l.bn_f, W)) {
+        ConvStrip &c = p.sfwd;
+        c = ConvStrip{};
+        if ((rc = conv_strip(c, x1, l.cin1, x2, l.cin2, l.wb, l.Kp, l.bn_f, ef, H, W, n, what))) return rc;
+        c.bias = s->params + l.b_off;
+        c.mask.s1 = nullptr;
+        c.out = l.out == T_OUT ? (void *)s->out_f32 : (void *)s->act[l.out];
+        c.M = M;
+        c.Nout = l.cout;
+        c.bn = l.bn_f;
+        c.relu = l.relu;
+        c.out_f32 = l.out == T_OUT;
+        p.f = 2;
+    } else if (ef && g128) {
         ConvTma &c = p.fwd;
         c = ConvTma{};
         if ((rc = nhwc_map(&c.x1, x1, l.cin1, W, H, n, ef, b128, what))) return rc;
@@ -448,6 +525,11 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
         c.nck = l.cin / ef;
         c.a_bytes = round1k((uint32_t)(BM * 2 * ef));
         c.b_bytes = round1k((uint32_t)(l.bn_f * 2 * ef));
+        c.res_bytes = 0;
+        c.acc_cols = tmem_cols(l.bn_f);
+        c.nbuf = 2;
+        c.ncols = l.bn_f;
+        c.cps = tma_fit(c);
         c.tx = (uint32_t)(BM * 2 * ef + l.bn_f * 2 * ef);
         c.bias = s->params + l.b_off;
         c.mask.s1 = nullptr;
@@ -457,11 +539,27 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
         c.bn = l.bn_f;
         c.relu = l.relu;
         c.out_f32 = l.out == T_OUT;
-        p.f = true;
+        p.f = c.cps ? 1 : 0;
     }
-    // data gradient: boxes of e output-gradient channels, weights wt [cin][Kpt]
+    // data gradient: row strips, or boxes of e output-gradient channels
+    // (weights wt [cin][Kpt])
     const int ed = chunk_of(l.cout);
-    if (i > 0 && ed && g128) {
+    if (i > 0 && ed && l.cin == l.bn_d && conv_strip_fits(l.cout, ed, l.bn_d, W)) {
+        ConvStrip &c = p.sdgr;
+        c = ConvStrip{};
+        if ((rc = conv_strip(c, s->grad[l.out], l.cout, nullptr, 0, l.wt, l.Kpt, l.bn_d, ed, H, W, n, what)))
+            return rc;
+        c.bias = nullptr;
+        if (l.pooled_in) c.mask.s1 = nullptr;
+        else c.mask = view_of(s, l, n);
+        c.out = l.dx;
+        c.M = M;
+        c.Nout = l.cin;
+        c.bn = l.bn_d;
+        c.relu = 0;
+        c.out_f32 = 0;
+        p.d = 2;
+    } else if (i > 0 && ed && g128) {
         ConvTma &c = p.dgr;
         c = ConvTma{};
         if ((rc = nhwc_map(&c.x1, s->grad[l.out], l.cout, W, H, n, ed, b128, what))) return rc;
@@ -477,6 +575,11 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
         c.nck = l.cout / ed;
         c.a_bytes = round1k((uint32_t)(BM * 2 * ed));
         c.b_bytes = round1k((uint32_t)(l.bn_d * 2 * ed));
+        c.res_bytes = 0;
+        c.acc_cols = tmem_cols(l.bn_d);
+        c.nbuf = 2;
+        c.ncols = l.bn_d;
+        c.cps = tma_fit(c);
         c.tx = (uint32_t)(BM * 2 * ed + l.bn_d * 2 * ed);
         c.bias = nullptr;
         if (l.pooled_in) c.mask.s1 = nullptr;
@@ -487,12 +590,65 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
         c.bn = l.bn_d;
         c.relu = 0;
         c.out_f32 = 0;
-        p.d = true;
+        p.d = c.cps ? 1 : 0;
     }
-    // weight gradient: blocks of ea input channels / eb output-gradient
-    // channels x 64 pixels
+    // weight gradient: row strips (whole gradient per pixel split), or blocks
+    // of ea input channels / eb output-gradient channels x 64 pixels
     const int ea = chunk_of(l.cin1, l.cin2), eb = chunk_of(l.bn_w);
-    if (ea && eb && g64) {
+    const uint32_t wcols = strip_wgrad_cols(l, W);
+    const int sr = BK + (BM / (ea ? ea : 64) - 1 > 3 ? BM / ea - 1 : 3);  // strip rows
+    const uint32_t wstrip = ea ? round1k((uint32_t)(sr * 2 * ea)) : 0;
+    const uint32_t wstage = 3u * (uint32_t)(l.cin / (ea ? ea : 1)) * wstrip + round1k((uint32_t)(l.bn_w * BK * 2));
+    TmaBase wb{};
+    wb.a_bytes = wstage;
+    wb.res_bytes = (uint32_t)(72 * 2 * ea);
+    wb.acc_cols = wcols;
+    wb.nbuf = 1;
+    const int wcps = wcols ? tma_fit(wb) : 0;
+    if (wcps) {
+        WgradStrip &w = p.swg;
+        w = WgradStrip{};
+        const PixBox strip{sr, 1, 1};
+        if ((rc = nhwc_map(&w.x1, x1, l.cin1, W, H, n, ea, strip, what))) return rc;
+        if (x2 && (rc = nhwc_map(&w.x2, x2, l.cin2, W, H, n, ea, strip, what))) return rc;
+        if (!x2) w.x2 = w.x1;
+        const cuuint64_t d[2] = {(cuuint64_t)ea, 72}, sd[1] = {128};
+        const cuuint32_t bx[2] = {(cuuint32_t)ea, 72};
+        if ((rc = bf16_map(&w.ones, s->ones, 2, d, sd, bx, 2 * ea, what))) return rc;
+        if ((rc = nhwc_map(&w.dy, s->grad[l.out], l.cout, W, H, n, eb, b64, what))) return rc;
+        const int nsteps = (M + BK - 1) / BK;
+        int want = kb::sm_count() * wcps;  // one pixel split per CTA
+        if (want > nsteps) want = nsteps;
+        const int sps = (nsteps + want - 1) / want;
+        p.wsplits = (nsteps + sps - 1) / sps;
+        w.part = s->part;
+        w.bn = l.bn_w;
+        w.ea = ea;
+        w.eb = eb;
+        w.c1 = l.cin1;
+        w.C = l.cin;
+        w.H = H;
+        w.W = W;
+        w.Nout = l.cout;
+        w.steps_per_split = sps;
+        w.nsteps = nsteps;
+        w.nck = l.cin / ea;
+        w.mtp = ea == 64 ? 2 : 1;
+        w.nb = l.bn_w / eb;
+        w.nmt = 3 * w.nck * w.mtp;
+        w.ea_shift = ea == 64 ? 6 : (ea == 32 ? 5 : 4);
+        w.bn_shift = 31 - __builtin_clz((unsigned)l.bn_w);
+        w.strip_bytes = wstrip;
+        w.tx = (uint32_t)(3 * w.nck * sr * 2 * ea + l.bn_w * BK * 2);
+        w.a_bytes = 3u * (uint32_t)w.nck * wstrip;
+        w.b_bytes = round1k((uint32_t)(l.bn_w * BK * 2));
+        w.res_bytes = (uint32_t)(72 * 2 * ea);
+        w.acc_cols = wcols;
+        w.nbuf = 1;  // one tile per CTA: nothing to overlap the epilogue with
+        w.ncols = (w.nmt + 1) * l.bn_w;
+        w.cps = wcps;
+        p.w = 2;
+    } else if (ea && eb && g64) {
         WgradTma &w = p.wg;
         w = WgradTma{};
         if ((rc = nhwc_map(&w.x1, x1, l.cin1, W, H, n, ea, b64, what))) return rc;
@@ -521,7 +677,12 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
         w.nb = l.bn_w / eb;
         w.a_bytes = BM * BK * 2;
         w.b_bytes = round1k((uint32_t)(l.bn_w * BK * 2));
-        p.w = true;
+        w.res_bytes = 0;
+        w.acc_cols = tmem_cols(l.bn_w);
+        w.nbuf = 2;
+        w.ncols = l.bn_w;
+        w.cps = tma_fit(w);
+        p.w = w.cps ? 1 : 0;
     }
     p.n = n;
     return 0;
@@ -545,8 +706,11 @@ int forward(kb_surrogate *s, const void *input, int n, cudaStream_t st) {
         if (tma) {
             if (l.in2 >= 0) upsample(s, l, n, st);
             if (int rc = prepare_tma(s, i, n)) return rc;
-            if (s->tp[i].f) {
-                if (int rc = launch_tma(s->tp[i].fwd, grid, s->err, st)) return rc;
+            const TmaPlan &tp = s->tp[i];
+            if (tp.f) {
+                if (int rc = tp.f == 2 ? launch_tma(tp.sfwd, grid, s->err, st)
+                                       : launch_tma(tp.fwd, grid, s->err, st))
+                    return rc;
                 continue;
             }
         }
@@ -590,7 +754,10 @@ int backward(kb_surrogate *s, int n, cudaStream_t st) {
         // weight gradient (split over pixels) and its reduction
         int sps = 0;
         int splits = wgrad_splits(l, M, sps);
-        if (tma && tp.w) {
+        if (tma && tp.w == 2) {
+            splits = tp.wsplits;
+            if (int rc = launch_tma(tp.swg, dim3(1, 1, splits), s->err, st)) return rc;
+        } else if (tma && tp.w == 1) {
             splits = tp.wsplits;
             const dim3 wg((R + 1 + BM - 1) / BM, l.cout / l.bn_w, splits);
             if (int rc = launch_tma(tp.wg, wg, s->err, st)) return rc;
@@ -613,7 +780,8 @@ int backward(kb_surrogate *s, int n, cudaStream_t st) {
         // data gradient
         const dim3 grid((M + BM - 1) / BM, l.cin / l.bn_d);
         if (tma && tp.d) {
-            if (int rc = launch_tma(tp.dgr, grid, s->err, st)) return rc;
+            if (int rc = tp.d == 2 ? launch_tma(tp.sdgr, grid, s->err, st) : launch_tma(tp.dgr, grid, s->err, st))
+                return rc;
         } else {
             ConvOp op{};
             op.x.s1 = s->grad[l.out];
@@ -749,7 +917,9 @@ int kb_surrogate_create(kb_surrogate **out, int max_batch, int H, int W, int bas
             else l.dx = s->grad[l.in1];
         }
         if (l.in2 >= 0) A((void **)&l.up, px * l.cin1 * sizeof(bf16));
-        const size_t need = (size_t)max_wgrad_splits(l) * (9 * l.cin + 1) * l.cout;
+        size_t need = (size_t)max_wgrad_splits(l) * (9 * l.cin + 1) * l.cout;
+        if (strip_wgrad_cols(l, W >> l.level))
+            need = std::max(need, (size_t)kb::sm_count() * kb::umma::TM_MAX_CPS * (9 * l.cin + 1) * l.cout);
         if (need > part) part = need;
     }
     s->part_floats = part;
@@ -760,7 +930,7 @@ int kb_surrogate_create(kb_surrogate **out, int max_batch, int H, int W, int bas
     A((void **)&s->adam_v, (size_t)s->n_params * sizeof(float));
     A((void **)&s->err, sizeof(int));
     A((void **)&s->loss, sizeof(float));
-    A((void **)&s->ones, 64 * 64 * sizeof(bf16));
+    A((void **)&s->ones, 72 * 64 * sizeof(bf16));
     s->tp.resize(N_LAYERS);
     if (rc) {
         for (void *p : s->allocs) cudaFree(p);
@@ -781,8 +951,8 @@ int kb_surrogate_create(kb_surrogate **out, int max_batch, int H, int W, int bas
     }
     cudaMemcpyAsync(s->params, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, st);
     static const std::vector<unsigned short> ones = [] {
-        std::vector<unsigned short> o(64 * 64, 0);
-        for (int k = 0; k < 64; ++k) o[k * 64] = 0x3F80u;  // BF16 1.0
+        std::vector<unsigned short> o(72 * 64, 0);
+        for (int k = 0; k < 72; ++k) o[k * 64] = 0x3F80u;  // BF16 1.0
         return o;
     }();
     cudaMemcpyAsync(s->ones, ones.data(), ones.size() * sizeof(unsigned short), cudaMemcpyHostToDevice, st);

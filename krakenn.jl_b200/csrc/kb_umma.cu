@@ -104,6 +104,11 @@ extern "C" int kb_gemm_bf16(const void *A, const void *B, float *C, int M, int N
             op.nb = bn / eb;
             op.a_bytes = ab;
             op.b_bytes = bb;
+            op.res_bytes = 0;
+            op.acc_cols = tmem_cols(bn);
+            op.nbuf = 2;
+            op.ncols = bn;
+            op.cps = tma_fit(op);
             return launch_tma(op, grid, err_device, st);
         };
         if (!a_mn && !b_mn) rc = go(GemmTma<false, false>{});

@@ -1,8 +1,12 @@
 // kb_umma_tma.cuh -- TMA-staged, warp-specialised tcgen05 engine (engine 2)
 // of the warm-start network's convolutions and of the plain BF16 GEMM.
 //
-// One persistent CTA per SM (64 + 128 TM_EPI threads) loops over the tiles
-// t = blockIdx.x, blockIdx.x + gridDim.x, ... of the grid `tiles` (x fastest):
+// cps persistent CTAs per SM (64 + 128 TM_EPI threads each) loop over the
+// tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... of the grid `tiles` (x
+// fastest).  One warp issues at most one tcgen05.mma about every 180 cycles
+// whatever N is, so an N = 32 tile reaches 1/8 of the tensor rate from one
+// issuer; several CTAs per SM, each with its own ring, MMA lane and share of
+// TMEM, multiply the issue rate.  In each CTA:
 //   warp 0    producer: lane 0 waits for a free ring stage (`empty`), posts
 //             the stage's byte count on its `full` barrier and issues the
 //             step's cp.async.bulk.tensor copies, one per operand box;
@@ -47,9 +51,14 @@
 namespace kb {
 namespace umma {
 
-constexpr int TM_EPI = 4;                       // epilogue warps per TMEM lane quarter
-constexpr int TM_THREADS = 64 + 128 * TM_EPI, TM_MAX_STAGES = 24;
-constexpr uint32_t TM_RING = 200u * 1024u;  // bytes of the operand ring
+constexpr int TM_EPI = 2;                       // epilogue warps per TMEM lane quarter
+constexpr int TM_THREADS = 64 + 128 * TM_EPI, TM_MAX_STAGES = 24, TM_MAX_CPS = 4;
+constexpr uint32_t TM_RING = 200u * 1024u;  // bytes of ring + resident operand, one CTA per SM
+// ... and with cps CTAs per SM (each CTA also takes barriers, alignment slack
+// and the 1 KB the runtime reserves)
+__host__ __device__ constexpr uint32_t tm_ring(int cps) {
+    return cps <= 1 ? TM_RING : (cps == 2 ? 108u * 1024u : (cps == 3 ? 72u * 1024u : 52u * 1024u));
+}
 
 // Shared-memory matrix descriptor of a swizzled layout (sm_100 version 1).
 __device__ __forceinline__ uint64_t sdesc_sw(uint32_t saddr, uint32_t lbo, uint32_t sbo, uint32_t swz) {
@@ -118,35 +127,49 @@ struct TileCursor {
     }
 };
 
-// Op interface (in addition to bn, k_range and store of the other engines):
+// Fields every operation carries (set on the host).
+struct TmaBase {
+    uint32_t a_bytes, b_bytes;  // operand bytes of one ring stage (multiples of 1024)
+    uint32_t res_bytes;         // operand bytes copied once per CTA and kept (0: none)
+    uint32_t acc_cols;          // TMEM columns of one accumulator (32..512, a power of two)
+    int nbuf;                   // accumulators: 2 (epilogue of tile j overlaps tile j+1) or 1
+    int ncols;                  // accumulator columns the epilogue stores (multiple of 8)
+    int cps;                    // CTAs per SM (tma_fit)
+};
+
+// Op interface (TmaBase plus bn, k_range and store as in the other engines):
 //   static constexpr bool A_MN, B_MN;
-//   uint32_t a_bytes, b_bytes                      stage bytes (multiples of 1024)
 //   __device__ uint32_t step_tx(const uint3 &t)    bytes the copies of one step of tile t bring
 //   __device__ void prefetch()                     prefetch the tensor maps
+//   __device__ void issue_res(uint32_t res, uint32_t bar)   copies of the resident operand
 //   struct Cursor; __device__ Cursor begin(const uint3 &t, int k0)   state of step k0 of tile t
 //   __device__ void issue(Cursor &c, const uint3 &t, uint32_t sa, uint32_t sb, uint32_t bar)
 //                                                  copies of the cursor's step; advance it
-//   __device__ void mma(uint32_t acc, uint32_t sa, uint32_t sb, bool first, uint32_t idesc)
+//   __device__ void mma(uint32_t acc, uint32_t sa, uint32_t sb, uint32_t res, int kt, int k0,
+//                       const uint3 &t, uint32_t idesc)   the MMAs of step kt of tile t
 template <class Op>
-__global__ void __launch_bounds__(TM_THREADS, 1)
+__global__ void __launch_bounds__(TM_THREADS, TM_MAX_CPS)
     umma_tma_k(const __grid_constant__ Op op, const uint3 tiles, const int nstages,
                int *__restrict__ err, const long long spin) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     const uint32_t stage_bytes = op.a_bytes + op.b_bytes;
-    uint64_t *full =
-        reinterpret_cast<uint64_t *>(smem_raw + (base - raw) + (size_t)nstages * stage_bytes);
+    const uint32_t res = base + (uint32_t)nstages * stage_bytes;  // resident operand
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + (base - raw) + (size_t)nstages * stage_bytes +
+                                                  op.res_bytes);
     uint64_t *empty = full + nstages;
     uint64_t *acc_full = empty + nstages, *acc_empty = acc_full + 2, *drain = acc_empty + 2;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    uint64_t *resbar = drain + 1;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(resbar + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t cols = tmem_cols(op.bn);  // per accumulator; two of them
+    const uint32_t cols = op.acc_cols;
+    const int nbuf = op.nbuf;
     const int ntiles = (int)(tiles.x * tiles.y * tiles.z);  // < 2^31 (checked by launch_tma)
 
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     ::"r"(smem_u32(tmem_slot)), "r"(2 * cols));
+                     ::"r"(smem_u32(tmem_slot)), "r"((uint32_t)nbuf * cols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (threadIdx.x == 0) {
@@ -159,6 +182,7 @@ __global__ void __launch_bounds__(TM_THREADS, 1)
             mbar_init(&acc_empty[i], 128 * TM_EPI);
         }
         mbar_init(drain, 1);
+        mbar_init(resbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -174,6 +198,10 @@ __global__ void __launch_bounds__(TM_THREADS, 1)
         // ---------------------------------------------------------- producer
         if (lane == 0) {
             op.prefetch();
+            if (op.res_bytes) {
+                expect_tx(smem_u32(resbar), op.res_bytes);
+                op.issue_res(res, smem_u32(resbar));
+            }
             long long g = 0;
             int s = 0;
             uint32_t par = 0;
@@ -206,6 +234,7 @@ __global__ void __launch_bounds__(TM_THREADS, 1)
                 --s;
                 if (!mbar_wait(&full[s], par, spin)) ok = false;
             }
+            if (op.res_bytes && !mbar_wait(resbar, 0u, spin)) ok = false;
         }
         __syncwarp();
     } else if (warp == 1) {
@@ -214,11 +243,11 @@ __global__ void __launch_bounds__(TM_THREADS, 1)
             const uint32_t idesc = idesc_bf16(op.bn, Op::A_MN, Op::B_MN);
             int s = 0, j = 0;
             uint32_t par = 0;
+            if (op.res_bytes) ok = mbar_wait(resbar, 0u, spin);
             TileCursor tc(tiles);
             for (int T = blockIdx.x; T < ntiles && ok; T += gridDim.x, ++j) {
-                const int buf = j & 1;
-                if (j >= 2 && !(ok = mbar_wait(&acc_empty[buf], (uint32_t)(((j >> 1) - 1) & 1), spin)))
-                    break;
+                const int buf = nbuf == 2 ? (j & 1) : 0, use = nbuf == 2 ? (j >> 1) : j;
+                if (use >= 1 && !(ok = mbar_wait(&acc_empty[buf], (uint32_t)((use - 1) & 1), spin))) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint3 t = tc.at(T);
                 int k0, k1;
@@ -228,7 +257,7 @@ __global__ void __launch_bounds__(TM_THREADS, 1)
                     if (!(ok = mbar_wait(&full[s], par, spin))) break;
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const uint32_t sa = base + (uint32_t)s * stage_bytes;
-                    op.mma(acc, sa, sa + op.a_bytes, kt == k0, idesc);
+                    op.mma(acc, sa, sa + op.a_bytes, res, kt, k0, t, idesc);
                     mma_commit(&empty[s]);
                     if (++s == nstages) {
                         s = 0;
@@ -250,21 +279,21 @@ __global__ void __launch_bounds__(TM_THREADS, 1)
         int j = 0;
         TileCursor tc(tiles);
         for (int T = blockIdx.x; T < ntiles && ok; T += gridDim.x, ++j) {
-            const int buf = j & 1;
-            if (!(ok = mbar_wait(&acc_full[buf], (uint32_t)((j >> 1) & 1), spin))) break;
+            const int buf = nbuf == 2 ? (j & 1) : 0, use = nbuf == 2 ? (j >> 1) : j;
+            if (!(ok = mbar_wait(&acc_full[buf], (uint32_t)(use & 1), spin))) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint3 t = tc.at(T);
             int k0, k1;
             op.k_range(t, k0, k1);
             if (k1 > k0) {
-                for (int c0 = grp * 8; c0 < op.bn; c0 += 8 * TM_EPI) {
+                for (int c0 = grp * 8; c0 < op.ncols; c0 += 8 * TM_EPI) {
                     float v[8];
                     tmem_ld8(tmem + (uint32_t)buf * cols + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
                     op.store(row, c0, v, t);
                 }
             } else {
                 const float z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-                for (int c0 = grp * 8; c0 < op.bn; c0 += 8 * TM_EPI) op.store(row, c0, z, t);
+                for (int c0 = grp * 8; c0 < op.ncols; c0 += 8 * TM_EPI) op.store(row, c0, z, t);
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             mbar_arrive(&acc_empty[buf]);
@@ -274,19 +303,31 @@ __global__ void __launch_bounds__(TM_THREADS, 1)
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 1)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * cols));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"((uint32_t)nbuf * cols));
 }
 
-// Ring stages that fit TM_RING for a stage of `stage_bytes`, and the dynamic
-// shared memory of a launch with that many stages.
-inline int tma_stages(uint32_t stage_bytes) {
-    const int n = (int)(TM_RING / stage_bytes);
+// Ring stages that fit beside a resident operand of `res_bytes` with cps
+// CTAs per SM, and the dynamic shared memory of a launch with that many stages.
+inline int tma_stages(uint32_t stage_bytes, uint32_t res_bytes, int cps = 1) {
+    const uint32_t ring = tm_ring(cps);
+    if (res_bytes >= ring) return 0;
+    const int n = (int)((ring - res_bytes) / stage_bytes);
     return n > TM_MAX_STAGES ? TM_MAX_STAGES : n;
 }
-inline size_t tma_smem_bytes(int nstages, uint32_t stage_bytes) {
-    return 1024 + (size_t)nstages * stage_bytes + (size_t)(2 * nstages + 5) * 8 + 16;
+inline size_t tma_smem_bytes(int nstages, uint32_t stage_bytes, uint32_t res_bytes) {
+    return 1024 + (size_t)nstages * stage_bytes + res_bytes + (size_t)(2 * nstages + 6) * 8 + 16;
 }
-constexpr size_t TM_SMEM_MAX = 1024 + TM_RING + (2 * TM_MAX_STAGES + 5) * 8 + 16;
+// Most CTAs per SM (<= TM_MAX_CPS) whose rings hold >= 2 stages and whose
+// accumulators fit TMEM together; 0 if not even one CTA fits.
+inline int tma_fit(const TmaBase &b) {
+    for (int c = TM_MAX_CPS; c >= 1; --c)
+        if (tma_stages(b.a_bytes + b.b_bytes, b.res_bytes, c) >= 2 &&
+            (uint32_t)c * (uint32_t)b.nbuf * b.acc_cols <= 512u && c * TM_THREADS <= 2048)
+            return c;
+    return 0;
+}
+constexpr size_t TM_SMEM_MAX = 1024 + TM_RING + (2 * TM_MAX_STAGES + 6) * 8 + 16;
 
 // ---------------------------------------------------------------------------
 // Operations.
@@ -304,12 +345,11 @@ __device__ __forceinline__ void split_pixel(int p, int H, int W, int &b, int &y,
 // X is channels [0, c1) of x1 and [c1, C) of x2 (both NHWC at H x W); a step
 // is one tap and one chunk of e channels (box e x 128 pixels), K-major with
 // swizzle 2e; the weights [Nout][Kp] are boxes of e K elements x bn rows.
-struct ConvTma : ConvStore {
+struct ConvTma : ConvStore, TmaBase {
     static constexpr bool A_MN = false, B_MN = false;
     CUtensorMap x1, x2, w;
     int e, c1, C, H, W, nck;
-    uint32_t a_bytes, b_bytes, tx;
-
+    uint32_t tx;
 
     __device__ void k_range(const uint3 &, int &k0, int &k1) const { k0 = 0; k1 = 9 * nck; }
     __device__ uint32_t step_tx(const uint3 &) const { return tx; }
@@ -344,11 +384,164 @@ struct ConvTma : ConvStore {
             }
         }
     }
-    __device__ void mma(uint32_t acc, uint32_t sa, uint32_t sb, bool first, uint32_t idesc) const {
+    __device__ void issue_res(uint32_t, uint32_t) const {}
+    __device__ void mma(uint32_t acc, uint32_t sa, uint32_t sb, uint32_t, int kt, int k0, const uint3 &,
+                        uint32_t idesc) const {
+        const bool first = kt == k0;
         const uint32_t s = 2u * (uint32_t)e;
         for (int kk = 0; kk < e / 16; ++kk)
             mma_bf16(acc, op_desc(sa, false, s, kk), op_desc(sb, false, s, kk), idesc,
                      (first && kk == 0) ? 0u : 1u);
+    }
+};
+
+// Convolution (forward or data gradient) of rows that are a multiple of 128
+// pixels wide, by row strips: a tile is 128 pixels of one row, a step is one
+// kernel row dy.  The step's copies are one strip per channel chunk, pixels
+// x0-1 .. x0+128 of row y+dy (box e x 130, K-major, swizzle 2e), so an
+// activation row crosses to shared memory three times instead of nine.  The
+// MMAs of tap dx read the strip from row dx+1 on: the tensor core applies the
+// swizzle to the absolute shared-memory address, so a start 2e bytes further
+// reads the rows shifted by one pixel.  The layer's weights (9 nck blocks of
+// bn x e, one output-channel tile) are the resident operand.  MMA order (tap,
+// chunk, 16-wide K group) is the order of the other engines.
+struct ConvStrip : ConvStore, TmaBase {
+    static constexpr bool A_MN = false, B_MN = false;
+    CUtensorMap x1, x2, w;
+    int e, c1, C, H, W, nck;
+    uint32_t strip_bytes, tx;
+
+    __device__ void k_range(const uint3 &, int &k0, int &k1) const { k0 = 0; k1 = 3; }
+    __device__ uint32_t step_tx(const uint3 &) const { return tx; }
+    __device__ void prefetch() const {
+        prefetch_map(&x1);
+        if (c1 < C) prefetch_map(&x2);
+        prefetch_map(&w);
+    }
+    __device__ void issue_res(uint32_t res, uint32_t bar) const {
+        const uint32_t blk = (uint32_t)(bn * 2 * e);
+        for (int j = 0, wk = 0; j < 9 * nck; ++j, wk += e) tma2(res + (uint32_t)j * blk, &w, wk, 0, bar);
+    }
+    struct Cursor { int dy, b, y, x; };
+    __device__ Cursor begin(const uint3 &t, int) const {
+        Cursor u;
+        split_pixel((int)t.x * BM, H, W, u.b, u.y, u.x);
+        u.dy = -1;
+        return u;
+    }
+    __device__ void issue(Cursor &u, const uint3 &, uint32_t sa, uint32_t, uint32_t bar) const {
+        uint32_t dst = sa;
+        for (int ci = 0, c = 0; ci < nck; ++ci, c += e, dst += strip_bytes) {
+            if (c < c1) tma4(dst, &x1, c, u.x - 1, u.y + u.dy, u.b, bar);
+            else tma4(dst, &x2, c - c1, u.x - 1, u.y + u.dy, u.b, bar);
+        }
+        ++u.dy;
+    }
+    __device__ void mma(uint32_t acc, uint32_t sa, uint32_t, uint32_t res, int kt, int, const uint3 &,
+                        uint32_t idesc) const {
+        const uint32_t S = 2u * (uint32_t)e, blk = (uint32_t)bn * S;
+        uint32_t wb = res + (uint32_t)(kt * 3 * nck) * blk;  // tap kt*3 + dx
+        for (int dx = 0; dx < 3; ++dx)
+            for (int ci = 0; ci < nck; ++ci, wb += blk) {
+                const uint32_t a = sa + (uint32_t)ci * strip_bytes + (uint32_t)dx * S;
+                for (int kk = 0; kk < e / 16; ++kk)
+                    mma_bf16(acc, op_desc(a, false, S, kk), op_desc(wb, false, S, kk), idesc,
+                             (kt == 0 && dx == 0 && ci == 0 && kk == 0) ? 0u : 1u);
+            }
+    }
+};
+
+// Weight gradient of rows that are a multiple of 64 pixels wide, one whole
+// gradient per tile: the tiles are the pixel splits, and a tile accumulates
+// every row r = tap C + c (and the bias row) in TMEM.  A step is 64 pixels
+// of one row.  Its copies are, per kernel row dy and channel chunk, one strip
+// of pixels x-1 .. x+sr-2 (box ea x sr, MN-major, swizzle 2ea), and the
+// step's output gradient (nb blocks of eb channels x 64 pixels), so each
+// input row crosses three times and each output-gradient row once.  M-tile m
+// = (dy, chunk, h) reads its strip with the blocks one row apart (LBO = 2ea
+// bytes): block j is the strip shifted by j pixels, i.e. tap dx = 2h - 1 + j
+// (blocks of taps beyond +1 are computed and not stored).  The bias M-tile
+// reads the resident `ones` rows (1 in channel 0).  Accumulator m holds
+// columns m bn .. m bn + bn - 1; the epilogue maps (m, row) to r.
+struct WgradStrip : TmaBase {
+    static constexpr bool A_MN = true, B_MN = true;
+    CUtensorMap x1, x2, ones, dy;
+    float *part;  // [splits][9C + 1][Nout]
+    int bn, ea, eb, c1, C, H, W, Nout, steps_per_split, nsteps;
+    int nck, mtp, nb, nmt, ea_shift, bn_shift;  // chunks, M-tiles per strip (1, 2), dY blocks, strip M-tiles
+    uint32_t strip_bytes, tx;
+
+    __device__ void k_range(const uint3 &t, int &k0, int &k1) const {
+        k0 = (int)t.z * steps_per_split;
+        k1 = min(nsteps, k0 + steps_per_split);
+    }
+    __device__ uint32_t step_tx(const uint3 &) const { return tx; }
+    __device__ void prefetch() const {
+        prefetch_map(&x1);
+        if (c1 < C) prefetch_map(&x2);
+        prefetch_map(&ones);
+        prefetch_map(&dy);
+    }
+    __device__ void issue_res(uint32_t res, uint32_t bar) const { tma2(res, &ones, 0, 0, bar); }
+    struct Cursor { int b, y, x; };
+    __device__ Cursor begin(const uint3 &, int k0) const {
+        Cursor u;
+        split_pixel(k0 * BK, H, W, u.b, u.y, u.x);
+        return u;
+    }
+    __device__ void issue(Cursor &u, const uint3 &, uint32_t sa, uint32_t sb, uint32_t bar) const {
+        uint32_t dst = sa;
+        for (int dyi = -1; dyi <= 1; ++dyi)
+            for (int ci = 0, c = 0; ci < nck; ++ci, c += ea, dst += strip_bytes) {
+                if (c < c1) tma4(dst, &x1, c, u.x - 1, u.y + dyi, u.b, bar);
+                else tma4(dst, &x2, c - c1, u.x - 1, u.y + dyi, u.b, bar);
+            }
+        for (int j = 0; j < nb; ++j) tma4(sb + (uint32_t)(j * 128 * eb), &dy, j * eb, u.x, u.y, u.b, bar);
+        u.x += BK;
+        if (u.x == W) {
+            u.x = 0;
+            if (++u.y == H) {
+                u.y = 0;
+                ++u.b;
+            }
+        }
+    }
+    __device__ void mma(uint32_t acc, uint32_t sa, uint32_t sb, uint32_t res, int kt, int k0, const uint3 &,
+                        uint32_t idesc) const {
+        const bool first = kt == k0;
+        const uint32_t sA = 2u * (uint32_t)ea, sB = 2u * (uint32_t)eb;
+        uint32_t a0 = sa, accm = acc;
+        for (int st = 0; st < 3 * nck; ++st, a0 += strip_bytes)
+            for (int h = 0; h < mtp; ++h, accm += (uint32_t)bn) {
+                const uint32_t start = a0 + (uint32_t)(2 * h) * sA;
+#pragma unroll
+                for (int kk = 0; kk < BK / 16; ++kk)
+                    mma_bf16(accm, sdesc_sw(start + (uint32_t)kk * 16u * sA, sA, 8u * sA, sA),
+                             op_desc(sb, true, sB, kk), idesc, (first && kk == 0) ? 0u : 1u);
+            }
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; ++kk)
+            mma_bf16(accm, sdesc_sw(res + (uint32_t)kk * 16u * sA, sA, 8u * sA, sA), op_desc(sb, true, sB, kk),
+                     idesc, (first && kk == 0) ? 0u : 1u);
+    }
+    __device__ void store(int row, int col, const float *v, const uint3 &t) const {
+        const int m = col >> bn_shift, n = col & (bn - 1);
+        const int R = 9 * C;
+        int r;
+        if (m == nmt) {
+            if (row != 0) return;
+            r = R;
+        } else {
+            const int st = mtp == 2 ? (m >> 1) : m, h = m - st * mtp;
+            const int dyi = st / nck, ci = st - dyi * nck;
+            const int j = row >> ea_shift, c = row & (ea - 1);
+            const int dx = 2 * h - 1 + j;
+            if (dx > 1) return;
+            r = (dyi * 3 + dx + 1) * C + ci * ea + c;
+        }
+        float4 *d = reinterpret_cast<float4 *>(part + ((size_t)t.z * (R + 1) + r) * Nout + n);
+        d[0] = make_float4(v[0], v[1], v[2], v[3]);
+        d[1] = make_float4(v[4], v[5], v[6], v[7]);
     }
 };
 
@@ -359,14 +552,13 @@ struct ConvTma : ConvStore {
 // channels x 64 pixels (swizzle 2e), the A tile is 128 / ea blocks of rows,
 // the B tile bn / eb blocks of output channels.  Blocks past the bias row
 // are not copied (their rows are not stored).
-struct WgradTma {
+struct WgradTma : TmaBase {
     static constexpr bool A_MN = true, B_MN = true;
     CUtensorMap x1, x2, ones, dy;
     float *part;  // [splits][9C + 1][Nout]
     int bn, ea, eb, c1, C, H, W, Nout, steps_per_split, nsteps;
     int py, pb;  // rows (W < 64) or images (H W < 64) per 64-pixel step, else 0
     int na, nb;  // blocks of the A tile (BM / ea) and of the B tile (bn / eb)
-    uint32_t a_bytes, b_bytes;
 
     __device__ void k_range(const uint3 &t, int &k0, int &k1) const {
         k0 = (int)t.z * steps_per_split;
@@ -437,7 +629,10 @@ struct WgradTma {
             }
         }
     }
-    __device__ void mma(uint32_t acc, uint32_t sa, uint32_t sb, bool first, uint32_t idesc) const {
+    __device__ void issue_res(uint32_t, uint32_t) const {}
+    __device__ void mma(uint32_t acc, uint32_t sa, uint32_t sb, uint32_t, int kt, int k0, const uint3 &,
+                        uint32_t idesc) const {
+        const bool first = kt == k0;
         const uint32_t s_a = 2u * (uint32_t)ea, s_b = 2u * (uint32_t)eb;
 #pragma unroll
         for (int kk = 0; kk < BK / 16; ++kk)
@@ -460,12 +655,11 @@ struct WgradTma {
 // boxes of 64 M x 64 K), B stored [N][K] (box 64 K x bn) or [K][N] (boxes of
 // eb N x 64 K).  A stage holds K = 64.
 template <bool AMN, bool BMN>
-struct GemmTma {
+struct GemmTma : TmaBase {
     static constexpr bool A_MN = AMN, B_MN = BMN;
     CUtensorMap ma, mb;
     float *c;
     int M, N, K, bn, eb, nb;  // nb = bn / eb
-    uint32_t a_bytes, b_bytes;
 
     __device__ void k_range(const uint3 &, int &k0, int &k1) const { k0 = 0; k1 = K / BK; }
     __device__ uint32_t step_tx(const uint3 &) const { return (uint32_t)(BM * BK * 2 + bn * BK * 2); }
@@ -490,7 +684,10 @@ struct GemmTma {
         }
         u.k += BK;
     }
-    __device__ void mma(uint32_t acc, uint32_t sa, uint32_t sb, bool first, uint32_t idesc) const {
+    __device__ void issue_res(uint32_t, uint32_t) const {}
+    __device__ void mma(uint32_t acc, uint32_t sa, uint32_t sb, uint32_t, int kt, int k0, const uint3 &,
+                        uint32_t idesc) const {
+        const bool first = kt == k0;
         const uint32_t s_b = BMN ? 2u * (uint32_t)eb : 128u;
 #pragma unroll
         for (int kk = 0; kk < BK / 16; ++kk)
@@ -561,13 +758,21 @@ int launch_tma(const Op &op, dim3 grid, int *err, cudaStream_t stream, long long
         configured[dev] = true;
     }
     const uint32_t stage = op.a_bytes + op.b_bytes;
-    const int ns = tma_stages(stage);
-    if (ns < 2) return kb::set_error(KB_ERR_ARG, "umma_tma_k: stage of %u bytes too large", stage);
+    const int cps = op.cps < 1 ? 1 : (op.cps > TM_MAX_CPS ? TM_MAX_CPS : op.cps);
+    const int ns = tma_stages(stage, op.res_bytes, cps);
+    if (ns < 2)
+        return kb::set_error(KB_ERR_ARG, "umma_tma_k: stage of %u bytes with %u resident bytes too large",
+                             stage, op.res_bytes);
+    if (op.nbuf < 1 || op.nbuf > 2 || (uint32_t)cps * op.nbuf * op.acc_cols > 512u || op.acc_cols < 32u ||
+        (op.acc_cols & (op.acc_cols - 1u)) || op.ncols > (int)op.acc_cols || op.ncols % 8)
+        return kb::set_error(KB_ERR_ARG, "umma_tma_k: accumulator shape %u x %d (store %d) invalid",
+                             op.acc_cols, op.nbuf, op.ncols);
     const long long ntiles = (long long)grid.x * grid.y * grid.z;
     if (ntiles >= (1ll << 31) - (1ll << 16))
         return kb::set_error(KB_ERR_ARG, "umma_tma_k: %lld tiles exceed the tile index range", ntiles);
-    const long long ctas = ntiles < kb::sm_count() ? ntiles : kb::sm_count();
-    umma_tma_k<Op><<<(unsigned)ctas, TM_THREADS, tma_smem_bytes(ns, stage), stream>>>(
+    const long long slots = (long long)kb::sm_count() * cps;
+    const long long ctas = ntiles < slots ? ntiles : slots;
+    umma_tma_k<Op><<<(unsigned)ctas, TM_THREADS, tma_smem_bytes(ns, stage, op.res_bytes), stream>>>(
         op, make_uint3(grid.x, grid.y, grid.z), ns, err, spin);
     return 0;
 }

@@ -174,9 +174,13 @@ def test_engines_agree_bit_for_bit(cuda, pkg, sur):
 
 def test_engines_agree_at_full_size(cuda, pkg, sur):
     """At the bench's shape (16 cavities at 256^2, 32 base channels) the
-    TMA-staged engine gives the per-tile engine's output and gradients bit
-    for bit: every layer's tiling (partial rows, whole rows, split-K weight
-    gradients, concatenated decoder inputs, the 16-channel head) is covered."""
+    TMA-staged engine gives the per-tile engine's output bit for bit, and its
+    gradients to FP32 summation order: every layer's tiling is covered (row
+    strips at 256^2 and 128^2, per-tap boxes of partial and whole rows,
+    concatenated decoder inputs, the 16-channel head).  The data gradients
+    keep the per-tile engine's K order; the row-strip weight gradients split
+    the pixels into one range per SM instead, so their FP32 partial sums
+    group differently (bound: 1e-4 of each layer's largest gradient)."""
     import numpy as np
     model = sur.Surrogate(max_batch=16, H=256, W=256, base_channels=32, seed=5)
     model.set_grad_weight(200.0)
@@ -194,7 +198,12 @@ def test_engines_agree_at_full_size(cuda, pkg, sur):
         pkg.set_umma_engine(DEFAULT_ENGINE)
     assert torch.isfinite(outs[0][0]).all() and torch.isfinite(outs[0][1]).all()
     assert torch.equal(outs[0][0], outs[1][0])
-    assert torch.equal(outs[0][1], outs[1][1])
+    g2, g1 = outs[0][1], outs[1][1]
+    for ly in model.layers():
+        n_w = ly["cout"] * 9 * ly["cin"]
+        for off, n in ((ly["w_off"], n_w), (ly["b_off"], ly["cout"])):
+            a, b = g2[off:off + n], g1[off:off + n]
+            assert float((a - b).abs().max()) <= 1e-4 * float(b.abs().max()), (ly, off)
     assert not model.timed_out()
     model.close()
 
