@@ -239,17 +239,35 @@ __global__ void unpack_k(float *__restrict__ out, const float *__restrict__ pred
     }
 }
 
-// Sum the split-K partials of a weight gradient into the flat gradient array:
-// part [splits][9C+1][Cout] -> gW[cout][9C], gb[cout] (row 9C).
+// Sum the split-K partials of a weight gradient into the flat gradient array,
+// in a fixed order: part [splits][Rp+1][Cout] (Rp = 9 Cp) -> gW[cout][9 Cs],
+// gb[cout] (row Rp).  With many splits a first pass sums groups of `per`
+// consecutive splits (grid.y = group) into tmp [groups][(Rp+1) Cout] and the
+// second pass sums the groups.  Cp > Cs: the partials carry zero-padded
+// input channels c >= Cs, which are dropped.
+__global__ void wgrad_group_k(float *__restrict__ tmp, const float *__restrict__ part, int splits, int per,
+                              int E) {
+    const int z0 = blockIdx.y * per, z1 = min(splits, z0 + per);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (int z = z0; z < z1; ++z) s += part[(size_t)z * E + e];
+        tmp[(size_t)blockIdx.y * E + e] = s;
+    }
+}
+
 __global__ void wgrad_reduce_k(float *__restrict__ gW, float *__restrict__ gb,
-                               const float *__restrict__ part, int splits, int R, int Cout) {
-    const int n = (R + 1) * Cout;
+                               const float *__restrict__ part, int splits, int Cp, int Cs, int Cout) {
+    const int Rp = 9 * Cp, n = (Rp + 1) * Cout;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         const int r = t / Cout, co = t - r * Cout;
         float s = 0.f;
-        for (int z = 0; z < splits; ++z) s += part[((size_t)z * (R + 1) + r) * Cout + co];
-        if (r < R) gW[(size_t)co * R + r] = s;
-        else gb[co] = s;
+        for (int z = 0; z < splits; ++z) s += part[((size_t)z * (Rp + 1) + r) * Cout + co];
+        if (r == Rp) {
+            gb[co] = s;
+        } else {
+            const int tap = r / Cp, c = r - tap * Cp;
+            if (c < Cs) gW[((size_t)co * 9 + tap) * Cs + c] = s;
+        }
     }
 }
 
@@ -309,6 +327,33 @@ __global__ void cavity_inputs_k(bf16 *__restrict__ in, const float *__restrict__
     }
 }
 
+// The network input (IN_CH = 8 channels) zero-padded to PAD_CH = 16 channels
+// per pixel, the narrowest channel run a swizzled TMA box copies.
+constexpr int PAD_CH = 16;
+__global__ void pad_input_k(bf16 *__restrict__ dst, const bf16 *__restrict__ src, long long npix) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix;
+         p += (long long)gridDim.x * blockDim.x) {
+        uint4 *d = reinterpret_cast<uint4 *>(dst + p * PAD_CH);
+        d[0] = *reinterpret_cast<const uint4 *>(src + p * IN_CH);
+        d[1] = make_uint4(0, 0, 0, 0);
+    }
+}
+
+// W [Cout][9 Cin] FP32 -> wp [Cout][Kp] BF16 for PAD_CH input channels (the
+// padding channels' weights are zero): wp[co][t*PAD_CH + c] = W[co][t*Cin + c].
+__global__ void pack_pad_k(bf16 *__restrict__ wp, const float *__restrict__ W, int Cin, int Cout, int Kp) {
+    const int n = Cout * Kp;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int co = t / Kp, k = t - co * Kp;
+        float x = 0.f;
+        if (k < 9 * PAD_CH) {
+            const int tap = k / PAD_CH, c = k - tap * PAD_CH;
+            if (c < Cin) x = W[((size_t)co * 9 + tap) * Cin + c];
+        }
+        wp[t] = __float2bfloat16_rn(x);
+    }
+}
+
 inline dim3 ew_grid(long long n) {
     long long b = (n + 255) / 256;
     const long long cap = (long long)kb::sm_count() * 16;
@@ -336,6 +381,7 @@ struct TmaPlan {
     int n = -1;
     int f = 0, d = 0, w = 0;  // 0: per-tile engine, 1: TMA per-tap boxes, 2: TMA row strips
     int wsplits = 0;
+    int cp = 0;               // input channels of the weight-gradient partials (padded first layer: PAD_CH)
     kb::umma::ConvTma fwd, dgr;
     kb::umma::ConvStrip sfwd, sdgr;
     kb::umma::WgradTma wg;
@@ -358,6 +404,8 @@ struct kb_surrogate {
     long long n_params = 0;
     float *part = nullptr;              // split-K partials
     size_t part_floats = 0;
+    float *tmp = nullptr;               // grouped sums of the partials
+    size_t tmp_floats = 0;
     int *err = nullptr;
     float *loss = nullptr;
     Norm norm{{1.f, 1.f, 1.f}, {0.f, 0.f, 0.f}};
@@ -365,6 +413,10 @@ struct kb_surrogate {
     std::vector<TmaPlan> tp;            // per layer, TMA engine
     bf16 *ones = nullptr;               // [72][64] BF16, column 0 = 1: the bias row's A block
     int up_batch = -1;                  // batch of the decoder inputs last upsampled
+    bf16 *in_pad = nullptr;             // [Bmax*H*W][PAD_CH]: the input padded for the TMA engine
+    bf16 *wb_pad = nullptr;             // [cout][Kp_pad]: first layer's weights for PAD_CH channels
+    int Kp_pad = 0;
+    int pad_batch = -1;                 // batch of the input last padded
     std::vector<void *> allocs;
     int H_at(int level) const { return H >> level; }
     int W_at(int level) const { return W >> level; }
@@ -422,11 +474,11 @@ void upsample(kb_surrogate *s, const Layer &l, int n, cudaStream_t st) {
 // Row-strip weight gradient of a layer: TMEM columns of its accumulators
 // (all taps, all channel chunks and the bias row of one output tile), or 0
 // when the layer does not take that form.
-uint32_t strip_wgrad_cols(const Layer &l, int W) {
+uint32_t strip_wgrad_cols(const Layer &l, int W, int cin1) {
     using namespace kb::umma;
-    const int ea = chunk_of(l.cin1, l.cin2), bn = l.bn_w;
+    const int ea = chunk_of(cin1, l.cin2), bn = l.bn_w;
     if (!ea || !chunk_of(bn) || W % BK || l.cout != bn || (bn & (bn - 1))) return 0;
-    const int nmt = 3 * (l.cin / ea) * (ea == 64 ? 2 : 1);
+    const int nmt = 3 * ((cin1 + l.cin2) / ea) * (ea == 64 ? 2 : 1);
     const uint32_t need = (uint32_t)((nmt + 1) * bn);
     uint32_t cols = 32;
     while (cols < need) cols <<= 1;
@@ -478,6 +530,12 @@ bool conv_strip_fits(int C, int e, int bn, int W) {
     return tma_fit(b) > 0;
 }
 
+// The network input (s->act[T_IN]) padded to PAD_CH channels (s->in_pad).
+void pad_input(kb_surrogate *s, int n, cudaStream_t st) {
+    const long long npix = (long long)n * s->H * s->W;
+    pad_input_k<<<ew_grid(npix), 256, 0, st>>>(s->in_pad, s->act[T_IN], npix);
+}
+
 // Build (or keep) the TMA engine's operations of layer i for n images.
 int prepare_tma(kb_surrogate *s, int i, int n) {
     using namespace kb::umma;
@@ -488,17 +546,23 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
     p.f = p.d = p.w = 0;
     const char *what = "kb_surrogate (TMA engine)";
     const int H = s->H_at(l.level), W = s->W_at(l.level), M = n * H * W;
-    const bf16 *x1 = l.in2 >= 0 ? l.up : s->act[l.in1];
+    // the first layer reads the input padded to PAD_CH channels
+    const bool padded = l.in1 == T_IN && l.cin1 % 16;
+    const int cin1 = padded ? PAD_CH : l.cin1, cin = cin1 + l.cin2;
+    const bf16 *x1 = padded ? s->in_pad : (l.in2 >= 0 ? l.up : s->act[l.in1]);
     const bf16 *x2 = l.in2 >= 0 ? s->act[l.in2] : nullptr;
+    const bf16 *wb = padded ? s->wb_pad : l.wb;
+    const int Kp = padded ? s->Kp_pad : l.Kp;
+    p.cp = cin;
     PixBox b128{}, b64{};
     const bool g128 = pix_box(BM, H, W, b128), g64 = pix_box(BK, H, W, b64);
     int rc = 0;
     // forward: row strips, or boxes of e input channels x 128 pixels (weights e x bn_f)
-    const int ef = chunk_of(l.cin1, l.cin2);
-    if (ef && l.cout == l.bn_f && conv_strip_fits(l.cin, ef, l.bn_f, W)) {
+    const int ef = chunk_of(cin1, l.cin2);
+    if (ef && l.cout == l.bn_f && conv_strip_fits(cin, ef, l.bn_f, W)) {
         ConvStrip &c = p.sfwd;
         c = ConvStrip{};
-        if ((rc = conv_strip(c, x1, l.cin1, x2, l.cin2, l.wb, l.Kp, l.bn_f, ef, H, W, n, what))) return rc;
+        if ((rc = conv_strip(c, x1, cin1, x2, l.cin2, wb, Kp, l.bn_f, ef, H, W, n, what))) return rc;
         c.bias = s->params + l.b_off;
         c.mask.s1 = nullptr;
         c.out = l.out == T_OUT ? (void *)s->out_f32 : (void *)s->act[l.out];
@@ -511,18 +575,18 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
     } else if (ef && g128) {
         ConvTma &c = p.fwd;
         c = ConvTma{};
-        if ((rc = nhwc_map(&c.x1, x1, l.cin1, W, H, n, ef, b128, what))) return rc;
+        if ((rc = nhwc_map(&c.x1, x1, cin1, W, H, n, ef, b128, what))) return rc;
         if (x2 && (rc = nhwc_map(&c.x2, x2, l.cin2, W, H, n, ef, b128, what))) return rc;
         if (!x2) c.x2 = c.x1;
-        const cuuint64_t d[2] = {(cuuint64_t)l.Kp, (cuuint64_t)l.cout}, sd[1] = {(cuuint64_t)l.Kp * 2};
+        const cuuint64_t d[2] = {(cuuint64_t)Kp, (cuuint64_t)l.cout}, sd[1] = {(cuuint64_t)Kp * 2};
         const cuuint32_t bx[2] = {(cuuint32_t)ef, (cuuint32_t)l.bn_f};
-        if ((rc = bf16_map(&c.w, l.wb, 2, d, sd, bx, 2 * ef, what))) return rc;
+        if ((rc = bf16_map(&c.w, wb, 2, d, sd, bx, 2 * ef, what))) return rc;
         c.e = ef;
-        c.c1 = l.cin1;
-        c.C = l.cin;
+        c.c1 = cin1;
+        c.C = cin;
         c.H = H;
         c.W = W;
-        c.nck = l.cin / ef;
+        c.nck = cin / ef;
         c.a_bytes = round1k((uint32_t)(BM * 2 * ef));
         c.b_bytes = round1k((uint32_t)(l.bn_f * 2 * ef));
         c.res_bytes = 0;
@@ -594,22 +658,22 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
     }
     // weight gradient: row strips (whole gradient per pixel split), or blocks
     // of ea input channels / eb output-gradient channels x 64 pixels
-    const int ea = chunk_of(l.cin1, l.cin2), eb = chunk_of(l.bn_w);
-    const uint32_t wcols = strip_wgrad_cols(l, W);
+    const int ea = chunk_of(cin1, l.cin2), eb = chunk_of(l.bn_w);
+    const uint32_t wcols = strip_wgrad_cols(l, W, cin1);
     const int sr = BK + (BM / (ea ? ea : 64) - 1 > 3 ? BM / ea - 1 : 3);  // strip rows
     const uint32_t wstrip = ea ? round1k((uint32_t)(sr * 2 * ea)) : 0;
-    const uint32_t wstage = 3u * (uint32_t)(l.cin / (ea ? ea : 1)) * wstrip + round1k((uint32_t)(l.bn_w * BK * 2));
-    TmaBase wb{};
-    wb.a_bytes = wstage;
-    wb.res_bytes = (uint32_t)(72 * 2 * ea);
-    wb.acc_cols = wcols;
-    wb.nbuf = 1;
-    const int wcps = wcols ? tma_fit(wb) : 0;
+    const uint32_t wstage = 3u * (uint32_t)(cin / (ea ? ea : 1)) * wstrip + round1k((uint32_t)(l.bn_w * BK * 2));
+    TmaBase wfit{};
+    wfit.a_bytes = wstage;
+    wfit.res_bytes = (uint32_t)(72 * 2 * ea);
+    wfit.acc_cols = wcols;
+    wfit.nbuf = 1;
+    const int wcps = wcols ? tma_fit(wfit) : 0;
     if (wcps) {
         WgradStrip &w = p.swg;
         w = WgradStrip{};
         const PixBox strip{sr, 1, 1};
-        if ((rc = nhwc_map(&w.x1, x1, l.cin1, W, H, n, ea, strip, what))) return rc;
+        if ((rc = nhwc_map(&w.x1, x1, cin1, W, H, n, ea, strip, what))) return rc;
         if (x2 && (rc = nhwc_map(&w.x2, x2, l.cin2, W, H, n, ea, strip, what))) return rc;
         if (!x2) w.x2 = w.x1;
         const cuuint64_t d[2] = {(cuuint64_t)ea, 72}, sd[1] = {128};
@@ -625,14 +689,14 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
         w.bn = l.bn_w;
         w.ea = ea;
         w.eb = eb;
-        w.c1 = l.cin1;
-        w.C = l.cin;
+        w.c1 = cin1;
+        w.C = cin;
         w.H = H;
         w.W = W;
         w.Nout = l.cout;
         w.steps_per_split = sps;
         w.nsteps = nsteps;
-        w.nck = l.cin / ea;
+        w.nck = cin / ea;
         w.mtp = ea == 64 ? 2 : 1;
         w.nb = l.bn_w / eb;
         w.nmt = 3 * w.nck * w.mtp;
@@ -651,7 +715,7 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
     } else if (ea && eb && g64) {
         WgradTma &w = p.wg;
         w = WgradTma{};
-        if ((rc = nhwc_map(&w.x1, x1, l.cin1, W, H, n, ea, b64, what))) return rc;
+        if ((rc = nhwc_map(&w.x1, x1, cin1, W, H, n, ea, b64, what))) return rc;
         if (x2 && (rc = nhwc_map(&w.x2, x2, l.cin2, W, H, n, ea, b64, what))) return rc;
         if (!x2) w.x2 = w.x1;
         const cuuint64_t d[2] = {(cuuint64_t)ea, 64}, sd[1] = {128};
@@ -664,8 +728,8 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
         w.bn = l.bn_w;
         w.ea = ea;
         w.eb = eb;
-        w.c1 = l.cin1;
-        w.C = l.cin;
+        w.c1 = cin1;
+        w.C = cin;
         w.H = H;
         w.W = W;
         w.Nout = l.cout;
@@ -692,6 +756,7 @@ int forward(kb_surrogate *s, const void *input, int n, cudaStream_t st) {
     using namespace kb::umma;
     s->act[T_IN] = (bf16 *)input;
     const bool tma = engine() == 2;
+    if (tma) pad_input(s, n, st);
     for (int i = 0; i < N_LAYERS; ++i) {
         const Layer &l = s->L[i];
         // pooled inputs are produced just before their consumer
@@ -733,13 +798,40 @@ int forward(kb_surrogate *s, const void *input, int n, cudaStream_t st) {
     return kb::check_launch("kb_surrogate forward");
 }
 
+// Reduce the split partials in s->part of layer l (input channels Cp in the
+// partials) into its gradient.
+int reduce_wgrad(kb_surrogate *s, const Layer &l, int splits, int Cp, cudaStream_t st) {
+    const long long E = (long long)(9 * Cp + 1) * l.cout;
+    int groups = 1;
+    if (splits >= 16) {
+        groups = (int)((300000 + E - 1) / E);
+        groups = std::min(groups, splits / 8);
+        groups = std::max(groups, 1);
+    }
+    const float *src = s->part;
+    int n = splits;
+    if (groups > 1 && (size_t)(groups * E) <= s->tmp_floats) {
+        const int per = (splits + groups - 1) / groups;
+        groups = (splits + per - 1) / per;
+        dim3 g1(ew_grid(E).x, groups);
+        wgrad_group_k<<<g1, 256, 0, st>>>(s->tmp, s->part, splits, per, (int)E);
+        src = s->tmp;
+        n = groups;
+    }
+    wgrad_reduce_k<<<ew_grid(E), 256, 0, st>>>(s->grads + l.w_off, s->grads + l.b_off, src, n, Cp, l.cin,
+                                                 l.cout);
+    return 0;
+}
+
 int backward(kb_surrogate *s, int n, cudaStream_t st) {
     using namespace kb::umma;
     const bool tma = engine() == 2;
     if (tma && s->up_batch != n) {
         // the forward pass ran on another engine: upsample the decoder inputs
+        // and pad the network input
         for (const Layer &l : s->L)
             if (l.in2 >= 0) upsample(s, l, n, st);
+        pad_input(s, n, st);
         s->up_batch = n;
     }
     for (int i = N_LAYERS - 1; i >= 0; --i) {
@@ -751,7 +843,9 @@ int backward(kb_surrogate *s, int n, cudaStream_t st) {
             if (int rc = prepare_tma(s, i, n)) return rc;
         const TmaPlan &tp = s->tp[i];
         const int R = 9 * l.cin;
-        // weight gradient (split over pixels) and its reduction
+        // weight gradient (split over pixels) and its reduction; the TMA
+        // engine's partials carry tp.cp input channels (the padded input's
+        // PAD_CH for the first layer)
         int sps = 0;
         int splits = wgrad_splits(l, M, sps);
         if (tma && tp.w == 2) {
@@ -759,7 +853,7 @@ int backward(kb_surrogate *s, int n, cudaStream_t st) {
             if (int rc = launch_tma(tp.swg, dim3(1, 1, splits), s->err, st)) return rc;
         } else if (tma && tp.w == 1) {
             splits = tp.wsplits;
-            const dim3 wg((R + 1 + BM - 1) / BM, l.cout / l.bn_w, splits);
+            const dim3 wg((9 * tp.cp + 1 + BM - 1) / BM, l.cout / l.bn_w, splits);
             if (int rc = launch_tma(tp.wg, wg, s->err, st)) return rc;
         } else {
             WgradOp wo{};
@@ -774,8 +868,7 @@ int backward(kb_surrogate *s, int n, cudaStream_t st) {
             const dim3 wg((R + 1 + BM - 1) / BM, l.cout / l.bn_w, splits);
             if (int rc = launch(wo, wg, s->err, st)) return rc;
         }
-        wgrad_reduce_k<<<ew_grid((long long)(R + 1) * l.cout), 256, 0, st>>>(
-            s->grads + l.w_off, s->grads + l.b_off, s->part, splits, R, l.cout);
+        if (int rc = reduce_wgrad(s, l, splits, (tma && tp.w) ? tp.cp : l.cin, st)) return rc;
         if (i == 0) break;
         // data gradient
         const dim3 grid((M + BM - 1) / BM, l.cin / l.bn_d);
@@ -835,6 +928,9 @@ int repack(kb_surrogate *s, cudaStream_t st) {
         const long long n = (long long)l.cout * l.Kp + (l.wt ? (long long)l.cin * l.Kpt : 0);
         pack_k<<<ew_grid(n), 256, 0, st>>>(l.wb, l.wt, s->params + l.w_off, l.cin, l.cout, l.Kp, l.Kpt);
     }
+    const Layer &l0 = s->L[0];
+    pack_pad_k<<<ew_grid((long long)l0.cout * s->Kp_pad), 256, 0, st>>>(s->wb_pad, s->params + l0.w_off, l0.cin,
+                                                                        l0.cout, s->Kp_pad);
     return kb::check_launch("kb_surrogate repack");
 }
 
@@ -917,13 +1013,16 @@ int kb_surrogate_create(kb_surrogate **out, int max_batch, int H, int W, int bas
             else l.dx = s->grad[l.in1];
         }
         if (l.in2 >= 0) A((void **)&l.up, px * l.cin1 * sizeof(bf16));
-        size_t need = (size_t)max_wgrad_splits(l) * (9 * l.cin + 1) * l.cout;
-        if (strip_wgrad_cols(l, W >> l.level))
-            need = std::max(need, (size_t)kb::sm_count() * kb::umma::TM_MAX_CPS * (9 * l.cin + 1) * l.cout);
+        const int cin1 = (l.in1 == T_IN && l.cin1 % 16) ? PAD_CH : l.cin1;
+        size_t need = (size_t)max_wgrad_splits(l) * (9 * (cin1 + l.cin2) + 1) * l.cout;
+        if (strip_wgrad_cols(l, W >> l.level, cin1))
+            need = std::max(need, (size_t)kb::sm_count() * kb::umma::TM_MAX_CPS * (9 * (cin1 + l.cin2) + 1) * l.cout);
         if (need > part) part = need;
     }
     s->part_floats = part;
     A((void **)&s->part, part * sizeof(float));
+    s->tmp_floats = 1u << 20;  // grouped sums where groups x (9 Cin + 1) Cout fits, else one pass
+    A((void **)&s->tmp, s->tmp_floats * sizeof(float));
     A((void **)&s->params, (size_t)s->n_params * sizeof(float));
     A((void **)&s->grads, (size_t)s->n_params * sizeof(float));
     A((void **)&s->adam_m, (size_t)s->n_params * sizeof(float));
@@ -931,6 +1030,9 @@ int kb_surrogate_create(kb_surrogate **out, int max_batch, int H, int W, int bas
     A((void **)&s->err, sizeof(int));
     A((void **)&s->loss, sizeof(float));
     A((void **)&s->ones, 72 * 64 * sizeof(bf16));
+    s->Kp_pad = round_up(9 * PAD_CH, kb::umma::BK);
+    A((void **)&s->in_pad, pix0 * PAD_CH * sizeof(bf16));
+    A((void **)&s->wb_pad, (size_t)s->L[0].cout * s->Kp_pad * sizeof(bf16));
     s->tp.resize(N_LAYERS);
     if (rc) {
         for (void *p : s->allocs) cudaFree(p);
