@@ -380,7 +380,7 @@ struct Layer {
 struct TmaPlan {
     int n = -1;
     int f = 0, d = 0, w = 0;  // 0: per-tile engine, 1: TMA per-tap boxes, 2: TMA row strips
-    int wsplits = 0;
+    int wsplits = 0, wgroups = 1;
     int cp = 0;               // input channels of the weight-gradient partials (padded first layer: PAD_CH)
     kb::umma::ConvTma fwd, dgr;
     kb::umma::ConvStrip sfwd, sdgr;
@@ -471,18 +471,41 @@ void upsample(kb_surrogate *s, const Layer &l, int n, cudaStream_t st) {
                                                                               W, l.cin1);
 }
 
-// Row-strip weight gradient of a layer: TMEM columns of its accumulators
-// (all taps, all channel chunks and the bias row of one output tile), or 0
-// when the layer does not take that form.
-uint32_t strip_wgrad_cols(const Layer &l, int W, int cin1) {
+// Row-strip weight gradient of a layer (input channels cin1 + cin2 in
+// chunks of ea): the chunks per tile (cpt, a divisor of the chunk count)
+// with the most MMA issuers per SM, the TMEM columns of a tile's
+// accumulators (all taps of its chunks plus the bias row) and the fit
+// (CTAs per SM); false when the layer does not take that form.
+struct StripWgradPlan { int ea, cpt, sr; uint32_t cols, strip, stage; kb::umma::TmaBase fit; };
+bool plan_strip_wgrad(const Layer &l, int W, int cin1, StripWgradPlan &P) {
     using namespace kb::umma;
     const int ea = chunk_of(cin1, l.cin2), bn = l.bn_w;
-    if (!ea || !chunk_of(bn) || W % BK || l.cout != bn || (bn & (bn - 1))) return 0;
-    const int nmt = 3 * ((cin1 + l.cin2) / ea) * (ea == 64 ? 2 : 1);
-    const uint32_t need = (uint32_t)((nmt + 1) * bn);
-    uint32_t cols = 32;
-    while (cols < need) cols <<= 1;
-    return cols <= 512 ? cols : 0;
+    if (!ea || !chunk_of(bn) || W % BK || l.cout != bn || (bn & (bn - 1))) return false;
+    const int nck = (cin1 + l.cin2) / ea, mtp = ea == 64 ? 2 : 1;
+    const int sr = BK + (BM / ea - 1 > 3 ? BM / ea - 1 : 3);  // strip rows
+    const uint32_t strip = round1k((uint32_t)(sr * 2 * ea));
+    bool found = false;
+    for (int cpt = nck; cpt >= 1; --cpt) {
+        if (nck % cpt) continue;
+        const uint32_t need = (uint32_t)((3 * cpt * mtp + 1) * bn);
+        uint32_t cols = 32;
+        while (cols < need) cols <<= 1;
+        if (cols > 512) continue;
+        TmaBase b{};
+        b.a_bytes = 3u * (uint32_t)cpt * strip;
+        b.b_bytes = round1k((uint32_t)(bn * BK * 2));
+        b.res_bytes = (uint32_t)(72 * 2 * ea);
+        b.acc_cols = cols;
+        b.nbuf = 1;
+        // one CTA per SM (512 accumulator columns) measured slower than the
+        // per-tap boxes: take this form only where CTAs share the SM
+        if ((b.cps = tma_fit(b)) < 2) continue;
+        if (!found || b.cps > P.fit.cps) {
+            P = StripWgradPlan{ea, cpt, sr, cols, strip, b.a_bytes + b.b_bytes, b};
+            found = true;
+        }
+    }
+    return found;
 }
 
 // Row-strip convolution (forward or data gradient): input channels c1 + c2
@@ -659,20 +682,11 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
     // weight gradient: row strips (whole gradient per pixel split), or blocks
     // of ea input channels / eb output-gradient channels x 64 pixels
     const int ea = chunk_of(cin1, l.cin2), eb = chunk_of(l.bn_w);
-    const uint32_t wcols = strip_wgrad_cols(l, W, cin1);
-    const int sr = BK + (BM / (ea ? ea : 64) - 1 > 3 ? BM / ea - 1 : 3);  // strip rows
-    const uint32_t wstrip = ea ? round1k((uint32_t)(sr * 2 * ea)) : 0;
-    const uint32_t wstage = 3u * (uint32_t)(cin / (ea ? ea : 1)) * wstrip + round1k((uint32_t)(l.bn_w * BK * 2));
-    TmaBase wfit{};
-    wfit.a_bytes = wstage;
-    wfit.res_bytes = (uint32_t)(72 * 2 * ea);
-    wfit.acc_cols = wcols;
-    wfit.nbuf = 1;
-    const int wcps = wcols ? tma_fit(wfit) : 0;
-    if (wcps) {
+    StripWgradPlan sp{};
+    if (eb && plan_strip_wgrad(l, W, cin1, sp)) {
         WgradStrip &w = p.swg;
         w = WgradStrip{};
-        const PixBox strip{sr, 1, 1};
+        const PixBox strip{sp.sr, 1, 1};
         if ((rc = nhwc_map(&w.x1, x1, cin1, W, H, n, ea, strip, what))) return rc;
         if (x2 && (rc = nhwc_map(&w.x2, x2, l.cin2, W, H, n, ea, strip, what))) return rc;
         if (!x2) w.x2 = w.x1;
@@ -680,11 +694,14 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
         const cuuint32_t bx[2] = {(cuuint32_t)ea, 72};
         if ((rc = bf16_map(&w.ones, s->ones, 2, d, sd, bx, 2 * ea, what))) return rc;
         if ((rc = nhwc_map(&w.dy, s->grad[l.out], l.cout, W, H, n, eb, b64, what))) return rc;
+        const int ngroups = cin / ea / sp.cpt;
         const int nsteps = (M + BK - 1) / BK;
-        int want = kb::sm_count() * wcps;  // one pixel split per CTA
+        // about one tile (chunk group, pixel split) per CTA
+        int want = (kb::sm_count() * sp.fit.cps + ngroups - 1) / ngroups;
         if (want > nsteps) want = nsteps;
         const int sps = (nsteps + want - 1) / want;
         p.wsplits = (nsteps + sps - 1) / sps;
+        p.wgroups = ngroups;
         w.part = s->part;
         w.bn = l.bn_w;
         w.ea = ea;
@@ -696,22 +713,22 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
         w.Nout = l.cout;
         w.steps_per_split = sps;
         w.nsteps = nsteps;
-        w.nck = cin / ea;
+        w.cpt = sp.cpt;
         w.mtp = ea == 64 ? 2 : 1;
         w.nb = l.bn_w / eb;
-        w.nmt = 3 * w.nck * w.mtp;
+        w.nmt = 3 * sp.cpt * w.mtp;
         w.ea_shift = ea == 64 ? 6 : (ea == 32 ? 5 : 4);
         w.bn_shift = 31 - __builtin_clz((unsigned)l.bn_w);
-        w.strip_bytes = wstrip;
-        w.tx = (uint32_t)(3 * w.nck * sr * 2 * ea + l.bn_w * BK * 2);
-        w.a_bytes = 3u * (uint32_t)w.nck * wstrip;
-        w.b_bytes = round1k((uint32_t)(l.bn_w * BK * 2));
-        w.res_bytes = (uint32_t)(72 * 2 * ea);
-        w.acc_cols = wcols;
-        w.nbuf = 1;  // one tile per CTA: nothing to overlap the epilogue with
+        w.strip_bytes = sp.strip;
+        w.tx = (uint32_t)(3 * sp.cpt * sp.sr * 2 * ea + l.bn_w * BK * 2);
+        w.a_bytes = sp.fit.a_bytes;
+        w.b_bytes = sp.fit.b_bytes;
+        w.res_bytes = sp.fit.res_bytes;
+        w.acc_cols = sp.cols;
+        w.nbuf = 1;  // about one tile per CTA: nothing to overlap the epilogue with
         w.ncols = (w.nmt + 1) * l.bn_w;
-        w.cps = wcps;
-        p.w = 2;
+        w.cps = tma_fit(w);
+        p.w = w.cps ? 2 : 0;
     } else if (ea && eb && g64) {
         WgradTma &w = p.wg;
         w = WgradTma{};
@@ -850,7 +867,7 @@ int backward(kb_surrogate *s, int n, cudaStream_t st) {
         int splits = wgrad_splits(l, M, sps);
         if (tma && tp.w == 2) {
             splits = tp.wsplits;
-            if (int rc = launch_tma(tp.swg, dim3(1, 1, splits), s->err, st)) return rc;
+            if (int rc = launch_tma(tp.swg, dim3(tp.wgroups, 1, splits), s->err, st)) return rc;
         } else if (tma && tp.w == 1) {
             splits = tp.wsplits;
             const dim3 wg((9 * tp.cp + 1 + BM - 1) / BM, l.cout / l.bn_w, splits);
@@ -1015,7 +1032,8 @@ int kb_surrogate_create(kb_surrogate **out, int max_batch, int H, int W, int bas
         if (l.in2 >= 0) A((void **)&l.up, px * l.cin1 * sizeof(bf16));
         const int cin1 = (l.in1 == T_IN && l.cin1 % 16) ? PAD_CH : l.cin1;
         size_t need = (size_t)max_wgrad_splits(l) * (9 * (cin1 + l.cin2) + 1) * l.cout;
-        if (strip_wgrad_cols(l, W >> l.level, cin1))
+        StripWgradPlan sp{};
+        if (plan_strip_wgrad(l, W >> l.level, cin1, sp))
             need = std::max(need, (size_t)kb::sm_count() * kb::umma::TM_MAX_CPS * (9 * (cin1 + l.cin2) + 1) * l.cout);
         if (need > part) part = need;
     }

@@ -468,7 +468,7 @@ struct WgradStrip : TmaBase {
     CUtensorMap x1, x2, ones, dy;
     float *part;  // [splits][9C + 1][Nout]
     int bn, ea, eb, c1, C, H, W, Nout, steps_per_split, nsteps;
-    int nck, mtp, nb, nmt, ea_shift, bn_shift;  // chunks, M-tiles per strip (1, 2), dY blocks, strip M-tiles
+    int cpt, mtp, nb, nmt, ea_shift, bn_shift;  // chunks per tile, M-tiles per strip (1, 2), dY blocks, strip M-tiles
     uint32_t strip_bytes, tx;
 
     __device__ void k_range(const uint3 &t, int &k0, int &k1) const {
@@ -489,10 +489,11 @@ struct WgradStrip : TmaBase {
         split_pixel(k0 * BK, H, W, u.b, u.y, u.x);
         return u;
     }
-    __device__ void issue(Cursor &u, const uint3 &, uint32_t sa, uint32_t sb, uint32_t bar) const {
+    __device__ void issue(Cursor &u, const uint3 &t, uint32_t sa, uint32_t sb, uint32_t bar) const {
         uint32_t dst = sa;
+        const int cg = (int)t.x * cpt * ea;  // first channel of this tile's chunk group
         for (int dyi = -1; dyi <= 1; ++dyi)
-            for (int ci = 0, c = 0; ci < nck; ++ci, c += ea, dst += strip_bytes) {
+            for (int ci = 0, c = cg; ci < cpt; ++ci, c += ea, dst += strip_bytes) {
                 if (c < c1) tma4(dst, &x1, c, u.x - 1, u.y + dyi, u.b, bar);
                 else tma4(dst, &x2, c - c1, u.x - 1, u.y + dyi, u.b, bar);
             }
@@ -506,12 +507,12 @@ struct WgradStrip : TmaBase {
             }
         }
     }
-    __device__ void mma(uint32_t acc, uint32_t sa, uint32_t sb, uint32_t res, int kt, int k0, const uint3 &,
+    __device__ void mma(uint32_t acc, uint32_t sa, uint32_t sb, uint32_t res, int kt, int k0, const uint3 &t,
                         uint32_t idesc) const {
         const bool first = kt == k0;
         const uint32_t sA = 2u * (uint32_t)ea, sB = 2u * (uint32_t)eb;
         uint32_t a0 = sa, accm = acc;
-        for (int st = 0; st < 3 * nck; ++st, a0 += strip_bytes)
+        for (int st = 0; st < 3 * cpt; ++st, a0 += strip_bytes)
             for (int h = 0; h < mtp; ++h, accm += (uint32_t)bn) {
                 const uint32_t start = a0 + (uint32_t)(2 * h) * sA;
 #pragma unroll
@@ -519,6 +520,7 @@ struct WgradStrip : TmaBase {
                     mma_bf16(accm, sdesc_sw(start + (uint32_t)kk * 16u * sA, sA, 8u * sA, sA),
                              op_desc(sb, true, sB, kk), idesc, (first && kk == 0) ? 0u : 1u);
             }
+        if (t.x != 0) return;  // the bias row belongs to chunk group 0
 #pragma unroll
         for (int kk = 0; kk < BK / 16; ++kk)
             mma_bf16(accm, sdesc_sw(res + (uint32_t)kk * 16u * sA, sA, 8u * sA, sA), op_desc(sb, true, sB, kk),
@@ -529,11 +531,11 @@ struct WgradStrip : TmaBase {
         const int R = 9 * C;
         int r;
         if (m == nmt) {
-            if (row != 0) return;
+            if (row != 0 || t.x != 0) return;
             r = R;
         } else {
             const int st = mtp == 2 ? (m >> 1) : m, h = m - st * mtp;
-            const int dyi = st / nck, ci = st - dyi * nck;
+            const int dyi = st / cpt, ci = (int)t.x * cpt + st - dyi * cpt;
             const int j = row >> ea_shift, c = row & (ea - 1);
             const int dx = 2 * h - 1 + j;
             if (dx > 1) return;
