@@ -95,7 +95,7 @@ __device__ bool grid_barrier(const BatchState &D, unsigned nblocks, long long li
 }
 
 template <typename R>
-__device__ __forceinline__ float ldv(const R *p, long long m) { return Dev<R>::ld(p[m]); }
+__device__ __forceinline__ float ldv(const R *p, int m) { return Dev<R>::ld(p[m]); }
 
 __device__ __forceinline__ double block_sum(double v, double *sh) {
 #pragma unroll
@@ -116,8 +116,8 @@ template <typename R, bool SR>
 __device__ __forceinline__ void node_update(const R *__restrict__ src, R *__restrict__ dst, int N,
                                             int i, int j, float s_nu, float u_lid, float &ux,
                                             float &uy, uint32_t key) {
-    const long long P = (long long)N * N;
-    const long long c = (long long)j * N + i;
+    const int P = N * N;  // 9 N^2 < 2^31 (kb_batch_create)
+    const int c = j * N + i;
     const bool w = i > 0, e = i < N - 1, s = j > 0, n = j < N - 1;
     float d[9];
     d[0] = ldv(src, c);
@@ -246,8 +246,8 @@ template <> struct Raw2<__nv_bfloat16> {
 
 template <typename R>
 __device__ __forceinline__ void pair_loads_raw(const R *__restrict__ src, int N, int i, int j, R *v) {
-    const long long P = (long long)N * N;
-    const long long c = (long long)j * N + i;  // node A = (i, j), node B = (i + 1, j)
+    const int P = N * N;  // 9 N^2 < 2^31 (kb_batch_create)
+    const int c = j * N + i;  // node A = (i, j), node B = (i + 1, j)
     const bool w = i > 0, e = i + 1 < N - 1, s = j > 0, n = j < N - 1;
     Raw2<R>::ld(src + c, v + 0);
     Raw2<R>::ld(s ? src + c - N + 2 * P : src + c + 4 * P, v + 4);
@@ -272,8 +272,8 @@ template <typename R, bool SR>
 __device__ __forceinline__ void pair_finish(float2 *d, R *__restrict__ dst, int N, int i, int j,
                                             float s_nu, float u_lid, float2 &ux, float2 &uy,
                                             uint32_t key) {
-    const long long P = (long long)N * N;
-    const long long c = (long long)j * N + i;
+    const int P = N * N;  // 9 N^2 < 2^31 (kb_batch_create)
+    const int c = j * N + i;
     const bool n = j < N - 1;
     const float2 z = make_float2(0.f, 0.f);
     if (!n) {
@@ -645,7 +645,8 @@ int kb_batch_create(kb_batch **out, int n_cases, const int *N, const double *nu,
     b->n_cases = n_cases; b->dtype = dtype; b->device = dev;
     long long fo = 0, mo = 0;
     for (int c = 0; c < n_cases; ++c) {
-        if (N[c] < 2 || N[c] > 46340 || !(nu[c] > 0.0)) {
+        // a case's 9 N^2 population elements are addressed with 32-bit offsets
+        if (N[c] < 2 || N[c] > 15000 || !(nu[c] > 0.0)) {
             delete b;
             return kb::set_error(KB_ERR_ARG, "kb_batch_create: case %d has N=%d nu=%g", c, N[c], nu[c]);
         }
