@@ -239,34 +239,59 @@ __global__ void unpack_k(float *__restrict__ out, const float *__restrict__ pred
     }
 }
 
-// Sum the split-K partials of a weight gradient into the flat gradient array,
-// in a fixed order: part [splits][Rp+1][Cout] (Rp = 9 Cp) -> gW[cout][9 Cs],
-// gb[cout] (row Rp).  With many splits a first pass sums groups of `per`
-// consecutive splits (grid.y = group) into tmp [groups][(Rp+1) Cout] and the
-// second pass sums the groups.  Cp > Cs: the partials carry zero-padded
+// Sum the split-K partials of the weight gradients of all layers into the
+// flat gradient array, in a fixed order, in two launches for the whole
+// network (the gradients are needed only after the backward pass).  Job k:
+// part [splits][Rp+1][Cout] (Rp = 9 Cp, E = (Rp+1) Cout elements) ->
+// gW[cout][9 Cs], gb[cout] (row Rp).  A job with many splits first sums groups
+// of `per` consecutive splits into tmp [groups][E] (wgrad_group_all_k), and
+// the final pass sums the groups.  Cp > Cs: the partials carry zero-padded
 // input channels c >= Cs, which are dropped.
-__global__ void wgrad_group_k(float *__restrict__ tmp, const float *__restrict__ part, int splits, int per,
-                              int E) {
-    const int z0 = blockIdx.y * per, z1 = min(splits, z0 + per);
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+struct RJob {
+    const float *part;
+    float *tmp, *gW, *gb;
+    int splits, groups, per, E, Cp, Cs, cout;
+    long long g_start, r_start;  // first work item of the job in each pass
+};
+constexpr int N_LAYERS_MAX = 16;  // >= N_LAYERS
+static_assert(N_LAYERS <= N_LAYERS_MAX, "job tables hold every layer");
+struct RJobs {
+    RJob j[N_LAYERS_MAX];
+    int n;
+    long long g_total, r_total;
+};
+
+__global__ void wgrad_group_all_k(const RJobs J) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < J.g_total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int k = 0;
+        while (k + 1 < J.n && t >= J.j[k + 1].g_start) ++k;
+        const RJob &b = J.j[k];
+        const int u = (int)(t - b.g_start), g = u / b.E, e = u - g * b.E;
+        const int z0 = g * b.per, z1 = min(b.splits, z0 + b.per);
         float s = 0.f;
-        for (int z = z0; z < z1; ++z) s += part[(size_t)z * E + e];
-        tmp[(size_t)blockIdx.y * E + e] = s;
+        for (int z = z0; z < z1; ++z) s += b.part[(size_t)z * b.E + e];
+        b.tmp[(size_t)g * b.E + e] = s;
     }
 }
 
-__global__ void wgrad_reduce_k(float *__restrict__ gW, float *__restrict__ gb,
-                               const float *__restrict__ part, int splits, int Cp, int Cs, int Cout) {
-    const int Rp = 9 * Cp, n = (Rp + 1) * Cout;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const int r = t / Cout, co = t - r * Cout;
+__global__ void wgrad_reduce_all_k(const RJobs J) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < J.r_total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int k = 0;
+        while (k + 1 < J.n && t >= J.j[k + 1].r_start) ++k;
+        const RJob &b = J.j[k];
+        const int e = (int)(t - b.r_start);
+        const float *src = b.groups > 1 ? b.tmp : b.part;
+        const int nz = b.groups > 1 ? b.groups : b.splits;
         float s = 0.f;
-        for (int z = 0; z < splits; ++z) s += part[((size_t)z * (Rp + 1) + r) * Cout + co];
+        for (int z = 0; z < nz; ++z) s += src[(size_t)z * b.E + e];
+        const int Rp = 9 * b.Cp, r = e / b.cout, co = e - r * b.cout;
         if (r == Rp) {
-            gb[co] = s;
+            b.gb[co] = s;
         } else {
-            const int tap = r / Cp, c = r - tap * Cp;
-            if (c < Cs) gW[((size_t)co * 9 + tap) * Cs + c] = s;
+            const int tap = r / b.Cp, c = r - tap * b.Cp;
+            if (c < b.Cs) b.gW[((size_t)co * 9 + tap) * b.Cs + c] = s;
         }
     }
 }
@@ -287,21 +312,48 @@ __global__ void adam_k(float *__restrict__ p, float *__restrict__ m, float *__re
 
 // W [Cout][9 Cin] FP32 -> wb [Cout][Kp] and wt [Cin][Kpt] BF16 (zero padded):
 //   wt[ci][t*Cout + co] = W[co][(8 - t)*Cin + ci]
-__global__ void pack_k(bf16 *__restrict__ wb, bf16 *__restrict__ wt, const float *__restrict__ W,
-                       int Cin, int Cout, int Kp, int Kpt) {
-    const int n1 = Cout * Kp, n2 = wt ? Cin * Kpt : 0;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n1 + n2; t += gridDim.x * blockDim.x) {
-        if (t < n1) {
-            const int co = t / Kp, k = t - co * Kp;
-            wb[t] = __float2bfloat16_rn(k < 9 * Cin ? W[(size_t)co * 9 * Cin + k] : 0.f);
-        } else {
-            const int u = t - n1, ci = u / Kpt, k = u - ci * Kpt;
+// The BF16 operand copies of every layer's weights in one launch.  Job k:
+// W [Cout][9 Cin] FP32 -> wb [Cout][Kp] and wt [Cin][Kpt] (zero padded):
+//   wt[ci][t*Cout + co] = W[co][(8 - t)*Cin + ci]
+// or, for a padded job (pad = Cp > Cin input channels, no wt):
+//   wb[co][t*Cp + c] = W[co][t*Cin + c] (0 for c >= Cin).
+struct PJob {
+    bf16 *wb, *wt;
+    const float *W;
+    int Cin, Cout, Kp, Kpt, pad;
+    long long start;
+};
+struct PJobs {
+    PJob j[N_LAYERS_MAX + 1];
+    int n;
+    long long total;
+};
+__global__ void pack_all_k(const PJobs J) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < J.total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int k = 0;
+        while (k + 1 < J.n && t >= J.j[k + 1].start) ++k;
+        const PJob &b = J.j[k];
+        const int u0 = (int)(t - b.start), n1 = b.Cout * b.Kp;
+        if (b.pad) {
+            const int co = u0 / b.Kp, kk = u0 - co * b.Kp;
             float x = 0.f;
-            if (k < 9 * Cout) {
-                const int tap = k / Cout, co = k - tap * Cout;
-                x = W[(size_t)co * 9 * Cin + (8 - tap) * Cin + ci];
+            if (kk < 9 * b.pad) {
+                const int tap = kk / b.pad, c = kk - tap * b.pad;
+                if (c < b.Cin) x = b.W[((size_t)co * 9 + tap) * b.Cin + c];
             }
-            wt[u] = __float2bfloat16_rn(x);
+            b.wb[u0] = __float2bfloat16_rn(x);
+        } else if (u0 < n1) {
+            const int co = u0 / b.Kp, kk = u0 - co * b.Kp;
+            b.wb[u0] = __float2bfloat16_rn(kk < 9 * b.Cin ? b.W[(size_t)co * 9 * b.Cin + kk] : 0.f);
+        } else {
+            const int u = u0 - n1, ci = u / b.Kpt, kk = u - ci * b.Kpt;
+            float x = 0.f;
+            if (kk < 9 * b.Cout) {
+                const int tap = kk / b.Cout, co = kk - tap * b.Cout;
+                x = b.W[(size_t)co * 9 * b.Cin + (8 - tap) * b.Cin + ci];
+            }
+            b.wt[u] = __float2bfloat16_rn(x);
         }
     }
 }
@@ -339,21 +391,6 @@ __global__ void pad_input_k(bf16 *__restrict__ dst, const bf16 *__restrict__ src
     }
 }
 
-// W [Cout][9 Cin] FP32 -> wp [Cout][Kp] BF16 for PAD_CH input channels (the
-// padding channels' weights are zero): wp[co][t*PAD_CH + c] = W[co][t*Cin + c].
-__global__ void pack_pad_k(bf16 *__restrict__ wp, const float *__restrict__ W, int Cin, int Cout, int Kp) {
-    const int n = Cout * Kp;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const int co = t / Kp, k = t - co * Kp;
-        float x = 0.f;
-        if (k < 9 * PAD_CH) {
-            const int tap = k / PAD_CH, c = k - tap * PAD_CH;
-            if (c < Cin) x = W[((size_t)co * 9 + tap) * Cin + c];
-        }
-        wp[t] = __float2bfloat16_rn(x);
-    }
-}
-
 inline dim3 ew_grid(long long n) {
     long long b = (n + 255) / 256;
     const long long cap = (long long)kb::sm_count() * 16;
@@ -369,6 +406,7 @@ struct Layer {
     bf16 *wb = nullptr, *wt = nullptr;
     bf16 *dx = nullptr;  // data-gradient output (own buffer for concat inputs)
     bf16 *up = nullptr;  // decoder layers: in1 upsampled to this level (TMA engine)
+    size_t part_off = 0, tmp_off = 0;  // this layer's regions of the weight-gradient buffers
 };
 
 // The TMA engine's operations of one layer for a batch of n images (the maps
@@ -702,7 +740,7 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
         const int sps = (nsteps + want - 1) / want;
         p.wsplits = (nsteps + sps - 1) / sps;
         p.wgroups = ngroups;
-        w.part = s->part;
+        w.part = s->part + l.part_off;
         w.bn = l.bn_w;
         w.ea = ea;
         w.eb = eb;
@@ -741,7 +779,7 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
         if ((rc = nhwc_map(&w.dy, s->grad[l.out], l.cout, W, H, n, eb, b64, what))) return rc;
         int sps = 0;
         p.wsplits = wgrad_splits(l, M, sps);
-        w.part = s->part;
+        w.part = s->part + l.part_off;
         w.bn = l.bn_w;
         w.ea = ea;
         w.eb = eb;
@@ -815,34 +853,45 @@ int forward(kb_surrogate *s, const void *input, int n, cudaStream_t st) {
     return kb::check_launch("kb_surrogate forward");
 }
 
-// Reduce the split partials in s->part of layer l (input channels Cp in the
-// partials) into its gradient.
-int reduce_wgrad(kb_surrogate *s, const Layer &l, int splits, int Cp, cudaStream_t st) {
+// Queue the reduction of layer l's split partials (input channels Cp in the
+// partials) into its gradient; run_reduce_jobs runs the queue.
+void add_reduce_job(kb_surrogate *s, RJobs &J, const Layer &l, int splits, int Cp) {
     const long long E = (long long)(9 * Cp + 1) * l.cout;
-    int groups = 1;
+    int groups = 1, per = splits;
     if (splits >= 16) {
         groups = (int)((300000 + E - 1) / E);
         groups = std::min(groups, splits / 8);
         groups = std::max(groups, 1);
-    }
-    const float *src = s->part;
-    int n = splits;
-    if (groups > 1 && (size_t)(groups * E) <= s->tmp_floats) {
-        const int per = (splits + groups - 1) / groups;
+        per = (splits + groups - 1) / groups;
         groups = (splits + per - 1) / per;
-        dim3 g1(ew_grid(E).x, groups);
-        wgrad_group_k<<<g1, 256, 0, st>>>(s->tmp, s->part, splits, per, (int)E);
-        src = s->tmp;
-        n = groups;
     }
-    wgrad_reduce_k<<<ew_grid(E), 256, 0, st>>>(s->grads + l.w_off, s->grads + l.b_off, src, n, Cp, l.cin,
-                                                 l.cout);
-    return 0;
+    RJob &b = J.j[J.n++];
+    b.part = s->part + l.part_off;
+    b.tmp = s->tmp + l.tmp_off;  // holds 300000 + E floats >= groups E
+    b.gW = s->grads + l.w_off;
+    b.gb = s->grads + l.b_off;
+    b.splits = splits;
+    b.groups = groups;
+    b.per = per;
+    b.E = (int)E;
+    b.Cp = Cp;
+    b.Cs = l.cin;
+    b.cout = l.cout;
+    b.g_start = J.g_total;
+    b.r_start = J.r_total;
+    if (groups > 1) J.g_total += groups * E;
+    J.r_total += E;
+}
+
+void run_reduce_jobs(const RJobs &J, cudaStream_t st) {
+    if (J.g_total) wgrad_group_all_k<<<ew_grid(J.g_total), 256, 0, st>>>(J);
+    if (J.r_total) wgrad_reduce_all_k<<<ew_grid(J.r_total), 256, 0, st>>>(J);
 }
 
 int backward(kb_surrogate *s, int n, cudaStream_t st) {
     using namespace kb::umma;
     const bool tma = engine() == 2;
+    RJobs jobs{};
     if (tma && s->up_batch != n) {
         // the forward pass ran on another engine: upsample the decoder inputs
         // and pad the network input
@@ -876,7 +925,7 @@ int backward(kb_surrogate *s, int n, cudaStream_t st) {
             WgradOp wo{};
             wo.x = xv;
             wo.dy = s->grad[l.out];
-            wo.part = s->part;
+            wo.part = s->part + l.part_off;
             wo.M = M;
             wo.Nout = l.cout;
             wo.bn = l.bn_w;
@@ -885,7 +934,7 @@ int backward(kb_surrogate *s, int n, cudaStream_t st) {
             const dim3 wg((R + 1 + BM - 1) / BM, l.cout / l.bn_w, splits);
             if (int rc = launch(wo, wg, s->err, st)) return rc;
         }
-        if (int rc = reduce_wgrad(s, l, splits, (tma && tp.w) ? tp.cp : l.cin, st)) return rc;
+        add_reduce_job(s, jobs, l, splits, (tma && tp.w) ? tp.cp : l.cin);
         if (i == 0) break;
         // data gradient
         const dim3 grid((M + BM - 1) / BM, l.cin / l.bn_d);
@@ -936,18 +985,40 @@ int backward(kb_surrogate *s, int n, cudaStream_t st) {
                 dec->cin1);
         }
     }
+    run_reduce_jobs(jobs, st);
     return kb::check_launch("kb_surrogate backward");
 }
 
 int repack(kb_surrogate *s, cudaStream_t st) {
+    PJobs J{};
     for (int i = 0; i < N_LAYERS; ++i) {
         const Layer &l = s->L[i];
-        const long long n = (long long)l.cout * l.Kp + (l.wt ? (long long)l.cin * l.Kpt : 0);
-        pack_k<<<ew_grid(n), 256, 0, st>>>(l.wb, l.wt, s->params + l.w_off, l.cin, l.cout, l.Kp, l.Kpt);
+        PJob &b = J.j[J.n++];
+        b.wb = l.wb;
+        b.wt = l.wt;
+        b.W = s->params + l.w_off;
+        b.Cin = l.cin;
+        b.Cout = l.cout;
+        b.Kp = l.Kp;
+        b.Kpt = l.Kpt;
+        b.pad = 0;
+        b.start = J.total;
+        J.total += (long long)l.cout * l.Kp + (l.wt ? (long long)l.cin * l.Kpt : 0);
     }
+    // the first layer's weights for the input padded to PAD_CH channels
     const Layer &l0 = s->L[0];
-    pack_pad_k<<<ew_grid((long long)l0.cout * s->Kp_pad), 256, 0, st>>>(s->wb_pad, s->params + l0.w_off, l0.cin,
-                                                                        l0.cout, s->Kp_pad);
+    PJob &b = J.j[J.n++];
+    b.wb = s->wb_pad;
+    b.wt = nullptr;
+    b.W = s->params + l0.w_off;
+    b.Cin = l0.cin;
+    b.Cout = l0.cout;
+    b.Kp = s->Kp_pad;
+    b.Kpt = 0;
+    b.pad = PAD_CH;
+    b.start = J.total;
+    J.total += (long long)l0.cout * s->Kp_pad;
+    pack_all_k<<<ew_grid(J.total), 256, 0, st>>>(J);
     return kb::check_launch("kb_surrogate repack");
 }
 
@@ -1019,7 +1090,7 @@ int kb_surrogate_create(kb_surrogate **out, int max_batch, int H, int W, int bas
     }
     A((void **)&s->out_f32, pix0 * OUT_CH * sizeof(float));
     A((void **)&s->grad[T_OUT], pix0 * OUT_CH * sizeof(bf16));
-    size_t part = 0;
+    size_t part = 0, tmp = 0;
     for (int i = 0; i < N_LAYERS && !rc; ++i) {
         Layer &l = s->L[i];
         A((void **)&l.wb, (size_t)l.cout * l.Kp * sizeof(bf16));
@@ -1031,15 +1102,21 @@ int kb_surrogate_create(kb_surrogate **out, int max_batch, int H, int W, int bas
         }
         if (l.in2 >= 0) A((void **)&l.up, px * l.cin1 * sizeof(bf16));
         const int cin1 = (l.in1 == T_IN && l.cin1 % 16) ? PAD_CH : l.cin1;
-        size_t need = (size_t)max_wgrad_splits(l) * (9 * (cin1 + l.cin2) + 1) * l.cout;
+        const size_t E = (size_t)(9 * (cin1 + l.cin2) + 1) * l.cout;
+        size_t need = (size_t)max_wgrad_splits(l) * E;
         StripWgradPlan sp{};
         if (plan_strip_wgrad(l, W >> l.level, cin1, sp))
-            need = std::max(need, (size_t)kb::sm_count() * kb::umma::TM_MAX_CPS * (9 * (cin1 + l.cin2) + 1) * l.cout);
-        if (need > part) part = need;
+            need = std::max(need, (size_t)kb::sm_count() * kb::umma::TM_MAX_CPS * E);
+        // every layer's partials and grouped sums have their own region, so
+        // the reductions of all layers run together after the backward pass
+        l.part_off = part;
+        part += (need + 63) & ~(size_t)63;
+        l.tmp_off = tmp;
+        tmp += (300000 + E + 63) & ~(size_t)63;
     }
     s->part_floats = part;
     A((void **)&s->part, part * sizeof(float));
-    s->tmp_floats = 1u << 20;  // grouped sums where groups x (9 Cin + 1) Cout fits, else one pass
+    s->tmp_floats = tmp;
     A((void **)&s->tmp, s->tmp_floats * sizeof(float));
     A((void **)&s->params, (size_t)s->n_params * sizeof(float));
     A((void **)&s->grads, (size_t)s->n_params * sizeof(float));
