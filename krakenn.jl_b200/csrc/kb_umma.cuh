@@ -508,6 +508,57 @@ struct ConvStore {
                 *reinterpret_cast<const uint4 *>(p);
         }
     }
+
+    // The same epilogue with the row's pixel and mask addresses derived once
+    // per tile row (row()) rather than once per 8 columns (store_row()).
+    struct Row {
+        const __nv_bfloat16 *m1, *m2;  // mask channels [0, c1) and [c1, c1 + c2) of the row's pixel
+        size_t o;                      // output offset of the row
+        bool live;
+    };
+    __device__ Row row(int r, const uint3 &t) const {
+        Row R;
+        const int m = t.x * BM + r;
+        R.live = m < M;
+        R.o = (size_t)m * Nout;
+        R.m1 = R.m2 = nullptr;
+        if (mask.s1 && R.live) {
+            int b, h, w;
+            pixel_of(m, mask.H, mask.W, b, h, w);
+            const int Hs = mask.H >> mask.up1, Ws = mask.W >> mask.up1;
+            R.m1 = mask.s1 + (((size_t)b * Hs + (h >> mask.up1)) * Ws + (w >> mask.up1)) * mask.c1;
+            if (mask.s2) R.m2 = mask.s2 + (((size_t)b * mask.H + h) * mask.W + w) * mask.c2;
+        }
+        return R;
+    }
+    __device__ void store_row(const Row &R, int col, const float *v, const uint3 &t) const {
+        if (!R.live) return;
+        const int n = t.y * bn + col;
+        float o[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            float t = v[i] + (bias ? bias[n + i] : 0.f);
+            o[i] = relu ? fmaxf(t, 0.f) : t;
+        }
+        if (mask.s1) {
+            const uint4 mv =
+                __ldg(reinterpret_cast<const uint4 *>(n < mask.c1 ? R.m1 + n : R.m2 + (n - mask.c1)));
+            const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&mv);
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                if (!(__bfloat162float(mb[i]) > 0.f)) o[i] = 0.f;
+        }
+        if (out_f32) {
+            float4 *d = reinterpret_cast<float4 *>((float *)out + R.o + n);
+            d[0] = make_float4(o[0], o[1], o[2], o[3]);
+            d[1] = make_float4(o[4], o[5], o[6], o[7]);
+        } else {
+            __align__(16) __nv_bfloat162 p[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) p[i] = __floats2bfloat162_rn(o[2 * i], o[2 * i + 1]);
+            *reinterpret_cast<uint4 *>((__nv_bfloat16 *)out + R.o + n) = *reinterpret_cast<const uint4 *>(p);
+        }
+    }
 };
 
 // Convolution forward (and data gradient): D[m, n] = sum_k X9[m, k] Wt[n, k],

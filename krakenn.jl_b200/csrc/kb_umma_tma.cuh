@@ -285,15 +285,16 @@ __global__ void __launch_bounds__(TM_THREADS, TM_MAX_CPS)
             const uint3 t = tc.at(T);
             int k0, k1;
             op.k_range(t, k0, k1);
+            const auto R = op.row(row, t);  // per-row state, once per tile
             if (k1 > k0) {
                 for (int c0 = grp * 8; c0 < op.ncols; c0 += 8 * TM_EPI) {
                     float v[8];
                     tmem_ld8(tmem + (uint32_t)buf * cols + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
-                    op.store(row, c0, v, t);
+                    op.store_row(R, c0, v, t);
                 }
             } else {
                 const float z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-                for (int c0 = grp * 8; c0 < op.ncols; c0 += 8 * TM_EPI) op.store(row, c0, z, t);
+                for (int c0 = grp * 8; c0 < op.ncols; c0 += 8 * TM_EPI) op.store_row(R, c0, z, t);
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             mbar_arrive(&acc_empty[buf]);
@@ -545,6 +546,11 @@ struct WgradStrip : TmaBase {
         d[0] = make_float4(v[0], v[1], v[2], v[3]);
         d[1] = make_float4(v[4], v[5], v[6], v[7]);
     }
+    struct Row { int r; };
+    __device__ Row row(int r, const uint3 &) const { return Row{r}; }
+    __device__ void store_row(const Row &R, int col, const float *v, const uint3 &t) const {
+        store(R.r, col, v, t);
+    }
 };
 
 // Weight gradient with TMA-staged operands, split over pixels:
@@ -650,6 +656,11 @@ struct WgradTma : TmaBase {
         d[0] = make_float4(v[0], v[1], v[2], v[3]);
         d[1] = make_float4(v[4], v[5], v[6], v[7]);
     }
+    struct Row { int r; };
+    __device__ Row row(int r, const uint3 &) const { return Row{r}; }
+    __device__ void store_row(const Row &R, int col, const float *v, const uint3 &t) const {
+        store(R.r, col, v, t);
+    }
 };
 
 // Plain GEMM (test of the swizzled layouts): C[M][N] = A B^T in FP32, A
@@ -701,6 +712,11 @@ struct GemmTma : TmaBase {
         float4 *d = reinterpret_cast<float4 *>(c + (size_t)m * N + n);
         d[0] = make_float4(v[0], v[1], v[2], v[3]);
         d[1] = make_float4(v[4], v[5], v[6], v[7]);
+    }
+    struct Row { int r; };
+    __device__ Row row(int r, const uint3 &) const { return Row{r}; }
+    __device__ void store_row(const Row &R, int col, const float *v, const uint3 &t) const {
+        store(R.r, col, v, t);
     }
 };
 
