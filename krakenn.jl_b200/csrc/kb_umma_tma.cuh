@@ -404,15 +404,21 @@ struct ConvTma : ConvStore, TmaBase {
 // MMAs of tap dx read the strip from row dx+1 on: the tensor core applies the
 // swizzle to the absolute shared-memory address, so a start 2e bytes further
 // reads the rows shifted by one pixel.  The layer's weights (9 nck blocks of
-// bn x e, one output-channel tile) are the resident operand.  MMA order (tap,
-// chunk, 16-wide K group) is the order of the other engines.
+// bn x e, one output-channel tile) are the resident operand, in tap, chunk,
+// 16-wide K group order (the other engines' order); or, where that lets more
+// CTAs share an SM, they are streamed: a stage is then one kernel row and one
+// chunk, its strip and the three taps' weight blocks (order row, chunk, tap).
 struct ConvStrip : ConvStore, TmaBase {
     static constexpr bool A_MN = false, B_MN = false;
     CUtensorMap x1, x2, w;
     int e, c1, C, H, W, nck;
+    int streamed;  // 1: weights copied per stage (kernel row dy, chunk) instead of resident
     uint32_t strip_bytes, tx;
 
-    __device__ void k_range(const uint3 &, int &k0, int &k1) const { k0 = 0; k1 = 3; }
+    __device__ void k_range(const uint3 &, int &k0, int &k1) const {
+        k0 = 0;
+        k1 = streamed ? 3 * nck : 3;
+    }
     __device__ uint32_t step_tx(const uint3 &) const { return tx; }
     __device__ void prefetch() const {
         prefetch_map(&x1);
@@ -420,17 +426,33 @@ struct ConvStrip : ConvStore, TmaBase {
         prefetch_map(&w);
     }
     __device__ void issue_res(uint32_t res, uint32_t bar) const {
+        if (streamed) return;
         const uint32_t blk = (uint32_t)(bn * 2 * e);
         for (int j = 0, wk = 0; j < 9 * nck; ++j, wk += e) tma2(res + (uint32_t)j * blk, &w, wk, 0, bar);
     }
-    struct Cursor { int dy, b, y, x; };
+    struct Cursor { int dy, ci, b, y, x; };
     __device__ Cursor begin(const uint3 &t, int) const {
         Cursor u;
         split_pixel((int)t.x * BM, H, W, u.b, u.y, u.x);
         u.dy = -1;
+        u.ci = 0;
         return u;
     }
-    __device__ void issue(Cursor &u, const uint3 &, uint32_t sa, uint32_t, uint32_t bar) const {
+    __device__ void issue(Cursor &u, const uint3 &, uint32_t sa, uint32_t sb, uint32_t bar) const {
+        if (streamed) {
+            // one strip (row y + dy, chunk ci) and the three taps' weight blocks
+            const int c = u.ci * e;
+            if (c < c1) tma4(sa, &x1, c, u.x - 1, u.y + u.dy, u.b, bar);
+            else tma4(sa, &x2, c - c1, u.x - 1, u.y + u.dy, u.b, bar);
+            const uint32_t blk = (uint32_t)(bn * 2 * e);
+            const int wk0 = (u.dy + 1) * 3 * C + c;  // tap (dy + 1) * 3 + (dx + 1)
+            for (int dx = 0; dx < 3; ++dx) tma2(sb + (uint32_t)dx * blk, &w, wk0 + dx * C, 0, bar);
+            if (++u.ci == nck) {
+                u.ci = 0;
+                ++u.dy;
+            }
+            return;
+        }
         uint32_t dst = sa;
         for (int ci = 0, c = 0; ci < nck; ++ci, c += e, dst += strip_bytes) {
             if (c < c1) tma4(dst, &x1, c, u.x - 1, u.y + u.dy, u.b, bar);
@@ -438,9 +460,17 @@ struct ConvStrip : ConvStore, TmaBase {
         }
         ++u.dy;
     }
-    __device__ void mma(uint32_t acc, uint32_t sa, uint32_t, uint32_t res, int kt, int, const uint3 &,
+    __device__ void mma(uint32_t acc, uint32_t sa, uint32_t sb, uint32_t res, int kt, int, const uint3 &,
                         uint32_t idesc) const {
         const uint32_t S = 2u * (uint32_t)e, blk = (uint32_t)bn * S;
+        if (streamed) {
+            for (int dx = 0; dx < 3; ++dx)
+                for (int kk = 0; kk < e / 16; ++kk)
+                    mma_bf16(acc, op_desc(sa + (uint32_t)dx * S, false, S, kk),
+                             op_desc(sb + (uint32_t)dx * blk, false, S, kk), idesc,
+                             (kt == 0 && dx == 0 && kk == 0) ? 0u : 1u);
+            return;
+        }
         uint32_t wb = res + (uint32_t)(kt * 3 * nck) * blk;  // tap kt*3 + dx
         for (int dx = 0; dx < 3; ++dx)
             for (int ci = 0; ci < nck; ++ci, wb += blk) {
