@@ -172,27 +172,46 @@ __global__ void skip_grad_k(bf16 *__restrict__ dst, const bf16 *__restrict__ dca
 // L to *loss.
 struct Norm { float scale[3], offset[3]; };
 
-__device__ __forceinline__ float loss_err(const float *__restrict__ pred, const float *__restrict__ target,
-                                          const Norm &nm, int b, int p, int c, int HW) {
-    const float t = (target[((size_t)b * 3 + c) * HW + p] - nm.offset[c]) * nm.scale[c];
-    return pred[((size_t)b * HW + p) * OUT_CH + c] - t;
-}
-
-__global__ void loss_k(bf16 *__restrict__ grad, float *__restrict__ loss, const float *__restrict__ pred,
-                       const float *__restrict__ target, Norm nm, int M, int H, int W, float gw) {
-    __shared__ float red[8];
-    float acc = 0.f;
-    const int HW = H * W;
+// One block per tile of LTX x LTY pixels of one image (grid x, y, image): the
+// errors of the tile and its one-pixel halo are computed once into shared
+// memory, then each pixel forms its loss terms and gradient from them.
+constexpr int LTX = 32, LTY = 8;
+__global__ void __launch_bounds__(LTX *LTY) loss_k(bf16 *__restrict__ grad, float *__restrict__ loss,
+                                                   const float *__restrict__ pred,
+                                                   const float *__restrict__ target, Norm nm, int M, int H,
+                                                   int W, float gw) {
+    __shared__ float E[3][LTY + 2][LTX + 2];
+    __shared__ float red[LTX * LTY / 32];
+    const int HW = H * W, b = blockIdx.z;
+    const int x0 = blockIdx.x * LTX, y0 = blockIdx.y * LTY;
     const float gs = 2.0f / (3.0f * (float)M);
-    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
-        const int b = m / HW, p = m - b * HW;
-        const int y = p / W, x = p - y * W;
+    for (int u = threadIdx.x; u < (LTX + 2) * (LTY + 2); u += LTX * LTY) {
+        const int ly = u / (LTX + 2), lx = u - ly * (LTX + 2);
+        const int x = x0 + lx - 1, y = y0 + ly - 1;
+        float e0 = 0.f, e1 = 0.f, e2 = 0.f;
+        if (x >= 0 && x < W && y >= 0 && y < H) {
+            const int p = y * W + x;
+            const float4 pr = *reinterpret_cast<const float4 *>(pred + ((size_t)b * HW + p) * OUT_CH);
+            const float *tg = target + (size_t)b * 3 * HW + p;
+            e0 = pr.x - (tg[0] - nm.offset[0]) * nm.scale[0];
+            e1 = pr.y - (tg[HW] - nm.offset[1]) * nm.scale[1];
+            e2 = pr.z - (tg[2 * HW] - nm.offset[2]) * nm.scale[2];
+        }
+        E[0][ly][lx] = e0;
+        E[1][ly][lx] = e1;
+        E[2][ly][lx] = e2;
+    }
+    __syncthreads();
+    const int tx = threadIdx.x % LTX, ty = threadIdx.x / LTX;
+    const int x = x0 + tx, y = y0 + ty;
+    float acc = 0.f;
+    if (x < W && y < H) {
         __align__(16) bf16 g[OUT_CH];
 #pragma unroll
         for (int c = 0; c < OUT_CH; ++c) g[c] = __float2bfloat16_rn(0.f);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const float e = loss_err(pred, target, nm, b, p, c, HW);
+            const float e = E[c][ty + 1][tx + 1];
             acc += e * e;
             float d = e;
             if (gw != 0.f) {
@@ -200,22 +219,22 @@ __global__ void loss_k(bf16 *__restrict__ grad, float *__restrict__ loss, const 
                 // gradient collects the differences with all four neighbours
                 float lap = 0.f;
                 if (x + 1 < W) {
-                    const float en = loss_err(pred, target, nm, b, p + 1, c, HW);
+                    const float en = E[c][ty + 1][tx + 2];
                     acc += gw * (en - e) * (en - e);
                     lap += e - en;
                 }
                 if (y + 1 < H) {
-                    const float en = loss_err(pred, target, nm, b, p + W, c, HW);
+                    const float en = E[c][ty + 2][tx + 1];
                     acc += gw * (en - e) * (en - e);
                     lap += e - en;
                 }
-                if (x > 0) lap += e - loss_err(pred, target, nm, b, p - 1, c, HW);
-                if (y > 0) lap += e - loss_err(pred, target, nm, b, p - W, c, HW);
+                if (x > 0) lap += e - E[c][ty + 1][tx];
+                if (y > 0) lap += e - E[c][ty][tx + 1];
                 d += gw * lap;
             }
             g[c] = __float2bfloat16_rn(gs * d);
         }
-        uint4 *dst = reinterpret_cast<uint4 *>(grad + (size_t)m * OUT_CH);
+        uint4 *dst = reinterpret_cast<uint4 *>(grad + ((size_t)b * HW + (size_t)y * W + x) * OUT_CH);
         dst[0] = reinterpret_cast<const uint4 *>(g)[0];
         dst[1] = reinterpret_cast<const uint4 *>(g)[1];
     }
@@ -224,7 +243,7 @@ __global__ void loss_k(bf16 *__restrict__ grad, float *__restrict__ loss, const 
     __syncthreads();
     if (threadIdx.x == 0) {
         float sum = 0.f;
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) sum += red[i];
+        for (int i = 0; i < LTX * LTY / 32; ++i) sum += red[i];
         atomicAdd(loss, sum / (3.0f * (float)M));
     }
 }
@@ -649,6 +668,7 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
         c.bn = l.bn_f;
         c.relu = l.relu;
         c.out_f32 = l.out == T_OUT;
+        c.store_cols = l.out == T_OUT ? 8 : 0;  // the head: the loss and unpacking read channels 0-2
         p.f = 2;
     } else if (ef && g128) {
         ConvTma &c = p.fwd;
@@ -681,6 +701,7 @@ int prepare_tma(kb_surrogate *s, int i, int n) {
         c.bn = l.bn_f;
         c.relu = l.relu;
         c.out_f32 = l.out == T_OUT;
+        c.store_cols = l.out == T_OUT ? 8 : 0;  // the head: the loss and unpacking read channels 0-2
         p.f = c.cps ? 1 : 0;
     }
     // data gradient: row strips, or boxes of e output-gradient channels
@@ -1282,8 +1303,9 @@ int kb_surrogate_loss_backward(kb_surrogate *s, const void *input, const float *
     if (int rc = forward(s, input, n, st)) return rc;
     const int M = n * s->H * s->W;
     cudaMemsetAsync(s->loss, 0, sizeof(float), st);
-    loss_k<<<ew_grid(M), 256, 0, st>>>(s->grad[T_OUT], s->loss, s->out_f32, target, s->norm, M,
-                                        s->H, s->W, s->grad_weight);
+    const dim3 lg((s->W + LTX - 1) / LTX, (s->H + LTY - 1) / LTY, n);
+    loss_k<<<lg, LTX * LTY, 0, st>>>(s->grad[T_OUT], s->loss, s->out_f32, target, s->norm, M, s->H, s->W,
+                                     s->grad_weight);
     if (int rc = backward(s, n, st)) return rc;
     if (loss_out) cudaMemcpyAsync(loss_out, s->loss, sizeof(float), cudaMemcpyDeviceToDevice, st);
     return kb::check_launch("kb_surrogate_loss_backward");

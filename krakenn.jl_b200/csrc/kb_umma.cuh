@@ -476,6 +476,7 @@ struct ConvStore {
     ActView mask;       // mask.s1 == null: no mask
     void *out;          // [M][Nout] BF16 or FP32
     int M, Nout, bn, relu, out_f32;
+    int store_cols;     // store_row(): output columns written (0: all); the rest nobody reads
 
     __device__ void store(int row, int col, const float *v, const uint3 &t) const {
         const int m = t.x * BM + row;
@@ -532,8 +533,8 @@ struct ConvStore {
         return R;
     }
     __device__ void store_row(const Row &R, int col, const float *v, const uint3 &t) const {
-        if (!R.live) return;
         const int n = t.y * bn + col;
+        if (!R.live || (store_cols && n >= store_cols)) return;
         float o[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
