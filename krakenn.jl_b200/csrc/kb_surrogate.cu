@@ -64,12 +64,12 @@ __host__ __device__ inline int round_up(int a, int b) { return (a + b - 1) / b *
 __global__ void pool_k(bf16 *__restrict__ out, const bf16 *__restrict__ in, int B, int Ho, int Wo,
                        int C) {
     const int cc = C / 8;
-    const long long n = (long long)B * Ho * Wo * cc;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(t % cc) * 8;
-        const long long p = t / cc;
-        const int w = (int)(p % Wo), h = (int)((p / Wo) % Ho), b = (int)(p / ((long long)Wo * Ho));
+    const unsigned n = (unsigned)B * Ho * Wo * cc;  // < 2^31 (kb_surrogate_create)
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const unsigned p = t / cc;
+        const int c = (int)(t - p * cc) * 8;
+        const unsigned r = p / Wo, b = r / Ho;
+        const int w = (int)(p - r * Wo), h = (int)(r - b * Ho);
         float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         for (int dy = 0; dy < 2; ++dy)
             for (int dx = 0; dx < 2; ++dx) {
@@ -91,12 +91,12 @@ __global__ void pool_k(bf16 *__restrict__ out, const bf16 *__restrict__ in, int 
 __global__ void upsample_k(bf16 *__restrict__ dst, const bf16 *__restrict__ src, int B, int H, int W,
                            int C) {
     const int cc = C / 8;
-    const long long n = (long long)B * H * W * cc;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(t % cc) * 8;
-        const long long p = t / cc;
-        const int w = (int)(p % W), h = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
+    const unsigned n = (unsigned)B * H * W * cc;  // < 2^31 (kb_surrogate_create)
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const unsigned p = t / cc;
+        const int c = (int)(t - p * cc) * 8;
+        const unsigned r = p / W, b = r / H;
+        const int w = (int)(p - r * W), h = (int)(r - b * H);
         const size_t q = (((size_t)b * (H / 2) + h / 2) * (W / 2) + w / 2) * C + c;
         *reinterpret_cast<uint4 *>(dst + (size_t)p * C + c) = *reinterpret_cast<const uint4 *>(src + q);
     }
@@ -107,12 +107,12 @@ __global__ void upsample_k(bf16 *__restrict__ dst, const bf16 *__restrict__ src,
 __global__ void upsum_k(bf16 *__restrict__ dst, const bf16 *__restrict__ src, int B, int Hl, int Wl,
                         int Cl, int Cs) {
     const int cc = Cl / 8;
-    const long long n = (long long)B * Hl * Wl * cc;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(t % cc) * 8;
-        const long long p = t / cc;
-        const int w = (int)(p % Wl), h = (int)((p / Wl) % Hl), b = (int)(p / ((long long)Wl * Hl));
+    const unsigned n = (unsigned)B * Hl * Wl * cc;  // < 2^31 (kb_surrogate_create)
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const unsigned p = t / cc;
+        const int c = (int)(t - p * cc) * 8;
+        const unsigned r = p / Wl, b = r / Hl;
+        const int w = (int)(p - r * Wl), h = (int)(r - b * Hl);
         float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         for (int dy = 0; dy < 2; ++dy)
             for (int dx = 0; dx < 2; ++dx) {
@@ -137,12 +137,12 @@ __global__ void skip_grad_k(bf16 *__restrict__ dst, const bf16 *__restrict__ dca
                             const bf16 *__restrict__ dpool, const bf16 *__restrict__ S, int B, int H,
                             int W, int C, int Cc, int off) {
     const int cc = C / 8;
-    const long long n = (long long)B * H * W * cc;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(t % cc) * 8;
-        const long long p = t / cc;
-        const int w = (int)(p % W), h = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
+    const unsigned n = (unsigned)B * H * W * cc;  // < 2^31 (kb_surrogate_create)
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const unsigned p = t / cc;
+        const int c = (int)(t - p * cc) * 8;
+        const unsigned r = p / W, b = r / H;
+        const int w = (int)(p - r * W), h = (int)(r - b * H);
         const size_t pp = (((size_t)b * (H / 2) + h / 2) * (W / 2) + w / 2) * C + c;
         const uint4 a = *reinterpret_cast<const uint4 *>(dcat + (size_t)p * Cc + off + c);
         const uint4 g = *reinterpret_cast<const uint4 *>(dpool + pp);
@@ -1081,6 +1081,11 @@ int kb_surrogate_create(kb_surrogate **out, int max_batch, int H, int W, int bas
     KB_REQUIRE(base_channels >= 16 && base_channels % 16 == 0 && base_channels <= 128,
                "kb_surrogate_create: base_channels=%d must be a multiple of 16 in [16, 128]",
                base_channels);
+    // the elementwise kernels index 8-channel chunks of an activation with 32
+    // bits: no tensor has more than 12 base_channels channels
+    KB_REQUIRE((double)max_batch * H * W * (12.0 * base_channels / 8) < 2147483647.0,
+               "kb_surrogate_create: max_batch x H x W = %d x %d x %d too large for %d base channels",
+               max_batch, H, W, base_channels);
     cudaStream_t st = kb::as_stream(stream);
     kb_surrogate *s = new kb_surrogate();
     s->Bmax = max_batch;
