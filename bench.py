@@ -296,7 +296,9 @@ def _cpu_sample(n, nz, steps, warmup, precision, threads):
 
 
 def run_reference(args):
-    rank, world, _ = dist_setup(args.gpus)
+    # the reference arm runs no collectives: rank 0 times the CPU path, the
+    # other ranks of a torchrun launch exit at once without joining a group
+    rank, world = _env_int("RANK", 0), _env_int("WORLD_SIZE", 1)
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
