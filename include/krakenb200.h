@@ -476,8 +476,10 @@ int kb_fused_trt_step_3d_zrange(void *f_out, const void *f_in, void *rho, void *
  * 2-element vector accesses (even Nx), 4 adjacent node quads with 8-byte accesses
  * (16-bit storages, Nx % 4 == 0), 5 persistent row tiles of 256 nodes whose
  * pull source rows are staged in shared memory by tensor-memory-accelerator
- * copies (16-bit storages, Nx % 8 == 0, 16-byte aligned populations).
- * Variants 2 to 5 collide in packed FP32x2 arithmetic.
+ * copies (16-bit storages, Nx % 8 == 0, 16-byte aligned populations; two
+ * rows per tile where Ny is even and the offsets fit in 32 bits), 6 the
+ * staged kernel with one row per tile.  Variants 2 to 6 collide in packed
+ * FP32x2 arithmetic.
  * kernel 2 = the tensor-core engine of the warm-start network and
  * kb_gemm_bf16: 0 warp-specialised persistent kernel with cp.async operand
  * staging, 1 one CTA per output tile with cp.async staging, 2 (default)

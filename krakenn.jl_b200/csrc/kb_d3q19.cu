@@ -688,7 +688,7 @@ int kb_set_kernel_variant(int kernel, int variant) {
         kb::umma::set_engine(variant);
         return KB_OK;
     }
-    KB_REQUIRE(variant >= 0 && variant <= 5, "kb_set_kernel_variant: variant %d not in 0..5", variant);
+    KB_REQUIRE(variant >= 0 && variant <= 6, "kb_set_kernel_variant: variant %d not in 0..6", variant);
     g_trt3d_dev_variant = variant;
     return KB_OK;
 }

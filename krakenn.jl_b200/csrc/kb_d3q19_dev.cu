@@ -656,9 +656,10 @@ __global__ void __launch_bounds__(128, KB_QUAD_MIN_BLOCKS) trt_dev_v4_k(R *__res
 
 // ---------------------------------------------------------------------------
 // Row tiles staged by the tensor memory accelerator (16-bit storages).
-// A persistent block walks tiles of TT = 256 nodes along x (one row segment
-// at fixed y, z).  A producer warp streams each tile's pull sources into a
-// ring of TSTAGES shared-memory stages with cp.async.bulk.tensor copies,
+// A persistent block walks tiles of TT = 256 nodes along x (a row segment at
+// fixed z, in TY = 1 or 2 consecutive rows).  A producer warp streams each
+// tile's pull sources into a ring of shared-memory stages with
+// cp.async.bulk.tensor copies,
 // each stage completed by a "full" mbarrier transaction count: for every
 // population q the 256-element run of plane q at the pull source row
 // (y - c_y, z - c_z), wrapped on periodic axes (13 copies: populations that
@@ -679,15 +680,26 @@ __global__ void __launch_bounds__(128, KB_QUAD_MIN_BLOCKS) trt_dev_v4_k(R *__res
 // Needs Nx % 8 == 0 and 16-byte aligned populations (tensor-map rules).
 constexpr int TT = 256;                 // nodes per row tile
 constexpr int THALO = 64;               // halo slot stride (elements, 128 bytes)
-constexpr int TSTAGES = 4;
 constexpr int TCONS = TT / 2;           // consumer threads: one per adjacent node pair
 constexpr int TTHREADS = TCONS + 32;    // + the producer warp
-constexpr int TCLS = 19 * TT + 10 * THALO;     // element offset of the class-byte run (cut-link steps)
-constexpr int TSTAGE = TCLS + TT / 2;           // elements per stage (row q at q * TT)
-constexpr size_t TSMEM = 128 + (size_t)TSTAGES * TSTAGE * 2;  // + alignment slack
-constexpr uint32_t TROWBYTES = 19u * TT * 2u;                 // the 19 row runs of a tile
-constexpr uint32_t TBYTES = TROWBYTES + 10u * 8u * 2u;           // + the 10 halo runs
 constexpr long long TWAIT = 4000000;    // bounded mbarrier wait (polls)
+
+// Stage layout of a tile of TY rows (y = j0 .. j0 + TY - 1): population q of
+// row r at element (q * TY + r) * TT, then the halo slots of THALO elements
+// (slot e of row r at (e * TY + r) * THALO: a tensor copy lands on a
+// 128-byte boundary, so each halo row has a slot and a copy of its own),
+// then the rows' class bytes of a cut-link step.  Two-row tiles halve the
+// row copies and the per-tile work of the consumers per node; their stages
+// are twice as large, so the ring holds 3 of them (3 blocks per SM fit in
+// shared memory either way).
+template <int TY> struct TileGeom {
+    static constexpr int STAGES = TY == 1 ? 4 : 3;
+    static constexpr int CLS = 19 * TT * TY + 10 * TY * THALO;  // element offset of the class bytes
+    static constexpr int STAGE = CLS + TT * TY / 2;        // elements per stage
+    static constexpr size_t SMEM = 128 + (size_t)STAGES * STAGE * 2;  // + alignment slack
+    static constexpr uint32_t ROWBYTES = 19u * TT * 2u * TY;         // the 19 row runs
+    static constexpr uint32_t BYTES = ROWBYTES + 10u * 8u * 2u * TY;  // + the 10 halo runs
+};
 
 #ifndef KB_TMA_MIN_BLOCKS
 #define KB_TMA_MIN_BLOCKS 3
@@ -730,30 +742,33 @@ __device__ __forceinline__ void tma_load4(uint32_t dst, const CUtensorMap *tm, i
         : "memory");
 }
 
-// Tiles are numbered x-segment fastest, then y, then z.  A block visits
-// tiles b, b + G, b + 2G, ... (G = grid size); a cursor (xt, j, k) advances
-// by G without a division per tile.  staged() says whether every pull
-// source row of a tile exists (interior or wrapped), i.e. it is staged.
-struct TileMap {
+// Tiles are numbered x-segment fastest, then row group (TY rows), then z.
+// A block visits tiles b, b + G, b + 2G, ... (G = grid size); a cursor
+// (xt, jt, k) advances by G without a division per tile (jt counts row
+// groups: rows jt * TY .. jt * TY + TY - 1).  staged() says whether every
+// pull source row of a tile exists (interior or wrapped), i.e. it is staged.
+template <int TY> struct TileMap {
     int ntx, Nx, Ny, Nz, per, zoff;
-    int dx, dj, dk;  // G decomposed as (x-segments, rows, planes)
+    int nyt;         // row groups per plane: Ny / TY
+    int dx, dj, dk;  // G decomposed as (x-segments, row groups, planes)
     __device__ __forceinline__ void at(int t, int &xt, int &j, int &k) const {
         xt = t % ntx;
         const int r = t / ntx;
-        j = r % Ny;
-        k = r / Ny;
+        j = r % nyt;
+        k = r / nyt;
     }
     __device__ __forceinline__ void advance(int &xt, int &j, int &k) const {
         xt += dx;
         int c = xt >= ntx;
         xt -= c ? ntx : 0;
         j += dj + c;
-        c = j >= Ny;
-        j -= c ? Ny : 0;
+        c = j >= nyt;
+        j -= c ? nyt : 0;
         k += dk + c;
     }
-    __device__ __forceinline__ bool staged(int j, int k) const {
-        return ((per & 2) || (j > 0 && j < Ny - 1)) && ((per & (4 | KB_ZHALO)) || (k > 0 && k < Nz - 1));
+    __device__ __forceinline__ bool staged(int jt, int k) const {
+        const int j0 = jt * TY;
+        return ((per & 2) || (j0 > 0 && j0 + TY < Ny)) && ((per & (4 | KB_ZHALO)) || (k > 0 && k < Nz - 1));
     }
 };
 
@@ -761,8 +776,10 @@ struct TileMap {
 // Maps: t1 / t2 / t3 copy 1 / 2 / 3 consecutive planes of a 256-element
 // row run, th an 8-element halo run of one plane.
 struct TileMaps {
-    const CUtensorMap *t1, *t2, *t3, *th;
-    const CUtensorMap *tc;  // the row's class bytes of a cut-link table, or null
+    const CUtensorMap *t1, *t2, *t3;  // boxes of TY rows
+    const CUtensorMap *th;  // one halo row
+    const CUtensorMap *tc;  // the rows' class bytes of a cut-link table, or null
+    const CUtensorMap *s1;  // one row of one plane (wrapped row groups)
 };
 __device__ __forceinline__ void tma_load3(uint32_t dst, const CUtensorMap *tm, int x, int y, int z,
                                           uint32_t bar) {
@@ -772,9 +789,16 @@ __device__ __forceinline__ void tma_load3(uint32_t dst, const CUtensorMap *tm, i
         "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(bar)
         : "memory");
 }
+// The copies of one staged tile of TY rows j .. j + TY - 1.  The source rows
+// of a population with c_y = +1 / -1 are ym .. / yp .. (wrapped); a group
+// whose rows would run past Ny - 1 (only where y wraps: row group 0 for
+// c_y = +1, the last one for c_y = -1) travels as one copy per row and plane.
+// Halo runs travel one row per copy.
+template <int TY>
 __device__ __forceinline__ void tma_issue_tile(const TileMaps &mp, uint32_t dst, uint32_t bar,
-                                               int x0, int j, int k, const TileMap &m, bool halos) {
-    const uint32_t bytes = (halos ? TBYTES : TROWBYTES) + (mp.tc ? (uint32_t)TT : 0u);
+                                               int x0, int j, int k, const TileMap<TY> &m, bool halos) {
+    using G = TileGeom<TY>;
+    const uint32_t bytes = (halos ? G::BYTES : G::ROWBYTES) + (mp.tc ? (uint32_t)(TT * TY) : 0u);
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                  : "memory");
     // tensor-map z coordinates: the map spans the whole allocation, this
@@ -784,38 +808,56 @@ __device__ __forceinline__ void tma_issue_tile(const TileMaps &mp, uint32_t dst,
     const int zm = ((k > 0 || zh) ? k - 1 : m.Nz - 1) + m.zoff;
     const int zp = ((k < m.Nz - 1 || zh) ? k + 1 : 0) + m.zoff;
     k += m.zoff;
-    if (mp.tc) tma_load3(dst + TCLS * 2, mp.tc, x0, j, k, bar);  // own row's class bytes
+    if (mp.tc) tma_load3(dst + G::CLS * 2, mp.tc, x0, j, k, bar);  // own rows' class bytes
     const uint32_t R = TT * 2;  // bytes per staged row
-    tma_load4(dst + 0 * R, mp.t3, x0, j, k, 0, bar);     // q 0, 1, 2: (0, 0)
-    tma_load4(dst + 3 * R, mp.t1, x0, ym, k, 3, bar);    // q 3: c_y = +1
-    tma_load4(dst + 4 * R, mp.t1, x0, yp, k, 4, bar);    // q 4: c_y = -1
-    tma_load4(dst + 5 * R, mp.t1, x0, j, zm, 5, bar);    // q 5: c_z = +1
-    tma_load4(dst + 6 * R, mp.t1, x0, j, zp, 6, bar);    // q 6: c_z = -1
-    tma_load4(dst + 7 * R, mp.t2, x0, ym, k, 7, bar);    // q 7, 8: c_y = +1
-    tma_load4(dst + 9 * R, mp.t2, x0, yp, k, 9, bar);    // q 9, 10: c_y = -1
-    tma_load4(dst + 11 * R, mp.t2, x0, j, zm, 11, bar);  // q 11, 12: c_z = +1
-    tma_load4(dst + 13 * R, mp.t2, x0, j, zp, 13, bar);  // q 13, 14: c_z = -1
-    tma_load4(dst + 15 * R, mp.t1, x0, ym, zm, 15, bar); // q 15: (+1, +1)
-    tma_load4(dst + 16 * R, mp.t1, x0, yp, zm, 16, bar); // q 16: (-1, +1)
-    tma_load4(dst + 17 * R, mp.t1, x0, ym, zp, 17, bar); // q 17: (+1, -1)
-    tma_load4(dst + 18 * R, mp.t1, x0, yp, zp, 18, bar); // q 18: (-1, -1)
+    // populations q0 .. q0 + nq - 1, row 0 sourced from row y of plane z
+    const auto rows = [&](const CUtensorMap *tm, int q0, int nq, int y, int z) {
+        if (TY == 1 || y + TY <= m.Ny) {
+            tma_load4(dst + (uint32_t)(q0 * TY) * R, tm, x0, y, z, q0, bar);
+        } else {
+            for (int q = q0; q < q0 + nq; ++q)
+                for (int r = 0; r < TY; ++r)
+                    tma_load4(dst + (uint32_t)(q * TY + r) * R, mp.s1, x0, y + r < m.Ny ? y + r : y + r - m.Ny,
+                              z, q, bar);
+        }
+    };
+    rows(mp.t3, 0, 3, j, k);     // q 0, 1, 2: (0, 0)
+    rows(mp.t1, 3, 1, ym, k);    // q 3: c_y = +1
+    rows(mp.t1, 4, 1, yp, k);    // q 4: c_y = -1
+    rows(mp.t1, 5, 1, j, zm);    // q 5: c_z = +1
+    rows(mp.t1, 6, 1, j, zp);    // q 6: c_z = -1
+    rows(mp.t2, 7, 2, ym, k);    // q 7, 8: c_y = +1
+    rows(mp.t2, 9, 2, yp, k);    // q 9, 10: c_y = -1
+    rows(mp.t2, 11, 2, j, zm);   // q 11, 12: c_z = +1
+    rows(mp.t2, 13, 2, j, zp);   // q 13, 14: c_z = -1
+    rows(mp.t1, 15, 1, ym, zm);  // q 15: (+1, +1)
+    rows(mp.t1, 16, 1, yp, zm);  // q 16: (-1, +1)
+    rows(mp.t1, 17, 1, ym, zp);  // q 17: (+1, -1)
+    rows(mp.t1, 18, 1, yp, zp);  // q 18: (-1, -1)
     if (!halos) return;  // a periodic row in one tile: the wrap sources are in the rows
-    // halos: slot e (left, c_x = +1) and 5 + e (right, c_x = -1).  At an x
-    // wall the slot holds the end node's own opposite population from its
-    // own row (node 0 at slot position 0, node Nx - 1 at position 7).
+    // halos: slot e (left, c_x = +1) and 5 + e (right, c_x = -1) of row r at
+    // (slot * TY + r) * THALO.  At an x wall the slot holds the end node's
+    // own opposite population from its own row (node 0 at slot position 0,
+    // node Nx - 1 at position 7).
     const bool px = m.per & 1;
-    const uint32_t hdst = dst + 19 * R;
+    const uint32_t hdst = dst + 19 * TY * R;
     const bool lwall = x0 == 0 && !px, rwall = x0 + TT >= m.Nx && !px;
     const int xl = lwall ? 0 : (x0 > 0 ? x0 - 8 : m.Nx - 8);       // x0 - 1 (or Nx - 1) at 7
     const int xr = rwall ? m.Nx - 8 : (x0 + TT < m.Nx ? x0 + TT : 0); // next column (or 0) at 0
+    const auto halo = [&](int slot, int x, int y, int z, int q) {
+#pragma unroll
+        for (int r = 0; r < TY; ++r)
+            tma_load4(hdst + (uint32_t)((slot * TY + r) * THALO * 2), mp.th, x,
+                      y + r < m.Ny ? y + r : y + r - m.Ny, z, q, bar);
+    };
 #pragma unroll
     for (int e = 0; e < 5; ++e) {
         const int yl = lwall ? j : (kEY[e] > 0 ? ym : kEY[e] < 0 ? yp : j);
         const int zl = lwall ? k : (kEZ[e] > 0 ? zm : kEZ[e] < 0 ? zp : k);
         const int yr = rwall ? j : (kEY[e] > 0 ? yp : kEY[e] < 0 ? ym : j);
         const int zr = rwall ? k : (kEZ[e] > 0 ? zp : kEZ[e] < 0 ? zm : k);
-        tma_load4(hdst + (uint32_t)(e * THALO * 2), mp.th, xl, yl, zl, lwall ? kQM[e] : kQP[e], bar);
-        tma_load4(hdst + (uint32_t)((5 + e) * THALO * 2), mp.th, xr, yr, zr, rwall ? kQP[e] : kQM[e], bar);
+        halo(e, xl, yl, zl, lwall ? kQM[e] : kQP[e]);
+        halo(5 + e, xr, yr, zr, rwall ? kQP[e] : kQM[e]);
     }
 }
 
@@ -858,31 +900,36 @@ __global__ void __launch_bounds__(BX) trt_dev_cut_k(R *__restrict__ fo, const R 
 }
 
 // LINKS: the compact cut-link table (row f1) in place of a solid mask: class
-// 1 nodes are solid; class 2 nodes are left to trt_dev_cut_k.
-template <typename R, bool MOM, bool SOLID, typename I, bool SR, bool LINKS = false>
+// 1 nodes are solid; class 2 nodes are left to trt_dev_cut_k.  TY: rows per
+// tile (1, or 2 for an even Ny); a consumer thread updates its pair of
+// nodes in each of the tile's rows in turn.
+template <typename R, bool MOM, bool SOLID, typename I, bool SR, bool LINKS = false, int TY = 1>
 __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
     trt_dev_tma_k(const __grid_constant__ CUtensorMap tmap1, const __grid_constant__ CUtensorMap tmap2,
                   const __grid_constant__ CUtensorMap tmap3, const __grid_constant__ CUtensorMap thalo,
-                  const __grid_constant__ CUtensorMap tcls,
+                  const __grid_constant__ CUtensorMap tcls, const __grid_constant__ CUtensorMap ts1,
                   R *__restrict__ fo, const R *__restrict__ fi, float *__restrict__ rho_o,
                   float *__restrict__ ux_o, float *__restrict__ uy_o, float *__restrict__ uz_o,
                   const uint8_t *__restrict__ solid, Grid3 g, float sp, float sm, LinkTable3 L) {
     constexpr bool HS = SOLID || LINKS;  // some nodes are solid
     constexpr int CX[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+    using G = TileGeom<TY>;
+    constexpr int NS = G::STAGES;
     extern __shared__ unsigned char tsm_raw[];
-    __shared__ __align__(8) uint64_t full[TSTAGES], empty[TSTAGES];
+    __shared__ __align__(8) uint64_t full[NS], empty[NS];
     R *stage0 = reinterpret_cast<R *>(tsm_raw + ((128u - (s_addr(tsm_raw) & 127u)) & 127u));
     const int t = threadIdx.x;
-    TileMap m;
+    TileMap<TY> m;
     m.ntx = (g.Nx + TT - 1) / TT;
     m.Nx = g.Nx;
     m.Ny = g.Ny;
+    m.nyt = g.Ny / TY;
     m.Nz = g.Nz;
     m.per = g.per;
     m.zoff = g.zoff;
     m.at((int)gridDim.x, m.dx, m.dj, m.dk);
     if (t == 0) {
-        for (int s = 0; s < TSTAGES; ++s) {
+        for (int s = 0; s < NS; ++s) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s_addr(&full[s])));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_addr(&empty[s])),
                          "r"(TCONS / 32));
@@ -895,7 +942,7 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
 
     if (t >= TCONS) {
         // ------------------------------------------------ producer warp --
-        const TileMaps mp{&tmap1, &tmap2, &tmap3, &thalo, LINKS ? &tcls : nullptr};
+        const TileMaps mp{&tmap1, &tmap2, &tmap3, &thalo, LINKS ? &tcls : nullptr, &ts1};
         if (t == TCONS) {
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap1)) : "memory");
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap2)) : "memory");
@@ -903,26 +950,29 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&thalo)) : "memory");
             if (LINKS)
                 asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tcls)) : "memory");
+            if (TY > 1)
+                asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&ts1)) : "memory");
         }
         // one tile spans a periodic row: its x wrap reads the staged rows, so
         // no halo runs are copied
         const bool halos = !((g.per & 1) && m.ntx == 1);
 #pragma unroll 1
         for (int n = 0; ck < g.Nz; m.advance(cx, cj, ck), ++n) {
-            const int s = n % TSTAGES;
+            const int s = n % NS;
             // the consumers have released this stage's previous tile; every
             // lane of the warp leaves the loop together on a timeout (the
             // __syncwarp below needs all of them)
-            if (n >= TSTAGES &&
+            if (n >= NS &&
                 !__all_sync(0xffffffffu,
-                            tbar_wait(s_addr(&empty[s]), (uint32_t)(n / TSTAGES - 1) & 1u))) {
+                            tbar_wait(s_addr(&empty[s]), (uint32_t)(n / NS - 1) & 1u))) {
                 if (t == TCONS) atomicExch(&g_tma_timeout, 1);
                 break;
             }
             if (t == TCONS) {
                 const uint32_t bar = s_addr(&full[s]);
                 if (m.staged(cj, ck))
-                    tma_issue_tile(mp, s_addr(stage0 + s * TSTAGE), bar, cx * TT, cj, ck, m, halos);
+                    tma_issue_tile<TY>(mp, s_addr(stage0 + s * G::STAGE), bar, cx * TT, cj * TY, ck, m,
+                                       halos);
                 else  // nothing to copy: the phase completes on the arrival
                     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], 0;" ::"r"(bar)
                                  : "memory");
@@ -948,146 +998,163 @@ __global__ void __launch_bounds__(TTHREADS, KB_TMA_MIN_BLOCKS)
     bool aborted = false;
 #pragma unroll 1
     for (; ck < g.Nz; m.advance(cx, cj, ck), ++it) {
-        const int s = it % TSTAGES;
-        const int x0 = cx * TT, j = cj, k = ck;
+        const int s = it % NS;
+        const int x0 = cx * TT, k = ck;
         const int iA = x0 + 2 * t;
         const bool live = iA < g.Nx;  // Nx even: both nodes of the pair or neither
-        const size_t cA = (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k) + iA;
-        uchar2 cl = make_uchar2(0, 0);  // LINKS: the pair's class bytes
-        if (!tbar_wait(s_addr(&full[s]), (uint32_t)(it / TSTAGES) & 1u)) {
+        if (!tbar_wait(s_addr(&full[s]), (uint32_t)(it / NS) & 1u)) {
             atomicExch(&g_tma_timeout, 1);
             aborted = true;
             break;
         }
-        float2 d[19];
-        if (m.staged(j, k)) {
-            if (LINKS)
-                cl = *reinterpret_cast<const uchar2 *>(
-                    reinterpret_cast<const unsigned char *>(stage0 + s * TSTAGE + TCLS) + 2 * t);
-            const R *st = stage0 + s * TSTAGE + 2 * t;
-            const DevLoad<R> ld;
+        const bool staged = m.staged(cj, k);
+        const R *stage = stage0 + s * G::STAGE;
+        // one row of the tile: rows one after the other (round to nearest) or
+        // unrolled (the stochastic-rounding loop spills at 128 registers unless
+        // unrolled)
+        const auto row = [&](const int r) {
+            const int j = cj * TY + r;
+            const size_t cA = (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k) + iA;
+            uchar2 cl = make_uchar2(0, 0);  // LINKS: the pair's class bytes
+            float2 d[19];
+            if (staged) {
+                if (LINKS)
+                    cl = *reinterpret_cast<const uchar2 *>(
+                        reinterpret_cast<const unsigned char *>(stage + G::CLS) + r * TT + 2 * t);
+                const R *st = stage + r * TT + 2 * t;
+                const DevLoad<R> ld;
 #pragma unroll
-            for (int q = 0; q < 19; ++q) {
-                const R *r = st + q * TT;  // reads at -1 / +256 fall in the neighbouring rows
-                if (CX[q] == 0) d[q] = Vec2<R>::ld(r);
-                else if (CX[q] > 0) d[q] = make_float2(ld(r[-1]), ld(r[0]));
-                else d[q] = make_float2(ld(r[1]), ld(r[2]));
-            }
-            // the tile ends take the halo slots (the thread holding the
-            // tile's last node: local index min(TT, Nx - x0) - 1, odd), or,
-            // when the tile is a whole periodic row, the other end of the
-            // staged row itself (x = Nx - 1 feeds node 0, x = 0 feeds Nx - 1)
-            const R *h = stage0 + s * TSTAGE + 19 * TT;
-            const R *rows = stage0 + s * TSTAGE;
-            if (t == 0) {
-                if (wrapx) {
-#pragma unroll
-                    for (int e = 0; e < 5; ++e) d[kQP[e]].x = ld(rows[kQP[e] * TT + g.Nx - 1]);
-                } else {
-                    const int pl = (x0 == 0 && !(g.per & 1)) ? 0 : 7;
-#pragma unroll
-                    for (int e = 0; e < 5; ++e) d[kQP[e]].x = ld(h[e * THALO + pl]);
+                for (int q = 0; q < 19; ++q) {
+                    const R *rq = st + q * TY * TT;  // reads at -1 / +256 fall in the neighbouring rows
+                    if (CX[q] == 0) d[q] = Vec2<R>::ld(rq);
+                    else if (CX[q] > 0) d[q] = make_float2(ld(rq[-1]), ld(rq[0]));
+                    else d[q] = make_float2(ld(rq[1]), ld(rq[2]));
                 }
-            }
-            if (t == (min(TT, g.Nx - x0) - 2) >> 1) {
-                if (wrapx) {
+                // the tile ends take the halo slots (the thread holding the
+                // tile's last node: local index min(TT, Nx - x0) - 1, odd), or,
+                // when the tile is a whole periodic row, the other end of the
+                // staged row itself (x = Nx - 1 feeds node 0, x = 0 feeds Nx - 1)
+                const R *h = stage + 19 * TY * TT + r * THALO;
+                const R *rows = stage + r * TT;
+                if (t == 0) {
+                    if (wrapx) {
 #pragma unroll
-                    for (int e = 0; e < 5; ++e) d[kQM[e]].y = ld(rows[kQM[e] * TT]);
-                } else {
-                    const int pr = (x0 + TT >= g.Nx && !(g.per & 1)) ? 7 : 0;
+                        for (int e = 0; e < 5; ++e) d[kQP[e]].x = ld(rows[kQP[e] * TY * TT + g.Nx - 1]);
+                    } else {
+                        const int pl = (x0 == 0 && !(g.per & 1)) ? 0 : 7;
 #pragma unroll
-                    for (int e = 0; e < 5; ++e) d[kQM[e]].y = ld(h[(5 + e) * THALO + pr]);
+                        for (int e = 0; e < 5; ++e) d[kQP[e]].x = ld(h[e * TY * THALO + pl]);
+                    }
                 }
-            }
-        } else if (live) {
-            // rows at a y or z wall: direct pull of both nodes
-            if (LINKS) cl = *reinterpret_cast<const uchar2 *>(L.cls + cA);
-            float a[19], b[19];
-            pull19_at(fi + cA, P, pull_geometry<I>(g, iA, j, k), a, DevLoad<R>());
-            pull19_at(fi + cA + 1, P, pull_geometry<I>(g, iA + 1, j, k), b, DevLoad<R>());
+                if (t == (min(TT, g.Nx - x0) - 2) >> 1) {
+                    if (wrapx) {
 #pragma unroll
-            for (int q = 0; q < 19; ++q) d[q] = make_float2(a[q], b[q]);
-        }
-        __syncwarp();
-        if ((t & 31) == 0) tbar_arrive(s_addr(&empty[s]));  // this warp is done with stage s
-        if (!live) continue;
-        uchar2 sm2 = make_uchar2(0, 0);
-        if (LINKS) {
-            sm2 = make_uchar2(cl.x == 1, cl.y == 1);
-        } else if (SOLID) {
-            sm2 = *reinterpret_cast<const uchar2 *>(solid + cA);
-        }
-        // the rates pass through opaque moves each tile so the collision's
-        // rate-derived constants are formed here, not held across the loop
-        float spl, sml;
-        asm volatile("mov.b32 %0, %1;" : "=f"(spl) : "f"(sp));
-        asm volatile("mov.b32 %0, %1;" : "=f"(sml) : "f"(sm));
-        float2 o[19], rho, ux, uy, uz;
-        trt_dev_collide(d, o, rho, ux, uy, uz, spl, sml);
-        // solid nodes store rest equilibrium (d = 0) and rho = 1, u = 0; only
-        // warps that hold one pay for the selects
-        if (HS && __any_sync(__activemask(), (sm2.x | sm2.y) != 0)) {
+                        for (int e = 0; e < 5; ++e) d[kQM[e]].y = ld(rows[kQM[e] * TY * TT]);
+                    } else {
+                        const int pr = (x0 + TT >= g.Nx && !(g.per & 1)) ? 7 : 0;
 #pragma unroll
-            for (int q = 0; q < 19; ++q) o[q] = make_float2(sm2.x ? 0.f : o[q].x, sm2.y ? 0.f : o[q].y);
-            rho = make_float2(sm2.x ? 1.f : rho.x, sm2.y ? 1.f : rho.y);
-            ux = make_float2(sm2.x ? 0.f : ux.x, sm2.y ? 0.f : ux.y);
-            uy = make_float2(sm2.x ? 0.f : uy.x, sm2.y ? 0.f : uy.y);
-            uz = make_float2(sm2.x ? 0.f : uz.x, sm2.y ? 0.f : uz.y);
-        }
-        // likewise the plane stride, so the 19 plane offsets are not hoisted
-        I Pl;
-        if constexpr (sizeof(I) == 4) asm volatile("mov.b32 %0, %1;" : "=r"(Pl) : "r"((int)P));
-        else asm volatile("mov.b64 %0, %1;" : "=l"(Pl) : "l"((long long)P));
-        R *o0 = fo + cA;
-        if (LINKS && (cl.x == 2 || cl.y == 2)) {
-            // a pair with a cut node: trt_dev_cut_k writes that node (it runs
-            // beside this kernel), so only the other node is stored here
-            const bool wA = cl.x != 2, wB = cl.y != 2;
-            const uint32_t key = SR ? (ekey + (uint32_t)it * 0x9E3779B9u) * 0x7FEB352Du : 0u;
-#pragma unroll
-            for (int q = 0; q < 19; ++q) {
-                const float vA = o[q].x, vB = o[q].y;
-                unsigned short *w = reinterpret_cast<unsigned short *>(o0 + (I)q * Pl);
-                if (SR) {
-                    const uint32_t v = SRPack<R>::pack(vA, vB, key + (uint32_t)q * 0x2C1B3C6Du);
-                    if (wA) w[0] = (unsigned short)(v & 0xFFFFu);
-                    if (wB) w[1] = (unsigned short)(v >> 16);
-                } else {
-                    if (wA) o0[(I)q * Pl] = Dev<R>::st(vA);
-                    if (wB) o0[(I)q * Pl + 1] = Dev<R>::st(vB);
+                        for (int e = 0; e < 5; ++e) d[kQM[e]].y = ld(h[(5 + e) * TY * THALO + pr]);
+                    }
                 }
+            } else if (live) {
+                // rows at a y or z wall: direct pull of both nodes
+                if (LINKS) cl = *reinterpret_cast<const uchar2 *>(L.cls + cA);
+                float a[19], b[19];
+                pull19_at(fi + cA, P, pull_geometry<I>(g, iA, j, k), a, DevLoad<R>());
+                pull19_at(fi + cA + 1, P, pull_geometry<I>(g, iA + 1, j, k), b, DevLoad<R>());
+#pragma unroll
+                for (int q = 0; q < 19; ++q) d[q] = make_float2(a[q], b[q]);
+            }
+            if (r == TY - 1) {
+                __syncwarp();
+                if ((t & 31) == 0) tbar_arrive(s_addr(&empty[s]));  // this warp is done with stage s
+            }
+            if (!live) return;
+            uchar2 sm2 = make_uchar2(0, 0);
+            if (LINKS) {
+                sm2 = make_uchar2(cl.x == 1, cl.y == 1);
+            } else if (SOLID) {
+                sm2 = *reinterpret_cast<const uchar2 *>(solid + cA);
+            }
+            // the rates pass through opaque moves each tile so the collision's
+            // rate-derived constants are formed here, not held across the loop
+            float spl, sml;
+            asm volatile("mov.b32 %0, %1;" : "=f"(spl) : "f"(sp));
+            asm volatile("mov.b32 %0, %1;" : "=f"(sml) : "f"(sm));
+            float2 o[19], rho, ux, uy, uz;
+            trt_dev_collide(d, o, rho, ux, uy, uz, spl, sml);
+            // solid nodes store rest equilibrium (d = 0) and rho = 1, u = 0; only
+            // warps that hold one pay for the selects
+            if (HS && __any_sync(__activemask(), (sm2.x | sm2.y) != 0)) {
+#pragma unroll
+                for (int q = 0; q < 19; ++q) o[q] = make_float2(sm2.x ? 0.f : o[q].x, sm2.y ? 0.f : o[q].y);
+                rho = make_float2(sm2.x ? 1.f : rho.x, sm2.y ? 1.f : rho.y);
+                ux = make_float2(sm2.x ? 0.f : ux.x, sm2.y ? 0.f : ux.y);
+                uy = make_float2(sm2.x ? 0.f : uy.x, sm2.y ? 0.f : uy.y);
+                uz = make_float2(sm2.x ? 0.f : uz.x, sm2.y ? 0.f : uz.y);
+            }
+            // likewise the plane stride, so the 19 plane offsets are not hoisted
+            I Pl;
+            if constexpr (sizeof(I) == 4) asm volatile("mov.b32 %0, %1;" : "=r"(Pl) : "r"((int)P));
+            else asm volatile("mov.b64 %0, %1;" : "=l"(Pl) : "l"((long long)P));
+            R *o0 = fo + cA;
+            if (LINKS && (cl.x == 2 || cl.y == 2)) {
+                // a pair with a cut node: trt_dev_cut_k writes that node (it runs
+                // beside this kernel), so only the other node is stored here
+                const bool wA = cl.x != 2, wB = cl.y != 2;
+                const uint32_t key = SR ? (ekey + (uint32_t)(it * TY + r) * 0x9E3779B9u) * 0x7FEB352Du : 0u;
+#pragma unroll
+                for (int q = 0; q < 19; ++q) {
+                    const float vA = o[q].x, vB = o[q].y;
+                    unsigned short *w = reinterpret_cast<unsigned short *>(o0 + (I)q * Pl);
+                    if (SR) {
+                        const uint32_t v = SRPack<R>::pack(vA, vB, key + (uint32_t)q * 0x2C1B3C6Du);
+                        if (wA) w[0] = (unsigned short)(v & 0xFFFFu);
+                        if (wB) w[1] = (unsigned short)(v >> 16);
+                    } else {
+                        if (wA) o0[(I)q * Pl] = Dev<R>::st(vA);
+                        if (wB) o0[(I)q * Pl + 1] = Dev<R>::st(vB);
+                    }
+                }
+                if (MOM) {
+                    if (wA) { rho_o[cA] = rho.x; ux_o[cA] = ux.x; uy_o[cA] = uy.x; uz_o[cA] = uz.x; }
+                    if (wB) { rho_o[cA + 1] = rho.y; ux_o[cA + 1] = ux.y; uy_o[cA + 1] = uy.y; uz_o[cA + 1] = uz.y; }
+                }
+                return;
+            }
+            if (SR) {
+                const uint32_t key = (ekey + (uint32_t)(it * TY + r) * 0x9E3779B9u) * 0x7FEB352Du;
+#pragma unroll
+                for (int q = 0; q < 19; ++q) {
+                    const uint32_t v = SRPack<R>::pack(o[q].x, o[q].y, key + (uint32_t)q * 0x2C1B3C6Du);
+                    *reinterpret_cast<uint32_t *>(o0 + (I)q * Pl) = v;
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 19; ++q)
+                    Vec2<R>::st(o0 + (I)q * Pl, o[q]);
             }
             if (MOM) {
-                if (wA) { rho_o[cA] = rho.x; ux_o[cA] = ux.x; uy_o[cA] = uy.x; uz_o[cA] = uz.x; }
-                if (wB) { rho_o[cA + 1] = rho.y; ux_o[cA + 1] = ux.y; uy_o[cA + 1] = uy.y; uz_o[cA + 1] = uz.y; }
+                *reinterpret_cast<float2 *>(rho_o + cA) = rho;
+                *reinterpret_cast<float2 *>(ux_o + cA) = ux;
+                *reinterpret_cast<float2 *>(uy_o + cA) = uy;
+                *reinterpret_cast<float2 *>(uz_o + cA) = uz;
             }
-            continue;
-        }
-        if (SR) {
-            const uint32_t key = (ekey + (uint32_t)it * 0x9E3779B9u) * 0x7FEB352Du;
+        };
+        if constexpr (SR) {
 #pragma unroll
-            for (int q = 0; q < 19; ++q) {
-                const uint32_t v = SRPack<R>::pack(o[q].x, o[q].y, key + (uint32_t)q * 0x2C1B3C6Du);
-                *reinterpret_cast<uint32_t *>(o0 + (I)q * Pl) = v;
-            }
+            for (int r = 0; r < TY; ++r) row(r);
         } else {
-#pragma unroll
-            for (int q = 0; q < 19; ++q)
-                Vec2<R>::st(o0 + (I)q * Pl, o[q]);
-        }
-        if (MOM) {
-            *reinterpret_cast<float2 *>(rho_o + cA) = rho;
-            *reinterpret_cast<float2 *>(ux_o + cA) = ux;
-            *reinterpret_cast<float2 *>(uy_o + cA) = uy;
-            *reinterpret_cast<float2 *>(uz_o + cA) = uz;
+#pragma unroll 1
+            for (int r = 0; r < TY; ++r) row(r);
         }
     }
     // after a timeout: wait (bounded) for copies the producer may still have
     // in flight, so none lands in shared memory after the block has exited
     if (aborted && (t & 31) == 0) {
-        for (int n = 0; n < TSTAGES && ck < g.Nz; ++n, m.advance(cx, cj, ck)) {
+        for (int n = 0; n < NS && ck < g.Nz; ++n, m.advance(cx, cj, ck)) {
             const int i2 = it + n;
-            tbar_wait(s_addr(&full[i2 % TSTAGES]), (uint32_t)(i2 / TSTAGES) & 1u);
+            tbar_wait(s_addr(&full[i2 % NS]), (uint32_t)(i2 / NS) & 1u);
         }
     }
     // stochastic rounding: this launch's last consumer warp advances the
@@ -1125,16 +1192,20 @@ static bool tma_eligible(const Grid3 &g, const void *f_out, const void *f_in, co
            tma_encode_fn() != nullptr;
 }
 
-// Maps of one population buffer: [0..2] 256-element row runs of 1, 2 and 3
-// consecutive planes, [3] 8-element halo runs of one plane.
+// Maps of one population buffer: [0..2] 256-element runs of TY rows of 1, 2
+// and 3 consecutive planes, [3] 8-element halo runs of one row of one plane,
+// [4] class bytes of a cut-link table (x, y, z) 256-byte runs of one row,
+// [5] one row of [0] (the copies of wrapped row groups).
 struct TmaMaps {
-    CUtensorMap m[5];  // [4]: class bytes of a cut-link table (x, y, z) 256-byte runs
+    CUtensorMap m[6];
 };
 
-template <typename R, bool MOM, bool SOLID, typename I, bool SR, bool LINKS = false>
+template <typename R, bool MOM, bool SOLID, typename I, bool SR, bool LINKS = false, int TY = 1>
 static int launch_tma_k(const TmaMaps &mp, R *fo, const R *fi, float *rho, float *ux, float *uy,
                         float *uz, const uint8_t *solid, const Grid3 &g, float sp, float sm,
                         cudaStream_t s, const LinkTable3 &L = LinkTable3{}) {
+    constexpr size_t smem = TileGeom<TY>::SMEM;
+    const auto kern = trt_dev_tma_k<R, MOM, SOLID, I, SR, LINKS, TY>;
     // resident blocks per SM of this instantiation, per device (the shared
     // memory opt-in below is a per-device attribute too)
     static int occ_dev[64] = {};
@@ -1145,30 +1216,35 @@ static int launch_tma_k(const TmaMaps &mp, R *fo, const R *fi, float *rho, float
     if (occ <= 0) {
         int n = 0;
         // the stage ring may exceed the 48 KB default of dynamic shared memory
-        if (cudaFuncSetAttribute(trt_dev_tma_k<R, MOM, SOLID, I, SR, LINKS>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TSMEM) !=
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
             cudaSuccess)
             return set_error(KB_ERR_CUDA, "kb_fused_trt_step_3d: %zu bytes of shared memory per "
-                             "block refused", TSMEM);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, trt_dev_tma_k<R, MOM, SOLID, I, SR, LINKS>,
-                                                          TTHREADS, TSMEM) != cudaSuccess || n < 1) {
+                             "block refused", smem);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, TTHREADS, smem) != cudaSuccess ||
+            n < 1) {
             cudaGetLastError();
             n = 1;
         }
         occ = n;
     }
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const long long tiles = (long long)((g.Nx + TT - 1) / TT) * g.Ny * g.Nz;
+    const long long tiles = (long long)((g.Nx + TT - 1) / TT) * (g.Ny / TY) * g.Nz;
     const int blocks = (int)std::min<long long>(tiles, (long long)sms * occ);
-    trt_dev_tma_k<R, MOM, SOLID, I, SR, LINKS><<<blocks, TTHREADS, TSMEM, s>>>(
-        mp.m[0], mp.m[1], mp.m[2], mp.m[3], mp.m[4], fo, fi, rho, ux, uy, uz, solid, g, sp, sm, L);
+    kern<<<blocks, TTHREADS, smem, s>>>(mp.m[0], mp.m[1], mp.m[2], mp.m[3], mp.m[4], mp.m[5], fo, fi,
+                                        rho, ux, uy, uz, solid, g, sp, sm, L);
     return KB_OK;
 }
 
+// ty: rows per tile, 0 automatic (2 where Ny is even, the offsets fit in int
+// and no cut-link table is staged; else 1).
 template <typename R, typename I, bool SR>
 static int launch_tma(void *f_out, const void *f_in, float *rho, float *ux, float *uy, float *uz,
                       const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s,
-                      const LinkTable3 *links = nullptr) {
+                      const LinkTable3 *links = nullptr, int ty = 0) {
+    constexpr bool I32 = sizeof(I) == 4;
+    if (ty == 0) ty = (I32 && !links && g.Ny % 2 == 0) ? 2 : 1;
+    if (ty != 1 && !(ty == 2 && I32 && !links && g.Ny % 2 == 0))
+        return set_error(KB_ERR_ARG, "kb_fused_trt_step_3d: two-row tiles need an even Ny");
     // the populations as a 4-D tensor (x, y, z, q) of 16-bit words over the
     // whole allocation (a z-range starts at its plane g.zoff)
     TmaMaps mp;
@@ -1177,10 +1253,13 @@ static int launch_tma(void *f_out, const void *f_in, float *rho, float *ux, floa
     const cuuint64_t dims[4] = {(cuuint64_t)g.Nx, (cuuint64_t)g.Ny, (cuuint64_t)(g.plane / nxy), 19};
     const cuuint64_t strides[3] = {(cuuint64_t)g.Nx * 2, (cuuint64_t)g.Nx * g.Ny * 2,
                                    (cuuint64_t)g.plane * 2};
-    const cuuint32_t boxes[4][4] = {{TT, 1, 1, 1}, {TT, 1, 1, 2}, {TT, 1, 1, 3}, {8, 1, 1, 1}};
+    const cuuint32_t y = (cuuint32_t)ty;
+    const cuuint32_t boxes[5][4] = {{TT, y, 1, 1}, {TT, y, 1, 2}, {TT, y, 1, 3}, {8, 1, 1, 1},
+                                    {TT, 1, 1, 1}};
+    const int slot[5] = {0, 1, 2, 3, 5};
     const cuuint32_t es[4] = {1, 1, 1, 1};
-    for (int n = 0; n < 4; ++n) {
-        const CUresult r = tma_encode_fn()(&mp.m[n], CU_TENSOR_MAP_DATA_TYPE_UINT16, 4,
+    for (int n = 0; n < 5; ++n) {
+        const CUresult r = tma_encode_fn()(&mp.m[slot[n]], CU_TENSOR_MAP_DATA_TYPE_UINT16, 4,
                                            const_cast<void *>(fbase), dims, strides, boxes[n], es,
                                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -1208,6 +1287,16 @@ static int launch_tma(void *f_out, const void *f_in, float *rho, float *ux, floa
     if (links) {
         if (rho) return launch_tma_k<R, true, false, I, SR, true>(mp, fo, fi, rho, ux, uy, uz, nullptr, g, sp, sm, s, *links);
         return launch_tma_k<R, false, false, I, SR, true>(mp, fo, fi, rho, ux, uy, uz, nullptr, g, sp, sm, s, *links);
+    }
+    if constexpr (I32) {
+        if (ty == 2) {
+            if (rho) {
+                if (solid) return launch_tma_k<R, true, true, I, SR, false, 2>(mp, fo, fi, rho, ux, uy, uz, solid, g, sp, sm, s);
+                return launch_tma_k<R, true, false, I, SR, false, 2>(mp, fo, fi, rho, ux, uy, uz, solid, g, sp, sm, s);
+            }
+            if (solid) return launch_tma_k<R, false, true, I, SR, false, 2>(mp, fo, fi, rho, ux, uy, uz, solid, g, sp, sm, s);
+            return launch_tma_k<R, false, false, I, SR, false, 2>(mp, fo, fi, rho, ux, uy, uz, solid, g, sp, sm, s);
+        }
     }
     if (rho) {
         if (solid) return launch_tma_k<R, true, true, I, SR>(mp, fo, fi, rho, ux, uy, uz, solid, g, sp, sm, s);
@@ -1276,10 +1365,11 @@ static int launch_r(void *f_out, const void *f_in, float *rho, float *ux, float 
                     const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s,
                     int kind) {
     if constexpr (sizeof(R) == 2) {
-        if (kind == 5) {
+        if (kind == 5 || kind == 6) {
+            const int ty = kind == 6 ? 1 : 0;  // 6: one-row tiles
             const int rc = offsets_fit_int(g, 19)
-                               ? launch_tma<R, int, SR>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s)
-                               : launch_tma<R, long long, SR>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s);
+                               ? launch_tma<R, int, SR>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, nullptr, ty)
+                               : launch_tma<R, long long, SR>(f_out, f_in, rho, ux, uy, uz, solid, g, sp, sm, s, nullptr, ty);
             // (the staged kernel advances the stochastic-rounding epoch itself)
             return rc;
         }
@@ -1299,13 +1389,15 @@ int launch_trt3d_dev(int dtype, void *f_out, const void *f_in, float *rho, float
     // thread, 3 adjacent node pairs with vector accesses (even Nx only),
     // 4 adjacent node quads with 8-byte accesses (16-bit storages, Nx % 4 == 0),
     // 5 row tiles staged by the tensor memory accelerator (16-bit storages,
-    // Nx % 8 == 0, aligned buffers).
+    // Nx % 8 == 0, aligned buffers; two rows per tile where Ny is even), 6
+    // the same with one row per tile.
     if (variant == 3 && g.Nx % 2 != 0)
         return set_error(KB_ERR_ARG, "kb_fused_trt_step_3d: the vector-pair kernel needs an even Nx");
     if (variant == 4 && (g.Nx % 4 != 0 || dtype == KB_F32_DEV))
         return set_error(KB_ERR_ARG,
                          "kb_fused_trt_step_3d: the quad kernel needs Nx %% 4 == 0 and 16-bit storage");
-    if (variant == 5 && (dtype == KB_F32_DEV || !tma_eligible(g, f_out, f_in, rho, ux, uy, uz, solid)))
+    if ((variant == 5 || variant == 6) &&
+        (dtype == KB_F32_DEV || !tma_eligible(g, f_out, f_in, rho, ux, uy, uz, solid)))
         return set_error(KB_ERR_ARG,
                          "kb_fused_trt_step_3d: the staged kernel needs 16-bit storage, Nx %% 8 == 0 "
                          "and 16-byte aligned populations");
@@ -1376,7 +1468,7 @@ static int launch_links_r(void *f_out, const void *f_in, float *rho, float *ux, 
         const int ntx = (g.Nx + TT - 1) / TT;
         const bool fill = 10 * g.Nx >= 9 * ntx * TT;
         // (the class-byte map needs a 16-byte row pitch: Nx % 16 == 0)
-        if ((variant == 5 || (variant == 0 && fill)) && g.Nx % 16 == 0 &&
+        if ((variant == 5 || variant == 6 || (variant == 0 && fill)) && g.Nx % 16 == 0 &&
             ((uintptr_t)L.cls & 15) == 0 && tma_eligible(g, f_out, f_in, rho, ux, uy, uz, L.cls)) {
             const bool i32 = offsets_fit_int(g, 19);
             // the cut nodes on the side stream (forked from s, joined back

@@ -736,7 +736,8 @@ def set_trt3d_variant(variant: int):
     3 adjacent node pairs with vector accesses (even Nx), 4 adjacent node
     quads with 8-byte accesses (16-bit storages, Nx % 4 == 0), 5 persistent
     256-node row tiles staged in shared memory by tensor-memory-accelerator
-    copies (16-bit storages, Nx % 8 == 0, 16-byte aligned buffers)."""
+    copies (16-bit storages, Nx % 8 == 0, 16-byte aligned buffers), two rows
+    per tile where Ny is even, 6 the staged kernel with one row per tile."""
     call("kb_set_kernel_variant", 1, int(variant))
 
 

@@ -228,7 +228,7 @@ def test_deviation_variants_agree(cuda, pkg, orc, dtype, shape, per, with_mask, 
         if Nx % 4 == 0 and dtype != torch.float32:
             variants += (4,)
         if Nx % 8 == 0 and dtype != torch.float32:
-            variants += (5,)
+            variants += (5, 6)
         for variant in variants:
             pkg.set_trt3d_variant(variant)
             fo = torch.empty_like(src)
@@ -268,20 +268,23 @@ def test_staged_kernel_rejects_what_it_cannot_stage(cuda, pkg):
         pkg.set_trt3d_variant(0)
 
 
-def test_staged_kernel_bit_identical_to_pair_kernel_without_sr(cuda, pkg):
-    """The staged kernel and the x / x+32 pair kernel run the same packed
-    FP32x2 collision on the same inputs, so their round-to-nearest outputs
-    agree bit for bit (the staging changes where the operands come from,
-    not their values), on a 256³-class row length with wraps and walls."""
+@pytest.mark.parametrize("Nx,Ny,Nz", [(264, 5, 4), (264, 6, 4), (264, 8, 3), (64, 6, 4), (256, 4, 3)])
+def test_staged_kernel_bit_identical_to_pair_kernel_without_sr(cuda, pkg, Nx, Ny, Nz):
+    """The staged kernel (two-row tiles where Ny is even, variant 5; one-row
+    tiles, variant 6) and the x / x+32 pair kernel run the same packed FP32x2
+    collision on the same inputs, so their round-to-nearest outputs agree bit
+    for bit (the staging changes where the operands come from, not their
+    values): rows longer than one tile (x halos) and rows of one tile (x wrap
+    from the staged row), with wraps and walls on every axis, row groups
+    whose sources wrap past the last row, and rows at y walls."""
     rng = np.random.default_rng(3)
-    Nx, Ny, Nz = 264, 5, 4
     f = W19[:, None, None, None] * (1 + 0.05 * rng.standard_normal((19, Nz, Ny, Nx)))
-    for per in ((1, 1, 1), (0, 0, 0), (1, 0, 1)):
+    for per in ((1, 1, 1), (0, 0, 0), (1, 0, 1), (0, 1, 0)):
         src = torch.empty((19, Nz, Ny, Nx), dtype=torch.float16, device=cuda)
         pkg.convert_populations(src, _g(f), dst_deviation=True)
         outs = []
         try:
-            for variant in (2, 5):
+            for variant in (2, 5, 6):
                 pkg.set_trt3d_variant(variant)
                 fo = torch.empty_like(src)
                 mt = [torch.empty((Nz, Ny, Nx), dtype=torch.float32, device=cuda) for _ in range(4)]
@@ -290,9 +293,11 @@ def test_staged_kernel_bit_identical_to_pair_kernel_without_sr(cuda, pkg):
                 outs.append((fo.clone(), [m.clone() for m in mt]))
         finally:
             pkg.set_trt3d_variant(0)
-        assert torch.equal(outs[0][0], outs[1][0]), per
-        for a, b in zip(outs[0][1], outs[1][1]):
-            assert torch.equal(a, b), per
+        for o in outs[1:]:
+            assert torch.equal(outs[0][0], o[0]), per
+            for a, b in zip(outs[0][1], o[1]):
+                assert torch.equal(a, b), per
+    assert not pkg.staged_step_timed_out()
 
 
 def test_quad_kernel_needs_nx_multiple_of_4_and_16bit(cuda, pkg):
