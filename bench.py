@@ -1454,7 +1454,8 @@ def main():
                     help="population storage of --workload batch (sr: stochastic rounding)")
     ap.add_argument("--trt-variant", type=int, default=0,
                     help="deviation-storage TRT kernel: 0 automatic, 1 node, 2 x/x+32 pairs, "
-                         "3 vector pairs, 4 16-bit quads")
+                         "3 vector pairs, 4 16-bit quads, 5 staged row tiles (two rows where Ny "
+                         "is even), 6 staged one-row tiles")
     ap.add_argument("--grid", type=int, default=N_GRID)
     ap.add_argument("--cases", type=int, default=256, help="--workload batch: number of cavities")
     ap.add_argument("--max-steps", type=int, default=50000,
