@@ -1407,6 +1407,7 @@ def run_other(args):
     rank, world, _ = dist_setup(args.gpus)
     pkg = graft.load_package()
     pkg._lib.load()
+    pkg.set_trt3d_variant(args.trt_variant)
     r = None
     if args.workload == "cavity2d":
         if rank == 0:

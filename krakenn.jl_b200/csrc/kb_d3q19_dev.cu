@@ -1194,7 +1194,7 @@ static bool tma_eligible(const Grid3 &g, const void *f_out, const void *f_in, co
 
 // Maps of one population buffer: [0..2] 256-element runs of TY rows of 1, 2
 // and 3 consecutive planes, [3] 8-element halo runs of one row of one plane,
-// [4] class bytes of a cut-link table (x, y, z) 256-byte runs of one row,
+// [4] class bytes of a cut-link table (x, y, z) 256-byte runs of TY rows,
 // [5] one row of [0] (the copies of wrapped row groups).
 struct TmaMaps {
     CUtensorMap m[6];
@@ -1235,15 +1235,15 @@ static int launch_tma_k(const TmaMaps &mp, R *fo, const R *fi, float *rho, float
     return KB_OK;
 }
 
-// ty: rows per tile, 0 automatic (2 where Ny is even, the offsets fit in int
-// and no cut-link table is staged; else 1).
+// ty: rows per tile, 0 automatic (2 where Ny is even and the offsets fit in
+// int; else 1).
 template <typename R, typename I, bool SR>
 static int launch_tma(void *f_out, const void *f_in, float *rho, float *ux, float *uy, float *uz,
                       const uint8_t *solid, const Grid3 &g, float sp, float sm, cudaStream_t s,
                       const LinkTable3 *links = nullptr, int ty = 0) {
     constexpr bool I32 = sizeof(I) == 4;
-    if (ty == 0) ty = (I32 && !links && g.Ny % 2 == 0) ? 2 : 1;
-    if (ty != 1 && !(ty == 2 && I32 && !links && g.Ny % 2 == 0))
+    if (ty == 0) ty = (I32 && g.Ny % 2 == 0) ? 2 : 1;
+    if (ty != 1 && !(ty == 2 && I32 && g.Ny % 2 == 0))
         return set_error(KB_ERR_ARG, "kb_fused_trt_step_3d: two-row tiles need an even Ny");
     // the populations as a 4-D tensor (x, y, z, q) of 16-bit words over the
     // whole allocation (a z-range starts at its plane g.zoff)
@@ -1272,7 +1272,7 @@ static int launch_tma(void *f_out, const void *f_in, float *rho, float *ux, floa
     if (links) {
         const cuuint64_t cd[3] = {(cuuint64_t)g.Nx, (cuuint64_t)g.Ny, (cuuint64_t)g.Nz};
         const cuuint64_t cs[2] = {(cuuint64_t)g.Nx, (cuuint64_t)g.Nx * g.Ny};
-        const cuuint32_t cb[3] = {TT, 1, 1};
+        const cuuint32_t cb[3] = {TT, (cuuint32_t)ty, 1};
         const CUresult r = tma_encode_fn()(&mp.m[4], CU_TENSOR_MAP_DATA_TYPE_UINT8, 3,
                                            const_cast<uint8_t *>(links->cls), cd, cs, cb, es,
                                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -1284,6 +1284,12 @@ static int launch_tma(void *f_out, const void *f_in, float *rho, float *ux, floa
     }
     R *fo = (R *)f_out;
     const R *fi = (const R *)f_in;
+    if constexpr (I32) {
+        if (ty == 2 && links) {
+            if (rho) return launch_tma_k<R, true, false, I, SR, true, 2>(mp, fo, fi, rho, ux, uy, uz, nullptr, g, sp, sm, s, *links);
+            return launch_tma_k<R, false, false, I, SR, true, 2>(mp, fo, fi, rho, ux, uy, uz, nullptr, g, sp, sm, s, *links);
+        }
+    }
     if (links) {
         if (rho) return launch_tma_k<R, true, false, I, SR, true>(mp, fo, fi, rho, ux, uy, uz, nullptr, g, sp, sm, s, *links);
         return launch_tma_k<R, false, false, I, SR, true>(mp, fo, fi, rho, ux, uy, uz, nullptr, g, sp, sm, s, *links);
@@ -1492,8 +1498,9 @@ static int launch_links_r(void *f_out, const void *f_in, float *rho, float *ux, 
                     else trt_dev_cut_k<R, false, long long, SR><<<nb, BX, 0, cs>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
                 }
             }
-            const int rc = i32 ? launch_tma<R, int, SR>(f_out, f_in, rho, ux, uy, uz, nullptr, g, sp, sm, s, &L)
-                               : launch_tma<R, long long, SR>(f_out, f_in, rho, ux, uy, uz, nullptr, g, sp, sm, s, &L);
+            const int ty = variant == 6 ? 1 : 0;  // 6: one-row tiles
+            const int rc = i32 ? launch_tma<R, int, SR>(f_out, f_in, rho, ux, uy, uz, nullptr, g, sp, sm, s, &L, ty)
+                               : launch_tma<R, long long, SR>(f_out, f_in, rho, ux, uy, uz, nullptr, g, sp, sm, s, &L, ty);
             if (cs != s && (cudaEventRecord(ss->join, cs) != cudaSuccess ||
                             cudaStreamWaitEvent(s, ss->join, 0) != cudaSuccess))
                 return set_error(KB_ERR_CUDA, "kb_fused_trt_libb_links_step_3d: joining the cut-node stream failed");

@@ -255,10 +255,12 @@ def test_sphere_geometry_on_device_equals_host(cuda, pkg):
                                           (torch.float16, True, 4e-3)])
 def test_staged_cut_link_step_matches_one_node_kernel(cuda, pkg, dtype, sr, tol):
     """The cut-link step on 16-bit storage through the staged row tiles
-    (variant 5, the automatic choice for full 256-node rows) and through the
-    one-node kernel agree within the storage rounding, and both stay within
+    (variant 5, the automatic choice for full 256-node rows: two rows per
+    tile as Ny is even; variant 6: one row per tile) and through the
+    one-node kernel agree within the storage rounding, and all stay within
     it of the FP64 table step: a sphere cut through 256-node rows, random
-    populations, walls in y and z, periodic x."""
+    populations, walls in y and z, periodic x.  Without stochastic rounding
+    the two staged forms agree bit for bit."""
     Nx, Ny, Nz = 256, 20, 18
     qw, solid = pkg.libb.precompute_q_wall_sphere_3d(Nx, Ny, Nz, 128.3, 9.7, 8.9, 7.3)
     f, _, _, _ = _random_case((Nz, Ny, Nx), 19, W19, 77)
@@ -276,7 +278,7 @@ def test_staged_cut_link_step_matches_one_node_kernel(cuda, pkg, dtype, sr, tol)
     pkg.convert_populations(src, _g(f), dst_deviation=True)
     got = []
     try:
-        for variant in (5, 1):
+        for variant in (5, 1, 6):
             pkg.set_trt3d_variant(variant)
             fo = torch.empty_like(src)
             mt = [torch.empty((Nz, Ny, Nx), dtype=torch.float32, device=cuda) for _ in range(4)]
@@ -294,4 +296,8 @@ def test_staged_cut_link_step_matches_one_node_kernel(cuda, pkg, dtype, sr, tol)
     assert np.max(np.abs(got[0][0] - got[1][0]) / w) < 2 * tol
     for a, b in zip(got[0][1], got[1][1]):
         assert np.max(np.abs(a - b)) < 50 * tol
+    if not sr:
+        assert np.array_equal(got[0][0], got[2][0])
+        for a, b in zip(got[0][1], got[2][1]):
+            assert np.array_equal(a, b)
     assert not pkg.staged_step_timed_out()
