@@ -1,7 +1,7 @@
 """Learned warm start for lid-driven cavities.
 
 The reference has no learned component; this module adds one beside the plain
-method and judges it by the plain method.  A convolutional encoder-decoder
+method and measures it against the plain method.  A convolutional encoder-decoder
 (`kb_surrogate_*`, BF16 tensor-core kernels in libkrakenb200.so) is trained on
 steady cavities that the batched LBM kernel produces, then predicts the
 steady (rho, ux, uy) of unseen cases.  The populations are initialised
