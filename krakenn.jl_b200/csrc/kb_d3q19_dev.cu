@@ -377,7 +377,10 @@ template <> struct Vec2<__nv_bfloat16> {
     }
 };
 
-template <typename R, bool MOM, bool SOLID, typename I, bool SR>
+// LINKS: `solid` is the class-byte row of a compact cut-link table (f1):
+// class 1 nodes are solid, class 2 (cut) nodes are left to trt_dev_cut_k,
+// which runs beside this kernel and writes only them.
+template <typename R, bool MOM, bool SOLID, typename I, bool SR, bool LINKS = false>
 __global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_v2_k(R *__restrict__ fo, const R *__restrict__ fi,
                                                     float *__restrict__ rho_o, float *__restrict__ ux_o,
                                                     float *__restrict__ uy_o, float *__restrict__ uz_o,
@@ -454,13 +457,45 @@ __global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_v2_k(R *__rest
     trt_dev_collide(d, o, rho, ux, uy, uz, sp, sm);
     const size_t oc = row + x0;
     uchar2 sm2 = make_uchar2(0, 0);
-    if (SOLID) sm2 = *reinterpret_cast<const uchar2 *>(solid + oc);
+    if (SOLID || LINKS) sm2 = *reinterpret_cast<const uchar2 *>(solid + oc);
     R *__restrict__ o0 = fo + oc;
     const uint32_t key = SR ? sr_key() : 0u;
+    if (LINKS) {
+        const bool wA = sm2.x != 2, wB = sm2.y != 2;
+        if (!(wA && wB)) {
+            // a pair with a cut node: only the other node is stored here
+            const bool zA = sm2.x == 1, zB = sm2.y == 1;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) {
+                const float vA = zA ? 0.f : o[q].x, vB = zB ? 0.f : o[q].y;
+                if (SR) {
+                    const uint32_t v = SRPack<R>::pack(vA, vB, sr_bits(key, q));
+                    unsigned short *w = reinterpret_cast<unsigned short *>(o0 + (size_t)(q * P));
+                    if (wA) w[0] = (unsigned short)(v & 0xFFFFu);
+                    if (wB) w[1] = (unsigned short)(v >> 16);
+                } else {
+                    if (wA) o0[(size_t)(q * P)] = Dev<R>::st(vA);
+                    if (wB) o0[(size_t)(q * P) + 1] = Dev<R>::st(vB);
+                }
+            }
+            if (MOM) {
+                if (wA) {
+                    rho_o[oc] = zA ? 1.f : rho.x; ux_o[oc] = zA ? 0.f : ux.x;
+                    uy_o[oc] = zA ? 0.f : uy.x; uz_o[oc] = zA ? 0.f : uz.x;
+                }
+                if (wB) {
+                    rho_o[oc + 1] = zB ? 1.f : rho.y; ux_o[oc + 1] = zB ? 0.f : ux.y;
+                    uy_o[oc + 1] = zB ? 0.f : uy.y; uz_o[oc + 1] = zB ? 0.f : uz.y;
+                }
+            }
+            return;
+        }
+    }
+    constexpr bool HS = SOLID || LINKS;  // a mask byte 1 means solid
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
         float2 v = o[q];
-        if (SOLID) { if (sm2.x) v.x = 0.f; if (sm2.y) v.y = 0.f; }
+        if (HS) { if (sm2.x) v.x = 0.f; if (sm2.y) v.y = 0.f; }
         if (SR)
             *reinterpret_cast<uint32_t *>(o0 + (size_t)(q * P)) = SRPack<R>::pack(v.x, v.y, sr_bits(key, q));
         else
@@ -468,7 +503,7 @@ __global__ void __launch_bounds__(BX, KB_PAIR_MIN_BLOCKS) trt_dev_v2_k(R *__rest
     }
     if (MOM) {
         float2 r = rho, aa = ux, bb = uy, cc = uz;
-        if (SOLID) {
+        if (HS) {
             if (sm2.x) { r.x = 1.f; aa.x = bb.x = cc.x = 0.f; }
             if (sm2.y) { r.y = 1.f; aa.y = bb.y = cc.y = 0.f; }
         }
@@ -1469,50 +1504,71 @@ template <typename R, bool SR>
 static int launch_links_r(void *f_out, const void *f_in, float *rho, float *ux, float *uy,
                           float *uz, const LinkTable3 &L, const Grid3 &g, float sp, float sm,
                           cudaStream_t s, int variant) {
+    // the staged row tiles with the table (16-bit storages, under the rules
+    // of the plain step; the class-byte map needs a 16-byte row pitch:
+    // Nx % 16 == 0), else adjacent node pairs with vector accesses (even Nx),
+    // else one node per thread (odd Nx, or variant 1).  The first two leave
+    // the cut nodes to trt_dev_cut_k.
+    bool staged = false;
     if constexpr (sizeof(R) == 2) {
-        // the staged row tiles with the table, under the rules of the plain step
         const int ntx = (g.Nx + TT - 1) / TT;
         const bool fill = 10 * g.Nx >= 9 * ntx * TT;
-        // (the class-byte map needs a 16-byte row pitch: Nx % 16 == 0)
-        if ((variant == 5 || variant == 6 || (variant == 0 && fill)) && g.Nx % 16 == 0 &&
-            ((uintptr_t)L.cls & 15) == 0 && tma_eligible(g, f_out, f_in, rho, ux, uy, uz, L.cls)) {
-            const bool i32 = offsets_fit_int(g, 19);
-            // the cut nodes on the side stream (forked from s, joined back
-            // before anything that follows on s), or on s itself
-            SideStream *ss = L.n_rec > 0 ? side_stream() : nullptr;
-            cudaStream_t cs = s;
-            if (ss && cudaEventRecord(ss->fork, s) == cudaSuccess &&
-                cudaStreamWaitEvent(ss->side, ss->fork, 0) == cudaSuccess)
-                cs = ss->side;
-            else
-                cudaGetLastError();
-            if (L.n_rec > 0) {
-                const unsigned nb = (unsigned)((L.n_rec + BX - 1) / BX);
-                R *fo = (R *)f_out;
-                const R *fi = (const R *)f_in;
-                if (i32) {
-                    if (rho) trt_dev_cut_k<R, true, int, SR><<<nb, BX, 0, cs>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
-                    else trt_dev_cut_k<R, false, int, SR><<<nb, BX, 0, cs>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
-                } else {
-                    if (rho) trt_dev_cut_k<R, true, long long, SR><<<nb, BX, 0, cs>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
-                    else trt_dev_cut_k<R, false, long long, SR><<<nb, BX, 0, cs>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
-                }
-            }
-            const int ty = variant == 6 ? 1 : 0;  // 6: one-row tiles
-            const int rc = i32 ? launch_tma<R, int, SR>(f_out, f_in, rho, ux, uy, uz, nullptr, g, sp, sm, s, &L, ty)
-                               : launch_tma<R, long long, SR>(f_out, f_in, rho, ux, uy, uz, nullptr, g, sp, sm, s, &L, ty);
-            if (cs != s && (cudaEventRecord(ss->join, cs) != cudaSuccess ||
-                            cudaStreamWaitEvent(s, ss->join, 0) != cudaSuccess))
-                return set_error(KB_ERR_CUDA, "kb_fused_trt_libb_links_step_3d: joining the cut-node stream failed");
-            if (rc != KB_OK) return rc;
-            if (SR) sr_advance_k<<<1, 1, 0, s>>>();
-            return KB_OK;
-        }
+        staged = (variant == 5 || variant == 6 || (variant == 0 && fill)) && g.Nx % 16 == 0 &&
+                 ((uintptr_t)L.cls & 15) == 0 && tma_eligible(g, f_out, f_in, rho, ux, uy, uz, L.cls);
     }
-    const dim3 grid((g.Nx + BX - 1) / BX, g.Ny, g.Nz);
+    const auto al = [](const void *q, uintptr_t n) { return ((uintptr_t)q & (n - 1)) == 0; };
+    const bool pairs = !staged && (variant == 0 || variant == 3) && g.Nx % 2 == 0 &&
+                       al(f_out, 2 * sizeof(R)) && al(f_in, 2 * sizeof(R)) && al(rho, 8) &&
+                       al(ux, 8) && al(uy, 8) && al(uz, 8) && al(L.cls, 2);
+    const bool i32 = offsets_fit_int(g, 19);
     R *fo = (R *)f_out;
     const R *fi = (const R *)f_in;
-    if (offsets_fit_int(g, 19)) {
+    if (staged || pairs) {
+        // the cut nodes on the side stream (forked from s, joined back
+        // before anything that follows on s), or on s itself
+        SideStream *ss = L.n_rec > 0 ? side_stream() : nullptr;
+        cudaStream_t cs = s;
+        if (ss && cudaEventRecord(ss->fork, s) == cudaSuccess &&
+            cudaStreamWaitEvent(ss->side, ss->fork, 0) == cudaSuccess)
+            cs = ss->side;
+        else
+            cudaGetLastError();
+        if (L.n_rec > 0) {
+            const unsigned nb = (unsigned)((L.n_rec + BX - 1) / BX);
+            if (i32) {
+                if (rho) trt_dev_cut_k<R, true, int, SR><<<nb, BX, 0, cs>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
+                else trt_dev_cut_k<R, false, int, SR><<<nb, BX, 0, cs>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
+            } else {
+                if (rho) trt_dev_cut_k<R, true, long long, SR><<<nb, BX, 0, cs>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
+                else trt_dev_cut_k<R, false, long long, SR><<<nb, BX, 0, cs>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
+            }
+        }
+        int rc = KB_OK;
+        if (staged) {
+            if constexpr (sizeof(R) == 2) {
+                const int ty = variant == 6 ? 1 : 0;  // 6: one-row tiles
+                rc = i32 ? launch_tma<R, int, SR>(f_out, f_in, rho, ux, uy, uz, nullptr, g, sp, sm, s, &L, ty)
+                         : launch_tma<R, long long, SR>(f_out, f_in, rho, ux, uy, uz, nullptr, g, sp, sm, s, &L, ty);
+            }
+        } else {
+            const dim3 grid((g.Nx / 2 + BX - 1) / BX, g.Ny, g.Nz);
+            if (i32) {
+                if (rho) trt_dev_v2_k<R, true, false, int, SR, true><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, L.cls, g, sp, sm);
+                else trt_dev_v2_k<R, false, false, int, SR, true><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, L.cls, g, sp, sm);
+            } else {
+                if (rho) trt_dev_v2_k<R, true, false, long long, SR, true><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, L.cls, g, sp, sm);
+                else trt_dev_v2_k<R, false, false, long long, SR, true><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, L.cls, g, sp, sm);
+            }
+        }
+        if (cs != s && (cudaEventRecord(ss->join, cs) != cudaSuccess ||
+                        cudaStreamWaitEvent(s, ss->join, 0) != cudaSuccess))
+            return set_error(KB_ERR_CUDA, "kb_fused_trt_libb_links_step_3d: joining the cut-node stream failed");
+        if (rc != KB_OK) return rc;
+        if (SR) sr_advance_k<<<1, 1, 0, s>>>();
+        return KB_OK;
+    }
+    const dim3 grid((g.Nx + BX - 1) / BX, g.Ny, g.Nz);
+    if (i32) {
         if (rho) trt_dev_links_k<R, true, int, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
         else trt_dev_links_k<R, false, int, SR><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
     } else {

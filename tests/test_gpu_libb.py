@@ -301,3 +301,52 @@ def test_staged_cut_link_step_matches_one_node_kernel(cuda, pkg, dtype, sr, tol)
         for a, b in zip(got[0][1], got[2][1]):
             assert np.array_equal(a, b)
     assert not pkg.staged_step_timed_out()
+
+
+@pytest.mark.parametrize("dtype,sr,tol", [(torch.float32, False, 2e-6), (torch.float16, False, 2e-3),
+                                          (torch.float16, True, 4e-3)])
+@pytest.mark.parametrize("per", [(True, False, False), (True, True, True)])
+def test_pair_cut_link_step_matches_one_node_kernel(cuda, pkg, dtype, sr, tol, per):
+    """The cut-link step through adjacent node pairs with vector accesses
+    (variant 3, the automatic choice for FP32 deviations and for 16-bit rows
+    the staged tiles do not take), with the cut nodes left to the cut-node
+    kernel, and through the one-node kernel (variant 1) agree within the
+    storage rounding and stay within it of the FP64 table step: a sphere cut
+    through 200-node rows, random populations, walls or wraps in y and z."""
+    Nx, Ny, Nz = 200, 20, 18
+    qw, solid = pkg.libb.precompute_q_wall_sphere_3d(Nx, Ny, Nz, 100.3, 9.7, 8.9, 7.3)
+    f, _, _, _ = _random_case((Nz, Ny, Nx), 19, W19, 78)
+    zeros = np.zeros_like(qw)
+    m = _g(solid, torch.uint8)
+    links64 = pkg.libb.CutLinks(m, *[_g(a) for a in (qw, zeros, zeros, zeros)])
+    ref = torch.empty_like(_g(f))
+    pkg.fused_trt_libb_links_step_3d_(ref, _g(f), None, None, None, None, links64, 0.04, periodic=per)
+    ref = _h(ref)
+    links64.close()
+    links = pkg.libb.CutLinks(m, *[_g(a, torch.float32) for a in (qw, zeros, zeros, zeros)])
+    assert links.nodes_with_links() > 100
+    src = torch.empty((19, Nz, Ny, Nx), dtype=dtype, device=cuda)
+    pkg.convert_populations(src, _g(f), dst_deviation=True)
+    got = []
+    try:
+        for variant in (3, 1):
+            pkg.set_trt3d_variant(variant)
+            fo = torch.empty_like(src)
+            mt = [torch.empty((Nz, Ny, Nx), dtype=torch.float32, device=cuda) for _ in range(4)]
+            pkg.fused_trt_libb_links_step_3d_(fo, src, *mt, links, 0.04, periodic=per,
+                                              deviation=True, stochastic_rounding=sr)
+            back = torch.empty((19, Nz, Ny, Nx), dtype=torch.float64, device=cuda)
+            pkg.convert_populations(back, fo, src_deviation=True)
+            got.append((_h(back), [_h(t) for t in mt]))
+    finally:
+        pkg.set_trt3d_variant(0)
+    links.close()
+    w = W19[:, None, None, None]
+    for g, _ in got:
+        assert np.max(np.abs(g - ref) / w) < tol
+    assert np.max(np.abs(got[0][0] - got[1][0]) / w) < 2 * tol
+    for a, b in zip(got[0][1], got[1][1]):
+        assert np.max(np.abs(a - b)) < 50 * tol
+    solid_nodes = solid.astype(bool)
+    for t in got[0][1][1:]:
+        assert np.all(t[solid_nodes] == 0)
