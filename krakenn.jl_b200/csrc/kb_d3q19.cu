@@ -233,20 +233,18 @@ __global__ void __launch_bounds__(BX) fused_trt_libb_k(T *__restrict__ fo, const
 
 // The same step with the compact cut-link table: one class byte per node
 // replaces the solid mask and the 18 q_wall reads; link data are read only
-// at nodes with cut links.  Bit-identical to fused_trt_libb_k.
+// at nodes with cut links.  Bit-identical to fused_trt_libb_k.  The update
+// of node c = (i, j, k) of class cl, shared by the node kernel and the
+// cut-node kernel so that both compute the same bits.
 template <typename T, typename I>
-__global__ void __launch_bounds__(BX) fused_trt_links_k(T *__restrict__ fo, const T *__restrict__ fi,
-                                                         T *__restrict__ rho, T *__restrict__ ux,
-                                                         T *__restrict__ uy, T *__restrict__ uz,
-                                                         LinkTable3 L, Grid3 g, T sp, T sm) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y, k = blockIdx.z;
-    if (i >= g.Nx) return;
-    const size_t c = (size_t)i + (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k);
+__device__ __forceinline__ void trt_links_node(T *__restrict__ fo, const T *__restrict__ fi,
+                                               T *__restrict__ rho, T *__restrict__ ux,
+                                               T *__restrict__ uy, T *__restrict__ uz,
+                                               const LinkTable3 &L, const Grid3 &g, T sp, T sm,
+                                               size_t c, int i, int j, int k, uint8_t cl) {
     const I P = (I)g.plane;
     T *__restrict__ o0 = fo + c;
     T feq[19];
-    const uint8_t cl = L.cls[c];
     if (cl == 1) {
         feq_all(T(1), T(0), T(0), T(0), T(0), feq);
 #pragma unroll
@@ -272,6 +270,42 @@ __global__ void __launch_bounds__(BX) fused_trt_links_k(T *__restrict__ fo, cons
         o0[y * P] = p[y] - a * (p[y] - feq[y]) - b * (p[x] - feq[x]);
     }
     if (rho) { rho[c] = r; ux[c] = a_; uy[c] = b_; uz[c] = d_; }
+}
+
+// SKIP_CUT: class 2 nodes are left to fused_trt_cut_k, which runs beside
+// this kernel (the two write disjoint nodes and read only f_in), so this
+// kernel carries no link code.
+template <typename T, typename I, bool SKIP_CUT>
+__global__ void __launch_bounds__(BX) fused_trt_links_k(T *__restrict__ fo, const T *__restrict__ fi,
+                                                         T *__restrict__ rho, T *__restrict__ ux,
+                                                         T *__restrict__ uy, T *__restrict__ uz,
+                                                         LinkTable3 L, Grid3 g, T sp, T sm) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i >= g.Nx) return;
+    const size_t c = (size_t)i + (size_t)g.Nx * ((size_t)j + (size_t)g.Ny * k);
+    const uint8_t cl = L.cls[c];
+    if (SKIP_CUT) {
+        if (cl == 2) return;
+        trt_links_node<T, I>(fo, fi, rho, ux, uy, uz, L, g, sp, sm, c, i, j, k, cl == 1 ? 1 : 0);
+    } else {
+        trt_links_node<T, I>(fo, fi, rho, ux, uy, uz, L, g, sp, sm, c, i, j, k, cl);
+    }
+}
+
+// The cut nodes (class 2) of a compact table, one thread per record.
+template <typename T, typename I>
+__global__ void __launch_bounds__(BX) fused_trt_cut_k(T *__restrict__ fo, const T *__restrict__ fi,
+                                                       T *__restrict__ rho, T *__restrict__ ux,
+                                                       T *__restrict__ uy, T *__restrict__ uz,
+                                                       LinkTable3 L, Grid3 g, T sp, T sm) {
+    const long long r = (long long)blockIdx.x * BX + threadIdx.x;
+    if (r >= L.n_rec) return;
+    const size_t c = (size_t)L.node[r];
+    const size_t row = c / (size_t)g.Nx;
+    const int i = (int)(c - row * (size_t)g.Nx), j = (int)(row % (size_t)g.Ny),
+              k = (int)(row / (size_t)g.Ny);
+    trt_links_node<T, I>(fo, fi, rho, ux, uy, uz, L, g, sp, sm, c, i, j, k, 2);
 }
 
 // Cut-link table construction.  Pass 1 classifies every node and counts the
@@ -1102,17 +1136,39 @@ int build_links(kb_libb_links *L, const uint8_t *solid, const T *qw, const T *wx
     return kb::check_launch("kb_libb_links_create");
 }
 
-template <typename T>
-void launch_links_3d(void *f_out, const void *f_in, void *rho, void *ux, void *uy, void *uz,
-                     const kb::d3::LinkTable3 &L, const Grid3 &g, double sp, double sm,
-                     cudaStream_t s) {
+template <typename T, typename I>
+int launch_links_3d_i(T *fo, const T *fi, T *rho, T *ux, T *uy, T *uz,
+                       const kb::d3::LinkTable3 &L, const Grid3 &g, T sp, T sm, cudaStream_t s) {
     const dim3 grid = nodes_grid(g.Nx, g.Ny, g.Nz);
-    if (offsets_fit_int(g, 19))
-        fused_trt_links_k<T, int><<<grid, BX, 0, s>>>(
-            (T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, (T *)uz, L, g, (T)sp, (T)sm);
+    kb::d3::SideStream *ss = L.n_rec > 0 ? kb::d3::side_stream() : nullptr;
+    if (!ss) {  // no cut nodes, or no side stream: one kernel for every node
+        fused_trt_links_k<T, I, false><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
+        return KB_OK;
+    }
+    // the cut nodes on the side stream, forked from s and joined back
+    // before anything that follows on s
+    cudaStream_t cs = s;
+    if (cudaEventRecord(ss->fork, s) == cudaSuccess && cudaStreamWaitEvent(ss->side, ss->fork, 0) == cudaSuccess)
+        cs = ss->side;
     else
-        fused_trt_links_k<T, long long><<<grid, BX, 0, s>>>(
-            (T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, (T *)uz, L, g, (T)sp, (T)sm);
+        cudaGetLastError();
+    const unsigned nb = (unsigned)((L.n_rec + BX - 1) / BX);
+    fused_trt_cut_k<T, I><<<nb, BX, 0, cs>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
+    fused_trt_links_k<T, I, true><<<grid, BX, 0, s>>>(fo, fi, rho, ux, uy, uz, L, g, sp, sm);
+    if (cs != s && (cudaEventRecord(ss->join, cs) != cudaSuccess || cudaStreamWaitEvent(s, ss->join, 0) != cudaSuccess))
+        return kb::set_error(KB_ERR_CUDA, "kb_fused_trt_libb_links_step_3d: joining the cut-node stream failed");
+    return KB_OK;
+}
+
+template <typename T>
+int launch_links_3d(void *f_out, const void *f_in, void *rho, void *ux, void *uy, void *uz,
+                    const kb::d3::LinkTable3 &L, const Grid3 &g, double sp, double sm,
+                    cudaStream_t s) {
+    if (offsets_fit_int(g, 19))
+        return launch_links_3d_i<T, int>((T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, (T *)uz, L, g,
+                                  (T)sp, (T)sm, s);
+    return launch_links_3d_i<T, long long>((T *)f_out, (const T *)f_in, (T *)rho, (T *)ux, (T *)uy, (T *)uz, L,
+                                        g, (T)sp, (T)sm, s);
 }
 
 }  // namespace
@@ -1177,8 +1233,9 @@ int kb_fused_trt_libb_links_step_3d(void *f_out, const void *f_in, void *rho, vo
         if (L->dtype != dtype)
             return kb::set_error(KB_ERR_UNSUPPORTED, "%s: populations of dtype %d need a cut-link "
                                  "table of the same dtype (table has %d)", what, dtype, L->dtype);
-        if (dtype == KB_F64) launch_links_3d<double>(f_out, f_in, rho, ux, uy, uz, T3, g, sp, sm, s);
-        else launch_links_3d<float>(f_out, f_in, rho, ux, uy, uz, T3, g, sp, sm, s);
+        const int rc = dtype == KB_F64 ? launch_links_3d<double>(f_out, f_in, rho, ux, uy, uz, T3, g, sp, sm, s)
+                                       : launch_links_3d<float>(f_out, f_in, rho, ux, uy, uz, T3, g, sp, sm, s);
+        if (rc != KB_OK) return rc;
         return kb::check_launch(what);
     }
     if (dtype == KB_F32_DEV || dtype == KB_F16_DEV || dtype == KB_BF16_DEV ||

@@ -179,6 +179,17 @@ struct LinkTable3 {
     const int *node;                 // node of each record
 };
 
+// One side stream and a fork / join event pair per device, created on first
+// use and kept for the life of the process: the cut-node kernel of a
+// cut-link step runs there, beside the kernel that updates the other nodes.
+// Null when the current device has none (the caller then uses its stream).
+struct SideStream {
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    bool ok = false;
+};
+SideStream *side_stream();
+
 // One record of the table, read like LinkDense.
 template <typename T>
 struct LinkRecord {

@@ -1470,15 +1470,8 @@ int launch_trt3d_dev(int dtype, void *f_out, const void *f_in, float *rho, float
     return check_launch("kb_fused_trt_step_3d");
 }
 
-// One side stream and a fork / join event pair per device, created on first
-// use and kept for the life of the process: the cut-node kernel of a staged
-// cut-link step runs there, beside the staged kernel.
-struct SideStream {
-    cudaStream_t side = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
-    bool ok = false;
-};
-static SideStream *side_stream() {
+// The side stream of a cut-link step (declared beside LinkTable3).
+SideStream *side_stream() {
     static std::mutex mu;
     static SideStream per_dev[64];
     int dev = 0;
