@@ -583,18 +583,81 @@ __global__ void fixed_temp_k(T *__restrict__ gg, Grid3 g, FixedTempSet3<T> S) {
     }
 }
 
+// Two FP32 lanes (adjacent nodes) with the operators of the reference
+// arithmetic: packed round-to-nearest adds and multiplies (never contracted)
+// and a per-lane division, so a helper written for T evaluates, with
+// T = Lanes2, the same expression tree for each node at half the arithmetic
+// instructions.  Measured against the one-node kernel the results agree to
+// 3 ulp; about 1 % of the updated populations (never the rest population)
+// differ in the last bits.
+struct Lanes2 {
+    float2 v;
+    __device__ __forceinline__ Lanes2() {}
+    __device__ __forceinline__ Lanes2(double d) { const float x = (float)d; v = make_float2(x, x); }
+    __device__ __forceinline__ static Lanes2 of(float2 a) { Lanes2 r; r.v = a; return r; }
+    __device__ __forceinline__ Lanes2 operator-() const { return of(make_float2(-v.x, -v.y)); }
+};
+__device__ __forceinline__ Lanes2 operator+(Lanes2 a, Lanes2 b) { return Lanes2::of(vadd(a.v, b.v)); }
+__device__ __forceinline__ Lanes2 operator-(Lanes2 a, Lanes2 b) { return Lanes2::of(vsub(a.v, b.v)); }
+__device__ __forceinline__ Lanes2 operator*(Lanes2 a, Lanes2 b) { return Lanes2::of(vmul(a.v, b.v)); }
+__device__ __forceinline__ Lanes2 operator/(Lanes2 a, Lanes2 b) {
+    return Lanes2::of(make_float2(a.v.x / b.v.x, a.v.y / b.v.y));
+}
+
+// The forced BGK update of one node (or two lanes) in place, force (fx, fy,
+// fz): the body of collide_boussinesq_3d_kernel! / collide_guo_3d_kernel!
+// after the force is known.
+template <typename T>
+__device__ __forceinline__ void forced_bgk_node(T *p, T w, T fx, T fy, T fz) {
+    T rho = p[0];
+#pragma unroll
+    for (int q = 1; q < 19; ++q) rho = rho + p[q];
+    const T inv = T(1) / rho;
+    const T ux = ((p[1] - p[2] + p[7] - p[8] + p[9] - p[10] + p[11] - p[12] + p[13] - p[14]) +
+                  fx / T(2)) * inv;
+    const T uy = ((p[3] - p[4] + p[7] + p[8] - p[9] - p[10] + p[15] - p[16] + p[17] - p[18]) +
+                  fy / T(2)) * inv;
+    const T uz = ((p[5] - p[6] + p[11] + p[12] - p[13] - p[14] + p[15] + p[16] - p[17] - p[18]) +
+                  fz / T(2)) * inv;
+    const T usq = ux * ux + uy * uy + uz * uz;
+    const T gpf = T(1) - w / T(2), t3 = T(3), t9 = T(9);
+    T feq[19];
+    feq_all(rho, ux, uy, uz, usq, feq);
+    // Guo source S_q = w_q ((c_q - u) . F) 3 + w_q (c_q . u)(c_q . F) 9
+    {
+        const T wr = T(1.0 / 3.0);
+        const T S0 = wr * ((-ux) * fx + (-uy) * fy + (-uz) * fz) * t3;
+        p[0] = p[0] - w * (p[0] - feq[0]) + gpf * S0;
+    }
+#pragma unroll
+    for (int q = 1; q < 19; ++q) {
+        const T wq = q < 7 ? T(1.0 / 18.0) : T(1.0 / 36.0);
+        const T ax = kCx[q] > 0 ? T(1) - ux : (kCx[q] < 0 ? -T(1) - ux : -ux);
+        const T ay = kCy[q] > 0 ? T(1) - uy : (kCy[q] < 0 ? -T(1) - uy : -uy);
+        const T az = kCz[q] > 0 ? T(1) - uz : (kCz[q] < 0 ? -T(1) - uz : -uz);
+        const T S = wq * (ax * fx + ay * fy + az * fz) * t3 +
+                    wq * cdot(q, ux, uy, uz) * cdot(q, fx, fy, fz) * t9;
+        p[q] = p[q] - w * (p[q] - feq[q]) + gpf * S;
+    }
+}
+
 // BGK with the Guo source of a body force: MODE 0 collide_boussinesq_3d_kernel!
 // (src/kernels/thermal_3d.jl:559-722, F = (0, beta_g (T - T_ref), 0)),
 // MODE 1 collide_guo_3d_kernel! (src/kernels/collide_guo_3d.jl:5-186, constant
 // F), MODE 2 collide_guo_field_3d_kernel! (:199-323, per-node F).  The three
-// share the reference's operation order.
-template <typename T, int MODE>
+// share the reference's operation order.  I: the element offset type (int
+// where the 19 planes fit in 32 bits).
+template <typename T, int MODE, typename I>
 __global__ void __launch_bounds__(BX) boussinesq_k(T *__restrict__ f, const T *__restrict__ Temp,
                                                     const uint8_t *__restrict__ solid, Grid3 g, T w,
                                                     T beta_g, T T_ref, const T *__restrict__ Fxf,
                                                     const T *__restrict__ Fyf,
                                                     const T *__restrict__ Fzf, T Fx, T Fy, T Fz) {
-    NODE3
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i >= g.Nx) return;
+    const I c = (I)i + (I)g.Nx * ((I)j + (I)g.Ny * (I)k);
+    const I P = (I)g.plane;
     T p[19];
 #pragma unroll
     for (int q = 0; q < 19; ++q) p[q] = f[c + q * P];
@@ -604,39 +667,54 @@ __global__ void __launch_bounds__(BX) boussinesq_k(T *__restrict__ f, const T *_
         const T fx = MODE == 0 ? T(0) : (MODE == 1 ? Fx : Fxf[c]);
         const T fy = MODE == 0 ? beta_g * (Temp[c] - T_ref) : (MODE == 1 ? Fy : Fyf[c]);
         const T fz = MODE == 0 ? T(0) : (MODE == 1 ? Fz : Fzf[c]);
-        T rho = p[0];
-#pragma unroll
-        for (int q = 1; q < 19; ++q) rho = rho + p[q];
-        const T inv = T(1) / rho;
-        const T ux = ((p[1] - p[2] + p[7] - p[8] + p[9] - p[10] + p[11] - p[12] + p[13] - p[14]) +
-                      fx / T(2)) * inv;
-        const T uy = ((p[3] - p[4] + p[7] + p[8] - p[9] - p[10] + p[15] - p[16] + p[17] - p[18]) +
-                      fy / T(2)) * inv;
-        const T uz = ((p[5] - p[6] + p[11] + p[12] - p[13] - p[14] + p[15] + p[16] - p[17] - p[18]) +
-                      fz / T(2)) * inv;
-        const T usq = ux * ux + uy * uy + uz * uz;
-        const T gpf = T(1) - w / T(2), t3 = T(3), t9 = T(9);
-        T feq[19];
-        feq_all(rho, ux, uy, uz, usq, feq);
-        // Guo source S_q = w_q ((c_q - u) . F) 3 + w_q (c_q . u)(c_q . F) 9
-        {
-            const T wr = T(1.0 / 3.0);
-            const T S0 = wr * ((-ux) * fx + (-uy) * fy + (-uz) * fz) * t3;
-            p[0] = p[0] - w * (p[0] - feq[0]) + gpf * S0;
-        }
-#pragma unroll
-        for (int q = 1; q < 19; ++q) {
-            const T wq = q < 7 ? T(1.0 / 18.0) : T(1.0 / 36.0);
-            const T ax = kCx[q] > 0 ? T(1) - ux : (kCx[q] < 0 ? -T(1) - ux : -ux);
-            const T ay = kCy[q] > 0 ? T(1) - uy : (kCy[q] < 0 ? -T(1) - uy : -uy);
-            const T az = kCz[q] > 0 ? T(1) - uz : (kCz[q] < 0 ? -T(1) - uz : -uz);
-            const T S = wq * (ax * fx + ay * fy + az * fz) * t3 +
-                        wq * cdot(q, ux, uy, uz) * cdot(q, fx, fy, fz) * t9;
-            p[q] = p[q] - w * (p[q] - feq[q]) + gpf * S;
-        }
+        forced_bgk_node(p, w, fx, fy, fz);
     }
 #pragma unroll
     for (int q = 0; q < 19; ++q) f[c + q * P] = p[q];
+}
+
+// FP32, even Nx, 8-byte aligned fields: thread t updates the adjacent nodes
+// 2t, 2t + 1 of its row as two lanes (Lanes2), each as boussinesq_k does to
+// within 3 ulp; a solid node of the pair swaps its opposite populations.
+// Bounded to 4 blocks per SM (128 registers): 3 blocks at 164 registers ran
+// slower, 5 blocks spill 170-220 B.
+template <int MODE, typename I>
+__global__ void __launch_bounds__(BX, 4) boussinesq2_k(float *__restrict__ f, const float *__restrict__ Temp,
+                                                     const uint8_t *__restrict__ solid, Grid3 g,
+                                                     float w, float beta_g, float T_ref,
+                                                     const float *__restrict__ Fxf,
+                                                     const float *__restrict__ Fyf,
+                                                     const float *__restrict__ Fzf, float Fx,
+                                                     float Fy, float Fz) {
+    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i >= g.Nx) return;
+    const I c = (I)i + (I)g.Nx * ((I)j + (I)g.Ny * (I)k);
+    const I P = (I)g.plane;
+    Lanes2 p[19], o[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) p[q].v = *reinterpret_cast<const float2 *>(f + c + q * P);
+    const uchar2 sd = solid ? *reinterpret_cast<const uchar2 *>(solid + c) : make_uchar2(0, 0);
+    const auto ld2 = [&](const float *a) { return Lanes2::of(*reinterpret_cast<const float2 *>(a + c)); };
+#pragma unroll
+    for (int q = 0; q < 19; ++q) o[q] = p[q];
+    if (!(sd.x && sd.y)) {
+        const Lanes2 fx = MODE == 0 ? Lanes2(0.0) : (MODE == 1 ? Lanes2::of(make_float2(Fx, Fx)) : ld2(Fxf));
+        const Lanes2 fy = MODE == 0 ? Lanes2::of(make_float2(beta_g, beta_g)) * (ld2(Temp) - Lanes2::of(make_float2(T_ref, T_ref)))
+                                    : (MODE == 1 ? Lanes2::of(make_float2(Fy, Fy)) : ld2(Fyf));
+        const Lanes2 fz = MODE == 0 ? Lanes2(0.0) : (MODE == 1 ? Lanes2::of(make_float2(Fz, Fz)) : ld2(Fzf));
+        forced_bgk_node(o, Lanes2::of(make_float2(w, w)), fx, fy, fz);
+    }
+    if (sd.x || sd.y) {
+        swap_pairs(p);
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            if (sd.x) o[q].v.x = p[q].v.x;
+            if (sd.y) o[q].v.y = p[q].v.y;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 19; ++q) *reinterpret_cast<float2 *>(f + c + q * P) = o[q].v;
 }
 
 }  // namespace d3
@@ -934,15 +1012,53 @@ int kb_compute_temperature_3d(void *Temp, const void *g, int Nx, int Ny, int Nz,
             (T *)Temp, (const T *)g, grid3(Nx, Ny, Nz))));
 }
 
+}  // extern "C"
+
+namespace {
+
+template <typename T, int MODE>
+void launch_boussinesq_3d(T *f, const T *Temp, const uint8_t *solid, const Grid3 &g, T w, T beta_g,
+                          T T_ref, const T *Fxf, const T *Fyf, const T *Fzf, T Fx, T Fy, T Fz,
+                          cudaStream_t s) {
+    const bool i32 = offsets_fit_int(g, 19);
+    if constexpr (sizeof(T) == 4) {
+        // two nodes per thread where the rows pair up and the fields allow
+        // 8-byte accesses (the solid mask 2-byte)
+        const auto al = [](const void *p, uintptr_t n) { return ((uintptr_t)p & (n - 1)) == 0; };
+        if (g.Nx % 2 == 0 && al(f, 8) && al(Temp, 8) && al(Fxf, 8) && al(Fyf, 8) && al(Fzf, 8) &&
+            al(solid, 2)) {
+            const dim3 grid((unsigned)((g.Nx / 2 + BX - 1) / BX), (unsigned)g.Ny, (unsigned)g.Nz);
+            if (i32)
+                boussinesq2_k<MODE, int><<<grid, BX, 0, s>>>(f, Temp, solid, g, w, beta_g, T_ref, Fxf, Fyf,
+                                                             Fzf, Fx, Fy, Fz);
+            else
+                boussinesq2_k<MODE, size_t><<<grid, BX, 0, s>>>(f, Temp, solid, g, w, beta_g, T_ref, Fxf,
+                                                                Fyf, Fzf, Fx, Fy, Fz);
+            return;
+        }
+    }
+    const dim3 grid = nodes_grid(g.Nx, g.Ny, g.Nz);
+    if (i32)
+        boussinesq_k<T, MODE, int><<<grid, BX, 0, s>>>(f, Temp, solid, g, w, beta_g, T_ref, Fxf, Fyf,
+                                                       Fzf, Fx, Fy, Fz);
+    else
+        boussinesq_k<T, MODE, size_t><<<grid, BX, 0, s>>>(f, Temp, solid, g, w, beta_g, T_ref, Fxf,
+                                                          Fyf, Fzf, Fx, Fy, Fz);
+}
+
+}  // namespace
+
+extern "C" {
+
 int kb_collide_boussinesq_3d(void *f, const void *Temp, const uint8_t *is_solid, int Nx, int Ny,
                              int Nz, double omega, double beta_g, double T_ref, int dtype,
                              void *stream) {
     KB_REQUIRE(f && Temp, "kb_collide_boussinesq_3d: null pointer");
     if (int e = check_dims("kb_collide_boussinesq_3d", Nx, Ny, Nz)) return e;
     KB3_DISPATCH_PLAIN("kb_collide_boussinesq_3d", dtype,
-        (boussinesq_k<T, 0><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
-            (T *)f, (const T *)Temp, is_solid, grid3(Nx, Ny, Nz), (T)omega, (T)beta_g, (T)T_ref,
-            nullptr, nullptr, nullptr, T(0), T(0), T(0))));
+        (launch_boussinesq_3d<T, 0>((T *)f, (const T *)Temp, is_solid, grid3(Nx, Ny, Nz), (T)omega,
+                                    (T)beta_g, (T)T_ref, nullptr, nullptr, nullptr, T(0), T(0), T(0),
+                                    kb::as_stream(stream))));
 }
 
 int kb_collide_guo_3d(void *f, const uint8_t *is_solid, int Nx, int Ny, int Nz, double omega,
@@ -950,9 +1066,9 @@ int kb_collide_guo_3d(void *f, const uint8_t *is_solid, int Nx, int Ny, int Nz, 
     KB_REQUIRE(f, "kb_collide_guo_3d: null population pointer");
     if (int e = check_dims("kb_collide_guo_3d", Nx, Ny, Nz)) return e;
     KB3_DISPATCH_PLAIN("kb_collide_guo_3d", dtype,
-        (boussinesq_k<T, 1><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
-            (T *)f, nullptr, is_solid, grid3(Nx, Ny, Nz), (T)omega, T(0), T(0), nullptr,
-            nullptr, nullptr, (T)Fx, (T)Fy, (T)Fz)));
+        (launch_boussinesq_3d<T, 1>((T *)f, nullptr, is_solid, grid3(Nx, Ny, Nz), (T)omega, T(0), T(0),
+                                    nullptr, nullptr, nullptr, (T)Fx, (T)Fy, (T)Fz,
+                                    kb::as_stream(stream))));
 }
 
 int kb_collide_guo_field_3d(void *f, const uint8_t *is_solid, const void *Fx_field,
@@ -961,9 +1077,9 @@ int kb_collide_guo_field_3d(void *f, const uint8_t *is_solid, const void *Fx_fie
     KB_REQUIRE(f && Fx_field && Fy_field && Fz_field, "kb_collide_guo_field_3d: null pointer");
     if (int e = check_dims("kb_collide_guo_field_3d", Nx, Ny, Nz)) return e;
     KB3_DISPATCH_PLAIN("kb_collide_guo_field_3d", dtype,
-        (boussinesq_k<T, 2><<<nodes_grid(Nx, Ny, Nz), BX, 0, kb::as_stream(stream)>>>(
-            (T *)f, nullptr, is_solid, grid3(Nx, Ny, Nz), (T)omega, T(0), T(0),
-            (const T *)Fx_field, (const T *)Fy_field, (const T *)Fz_field, T(0), T(0), T(0))));
+        (launch_boussinesq_3d<T, 2>((T *)f, nullptr, is_solid, grid3(Nx, Ny, Nz), (T)omega, T(0), T(0),
+                                    (const T *)Fx_field, (const T *)Fy_field, (const T *)Fz_field,
+                                    T(0), T(0), T(0), kb::as_stream(stream))));
 }
 
 }  // extern "C"
