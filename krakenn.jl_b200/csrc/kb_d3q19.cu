@@ -646,9 +646,10 @@ __device__ __forceinline__ void forced_bgk_node(T *p, T w, T fx, T fy, T fz) {
 // MODE 1 collide_guo_3d_kernel! (src/kernels/collide_guo_3d.jl:5-186, constant
 // F), MODE 2 collide_guo_field_3d_kernel! (:199-323, per-node F).  The three
 // share the reference's operation order.  I: the element offset type (int
-// where the 19 planes fit in 32 bits).
+// where the 19 planes fit in 32 bits).  FP64 is bounded to 4 blocks per SM
+// (128 registers instead of 166 at 3 blocks).
 template <typename T, int MODE, typename I>
-__global__ void __launch_bounds__(BX) boussinesq_k(T *__restrict__ f, const T *__restrict__ Temp,
+__global__ void __launch_bounds__(BX, sizeof(T) == 8 ? 4 : 1) boussinesq_k(T *__restrict__ f, const T *__restrict__ Temp,
                                                     const uint8_t *__restrict__ solid, Grid3 g, T w,
                                                     T beta_g, T T_ref, const T *__restrict__ Fxf,
                                                     const T *__restrict__ Fyf,
