@@ -986,6 +986,54 @@ __global__ void __launch_bounds__(BX) guo_k(T *__restrict__ f, const uint8_t *__
     for (int q = 0; q < 9; ++q) f[c + q * P] = p[q];
 }
 
+// FP32 forced BGK of two adjacent nodes per thread (even Nx, 8-byte aligned
+// fields) as two lanes (Lanes2): KIND 0 collide_boussinesq_2d (force
+// (0, beta_g (T - T_ref)), omega), 1 collide_guo_2d (constant force), 2
+// collide_guo_field_2d (per-node force).  Each lane evaluates the expression
+// tree of boussinesq_k / guo_k, with packed round-to-nearest adds and
+// multiplies, to within 3 ulp of them; a solid node of the pair swaps its
+// opposite populations.  I: the element offset type.
+template <int KIND, typename I>
+__global__ void __launch_bounds__(BX) forced2_k(float *__restrict__ f, const float *__restrict__ Temp,
+                                                 const uint8_t *__restrict__ solid,
+                                                 const float *__restrict__ Fxf,
+                                                 const float *__restrict__ Fyf, Grid2<float> g,
+                                                 float omega, float beta_g, float T_ref, float Fx,
+                                                 float Fy) {
+    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int j = blockIdx.y;
+    if (i >= g.Nx) return;
+    const I c = (I)i + (I)g.Nx * (I)j;
+    const I P = (I)g.plane;
+    Lanes2 p[9], o[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) p[q].v = *reinterpret_cast<const float2 *>(f + c + q * P);
+    const uchar2 sd = solid ? *reinterpret_cast<const uchar2 *>(solid + c) : make_uchar2(0, 0);
+    const auto ld2 = [&](const float *a) { return Lanes2::of(*reinterpret_cast<const float2 *>(a + c)); };
+    const auto sp = [](float x) { return Lanes2::of(make_float2(x, x)); };
+#pragma unroll
+    for (int q = 0; q < 9; ++q) o[q] = p[q];
+    if (!(sd.x && sd.y)) {
+        const Lanes2 fx = KIND == 0 ? Lanes2(0.0) : (KIND == 1 ? sp(Fx) : ld2(Fxf));
+        const Lanes2 fy = KIND == 0 ? sp(beta_g) * (ld2(Temp) - sp(T_ref)) : (KIND == 1 ? sp(Fy) : ld2(Fyf));
+        const Lanes2 rho = o[0] + o[1] + o[2] + o[3] + o[4] + o[5] + o[6] + o[7] + o[8];
+        const Lanes2 inv = Lanes2(1.0) / rho;
+        const Lanes2 a = ((o[1] - o[3] + o[5] - o[6] - o[7] + o[8]) + fx / Lanes2(2.0)) * inv;
+        const Lanes2 b = ((o[2] - o[4] + o[5] + o[6] - o[7] - o[8]) + fy / Lanes2(2.0)) * inv;
+        collide_guo(o, rho, a, b, fx, fy, sp(omega));
+    }
+    if (sd.x || sd.y) {
+        swap_pairs(p);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            if (sd.x) o[q].v.x = p[q].v.x;
+            if (sd.y) o[q].v.y = p[q].v.y;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) *reinterpret_cast<float2 *>(f + c + q * P) = o[q].v;
+}
+
 }  // namespace d2
 }  // namespace kb
 
@@ -1003,6 +1051,35 @@ Grid2<T> grid2(int Nx, int Ny) {
 
 inline dim3 nodes_grid(int Nx, int Ny) { return dim3((Nx + BX - 1) / BX, Ny); }
 inline unsigned line_grid(int n) { return (unsigned)((n + BX - 1) / BX); }
+
+// Forced BGK (KIND 0 Boussinesq, 1 constant Guo force, 2 per-node Guo force):
+// FP32 on even Nx with 8-byte aligned fields takes two nodes per thread
+// (forced2_k), everything else one node per thread.
+template <typename T, int KIND>
+void launch_forced_2d(T *f, const T *Temp, const uint8_t *solid, const T *Fxf, const T *Fyf, int Nx,
+                      int Ny, T omega, T beta_g, T T_ref, T Fx, T Fy, cudaStream_t s) {
+    const Grid2<T> g = grid2<T>(Nx, Ny);
+    if constexpr (sizeof(T) == 4) {
+        const auto al = [](const void *q, uintptr_t n) { return ((uintptr_t)q & (n - 1)) == 0; };
+        if (Nx % 2 == 0 && al(f, 8) && al(Temp, 8) && al(Fxf, 8) && al(Fyf, 8) && al(solid, 2)) {
+            const dim3 grid((unsigned)((Nx / 2 + BX - 1) / BX), (unsigned)Ny);
+            if (9.0 * (double)g.plane < 2147483647.0)
+                forced2_k<KIND, int><<<grid, BX, 0, s>>>(f, Temp, solid, Fxf, Fyf, g, omega, beta_g,
+                                                         T_ref, Fx, Fy);
+            else
+                forced2_k<KIND, size_t><<<grid, BX, 0, s>>>(f, Temp, solid, Fxf, Fyf, g, omega, beta_g,
+                                                            T_ref, Fx, Fy);
+            return;
+        }
+    }
+    if (KIND == 0)
+        boussinesq_k<T, 0><<<nodes_grid(Nx, Ny), BX, 0, s>>>(f, Temp, solid, g, omega, T(0), T(0), T(0),
+                                                             beta_g, T_ref);
+    else if (KIND == 1)
+        guo_k<T, false><<<nodes_grid(Nx, Ny), BX, 0, s>>>(f, solid, nullptr, nullptr, g, omega, Fx, Fy);
+    else
+        guo_k<T, true><<<nodes_grid(Nx, Ny), BX, 0, s>>>(f, solid, Fxf, Fyf, g, omega, T(0), T(0));
+}
 
 int check_dims(const char *what, int Nx, int Ny) {
     if (Nx < 1 || Ny < 1 || Ny > 65535)
@@ -1471,9 +1548,8 @@ int kb_collide_boussinesq_2d(void *f, const void *Temp, const uint8_t *is_solid,
     KB_REQUIRE(f && Temp, "kb_collide_boussinesq_2d: null pointer");
     if (int e = check_dims("kb_collide_boussinesq_2d", Nx, Ny)) return e;
     KB_DISPATCH_PLAIN("kb_collide_boussinesq_2d", dtype,
-        (boussinesq_k<T, 0><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
-            (T *)f, (const T *)Temp, is_solid, grid2<T>(Nx, Ny), (T)omega, T(0), T(0), T(0),
-            (T)beta_g, (T)T_ref)));
+        (launch_forced_2d<T, 0>((T *)f, (const T *)Temp, is_solid, nullptr, nullptr, Nx, Ny, (T)omega,
+                                (T)beta_g, (T)T_ref, T(0), T(0), kb::as_stream(stream))));
 }
 
 int kb_collide_boussinesq_vt_2d(void *f, const void *Temp, const uint8_t *is_solid, int Nx, int Ny,
@@ -1508,8 +1584,8 @@ int kb_collide_guo_2d(void *f, const uint8_t *is_solid, int Nx, int Ny, double o
     KB_REQUIRE(f, "kb_collide_guo_2d: null population pointer");
     if (int e = check_dims("kb_collide_guo_2d", Nx, Ny)) return e;
     KB_DISPATCH_PLAIN("kb_collide_guo_2d", dtype,
-        (guo_k<T, false><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
-            (T *)f, is_solid, nullptr, nullptr, grid2<T>(Nx, Ny), (T)omega, (T)Fx, (T)Fy)));
+        (launch_forced_2d<T, 1>((T *)f, nullptr, is_solid, nullptr, nullptr, Nx, Ny, (T)omega, T(0), T(0),
+                                (T)Fx, (T)Fy, kb::as_stream(stream))));
 }
 
 int kb_collide_guo_field_2d(void *f, const uint8_t *is_solid, const void *Fx_field,
@@ -1518,9 +1594,8 @@ int kb_collide_guo_field_2d(void *f, const uint8_t *is_solid, const void *Fx_fie
     KB_REQUIRE(f && Fx_field && Fy_field, "kb_collide_guo_field_2d: null pointer");
     if (int e = check_dims("kb_collide_guo_field_2d", Nx, Ny)) return e;
     KB_DISPATCH_PLAIN("kb_collide_guo_field_2d", dtype,
-        (guo_k<T, true><<<nodes_grid(Nx, Ny), BX, 0, kb::as_stream(stream)>>>(
-            (T *)f, is_solid, (const T *)Fx_field, (const T *)Fy_field, grid2<T>(Nx, Ny),
-            (T)omega, T(0), T(0))));
+        (launch_forced_2d<T, 2>((T *)f, nullptr, is_solid, (const T *)Fx_field, (const T *)Fy_field, Nx,
+                                Ny, (T)omega, T(0), T(0), T(0), T(0), kb::as_stream(stream))));
 }
 
 }  // extern "C"

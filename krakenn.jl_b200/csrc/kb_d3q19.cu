@@ -583,27 +583,6 @@ __global__ void fixed_temp_k(T *__restrict__ gg, Grid3 g, FixedTempSet3<T> S) {
     }
 }
 
-// Two FP32 lanes (adjacent nodes) with the operators of the reference
-// arithmetic: packed round-to-nearest adds and multiplies (never contracted)
-// and a per-lane division, so a helper written for T evaluates, with
-// T = Lanes2, the same expression tree for each node at half the arithmetic
-// instructions.  Measured against the one-node kernel the results agree to
-// 3 ulp; about 1 % of the updated populations (never the rest population)
-// differ in the last bits.
-struct Lanes2 {
-    float2 v;
-    __device__ __forceinline__ Lanes2() {}
-    __device__ __forceinline__ Lanes2(double d) { const float x = (float)d; v = make_float2(x, x); }
-    __device__ __forceinline__ static Lanes2 of(float2 a) { Lanes2 r; r.v = a; return r; }
-    __device__ __forceinline__ Lanes2 operator-() const { return of(make_float2(-v.x, -v.y)); }
-};
-__device__ __forceinline__ Lanes2 operator+(Lanes2 a, Lanes2 b) { return Lanes2::of(vadd(a.v, b.v)); }
-__device__ __forceinline__ Lanes2 operator-(Lanes2 a, Lanes2 b) { return Lanes2::of(vsub(a.v, b.v)); }
-__device__ __forceinline__ Lanes2 operator*(Lanes2 a, Lanes2 b) { return Lanes2::of(vmul(a.v, b.v)); }
-__device__ __forceinline__ Lanes2 operator/(Lanes2 a, Lanes2 b) {
-    return Lanes2::of(make_float2(a.v.x / b.v.x, a.v.y / b.v.y));
-}
-
 // The forced BGK update of one node (or two lanes) in place, force (fx, fy,
 // fz): the body of collide_boussinesq_3d_kernel! / collide_guo_3d_kernel!
 // after the force is known.

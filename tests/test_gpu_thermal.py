@@ -275,3 +275,40 @@ def test_f32_forced_collisions_two_lanes_match_one_node_kernel(cuda, pkg, with_m
         if m is not None:
             s = _h(m).astype(bool)
             assert np.array_equal(A[:, s], B[:, s])
+
+
+@pytest.mark.parametrize("with_mask", [False, True])
+def test_f32_forced_collisions_2d_two_lanes_match_one_node_kernel(cuda, pkg, with_mask):
+    """FP32 forced BGK in 2D (Boussinesq, constant and per-node Guo force):
+    the two-node kernel (even Nx, 8-byte aligned fields, packed FP32x2
+    arithmetic) and the one-node kernel (the same populations one element off
+    the 8-byte boundary) agree to 4 ulp, solid nodes (pairs with one or two
+    solid nodes) bit for bit."""
+    Nx, Ny = 66, 24
+    shape = (Ny, Nx)
+    rng = np.random.default_rng(41)
+    f = (W9[:, None, None] * (1 + 0.05 * rng.standard_normal((9,) + shape))).astype(np.float32)
+    Temp = torch.from_numpy((0.5 + 0.3 * rng.random(shape)).astype(np.float32)).to(cuda)
+    F = [torch.from_numpy((1e-3 * rng.standard_normal(shape)).astype(np.float32)).to(cuda) for _ in range(2)]
+    m = _g(_mask(shape, 17), torch.uint8) if with_mask else None
+
+    def pair():
+        a = torch.from_numpy(f.copy()).to(cuda)
+        buf = torch.empty(f.size + 1, dtype=torch.float32, device=cuda)
+        b = buf[1:].view(f.shape)
+        b.copy_(a)
+        assert a.data_ptr() % 8 == 0 and b.data_ptr() % 8 == 4
+        return a, b
+
+    for run in (lambda x: pkg.collide_boussinesq_2d_(x, Temp, m, 1.33, 4e-4, 0.5),
+                lambda x: pkg.collide_guo_2d_(x, m, 1.27, 2e-4, -1e-4),
+                lambda x: pkg.collide_guo_field_2d_(x, m, *F, 1.27)):
+        a, b = pair()
+        run(a)
+        run(b)
+        A, B = _h(a), _h(b)
+        ulp = np.spacing(np.maximum(np.abs(A), np.abs(B)).astype(np.float32))
+        assert np.all(np.abs(A - B) <= 4 * ulp)
+        if m is not None:
+            s = _h(m).astype(bool)
+            assert np.array_equal(A[:, s], B[:, s])
