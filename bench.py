@@ -1433,6 +1433,9 @@ def run_other(args):
         if rank == 0:
             r = bench_libb(pkg, N=args.grid, R=40.0 * args.grid / 256,
                            steps=min(max(args.steps, 20), 200), warmup=args.warmup)
+    elif args.workload == "thermal":
+        if rank == 0:
+            r = bench_thermal_guo_paths(pkg, steps=min(max(args.steps, 4), 200), warmup=args.warmup)
     elif rank == 0:
         r = bench_natconv_validation(pkg)
     if rank == 0:
@@ -1468,7 +1471,7 @@ def main():
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the short measurements of the other configurations")
     ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "cavity2d", "batch", "natconv", "warmstart", "surrogate", "slab", "slab2d",
-                             "libb", "output"])
+                             "libb", "output", "thermal"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
