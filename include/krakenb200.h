@@ -135,7 +135,12 @@ int kb_fused_trt_step(void *f_out, const void *f_in, void *rho, void *ux, void *
                       void *stream);
 
 /* collide_guo_2d!(f, is_solid, omega, Fx, Fy) -- src/kernels/collide_guo_2d.jl:5-90:
- * in-place BGK with the Guo source of a constant body force. */
+ * in-place BGK with the Guo source of a constant body force.
+ * The forced collisions (kb_collide_guo_*, kb_collide_boussinesq_2d/_3d) in
+ * KB_F64 give the reference arithmetic bit for bit.  In KB_F32, on an even Nx
+ * with 8-byte aligned fields (2-byte aligned mask), two adjacent nodes are
+ * updated per thread in packed FP32x2 round-to-nearest arithmetic: the same
+ * operations, within 3 ulp of the one-node form. */
 int kb_collide_guo_2d(void *f, const uint8_t *is_solid, int Nx, int Ny, double omega, double Fx,
                       double Fy, int dtype, void *stream);
 
